@@ -1,0 +1,224 @@
+"""Seeded synthetic inputs for the solve path, in the reference's ``hfmIn`` key vocabulary.
+
+Every generator returns a plain ``dict`` of numpy float64 arrays / scalars / strings that can be
+handed unchanged to the reference's FileHFM executables (``arrayOrdering='RowMajor'``, arrays
+indexed ``[i, j(, k)]`` along x, y(, z|theta)) or to :class:`hamiltonfastmarching_b200.HFMIO`.
+
+Conventions (shared by the tests, the benchmark and the golden-vector script):
+
+* grid points sit at cell centres ``x_i = origin + (i + 1/2) h`` (reference ``BaseGrid.h:69-75``);
+* a *smooth field* is ``K**-0.5 * sum_k A_k cos(2 pi k.x + phi_k)`` over ``K`` random integer
+  wave vectors with ``|k|_inf <= 4``, ``A_k ~ N(0,1)``, ``phi_k ~ U[0, 2 pi)``;
+* symmetric matrices are packed in the reference's order ``(xx, xy, yy[, xz, yz, zz])``
+  (``SymmetricMatrixType.hxx:11-16``), component axis last.
+
+No public dataset is involved; these stand in for the workloads the benchmarks are quoted on.
+"""
+from __future__ import annotations
+
+import math
+from typing import Dict, Tuple
+
+import numpy as np
+
+__all__ = [
+    "smooth_field",
+    "riemann2_case",
+    "riemann3_case",
+    "tubular_image",
+    "curvature2_case",
+    "pack_sym2",
+    "pack_sym3",
+]
+
+
+def _grid_axes(shape, h, origin=None):
+    origin = np.zeros(len(shape)) if origin is None else np.asarray(origin, float)
+    return [origin[d] + (np.arange(n) + 0.5) * h for d, n in enumerate(shape)]
+
+
+def smooth_field(rng: np.random.Generator, shape, h, K: int = 8, kmax: int = 4,
+                 dtype=np.float64) -> np.ndarray:
+    """Sum of ``K`` random-phase Fourier modes on the unit-periodic domain, normalised by sqrt(K)."""
+    axes = _grid_axes(shape, h)
+    d = len(shape)
+    out = np.zeros(shape, dtype=dtype)
+    for _ in range(K):
+        k = rng.integers(-kmax, kmax + 1, size=d)
+        amp = rng.standard_normal()
+        phase = rng.uniform(0.0, 2.0 * math.pi)
+        # cos(sum_d a_d + phase) evaluated by broadcasting 1-D phase ramps
+        arg = np.full((1,) * d, phase, dtype=dtype)
+        for ax in range(d):
+            sh = [1] * d
+            sh[ax] = shape[ax]
+            arg = arg + (2.0 * math.pi * k[ax] * axes[ax]).reshape(sh).astype(dtype)
+        out += amp * np.cos(arg)
+    out /= math.sqrt(K)
+    return out
+
+
+def pack_sym2(m00, m01, m11) -> np.ndarray:
+    return np.stack([m00, m01, m11], axis=-1)
+
+
+def pack_sym3(m00, m01, m11, m02, m12, m22) -> np.ndarray:
+    return np.stack([m00, m01, m11, m02, m12, m22], axis=-1)
+
+
+def riemann2_case(n: int = 256, aniso: float = 5.0, seed: int = 0, n_seeds: int = 1,
+                  seed_points=None) -> Dict:
+    """Riemann2 on [0,1]^2, M = R(theta) diag(1, 1/a^2) R(theta)^T with smooth random theta.
+
+    Default arguments reproduce the 256x256, a=5, single centre seed workload.
+    """
+    rng = np.random.default_rng(seed)
+    h = 1.0 / n
+    theta = math.pi * smooth_field(rng, (n, n), h)
+    c, s = np.cos(theta), np.sin(theta)
+    l0, l1 = 1.0, 1.0 / aniso ** 2
+    m00 = l0 * c * c + l1 * s * s
+    m01 = (l0 - l1) * c * s
+    m11 = l0 * s * s + l1 * c * c
+    if seed_points is None:
+        if n_seeds == 1:
+            seed_points = np.array([[0.5, 0.5]])
+        else:
+            seed_points = rng.uniform(0.05, 0.95, size=(n_seeds, 2))
+    return {
+        "model": "Riemann2",
+        "arrayOrdering": "RowMajor",
+        "dims": np.array([n, n], dtype=float),
+        "gridScale": h,
+        "metric": pack_sym2(m00, m01, m11),
+        "seeds": np.asarray(seed_points, dtype=float),
+        "exportValues": 1.0,
+    }
+
+
+def _rodrigues(wx, wy, wz):
+    """Rotation matrices exp(skew(w)) for fields of axis-angle vectors (returns 3x3 nested lists)."""
+    th = np.sqrt(wx * wx + wy * wy + wz * wz)
+    small = th < 1e-12
+    ths = np.where(small, 1.0, th)
+    kx, ky, kz = wx / ths, wy / ths, wz / ths
+    c, s = np.cos(th), np.sin(th)
+    v = 1.0 - c
+    R = [[c + kx * kx * v, kx * ky * v - kz * s, kx * kz * v + ky * s],
+         [ky * kx * v + kz * s, c + ky * ky * v, ky * kz * v - kx * s],
+         [kz * kx * v - ky * s, kz * ky * v + kx * s, c + kz * kz * v]]
+    one = np.ones_like(th)
+    zero = np.zeros_like(th)
+    eye = [[one, zero, zero], [zero, one, zero], [zero, zero, one]]
+    return [[np.where(small, eye[i][j], R[i][j]) for j in range(3)] for i in range(3)]
+
+
+def riemann3_case(n: int = 192, seed: int = 1, n_spheres: int = 40, n_seeds: int = 16,
+                  rmin: float = 0.02, rmax: float = 0.08, walls: bool = True) -> Dict:
+    """Riemann3 on [0,1]^3 with M = R diag(1, a1^-2, a2^-2) R^T, spherical walls and random seeds.
+
+    a1, a2 = exp(ln 20 * (1/2 + 1/2 tanh(smooth))) lie in [1, 20]; R = exp(skew(pi * smooth^3)).
+    Walls are the union of ``n_spheres`` balls (centres U[0,1]^3, radii U[rmin, rmax]);
+    seeds are uniform points whose cell is not a wall.
+    """
+    rng = np.random.default_rng(seed)
+    h = 1.0 / n
+    shape = (n, n, n)
+    f = lambda: smooth_field(rng, shape, h)
+    a1 = np.exp(math.log(20.0) * (0.5 + 0.5 * np.tanh(f())))
+    a2 = np.exp(math.log(20.0) * (0.5 + 0.5 * np.tanh(f())))
+    w = [math.pi * f() for _ in range(3)]
+    R = _rodrigues(*w)
+    lam = [np.ones(shape), a1 ** -2, a2 ** -2]
+    del a1, a2, w
+
+    def m(i, j):
+        return sum(R[i][k] * lam[k] * R[j][k] for k in range(3))
+
+    metric = pack_sym3(m(0, 0), m(0, 1), m(1, 1), m(0, 2), m(1, 2), m(2, 2))
+    del R, lam
+    out = {
+        "model": "Riemann3",
+        "arrayOrdering": "RowMajor",
+        "dims": np.array([n, n, n], dtype=float),
+        "gridScale": h,
+        "metric": metric,
+        "exportValues": 1.0,
+    }
+    wall = np.zeros(shape, dtype=bool)
+    if walls and n_spheres > 0:
+        ax = _grid_axes(shape, h)
+        centres = rng.uniform(0.0, 1.0, size=(n_spheres, 3))
+        radii = rng.uniform(rmin, rmax, size=n_spheres)
+        for c, r in zip(centres, radii):
+            lo = np.clip(np.floor((c - r) / h).astype(int) - 1, 0, n)
+            hi = np.clip(np.ceil((c + r) / h).astype(int) + 1, 0, n)
+            X = ax[0][lo[0]:hi[0]].reshape(-1, 1, 1)
+            Y = ax[1][lo[1]:hi[1]].reshape(1, -1, 1)
+            Z = ax[2][lo[2]:hi[2]].reshape(1, 1, -1)
+            inside = (X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r
+            wall[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] |= inside
+        out["walls"] = wall.astype(float)
+    seeds = []
+    while len(seeds) < n_seeds:
+        p = rng.uniform(0.0, 1.0, size=3)
+        idx = np.minimum((p / h).astype(int), n - 1)
+        if not wall[tuple(idx)]:
+            seeds.append(p)
+    out["seeds"] = np.array(seeds, dtype=float)
+    return out
+
+
+def tubular_image(rng: np.random.Generator, n: int, n_curves: int = 20, width_px: float = 2.0,
+                  samples: int = 400) -> np.ndarray:
+    """Max over random cubic Bezier curves of the Gaussian profile exp(-d^2 / (2 (width h)^2))."""
+    h = 1.0 / n
+    ax = (np.arange(n) + 0.5) * h
+    X, Y = np.meshgrid(ax, ax, indexing="ij")
+    img = np.zeros((n, n))
+    sig = width_px * h
+    t = np.linspace(0.0, 1.0, samples)
+    b = np.stack([(1 - t) ** 3, 3 * t * (1 - t) ** 2, 3 * t ** 2 * (1 - t), t ** 3], axis=1)
+    for _ in range(n_curves):
+        P = rng.uniform(0.0, 1.0, size=(4, 2))
+        curve = b @ P  # (samples, 2)
+        d2 = np.full((n, n), np.inf)
+        # distance to the sampled polyline, evaluated on a bounding window only
+        lo = np.clip(((curve.min(0) - 4 * sig) / h).astype(int), 0, n)
+        hi = np.clip(((curve.max(0) + 4 * sig) / h).astype(int) + 1, 0, n)
+        Xw = X[lo[0]:hi[0], lo[1]:hi[1]]
+        Yw = Y[lo[0]:hi[0], lo[1]:hi[1]]
+        dw = np.full(Xw.shape, np.inf)
+        for q in curve:
+            np.minimum(dw, (Xw - q[0]) ** 2 + (Yw - q[1]) ** 2, out=dw)
+        d2[lo[0]:hi[0], lo[1]:hi[1]] = dw
+        np.maximum(img, np.exp(-d2 / (2.0 * sig * sig)), out=img)
+    return img
+
+
+def curvature2_case(n: int = 128, ntheta: int = 60, model: str = "ReedsShepp2", seed: int = 2,
+                    xi: float = 0.1, eps: float = 0.1, n_curves: int = 20, n_seeds: int = 1,
+                    seed_points=None) -> Dict:
+    """ReedsShepp2 / Elastica2 on the lifted grid (x, y, theta) of n x n x ntheta points.
+
+    The cost is the physical (n, n) field 1/(0.05 + I) with I a synthetic tubular image;
+    seeds are full (x, y, theta) points.
+    """
+    rng = np.random.default_rng(seed)
+    img = tubular_image(rng, n, n_curves=n_curves)
+    cost = 1.0 / (0.05 + img)
+    if seed_points is None:
+        pts = rng.uniform(0.2, 0.8, size=(n_seeds, 2))
+        th = rng.uniform(0.0, 2.0 * math.pi, size=(n_seeds, 1))
+        seed_points = np.concatenate([pts, th], axis=1)
+    return {
+        "model": model,
+        "arrayOrdering": "RowMajor",
+        "dims": np.array([n, n, ntheta], dtype=float),
+        "gridScale": 1.0 / n,
+        "xi": float(xi),
+        "eps": float(eps),
+        "cost": cost,
+        "seeds": np.asarray(seed_points, dtype=float),
+        "exportValues": 1.0,
+    }

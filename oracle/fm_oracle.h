@@ -1,0 +1,75 @@
+/* CPU restatement of the reference solve path (test infrastructure, never shipped).
+ *
+ * This oracle restates, in plain C99, the arithmetic of the reference's sequential fast-marching
+ * path for Eulerian schemes so that tests can check the CUDA path against it in-process:
+ *   - Selling / Voronoi stencil construction (2D and 3D), Riemann metric rescaling, the
+ *     relaxed rank-one (Voronoi1Vec) stencils of the curvature models;
+ *   - wall distance and line-of-sight visibility;
+ *   - Dijkstra-ordered fast marching with the incremental Hopf-Lax quadratic solve, using the
+ *     same binary-heap algorithm as libstdc++'s std::priority_queue so that tie order matches;
+ *   - the reverse-mode first variation (costSensitivity).
+ * Each function cites the reference file:line it follows. Compiled with -ffp-contract=off.
+ */
+#ifndef HFM_FM_ORACLE_H
+#define HFM_FM_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Selling decomposition of a packed SPD matrix (xx,xy,yy[,xz,yz,zz]) into 3 (2D) or 6 (3D)
+ * integer offsets and weights, including the 1000*eps*Tr tolerance. Returns 0, or -1 if the
+ * matrix is rejected (non positive determinant/trace) or Selling did not terminate. */
+int fmo_selling_mat(int ndim, const double *d, int8_t *offsets, double *weights);
+
+/* Riemann stencil at one point: packed metric (or dual metric), grid scales h[ndim]. */
+int fmo_riemann_stencil(int ndim, const double *metric, int dual, const double *h,
+                        int8_t *offsets, double *weights);
+
+/* Voronoi1Vec: relaxed rank-one decomposition with reorientation (<v,e> <= 0). */
+int fmo_voronoi1vec(int ndim, const double *v, double eps, int8_t *offsets, double *weights);
+
+/* Per-angle stencil tables of the curvature models, nd = 3 components per offset.
+ * ReedsShepp2: 4 symmetric differences per angle. Elastica2<5>: 27 forward differences. */
+int fmo_reedsshepp2_table(int ntheta, double h, double xi, double eps, int projective,
+                          int8_t *offsets, double *weights);
+int fmo_elastica2_table(int ntheta, double h, double xi, double eps,
+                        int8_t *offsets, double *weights);
+
+typedef struct {
+    int ndim;
+    int64_t dims[3];
+    int periodic[3];
+    int nfwd, nsym;            /* differences per stencil: forward first, then symmetric */
+    int share;                 /* 0: one stencil per cell, 1: one stencil per index of the last axis */
+    const int8_t *off;         /* [nstencil][nfwd+nsym][3] */
+    const double *w;           /* [nstencil][nfwd+nsym] base weights */
+    const double *mult;        /* [N] speed multiplier (weights scale by mult^2) or NULL */
+    const uint8_t *walls;      /* [N] or NULL */
+    int nseeds;
+    const int64_t *seed_index; /* row-major linear indices */
+    const double *seed_value;
+} fmo_problem;
+
+/* Fast marching. values[N] out; active[N] out (bitset, forward bits then symmetric +/- pairs,
+ * as the reference's ActiveNeighFlagType) may be NULL. Returns accepted count, or -1. */
+int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active,
+                          int *max_stencil_width);
+
+/* Reverse first variation from weighted points (linear indices). sensitivity[N] out;
+ * seed_out_index/seed_out_weight receive up to max_seeds sensitive seeds. Returns the number of
+ * sensitive seeds, or -1. */
+int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const uint64_t *active,
+                               int npts, const int64_t *pt_index, const double *pt_weight,
+                               double *sensitivity, int64_t max_seeds, int64_t *seed_out_index,
+                               double *seed_out_weight);
+
+/* Wall distance (capped BFS) and visibility, exposed for tests of the visibility kernel.
+ * visible[N][nfwd + 2*nsym] receives 1 if the neighbour (x+e) may update x. */
+int fmo_visibility(const fmo_problem *p, int max_width, uint8_t *visible);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

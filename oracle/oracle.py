@@ -1,0 +1,312 @@
+"""ctypes front-end of the C oracle (``oracle/fm_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: used by ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s
+CPU-baseline leg as the checker; the product path never imports it.
+
+:func:`solve` takes an ``hfmIn``-style dict (RowMajor arrays) and reproduces the reference's
+``Run`` for the Eulerian models Riemann2/3, ReedsShepp2, Elastica2 (and Isotropic2 as a
+Riemann metric ``cost^2 Id``) with seeds and walls: the input semantics follow
+``Headers/Base/Implementation/HFM_ParamDefault.hxx`` (point -> index), ``StaticFactoring.hxx:242-393``
+(seeds), ``HFM_StencilShare.hxx:61-71`` (speed = 1/cost), ``WallObstructionTest.h:30-36`` (walls).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from typing import Dict
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle_fm.so")
+_lib = None
+
+_P = ctypes.c_void_p
+
+
+class _Problem(ctypes.Structure):
+    _fields_ = [
+        ("ndim", ctypes.c_int),
+        ("dims", ctypes.c_int64 * 3),
+        ("periodic", ctypes.c_int * 3),
+        ("nfwd", ctypes.c_int),
+        ("nsym", ctypes.c_int),
+        ("share", ctypes.c_int),
+        ("off", _P),
+        ("w", _P),
+        ("mult", _P),
+        ("walls", _P),
+        ("nseeds", ctypes.c_int),
+        ("seed_index", _P),
+        ("seed_value", _P),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle shared library (``make -C oracle``) if needed; returns its path."""
+    src = os.path.join(_HERE, "fm_oracle.c")
+    if (not os.path.exists(_LIB_PATH)) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.fmo_selling_mat.argtypes = [ctypes.c_int, _P, _P, _P]
+        L.fmo_riemann_stencils.argtypes = [ctypes.c_int, ctypes.c_int64, _P, ctypes.c_int, _P, _P, _P]
+        L.fmo_voronoi1vec.argtypes = [ctypes.c_int, _P, ctypes.c_double, _P, _P]
+        L.fmo_reedsshepp2_table.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, _P, _P]
+        L.fmo_elastica2_table.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, _P, _P]
+        L.fmo_fast_marching.argtypes = [ctypes.POINTER(_Problem), _P, _P, _P]
+        L.fmo_fast_marching.restype = ctypes.c_int64
+        L.fmo_backward_variation.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, _P,
+                                             _P, ctypes.c_int64, _P, _P]
+        L.fmo_backward_variation.restype = ctypes.c_int64
+        L.fmo_visibility.argtypes = [ctypes.POINTER(_Problem), ctypes.c_int, _P]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ----------------------------------------------------------------------------------- stencils
+
+def selling(mats: np.ndarray, ndim: int):
+    """Selling decomposition of packed SPD matrices ``(..., 3|6)`` -> offsets (..., k, 3) int8, weights."""
+    mats = np.ascontiguousarray(mats, dtype=np.float64)
+    ns = 3 if ndim == 2 else 6
+    nk = 3 if ndim == 2 else 6
+    flat = mats.reshape(-1, ns)
+    off = np.zeros((flat.shape[0], nk, 3), np.int8)
+    w = np.zeros((flat.shape[0], nk), np.float64)
+    L = lib()
+    for i in range(flat.shape[0]):
+        row = np.ascontiguousarray(flat[i])
+        if L.fmo_selling_mat(ndim, _ptr(row), _ptr(off[i]), _ptr(w[i])):
+            raise ValueError(f"matrix {i} is not positive definite")
+    return off.reshape(mats.shape[:-1] + (nk, 3)), w.reshape(mats.shape[:-1] + (nk,))
+
+
+def riemann_stencils(metric: np.ndarray, h, dual: bool = False):
+    ndim = 2 if metric.shape[-1] == 3 else 3
+    nk = 3 if ndim == 2 else 6
+    metric = np.ascontiguousarray(metric, dtype=np.float64)
+    n = int(np.prod(metric.shape[:-1]))
+    h = np.ascontiguousarray(np.broadcast_to(np.asarray(h, float), (ndim,)), dtype=np.float64)
+    off = np.zeros((n, nk, 3), np.int8)
+    w = np.zeros((n, nk), np.float64)
+    if lib().fmo_riemann_stencils(ndim, n, _ptr(metric), int(dual), _ptr(h), _ptr(off), _ptr(w)):
+        raise ValueError("ObtuseSuperbase error : input must be positive definite")
+    return off, w
+
+
+def curvature2_table(model: str, ntheta: int, h: float, xi: float, eps: float, projective=False):
+    L = lib()
+    if model == "ReedsShepp2":
+        off = np.zeros((ntheta, 4, 3), np.int8)
+        w = np.zeros((ntheta, 4), np.float64)
+        rc = L.fmo_reedsshepp2_table(ntheta, h, xi, eps, int(projective), _ptr(off), _ptr(w))
+    elif model == "Elastica2":
+        off = np.zeros((ntheta, 27, 3), np.int8)
+        w = np.zeros((ntheta, 27), np.float64)
+        rc = L.fmo_elastica2_table(ntheta, h, xi, eps, _ptr(off), _ptr(w))
+    else:
+        raise ValueError(model)
+    if rc:
+        raise ValueError("stencil construction failed")
+    return off, w
+
+
+# ----------------------------------------------------------------------------------- problems
+
+def _get(params, key, default=None):
+    return params[key] if key in params else default
+
+
+def _seed_indices(params, adim, dims, periodic):
+    """Seeds -> unique row-major indices in increasing order, first value kept
+    (``StaticFactoring.hxx:256-274, 384-390``; std::map insert semantics)."""
+    if "seeds" not in params:
+        return np.zeros(0, np.int64), np.zeros(0)
+    pts = np.atleast_2d(np.asarray(params["seeds"], float))
+    vals = np.asarray(_get(params, "seedValues", np.zeros(len(pts))), float).ravel()
+    if len(vals) != len(pts):
+        raise ValueError("Error : Inconsistent size of seedValues.")
+    seen = {}
+    for p, v in zip(pts, vals):
+        q = adim(p)
+        idx = [int(math.floor(c)) for c in q]
+        ok = True
+        for a, n in enumerate(dims):
+            if periodic[a]:
+                idx[a] %= n
+            elif not (0 <= idx[a] < n):
+                ok = False
+        if not ok:
+            continue
+        lin = int(np.ravel_multi_index(tuple(idx), dims))
+        seen.setdefault(lin, float(v))
+    keys = sorted(seen)
+    return np.array(keys, np.int64), np.array([seen[k] for k in keys], float)
+
+
+class Problem:
+    """Owns the arrays referenced by the C problem structure."""
+
+    def __init__(self, params: Dict):
+        model = params["model"]
+        dims = tuple(int(round(d)) for d in np.asarray(params["dims"]).ravel())
+        self.model, self.dims = model, dims
+        ndim = len(dims)
+        self.ndim = ndim
+        periodic = [0, 0, 0]
+        mult = None
+        if model in ("Riemann2", "Riemann3", "Isotropic2"):
+            origin = np.asarray(_get(params, "origin", np.zeros(ndim)), float)
+            if "gridScales" in params:
+                hs = np.asarray(params["gridScales"], float).ravel()
+            else:
+                hs = np.full(ndim, float(params["gridScale"]))
+            if model == "Isotropic2":
+                cost = np.broadcast_to(np.asarray(_get(params, "cost", 1.0), float), dims)
+                metric = np.zeros(dims + (3,))
+                metric[..., 0] = cost ** 2
+                metric[..., 2] = cost ** 2
+                dual = False
+            else:
+                dual = "dualMetric" in params
+                metric = np.asarray(params["dualMetric" if dual else "metric"], float)
+                ns = 3 if ndim == 2 else 6
+                if metric.shape == (ns,):
+                    metric = np.broadcast_to(metric, dims + (ns,))
+            off, w = riemann_stencils(np.ascontiguousarray(metric), hs, dual)
+            nfwd, nsym, share = 0, off.shape[1], 0
+            adim = lambda p: (np.asarray(p, float) - origin) / hs
+        elif model in ("ReedsShepp2", "Elastica2"):
+            periodic = [0, 0, 1]
+            h = float(params["gridScale"])
+            xi = float(_get(params, "xi", 1.0))
+            eps = float(_get(params, "eps", 0.1))
+            projective = bool(_get(params, "projective", 0.0)) if model == "ReedsShepp2" else False
+            nth = dims[2]
+            ds = (math.pi if projective else 2 * math.pi) / nth
+            off, w = curvature2_table(model, nth, h, xi, eps, projective)
+            if model == "ReedsShepp2":
+                nfwd, nsym = 0, 4
+            else:
+                nfwd, nsym = 27, 0
+            share = 1
+            if "speed" in params:
+                sp = np.asarray(params["speed"], float)
+            else:
+                sp = 1.0 / np.asarray(params["cost"], float)
+            if sp.ndim == 0:
+                sp = np.full(dims, float(sp))
+            elif sp.shape == dims[:2]:
+                sp = np.repeat(sp[:, :, None], nth, axis=2)
+            elif sp.shape == (nth,):
+                sp = np.broadcast_to(sp[None, None, :], dims)
+            mult = np.ascontiguousarray(sp, dtype=np.float64)
+            o = np.asarray(_get(params, "origin", np.zeros(2)), float)
+            origin = np.array([o[0], o[1], -ds / 2.0])
+            scale = np.array([h, h, ds])
+            adim = lambda p: (np.asarray(p, float) - origin) / scale
+        else:
+            raise NotImplementedError(model)
+        self.off = np.ascontiguousarray(off.reshape(-1, nfwd + nsym, 3), dtype=np.int8)
+        self.w = np.ascontiguousarray(w.reshape(-1, nfwd + nsym), dtype=np.float64)
+        self.nfwd, self.nsym, self.share = nfwd, nsym, share
+        self.mult = mult
+        self.periodic = periodic
+        walls = None
+        if "walls" in params:
+            wl = np.asarray(params["walls"], float)
+            if wl.shape != dims and ndim == 3 and wl.shape == dims[:2]:
+                wl = np.repeat(wl[:, :, None], dims[2], axis=2)
+            walls = np.ascontiguousarray(wl != 0, dtype=np.uint8)
+        self.walls = walls
+        self.seed_index, self.seed_value = _seed_indices(params, adim, dims, periodic)
+        self._adim = adim
+        s = _Problem()
+        s.ndim = ndim
+        for a in range(3):
+            s.dims[a] = dims[a] if a < ndim else 1
+            s.periodic[a] = periodic[a]
+        s.nfwd, s.nsym, s.share = nfwd, nsym, share
+        s.off, s.w = _ptr(self.off), _ptr(self.w)
+        s.mult = _ptr(self.mult)
+        s.walls = _ptr(self.walls)
+        s.nseeds = len(self.seed_index)
+        s.seed_index, s.seed_value = _ptr(self.seed_index), _ptr(self.seed_value)
+        self.struct = s
+
+    def index_of_point(self, p):
+        q = self._adim(p)
+        idx = [int(math.floor(c)) for c in q]
+        for a, n in enumerate(self.dims):
+            if self.periodic[a]:
+                idx[a] %= n
+            elif not (0 <= idx[a] < n):
+                return None
+        return int(np.ravel_multi_index(tuple(idx), self.dims))
+
+
+def solve(params: Dict, with_active: bool = True) -> Dict:
+    """Fast-marching solve of ``params`` on the CPU. Returns values (dims), activeNeighs (uint64),
+    nAccepted, MaxStencilWidth and the :class:`Problem` used."""
+    P = Problem(params)
+    n = int(np.prod(P.dims))
+    values = np.empty(n, np.float64)
+    active = np.zeros(n, np.uint64) if with_active else None
+    mw = ctypes.c_int(0)
+    nacc = lib().fmo_fast_marching(ctypes.byref(P.struct), _ptr(values), _ptr(active), ctypes.byref(mw))
+    if nacc < 0:
+        raise RuntimeError("oracle fast marching failed")
+    return {"values": values.reshape(P.dims), "activeNeighs": active, "nAccepted": int(nacc),
+            "MaxStencilWidth": int(mw.value), "problem": P}
+
+
+def backward_variation(res: Dict, points, weights=None):
+    """Reverse first variation from weighted physical points (one ``inspectSensitivity`` group)."""
+    P: Problem = res["problem"]
+    pts = np.atleast_2d(np.asarray(points, float))
+    wts = np.ones(len(pts)) if weights is None else np.asarray(weights, float).ravel()
+    idx = []
+    for p in pts:
+        i = P.index_of_point(p)
+        if i is None:
+            raise ValueError("Error : inspectSensitivity data points are out of range")
+        idx.append(i)
+    idx = np.array(idx, np.int64)
+    n = int(np.prod(P.dims))
+    sens = np.zeros(n, np.float64)
+    max_seeds = max(16, len(P.seed_index) + 16)
+    so_i = np.zeros(max_seeds, np.int64)
+    so_w = np.zeros(max_seeds, np.float64)
+    values = np.ascontiguousarray(res["values"].ravel())
+    ns = lib().fmo_backward_variation(ctypes.byref(P.struct), _ptr(values), _ptr(res["activeNeighs"]),
+                                      len(idx), _ptr(idx), _ptr(wts), _ptr(sens), max_seeds,
+                                      _ptr(so_i), _ptr(so_w))
+    if ns < 0:
+        raise RuntimeError("oracle backward variation failed")
+    ns = min(int(ns), max_seeds)
+    return sens.reshape(P.dims), so_i[:ns].copy(), so_w[:ns].copy()
+
+
+def visibility(params: Dict, max_width: int):
+    P = Problem(params)
+    n = int(np.prod(P.dims))
+    nb = P.nfwd + 2 * P.nsym
+    vis = np.zeros((n, nb), np.uint8)
+    if lib().fmo_visibility(ctypes.byref(P.struct), max_width, _ptr(vis)):
+        raise RuntimeError("oracle visibility failed")
+    return vis
