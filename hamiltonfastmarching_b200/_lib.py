@@ -1,0 +1,56 @@
+"""ctypes binding of the in-tree C ABI library ``libhfm_b200.so`` (include/hfm_b200.h).
+
+The library is loaded from this package directory only; if it is missing the import fails loudly
+(run ``python -m hamiltonfastmarching_b200.build``). There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhfm_b200.so")
+
+HFM_OK = 0
+ERROR_NAMES = {1: "HFM_ERR_KEY", 2: "HFM_ERR_VALUE", 3: "HFM_ERR_UNSUPPORTED", 4: "HFM_ERR_CUDA",
+               5: "HFM_ERR_NOT_CONVERGED", 6: "HFM_ERR_NOMEM", 7: "HFM_ERR_ARG"}
+ORDERINGS = {"RowMajor": 0, "ColumnMajor": 1, "YXZ_RowMajor": 2, "YXZ_ColumnMajor": 3}
+
+# Every symbol include/hfm_b200.h declares, with its ctypes signature.
+_P, _I, _D, _S, _SZ, _I64P = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t, \
+    ctypes.POINTER(ctypes.c_int64)
+SIGNATURES = {
+    "hfm_io_create": ([_I], _P),
+    "hfm_io_destroy": ([_P], None),
+    "hfm_io_set_scalar": ([_P, _S, _D], _I),
+    "hfm_io_set_string": ([_P, _S, _S], _I),
+    "hfm_io_set_array": ([_P, _S, _P, _I, _I64P], _I),
+    "hfm_io_get_scalar": ([_P, _S, ctypes.POINTER(_D)], _I),
+    "hfm_io_get_string": ([_P, _S, _P, _SZ, ctypes.POINTER(_SZ)], _I),
+    "hfm_io_get_array_info": ([_P, _S, ctypes.POINTER(_I), _I64P, _I], _I),
+    "hfm_io_get_array": ([_P, _S, _P, _SZ], _I),
+    "hfm_io_has_field": ([_P, _S], _I),
+    "hfm_io_erase_field": ([_P, _S], _I),
+    "hfm_io_computed_keys": ([_P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
+    "hfm_run": ([_P, _S], _I),
+    "hfm_io_last_error": ([_P], _S),
+    "hfm_version": ([], _S),
+    "hfm_device_count": ([ctypes.POINTER(_I)], _I),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library and declare every exported symbol; raises ImportError if absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hamiltonfastmarching_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib

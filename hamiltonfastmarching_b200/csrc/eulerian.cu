@@ -1,0 +1,1366 @@
+// GPU solve path for Eulerian schemes: per-cell Selling stencils (Riemann) or per-angle shared
+// stencils (ReedsShepp2, Elastica2), wall visibility, and a tiled fast-iterative solver.
+//
+// The fixed point solved here is the one the reference's fast marching reaches
+// (Headers/Base/Implementation/HamiltonFastMarching.hxx:86-169 with the Hopf-Lax update of
+// Headers/Base/Implementation/EulerianStencil.hxx:104-153): at every cell x the value is the root of
+//     sum_i w_i (t - v_i)^2 = 1
+// over the neighbour values v_i sorted increasingly, a neighbour being used only while it is
+// strictly below the root obtained from the smaller ones; the accumulation starts from the
+// smallest value (minVal), adds (w, w v, w v^2) in increasing order, and takes
+// (b + sqrt(max(0, b^2 - a c)))/a. Fast marching adds neighbours exactly in that order (they are
+// accepted by increasing value), so with unfused FP64 arithmetic the converged tiles reproduce
+// its arrival times.
+//
+// Layout in HBM: values RowMajor (the output array itself); per-cell stencil data tile-major
+// (64 consecutive entries per tile and slot) so that a warp streams its tile's stencils with
+// coalesced loads. Scheduling: a persistent cooperative kernel processes an active-tile list
+// round by round (one warp per tile, local Jacobi sweeps voted with __any_sync), and appends to
+// the next list, through atomics, the tiles whose stencils read a cell that changed.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <execinfo.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "device_buffer.hpp"
+#include "selling.cuh"
+#include "solver.hpp"
+
+namespace hfm {
+
+static void trace_at_exit() {
+    void *frames[64];
+    const int n = backtrace(frames, 64);
+    std::fprintf(stderr, "[hfm] process exit requested; native backtrace:\n");
+    backtrace_symbols_fd(frames, n, 2);
+}
+
+void trace_step(const char *what) {
+    static const bool on = std::getenv("HFM_DEBUG") != nullptr;
+    if (!on) return;
+    static const bool registered = (std::atexit(trace_at_exit), true);
+    (void)registered;
+    const cudaError_t e = cudaDeviceSynchronize();
+    std::fprintf(stderr, "[hfm] %s: %s\n", what, cudaGetErrorString(e));
+    std::fflush(stderr);
+}
+
+GridGeom make_geom(int ndim, const int *dims, const int *periodic) {
+    GridGeom g{};
+    for (int a = 0; a < 3; ++a) {
+        g.dims[a] = a < ndim ? dims[a] : 1;
+        g.periodic[a] = a < ndim ? periodic[a] : 0;
+    }
+    if (ndim == 2) { g.tshift[0] = 3; g.tshift[1] = 3; g.tshift[2] = 0; }
+    else { g.tshift[0] = 2; g.tshift[1] = 2; g.tshift[2] = 2; }
+    g.ncells = 1;
+    g.ntile = 1;
+    for (int a = 0; a < 3; ++a) {
+        g.ntiles[a] = (g.dims[a] + (1 << g.tshift[a]) - 1) >> g.tshift[a];
+        g.ncells *= g.dims[a];
+        g.ntile *= g.ntiles[a];
+    }
+    return g;
+}
+
+// Kernels live in a named namespace: nvcc's host launch wrappers for __global__ templates do not
+// bind to their generated stubs inside an anonymous namespace.
+namespace detail {
+
+constexpr unsigned kVisPlus = 1u << 24, kVisMinus = 1u << 25, kFixed = 1u << 28, kDead = 1u << 29;
+constexpr unsigned kShFixed = 1u << 30, kShDead = 1u << 31;
+constexpr int kWarpsPerCta = 4;
+constexpr int kDepWarps = 2;
+constexpr int kDepCap = 2048;
+constexpr unsigned long long kBarrierPolls = 1ull << 25;
+
+__host__ __device__ __forceinline__ unsigned pack_off(int o0, int o1, int o2) {
+    return (unsigned)(uint8_t)(int8_t)o0 | ((unsigned)(uint8_t)(int8_t)o1 << 8) | ((unsigned)(uint8_t)(int8_t)o2 << 16);
+}
+__device__ __forceinline__ int off_c(unsigned code, int c) { return (int)(int8_t)((code >> (8 * c)) & 0xffu); }
+
+template <typename Real>
+struct Dev {
+    GridGeom g;
+    long long ntc;            // tile-major cell count = ntile * 64
+    Real *values;             // RowMajor
+    unsigned *code;           // [ND][ntc] per-cell offsets + visibility/flags (per-cell stencils)
+    Real *weight;             // [ND][ntc]
+    Real *mult;               // [ntc] speed multiplier (shared stencils)
+    unsigned *vis;            // [ntc] slot visibility + flags (shared stencils)
+    const int8_t *cls_off;    // [nclass][ND][3]
+    const Real *cls_w;        // [nclass][ND]
+    // reverse tile dependencies: tile T -> tiles whose stencils read T, with the cells they read
+    const long long *dep_ptr;
+    const int *dep_tile;
+    const unsigned long long *dep_mask;
+    // active-tile lists (triple buffered) and their dedupe flags
+    int *list[3];
+    unsigned *count[3];
+    unsigned *claim[3];
+    unsigned *flag[3];
+    unsigned *bar_count;
+    unsigned *bar_gen;
+    unsigned *status;
+    unsigned long long *stats;  // rounds, tile activations, local solves
+    int max_rounds;
+    int sweeps;
+};
+
+// --------------------------------------------------------------------------------------------
+// Hopf-Lax update over neighbour candidates v[k] (+inf if unusable) with weights w[k], taken in
+// increasing order (ties by k); see the file header. `used` receives the bitmask of taken k.
+template <typename Real, int ND>
+__device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real (&w)[ND], unsigned *used) {
+    using A = Arith<Real>;
+    const Real INF = A::inf();
+    unsigned taken = 0;
+    Real minVal = 0, a = 0, b = 0, c = -1, r = INF;
+    for (int it = 0; it < ND; ++it) {
+        Real bv = INF, bw = 0;
+        int bk = -1;
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+            if (!((taken >> k) & 1u) && v[k] < bv) { bv = v[k]; bw = w[k]; bk = k; }
+        }
+        if (bk < 0) break;
+        if (it > 0 && !(bv < r)) break;
+        if (it == 0) minVal = bv;
+        const Real dv = A::sub(bv, minVal);
+        const Real wv = A::mul(bw, dv);
+        a = A::add(a, bw);
+        b = A::add(b, wv);
+        c = A::add(c, A::mul(wv, dv));
+        if (a == Real(0)) {
+            r = INF;
+        } else {
+            const Real d2 = A::sub(A::mul(b, b), A::mul(a, c));
+            const Real d = A::sqrt(Real(0) < d2 ? d2 : Real(0));
+            r = A::add(minVal, A::div(A::add(b, d), a));
+        }
+        taken |= 1u << bk;
+    }
+    if (used) *used = taken;
+    return r;
+}
+
+// Local solve at one cell. `sv` holds the current values of the warp's tile (nullptr: read all
+// neighbours from global memory). `side` receives, per symmetric difference, 1 if the -e
+// neighbour provided the candidate.
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__device__ __forceinline__ Real solve_cell(const Dev<Real> &P, long long c, int x0, int x1, int x2, int tx0, int tx1,
+                                           int tx2, const Real *sv, unsigned *used, unsigned *side) {
+    constexpr int ND = NFWD + NSYM;
+    using A = Arith<Real>;
+    const Real INF = A::inf();
+    const GridGeom &g = P.g;
+    Real v[ND], w[ND];
+    Real m2 = 1;
+    unsigned visw = 0;
+    if (SHARE) {
+        const Real m = P.mult[c];
+        m2 = A::mul(m, m);
+        visw = P.vis[c];
+    }
+    unsigned sides = 0;
+    auto fetch = [&](int o0, int o1, int o2) -> Real {
+        const int n0 = x0 + o0, n1 = x1 + o1;
+        int n2 = x2 + o2;
+        if (SHARE && g.periodic[2]) {
+            n2 %= g.dims[2];
+            if (n2 < 0) n2 += g.dims[2];
+        }
+        if (sv) {
+            const unsigned l0 = n0 - tx0, l1 = n1 - tx1, l2 = n2 - tx2;
+            if (l0 < (1u << g.tshift[0]) && l1 < (1u << g.tshift[1]) && l2 < (1u << g.tshift[2]))
+                return sv[((l0 << g.tshift[1] | l1) << g.tshift[2]) | l2];
+        }
+        return __ldcg(P.values + g.lin(n0, n1, n2));
+    };
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+        int o0, o1, o2;
+        bool vp, vm = false;
+        if (SHARE) {
+            const int8_t *o = P.cls_off + ((long long)x2 * ND + k) * 3;
+            o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
+            w[k] = A::mul(__ldg(P.cls_w + (long long)x2 * ND + k), m2);
+            if (k < NFWD) {
+                vp = (visw >> k) & 1u;
+            } else {
+                const int s = NFWD + 2 * (k - NFWD);
+                vp = (visw >> s) & 1u;
+                vm = (visw >> (s + 1)) & 1u;
+            }
+        } else {
+            const unsigned cd = P.code[k * P.ntc + c];
+            o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
+            w[k] = P.weight[k * P.ntc + c];
+            vp = cd & kVisPlus;
+            vm = (k >= NFWD) && (cd & kVisMinus);
+        }
+        Real val = INF;
+        if (vp) val = fetch(o0, o1, o2);
+        if (vm) {
+            const Real vv = fetch(-o0, -o1, -o2);
+            if (vv < val) { val = vv; if (k >= NFWD) sides |= 1u << (k - NFWD); }
+        }
+        v[k] = val;
+    }
+    if (side) *side = sides;
+    return hopf_lax_sorted<Real, ND>(v, w, used);
+}
+
+template <typename Real, bool SHARE>
+__device__ __forceinline__ void cell_flags(const Dev<Real> &P, long long c, bool &fixed, bool &dead) {
+    if (SHARE) {
+        const unsigned f = P.vis[c];
+        fixed = f & kShFixed;
+        dead = f & kShDead;
+    } else {
+        const unsigned f = P.code[c];
+        fixed = f & kFixed;
+        dead = f & kDead;
+    }
+}
+
+// Appends tile D to list `li` unless it is already there (flag dedupe). Called by all lanes with
+// their own `want`; one atomicAdd per warp reserves the slots.
+template <typename Real>
+__device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bool want, int lane) {
+    if (want) want = atomicExch(&P.flag[li][D], 1u) == 0u;
+    const unsigned ballot = __ballot_sync(0xffffffffu, want);
+    if (!ballot) return;
+    unsigned base = 0;
+    if (lane == __ffs(ballot) - 1) base = atomicAdd(P.count[li], (unsigned)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, __ffs(ballot) - 1);
+    if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
+}
+
+// Pushes the dependents of tile T that read a cell of `mask` (plus T itself if `self`).
+template <typename Real>
+__device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int T, unsigned long long mask, bool self,
+                                                int lane) {
+    if (mask) {
+        const long long b = P.dep_ptr[T], e = P.dep_ptr[T + 1];
+        for (long long base = b; base < e; base += 32) {
+            const long long i = base + lane;
+            bool want = false;
+            int D = 0;
+            if (i < e) {
+                D = P.dep_tile[i];
+                want = (P.dep_mask[i] & mask) != 0ull;
+            }
+            push_tiles(P, li, D, want, lane);
+        }
+    }
+    push_tiles(P, li, T, self && lane == 0, lane);
+}
+
+// Processes one tile with local Jacobi sweeps; returns through `mask` the cells that changed.
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next,
+                                             unsigned long long &n_solves) {
+    const GridGeom &g = P.g;
+    int t0, t1, t2;
+    g.tile_coords(T, t0, t1, t2);
+    const int tx0 = t0 << g.tshift[0], tx1 = t1 << g.tshift[1], tx2 = t2 << g.tshift[2];
+    Real cur[2];
+    bool upd[2], chg[2] = {false, false};
+    int xs[2][3];
+    long long gi[2];
+    const Real INF = Arith<Real>::inf();
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int l = lane + 32 * j;
+        int l0, l1, l2;
+        g.local_coords(l, l0, l1, l2);
+        xs[j][0] = tx0 + l0; xs[j][1] = tx1 + l1; xs[j][2] = tx2 + l2;
+        const bool valid = xs[j][0] < g.dims[0] && xs[j][1] < g.dims[1] && xs[j][2] < g.dims[2];
+        bool fixed = true, dead = true;
+        const long long c = (long long)T * 64 + l;
+        if (valid) cell_flags<Real, SHARE>(P, c, fixed, dead);
+        gi[j] = valid ? g.lin(xs[j][0], xs[j][1], xs[j][2]) : 0;
+        cur[j] = (valid && !dead) ? __ldcg(P.values + gi[j]) : INF;
+        upd[j] = valid && !dead && !fixed;
+        sv[l] = cur[j];
+    }
+    __syncwarp();
+    bool converged = false;
+    for (int sweep = 0; sweep < P.sweeps; ++sweep) {
+        Real nv[2];
+#pragma unroll 1
+        for (int j = 0; j < 2; ++j) {
+            nv[j] = cur[j];
+            if (upd[j]) {
+                nv[j] = solve_cell<Real, NFWD, NSYM, SHARE>(P, (long long)T * 64 + lane + 32 * j, xs[j][0], xs[j][1],
+                                                            xs[j][2], tx0, tx1, tx2, sv, nullptr, nullptr);
+                ++n_solves;
+            }
+        }
+        __syncwarp();
+        bool ch = false;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (nv[j] != cur[j]) {
+                cur[j] = nv[j];
+                sv[lane + 32 * j] = nv[j];
+                ch = true;
+                chg[j] = true;
+            }
+        }
+        __syncwarp();
+        if (!__any_sync(0xffffffffu, ch)) { converged = true; break; }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+        if (chg[j]) __stcg(P.values + gi[j], cur[j]);
+    const unsigned lo = __ballot_sync(0xffffffffu, chg[0]);
+    const unsigned hi = __ballot_sync(0xffffffffu, chg[1]);
+    const unsigned long long mask = (unsigned long long)lo | ((unsigned long long)hi << 32);
+    __threadfence();
+    push_dependents(P, li_next, T, mask, !converged, lane);
+}
+
+// Persistent cooperative solver: rounds over the triple-buffered active-tile lists.
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__global__ void __launch_bounds__(kWarpsPerCta * 32) fim_kernel(Dev<Real> P) {
+    __shared__ Real s_vals[kWarpsPerCta][64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long n_act = 0, n_solves = 0;
+    int r = 0;
+    bool ok = true;
+    for (; r < P.max_rounds; ++r) {
+        const int cur = r % 3, nxt = (r + 1) % 3, old = (r + 2) % 3;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            *P.count[old] = 0;
+            *P.claim[old] = 0;
+        }
+        const unsigned n = *(volatile unsigned *)P.count[cur];
+        while (true) {
+            unsigned i = 0;
+            if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= n) break;
+            const int T = P.list[cur][i];
+            if (lane == 0) P.flag[cur][T] = 0u;
+            process_tile<Real, NFWD, NSYM, SHARE>(P, T, s_vals[warp], lane, nxt, n_solves);
+            ++n_act;
+        }
+        ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
+        if (!ok) break;
+        if (*(volatile unsigned *)P.count[nxt] == 0u) { ++r; break; }
+    }
+    if (ok && r >= P.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(P.status, (unsigned)kErrRoundCap);
+    if (lane == 0) {
+        atomicAdd(P.stats + 1, n_act);
+    }
+    n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 16);
+    n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 8);
+    n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 4);
+    n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 2);
+    n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 1);
+    if (lane == 0) atomicAdd(P.stats + 2, n_solves);
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.stats[0] = (unsigned long long)r;
+}
+
+// Seeds the first list: every tile holding a seed, and the dependents reading a seed cell.
+template <typename Real>
+__global__ void init_lists_kernel(Dev<Real> P, const int *seed_tiles, const unsigned long long *seed_masks, int n) {
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (wid >= n) return;
+    push_dependents(P, 0, seed_tiles[wid], seed_masks[wid], true, lane);
+}
+
+// --------------------------------------------------------------------------------------------
+// Stencil construction and layout.
+
+template <typename Real>
+__global__ void fill_kernel(Real *p, long long n, Real v) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// One thread per cell: Riemann Selling stencil, written tile-major for the solver and optionally
+// RowMajor for export. Non positive definite metrics set kErrSelling.
+template <int D, typename Real>
+__global__ void riemann_stencil_kernel(GridGeom g, long long ntc, const double *metric, int metric_const, int dual,
+                                       double h0, double h1, double h2, unsigned *code, Real *weight,
+                                       int8_t *plain_off, double *plain_w, unsigned *status) {
+    constexpr int NS = D * (D + 1) / 2, NK = D == 2 ? 3 : 6;
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= g.ncells) return;
+    const int x2 = (int)(x % g.dims[2]);
+    const long long r = x / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    double m[6];
+    const double *src = metric + (metric_const ? 0 : x * NS);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) m[k] = src[k];
+    const double h[3] = {h0, h1, h2};
+    int off[6][3];
+    double w[6];
+    if (!riemann_stencil<D>(m, dual != 0, h, off, w)) {
+        atomicOr(status, (unsigned)kErrSelling);
+#pragma unroll
+        for (int k = 0; k < NK; ++k) { w[k] = 0.0; off[k][0] = off[k][1] = off[k][2] = 0; }
+    }
+    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        code[k * ntc + c] = pack_off(off[k][0], off[k][1], off[k][2]);
+        weight[k * ntc + c] = (Real)w[k];
+        if (plain_off) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) plain_off[(x * NK + k) * 3 + a] = (int8_t)off[k][a];
+            plain_w[x * NK + k] = w[k];
+        }
+    }
+}
+
+// Largest L1 norm of a non-zero-weight offset whose target lies in the domain (MaxStencilWidth,
+// HamiltonFastMarching.hxx:36-45 over the reversed offsets of HFM_StencilRecompute.hxx:91-116).
+template <typename Real, int NSYM>
+__global__ void width_kernel(Dev<Real> P, unsigned *maxw) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const GridGeom &g = P.g;
+    if (x >= g.ncells) return;
+    const int x2 = (int)(x % g.dims[2]);
+    const long long r = x / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    int best = 0;
+#pragma unroll
+    for (int k = 0; k < NSYM; ++k) {
+        if (P.weight[k * P.ntc + c] == Real(0)) continue;
+        const unsigned cd = P.code[k * P.ntc + c];
+        const int o0 = off_c(cd, 0), o1 = off_c(cd, 1), o2 = off_c(cd, 2);
+        const int l1 = abs(o0) + abs(o1) + abs(o2);
+        for (int s = 1; s >= -1; s -= 2) {
+            int n0 = x0 + s * o0, n1 = x1 + s * o1, n2 = x2 + s * o2;
+            if (g.wrap(n0, n1, n2) && l1 > best) best = l1;
+        }
+    }
+    if (best) atomicMax(maxw, (unsigned)best);
+}
+
+// Speed multiplier to the tile-major layout (shared stencils).
+template <typename Real>
+__global__ void mult_layout_kernel(GridGeom g, const double *mult_rm, Real *mult_tm) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= g.ncells) return;
+    const int x2 = (int)(x % g.dims[2]);
+    const long long r = x / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    mult_tm[g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2)] = (Real)mult_rm[x];
+}
+
+// --------------------------------------------------------------------------------------------
+// Walls: distance to the nearest wall cell (breadth-first search distance of
+// Headers/ExtraAlgorithms/WallObstructionTest.h:48-88, which on a box grid is the L1 distance,
+// computed here by separable forward/backward scans per axis), capped at the stencil width.
+
+__global__ void wall_init_kernel(long long n, const uint8_t *walls, int *d) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < n) d[x] = walls[x] ? 0 : (1 << 29);
+}
+
+__global__ void wall_scan_kernel(GridGeom g, int axis, int *d) {
+    const long long nl = g.ncells / g.dims[axis];
+    const long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (line >= nl) return;
+    long long stride = 1;
+    for (int a = 2; a > axis; --a) stride *= g.dims[a];
+    const long long inner = stride;
+    const long long base = (line / inner) * inner * g.dims[axis] + (line % inner);
+    const int n = g.dims[axis];
+    const int laps = g.periodic[axis] ? 2 : 1;
+    int prev = 1 << 29;
+    for (int lap = 0; lap < laps; ++lap)
+        for (int i = 0; i < n; ++i) {
+            int v = d[base + i * stride];
+            if (prev + 1 < v) { v = prev + 1; d[base + i * stride] = v; }
+            prev = v;
+        }
+    prev = 1 << 29;
+    for (int lap = 0; lap < laps; ++lap)
+        for (int i = n - 1; i >= 0; --i) {
+            int v = d[base + i * stride];
+            if (prev + 1 < v) { v = prev + 1; d[base + i * stride] = v; }
+            prev = v;
+        }
+}
+
+__global__ void wall_cap_kernel(long long n, const int *d, int cap, int8_t *wd) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < n) wd[x] = d[x] <= cap ? (int8_t)d[x] : (int8_t)127;
+}
+
+// Visible(base, v, sum) of WallObstructionTest.h:95-150: a discrete walk from `base` toward `sum`.
+__device__ bool wall_visible(const GridGeom &g, const int8_t *wd, int b0, int b1, int b2, int v0, int v1, int v2,
+                             int s0, int s1, int s2) {
+    int w = wd[g.lin(s0, s1, s2)];
+    if (w == 127) return true;
+    if (w == 0) return false;
+    const int v[3] = {v0, v1, v2};
+    int vSign[3] = {0, 0, 0};
+    int vSum = 0, vProd = 1, vMax = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (v[i] != 0) {
+            vSign[i] = v[i] > 0 ? 1 : -1;
+            const int av = abs(v[i]);
+            vSum += av;
+            vProd *= av;
+            vMax = max(vMax, av);
+        }
+    }
+    if (vSum <= w) return true;
+    int pos[3] = {b0, b1, b2};
+    long long vNext[3], vInc[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        vNext[i] = v[i] == 0 ? 2147483647LL : (long long)(vProd / abs(v[i]));
+        vInc[i] = 2 * vNext[i];
+    }
+    for (int i = 1; i < vMax; ++i) {
+        const long long thr = (2LL * i * vProd) / vMax;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (v[j] != 0 && vNext[j] <= thr) {
+                vNext[j] += vInc[j];
+                --vSum;
+                pos[j] += vSign[j];
+            }
+        }
+        int p0 = pos[0], p1 = pos[1], p2 = pos[2];
+        g.wrap(p0, p1, p2);
+        w = wd[g.lin(p0, p1, p2)];
+        if (vSum <= w) return true;
+        if (w == 0) return false;
+    }
+    return true;
+}
+
+// Visibility bits of every (cell, neighbour slot): the neighbour y = x + s e may update x iff the
+// difference has non-zero weight, y lies in the domain, and Visible(y, -s e, x) holds
+// (ConditionalUpdate, HamiltonFastMarching.hxx:136-154). Also marks padding cells dead.
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__global__ void visibility_kernel(Dev<Real> P, const int8_t *wd, const uint8_t *cls_enabled) {
+    constexpr int ND = NFWD + NSYM;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const GridGeom &g = P.g;
+    if (c >= P.ntc) return;
+    const int T = (int)(c >> 6), l = (int)(c & 63);
+    int t0, t1, t2, l0, l1, l2;
+    g.tile_coords(T, t0, t1, t2);
+    g.local_coords(l, l0, l1, l2);
+    const int x0 = (t0 << g.tshift[0]) + l0, x1 = (t1 << g.tshift[1]) + l1, x2 = (t2 << g.tshift[2]) + l2;
+    if (x0 >= g.dims[0] || x1 >= g.dims[1] || x2 >= g.dims[2]) {
+        if (SHARE) P.vis[c] = kShDead;
+        else P.code[c] = kDead;
+        return;
+    }
+    unsigned visw = 0;
+#pragma unroll 1
+    for (int k = 0; k < ND; ++k) {
+        int o[3];
+        bool nonzero;
+        if (SHARE) {
+            const int8_t *oo = P.cls_off + ((long long)x2 * ND + k) * 3;
+            o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
+            nonzero = P.cls_w[(long long)x2 * ND + k] != Real(0);
+        } else {
+            const unsigned cd = P.code[k * P.ntc + c];
+            o[0] = off_c(cd, 0); o[1] = off_c(cd, 1); o[2] = off_c(cd, 2);
+            nonzero = P.weight[k * P.ntc + c] != Real(0);
+        }
+        unsigned bits = 0;
+        for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
+            const int s = si == 0 ? 1 : -1;
+            const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
+            if (!nonzero) continue;
+            if (SHARE && !cls_enabled[(long long)x2 * (NFWD + 2 * NSYM) + slot]) continue;
+            int y0 = x0 + s * o[0], y1 = x1 + s * o[1], y2 = x2 + s * o[2];
+            if (!g.wrap(y0, y1, y2)) continue;
+            if (wd && !wall_visible(g, wd, y0, y1, y2, -s * o[0], -s * o[1], -s * o[2], x0, x1, x2)) continue;
+            if (SHARE) visw |= 1u << slot;
+            else bits |= si == 0 ? kVisPlus : kVisMinus;
+        }
+        if (!SHARE) P.code[k * P.ntc + c] |= bits;
+    }
+    if (SHARE) P.vis[c] = visw;
+}
+
+template <typename Real, bool SHARE>
+__global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *val, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const GridGeom &g = P.g;
+    const long long x = idx[i];
+    const int x2 = (int)(x % g.dims[2]);
+    const long long r = x / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    P.values[x] = (Real)val[i];
+    if (SHARE) P.vis[c] |= kShFixed;
+    else P.code[c] |= kFixed;
+}
+
+// --------------------------------------------------------------------------------------------
+// Tile dependency graph. Pass 0 counts, pass 1 writes, for every tile D, the distinct source
+// tiles T != D its visible stencil entries read, with the 64-bit mask of the cells read in T.
+
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__global__ void __launch_bounds__(kDepWarps * 32)
+    deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
+                unsigned long long *msk) {
+    constexpr int ND = NFWD + NSYM;
+    __shared__ int keys[kDepWarps][kDepCap];
+    __shared__ unsigned long long masks[kDepWarps][kDepCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long D = (long long)blockIdx.x * kDepWarps + warp;
+    if (D >= P.g.ntile) return;
+    int *K = keys[warp];
+    unsigned long long *M = masks[warp];
+    for (int i = lane; i < kDepCap; i += 32) { K[i] = -1; M[i] = 0ull; }
+    __syncwarp();
+    const GridGeom &g = P.g;
+    int t0, t1, t2;
+    g.tile_coords(D, t0, t1, t2);
+    bool overflow = false;
+    for (int j = 0; j < 2; ++j) {
+        const int l = lane + 32 * j;
+        int l0, l1, l2;
+        g.local_coords(l, l0, l1, l2);
+        const int x0 = (t0 << g.tshift[0]) + l0, x1 = (t1 << g.tshift[1]) + l1, x2 = (t2 << g.tshift[2]) + l2;
+        const long long c = D * 64 + l;
+        if (x0 >= g.dims[0] || x1 >= g.dims[1] || x2 >= g.dims[2]) continue;
+        unsigned visw = SHARE ? P.vis[c] : 0u;
+        for (int k = 0; k < ND; ++k) {
+            int o[3];
+            unsigned bits;
+            if (SHARE) {
+                const int8_t *oo = P.cls_off + ((long long)x2 * ND + k) * 3;
+                o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
+                bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
+            } else {
+                const unsigned cd = P.code[k * P.ntc + c];
+                o[0] = off_c(cd, 0); o[1] = off_c(cd, 1); o[2] = off_c(cd, 2);
+                bits = ((cd & kVisPlus) ? 1u : 0u) | ((cd & kVisMinus) ? 2u : 0u);
+            }
+            for (int si = 0; si < 2; ++si) {
+                if (!((bits >> si) & 1u)) continue;
+                const int s = si == 0 ? 1 : -1;
+                int y0 = x0 + s * o[0], y1 = x1 + s * o[1], y2 = x2 + s * o[2];
+                g.wrap(y0, y1, y2);
+                const int T = (int)g.tile_of(y0, y1, y2);
+                if (T == D) continue;
+                const int b = g.local_of(y0, y1, y2);
+                unsigned h = ((unsigned)T * 2654435761u) & (kDepCap - 1);
+                int probes = 0;
+                while (true) {
+                    const int prev = atomicCAS(&K[h], -1, T);
+                    if (prev == -1 || prev == T) { atomicOr(&M[h], 1ull << b); break; }
+                    h = (h + 1) & (kDepCap - 1);
+                    if (++probes >= kDepCap) { overflow = true; break; }
+                }
+            }
+        }
+    }
+    if (overflow) atomicOr(P.status, (unsigned)kErrTableOverflow);
+    __syncwarp();
+    unsigned total = 0;
+    for (int base = 0; base < kDepCap; base += 32) {
+        const bool has = K[base + lane] != -1;
+        const unsigned bal = __ballot_sync(0xffffffffu, has);
+        if (pass == 1 && has) {
+            const long long pos = offs[D] + total + __popc(bal & ((1u << lane) - 1u));
+            src[pos] = K[base + lane];
+            dst[pos] = (int)D;
+            msk[pos] = M[base + lane];
+        }
+        total += __popc(bal);
+    }
+    if (pass == 0 && lane == 0) cnt[D] = total;
+}
+
+__global__ void dep_count_kernel(long long n, const int *src, unsigned *rcnt) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(rcnt + src[i], 1u);
+}
+
+__global__ void dep_scatter_kernel(long long n, const int *src, const int *dst, const unsigned long long *msk,
+                                   const long long *rptr, unsigned *cursor, int *rtile, unsigned long long *rmask) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int T = src[i];
+    const long long pos = rptr[T] + atomicAdd(cursor + T, 1u);
+    rtile[pos] = dst[i];
+    rmask[pos] = msk[i];
+}
+
+// --------------------------------------------------------------------------------------------
+// Post-processing.
+
+template <typename Real>
+__global__ void count_finite_kernel(const Real *v, long long n, unsigned long long *out) {
+    unsigned long long cnt = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        cnt += (v[i] < Arith<Real>::inf()) ? 1ull : 0ull;
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+// activeNeighs bitsets in the reference layout (EulerianStencil.h:35-49): forward difference k
+// at bit k, symmetric difference j at bits nfwd+2j (+e) and nfwd+2j+1 (-e). A used forward
+// difference also marks the other forward differences with the same offset, as the reference's
+// update adds every difference matching the accepted offset (EulerianStencil.hxx:114-123).
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
+    constexpr int ND = NFWD + NSYM;
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const GridGeom &g = P.g;
+    if (x >= g.ncells) return;
+    const int x2 = (int)(x % g.dims[2]);
+    const long long r = x / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    bool fixed, dead;
+    cell_flags<Real, SHARE>(P, c, fixed, dead);
+    unsigned long long bits = 0;
+    if (!fixed && !dead) {
+        unsigned used = 0, side = 0;
+        solve_cell<Real, NFWD, NSYM, SHARE>(P, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+        for (int k = 0; k < ND; ++k) {
+            if (!((used >> k) & 1u)) continue;
+            if (k < NFWD) {
+                bits |= 1ull << k;
+                if (SHARE) {
+                    const int8_t *ok = P.cls_off + ((long long)x2 * ND + k) * 3;
+                    for (int k2 = 0; k2 < NFWD; ++k2) {
+                        const int8_t *o2 = P.cls_off + ((long long)x2 * ND + k2) * 3;
+                        if (o2[0] == ok[0] && o2[1] == ok[1] && o2[2] == ok[2]) bits |= 1ull << k2;
+                    }
+                }
+            } else {
+                bits |= 1ull << (NFWD + 2 * (k - NFWD) + ((side >> (k - NFWD)) & 1u));
+            }
+        }
+    }
+    active[x] = bits;
+}
+
+template <typename Real>
+__global__ void to_double_kernel(const Real *in, double *out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+struct EventTimer {
+    cudaEvent_t a, b;
+    EventTimer() { cudaEventCreate(&a); cudaEventCreate(&b); }
+    ~EventTimer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    void start(cudaStream_t s) { cudaEventRecord(a, s); }
+    float stop(cudaStream_t s) {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+};
+
+void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
+    unsigned st = 0;
+    status.download(&st, 1);
+    HFM_CUDA(cudaDeviceSynchronize());
+    if (st & kErrSelling)
+        throw Error(HFM_ERR_VALUE, "ObtuseSuperbase error : input must be positive definite (metric rejected by Selling)");
+    if (st & kErrTableOverflow) throw Error(HFM_ERR_UNSUPPORTED, "stencil too wide for the tile dependency table");
+    if (st & kErrBarrierTimeout)
+        throw Error(HFM_ERR_NOT_CONVERGED, std::string(phase) + ": a grid barrier wait exceeded its limit");
+    if (st & kErrRoundCap) throw Error(HFM_ERR_NOT_CONVERGED, std::string(phase) + ": round cap reached before convergence");
+}
+
+// --------------------------------------------------------------------------------------------
+// Reverse first variation (Headers/ExtraAlgorithms/FirstVariation.h:198-251, 341-385).
+//
+// flow_kernel stores, for every reached cell x, the upwind differences of its final update in
+// stencil order with w_i = Weight_i * max(0, u(x) - u(y_i)), normalised by their sum, and
+// var(x) = (sum_i w_i (u - u_i)) / sum_i w_i (times the speed multiplier for shared stencils):
+// the same products and sums, in the same order, as ValueVariation. adjoint_kernel then sweeps
+// the upwind graph in reverse topological order: a cell is ready once every downwind cell that
+// reads it has pushed lambda * w into its accumulator (in-degree counters, atomics), which is the
+// order of the reference's decreasing-value traversal restricted to the actual dependencies.
+
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
+    constexpr int ND = NFWD + NSYM;
+    using A = Arith<double>;
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const GridGeom &g = P.g;
+    const long long N = g.ncells;
+    if (x >= N) return;
+    const int x2 = (int)(x % g.dims[2]);
+    const long long r = x / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    bool fixed, dead;
+    cell_flags<Real, SHARE>(P, c, fixed, dead);
+    const double u = (double)P.values[x];
+    nflow[x] = 0;
+    var[x] = 0.0;
+    if (fixed || dead || !(u < Arith<double>::inf())) return;
+    unsigned used = 0, side = 0;
+    solve_cell<Real, NFWD, NSYM, SHARE>(P, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+    double m = 1.0;
+    if (SHARE) m = (double)P.mult[c];
+    double ws = 0.0, v = 0.0;
+    int n = 0;
+    int ys[2 * ND > 32 ? 32 : 2 * ND];
+    double ww[2 * ND > 32 ? 32 : 2 * ND];
+    for (int k = 0; k < ND; ++k) {
+        int o0, o1, o2;
+        double wb;
+        if (SHARE) {
+            const int8_t *o = P.cls_off + ((long long)x2 * ND + k) * 3;
+            o0 = o[0]; o1 = o[1]; o2 = o[2];
+            wb = A::mul((double)P.cls_w[(long long)x2 * ND + k], A::mul(m, m));
+        } else {
+            const unsigned cd = P.code[k * P.ntc + c];
+            o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
+            wb = (double)P.weight[k * P.ntc + c];
+        }
+        // active bits of this difference (see active_kernel)
+        unsigned act = 0;  // bit0: +e, bit1: -e
+        if (k < NFWD) {
+            if ((used >> k) & 1u) act = 1;
+            else if (SHARE) {
+                for (int k2 = 0; k2 < NFWD; ++k2) {
+                    if (!((used >> k2) & 1u)) continue;
+                    const int8_t *o2p = P.cls_off + ((long long)x2 * ND + k2) * 3;
+                    if (o2p[0] == o0 && o2p[1] == o1 && o2p[2] == o2) { act = 1; break; }
+                }
+            }
+        } else if ((used >> k) & 1u) {
+            act = ((side >> (k - NFWD)) & 1u) ? 2u : 1u;
+        }
+        for (int si = 0; si < 2; ++si) {
+            if (!((act >> si) & 1u)) continue;
+            const int s = si ? -1 : 1;
+            int y0 = x0 + s * o0, y1 = x1 + s * o1, y2 = x2 + s * o2;
+            g.wrap(y0, y1, y2);
+            const long long y = g.lin(y0, y1, y2);
+            const double d = A::sub(u, (double)P.values[y]);
+            const double vd = 0.0 < d ? d : 0.0;
+            const double w = A::mul(wb, vd);
+            ws = A::add(ws, w);
+            v = A::add(v, A::mul(w, vd));
+            if (n < 32) { ys[n] = (int)y; ww[n] = w; ++n; }
+        }
+    }
+    if (ws != 0.0) {
+        const double inv = A::div(1.0, ws);
+        for (int j = 0; j < n; ++j) ww[j] = A::mul(ww[j], inv);
+        v = SHARE ? A::mul(inv, A::mul(m, v)) : A::mul(inv, v);
+    }
+    var[x] = v;
+    nflow[x] = (uint8_t)n;
+    for (int j = 0; j < n; ++j) {
+        fidx[j * N + x] = ys[j];
+        fw[j * N + x] = ww[j];
+        atomicAdd(indeg + ys[j], 1);
+    }
+}
+
+struct AdjDev {
+    long long N;
+    const int *fidx;
+    const double *fw;
+    const double *var;
+    const uint8_t *nflow;
+    int *indeg;
+    double *acc;
+    double *sens;
+    int *list[3];
+    unsigned *count[3];
+    long long *seed_idx;
+    double *seed_w;
+    unsigned *seed_count;
+    unsigned seed_cap;
+    unsigned *bar_count;
+    unsigned *bar_gen;
+    unsigned *status;
+    unsigned long long *rounds;
+    long long max_rounds;
+};
+
+__global__ void adjoint_roots_kernel(AdjDev A) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool want = x < A.N && A.indeg[x] == 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, want);
+    if (!bal) return;
+    unsigned base = 0;
+    if (lane == __ffs(bal) - 1) base = atomicAdd(A.count[0], (unsigned)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+    if (want) A.list[0][base + __popc(bal & ((1u << lane) - 1u))] = (int)x;
+}
+
+__global__ void adjoint_kernel(AdjDev A) {
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nth = (long long)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    long long r = 0;
+    bool ok = true;
+    for (; r < A.max_rounds; ++r) {
+        const int cur = (int)(r % 3), nxt = (int)((r + 1) % 3), old = (int)((r + 2) % 3);
+        if (blockIdx.x == 0 && threadIdx.x == 0) *A.count[old] = 0;
+        const long long n = *(volatile unsigned *)A.count[cur];
+        const long long nround = (n + 31) / 32 * 32;
+        for (long long i = tid; i < nround; i += nth) {
+            int x = -1;
+            if (i < n) x = A.list[cur][i];
+            int nf = 0;
+            double lam = 0.0;
+            if (x >= 0) {
+                lam = __ldcg(A.acc + x);
+                nf = A.nflow[x];
+                if (lam != 0.0) {
+                    A.sens[x] = lam * A.var[x];
+                    if (nf == 0) {
+                        const unsigned si = atomicAdd(A.seed_count, 1u);
+                        if (si < A.seed_cap) { A.seed_idx[si] = x; A.seed_w[si] = lam; }
+                    }
+                }
+            }
+            for (int j = 0; j < 32; ++j) {
+                bool want = false;
+                int y = 0;
+                if (j < nf) {
+                    y = A.fidx[j * A.N + x];
+                    if (lam != 0.0) atomicAdd(A.acc + y, A.fw[j * A.N + x] * lam);
+                    __threadfence();
+                    want = atomicSub(A.indeg + y, 1) == 1;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, want);
+                if (bal) {
+                    unsigned base = 0;
+                    if (lane == __ffs(bal) - 1) base = atomicAdd(A.count[nxt], (unsigned)__popc(bal));
+                    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+                    if (want) A.list[nxt][base + __popc(bal & ((1u << lane) - 1u))] = y;
+                }
+                if (!__any_sync(0xffffffffu, j + 1 < nf)) break;
+            }
+        }
+        ok = grid_barrier(A.bar_count, A.bar_gen, gridDim.x, A.status, kBarrierPolls);
+        if (!ok) break;
+        if (*(volatile unsigned *)A.count[nxt] == 0u) { ++r; break; }
+    }
+    if (ok && r >= A.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(A.status, (unsigned)kErrRoundCap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *A.rounds = (unsigned long long)r;
+}
+
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+void run_adjoint(const Dev<Real> &P, const EulerProblem &p, EulerResult &res, DeviceBuffer<unsigned> &status,
+                 cudaStream_t s) {
+    constexpr int ND = NFWD + NSYM;
+    constexpr int NF = 2 * ND > 32 ? 32 : 2 * ND;
+    const long long N = P.g.ncells;
+    if (N >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large for the adjoint");
+    DeviceBuffer<int> fidx((size_t)NF * N), indeg0(N), indeg(N);
+    DeviceBuffer<double> fw((size_t)NF * N), var(N), acc(N), sens(N);
+    DeviceBuffer<uint8_t> nflow(N);
+    indeg0.zero(s);
+    flow_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(N, 128), 128, 0, s>>>(P, fidx.get(), fw.get(), var.get(),
+                                                                          nflow.get(), indeg0.get());
+    HFM_CUDA(cudaGetLastError());
+    DeviceBuffer<int> lists(3 * N);
+    DeviceBuffer<unsigned> counters(8);
+    const unsigned seed_cap = 1u << 20;
+    DeviceBuffer<long long> seed_idx(seed_cap);
+    DeviceBuffer<double> seed_w(seed_cap);
+    DeviceBuffer<unsigned long long> rounds(1);
+    AdjDev A{};
+    A.N = N;
+    A.fidx = fidx.get();
+    A.fw = fw.get();
+    A.var = var.get();
+    A.nflow = nflow.get();
+    A.indeg = indeg.get();
+    A.acc = acc.get();
+    A.sens = sens.get();
+    for (int i = 0; i < 3; ++i) { A.list[i] = lists.get() + i * N; A.count[i] = counters.get() + i; }
+    A.seed_count = counters.get() + 3;
+    A.bar_count = counters.get() + 4;
+    A.bar_gen = counters.get() + 5;
+    A.seed_idx = seed_idx.get();
+    A.seed_w = seed_w.get();
+    A.seed_cap = seed_cap;
+    A.status = status.get();
+    A.rounds = rounds.get();
+    A.max_rounds = N + 2;
+    int dev = 0, nsm = 0, per_sm = 0;
+    HFM_CUDA(cudaGetDevice(&dev));
+    HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 256, 0));
+    if (per_sm < 1) throw Error(HFM_ERR_CUDA, "adjoint kernel cannot be resident");
+    std::vector<double> hvals = res.values;
+    for (size_t gi = 0; gi < p.adjoint_index.size(); ++gi) {
+        HFM_CUDA(cudaMemcpyAsync(indeg.get(), indeg0.get(), N * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        acc.zero(s);
+        sens.zero(s);
+        counters.zero(s);
+        // std::map::insert keeps the first weight of a repeated point
+        std::vector<double> hacc_w;
+        std::vector<long long> hacc_i;
+        for (size_t k = 0; k < p.adjoint_index[gi].size(); ++k) {
+            const long long x = p.adjoint_index[gi][k];
+            if (std::find(hacc_i.begin(), hacc_i.end(), x) != hacc_i.end()) continue;
+            hacc_i.push_back(x);
+            hacc_w.push_back(p.adjoint_weight[gi][k]);
+        }
+        for (size_t k = 0; k < hacc_i.size(); ++k)
+            HFM_CUDA(cudaMemcpyAsync(acc.get() + hacc_i[k], &hacc_w[k], sizeof(double), cudaMemcpyHostToDevice, s));
+        HFM_CUDA(cudaStreamSynchronize(s));
+        adjoint_roots_kernel<<<nblocks(N, 256), 256, 0, s>>>(A);
+        void *args[] = {&A};
+        HFM_CUDA(cudaLaunchCooperativeKernel((void *)adjoint_kernel, dim3(nsm * per_sm), dim3(256), args, 0, s));
+        check_status(status, "adjoint");
+        AdjointResult ar;
+        ar.sensitivity.resize(N);
+        sens.download(ar.sensitivity.data(), N, s);
+        unsigned hc[8];
+        counters.download(hc, 8, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        const unsigned nseed = std::min(hc[3], seed_cap);
+        std::vector<long long> si(nseed);
+        std::vector<double> sw(nseed);
+        seed_idx.download(si.data(), nseed, s);
+        seed_w.download(sw.data(), nseed, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        std::vector<size_t> order(nseed);
+        for (size_t k = 0; k < nseed; ++k) order[k] = k;
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            const double va = hvals[si[a]], vb = hvals[si[b]];
+            return va != vb ? va > vb : si[a] > si[b];
+        });
+        for (size_t k : order) { ar.seed_index.push_back(si[k]); ar.seed_weight.push_back(sw[k]); }
+        res.adjoints.push_back(std::move(ar));
+    }
+}
+
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+void run_impl(const EulerProblem &p, EulerResult &res) {
+    constexpr int ND = NFWD + NSYM;
+    const auto wall_t0 = std::chrono::steady_clock::now();
+    cudaStream_t s = 0;
+    const GridGeom g = make_geom(p.ndim, p.dims, p.periodic);
+    const long long N = g.ncells, ntc = g.ntile * 64;
+    if (g.ntile >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large");
+    Dev<Real> P{};
+    P.g = g;
+    P.ntc = ntc;
+    HFM_TRACE("run_impl enter");
+    DeviceBuffer<unsigned> status(1);
+    status.zero(s);
+    HFM_TRACE("status alloc");
+    P.status = status.get();
+    DeviceBuffer<Real> values(N);
+    P.values = values.get();
+    fill_kernel<Real><<<nblocks(N, 256) > 4096 ? 4096 : nblocks(N, 256), 256, 0, s>>>(values.get(), N, Arith<Real>::inf());
+    EventTimer tm;
+
+    // ---- stencils
+    tm.start(s);
+    DeviceBuffer<unsigned> code, vis, maxw(1);
+    DeviceBuffer<Real> weight, mult, cls_w;
+    DeviceBuffer<int8_t> cls_off, plain_off;
+    DeviceBuffer<uint8_t> cls_en;
+    DeviceBuffer<double> metric, plain_w, mult_rm;
+    maxw.zero(s);
+    int max_width = 0;
+    if (!SHARE) {
+        code.alloc(ND * ntc);
+        code.zero(s);
+        weight.alloc(ND * ntc);
+        weight.zero(s);
+        P.code = code.get();
+        P.weight = weight.get();
+        metric.upload(p.metric, s);
+        if (p.want_stencils) {
+            plain_off.alloc(N * ND * 3);
+            plain_w.alloc(N * ND);
+        }
+        if (p.ndim == 2)
+            riemann_stencil_kernel<2, Real><<<nblocks(N, 128), 128, 0, s>>>(
+                g, ntc, metric.get(), p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
+                plain_off.get(), plain_w.get(), status.get());
+        else
+            riemann_stencil_kernel<3, Real><<<nblocks(N, 128), 128, 0, s>>>(
+                g, ntc, metric.get(), p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
+                plain_off.get(), plain_w.get(), status.get());
+        HFM_CUDA(cudaGetLastError());
+        HFM_TRACE("stencil kernel");
+        width_kernel<Real, NSYM><<<nblocks(N, 256), 256, 0, s>>>(P, maxw.get());
+        unsigned mw = 0;
+        maxw.download(&mw, 1, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        max_width = (int)mw;
+    } else {
+        std::vector<Real> w(p.cls_w.size());
+        for (size_t i = 0; i < w.size(); ++i) w[i] = (Real)p.cls_w[i];
+        cls_w.upload(w, s);
+        cls_off.upload(p.cls_off, s);
+        cls_en.upload(p.cls_enabled, s);
+        P.cls_w = cls_w.get();
+        P.cls_off = cls_off.get();
+        mult.alloc(ntc);
+        mult.zero(s);
+        P.mult = mult.get();
+        mult_rm.upload(p.mult, s);
+        mult_layout_kernel<Real><<<nblocks(N, 256), 256, 0, s>>>(g, mult_rm.get(), mult.get());
+        vis.alloc(ntc);
+        vis.zero(s);
+        P.vis = vis.get();
+        // width over the class tables, from each class centre (HFM_StencilShare.hxx:152-175)
+        const int NB = NFWD + 2 * NSYM;
+        for (int cl = 0; cl < p.nclass; ++cl)
+            for (int k = 0; k < ND; ++k) {
+                if (p.cls_w[cl * ND + k] == 0.0) continue;
+                const int8_t *o = &p.cls_off[(cl * ND + k) * 3];
+                for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
+                    const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
+                    if (!p.cls_enabled[cl * NB + slot]) continue;
+                    max_width = std::max(max_width, std::abs(o[0]) + std::abs(o[1]) + std::abs(o[2]));
+                }
+            }
+    }
+    res.max_stencil_width = max_width;
+
+    // ---- walls and visibility
+    DeviceBuffer<uint8_t> walls;
+    DeviceBuffer<int> wdist;
+    DeviceBuffer<int8_t> wd8;
+    if (!p.walls.empty()) {
+        walls.upload(p.walls, s);
+        wdist.alloc(N);
+        wd8.alloc(N);
+        wall_init_kernel<<<nblocks(N, 256), 256, 0, s>>>(N, walls.get(), wdist.get());
+        for (int a = 0; a < 3; ++a) {
+            if (g.dims[a] == 1) continue;
+            const long long nl = N / g.dims[a];
+            wall_scan_kernel<<<nblocks(nl, 128), 128, 0, s>>>(g, a, wdist.get());
+        }
+        wall_cap_kernel<<<nblocks(N, 256), 256, 0, s>>>(N, wdist.get(), max_width, wd8.get());
+        HFM_CUDA(cudaGetLastError());
+    }
+    HFM_TRACE("walls");
+    visibility_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(ntc, 128), 128, 0, s>>>(P, wd8.get(), cls_en.get());
+    HFM_CUDA(cudaGetLastError());
+    wdist.release();
+    HFM_TRACE("visibility");
+
+    // ---- seeds
+    const int ns = (int)p.seed_index.size();
+    DeviceBuffer<long long> sidx;
+    DeviceBuffer<double> sval;
+    if (ns) {
+        std::vector<long long> si(p.seed_index.begin(), p.seed_index.end());
+        sidx.upload(si, s);
+        sval.upload(p.seed_value, s);
+        seeds_kernel<Real, SHARE><<<nblocks(ns, 128), 128, 0, s>>>(P, sidx.get(), sval.get(), ns);
+    }
+
+    // ---- tile dependency graph (reverse CSR)
+    const long long nt = g.ntile;
+    HFM_TRACE("seeds");
+    DeviceBuffer<unsigned> dcnt(nt);
+    deps_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(nt, kDepWarps), kDepWarps * 32, 0, s>>>(
+        P, 0, dcnt.get(), nullptr, nullptr, nullptr, nullptr);
+    HFM_CUDA(cudaGetLastError());
+    DeviceBuffer<long long> doff(nt + 1), rptr(nt + 1);
+    {
+        std::vector<unsigned> hc(nt);
+        dcnt.download(hc.data(), nt, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        std::vector<long long> ho(nt + 1, 0);
+        long long tot = 0;
+        for (long long t = 0; t < nt; ++t) { ho[t] = tot; tot += hc[t]; }
+        ho[nt] = tot;
+        doff.upload(ho, s);
+        const long long nE = tot;
+        DeviceBuffer<int> esrc(nE), edst(nE);
+        DeviceBuffer<unsigned long long> emsk(nE);
+        if (nE)
+            deps_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(nt, kDepWarps), kDepWarps * 32, 0, s>>>(
+                P, 1, nullptr, doff.get(), esrc.get(), edst.get(), emsk.get());
+        DeviceBuffer<unsigned> rcnt(nt), cursor(nt);
+        rcnt.zero(s);
+        cursor.zero(s);
+        if (nE) dep_count_kernel<<<nblocks(nE, 256), 256, 0, s>>>(nE, esrc.get(), rcnt.get());
+        std::vector<unsigned> hr(nt);
+        rcnt.download(hr.data(), nt, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        std::vector<long long> hrp(nt + 1, 0);
+        tot = 0;
+        for (long long t = 0; t < nt; ++t) { hrp[t] = tot; tot += hr[t]; }
+        hrp[nt] = tot;
+        rptr.upload(hrp, s);
+        P.dep_ptr = rptr.get();
+        // reverse arrays live until the end of the solve
+        DeviceBuffer<int> rtile(nE);
+        DeviceBuffer<unsigned long long> rmask(nE);
+        if (nE)
+            dep_scatter_kernel<<<nblocks(nE, 256), 256, 0, s>>>(nE, esrc.get(), edst.get(), emsk.get(), rptr.get(),
+                                                                cursor.get(), rtile.get(), rmask.get());
+        HFM_CUDA(cudaGetLastError());
+        HFM_TRACE("deps");
+        P.dep_tile = rtile.get();
+        P.dep_mask = rmask.get();
+        res.t_stencil_ms = tm.stop(s);
+        check_status(status, "stencil");
+
+        // ---- solve
+        DeviceBuffer<int> lists(3 * nt);
+        DeviceBuffer<unsigned> counters(16), flags(3 * nt);
+        counters.zero(s);
+        flags.zero(s);
+        DeviceBuffer<unsigned long long> stats(4);
+        stats.zero(s);
+        for (int i = 0; i < 3; ++i) {
+            P.list[i] = lists.get() + i * nt;
+            P.flag[i] = flags.get() + i * nt;
+            P.count[i] = counters.get() + i;
+            P.claim[i] = counters.get() + 3 + i;
+        }
+        P.bar_count = counters.get() + 6;
+        P.bar_gen = counters.get() + 7;
+        P.stats = stats.get();
+        P.max_rounds = p.max_rounds;
+        P.sweeps = p.sweeps_per_tile;
+        // seed tiles and the cells they hold
+        std::vector<int> st;
+        std::vector<unsigned long long> sm;
+        for (int i = 0; i < ns; ++i) {
+            const long long x = p.seed_index[i];
+            const int x2 = (int)(x % g.dims[2]);
+            const long long rr = x / g.dims[2];
+            const int x1 = (int)(rr % g.dims[1]), x0 = (int)(rr / g.dims[1]);
+            const int T = (int)g.tile_of(x0, x1, x2);
+            const int b = g.local_of(x0, x1, x2);
+            auto it = std::find(st.begin(), st.end(), T);
+            if (it == st.end()) { st.push_back(T); sm.push_back(1ull << b); }
+            else sm[it - st.begin()] |= 1ull << b;
+        }
+        DeviceBuffer<int> stile;
+        DeviceBuffer<unsigned long long> smask;
+        tm.start(s);
+        if (!st.empty()) {
+            stile.upload(st, s);
+            smask.upload(sm, s);
+            init_lists_kernel<Real><<<nblocks((long long)st.size() * 32, 128), 128, 0, s>>>(P, stile.get(), smask.get(),
+                                                                                             (int)st.size());
+            HFM_CUDA(cudaGetLastError());
+            HFM_TRACE("init lists");
+            int dev = 0, nsm = 0, per_sm = 0;
+            HFM_CUDA(cudaGetDevice(&dev));
+            HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_kernel<Real, NFWD, NSYM, SHARE>,
+                                                                   kWarpsPerCta * 32, 0));
+            if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
+            const int grid = nsm * per_sm;
+            void *args[] = {&P};
+            HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, SHARE>, dim3(grid),
+                                                 dim3(kWarpsPerCta * 32), args, 0, s));
+        }
+        HFM_TRACE("fim kernel");
+        res.t_solve_ms = tm.stop(s);
+        check_status(status, "solver");
+        unsigned long long hs[4] = {0, 0, 0, 0};
+        stats.download(hs, 4, s);
+        DeviceBuffer<unsigned long long> nacc(1);
+        nacc.zero(s);
+        count_finite_kernel<Real><<<std::min<unsigned>(nblocks(N, 256), 2048), 256, 0, s>>>(values.get(), N, nacc.get());
+        unsigned long long hn = 0;
+        nacc.download(&hn, 1, s);
+        res.values.resize(N);
+        if (std::is_same<Real, double>::value) {
+            values.download(reinterpret_cast<Real *>(res.values.data()), N, s);
+        } else {
+            DeviceBuffer<double> vd(N);
+            to_double_kernel<Real><<<std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s>>>(values.get(), vd.get(), N);
+            vd.download(res.values.data(), N, s);
+            HFM_CUDA(cudaStreamSynchronize(s));
+        }
+        if (p.want_active) {
+            DeviceBuffer<unsigned long long> act(N);
+            active_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(N, 128), 128, 0, s>>>(P, act.get());
+            res.active.resize(N);
+            act.download(reinterpret_cast<unsigned long long *>(res.active.data()), N, s);
+        }
+        if (!p.adjoint_index.empty()) {
+            tm.start(s);
+            run_adjoint<Real, NFWD, NSYM, SHARE>(P, p, res, status, s);
+            res.t_adjoint_ms = tm.stop(s);
+        }
+        if (p.want_stencils && !SHARE) {
+            res.stencil_off.resize(N * ND * 3);
+            res.stencil_w.resize(N * ND);
+            plain_off.download(res.stencil_off.data(), N * ND * 3, s);
+            plain_w.download(res.stencil_w.data(), N * ND, s);
+        }
+        HFM_CUDA(cudaStreamSynchronize(s));
+        HFM_CUDA(cudaGetLastError());
+        res.n_accepted = (int64_t)hn;
+        res.rounds = (long long)hs[0];
+        res.tile_activations = (long long)hs[1];
+        res.local_solves = (long long)hs[2];
+    }
+    res.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall_t0).count();
+}
+
+}  // namespace detail
+
+using detail::run_impl;
+
+void solve_eulerian(const EulerProblem &p, EulerResult &r) {
+    if (p.kind == StencilKind::RiemannPerCell) {
+        if (p.ndim == 2) {
+            if (p.fp64) run_impl<double, 0, 3, false>(p, r);
+            else run_impl<float, 0, 3, false>(p, r);
+        } else if (p.ndim == 3) {
+            if (p.fp64) run_impl<double, 0, 6, false>(p, r);
+            else run_impl<float, 0, 6, false>(p, r);
+        } else {
+            throw Error(HFM_ERR_UNSUPPORTED, "Riemann models support dimensions 2 and 3");
+        }
+    } else {
+        if (p.nfwd == 0 && p.nsym == 4) {
+            if (p.fp64) run_impl<double, 0, 4, true>(p, r);
+            else run_impl<float, 0, 4, true>(p, r);
+        } else if (p.nfwd == 27 && p.nsym == 0) {
+            if (p.fp64) run_impl<double, 27, 0, true>(p, r);
+            else run_impl<float, 27, 0, true>(p, r);
+        } else {
+            throw Error(HFM_ERR_UNSUPPORTED, "unsupported shared stencil shape");
+        }
+    }
+}
+
+}  // namespace hfm

@@ -1,0 +1,94 @@
+// Key-value store with the reference IO semantics (host side of the C ABI).
+//
+// Follows JMM_CPPLibs/JMM_CPPLibs/Output/BaseIO.h:16-43 / BaseIO.hxx:8-160 (raw elements, setter
+// tags, the unused/defaulted/visitedUnset bookkeeping and UsageReport) and IO.hxx:33-170 (typed
+// getters with defaults, the four array orderings). Internally every domain array is RowMajor
+// with axes in (x, y, z|theta) order and the component axis last.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace hfm {
+
+// Error carrying an hfm_b200.h status code.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+enum class Setter { User, Compute, Unknown };
+enum class Ordering { RowMajor = 0, ColumnMajor = 1, YXZ_RowMajor = 2, YXZ_ColumnMajor = 3 };
+
+struct RawElement {
+    std::string str;
+    std::vector<int64_t> dims;
+    std::vector<double> data;
+    Setter setter = Setter::Unknown;
+    bool is_string() const { return data.empty() && dims.empty(); }
+    bool is_scalar() const { return !data.empty() && dims.empty(); }
+};
+
+// A domain field read from the store: RowMajor over `dims` (x, y, z order), `ncomp` components
+// per point (component fastest). `dims` is empty for a constant field given as a single element.
+struct Field {
+    std::vector<int64_t> dims;
+    int ncomp = 1;
+    std::vector<double> data;
+    bool constant() const { return dims.empty(); }
+};
+
+class Store {
+public:
+    explicit Store(Ordering def) : default_ordering_(def), ordering_(def) {}
+
+    Setter current_setter = Setter::User;
+    int verbosity = 1;
+
+    // --- raw access (BaseIO) ---
+    bool has_field(const std::string &key) const;
+    bool erase_field(const std::string &key);
+    std::string get_string(const std::string &key) const;
+    void set_string(const std::string &key, const std::string &val);
+    void set_scalar(const std::string &key, double v);
+    void set_array(const std::string &key, const double *data, const std::vector<int64_t> &dims);
+    const RawElement &raw(const std::string &key, bool for_use = true) const;
+    std::string computed_keys() const;
+    void usage_report();
+
+    // --- typed getters (IO_) ---
+    double get_scalar(const std::string &key) const;
+    double get_scalar(const std::string &key, double def, int verb = 1) const;
+    std::string get_string(const std::string &key, const std::string &def, int verb = 1) const;
+    // Vector of points / scalars: raw dims (n) or (n, ncomp); ordering does not apply to vectors.
+    std::vector<double> get_vector(const std::string &key, int ncomp, int64_t *count) const;
+    // Domain field: depth must be `ndim` (or 0 for a constant element); component axis last.
+    Field get_field(const std::string &key, int ndim, int ncomp) const;
+    std::vector<int64_t> field_domain_dims(const std::string &key, int ncomp) const;
+    // Output of a RowMajor domain array (x, y, z order) with `ncomp` trailing components.
+    void set_field(const std::string &key, const std::vector<int64_t> &dims, int ncomp,
+                   const double *data);
+    void set_vector(const std::string &key, int64_t count, int ncomp, const double *data);
+
+    void set_ordering(Ordering o) { ordering_ = o; }
+    Ordering ordering() const { return ordering_; }
+    Ordering default_ordering() const { return default_ordering_; }
+
+    void msg(const std::string &m) const;
+    void warn(const std::string &m) const;
+
+private:
+    RawElement &create(const std::string &key);
+    std::map<std::string, RawElement> elems_;
+    mutable std::set<std::string> unused_, defaulted_, visited_unset_;
+    Ordering default_ordering_, ordering_;
+};
+
+const char *ordering_name(Ordering o);
+bool ordering_from_name(const std::string &s, Ordering *o);
+
+}  // namespace hfm

@@ -1,0 +1,610 @@
+// hfm_run: the reference's Run(IO&) for the GPU solve path, and the C ABI of include/hfm_b200.h.
+//
+// Orchestration mirrors HFMInterface<T>::Run (Headers/Base/Implementation/HFMInterface.hxx:296-579):
+// set up IO (verbosity, arrayOrdering), read the model's fields (Riemannian.h:46-61,
+// Curvature2.h:61-66 and 219-224, HFM_StencilShare.hxx:61-71), place seeds (StaticFactoring.hxx:242-393),
+// solve, export values / activeNeighs / sensitivities, then IO::UsageReport (BaseIO.hxx:64-104).
+// Options outside the GPU path fail with HFM_ERR_UNSUPPORTED instead of being ignored.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <sstream>
+
+#include "common.cuh"
+#include "io.hpp"
+#include "solver.hpp"
+
+struct hfm_io {
+    hfm::Store store;
+    std::string last_error;
+    explicit hfm_io(hfm::Ordering o) : store(o) {}
+};
+
+namespace hfm {
+namespace {
+
+const double kPi = 3.141592653589793238462643383279502884;
+
+struct Param {
+    int ndim = 2;
+    int dims[3] = {1, 1, 1};
+    int periodic[3] = {0, 0, 0};
+    double origin[3] = {0, 0, 0};
+    double scale[3] = {1, 1, 1};  // grid scale per axis (dependScale on the angular axis)
+    // point -> index (HFM_ParamDefault.hxx ADim + BaseGrid::IndexFromPoint + PeriodizeNoBase)
+    bool index_of(const double *p, int64_t *lin) const {
+        int64_t r = 0;
+        for (int a = 0; a < ndim; ++a) {
+            long long i = (long long)std::floor((p[a] - origin[a]) / scale[a]);
+            if (periodic[a]) {
+                i %= dims[a];
+                if (i < 0) i += dims[a];
+            } else if (i < 0 || i >= dims[a]) {
+                return false;
+            }
+            r = r * dims[a] + i;
+        }
+        *lin = r;
+        return true;
+    }
+};
+
+std::vector<int> read_dims(Store &io, int ndim) {
+    int64_t n = 0;
+    std::vector<double> d = io.get_vector("dims", 1, &n);
+    if ((int)n != ndim)
+        throw Error(HFM_ERR_VALUE, "dims must have " + std::to_string(ndim) + " entries, found " + std::to_string(n));
+    std::vector<int> out(ndim);
+    for (int a = 0; a < ndim; ++a) {
+        out[a] = (int)d[a];
+        if (out[a] <= 0) throw Error(HFM_ERR_VALUE, "BaseGrid error : domain size must be positive");
+    }
+    return out;
+}
+
+std::vector<double> read_point(Store &io, const std::string &key, int n, const std::vector<double> &def) {
+    if (!io.has_field(key)) {
+        std::ostringstream o;
+        o << "{";
+        for (int i = 0; i < n; ++i) o << (i ? "," : "") << def[i];
+        o << "}";
+        if (io.verbosity >= 1) io.msg("Field " + key + " defaults to " + o.str() + "\n");
+        io.get_scalar(key, 0.0, 99);  // record as defaulted (message already printed)
+        return def;
+    }
+    int64_t cnt = 0;
+    const RawElement &r = io.raw(key);
+    if (r.dims.size() != 1 || r.dims[0] != n)
+        throw Error(HFM_ERR_VALUE, "Field " + key + " must be a vector of " + std::to_string(n) + " entries");
+    (void)cnt;
+    return r.data;
+}
+
+void reject_unsupported(Store &io) {
+    static const char *keys[] = {"tips", "tips_Unoriented", "factoringValues", "speed_times", "cost_times",
+                                 "metric_times", "dualMetric_times", "stopAtDistance", "nMaxAccepted",
+                                 "stopWhenAnyAccepted", "stopWhenAllAccepted", "stopWhenAnyAccepted_Unoriented",
+                                 "stopWhenAllAccepted_Unoriented", "costVariation", "seedValueVariation",
+                                 "euclideanScale", "seedFlags", "getStencils", "activeNeighs", "values",
+                                 "factoringPointChoice"};
+    for (const char *k : keys)
+        if (io.has_field(k))
+            throw Error(HFM_ERR_UNSUPPORTED, std::string("option '") + k + "' is not supported by the GPU solve path");
+    if (io.has_field("factoringRadius") && io.get_scalar("factoringRadius") != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, "option 'factoringRadius' (static factoring) is not supported by the GPU solve path");
+    if (io.has_field("order") && io.get_scalar("order") != 1)
+        throw Error(HFM_ERR_UNSUPPORTED, "only order=1 is supported by the GPU solve path");
+    if (io.get_scalar("exportGeodesicFlow", 0.0, 2) != 0 || io.get_scalar("exportActiveOffsets", 0.0, 3) != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, "geodesic flow exports are not supported by the GPU solve path");
+    if (io.get_scalar("refineStencilAtWallBoundary", 0.0, 3) != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, "refineStencilAtWallBoundary is not supported by the GPU solve path");
+}
+
+// Seeds: points -> unique indices (first value kept), sorted; seedRadius must be 0.
+void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_allowed) {
+    std::map<int64_t, double> seeds;
+    std::vector<double> pts;
+    int64_t n = 0;
+    if (io.has_field("seeds")) {
+        pts = io.get_vector("seeds", pm.ndim, &n);
+        std::vector<double> vals(n, 0.0);
+        if (io.has_field("seedValues")) {
+            int64_t nv = 0;
+            vals = io.get_vector("seedValues", 1, &nv);
+            if (nv != n) throw Error(HFM_ERR_VALUE, "Error : Inconsistent size of seedValues.");
+        }
+        const double radius = io.get_scalar("seedRadius", 0.0);
+        if (radius != 0) throw Error(HFM_ERR_UNSUPPORTED, "seedRadius != 0 is not supported by the GPU solve path");
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t lin;
+            if (!pm.index_of(&pts[i * pm.ndim], &lin)) {
+                std::ostringstream o;
+                o << "Error : seed {";
+                for (int a = 0; a < pm.ndim; ++a) o << (a ? "," : "") << pts[i * pm.ndim + a];
+                o << "} is out of range.\n";
+                io.warn(o.str());
+                continue;
+            }
+            seeds.emplace(lin, vals[i]);
+        }
+    }
+    int64_t nu = 0;
+    if (unoriented_allowed && io.has_field("seeds_Unoriented")) {
+        std::vector<double> up = io.get_vector("seeds_Unoriented", 2, &nu);
+        std::vector<double> uv(nu, 0.0);
+        if (io.has_field("seedValues_Unoriented")) {
+            int64_t nv = 0;
+            uv = io.get_vector("seedValues_Unoriented", 1, &nv);
+            if (nv != nu) throw Error(HFM_ERR_VALUE, "Error : Inconsistent size of seedValues_Unoriented.");
+        }
+        for (int64_t i = 0; i < nu; ++i)
+            for (int t = 0; t < pm.dims[2]; ++t) {
+                const double q[3] = {up[2 * i], up[2 * i + 1], pm.origin[2] + (t + 0.5) * pm.scale[2]};
+                int64_t lin;
+                if (!pm.index_of(q, &lin)) continue;
+                seeds.emplace(lin, uv[i]);
+            }
+    }
+    if (seeds.empty() && (n + nu) > 0) throw Error(HFM_ERR_VALUE, "Error : seeds incorrectly set");
+    for (const auto &kv : seeds) {
+        p.seed_index.push_back(kv.first);
+        p.seed_value.push_back(kv.second);
+    }
+}
+
+// A scalar field over the lifted grid given with depth 0 (constant), 3 (full), 2 (physical x,y)
+// or 1 (angle only) (HFMInterface.hxx:23-32).
+std::vector<double> read_lifted_scalar(Store &io, const std::string &key, const int *dims) {
+    const std::vector<int64_t> dd = io.field_domain_dims(key, 1);
+    const int depth = (int)dd.size();
+    const int64_t N = (int64_t)dims[0] * dims[1] * dims[2];
+    std::vector<double> out(N);
+    Field f = io.get_field(key, depth, 1);
+    if (depth == 0) {
+        std::fill(out.begin(), out.end(), f.data[0]);
+    } else if (depth == 3) {
+        if (f.dims[0] != dims[0] || f.dims[1] != dims[1] || f.dims[2] != dims[2])
+            throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+        out = f.data;
+    } else if (depth == 2) {
+        if (f.dims[0] != dims[0] || f.dims[1] != dims[1])
+            throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+        for (int64_t i = 0; i < (int64_t)dims[0] * dims[1]; ++i)
+            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.data[i];
+    } else if (depth == 1) {
+        if (f.dims[0] != dims[2]) throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+        for (int64_t i = 0; i < (int64_t)dims[0] * dims[1]; ++i)
+            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.data[t];
+    } else {
+        throw Error(HFM_ERR_VALUE, "Field " + key + " has incorrect depth.\n");
+    }
+    return out;
+}
+
+std::vector<uint8_t> read_walls(Store &io, const Param &pm, bool lifted) {
+    std::vector<uint8_t> w;
+    if (!io.has_field("walls")) return w;
+    const int64_t N = (int64_t)pm.dims[0] * pm.dims[1] * pm.dims[2];
+    std::vector<double> v;
+    if (lifted) {
+        v = read_lifted_scalar(io, "walls", pm.dims);
+    } else {
+        const std::vector<int64_t> dd = io.field_domain_dims("walls", 1);
+        Field f = io.get_field("walls", dd.empty() ? 0 : pm.ndim, 1);
+        if (f.constant()) v.assign(N, f.data[0]);
+        else {
+            for (int a = 0; a < pm.ndim; ++a)
+                if (f.dims[a] != pm.dims[a]) throw Error(HFM_ERR_VALUE, "Error : walls have inconsistent dims");
+            v = f.data;
+        }
+    }
+    w.resize(N);
+    for (int64_t i = 0; i < N; ++i) w[i] = v[i] != 0.0;  // GetIntegralField<bool>: (bool)double
+    return w;
+}
+
+void set_common_solver_options(Store &io, EulerProblem &p) {
+    const std::string prec = io.get_string("solverPrecision", "float64", 2);
+    if (prec == "float64") p.fp64 = true;
+    else if (prec == "float32") p.fp64 = false;
+    else throw Error(HFM_ERR_VALUE, "solverPrecision must be float64 or float32");
+    p.sweeps_per_tile = (int)io.get_scalar("tileSweeps", 16, 3);
+    if (p.sweeps_per_tile < 1 || p.sweeps_per_tile > 1024) throw Error(HFM_ERR_VALUE, "tileSweeps out of range");
+    p.max_rounds = (int)io.get_scalar("maxRounds", (double)(1 << 20), 3);
+}
+
+// ------------------------------------------------------------------------------------------
+void setup_riemann(Store &io, int ndim, Param &pm, EulerProblem &p) {
+    const std::vector<int> dims = read_dims(io, ndim);
+    pm.ndim = ndim;
+    for (int a = 0; a < ndim; ++a) pm.dims[a] = dims[a];
+    const std::vector<double> origin = read_point(io, "origin", ndim, std::vector<double>(ndim, 0.0));
+    std::vector<double> hs(ndim);
+    if (io.has_field("gridScales")) {
+        hs = read_point(io, "gridScales", ndim, hs);
+    } else {
+        const double h = io.get_scalar("gridScale");
+        std::fill(hs.begin(), hs.end(), h);
+    }
+    for (int a = 0; a < ndim; ++a) {
+        if (!(hs[a] > 0)) throw Error(HFM_ERR_VALUE, "Parametrization error : gridscales should be positive");
+        pm.origin[a] = origin[a];
+        pm.scale[a] = hs[a];
+        p.h[a] = hs[a];
+        p.dims[a] = dims[a];
+    }
+    p.ndim = ndim;
+    p.kind = StencilKind::RiemannPerCell;
+    const int ns = ndim * (ndim + 1) / 2;
+    std::string key = "metric";
+    if (io.has_field("dualMetric")) {
+        if (io.has_field("metric")) throw Error(HFM_ERR_VALUE, "Error: both primal and dual metric provided");
+        key = "dualMetric";
+        p.dual = true;
+    }
+    const std::vector<int64_t> dd = io.field_domain_dims(key, ns);
+    Field f = io.get_field(key, dd.empty() ? 0 : ndim, ns);
+    if (!f.constant()) {
+        for (int a = 0; a < ndim; ++a)
+            if (f.dims[a] != dims[a]) throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+    }
+    p.metric_constant = f.constant();
+    p.metric = std::move(f.data);
+}
+
+void setup_isotropic2(Store &io, Param &pm, EulerProblem &p) {
+    // Isotropic2 solved as the Riemann metric cost^2 Id: its 4-point stencil is what Selling returns
+    // for a multiple of the identity, so values match the reference's isotropic scheme.
+    const std::vector<int> dims = read_dims(io, 2);
+    pm.ndim = 2;
+    p.ndim = 2;
+    const std::vector<double> origin = read_point(io, "origin", 2, {0.0, 0.0});
+    const double h = io.get_scalar("gridScale");
+    for (int a = 0; a < 2; ++a) {
+        pm.dims[a] = p.dims[a] = dims[a];
+        pm.origin[a] = origin[a];
+        pm.scale[a] = p.h[a] = h;
+    }
+    p.kind = StencilKind::RiemannPerCell;
+    const int64_t N = (int64_t)dims[0] * dims[1];
+    std::vector<double> speed;
+    const char *key = io.has_field("speed") ? "speed" : "cost";
+    const std::vector<int64_t> dd = io.field_domain_dims(key, 1);
+    Field f = io.get_field(key, dd.empty() ? 0 : 2, 1);
+    p.metric.resize(f.constant() ? 3 : N * 3);
+    p.metric_constant = f.constant();
+    for (size_t i = 0; i < f.data.size(); ++i) {
+        const double c = (std::string(key) == "speed") ? 1.0 / f.data[i] : f.data[i];
+        p.metric[3 * i] = c * c;
+        p.metric[3 * i + 1] = 0.0;
+        p.metric[3 * i + 2] = c * c;
+    }
+}
+
+void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProblem &p) {
+    const std::vector<int> dims = read_dims(io, 3);
+    pm.ndim = 3;
+    p.ndim = 3;
+    for (int a = 0; a < 3; ++a) pm.dims[a] = p.dims[a] = dims[a];
+    pm.periodic[2] = p.periodic[2] = 1;
+    const bool rs = model == "ReedsShepp2";
+    const double eps = io.get_scalar("eps", 0.1);
+    const double xi = io.get_scalar("xi", 1.0);
+    const bool projective = rs ? io.get_scalar("projective", 0.0) != 0 : false;
+    const double h = io.get_scalar("gridScale");
+    if (!(h > 0)) throw Error(HFM_ERR_VALUE, "Parametrization error : gridscale should be positive");
+    const double ds = ((projective ? kPi : 2.0 * kPi)) / (double)dims[2];
+    const std::vector<double> origin = read_point(io, "origin", 2, {0.0, 0.0});
+    pm.origin[0] = origin[0];
+    pm.origin[1] = origin[1];
+    pm.origin[2] = -ds / 2.0;
+    pm.scale[0] = pm.scale[1] = h;
+    pm.scale[2] = ds;
+    p.kind = StencilKind::SharedByTheta;
+    p.nclass = dims[2];
+    if (rs) {
+        p.nfwd = 0;
+        p.nsym = 4;
+        reedsshepp2_table(dims[2], h, xi, eps, projective, p.cls_off, p.cls_w);
+    } else {
+        p.nfwd = 27;
+        p.nsym = 0;
+        elastica2_table(dims[2], h, xi, eps, p.cls_off, p.cls_w);
+    }
+    // Slots reachable from each class centre (dims/2, dims/2, theta) (HFM_StencilShare.hxx:114-175).
+    const int ND = p.nfwd + p.nsym, NB = p.nfwd + 2 * p.nsym;
+    p.cls_enabled.assign((size_t)p.nclass * NB, 0);
+    for (int c = 0; c < p.nclass; ++c)
+        for (int k = 0; k < ND; ++k) {
+            const int8_t *o = &p.cls_off[(c * ND + k) * 3];
+            for (int si = 0; si < (k < p.nfwd ? 1 : 2); ++si) {
+                const int s = si ? -1 : 1;
+                const int slot = k < p.nfwd ? k : p.nfwd + 2 * (k - p.nfwd) + si;
+                const int y0 = dims[0] / 2 + s * o[0], y1 = dims[1] / 2 + s * o[1];
+                p.cls_enabled[c * NB + slot] = (y0 >= 0 && y0 < dims[0] && y1 >= 0 && y1 < dims[1]) ? 1 : 0;
+            }
+        }
+    if (io.has_field("speed")) {
+        p.mult = read_lifted_scalar(io, "speed", dims.data());
+    } else {
+        std::vector<double> cost = read_lifted_scalar(io, "cost", dims.data());
+        for (double &c : cost) c = 1. / c;  // DataSource_Inverse (HFMInterface.hxx:131-150)
+        p.mult = std::move(cost);
+    }
+}
+
+void run_model(Store &io, const std::string &model) {
+    // Run_SetupIO (HFMInterface.hxx:311-341)
+    io.verbosity = (int)io.get_scalar("verbosity", io.verbosity);
+    if (io.has_field("keyHelp")) io.get_string("keyHelp");
+    const std::string ord = io.get_string("arrayOrdering", ordering_name(io.ordering()));
+    Ordering o;
+    if (!ordering_from_name(ord, &o)) throw Error(HFM_ERR_VALUE, "Error : unrecognized array ordering");
+    io.set_ordering(o);
+    reject_unsupported(io);
+
+    Param pm;
+    EulerProblem p;
+    const bool lifted = model == "ReedsShepp2" || model == "Elastica2";
+    if (model == "Riemann2") setup_riemann(io, 2, pm, p);
+    else if (model == "Riemann3") setup_riemann(io, 3, pm, p);
+    else if (model == "Isotropic2") setup_isotropic2(io, pm, p);
+    else if (lifted) setup_curvature(io, model, pm, p);
+    else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);
+    set_common_solver_options(io, p);
+    p.walls = read_walls(io, pm, lifted);
+    read_seeds(io, pm, p, lifted);
+
+    const bool export_values = io.get_scalar("exportValues", 0.0, 2) != 0;
+    const bool export_active = io.get_scalar("exportActiveNeighs", 0.0, 3) != 0;
+    const bool inspect = io.has_field("inspectSensitivity");
+    p.want_active = export_active;
+
+    std::vector<int64_t> dims(pm.dims, pm.dims + pm.ndim);
+    if (p.seed_index.empty()) {
+        io.warn("No seeds to run fast marching solver, and missing values or activeNeighs to compute geodesics.\n");
+        return;
+    }
+    if (inspect) {
+        // FirstVariation::Finally (FirstVariation.h:60-102): groups of weighted points
+        int64_t n = 0;
+        const std::vector<double> pts = io.get_vector("inspectSensitivity", pm.ndim, &n);
+        std::vector<double> lengths(n, 1.0);
+        if (io.has_field("inspectSensitivityLengths")) {
+            int64_t nl = 0;
+            lengths = io.get_vector("inspectSensitivityLengths", 1, &nl);
+            double tot = 0;
+            for (double l : lengths) tot += l;
+            if (tot != (double)n) throw Error(HFM_ERR_VALUE, "Error : inconsistent inspectSensitivityLengths");
+        }
+        std::vector<double> weights(n, 1.0);
+        if (io.has_field("inspectSensitivityWeights")) {
+            int64_t nw = 0;
+            weights = io.get_vector("inspectSensitivityWeights", 1, &nw);
+            if (nw != n) throw Error(HFM_ERR_VALUE, "Error: Inconsistent inspectSensitivityWeights size");
+        }
+        int64_t pos = 0;
+        for (size_t gi = 0; gi < lengths.size(); ++gi) {
+            std::vector<int64_t> idx;
+            std::vector<double> wts;
+            for (int64_t k = 0; k < (int64_t)lengths[gi]; ++k, ++pos) {
+                int64_t lin;
+                if (!pm.index_of(&pts[pos * pm.ndim], &lin))
+                    throw Error(HFM_ERR_VALUE, "Error : inspectSensitivity data points are out of range");
+                idx.push_back(lin);
+                wts.push_back(weights[pos]);
+            }
+            p.adjoint_index.push_back(std::move(idx));
+            p.adjoint_weight.push_back(std::move(wts));
+        }
+    }
+    EulerResult r;
+    solve_eulerian(p, r);
+
+    // Outputs (Run_SetupSolver/Run_RunSolver/Run_ExportData, CommonStoppingCriteria::Finally)
+    io.set_scalar("MaxStencilWidth", r.max_stencil_width);
+    io.set_scalar("StencilCPUTime", r.t_stencil_ms * 1e-3);
+    io.set_scalar("FMCPUTime", r.t_solve_ms * 1e-3);
+    io.set_scalar("GeodesicCPUTime", 0.0);
+    io.set_scalar("GPUStencilTime", r.t_stencil_ms * 1e-3);
+    io.set_scalar("GPUSolveTime", r.t_solve_ms * 1e-3);
+    io.set_scalar("solverRounds", (double)r.rounds);
+    io.set_scalar("tileActivations", (double)r.tile_activations);
+    io.set_scalar("executedUpdates", (double)r.local_solves);
+    if (io.verbosity >= 1) {
+        std::ostringstream m;
+        m << "Fast marching solver completed in " << r.t_solve_ms * 1e-3 << " s.\n";
+        io.msg(m.str());
+    }
+    if (export_values) io.set_field("values", dims, 1, r.values.data());
+    if (export_active) {
+        std::vector<double> a(r.active.size());
+        for (size_t i = 0; i < a.size(); ++i) a[i] = (double)r.active[i];
+        io.set_field("activeNeighs", dims, 1, a.data());
+    }
+    for (size_t gi = 0; gi < r.adjoints.size(); ++gi) {
+        const AdjointResult &ar = r.adjoints[gi];
+        io.set_field("costSensitivity_" + std::to_string(gi), dims, 1, ar.sensitivity.data());
+        std::vector<double> ss;
+        for (size_t k = 0; k < ar.seed_index.size(); ++k) {
+            int64_t x = ar.seed_index[k];
+            double q[3];
+            for (int a = pm.ndim - 1; a >= 0; --a) {
+                const int64_t i = x % pm.dims[a];
+                x /= pm.dims[a];
+                q[a] = (i + 0.5) * pm.scale[a] + pm.origin[a];  // ReDim(PointFromIndex)
+            }
+            for (int a = 0; a < pm.ndim; ++a) ss.push_back(q[a]);
+            ss.push_back(ar.seed_weight[k]);
+        }
+        io.set_vector("seedSensitivity_" + std::to_string(gi), (int64_t)ar.seed_index.size(), pm.ndim + 1,
+                      ss.data());
+    }
+    io.set_scalar("nAccepted", (double)r.n_accepted);
+}
+
+}  // namespace
+}  // namespace hfm
+
+// =============================================================================== C ABI
+using hfm::Error;
+
+template <typename F>
+static int guarded(hfm_io *io, F f) {
+    if (!io) return HFM_ERR_ARG;
+    io->last_error.clear();
+    try {
+        f();
+        return HFM_OK;
+    } catch (const Error &e) {
+        io->last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        io->last_error = "host allocation failure";
+        return HFM_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        io->last_error = e.what();
+        return HFM_ERR_VALUE;
+    }
+}
+
+extern "C" {
+
+hfm_io *hfm_io_create(int default_ordering) {
+    if (default_ordering < 0 || default_ordering > 3) return nullptr;
+    try {
+        return new hfm_io(static_cast<hfm::Ordering>(default_ordering));
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+void hfm_io_destroy(hfm_io *io) { delete io; }
+
+int hfm_io_set_scalar(hfm_io *io, const char *key, double value) {
+    return guarded(io, [&] {
+        if (!key) throw Error(HFM_ERR_ARG, "null key");
+        io->store.set_scalar(key, value);
+    });
+}
+
+int hfm_io_set_string(hfm_io *io, const char *key, const char *value) {
+    return guarded(io, [&] {
+        if (!key || !value) throw Error(HFM_ERR_ARG, "null argument");
+        io->store.set_string(key, value);
+    });
+}
+
+int hfm_io_set_array(hfm_io *io, const char *key, const double *data, int ndim, const int64_t *shape) {
+    return guarded(io, [&] {
+        if (!key || ndim < 0 || (ndim > 0 && !shape)) throw Error(HFM_ERR_ARG, "null argument");
+        std::vector<int64_t> dims(shape, shape + ndim);
+        int64_t n = 1;
+        for (int64_t d : dims) n *= d;
+        if (n > 0 && !data) throw Error(HFM_ERR_ARG, "null data");
+        io->store.set_array(key, data, dims);
+    });
+}
+
+int hfm_io_get_scalar(hfm_io *io, const char *key, double *value) {
+    return guarded(io, [&] {
+        if (!key || !value) throw Error(HFM_ERR_ARG, "null argument");
+        *value = io->store.get_scalar(key);
+    });
+}
+
+int hfm_io_get_string(hfm_io *io, const char *key, char *buf, size_t cap, size_t *len) {
+    return guarded(io, [&] {
+        if (!key) throw Error(HFM_ERR_ARG, "null key");
+        const std::string s = io->store.get_string(key);
+        if (len) *len = s.size();
+        if (buf && cap) {
+            const size_t n = std::min(cap - 1, s.size());
+            std::memcpy(buf, s.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+int hfm_io_get_array_info(hfm_io *io, const char *key, int *ndim, int64_t *shape, int max_ndim) {
+    return guarded(io, [&] {
+        if (!key || !ndim) throw Error(HFM_ERR_ARG, "null argument");
+        const hfm::RawElement &r = io->store.raw(key, false);
+        if (r.is_string()) throw Error(HFM_ERR_KEY, "PythonIO error : field " + std::string(key) + " is a string, not an array");
+        *ndim = (int)r.dims.size();
+        for (int i = 0; i < *ndim && i < max_ndim; ++i)
+            if (shape) shape[i] = r.dims[i];
+    });
+}
+
+int hfm_io_get_array(hfm_io *io, const char *key, double *out, size_t count) {
+    return guarded(io, [&] {
+        if (!key || (count && !out)) throw Error(HFM_ERR_ARG, "null argument");
+        const hfm::RawElement &r = io->store.raw(key);
+        if (r.is_string()) throw Error(HFM_ERR_KEY, "PythonIO error : field " + std::string(key) + " is a string, not an array");
+        if (r.dims.empty()) throw Error(HFM_ERR_KEY, "PythonIO error : field " + std::string(key) + " is a scalar, not an array");
+        if (count != r.data.size()) throw Error(HFM_ERR_ARG, "buffer size does not match field " + std::string(key));
+        std::memcpy(out, r.data.data(), count * sizeof(double));
+    });
+}
+
+int hfm_io_has_field(hfm_io *io, const char *key) {
+    if (!io || !key) return -HFM_ERR_ARG;
+    return io->store.has_field(key) ? 1 : 0;
+}
+
+int hfm_io_erase_field(hfm_io *io, const char *key) {
+    return guarded(io, [&] {
+        if (!key) throw Error(HFM_ERR_ARG, "null key");
+        if (!io->store.erase_field(key)) throw Error(HFM_ERR_KEY, "field " + std::string(key) + " not found");
+    });
+}
+
+int hfm_io_computed_keys(hfm_io *io, char *buf, size_t cap, size_t *len) {
+    return guarded(io, [&] {
+        const std::string s = io->store.computed_keys();
+        if (len) *len = s.size();
+        if (buf && cap) {
+            const size_t n = std::min(cap - 1, s.size());
+            std::memcpy(buf, s.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+int hfm_run(hfm_io *io, const char *expected_model) {
+    return guarded(io, [&] {
+        hfm::Store &st = io->store;
+        const std::string model = st.get_string("model");
+        if (expected_model && model != expected_model)
+            throw Error(HFM_ERR_VALUE, std::string("Executable applies to ") + expected_model + ", not to " + model + ".");
+        st.current_setter = hfm::Setter::Compute;
+        struct Restore {
+            hfm::Store &s;
+            ~Restore() { s.current_setter = hfm::Setter::User; }
+        } restore{st};
+        hfm::run_model(st, model == "Elastica2_5" ? "Elastica2" : model);
+        st.usage_report();
+    });
+}
+
+const char *hfm_io_last_error(hfm_io *io) { return io ? io->last_error.c_str() : "null hfm_io"; }
+
+const char *hfm_version(void) { return "hfm_b200 0.1 (sm_100a)"; }
+
+int hfm_device_count(int *count) {
+    if (!count) return HFM_ERR_ARG;
+    const cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? HFM_OK : HFM_ERR_CUDA;
+    }
+    return HFM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,80 @@
+// Host interface of the GPU solve path for Eulerian schemes (Riemann, ReedsShepp2, Elastica2).
+//
+// The host orchestration (run.cpp) turns hfmIn keys into an EulerProblem; solve_eulerian builds the
+// stencils on the GPU, computes wall visibility, runs the tiled fast-iterative solver to the
+// upwind fixed point of the reference's fast marching, and returns the arrival times.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace hfm {
+
+enum class StencilKind {
+    RiemannPerCell,   // Selling stencil of a metric at every cell (Recomp policy)
+    SharedByTheta,    // one stencil per index of the last axis times a speed multiplier (Share policy)
+};
+
+struct EulerProblem {
+    int ndim = 2;
+    int dims[3] = {1, 1, 1};
+    int periodic[3] = {0, 0, 0};
+    bool fp64 = true;
+    StencilKind kind = StencilKind::RiemannPerCell;
+
+    // RiemannPerCell: packed metric (xx,xy,yy[,xz,yz,zz]) RowMajor, one per cell or a single one.
+    std::vector<double> metric;
+    bool metric_constant = false;
+    bool dual = false;
+    double h[3] = {1, 1, 1};
+
+    // SharedByTheta: nclass stencils of nfwd forward + nsym symmetric differences.
+    int nfwd = 0, nsym = 0, nclass = 0;
+    std::vector<int8_t> cls_off;       // [nclass][nfwd+nsym][3]
+    std::vector<double> cls_w;         // [nclass][nfwd+nsym]
+    std::vector<uint8_t> cls_enabled;  // [nclass][nfwd+2*nsym] slot reachable from the class centre
+    std::vector<double> mult;          // [N] speed multiplier (RowMajor)
+
+    std::vector<uint8_t> walls;        // [N] or empty
+    std::vector<int64_t> seed_index;   // sorted, unique
+    std::vector<double> seed_value;
+
+    bool want_active = false;          // export the activeNeighs bitsets
+    // Reverse first variation: groups of (linear index, weight) points (inspectSensitivity).
+    std::vector<std::vector<int64_t>> adjoint_index;
+    std::vector<std::vector<double>> adjoint_weight;
+    bool want_stencils = false;        // export per-cell offsets/weights (RiemannPerCell)
+    int sweeps_per_tile = 16;          // local Jacobi sweeps before a tile re-queues itself
+    int max_rounds = 1 << 20;
+};
+
+// FirstVariation::BackwardVariation output for one group of inspected points.
+struct AdjointResult {
+    std::vector<double> sensitivity;   // costSensitivity, RowMajor
+    std::vector<int64_t> seed_index;   // sensitive seeds, by decreasing (value, index)
+    std::vector<double> seed_weight;
+};
+
+struct EulerResult {
+    std::vector<double> values;        // RowMajor, +inf where unreached
+    std::vector<uint64_t> active;      // activeNeighs bitsets (if requested)
+    std::vector<int8_t> stencil_off;   // [N][K][3] (if requested)
+    std::vector<double> stencil_w;     // [N][K]
+    int64_t n_accepted = 0;
+    int max_stencil_width = 0;
+    std::vector<AdjointResult> adjoints;
+    double t_stencil_ms = 0, t_solve_ms = 0, t_adjoint_ms = 0, t_total_ms = 0;
+    long long rounds = 0, tile_activations = 0, local_solves = 0;
+};
+
+void solve_eulerian(const EulerProblem &p, EulerResult &r);
+
+// Curvature model stencil tables built on the host with the C library's cos/sin
+// (Headers/Specializations/Curvature2.h:48-66, 178-234, CommonTraits.h:118-161).
+void reedsshepp2_table(int ntheta, double h, double xi, double eps, bool projective,
+                       std::vector<int8_t> &off, std::vector<double> &w);
+void elastica2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,
+                     std::vector<double> &w);
+
+}  // namespace hfm

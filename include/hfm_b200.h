@@ -1,0 +1,89 @@
+/* hfm_b200 — C ABI of the B200-native eikonal solve path.
+ *
+ * Drop-in boundary for the reference HamiltonFastMarching solve path. The reference exposes one
+ * entry point, `void Run(IO&)` (Headers/DispatchAndRun.h:224-244), behind a key-value IO object
+ * (JMM_CPPLibs/JMM_CPPLibs/Output/IO.h:77-118, BaseIO.h:16-43) that its front-ends fill and read:
+ * the FileHFM executable (Interfaces/FileHFM/FileHFM.cpp:12-26) and the pybind11 class HFMIO
+ * (Interfaces/PythonHFM/src/main.cpp:11-47). The functions below are what such a front-end binds:
+ * an opaque `hfm_io` store with the same key semantics and a `hfm_run` that solves on the GPU.
+ *
+ * Conventions: plain pointers and sizes, no exceptions across the boundary. Every function
+ * returns HFM_OK (0) or a positive HFM_ERR_* code; the message of the last failure on an object
+ * is available from hfm_io_last_error(). Host arrays are copied in and out (the caller keeps its
+ * buffers), exactly as PythonIO::PySetArray/PyGetArray do (PythonIO.hxx:7-35).
+ * Distinct hfm_io objects may be used from distinct threads concurrently.
+ */
+#ifndef HFM_B200_H
+#define HFM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HFM_OK 0
+#define HFM_ERR_KEY 1           /* missing key, wrong field kind (string/scalar/array)            */
+#define HFM_ERR_VALUE 2         /* invalid value: shape mismatch, non-SPD metric, bad ordering    */
+#define HFM_ERR_UNSUPPORTED 3   /* a reference option this build does not implement              */
+#define HFM_ERR_CUDA 4          /* CUDA runtime failure (message carries cudaGetErrorString)      */
+#define HFM_ERR_NOT_CONVERGED 5 /* solver iteration cap reached, or a bounded device wait expired */
+#define HFM_ERR_NOMEM 6         /* device or host allocation failure                              */
+#define HFM_ERR_ARG 7           /* null pointer or buffer too small                               */
+
+typedef struct hfm_io hfm_io;
+
+/* Array orderings of the reference IO layer (IO.h:36): index of the ordering names
+ * "RowMajor", "ColumnMajor", "YXZ_RowMajor", "YXZ_ColumnMajor". */
+#define HFM_ORDER_ROW_MAJOR 0
+#define HFM_ORDER_COLUMN_MAJOR 1
+#define HFM_ORDER_YXZ_ROW_MAJOR 2
+#define HFM_ORDER_YXZ_COLUMN_MAJOR 3
+
+/* Replaces constructing an IO object (FileIO, PythonIO). `default_ordering` is the ordering used
+ * when the "arrayOrdering" key is absent: RowMajor for files (IO.h:40), YXZ_RowMajor for Python
+ * (PythonIO.h:20). */
+hfm_io *hfm_io_create(int default_ordering);
+void hfm_io_destroy(hfm_io *io);
+
+/* Setters: HFMIO::SetScalar / SetString / SetArray (main.cpp:19-22). Arrays are float64, `shape`
+ * lists `ndim` extents in the caller's storage order (component axis last). */
+int hfm_io_set_scalar(hfm_io *io, const char *key, double value);
+int hfm_io_set_string(hfm_io *io, const char *key, const char *value);
+int hfm_io_set_array(hfm_io *io, const char *key, const double *data, int ndim, const int64_t *shape);
+
+/* Getters: HFMIO::GetScalar / GetString / GetArray (main.cpp:17-21).
+ * hfm_io_get_string copies at most `cap` bytes including the terminating NUL and stores the full
+ * length (without NUL) in *len. hfm_io_get_array_info reports depth and extents (up to max_ndim);
+ * hfm_io_get_array copies `count` doubles (must equal the product of the extents). */
+int hfm_io_get_scalar(hfm_io *io, const char *key, double *value);
+int hfm_io_get_string(hfm_io *io, const char *key, char *buf, size_t cap, size_t *len);
+int hfm_io_get_array_info(hfm_io *io, const char *key, int *ndim, int64_t *shape, int max_ndim);
+int hfm_io_get_array(hfm_io *io, const char *key, double *out, size_t count);
+
+/* Field inspection: HFMIO::HasField / EraseField / GetComputedKeys (main.cpp:25-27,
+ * BaseIO.hxx:38-47, PythonIO.hxx:37-48). has_field returns 1/0 (negative on a null argument). */
+int hfm_io_has_field(hfm_io *io, const char *key);
+int hfm_io_erase_field(hfm_io *io, const char *key);
+int hfm_io_computed_keys(hfm_io *io, char *buf, size_t cap, size_t *len);
+
+/* Replaces `void Run(IO&)` (DispatchAndRun.h:224-244) followed by IO::UsageReport
+ * (main.cpp:14, BaseIO.hxx:64-104): dispatches at run time on the "model" key
+ * (Riemann2, Riemann3, ReedsShepp2, Elastica2, Isotropic2), solves on the current CUDA device and
+ * writes the outputs (values, nAccepted, MaxStencilWidth, costSensitivity_i, ...) into `io`.
+ * If `expected_model` is non-NULL the call fails when "model" names another model, as the
+ * single-model FileHFM_<Model> executables do (DispatchAndRun.h:227-233). */
+int hfm_run(hfm_io *io, const char *expected_model);
+
+/* Message of the last failure on `io` ("" if none). Valid until the next call on `io`. */
+const char *hfm_io_last_error(hfm_io *io);
+
+/* Library identification and device presence check (no GPU work). */
+const char *hfm_version(void);
+int hfm_device_count(int *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFM_B200_H */

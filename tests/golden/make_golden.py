@@ -1,0 +1,151 @@
+"""Regenerate the golden fixtures of this directory by running the reference's own FileHFM
+executables (``make -C oracle ref`` builds them from the reference sources into ``oracle/_ref``).
+
+    python tests/golden/make_golden.py
+
+Each fixture stores the inputs (hfmIn keys, RowMajor) and the reference outputs: exact float64
+``values``, ``activeNeighs``, ``nAccepted``, ``MaxStencilWidth``, ``costSensitivity_0`` /
+``seedSensitivity_0`` where an ``inspectSensitivity`` group is given, and for the stencil fixtures
+the reference's ``getStencils`` answer (integer offsets exactly; weights as printed, 6 digits).
+"""
+from __future__ import annotations
+
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.refrun import run_reference  # noqa: E402
+from hamiltonfastmarching_b200 import workloads as W  # noqa: E402
+
+def parse_stencils(text: str, ndim: int):
+    """Parse the reference's ``stencils`` string into per-point (offsets, weights) arrays.
+
+    The string nests ``{index, {"forward" -> {{diffs}}, "symmetric" -> {{diffs}}}}`` per point,
+    each diff being ``{weight, {offset}}``; braces are turned into JSON lists.
+    """
+    import json
+    s = text.replace('"forward" -> ', "").replace('"symmetric" -> ', "")
+    s = re.sub(r",\s*}", "}", s).replace("{", "[").replace("}", "]")
+    out = []
+    for point in json.loads(s):
+        _, (fw, sym) = point
+        diffs = [d for grp in fw for d in grp] + [d for grp in sym for d in grp]
+        out.append((np.array([d[1] for d in diffs], np.int64), np.array([d[0] for d in diffs], float)))
+    return out
+
+
+def random_spd(rng, n, ndim, amax=100.0):
+    """Random SPD matrices, anisotropy log-uniform in [1, amax], plus diagonal and tie cases."""
+    mats = []
+    for i in range(n):
+        if ndim == 2:
+            th = rng.uniform(0, np.pi)
+            a = np.exp(rng.uniform(0, np.log(amax)))
+            R = np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+            M = R @ np.diag([1.0, a ** -2]) @ R.T
+            if i % 17 == 0:
+                M = np.diag(rng.uniform(0.5, 2.0, 2))
+            if i % 23 == 0:   # exact tie <b_i, M b_j> = 0 on the canonical superbase
+                M = np.array([[2.0, -1.0], [-1.0, 2.0]])
+            mats.append([M[0, 0], M[0, 1], M[1, 1]])
+        else:
+            Q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+            a1 = np.exp(rng.uniform(0, np.log(amax)))
+            a2 = np.exp(rng.uniform(0, np.log(amax)))
+            M = Q @ np.diag([1.0, a1 ** -2, a2 ** -2]) @ Q.T
+            if i % 17 == 0:
+                M = np.diag(rng.uniform(0.5, 2.0, 3))
+            if i % 23 == 0:
+                M = np.array([[2.0, -1.0, 0.0], [-1.0, 2.0, -1.0], [0.0, -1.0, 2.0]])
+            mats.append([M[0, 0], M[0, 1], M[1, 1], M[0, 2], M[1, 2], M[2, 2]])
+    return np.array(mats)
+
+
+def stencil_fixture(name, ndim, side, seed, dual):
+    rng = np.random.default_rng(seed)
+    dims = (side,) * ndim
+    ncell = side ** ndim
+    mats = random_spd(rng, ncell, ndim).reshape(dims + (-1,))
+    h = 1.0 / side
+    params = {
+        "model": "Riemann2" if ndim == 2 else "Riemann3",
+        "arrayOrdering": "RowMajor",
+        "dims": np.array(dims, float),
+        "gridScale": h,
+        "dualMetric" if dual else "metric": mats,
+        "seeds": np.full((1, ndim), 0.5),
+        "exportValues": 1.0,
+        "exportActiveNeighs": 1.0,
+    }
+    grid = np.stack(np.meshgrid(*[(np.arange(side) + 0.5) * h] * ndim, indexing="ij"), -1).reshape(-1, ndim)
+    params["getStencils"] = grid
+    out = run_reference(params)
+    assert out["retcode"] == 0, out["log"]
+    st = parse_stencils(out["stencils"], ndim)
+    assert len(st) == ncell, (len(st), ncell)
+    nk = 3 if ndim == 2 else 6
+    offs = np.zeros((ncell, nk, ndim), np.int8)
+    ws = np.zeros((ncell, nk))
+    for i, (o, w) in enumerate(st):
+        offs[i] = o
+        ws[i] = w
+    del params["getStencils"]
+    save(name, params, out, stencil_offsets=offs, stencil_weights_6digits=ws)
+
+
+def save(name, params, out, **extra):
+    blob = {}
+    for k, v in params.items():
+        blob["in_" + k] = np.asarray(v) if not isinstance(v, str) else np.array(v)
+    for k in ("values", "activeNeighs", "nAccepted", "MaxStencilWidth", "costSensitivity_0",
+              "seedSensitivity_0", "spreadedSeeds", "spreadedSeedValues"):
+        if k in out:
+            blob["out_" + k] = np.asarray(out[k])
+    blob.update(extra)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **blob)
+    print(name, {k: getattr(v, "shape", None) for k, v in blob.items() if k.startswith("out_")})
+
+
+def solve_fixture(name, params, inspect=None):
+    params = dict(params)
+    params["exportActiveNeighs"] = 1.0
+    if inspect is not None:
+        pts, wts = inspect
+        params["inspectSensitivity"] = np.asarray(pts, float)
+        params["inspectSensitivityWeights"] = np.asarray(wts, float)
+        params["inspectSensitivityLengths"] = np.array([len(wts)], float)
+    out = run_reference(params)
+    assert out["retcode"] == 0, out["log"]
+    save(name, params, out)
+
+
+def main():
+    rng = np.random.default_rng(1234)
+    stencil_fixture("selling2_32", 2, 32, 11, dual=False)
+    stencil_fixture("selling2_dual_24", 2, 24, 12, dual=True)
+    stencil_fixture("selling3_10", 3, 10, 13, dual=False)
+    solve_fixture("riemann2_64", W.riemann2_case(64),
+                  (rng.uniform(0.05, 0.95, (6, 2)), rng.uniform(0.5, 2.0, 6)))
+    p = W.riemann2_case(48, aniso=10.0, seed=5, n_seeds=3)
+    p["seedValues"] = np.array([0.0, 0.1, 0.05])
+    solve_fixture("riemann2_48_seeds", p)
+    solve_fixture("riemann3_16_walls", W.riemann3_case(16, n_spheres=5, n_seeds=3, rmin=0.1, rmax=0.25),
+                  (rng.uniform(0.05, 0.95, (4, 3)), rng.uniform(0.5, 2.0, 4)))
+    pts = np.c_[rng.uniform(0.1, 0.9, (4, 2)), rng.uniform(0, 6, (4, 1))]
+    solve_fixture("reedsshepp2_32x24", W.curvature2_case(32, 24, "ReedsShepp2", n_curves=6),
+                  (pts, rng.uniform(0.5, 2.0, 4)))
+    p = W.curvature2_case(24, 16, "ReedsShepp2", seed=7, n_curves=4)
+    p["walls"] = (np.random.default_rng(8).uniform(size=(24, 24)) < 0.08).astype(float)
+    solve_fixture("reedsshepp2_24x16_walls", p)
+    solve_fixture("elastica2_24x16", W.curvature2_case(24, 16, "Elastica2", seed=9, n_curves=5),
+                  (pts[:2], rng.uniform(0.5, 2.0, 2)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,113 @@
+"""The C ABI library without a GPU: it loads, exports every symbol include/hfm_b200.h declares,
+and its key-value store follows the reference IO semantics. No compute call is made."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+import hamiltonfastmarching_b200 as H
+from hamiltonfastmarching_b200 import _lib
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "hfm_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hfm_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    syms = declared_symbols()
+    assert len(syms) >= 16
+    lib = _lib.load()
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) == set(_lib.SIGNATURES)
+    nm = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    for s in syms:
+        assert re.search(rf"\bT {s}\b", nm), f"{s} not exported"
+
+
+def test_version_and_device_count_without_gpu():
+    assert "sm_100a" in H.version()
+    n = _lib.load()
+    import ctypes
+    c = ctypes.c_int(-1)
+    assert n.hfm_device_count(ctypes.byref(c)) in (0, 4)
+    assert c.value >= 0
+
+
+def test_store_roundtrip_and_bookkeeping():
+    io = H.HFMIO("RowMajor")
+    io.set_string("model", "Riemann2")
+    io.set_scalar("gridScale", 0.25)
+    a = np.arange(24, dtype=float).reshape(2, 4, 3)
+    io.set_array("metric", a)
+    assert io.get_string("model") == "Riemann2"
+    assert io.get_scalar("gridScale") == 0.25
+    np.testing.assert_array_equal(io.get_array("metric"), a)
+    assert io.has_field("metric") and not io.has_field("nothing")
+    assert io.erase_field("metric") and not io.has_field("metric")
+    assert io.computed_keys() == "[]"   # nothing computed yet
+
+
+def test_store_errors_raise_not_crash():
+    io = H.HFMIO()
+    with pytest.raises(H.PyExp) as e:
+        io.get_scalar("missing")
+    assert e.value.code == 1
+    io.set_array("v", np.zeros(3))
+    with pytest.raises(H.PyExp):
+        io.get_scalar("v")     # array field read as scalar
+    io.set_scalar("s", 1.0)
+    with pytest.raises(H.PyExp):
+        io.get_array("s")      # scalar read as array
+    with pytest.raises(H.PyExp):
+        io.run()               # no model key: reported, not a segfault
+
+
+@pytest.mark.parametrize("key,val", [("tips", np.zeros((1, 2))), ("order", 2.0), ("factoringRadius", 5.0),
+                                     ("stopAtDistance", 1.0), ("seedRadius", 2.0)])
+def test_unsupported_options_rejected_before_gpu_work(key, val):
+    p = {"model": "Riemann2", "arrayOrdering": "RowMajor", "dims": np.array([8., 8.]), "gridScale": 0.125,
+         "metric": np.array([1., 0., 1.]), "seeds": np.array([[0.5, 0.5]]), "verbosity": 0.0, key: val}
+    with pytest.raises(H.PyExp) as e:
+        H.run(p)
+    assert e.value.code == 3, str(e.value)
+
+
+def test_model_mismatch_is_reported():
+    p = {"model": "Riemann3", "dims": np.array([8., 8.]), "verbosity": 0.0}
+    io = H.HFMIO("RowMajor")
+    io.set_dict(p)
+    with pytest.raises(H.PyExp) as e:
+        io.run("Riemann2")
+    assert "Executable applies to Riemann2" in str(e.value)
+
+
+def test_cli_reports_missing_input(tmp_path):
+    exe = os.path.join(ROOT, "hamiltonfastmarching_b200", "bin", "FileHFM_b200")
+    if not os.path.exists(exe):
+        pytest.skip("CLI not built")
+    r = subprocess.run([exe, str(tmp_path / "nope"), str(tmp_path / "out")], capture_output=True, text=True)
+    assert r.returncode != 0
+    assert "could not be opened" in r.stdout
+
+
+def test_no_host_path_exits_the_process():
+    """Only host stubs of __device__ functions may contain a call to exit: a host launch path that
+    reaches one (a device-only helper called from host code) would end the caller's process."""
+    out = subprocess.run(["objdump", "-d", "--no-show-raw-insn", "-C", _lib.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    fn, callers = None, set()
+    for line in out.splitlines():
+        m = re.match(r"^[0-9a-f]+ <(.*)>:$", line)
+        if m:
+            fn = m.group(1)
+        elif "<exit@plt>" in line and "call" in line:
+            callers.add(fn)
+    allowed = {"wall_visible"}
+    bad = [c for c in callers if not any(a in c for a in allowed)]
+    assert not bad, bad

@@ -1,0 +1,137 @@
+"""Parity of the CUDA solve path (through the C ABI) with the reference and the C oracle.
+
+Tolerances: FP64 arrival times within 1e-10 relative max-norm of the reference (the solver
+reproduces fast marching's accumulation order, so most cells are bit-identical); stencil-derived
+integers (nAccepted, MaxStencilWidth) exact; FP32 path within 1e-4 relative of FP64.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_SOLVES, GOLDEN_STENCILS, ROOT, load_golden
+import hamiltonfastmarching_b200 as H
+from hamiltonfastmarching_b200 import workloads as W
+from oracle import oracle as O
+from oracle.refrun import read_output, write_input
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-10
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    assert np.array_equal(np.isinf(a), np.isinf(b)), "reached sets differ"
+    fin = np.isfinite(a)
+    if not fin.any():
+        return 0.0
+    return float(np.max(np.abs(a[fin] - b[fin])) / max(np.max(np.abs(a[fin])), 1e-300))
+
+
+def gpu_solve(params, **extra):
+    p = dict(params)
+    p.setdefault("verbosity", 0.0)
+    p.update(extra)
+    return H.run(p)
+
+
+@pytest.mark.parametrize("name", GOLDEN_SOLVES + GOLDEN_STENCILS)
+def test_golden_values(name):
+    params, ref, _ = load_golden(name)
+    out = gpu_solve(params)
+    assert rel_err(ref["values"], out["values"]) <= FP64_RTOL
+    assert int(out["nAccepted"]) == int(ref["nAccepted"])
+    assert int(out["MaxStencilWidth"]) == int(ref["MaxStencilWidth"])
+    same = np.mean(ref["values"] == out["values"])
+    assert same > 0.99, f"only {same:.4f} of the cells are bit-identical"
+    act_ref = ref["activeNeighs"].astype(np.uint64)
+    act = out["activeNeighs"].astype(np.uint64)
+    assert np.mean(act_ref != act) <= 1e-2
+
+
+@pytest.mark.parametrize("name", GOLDEN_SOLVES)
+def test_golden_sensitivity(name):
+    params, ref, _ = load_golden(name)
+    if "costSensitivity_0" not in ref:
+        pytest.skip("fixture has no inspectSensitivity group")
+    out = gpu_solve(params)
+    a, b = ref["costSensitivity_0"], out["costSensitivity_0"]
+    assert np.max(np.abs(a - b)) <= FP64_RTOL * np.max(np.abs(a))
+    sr, so = ref["seedSensitivity_0"], out["seedSensitivity_0"]
+    assert sr.shape == so.shape
+    np.testing.assert_allclose(so, sr, rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize("case", ["riemann2_256", "riemann3_40_walls", "rs2_64x36", "elastica2_48x30"])
+def test_oracle_parity_larger(case):
+    if case == "riemann2_256":
+        p = W.riemann2_case(256)
+    elif case == "riemann3_40_walls":
+        p = W.riemann3_case(40)
+    elif case == "rs2_64x36":
+        p = W.curvature2_case(64, 36, "ReedsShepp2")
+    else:
+        p = W.curvature2_case(48, 30, "Elastica2")
+    ora = O.solve(p)
+    out = gpu_solve(p)
+    assert rel_err(ora["values"], out["values"]) <= FP64_RTOL
+    assert int(out["nAccepted"]) == ora["nAccepted"]
+
+
+@pytest.mark.parametrize("case", ["riemann2_128", "riemann3_32_walls", "rs2_48x30"])
+def test_fp32_path_close_to_fp64(case):
+    p = {"riemann2_128": lambda: W.riemann2_case(128),
+         "riemann3_32_walls": lambda: W.riemann3_case(32, n_spheres=10, n_seeds=4),
+         "rs2_48x30": lambda: W.curvature2_case(48, 30, "ReedsShepp2")}[case]()
+    o64 = gpu_solve(p)
+    o32 = gpu_solve(p, solverPrecision="float32")
+    assert rel_err(o64["values"], o32["values"]) <= 1e-4
+
+
+def test_yxz_ordering_default_of_python_binding():
+    """HFMIO defaults to YXZ_RowMajor like the reference Python binding: arrays are transposed."""
+    p = W.riemann2_case(48, aniso=8.0, seed=3)
+    ref = gpu_solve(p)["values"]
+    io = H.HFMIO()  # YXZ_RowMajor
+    q = dict(p)
+    del q["arrayOrdering"]
+    q["metric"] = np.ascontiguousarray(np.transpose(p["metric"], (1, 0, 2)))
+    q["verbosity"] = 0.0
+    io.set_dict(q)
+    io.run()
+    np.testing.assert_array_equal(io.get_array("values"), ref.T)
+
+
+def test_non_spd_metric_is_an_error():
+    p = W.riemann2_case(16)
+    p["metric"] = p["metric"].copy()
+    p["metric"][3, 4] = [1.0, 2.0, 1.0]   # determinant < 0
+    with pytest.raises(H.PyExp) as e:
+        gpu_solve(p)
+    assert e.value.code == 2
+
+
+def test_cli_matches_library(tmp_path):
+    exe = os.path.join(ROOT, "hamiltonfastmarching_b200", "bin", "FileHFM_b200")
+    params, ref, _ = load_golden("riemann3_16_walls")
+    write_input(params, str(tmp_path / "input"))
+    r = subprocess.run([exe, str(tmp_path / "input"), str(tmp_path / "output")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = read_output(str(tmp_path / "output"))
+    assert rel_err(ref["values"], out["values"]) <= FP64_RTOL
+    assert out["nAccepted"] == ref["nAccepted"]
+    link = tmp_path / "FileHFM_Riemann2"
+    os.symlink(exe, link)
+    r = subprocess.run([str(link), str(tmp_path / "input"), str(tmp_path / "o2")], capture_output=True, text=True)
+    assert r.returncode != 0 and "Executable applies to Riemann2" in r.stdout
+
+
+def test_repeatable_and_seeds_fixed():
+    p = W.riemann3_case(32, n_spheres=8, n_seeds=5)
+    a = gpu_solve(p)["values"]
+    b = gpu_solve(p)["values"]
+    np.testing.assert_array_equal(a, b)
+    P = O.Problem(p)
+    np.testing.assert_array_equal(a.ravel()[P.seed_index], 0.0)

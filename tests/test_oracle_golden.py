@@ -1,0 +1,51 @@
+"""The C oracle against the reference's golden vectors (CPU only).
+
+The fixtures were produced by the reference's own FileHFM executables
+(tests/golden/make_golden.py); the oracle must reproduce them bit for bit.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_SOLVES, GOLDEN_STENCILS, load_golden
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("name", GOLDEN_SOLVES + GOLDEN_STENCILS)
+def test_oracle_values_bit_exact(name):
+    params, ref, _ = load_golden(name)
+    res = O.solve(params)
+    a, b = ref["values"], res["values"]
+    assert np.array_equal(np.isinf(a), np.isinf(b))
+    fin = np.isfinite(a)
+    assert np.array_equal(a[fin], b[fin]), "oracle values differ from the reference"
+    assert int(ref["nAccepted"]) == res["nAccepted"]
+    assert int(ref["MaxStencilWidth"]) == res["MaxStencilWidth"]
+    assert np.array_equal(ref["activeNeighs"].ravel().astype(np.uint64), res["activeNeighs"])
+
+
+@pytest.mark.parametrize("name", [n for n in GOLDEN_SOLVES])
+def test_oracle_sensitivity_bit_exact(name):
+    params, ref, _ = load_golden(name)
+    if "costSensitivity_0" not in ref:
+        pytest.skip("fixture has no inspectSensitivity group")
+    res = O.solve(params)
+    sens, si, sw = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
+    assert np.array_equal(ref["costSensitivity_0"], sens)
+    seeds = ref["seedSensitivity_0"]
+    assert len(seeds) == len(si)
+    np.testing.assert_array_equal(seeds[:, -1], sw)
+
+
+@pytest.mark.parametrize("name", GOLDEN_STENCILS)
+def test_oracle_stencils_match_reference(name):
+    """Offsets bit-exact against the reference's getStencils export; weights to its 6 printed digits."""
+    params, _, extra = load_golden(name)
+    ndim = len(params["dims"])
+    dual = "dualMetric" in params
+    metric = params["dualMetric" if dual else "metric"]
+    h = params["gridScale"]
+    off, w = O.riemann_stencils(metric, h, dual)
+    ref_off = extra["stencil_offsets"].astype(np.int64)
+    ref_w = extra["stencil_weights_6digits"]
+    np.testing.assert_array_equal(off[..., :ndim].astype(np.int64), ref_off)
+    np.testing.assert_allclose(w, ref_w, rtol=5e-6, atol=0)
