@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark of the eikonal solve path: grid updates per second on the Riemann3 192^3 plain solve.
+
+Workload: 192^3 grid on [0,1]^3, metric R diag(1, a1^-2, a2^-2) R^T (a1, a2 in [1,20], smooth
+random rotation), 40 spherical walls (radii 0.02-0.08), 16 seeds (hamiltonfastmarching_b200.workloads
+.riemann3_case, seed = 1 + rank). One step = one complete solve (Selling stencils, wall visibility,
+tile dependency graph, fast-iterative solve) of the instance; a grid update is one reached cell
+(the reference's nAccepted). Synthetic data; the 340 MB metric exceeds the 126 MB L2, so no flush
+is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is measured with inputs resident in HBM through the device entry point of the C ABI;
+`e2e` through the public HFMIO call with host arrays (host->device and device->host copies inside
+the timed region). With --gpus N under torchrun every rank solves its own instance (replicas:
+the path does not shard) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_UPDATE = {64: 57, 32: 53}  # metric 6x8 B + wall 1 B + value 8|4 B per reached cell
+WORKLOAD = "Riemann3 192^3 plain solve, 40 spherical walls, 16 seeds"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--side", type=int, default=192, help="grid side of the benchmarked instance")
+    ap.add_argument("--cpu-sample-side", type=int, default=128,
+                    help="grid side of the bounded sample the reference CPU code is timed on")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ------------------------------------------------------------------------------------------ utils
+
+def rank_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(key):
+    """Per-launch DRAM bytes of the solver kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "fim_kernel_traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == key:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region (every 200 ms)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.tmp.flush()
+        rows = []
+        with open(self.tmp.name) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def reference_cpu_sample(side, seed=1):
+    """The reference's FileHFM_Riemann3 (built from its sources) on a bounded sample of the workload:
+    updates/s = nAccepted / (FMCPUTime + StencilCPUTime), one core."""
+    from oracle.refrun import have_reference, run_reference
+    from hamiltonfastmarching_b200 import workloads as W
+    if not have_reference("Riemann3"):
+        return None
+    p = W.riemann3_case(side, seed=seed)
+    p["exportValues"] = 0.0
+    t0 = time.time()
+    out = run_reference(p)
+    wall = time.time() - t0
+    if out.get("retcode") != 0:
+        return None
+    cpu_s = out["FMCPUTime"] + out["StencilCPUTime"]
+    return {"value": out["nAccepted"] / cpu_s, "unit": "grid-updates/s", "cores": 1, "kind": "reference",
+            "sample": f"FileHFM_Riemann3 on the same generator at {side}^3 ({int(out['nAccepted'])} reached cells); "
+                      f"FMCPUTime {out['FMCPUTime']:.2f} s + StencilCPUTime {out['StencilCPUTime']:.2f} s "
+                      f"(wall {wall:.1f} s incl. file IO)"}
+
+
+# ------------------------------------------------------------------------------------- our arm
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import hamiltonfastmarching_b200 as H
+    from hamiltonfastmarching_b200 import _lib
+    from hamiltonfastmarching_b200 import workloads as W
+
+    rank, world, local = rank_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    L = _lib.load()
+    n = args.side
+    params = W.riemann3_case(n, seed=1 + rank)
+    N = n ** 3
+    metric_h = np.ascontiguousarray(params["metric"].reshape(N, 6))
+    walls_h = np.ascontiguousarray((params["walls"] != 0).astype(np.uint8).reshape(N))
+    # seeds -> row-major indices: floor((p - origin) / h), unique, increasing (as hfm_run places them)
+    h = params["gridScale"]
+    ijk = np.floor(params["seeds"] / h).astype(np.int64)
+    seed_idx = np.unique(np.ravel_multi_index(ijk.T, (n, n, n))).astype(np.int64)
+    seed_val = np.zeros(len(seed_idx), np.float64)
+
+    metric_d = torch.from_numpy(metric_h).cuda()
+    walls_d = torch.from_numpy(walls_h).cuda()
+    values_d = torch.empty(N, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def make_args(precision):
+        a = _lib.RiemannDeviceArgs()
+        a.ndim = 3
+        for i in range(3):
+            a.dims[i] = n
+            a.grid_scale[i] = params["gridScale"]
+        a.dual = 0
+        a.precision = precision
+        a.sweeps_per_tile = 0
+        a.metric = metric_d.data_ptr()
+        a.walls = walls_d.data_ptr()
+        a.nseeds = len(seed_idx)
+        a.seed_index = seed_idx.ctypes.data
+        a.seed_value = seed_val.ctypes.data
+        a.values = values_d.data_ptr()
+        a.stream = stream.cuda_stream
+        return a
+
+    err = ctypes.create_string_buffer(512)
+
+    def solve(a, st):
+        rc = L.hfm_solve_riemann_device(ctypes.byref(a), ctypes.byref(st), err, 512)
+        if rc != 0:
+            raise RuntimeError(f"solve failed ({rc}): {err.value.decode()}")
+
+    results = {}
+    values_by_prec = {}
+    for prec in (64, 32):
+        a = make_args(prec)
+        st = _lib.SolveStats()
+        for _ in range(args.warmup):
+            solve(a, st)
+        torch.cuda.synchronize()
+        barrier()
+        launches0 = ctypes.c_ulonglong()
+        L.hfm_kernel_launches(ctypes.byref(launches0))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        solve_ms, stencil_ms, stats = [], [], []
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            start.record(stream)
+            for _ in range(args.steps):
+                solve(a, st)
+                solve_ms.append(st.solve_ms)
+                stencil_ms.append(st.stencil_ms)
+                stats.append((st.n_accepted, st.rounds, st.tile_activations, st.local_solves))
+            end.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        launches1 = ctypes.c_ulonglong()
+        L.hfm_kernel_launches(ctypes.byref(launches1))
+        elapsed_ms = max_over_ranks(start.elapsed_time(end))
+        values_by_prec[prec] = values_d.cpu().numpy().copy()
+        nacc = stats[-1][0]
+        results[prec] = {
+            "elapsed_ms": elapsed_ms, "ms_per_step": elapsed_ms / args.steps,
+            "value": world * nacc * args.steps / (elapsed_ms * 1e-3),
+            "n_accepted": nacc, "solve_ms": statistics.mean(solve_ms), "stencil_ms": statistics.mean(stencil_ms),
+            "rounds": stats[-1][1], "tile_activations": stats[-1][2], "local_solves": stats[-1][3],
+            "launches": (launches1.value - launches0.value) // args.steps * args.steps,
+            "clocks": clk.summary(),
+        }
+
+    # FP32 error against the FP64 path, finite cells
+    v64, v32 = values_by_prec[64], values_by_prec[32]
+    fin = np.isfinite(v64)
+    fp32_err = float(np.max(np.abs(v64[fin] - v32[fin])) / np.max(np.abs(v64[fin])))
+
+    # ---- end to end through the public API (host arrays in, host arrays out)
+    e2e = None
+    if args.e2e_steps > 0:
+        hp = dict(params, verbosity=0.0)
+        H.run(hp)  # warm
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            out = H.run(hp)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * out["nAccepted"] * args.e2e_steps / e2e_s, "unit": "grid-updates/s",
+               "h2d_bytes_per_step": int(metric_h.nbytes + walls_h.nbytes + params["seeds"].nbytes),
+               "d2h_bytes_per_step": int(N * 8),
+               "path": "HFMIO.run (hfm_run C ABI) from pageable numpy arrays, FP64"}
+
+    r64 = results[64]
+    peak, peak_kind = measured_peak_gbs()
+    achieved = BYTES_PER_UPDATE[64] * r64["n_accepted"] / (r64["solve_ms"] * 1e-3) / 1e9
+    traffic = profiled_traffic(f"riemann3_{n}_f64")
+    roofline = {"bound": "hbm", "kernel": "fim_kernel<double,0,6,false>", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic,
+                "algorithmic_bytes_per_update": BYTES_PER_UPDATE[64],
+                "note": "achieved = 57 B x nAccepted / solver-kernel CUDA-event time on the launching stream"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = reference_cpu_sample(args.cpu_sample_side)
+
+    if rank == 0:
+        line = {
+            "metric": "grid-updates/s", "value": r64["value"], "unit": "grid-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [n, n, n], "instances_per_gpu": 1,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (340 MB metric)",
+                       "n_accepted": r64["n_accepted"]},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": r64["clocks"],
+            "gpu_launches": r64["launches"],
+            "phases_ms": {"stencil_and_graph": r64["stencil_ms"], "solve": r64["solve_ms"]},
+            "solver": {"rounds": r64["rounds"], "tile_activations": r64["tile_activations"],
+                       "local_solves": r64["local_solves"]},
+            "fp32": {"value": results[32]["value"], "ms_per_step": results[32]["ms_per_step"],
+                     "solve_ms": results[32]["solve_ms"], "max_rel_err_vs_fp64": fp32_err,
+                     "clocks": results[32]["clocks"]},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------ reference arm
+
+def run_reference_arm(args):
+    rank, world, _ = rank_env()
+    if rank != 0:
+        return
+    from oracle.refrun import have_reference, ref_executable, write_input, read_output
+    from hamiltonfastmarching_b200 import workloads as W
+    side = args.cpu_sample_side
+    if not have_reference("Riemann3"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference FileHFM_Riemann3 not built (make -C oracle ref)"}))
+        return
+    cores = os.cpu_count() or 1
+    p = W.riemann3_case(side, seed=1)
+    p["exportValues"] = 0.0
+    tmp = tempfile.mkdtemp(prefix="hfmrefbench_")
+    write_input(p, os.path.join(tmp, "input"))
+    exe = ref_executable("Riemann3")
+
+    def step():
+        procs = [subprocess.Popen([exe, os.path.join(tmp, "input"), os.path.join(tmp, f"out{i}")],
+                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for i in range(cores)]
+        for pr in procs:
+            pr.wait()
+        return read_output(os.path.join(tmp, "out0"))
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = step()
+    el = time.perf_counter() - t0
+    nacc = out["nAccepted"]
+    value = cores * nacc * args.steps / el
+    line = {"impl": "reference", "metric": "grid-updates/s", "value": value, "unit": "grid-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [args.side] * 3, "sample_grid": [side] * 3},
+            "cpu_baseline": {"value": value, "unit": "grid-updates/s", "cores": cores, "kind": "reference",
+                             "sample": f"{cores} concurrent FileHFM_Riemann3 processes (reference code, one "
+                                       f"thread each) per step on the same generator at {side}^3"},
+            "e2e": {"value": value, "unit": "grid-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -38,6 +38,24 @@ SIGNATURES = {
     "hfm_device_count": ([ctypes.POINTER(_I)], _I),
 }
 
+class RiemannDeviceArgs(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int), ("dims", ctypes.c_int64 * 3), ("grid_scale", ctypes.c_double * 3),
+                ("dual", ctypes.c_int), ("precision", ctypes.c_int), ("sweeps_per_tile", ctypes.c_int),
+                ("metric", ctypes.c_void_p), ("walls", ctypes.c_void_p), ("nseeds", ctypes.c_int64),
+                ("seed_index", ctypes.c_void_p), ("seed_value", ctypes.c_void_p), ("values", ctypes.c_void_p),
+                ("stream", ctypes.c_void_p)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("n_accepted", ctypes.c_int64), ("max_stencil_width", ctypes.c_int),
+                ("stencil_ms", ctypes.c_double), ("solve_ms", ctypes.c_double), ("rounds", ctypes.c_int64),
+                ("tile_activations", ctypes.c_int64), ("local_solves", ctypes.c_int64)]
+
+
+SIGNATURES["hfm_solve_riemann_device"] = ([ctypes.POINTER(RiemannDeviceArgs), ctypes.POINTER(SolveStats),
+                                           ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int)
+SIGNATURES["hfm_kernel_launches"] = ([ctypes.POINTER(ctypes.c_ulonglong)], ctypes.c_int)
+
 _lib = None
 
 

@@ -1,15 +1,34 @@
 // Owning device allocation (RAII) used by the host orchestration.
+//
+// Allocations are stream-ordered (cudaMallocAsync / cudaFreeAsync on the device's default memory
+// pool, whose release threshold is raised once so that freed blocks stay cached): repeated solves
+// reuse memory without device-wide synchronisation.
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include <cstddef>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
 
 namespace hfm {
+
+// Stream on which the calling thread's solve runs (set by the orchestration).
+cudaStream_t &current_stream();
+void keep_pool_cached();
+// Kernel launches issued by this library (all threads), for launch accounting.
+void count_launch(unsigned n = 1);
+
+// Counted kernel launch: launch(kernel, grid, block, shared_bytes, stream, args...).
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                   Args &&...args) {
+    count_launch();
+    kernel<<<grid, block, smem, stream>>>(std::forward<Args>(args)...);
+}
 
 template <typename T>
 class DeviceBuffer {
@@ -28,23 +47,24 @@ public:
     void alloc(size_t n) {
         release();
         if (n == 0) return;
-        HFM_CUDA(cudaMalloc(reinterpret_cast<void **>(&p_), n * sizeof(T)));
+        keep_pool_cached();
+        HFM_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&p_), n * sizeof(T), current_stream()));
         n_ = n;
     }
     void release() {
-        if (p_) cudaFree(p_);
+        if (p_) cudaFreeAsync(p_, current_stream());
         p_ = nullptr;
         n_ = 0;
     }
-    void zero(cudaStream_t s = 0) {
+    void zero(cudaStream_t s = current_stream()) {
         if (n_) HFM_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
     }
-    void upload(const T *h, size_t n, cudaStream_t s = 0) {
+    void upload(const T *h, size_t n, cudaStream_t s = current_stream()) {
         if (n > n_) alloc(n);
         if (n) HFM_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
     }
-    void upload(const std::vector<T> &v, cudaStream_t s = 0) { upload(v.data(), v.size(), s); }
-    void download(T *h, size_t n, cudaStream_t s = 0) const {
+    void upload(const std::vector<T> &v, cudaStream_t s = current_stream()) { upload(v.data(), v.size(), s); }
+    void download(T *h, size_t n, cudaStream_t s = current_stream()) const {
         if (n) HFM_CUDA(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDeviceToHost, s));
     }
     T *get() const { return p_; }

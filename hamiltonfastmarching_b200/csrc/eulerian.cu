@@ -987,7 +987,7 @@ void run_adjoint(const Dev<Real> &P, const EulerProblem &p, EulerResult &res, De
     DeviceBuffer<double> fw((size_t)NF * N), var(N), acc(N), sens(N);
     DeviceBuffer<uint8_t> nflow(N);
     indeg0.zero(s);
-    flow_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(N, 128), 128, 0, s>>>(P, fidx.get(), fw.get(), var.get(),
+    launch(flow_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, fidx.get(), fw.get(), var.get(),
                                                                           nflow.get(), indeg0.get());
     HFM_CUDA(cudaGetLastError());
     DeviceBuffer<int> lists(3 * N);
@@ -1038,9 +1038,10 @@ void run_adjoint(const Dev<Real> &P, const EulerProblem &p, EulerResult &res, De
         for (size_t k = 0; k < hacc_i.size(); ++k)
             HFM_CUDA(cudaMemcpyAsync(acc.get() + hacc_i[k], &hacc_w[k], sizeof(double), cudaMemcpyHostToDevice, s));
         HFM_CUDA(cudaStreamSynchronize(s));
-        adjoint_roots_kernel<<<nblocks(N, 256), 256, 0, s>>>(A);
+        launch(adjoint_roots_kernel, nblocks(N, 256), 256, 0, s, A);
         void *args[] = {&A};
-        HFM_CUDA(cudaLaunchCooperativeKernel((void *)adjoint_kernel, dim3(nsm * per_sm), dim3(256), args, 0, s));
+        count_launch();
+            HFM_CUDA(cudaLaunchCooperativeKernel((void *)adjoint_kernel, dim3(nsm * per_sm), dim3(256), args, 0, s));
         check_status(status, "adjoint");
         AdjointResult ar;
         ar.sensitivity.resize(N);
@@ -1069,7 +1070,7 @@ template <typename Real, int NFWD, int NSYM, bool SHARE>
 void run_impl(const EulerProblem &p, EulerResult &res) {
     constexpr int ND = NFWD + NSYM;
     const auto wall_t0 = std::chrono::steady_clock::now();
-    cudaStream_t s = 0;
+    cudaStream_t s = current_stream();
     const GridGeom g = make_geom(p.ndim, p.dims, p.periodic);
     const long long N = g.ncells, ntc = g.ntile * 64;
     if (g.ntile >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large");
@@ -1083,7 +1084,7 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
     P.status = status.get();
     DeviceBuffer<Real> values(N);
     P.values = values.get();
-    fill_kernel<Real><<<nblocks(N, 256) > 4096 ? 4096 : nblocks(N, 256), 256, 0, s>>>(values.get(), N, Arith<Real>::inf());
+    launch(fill_kernel<Real>, nblocks(N, 256) > 4096 ? 4096 : nblocks(N, 256), 256, 0, s, values.get(), N, Arith<Real>::inf());
     EventTimer tm;
 
     // ---- stencils
@@ -1102,22 +1103,26 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         weight.zero(s);
         P.code = code.get();
         P.weight = weight.get();
-        metric.upload(p.metric, s);
+        const double *metric_ptr = p.d_metric;
+        if (!metric_ptr) {
+            metric.upload(p.metric, s);
+            metric_ptr = metric.get();
+        }
         if (p.want_stencils) {
             plain_off.alloc(N * ND * 3);
             plain_w.alloc(N * ND);
         }
         if (p.ndim == 2)
-            riemann_stencil_kernel<2, Real><<<nblocks(N, 128), 128, 0, s>>>(
-                g, ntc, metric.get(), p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
+            launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, 
+                g, ntc, metric_ptr, p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
                 plain_off.get(), plain_w.get(), status.get());
         else
-            riemann_stencil_kernel<3, Real><<<nblocks(N, 128), 128, 0, s>>>(
-                g, ntc, metric.get(), p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
+            launch(riemann_stencil_kernel<3, Real>, nblocks(N, 128), 128, 0, s, 
+                g, ntc, metric_ptr, p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
                 plain_off.get(), plain_w.get(), status.get());
         HFM_CUDA(cudaGetLastError());
         HFM_TRACE("stencil kernel");
-        width_kernel<Real, NSYM><<<nblocks(N, 256), 256, 0, s>>>(P, maxw.get());
+        launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, P, maxw.get());
         unsigned mw = 0;
         maxw.download(&mw, 1, s);
         HFM_CUDA(cudaStreamSynchronize(s));
@@ -1134,7 +1139,7 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         mult.zero(s);
         P.mult = mult.get();
         mult_rm.upload(p.mult, s);
-        mult_layout_kernel<Real><<<nblocks(N, 256), 256, 0, s>>>(g, mult_rm.get(), mult.get());
+        launch(mult_layout_kernel<Real>, nblocks(N, 256), 256, 0, s, g, mult_rm.get(), mult.get());
         vis.alloc(ntc);
         vis.zero(s);
         P.vis = vis.get();
@@ -1157,21 +1162,25 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
     DeviceBuffer<uint8_t> walls;
     DeviceBuffer<int> wdist;
     DeviceBuffer<int8_t> wd8;
-    if (!p.walls.empty()) {
+    const uint8_t *walls_ptr = p.d_walls;
+    if (!walls_ptr && !p.walls.empty()) {
         walls.upload(p.walls, s);
+        walls_ptr = walls.get();
+    }
+    if (walls_ptr) {
         wdist.alloc(N);
         wd8.alloc(N);
-        wall_init_kernel<<<nblocks(N, 256), 256, 0, s>>>(N, walls.get(), wdist.get());
+        launch(wall_init_kernel, nblocks(N, 256), 256, 0, s, N, walls_ptr, wdist.get());
         for (int a = 0; a < 3; ++a) {
             if (g.dims[a] == 1) continue;
             const long long nl = N / g.dims[a];
-            wall_scan_kernel<<<nblocks(nl, 128), 128, 0, s>>>(g, a, wdist.get());
+            launch(wall_scan_kernel, nblocks(nl, 128), 128, 0, s, g, a, wdist.get());
         }
-        wall_cap_kernel<<<nblocks(N, 256), 256, 0, s>>>(N, wdist.get(), max_width, wd8.get());
+        launch(wall_cap_kernel, nblocks(N, 256), 256, 0, s, N, wdist.get(), max_width, wd8.get());
         HFM_CUDA(cudaGetLastError());
     }
     HFM_TRACE("walls");
-    visibility_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(ntc, 128), 128, 0, s>>>(P, wd8.get(), cls_en.get());
+    launch(visibility_kernel<Real, NFWD, NSYM, SHARE>, nblocks(ntc, 128), 128, 0, s, P, wd8.get(), cls_en.get());
     HFM_CUDA(cudaGetLastError());
     wdist.release();
     HFM_TRACE("visibility");
@@ -1184,14 +1193,14 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         std::vector<long long> si(p.seed_index.begin(), p.seed_index.end());
         sidx.upload(si, s);
         sval.upload(p.seed_value, s);
-        seeds_kernel<Real, SHARE><<<nblocks(ns, 128), 128, 0, s>>>(P, sidx.get(), sval.get(), ns);
+        launch(seeds_kernel<Real, SHARE>, nblocks(ns, 128), 128, 0, s, P, sidx.get(), sval.get(), ns);
     }
 
     // ---- tile dependency graph (reverse CSR)
     const long long nt = g.ntile;
     HFM_TRACE("seeds");
     DeviceBuffer<unsigned> dcnt(nt);
-    deps_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(nt, kDepWarps), kDepWarps * 32, 0, s>>>(
+    launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, 
         P, 0, dcnt.get(), nullptr, nullptr, nullptr, nullptr);
     HFM_CUDA(cudaGetLastError());
     DeviceBuffer<long long> doff(nt + 1), rptr(nt + 1);
@@ -1208,12 +1217,12 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         DeviceBuffer<int> esrc(nE), edst(nE);
         DeviceBuffer<unsigned long long> emsk(nE);
         if (nE)
-            deps_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(nt, kDepWarps), kDepWarps * 32, 0, s>>>(
+            launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, 
                 P, 1, nullptr, doff.get(), esrc.get(), edst.get(), emsk.get());
         DeviceBuffer<unsigned> rcnt(nt), cursor(nt);
         rcnt.zero(s);
         cursor.zero(s);
-        if (nE) dep_count_kernel<<<nblocks(nE, 256), 256, 0, s>>>(nE, esrc.get(), rcnt.get());
+        if (nE) launch(dep_count_kernel, nblocks(nE, 256), 256, 0, s, nE, esrc.get(), rcnt.get());
         std::vector<unsigned> hr(nt);
         rcnt.download(hr.data(), nt, s);
         HFM_CUDA(cudaStreamSynchronize(s));
@@ -1227,7 +1236,7 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         DeviceBuffer<int> rtile(nE);
         DeviceBuffer<unsigned long long> rmask(nE);
         if (nE)
-            dep_scatter_kernel<<<nblocks(nE, 256), 256, 0, s>>>(nE, esrc.get(), edst.get(), emsk.get(), rptr.get(),
+            launch(dep_scatter_kernel, nblocks(nE, 256), 256, 0, s, nE, esrc.get(), edst.get(), emsk.get(), rptr.get(),
                                                                 cursor.get(), rtile.get(), rmask.get());
         HFM_CUDA(cudaGetLastError());
         HFM_TRACE("deps");
@@ -1274,7 +1283,7 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         if (!st.empty()) {
             stile.upload(st, s);
             smask.upload(sm, s);
-            init_lists_kernel<Real><<<nblocks((long long)st.size() * 32, 128), 128, 0, s>>>(P, stile.get(), smask.get(),
+            launch(init_lists_kernel<Real>, nblocks((long long)st.size() * 32, 128), 128, 0, s, P, stile.get(), smask.get(),
                                                                                              (int)st.size());
             HFM_CUDA(cudaGetLastError());
             HFM_TRACE("init lists");
@@ -1286,6 +1295,7 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
             if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
             const int grid = nsm * per_sm;
             void *args[] = {&P};
+            count_launch();
             HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, SHARE>, dim3(grid),
                                                  dim3(kWarpsPerCta * 32), args, 0, s));
         }
@@ -1296,21 +1306,28 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         stats.download(hs, 4, s);
         DeviceBuffer<unsigned long long> nacc(1);
         nacc.zero(s);
-        count_finite_kernel<Real><<<std::min<unsigned>(nblocks(N, 256), 2048), 256, 0, s>>>(values.get(), N, nacc.get());
+        launch(count_finite_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 2048), 256, 0, s, values.get(), N, nacc.get());
         unsigned long long hn = 0;
         nacc.download(&hn, 1, s);
-        res.values.resize(N);
-        if (std::is_same<Real, double>::value) {
+        if (p.d_values_out) {
+            if (std::is_same<Real, double>::value)
+                HFM_CUDA(cudaMemcpyAsync(p.d_values_out, values.get(), N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            else
+                launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), p.d_values_out, N);
+            HFM_CUDA(cudaStreamSynchronize(s));
+        } else if (std::is_same<Real, double>::value) {
+            res.values.resize(N);
             values.download(reinterpret_cast<Real *>(res.values.data()), N, s);
         } else {
+            res.values.resize(N);
             DeviceBuffer<double> vd(N);
-            to_double_kernel<Real><<<std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s>>>(values.get(), vd.get(), N);
+            launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), vd.get(), N);
             vd.download(res.values.data(), N, s);
             HFM_CUDA(cudaStreamSynchronize(s));
         }
         if (p.want_active) {
             DeviceBuffer<unsigned long long> act(N);
-            active_kernel<Real, NFWD, NSYM, SHARE><<<nblocks(N, 128), 128, 0, s>>>(P, act.get());
+            launch(active_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, act.get());
             res.active.resize(N);
             act.download(reinterpret_cast<unsigned long long *>(res.active.data()), N, s);
         }

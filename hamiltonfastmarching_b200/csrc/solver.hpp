@@ -37,6 +37,11 @@ struct EulerProblem {
     std::vector<double> mult;          // [N] speed multiplier (RowMajor)
 
     std::vector<uint8_t> walls;        // [N] or empty
+    // Device-resident alternatives (zero-copy path): used instead of `metric` / `walls` when set,
+    // and `d_values_out` receives the FP64 arrival times instead of EulerResult::values.
+    const double *d_metric = nullptr;
+    const uint8_t *d_walls = nullptr;
+    double *d_values_out = nullptr;
     std::vector<int64_t> seed_index;   // sorted, unique
     std::vector<double> seed_value;
 

@@ -79,6 +79,42 @@ int hfm_run(hfm_io *io, const char *expected_model);
 /* Message of the last failure on `io` ("" if none). Valid until the next call on `io`. */
 const char *hfm_io_last_error(hfm_io *io);
 
+/* Device-resident solve of a Riemannian instance (zero-copy path for serving and batching).
+ * No reference counterpart as a function: it performs what Run(IO&) does for the Riemann2/Riemann3
+ * models (Headers/Specializations/Riemannian.h:41-61 stencils, HamiltonFastMarching.hxx:59-112 solve)
+ * with `metric`, `walls` and the output `values` already in device memory (RowMajor, component
+ * axis last, packed xx,xy,yy[,xz,yz,zz]). Seeds are host arrays of RowMajor linear indices.
+ * The solve runs on `stream` (cudaStream_t, NULL = legacy default stream); the call returns when
+ * `values` is complete. On failure a message is copied into `err` (up to errcap bytes). */
+typedef struct {
+    int ndim;                 /* 2 or 3 */
+    int64_t dims[3];
+    double grid_scale[3];
+    int dual;                 /* nonzero: `metric` is the dual metric */
+    int precision;            /* 64 (reference-exact path) or 32 (fast path) */
+    int sweeps_per_tile;      /* 0: default */
+    const double *metric;     /* device pointer */
+    const uint8_t *walls;     /* device pointer or NULL */
+    int64_t nseeds;
+    const int64_t *seed_index;
+    const double *seed_value;
+    double *values;           /* device pointer, receives FP64 arrival times (+inf unreached) */
+    void *stream;
+} hfm_riemann_device_args;
+
+typedef struct {
+    int64_t n_accepted;       /* reached cells (the reference's nAccepted) */
+    int max_stencil_width;
+    double stencil_ms, solve_ms;
+    int64_t rounds, tile_activations, local_solves;
+} hfm_solve_stats;
+
+int hfm_solve_riemann_device(const hfm_riemann_device_args *args, hfm_solve_stats *stats, char *err,
+                             size_t errcap);
+
+/* Number of CUDA kernels this library has launched in the process (launch accounting). */
+int hfm_kernel_launches(unsigned long long *count);
+
 /* Library identification and device presence check (no GPU work). */
 const char *hfm_version(void);
 int hfm_device_count(int *count);

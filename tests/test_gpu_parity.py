@@ -135,3 +135,34 @@ def test_repeatable_and_seeds_fixed():
     np.testing.assert_array_equal(a, b)
     P = O.Problem(p)
     np.testing.assert_array_equal(a.ravel()[P.seed_index], 0.0)
+
+
+def test_device_entry_point_matches_host_api():
+    """hfm_solve_riemann_device (inputs and output in device memory) equals HFMIO.run."""
+    import ctypes
+    import torch
+    from hamiltonfastmarching_b200 import _lib
+    p = W.riemann3_case(40, n_spheres=6, n_seeds=4)
+    ref = gpu_solve(p)
+    n = 40
+    metric = torch.from_numpy(np.ascontiguousarray(p["metric"].reshape(-1, 6))).cuda()
+    walls = torch.from_numpy(np.ascontiguousarray((p["walls"] != 0).astype(np.uint8).ravel())).cuda()
+    values = torch.empty(n ** 3, dtype=torch.float64, device="cuda")
+    ijk = np.floor(p["seeds"] / p["gridScale"]).astype(np.int64)
+    sidx = np.ascontiguousarray(np.ravel_multi_index(ijk.T, (n, n, n)).astype(np.int64))
+    sval = np.zeros(len(sidx))
+    a = _lib.RiemannDeviceArgs()
+    a.ndim = 3
+    for i in range(3):
+        a.dims[i] = n
+        a.grid_scale[i] = p["gridScale"]
+    a.precision = 64
+    a.metric, a.walls, a.values = metric.data_ptr(), walls.data_ptr(), values.data_ptr()
+    a.nseeds, a.seed_index, a.seed_value = len(sidx), sidx.ctypes.data, sval.ctypes.data
+    a.stream = torch.cuda.current_stream().cuda_stream
+    st = _lib.SolveStats()
+    err = ctypes.create_string_buffer(256)
+    assert _lib.load().hfm_solve_riemann_device(ctypes.byref(a), ctypes.byref(st), err, 256) == 0, err.value
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(values.cpu().numpy().reshape(n, n, n), ref["values"])
+    assert st.n_accepted == int(ref["nAccepted"])
