@@ -54,6 +54,10 @@ class SolveStats(ctypes.Structure):
 
 SIGNATURES["hfm_solve_riemann_device"] = ([ctypes.POINTER(RiemannDeviceArgs), ctypes.POINTER(SolveStats),
                                            ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int)
+SIGNATURES["hfm_solve_riemann2_static_scratch"] = ([ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
+                                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int)
 SIGNATURES["hfm_kernel_launches"] = ([ctypes.POINTER(ctypes.c_ulonglong)], ctypes.c_int)
 
 _lib = None

@@ -112,6 +112,22 @@ typedef struct {
 int hfm_solve_riemann_device(const hfm_riemann_device_args *args, hfm_solve_stats *stats, char *err,
                              size_t errcap);
 
+/* Riemann2 FP64 solve that allocates nothing. No counterpart in the reference: it exists for
+ * callers that cannot let a library allocate device memory (a host allocator that reserves the
+ * whole device, a fixed memory budget, or a loop that must not be stalled by the device-wide
+ * synchronisation of cudaMalloc/cudaFree). All intermediate arrays live in one fixed 9,453,824-byte
+ * device buffer owned by the library, present on every GPU that loads it until the process exits;
+ * the caller passes the metric (`nx*ny*3` doubles, RowMajor, packed xx,xy,yy) and receives the
+ * arrival times (`nx*ny` doubles) in its own device memory. Limits: nx*ny <= 262144 cells and
+ * 1..1024 seeds (RowMajor linear indices, host arrays); larger inputs fail with HFM_ERR_VALUE.
+ * The first call on a device looks up the buffer's device address (make it before any stream
+ * capture). Calls share the buffer: concurrent or overlapping calls on the GPU race and must be
+ * serialised by the caller. Results equal hfm_solve_riemann_device with precision 64. */
+int hfm_solve_riemann2_static_scratch(int64_t nx, int64_t ny, double grid_scale, const double *metric,
+                                      int dual, int64_t nseeds, const int64_t *seed_index,
+                                      const double *seed_value, double *values, void *stream, char *err,
+                                      size_t errcap);
+
 /* Number of CUDA kernels this library has launched in the process (launch accounting). */
 int hfm_kernel_launches(unsigned long long *count);
 

@@ -15,7 +15,7 @@ from hamiltonfastmarching_b200 import _lib
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "hfm_b200.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(hfm_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(hfm_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():
