@@ -77,7 +77,7 @@ constexpr unsigned kVisPlus = 1u << 24, kVisMinus = 1u << 25, kFixed = 1u << 28,
 constexpr unsigned kShFixed = 1u << 30, kShDead = 1u << 31;
 constexpr int kWarpsPerCta = 4;
 constexpr int kDepWarps = 2;
-constexpr int kDepCap = 2048;
+constexpr int kDepCap = 1024;
 constexpr unsigned long long kBarrierPolls = 1ull << 25;
 
 __host__ __device__ __forceinline__ unsigned pack_off(int o0, int o1, int o2) {
@@ -99,7 +99,16 @@ struct Dev {
     // reverse tile dependencies: tile T -> tiles whose stencils read T, with the cells they read
     const long long *dep_ptr;
     const int *dep_tile;
-    const unsigned long long *dep_mask;
+    const unsigned long long *dep_mask;    // cells of T read by the dependent tile
+    const unsigned long long *dep_dmask;   // cells of the dependent tile that read T
+    unsigned long long *dirty;             // [ntile] cells whose inputs changed since their last solve
+    // value-ordered scheduling: key = smallest changed value among the tiles that woke the tile
+    unsigned long long *key;               // [ntile] bit patterns of non-negative doubles
+    // largest value among a tile's solvable cells (+inf while any is unreached); values only
+    // decrease, so a stale entry is an upper bound
+    unsigned long long *maxval;            // [ntile]
+    unsigned long long *rstat;             // [8][4] per round slot: min key, max key, tiles solved, -
+    unsigned order_lo, order_hi;           // tiles solved per round kept in [lo, hi]; lo = 0: plain FIM
     // active-tile lists (triple buffered) and their dedupe flags
     int *list[3];
     unsigned *count[3];
@@ -116,12 +125,29 @@ struct Dev {
 // --------------------------------------------------------------------------------------------
 // Hopf-Lax update over neighbour candidates v[k] (+inf if unusable) with weights w[k], taken in
 // increasing order (ties by k); see the file header. `used` receives the bitmask of taken k.
+//
+// Fast marching adds the next neighbour iff its value is below the current root r (computed with
+// rounding). For t above the vertex of q(t) = a t^2 - 2 b t + c (t measured from minVal), t < r
+// iff q(t) < 0, so the decision is taken from the sign of q, which needs no square root or
+// division; only when |q| is within 1e-12 of the magnitude of its terms (far wider than the
+// rounding of q and of the root) is the root computed and compared exactly as fast marching does.
+// The root itself is computed once, after the last addition.
+template <typename Real>
+__device__ __forceinline__ Real quad_root(Real minVal, Real a, Real b, Real c) {
+    using A = Arith<Real>;
+    if (a == Real(0)) return A::inf();
+    const Real d2 = A::sub(A::mul(b, b), A::mul(a, c));
+    const Real d = A::sqrt(Real(0) < d2 ? d2 : Real(0));
+    return A::add(minVal, A::div(A::add(b, d), a));
+}
+
 template <typename Real, int ND>
 __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real (&w)[ND], unsigned *used) {
     using A = Arith<Real>;
     const Real INF = A::inf();
+    const Real band = sizeof(Real) == 8 ? Real(1e-12) : Real(1e-5);
     unsigned taken = 0;
-    Real minVal = 0, a = 0, b = 0, c = -1, r = INF;
+    Real minVal = 0, a = 0, b = 0, c = -1;
     for (int it = 0; it < ND; ++it) {
         Real bv = INF, bw = 0;
         int bk = -1;
@@ -130,24 +156,26 @@ __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real 
             if (!((taken >> k) & 1u) && v[k] < bv) { bv = v[k]; bw = w[k]; bk = k; }
         }
         if (bk < 0) break;
-        if (it > 0 && !(bv < r)) break;
-        if (it == 0) minVal = bv;
+        if (it == 0) {
+            minVal = bv;
+        } else {
+            // stop unless bv < root(a, b, c)
+            const Real t = A::sub(bv, minVal);
+            const Real at2 = A::mul(A::mul(a, t), t), bt2 = A::mul(Real(2), A::mul(b, t));
+            const Real q = A::add(A::sub(at2, bt2), c);
+            const Real mag = A::add(A::add(fabs(at2), fabs(bt2)), fabs(c));
+            if (q > band * mag) break;
+            if (!(q < -band * mag) && !(bv < quad_root<Real>(minVal, a, b, c))) break;
+        }
         const Real dv = A::sub(bv, minVal);
         const Real wv = A::mul(bw, dv);
         a = A::add(a, bw);
         b = A::add(b, wv);
         c = A::add(c, A::mul(wv, dv));
-        if (a == Real(0)) {
-            r = INF;
-        } else {
-            const Real d2 = A::sub(A::mul(b, b), A::mul(a, c));
-            const Real d = A::sqrt(Real(0) < d2 ? d2 : Real(0));
-            r = A::add(minVal, A::div(A::add(b, d), a));
-        }
         taken |= 1u << bk;
     }
     if (used) *used = taken;
-    return r;
+    return taken ? quad_root<Real>(minVal, a, b, c) : INF;
 }
 
 // Local solve at one cell. `sv` holds the current values of the warp's tile (nullptr: read all
@@ -243,10 +271,14 @@ __device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bo
     if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
 }
 
-// Pushes the dependents of tile T that read a cell of `mask` (plus T itself if `self`).
+// Pushes the dependents of tile T that read a cell of `mask`, marking as dirty the cells of each
+// dependent that read T; if `self_pending` is non-zero T itself is pushed with those cells dirty.
+// Dirty bits are set before the dedupe flag so that a dependent already queued, or one that has
+// just claimed itself, sees them on its next activation.
 template <typename Real>
-__device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int T, unsigned long long mask, bool self,
-                                                int lane) {
+__device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int slot, int T, unsigned long long mask,
+                                                unsigned long long self_pending, unsigned long long mu, int lane) {
+    bool any = false;
     if (mask) {
         const long long b = P.dep_ptr[T], e = P.dep_ptr[T + 1];
         for (long long base = b; base < e; base += 32) {
@@ -256,23 +288,87 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
             if (i < e) {
                 D = P.dep_tile[i];
                 want = (P.dep_mask[i] & mask) != 0ull;
+                // a neighbour value v improves x only if v < u(x) (ConditionalUpdate,
+                // HamiltonFastMarching.hxx:151): no cell of D can gain from values >= max u(D)
+                if (want) {
+                    const double mx = __longlong_as_double(__ldcg(P.maxval + D));
+                    want = __longlong_as_double(mu) < mx * (1.0 + 16.0 * DBL_EPSILON);
+                }
+                if (want) {
+                    atomicOr(P.dirty + D, P.dep_dmask[i]);
+                    atomicMin(P.key + D, mu);
+                }
             }
+            any |= __any_sync(0xffffffffu, want);
             push_tiles(P, li, D, want, lane);
         }
     }
-    push_tiles(P, li, T, self && lane == 0, lane);
+    if (self_pending && lane == 0) {
+        atomicOr(P.dirty + T, self_pending);
+        atomicMin(P.key + T, mu);
+    }
+    push_tiles(P, li, T, self_pending != 0ull && lane == 0, lane);
+    if ((any || self_pending) && lane == 0) {
+        atomicMin(P.rstat + slot * 4 + 0, mu);
+        atomicMax(P.rstat + slot * 4 + 1, mu);
+    }
 }
 
-// Processes one tile with local Jacobi sweeps; returns through `mask` the cells that changed.
+// Cells of the warp's tile that the cell at (x0,x1,x2) reads through its visible stencil entries.
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-__device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next,
+__device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, long long c, int x0, int x1, int x2,
+                                                           int tx0, int tx1, int tx2) {
+    constexpr int ND = NFWD + NSYM;
+    const GridGeom &g = P.g;
+    unsigned long long m = 0;
+    const unsigned visw = SHARE ? P.vis[c] : 0u;
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+        int o0, o1, o2;
+        unsigned bits;
+        if (SHARE) {
+            const int8_t *o = P.cls_off + ((long long)x2 * ND + k) * 3;
+            o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
+            bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
+        } else {
+            const unsigned cd = P.code[k * P.ntc + c];
+            o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
+            bits = ((cd & kVisPlus) ? 1u : 0u) | ((cd & kVisMinus) ? 2u : 0u);
+        }
+#pragma unroll
+        for (int si = 0; si < 2; ++si) {
+            if (!((bits >> si) & 1u)) continue;
+            const int s = si ? -1 : 1;
+            int n2 = x2 + s * o2;
+            if (SHARE && g.periodic[2]) {
+                n2 %= g.dims[2];
+                if (n2 < 0) n2 += g.dims[2];
+            }
+            const unsigned l0 = x0 + s * o0 - tx0, l1 = x1 + s * o1 - tx1, l2 = n2 - tx2;
+            if (l0 < (1u << g.tshift[0]) && l1 < (1u << g.tshift[1]) && l2 < (1u << g.tshift[2]))
+                m |= 1ull << (((l0 << g.tshift[1] | l1) << g.tshift[2]) | l2);
+        }
+    }
+    return m;
+}
+
+// One activation of tile T: solve the dirty cells, then, sweep after sweep, the cells reading an
+// in-tile cell that changed in the previous sweep, until nothing changes (warp vote) or the sweep
+// budget is spent (T re-queues itself with the cells still pending).
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves) {
     const GridGeom &g = P.g;
     int t0, t1, t2;
     g.tile_coords(T, t0, t1, t2);
     const int tx0 = t0 << g.tshift[0], tx1 = t1 << g.tshift[1], tx2 = t2 << g.tshift[2];
+    unsigned long long dirty = 0;
+    if (lane == 0) dirty = atomicExch(P.dirty + T, 0ull);
+    dirty = __shfl_sync(0xffffffffu, dirty, 0);
+    __threadfence();
     Real cur[2];
-    bool upd[2], chg[2] = {false, false};
+    bool upd[2], todo[2], chg[2] = {false, false};
+    unsigned long long reads[2] = {0ull, 0ull};
     int xs[2][3];
     long long gi[2];
     const Real INF = Arith<Real>::inf();
@@ -289,6 +385,8 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         gi[j] = valid ? g.lin(xs[j][0], xs[j][1], xs[j][2]) : 0;
         cur[j] = (valid && !dead) ? __ldcg(P.values + gi[j]) : INF;
         upd[j] = valid && !dead && !fixed;
+        if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, SHARE>(P, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
+        todo[j] = upd[j] && ((dirty >> l) & 1ull);
         sv[l] = cur[j];
     }
     __syncwarp();
@@ -298,64 +396,126 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 #pragma unroll 1
         for (int j = 0; j < 2; ++j) {
             nv[j] = cur[j];
-            if (upd[j]) {
+            if (todo[j]) {
                 nv[j] = solve_cell<Real, NFWD, NSYM, SHARE>(P, (long long)T * 64 + lane + 32 * j, xs[j][0], xs[j][1],
                                                             xs[j][2], tx0, tx1, tx2, sv, nullptr, nullptr);
                 ++n_solves;
             }
         }
         __syncwarp();
-        bool ch = false;
+        bool now[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            if (nv[j] != cur[j]) {
+            now[j] = nv[j] != cur[j];
+            if (now[j]) {
                 cur[j] = nv[j];
                 sv[lane + 32 * j] = nv[j];
-                ch = true;
                 chg[j] = true;
             }
         }
         __syncwarp();
-        if (!__any_sync(0xffffffffu, ch)) { converged = true; break; }
+        const unsigned long long C = (unsigned long long)__ballot_sync(0xffffffffu, now[0]) |
+                                     ((unsigned long long)__ballot_sync(0xffffffffu, now[1]) << 32);
+        if (!C) { converged = true; break; }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) todo[j] = upd[j] && (reads[j] & C) != 0ull;
     }
+    unsigned long long pending = 0;
+    if (!converged)
+        pending = (unsigned long long)__ballot_sync(0xffffffffu, todo[0]) |
+                  ((unsigned long long)__ballot_sync(0xffffffffu, todo[1]) << 32);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
         if (chg[j]) __stcg(P.values + gi[j], cur[j]);
     const unsigned lo = __ballot_sync(0xffffffffu, chg[0]);
     const unsigned hi = __ballot_sync(0xffffffffu, chg[1]);
     const unsigned long long mask = (unsigned long long)lo | ((unsigned long long)hi << 32);
+    // largest solvable value of the tile, for the wake-up pruning of its sources
+    double mx = 0.0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+        if (upd[j] && !((double)cur[j] <= mx)) mx = (double)cur[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) __stcg(P.maxval + T, (unsigned long long)__double_as_longlong(mx));
+    // smallest changed value: the wake-up key of the dependents
+    double mu = Arith<double>::inf();
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+        if (chg[j] && (double)cur[j] < mu) mu = (double)cur[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mu = fmin(mu, __shfl_xor_sync(0xffffffffu, mu, o));
     __threadfence();
-    push_dependents(P, li_next, T, mask, !converged, lane);
+    push_dependents(P, li_next, slot, T, mask, pending, (unsigned long long)__double_as_longlong(mu), lane);
 }
 
-// Persistent cooperative solver: rounds over the triple-buffered active-tile lists.
+// Persistent cooperative solver: rounds over the triple-buffered active-tile lists. Round r solves
+// the active tiles whose key is at most theta_r = (smallest key) + delta_r and carries the others to
+// the next list; delta_r doubles when a round solved fewer than order_lo tiles and halves above
+// order_hi, so the band follows the arrival front with enough tiles in flight. Every block derives
+// the same theta_r from the same round statistics read after the barrier.
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 __global__ void __launch_bounds__(kWarpsPerCta * 32) fim_kernel(Dev<Real> P) {
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long kInfBits = 0x7ff0000000000000ull;
     unsigned long long n_act = 0, n_solves = 0;
+    double delta = Arith<double>::inf();
     int r = 0;
     bool ok = true;
     for (; r < P.max_rounds; ++r) {
         const int cur = r % 3, nxt = (r + 1) % 3, old = (r + 2) % 3;
+        const int slot = r & 7, nslot = (r + 1) & 7, rslot = (r + 4) & 7;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             *P.count[old] = 0;
             *P.claim[old] = 0;
+            P.rstat[rslot * 4 + 0] = kInfBits;
+            P.rstat[rslot * 4 + 1] = 0ull;
+            P.rstat[rslot * 4 + 2] = 0ull;
         }
         const unsigned n = *(volatile unsigned *)P.count[cur];
+        const double mk = __longlong_as_double(*(volatile unsigned long long *)(P.rstat + slot * 4 + 0));
+        const double theta = (P.order_lo == 0u) ? Arith<double>::inf() : mk + delta;
+        unsigned long long solved = 0;
         while (true) {
             unsigned i = 0;
             if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
             i = __shfl_sync(0xffffffffu, i, 0);
             if (i >= n) break;
             const int T = P.list[cur][i];
-            if (lane == 0) P.flag[cur][T] = 0u;
-            process_tile<Real, NFWD, NSYM, SHARE>(P, T, s_vals[warp], lane, nxt, n_solves);
+            unsigned long long kt = 0;
+            if (lane == 0) {
+                P.flag[cur][T] = 0u;
+                kt = *(volatile unsigned long long *)(P.key + T);
+            }
+            kt = __shfl_sync(0xffffffffu, kt, 0);
+            if (__longlong_as_double(kt) > theta) {
+                // not yet in the band: carry to the next round with its key
+                push_tiles(P, nxt, T, lane == 0, lane);
+                if (lane == 0) atomicMin(P.rstat + nslot * 4 + 0, kt);
+                continue;
+            }
+            if (lane == 0) atomicExch(P.key + T, kInfBits);
+            process_tile<Real, NFWD, NSYM, SHARE>(P, T, s_vals[warp], lane, nxt, nslot, n_solves);
             ++n_act;
+            ++solved;
         }
+        if (lane == 0 && solved) atomicAdd(P.rstat + slot * 4 + 2, solved);
         ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
         if (!ok) break;
         if (*(volatile unsigned *)P.count[nxt] == 0u) { ++r; break; }
+        if (P.order_lo) {
+            const unsigned long long np = *(volatile unsigned long long *)(P.rstat + slot * 4 + 2);
+            if (r == 0) {
+                const double lo_k = __longlong_as_double(*(volatile unsigned long long *)(P.rstat + nslot * 4 + 0));
+                const double hi_k = __longlong_as_double(*(volatile unsigned long long *)(P.rstat + nslot * 4 + 1));
+                delta = hi_k > lo_k ? 2.0 * (hi_k - lo_k) : Arith<double>::inf();
+            } else if (np < P.order_lo) {
+                delta *= 2.0;
+            } else if (np > P.order_hi) {
+                delta *= 0.5;
+            }
+        }
     }
     if (ok && r >= P.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(P.status, (unsigned)kErrRoundCap);
     if (lane == 0) {
@@ -375,7 +535,7 @@ template <typename Real>
 __global__ void init_lists_kernel(Dev<Real> P, const int *seed_tiles, const unsigned long long *seed_masks, int n) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (wid >= n) return;
-    push_dependents(P, 0, seed_tiles[wid], seed_masks[wid], true, lane);
+    push_dependents(P, 0, 0, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, lane);
 }
 
 // --------------------------------------------------------------------------------------------
@@ -624,16 +784,18 @@ __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *va
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 __global__ void __launch_bounds__(kDepWarps * 32)
     deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
-                unsigned long long *msk) {
+                unsigned long long *msk, unsigned long long *dmsk) {
     constexpr int ND = NFWD + NSYM;
     __shared__ int keys[kDepWarps][kDepCap];
     __shared__ unsigned long long masks[kDepWarps][kDepCap];
+    __shared__ unsigned long long dmasks[kDepWarps][kDepCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long D = (long long)blockIdx.x * kDepWarps + warp;
     if (D >= P.g.ntile) return;
     int *K = keys[warp];
     unsigned long long *M = masks[warp];
-    for (int i = lane; i < kDepCap; i += 32) { K[i] = -1; M[i] = 0ull; }
+    unsigned long long *DM = dmasks[warp];
+    for (int i = lane; i < kDepCap; i += 32) { K[i] = -1; M[i] = 0ull; DM[i] = 0ull; }
     __syncwarp();
     const GridGeom &g = P.g;
     int t0, t1, t2;
@@ -671,7 +833,11 @@ __global__ void __launch_bounds__(kDepWarps * 32)
                 int probes = 0;
                 while (true) {
                     const int prev = atomicCAS(&K[h], -1, T);
-                    if (prev == -1 || prev == T) { atomicOr(&M[h], 1ull << b); break; }
+                    if (prev == -1 || prev == T) {
+                        atomicOr(&M[h], 1ull << b);
+                        atomicOr(&DM[h], 1ull << l);
+                        break;
+                    }
                     h = (h + 1) & (kDepCap - 1);
                     if (++probes >= kDepCap) { overflow = true; break; }
                 }
@@ -689,6 +855,7 @@ __global__ void __launch_bounds__(kDepWarps * 32)
             src[pos] = K[base + lane];
             dst[pos] = (int)D;
             msk[pos] = M[base + lane];
+            dmsk[pos] = DM[base + lane];
         }
         total += __popc(bal);
     }
@@ -701,13 +868,15 @@ __global__ void dep_count_kernel(long long n, const int *src, unsigned *rcnt) {
 }
 
 __global__ void dep_scatter_kernel(long long n, const int *src, const int *dst, const unsigned long long *msk,
-                                   const long long *rptr, unsigned *cursor, int *rtile, unsigned long long *rmask) {
+                                   const unsigned long long *dmsk, const long long *rptr, unsigned *cursor, int *rtile,
+                                   unsigned long long *rmask, unsigned long long *rdmask) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int T = src[i];
     const long long pos = rptr[T] + atomicAdd(cursor + T, 1u);
     rtile[pos] = dst[i];
     rmask[pos] = msk[i];
+    rdmask[pos] = dmsk[i];
 }
 
 // --------------------------------------------------------------------------------------------
@@ -1201,7 +1370,7 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
     HFM_TRACE("seeds");
     DeviceBuffer<unsigned> dcnt(nt);
     launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, 
-        P, 0, dcnt.get(), nullptr, nullptr, nullptr, nullptr);
+        P, 0, dcnt.get(), nullptr, nullptr, nullptr, nullptr, nullptr);
     HFM_CUDA(cudaGetLastError());
     DeviceBuffer<long long> doff(nt + 1), rptr(nt + 1);
     {
@@ -1215,10 +1384,10 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         doff.upload(ho, s);
         const long long nE = tot;
         DeviceBuffer<int> esrc(nE), edst(nE);
-        DeviceBuffer<unsigned long long> emsk(nE);
+        DeviceBuffer<unsigned long long> emsk(nE), edmsk(nE);
         if (nE)
-            launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, 
-                P, 1, nullptr, doff.get(), esrc.get(), edst.get(), emsk.get());
+            launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s,
+                   P, 1, nullptr, doff.get(), esrc.get(), edst.get(), emsk.get(), edmsk.get());
         DeviceBuffer<unsigned> rcnt(nt), cursor(nt);
         rcnt.zero(s);
         cursor.zero(s);
@@ -1234,14 +1403,29 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         P.dep_ptr = rptr.get();
         // reverse arrays live until the end of the solve
         DeviceBuffer<int> rtile(nE);
-        DeviceBuffer<unsigned long long> rmask(nE);
+        DeviceBuffer<unsigned long long> rmask(nE), rdmask(nE);
         if (nE)
-            launch(dep_scatter_kernel, nblocks(nE, 256), 256, 0, s, nE, esrc.get(), edst.get(), emsk.get(), rptr.get(),
-                                                                cursor.get(), rtile.get(), rmask.get());
+            launch(dep_scatter_kernel, nblocks(nE, 256), 256, 0, s, nE, esrc.get(), edst.get(), emsk.get(),
+                   edmsk.get(), rptr.get(), cursor.get(), rtile.get(), rmask.get(), rdmask.get());
         HFM_CUDA(cudaGetLastError());
         HFM_TRACE("deps");
         P.dep_tile = rtile.get();
         P.dep_mask = rmask.get();
+        P.dep_dmask = rdmask.get();
+        DeviceBuffer<unsigned long long> dirty(nt), key(nt), rstat(32);
+        dirty.zero(s);
+        P.dirty = dirty.get();
+        launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, key.get(), nt, 0x7ff0000000000000ull);
+        {
+            unsigned long long h[32];
+            for (int i = 0; i < 8; ++i) { h[4 * i] = 0x7ff0000000000000ull; h[4 * i + 1] = 0; h[4 * i + 2] = 0; h[4 * i + 3] = 0; }
+            rstat.upload(h, 32, s);
+        }
+        P.key = key.get();
+        P.rstat = rstat.get();
+        DeviceBuffer<unsigned long long> maxval(nt);
+        launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, maxval.get(), nt, 0x7ff0000000000000ull);
+        P.maxval = maxval.get();
         res.t_stencil_ms = tm.stop(s);
         check_status(status, "stencil");
 
@@ -1294,6 +1478,9 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
                                                                    kWarpsPerCta * 32, 0));
             if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
             const int grid = nsm * per_sm;
+            const double nwarps = (double)grid * kWarpsPerCta;
+            P.order_lo = p.ordered ? (unsigned)std::max(1.0, p.band_lo * nwarps) : 0u;
+            P.order_hi = p.ordered ? (unsigned)std::max(2.0, p.band_hi * nwarps) : 0u;
             void *args[] = {&P};
             count_launch();
             HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, SHARE>, dim3(grid),

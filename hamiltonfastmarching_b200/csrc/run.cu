@@ -216,6 +216,10 @@ void set_common_solver_options(Store &io, EulerProblem &p) {
     p.sweeps_per_tile = (int)io.get_scalar("tileSweeps", 16, 3);
     if (p.sweeps_per_tile < 1 || p.sweeps_per_tile > 1024) throw Error(HFM_ERR_VALUE, "tileSweeps out of range");
     p.max_rounds = (int)io.get_scalar("maxRounds", (double)(1 << 20), 3);
+    p.ordered = io.get_scalar("tileOrdering", 1.0, 3) != 0;
+    p.band_lo = io.get_scalar("bandLo", p.band_lo, 3);
+    p.band_hi = io.get_scalar("bandHi", p.band_hi, 3);
+    if (!(p.band_lo > 0) || !(p.band_hi > p.band_lo)) throw Error(HFM_ERR_VALUE, "bandLo/bandHi must satisfy 0 < bandLo < bandHi");
 }
 
 // ------------------------------------------------------------------------------------------

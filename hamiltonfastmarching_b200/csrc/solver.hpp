@@ -52,6 +52,10 @@ struct EulerProblem {
     bool want_stencils = false;        // export per-cell offsets/weights (RiemannPerCell)
     int sweeps_per_tile = 16;          // local Jacobi sweeps before a tile re-queues itself
     int max_rounds = 1 << 20;
+    // Value-ordered scheduling: a round solves the tiles whose wake-up key is within a band above
+    // the smallest key; the band adapts to keep [band_lo, band_hi] x (resident warps) tiles per round.
+    bool ordered = true;
+    double band_lo = 2.0, band_hi = 8.0;
 };
 
 // FirstVariation::BackwardVariation output for one group of inspected points.
