@@ -33,6 +33,7 @@ inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
 template <typename T>
 class DeviceBuffer {
 public:
+    static constexpr size_t kPinThreshold = size_t(64) << 20;
     DeviceBuffer() = default;
     explicit DeviceBuffer(size_t n) { alloc(n); }
     ~DeviceBuffer() { release(); }
@@ -61,7 +62,21 @@ public:
     }
     void upload(const T *h, size_t n, cudaStream_t s = current_stream()) {
         if (n > n_) alloc(n);
-        if (n) HFM_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+        if (!n) return;
+        // Large pageable sources are page-locked for the transfer (DMA at full link speed instead
+        // of staged copies); if locking is refused the copy proceeds from pageable memory.
+        const size_t bytes = n * sizeof(T);
+        if (bytes >= kPinThreshold &&
+            cudaHostRegister(const_cast<T *>(h), bytes, cudaHostRegisterReadOnly) == cudaSuccess) {
+            const cudaError_t e = cudaMemcpyAsync(p_, h, bytes, cudaMemcpyHostToDevice, s);
+            const cudaError_t e2 = cudaStreamSynchronize(s);
+            cudaHostUnregister(const_cast<T *>(h));
+            HFM_CUDA(e);
+            HFM_CUDA(e2);
+            return;
+        }
+        cudaGetLastError();
+        HFM_CUDA(cudaMemcpyAsync(p_, h, bytes, cudaMemcpyHostToDevice, s));
     }
     void upload(const std::vector<T> &v, cudaStream_t s = current_stream()) { upload(v.data(), v.size(), s); }
     void download(T *h, size_t n, cudaStream_t s = current_stream()) const {

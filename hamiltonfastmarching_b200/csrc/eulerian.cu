@@ -1189,7 +1189,7 @@ void run_adjoint(const Dev<Real> &P, const EulerProblem &p, EulerResult &res, De
     HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 256, 0));
     if (per_sm < 1) throw Error(HFM_ERR_CUDA, "adjoint kernel cannot be resident");
-    std::vector<double> hvals = res.values;
+    const double *hvals = p.h_values_out ? p.h_values_out : res.values.data();
     for (size_t gi = 0; gi < p.adjoint_index.size(); ++gi) {
         HFM_CUDA(cudaMemcpyAsync(indeg.get(), indeg0.get(), N * sizeof(int), cudaMemcpyDeviceToDevice, s));
         acc.zero(s);
@@ -1274,7 +1274,8 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         P.weight = weight.get();
         const double *metric_ptr = p.d_metric;
         if (!metric_ptr) {
-            metric.upload(p.metric, s);
+            if (p.metric_ptr) metric.upload(p.metric_ptr, p.metric_len, s);
+            else metric.upload(p.metric, s);
             metric_ptr = metric.get();
         }
         if (p.want_stencils) {
@@ -1503,13 +1504,21 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
                 launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), p.d_values_out, N);
             HFM_CUDA(cudaStreamSynchronize(s));
         } else if (std::is_same<Real, double>::value) {
-            res.values.resize(N);
-            values.download(reinterpret_cast<Real *>(res.values.data()), N, s);
+            double *dst = p.h_values_out;
+            if (!dst) {
+                res.values.resize(N);
+                dst = res.values.data();
+            }
+            values.download(reinterpret_cast<Real *>(dst), N, s);
         } else {
-            res.values.resize(N);
+            double *dst = p.h_values_out;
+            if (!dst) {
+                res.values.resize(N);
+                dst = res.values.data();
+            }
             DeviceBuffer<double> vd(N);
             launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), vd.get(), N);
-            vd.download(res.values.data(), N, s);
+            vd.download(dst, N, s);
             HFM_CUDA(cudaStreamSynchronize(s));
         }
         if (p.want_active) {

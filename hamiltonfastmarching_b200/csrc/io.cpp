@@ -177,7 +177,7 @@ std::vector<double> Store::get_vector(const std::string &key, int ncomp, int64_t
         throw Error(HFM_ERR_VALUE, "IO::GetArray error : Field " + key + " has depth " + std::to_string(dims.size()) +
                                        " instead of expected 1.");
     *count = dims[0];
-    return r.data;
+    return std::vector<double>(r.data.begin(), r.data.end());
 }
 
 // Element permutations of the four orderings (IO.hxx:87-110, 153-233).
@@ -256,11 +256,12 @@ Field Store::get_field(const std::string &key, int ndim, int ncomp) const {
                                        " instead of expected " + std::to_string(ndim) + ".");
     int64_t n = 1;
     for (int64_t d : sd) n *= d;
-    f.data.resize(n * ncomp);
+    if (ordering_ != Ordering::RowMajor) f.data.resize(n * ncomp);
     switch (ordering_) {
         case Ordering::RowMajor:
             f.dims = sd;
-            std::copy(r.data.begin(), r.data.begin() + n * ncomp, f.data.begin());
+            f.data.clear();
+            f.view = r.data.data();
             break;
         case Ordering::YXZ_RowMajor:
             f.dims = transpose_dims(sd);
@@ -308,6 +309,17 @@ void Store::set_field(const std::string &key, const std::vector<int64_t> &dims, 
     }
     if (ncomp > 1) od.push_back(ncomp);
     set_array(key, out.data(), od);
+}
+
+double *Store::create_field(const std::string &key, const std::vector<int64_t> &dims, int ncomp) {
+    if (ordering_ != Ordering::RowMajor) return nullptr;
+    int64_t n = ncomp;
+    for (int64_t d : dims) n *= d;
+    RawElement &r = create(key);
+    r.dims = dims;
+    if (ncomp > 1) r.dims.push_back(ncomp);
+    r.data.resize(n);
+    return r.data.data();
 }
 
 void Store::set_vector(const std::string &key, int64_t count, int ncomp, const double *data) {

@@ -6,8 +6,12 @@
 // with axes in (x, y, z|theta) order and the component axis last.
 #pragma once
 
+#include <sys/mman.h>
+
 #include <cstdint>
+#include <cstdlib>
 #include <map>
+#include <new>
 #include <set>
 #include <stdexcept>
 #include <string>
@@ -21,13 +25,43 @@ struct Error : std::runtime_error {
     Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
 };
 
+// Allocator of the store's numerical arrays: blocks of 4 MiB and more are mapped directly and
+// advised for transparent huge pages, so copying a large field in or out costs few page faults.
+template <typename T>
+struct BigAlloc {
+    using value_type = T;
+    static constexpr size_t kThreshold = size_t(4) << 20;
+    BigAlloc() = default;
+    template <typename U> BigAlloc(const BigAlloc<U> &) {}
+    T *allocate(size_t n) {
+        const size_t bytes = n * sizeof(T);
+        if (bytes >= kThreshold) {
+            void *p = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+            if (p == MAP_FAILED) throw std::bad_alloc();
+            madvise(p, bytes, MADV_HUGEPAGE);
+            return static_cast<T *>(p);
+        }
+        void *p = std::malloc(bytes ? bytes : 1);
+        if (!p) throw std::bad_alloc();
+        return static_cast<T *>(p);
+    }
+    void deallocate(T *p, size_t n) {
+        const size_t bytes = n * sizeof(T);
+        if (bytes >= kThreshold) munmap(p, bytes);
+        else std::free(p);
+    }
+    template <typename U> bool operator==(const BigAlloc<U> &) const { return true; }
+    template <typename U> bool operator!=(const BigAlloc<U> &) const { return false; }
+};
+using DoubleArray = std::vector<double, BigAlloc<double>>;
+
 enum class Setter { User, Compute, Unknown };
 enum class Ordering { RowMajor = 0, ColumnMajor = 1, YXZ_RowMajor = 2, YXZ_ColumnMajor = 3 };
 
 struct RawElement {
     std::string str;
     std::vector<int64_t> dims;
-    std::vector<double> data;
+    DoubleArray data;
     Setter setter = Setter::Unknown;
     bool is_string() const { return data.empty() && dims.empty(); }
     bool is_scalar() const { return !data.empty() && dims.empty(); }
@@ -35,11 +69,20 @@ struct RawElement {
 
 // A domain field read from the store: RowMajor over `dims` (x, y, z order), `ncomp` components
 // per point (component fastest). `dims` is empty for a constant field given as a single element.
+// `view` points into the store when no reordering is needed (RowMajor); it stays valid until the
+// field is modified or erased.
 struct Field {
     std::vector<int64_t> dims;
     int ncomp = 1;
     std::vector<double> data;
+    const double *view = nullptr;
     bool constant() const { return dims.empty(); }
+    const double *ptr() const { return view ? view : data.data(); }
+    size_t size() const {
+        size_t n = (size_t)ncomp;
+        for (int64_t d : dims) n *= (size_t)d;
+        return n;
+    }
 };
 
 class Store {
@@ -73,6 +116,9 @@ public:
     void set_field(const std::string &key, const std::vector<int64_t> &dims, int ncomp,
                    const double *data);
     void set_vector(const std::string &key, int64_t count, int ncomp, const double *data);
+    // A computed RowMajor domain array to be filled in place by the caller; nullptr when the
+    // ordering requires a permutation (then use set_field).
+    double *create_field(const std::string &key, const std::vector<int64_t> &dims, int ncomp);
 
     void set_ordering(Ordering o) { ordering_ = o; }
     Ordering ordering() const { return ordering_; }

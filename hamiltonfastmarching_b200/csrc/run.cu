@@ -77,12 +77,10 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
         io.get_scalar(key, 0.0, 99);  // record as defaulted (message already printed)
         return def;
     }
-    int64_t cnt = 0;
     const RawElement &r = io.raw(key);
     if (r.dims.size() != 1 || r.dims[0] != n)
         throw Error(HFM_ERR_VALUE, "Field " + key + " must be a vector of " + std::to_string(n) + " entries");
-    (void)cnt;
-    return r.data;
+    return std::vector<double>(r.data.begin(), r.data.end());
 }
 
 void reject_unsupported(Store &io) {
@@ -166,20 +164,20 @@ std::vector<double> read_lifted_scalar(Store &io, const std::string &key, const 
     std::vector<double> out(N);
     Field f = io.get_field(key, depth, 1);
     if (depth == 0) {
-        std::fill(out.begin(), out.end(), f.data[0]);
+        std::fill(out.begin(), out.end(), f.ptr()[0]);
     } else if (depth == 3) {
         if (f.dims[0] != dims[0] || f.dims[1] != dims[1] || f.dims[2] != dims[2])
             throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
-        out = f.data;
+        out.assign(f.ptr(), f.ptr() + f.size());
     } else if (depth == 2) {
         if (f.dims[0] != dims[0] || f.dims[1] != dims[1])
             throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
         for (int64_t i = 0; i < (int64_t)dims[0] * dims[1]; ++i)
-            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.data[i];
+            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.ptr()[i];
     } else if (depth == 1) {
         if (f.dims[0] != dims[2]) throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
         for (int64_t i = 0; i < (int64_t)dims[0] * dims[1]; ++i)
-            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.data[t];
+            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.ptr()[t];
     } else {
         throw Error(HFM_ERR_VALUE, "Field " + key + " has incorrect depth.\n");
     }
@@ -190,21 +188,22 @@ std::vector<uint8_t> read_walls(Store &io, const Param &pm, bool lifted) {
     std::vector<uint8_t> w;
     if (!io.has_field("walls")) return w;
     const int64_t N = (int64_t)pm.dims[0] * pm.dims[1] * pm.dims[2];
-    std::vector<double> v;
-    if (lifted) {
-        v = read_lifted_scalar(io, "walls", pm.dims);
-    } else {
-        const std::vector<int64_t> dd = io.field_domain_dims("walls", 1);
-        Field f = io.get_field("walls", dd.empty() ? 0 : pm.ndim, 1);
-        if (f.constant()) v.assign(N, f.data[0]);
-        else {
-            for (int a = 0; a < pm.ndim; ++a)
-                if (f.dims[a] != pm.dims[a]) throw Error(HFM_ERR_VALUE, "Error : walls have inconsistent dims");
-            v = f.data;
-        }
-    }
     w.resize(N);
-    for (int64_t i = 0; i < N; ++i) w[i] = v[i] != 0.0;  // GetIntegralField<bool>: (bool)double
+    if (lifted) {
+        const std::vector<double> v = read_lifted_scalar(io, "walls", pm.dims);
+        for (int64_t i = 0; i < N; ++i) w[i] = v[i] != 0.0;  // GetIntegralField<bool>: (bool)double
+        return w;
+    }
+    const std::vector<int64_t> dd = io.field_domain_dims("walls", 1);
+    Field f = io.get_field("walls", dd.empty() ? 0 : pm.ndim, 1);
+    if (f.constant()) {
+        std::fill(w.begin(), w.end(), f.ptr()[0] != 0.0);
+        return w;
+    }
+    for (int a = 0; a < pm.ndim; ++a)
+        if (f.dims[a] != pm.dims[a]) throw Error(HFM_ERR_VALUE, "Error : walls have inconsistent dims");
+    const double *v = f.ptr();
+    for (int64_t i = 0; i < N; ++i) w[i] = v[i] != 0.0;
     return w;
 }
 
@@ -258,7 +257,12 @@ void setup_riemann(Store &io, int ndim, Param &pm, EulerProblem &p) {
             if (f.dims[a] != dims[a]) throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
     }
     p.metric_constant = f.constant();
-    p.metric = std::move(f.data);
+    if (f.view) {
+        p.metric_ptr = f.view;
+        p.metric_len = f.size();
+    } else {
+        p.metric = std::move(f.data);
+    }
 }
 
 void setup_isotropic2(Store &io, Param &pm, EulerProblem &p) {
@@ -282,8 +286,9 @@ void setup_isotropic2(Store &io, Param &pm, EulerProblem &p) {
     Field f = io.get_field(key, dd.empty() ? 0 : 2, 1);
     p.metric.resize(f.constant() ? 3 : N * 3);
     p.metric_constant = f.constant();
-    for (size_t i = 0; i < f.data.size(); ++i) {
-        const double c = (std::string(key) == "speed") ? 1.0 / f.data[i] : f.data[i];
+    const size_t nf = f.size();
+    for (size_t i = 0; i < nf; ++i) {
+        const double c = (std::string(key) == "speed") ? 1.0 / f.ptr()[i] : f.ptr()[i];
         p.metric[3 * i] = c * c;
         p.metric[3 * i + 1] = 0.0;
         p.metric[3 * i + 2] = c * c;
@@ -407,8 +412,16 @@ void run_model(Store &io, const std::string &model) {
             p.adjoint_weight.push_back(std::move(wts));
         }
     }
+    // the arrival times are downloaded straight into the output field when no reordering is needed
+    double *values_dst = export_values ? io.create_field("values", dims, 1) : nullptr;
+    p.h_values_out = values_dst;
     EulerResult r;
-    solve_eulerian(p, r);
+    try {
+        solve_eulerian(p, r);
+    } catch (...) {
+        if (values_dst) io.erase_field("values");
+        throw;
+    }
 
     // Outputs (Run_SetupSolver/Run_RunSolver/Run_ExportData, CommonStoppingCriteria::Finally)
     io.set_scalar("MaxStencilWidth", r.max_stencil_width);
@@ -425,7 +438,7 @@ void run_model(Store &io, const std::string &model) {
         m << "Fast marching solver completed in " << r.t_solve_ms * 1e-3 << " s.\n";
         io.msg(m.str());
     }
-    if (export_values) io.set_field("values", dims, 1, r.values.data());
+    if (export_values && !values_dst) io.set_field("values", dims, 1, r.values.data());
     if (export_active) {
         std::vector<double> a(r.active.size());
         for (size_t i = 0; i < a.size(); ++i) a[i] = (double)r.active[i];

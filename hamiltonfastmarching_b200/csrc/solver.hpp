@@ -25,6 +25,8 @@ struct EulerProblem {
 
     // RiemannPerCell: packed metric (xx,xy,yy[,xz,yz,zz]) RowMajor, one per cell or a single one.
     std::vector<double> metric;
+    const double *metric_ptr = nullptr;  // used instead of `metric` when set (host, not owned)
+    size_t metric_len = 0;
     bool metric_constant = false;
     bool dual = false;
     double h[3] = {1, 1, 1};
@@ -42,6 +44,7 @@ struct EulerProblem {
     const double *d_metric = nullptr;
     const uint8_t *d_walls = nullptr;
     double *d_values_out = nullptr;
+    double *h_values_out = nullptr;   // host destination of the arrival times instead of EulerResult::values
     std::vector<int64_t> seed_index;   // sorted, unique
     std::vector<double> seed_value;
 
