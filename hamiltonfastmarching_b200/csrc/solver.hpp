@@ -53,7 +53,7 @@ struct EulerProblem {
     std::vector<std::vector<int64_t>> adjoint_index;
     std::vector<std::vector<double>> adjoint_weight;
     bool want_stencils = false;        // export per-cell offsets/weights (RiemannPerCell)
-    int sweeps_per_tile = 16;          // local Jacobi sweeps before a tile re-queues itself
+    int sweeps_per_tile = 4;           // local Jacobi sweeps before a tile re-queues itself
     int max_rounds = 1 << 20;
     // Value-ordered scheduling: a round solves the tiles whose wake-up key is within a band above
     // the smallest key; the band adapts to keep [band_lo, band_hi] x (resident warps) tiles per round.
