@@ -9,6 +9,8 @@
 
 :func:`run` is the dictionary-in / dictionary-out convenience of the file-based interface
 (``JMM_CPPLibs/FileIO/FileIO.py:54-73``), with the file interface's default ordering ``RowMajor``.
+:func:`run_batch` solves many such dictionaries in one batched launch sequence
+(``hfm_run_batch``); each gets what :func:`run` would return for it alone.
 
 Everything runs through the C ABI of ``include/hfm_b200.h`` on the GPU; there is no CPU fallback.
 """
@@ -22,7 +24,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["HFMIO", "PyExp", "run", "version"]
+__all__ = ["HFMIO", "PyExp", "run", "run_batch", "run_ios", "version"]
 
 
 class PyExp(RuntimeError):
@@ -134,3 +136,41 @@ def run(params: Dict, arrayOrdering: str = "RowMajor", expected_model: str = Non
     io.set_dict(params)
     io.run(expected_model)
     return io.get_computed()
+
+
+def run_ios(ios, expected_model: str = None):
+    """Run several :class:`HFMIO` stores as one batch (``hfm_run_batch``).
+
+    Returns the list of per-store status codes (0 = success); the message of a failed store is
+    ``hfm_io_last_error`` of that store.
+    """
+    L = _lib.load()
+    n = len(ios)
+    handles = (ctypes.c_void_p * max(n, 1))(*[io._h for io in ios])
+    codes = (ctypes.c_int * max(n, 1))()
+    L.hfm_run_batch(handles, n, expected_model.encode() if expected_model else None, codes)
+    return [codes[i] for i in range(n)]
+
+
+def run_batch(params_list, arrayOrdering: str = "RowMajor", expected_model: str = None, raise_errors: bool = True):
+    """Solve a list of ``hfmIn`` dictionaries as one batch; returns the list of ``hfmOut``.
+
+    With ``raise_errors`` False a failed instance yields a :class:`PyExp` in its slot instead of
+    raising.
+    """
+    ios = []
+    for params in params_list:
+        io = HFMIO(arrayOrdering)
+        io.set_dict(params)
+        ios.append(io)
+    codes = run_ios(ios, expected_model)
+    out = []
+    for io, rc in zip(ios, codes):
+        if rc != _lib.HFM_OK:
+            e = PyExp(rc, io._L.hfm_io_last_error(io._h).decode())
+            if raise_errors:
+                raise e
+            out.append(e)
+        else:
+            out.append(io.get_computed())
+    return out

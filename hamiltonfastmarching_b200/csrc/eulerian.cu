@@ -85,9 +85,36 @@ __host__ __device__ __forceinline__ unsigned pack_off(int o0, int o1, int o2) {
 }
 __device__ __forceinline__ int off_c(unsigned code, int c) { return (int)(int8_t)((code >> (8 * c)) & 0xffu); }
 
+// One instance of a batch: its grid and where its tiles, cells and tables start in the batch's
+// global arrays. A single solve is a batch of one.
+struct Inst {
+    GridGeom g;
+    long long tile0;     // first global tile
+    long long cell0;     // first global cell (RowMajor values of the instance start here)
+    long long cls0;      // first class of its shared-stencil table
+    long long metric0;   // first metric row
+    double h[3];
+    int dual, metric_const, has_walls, pad;
+};
+
+// Instance holding global cell x (binary search over the increasing cell0 offsets).
+__device__ __forceinline__ int inst_of_cell(const Inst *inst, int n, long long x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (inst[mid].cell0 <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <typename Real>
 struct Dev {
-    GridGeom g;
+    const Inst *inst;         // [ninst]
+    int ninst;
+    const int *tile_inst;     // [ntile] instance of each global tile
+    long long ncells;         // total cells
+    long long ntile;          // total tiles
     long long ntc;            // tile-major cell count = ntile * 64
     Real *values;             // RowMajor
     unsigned *code;           // [ND][ntc] per-cell offsets + visibility/flags (per-cell stencils)
@@ -182,12 +209,14 @@ __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real 
 // neighbours from global memory). `side` receives, per symmetric difference, 1 if the -e
 // neighbour provided the candidate.
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-__device__ __forceinline__ Real solve_cell(const Dev<Real> &P, long long c, int x0, int x1, int x2, int tx0, int tx1,
-                                           int tx2, const Real *sv, unsigned *used, unsigned *side) {
+__device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1, int x2,
+                                           int tx0, int tx1, int tx2, const Real *sv, unsigned *used, unsigned *side) {
     constexpr int ND = NFWD + NSYM;
     using A = Arith<Real>;
     const Real INF = A::inf();
-    const GridGeom &g = P.g;
+    const GridGeom &g = I.g;
+    const Real *values = P.values + I.cell0;
+    const long long cls = I.cls0 + x2;
     Real v[ND], w[ND];
     Real m2 = 1;
     unsigned visw = 0;
@@ -209,16 +238,16 @@ __device__ __forceinline__ Real solve_cell(const Dev<Real> &P, long long c, int 
             if (l0 < (1u << g.tshift[0]) && l1 < (1u << g.tshift[1]) && l2 < (1u << g.tshift[2]))
                 return sv[((l0 << g.tshift[1] | l1) << g.tshift[2]) | l2];
         }
-        return __ldcg(P.values + g.lin(n0, n1, n2));
+        return __ldcg(values + g.lin(n0, n1, n2));
     };
 #pragma unroll
     for (int k = 0; k < ND; ++k) {
         int o0, o1, o2;
         bool vp, vm = false;
         if (SHARE) {
-            const int8_t *o = P.cls_off + ((long long)x2 * ND + k) * 3;
+            const int8_t *o = P.cls_off + (cls * ND + k) * 3;
             o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
-            w[k] = A::mul(__ldg(P.cls_w + (long long)x2 * ND + k), m2);
+            w[k] = A::mul(__ldg(P.cls_w + cls * ND + k), m2);
             if (k < NFWD) {
                 vp = (visw >> k) & 1u;
             } else {
@@ -316,10 +345,10 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
 
 // Cells of the warp's tile that the cell at (x0,x1,x2) reads through its visible stencil entries.
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-__device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, long long c, int x0, int x1, int x2,
-                                                           int tx0, int tx1, int tx2) {
+__device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, const Inst &I, long long c, int x0,
+                                                           int x1, int x2, int tx0, int tx1, int tx2) {
     constexpr int ND = NFWD + NSYM;
-    const GridGeom &g = P.g;
+    const GridGeom &g = I.g;
     unsigned long long m = 0;
     const unsigned visw = SHARE ? P.vis[c] : 0u;
 #pragma unroll
@@ -327,7 +356,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, l
         int o0, o1, o2;
         unsigned bits;
         if (SHARE) {
-            const int8_t *o = P.cls_off + ((long long)x2 * ND + k) * 3;
+            const int8_t *o = P.cls_off + ((I.cls0 + x2) * ND + k) * 3;
             o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
             bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
         } else {
@@ -358,9 +387,10 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, l
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves) {
-    const GridGeom &g = P.g;
+    const Inst &I = P.inst[P.tile_inst[T]];
+    const GridGeom &g = I.g;
     int t0, t1, t2;
-    g.tile_coords(T, t0, t1, t2);
+    g.tile_coords(T - I.tile0, t0, t1, t2);
     const int tx0 = t0 << g.tshift[0], tx1 = t1 << g.tshift[1], tx2 = t2 << g.tshift[2];
     unsigned long long dirty = 0;
     if (lane == 0) dirty = atomicExch(P.dirty + T, 0ull);
@@ -382,10 +412,10 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         bool fixed = true, dead = true;
         const long long c = (long long)T * 64 + l;
         if (valid) cell_flags<Real, SHARE>(P, c, fixed, dead);
-        gi[j] = valid ? g.lin(xs[j][0], xs[j][1], xs[j][2]) : 0;
+        gi[j] = valid ? I.cell0 + g.lin(xs[j][0], xs[j][1], xs[j][2]) : 0;
         cur[j] = (valid && !dead) ? __ldcg(P.values + gi[j]) : INF;
         upd[j] = valid && !dead && !fixed;
-        if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, SHARE>(P, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
+        if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, SHARE>(P, I, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
         todo[j] = upd[j] && ((dirty >> l) & 1ull);
         sv[l] = cur[j];
     }
@@ -397,7 +427,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         for (int j = 0; j < 2; ++j) {
             nv[j] = cur[j];
             if (todo[j]) {
-                nv[j] = solve_cell<Real, NFWD, NSYM, SHARE>(P, (long long)T * 64 + lane + 32 * j, xs[j][0], xs[j][1],
+                nv[j] = solve_cell<Real, NFWD, NSYM, SHARE>(P, I, (long long)T * 64 + lane + 32 * j, xs[j][0], xs[j][1],
                                                             xs[j][2], tx0, tx1, tx2, sv, nullptr, nullptr);
                 ++n_solves;
             }
@@ -549,34 +579,48 @@ __global__ void fill_kernel(Real *p, long long n, Real v) {
 
 // One thread per cell: Riemann Selling stencil, written tile-major for the solver and optionally
 // RowMajor for export. Non positive definite metrics set kErrSelling.
+// Global cell x of a batch -> its instance, coordinates and global tile-major index.
+struct CellRef {
+    int i;
+    int x0, x1, x2;
+    long long xl;   // cell index within the instance
+    long long c;    // global tile-major index
+};
+__device__ __forceinline__ CellRef cell_ref(const Inst *inst, int ninst, long long x) {
+    CellRef r;
+    r.i = inst_of_cell(inst, ninst, x);
+    const Inst &I = inst[r.i];
+    r.xl = x - I.cell0;
+    r.x2 = (int)(r.xl % I.g.dims[2]);
+    const long long q = r.xl / I.g.dims[2];
+    r.x1 = (int)(q % I.g.dims[1]);
+    r.x0 = (int)(q / I.g.dims[1]);
+    r.c = (I.tile0 + I.g.tile_of(r.x0, r.x1, r.x2)) * 64 + I.g.local_of(r.x0, r.x1, r.x2);
+    return r;
+}
+
 template <int D, typename Real>
-__global__ void riemann_stencil_kernel(GridGeom g, long long ntc, const double *metric, int metric_const, int dual,
-                                       double h0, double h1, double h2, unsigned *code, Real *weight,
-                                       int8_t *plain_off, double *plain_w, unsigned *status) {
+__global__ void riemann_stencil_kernel(Dev<Real> P, const double *metric, int8_t *plain_off, double *plain_w) {
     constexpr int NS = D * (D + 1) / 2, NK = D == 2 ? 3 : 6;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (x >= g.ncells) return;
-    const int x2 = (int)(x % g.dims[2]);
-    const long long r = x / g.dims[2];
-    const int x1 = (int)(r % g.dims[1]);
-    const int x0 = (int)(r / g.dims[1]);
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[R.i];
     double m[6];
-    const double *src = metric + (metric_const ? 0 : x * NS);
+    const double *src = metric + (I.metric0 + (I.metric_const ? 0 : R.xl)) * NS;
 #pragma unroll
     for (int k = 0; k < NS; ++k) m[k] = src[k];
-    const double h[3] = {h0, h1, h2};
     int off[6][3];
     double w[6];
-    if (!riemann_stencil<D>(m, dual != 0, h, off, w)) {
-        atomicOr(status, (unsigned)kErrSelling);
+    if (!riemann_stencil<D>(m, I.dual != 0, I.h, off, w)) {
+        atomicOr(P.status, (unsigned)kErrSelling);
 #pragma unroll
         for (int k = 0; k < NK; ++k) { w[k] = 0.0; off[k][0] = off[k][1] = off[k][2] = 0; }
     }
-    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-        code[k * ntc + c] = pack_off(off[k][0], off[k][1], off[k][2]);
-        weight[k * ntc + c] = (Real)w[k];
+        P.code[k * P.ntc + R.c] = pack_off(off[k][0], off[k][1], off[k][2]);
+        P.weight[k * P.ntc + R.c] = (Real)w[k];
         if (plain_off) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) plain_off[(x * NK + k) * 3 + a] = (int8_t)off[k][a];
@@ -586,42 +630,36 @@ __global__ void riemann_stencil_kernel(GridGeom g, long long ntc, const double *
 }
 
 // Largest L1 norm of a non-zero-weight offset whose target lies in the domain (MaxStencilWidth,
-// HamiltonFastMarching.hxx:36-45 over the reversed offsets of HFM_StencilRecompute.hxx:91-116).
+// HamiltonFastMarching.hxx:36-45 over the reversed offsets of HFM_StencilRecompute.hxx:91-116),
+// per instance.
 template <typename Real, int NSYM>
 __global__ void width_kernel(Dev<Real> P, unsigned *maxw) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const GridGeom &g = P.g;
-    if (x >= g.ncells) return;
-    const int x2 = (int)(x % g.dims[2]);
-    const long long r = x / g.dims[2];
-    const int x1 = (int)(r % g.dims[1]);
-    const int x0 = (int)(r / g.dims[1]);
-    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const GridGeom &g = P.inst[R.i].g;
     int best = 0;
 #pragma unroll
     for (int k = 0; k < NSYM; ++k) {
-        if (P.weight[k * P.ntc + c] == Real(0)) continue;
-        const unsigned cd = P.code[k * P.ntc + c];
+        if (P.weight[k * P.ntc + R.c] == Real(0)) continue;
+        const unsigned cd = P.code[k * P.ntc + R.c];
         const int o0 = off_c(cd, 0), o1 = off_c(cd, 1), o2 = off_c(cd, 2);
         const int l1 = abs(o0) + abs(o1) + abs(o2);
         for (int s = 1; s >= -1; s -= 2) {
-            int n0 = x0 + s * o0, n1 = x1 + s * o1, n2 = x2 + s * o2;
+            int n0 = R.x0 + s * o0, n1 = R.x1 + s * o1, n2 = R.x2 + s * o2;
             if (g.wrap(n0, n1, n2) && l1 > best) best = l1;
         }
     }
-    if (best) atomicMax(maxw, (unsigned)best);
+    if (best) atomicMax(maxw + R.i, (unsigned)best);
 }
 
 // Speed multiplier to the tile-major layout (shared stencils).
 template <typename Real>
-__global__ void mult_layout_kernel(GridGeom g, const double *mult_rm, Real *mult_tm) {
+__global__ void mult_layout_kernel(Dev<Real> P, const double *mult_rm) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (x >= g.ncells) return;
-    const int x2 = (int)(x % g.dims[2]);
-    const long long r = x / g.dims[2];
-    const int x1 = (int)(r % g.dims[1]);
-    const int x0 = (int)(r / g.dims[1]);
-    mult_tm[g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2)] = (Real)mult_rm[x];
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    P.mult[R.c] = (Real)mult_rm[x];
 }
 
 // --------------------------------------------------------------------------------------------
@@ -635,6 +673,7 @@ __global__ void wall_init_kernel(long long n, const uint8_t *walls, int *d) {
 }
 
 __global__ void wall_scan_kernel(GridGeom g, int axis, int *d) {
+    // d points at the instance's first cell
     const long long nl = g.ncells / g.dims[axis];
     const long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (line >= nl) return;
@@ -660,9 +699,12 @@ __global__ void wall_scan_kernel(GridGeom g, int axis, int *d) {
         }
 }
 
-__global__ void wall_cap_kernel(long long n, const int *d, int cap, int8_t *wd) {
+template <typename Real>
+__global__ void wall_cap_kernel(Dev<Real> P, const int *d, const unsigned *cap, int8_t *wd) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (x < n) wd[x] = d[x] <= cap ? (int8_t)d[x] : (int8_t)127;
+    if (x >= P.ncells) return;
+    const int i = inst_of_cell(P.inst, P.ninst, x);
+    wd[x] = d[x] <= (int)cap[i] ? (int8_t)d[x] : (int8_t)127;
 }
 
 // Visible(base, v, sum) of WallObstructionTest.h:95-150: a discrete walk from `base` toward `sum`.
@@ -715,14 +757,17 @@ __device__ bool wall_visible(const GridGeom &g, const int8_t *wd, int b0, int b1
 // difference has non-zero weight, y lies in the domain, and Visible(y, -s e, x) holds
 // (ConditionalUpdate, HamiltonFastMarching.hxx:136-154). Also marks padding cells dead.
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-__global__ void visibility_kernel(Dev<Real> P, const int8_t *wd, const uint8_t *cls_enabled) {
+__global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8_t *cls_enabled) {
     constexpr int ND = NFWD + NSYM;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const GridGeom &g = P.g;
     if (c >= P.ntc) return;
     const int T = (int)(c >> 6), l = (int)(c & 63);
+    const Inst &I = P.inst[P.tile_inst[T]];
+    const GridGeom &g = I.g;
+    const int8_t *wd = (wd_all && I.has_walls) ? wd_all + I.cell0 : nullptr;
+    const long long cls = I.cls0;
     int t0, t1, t2, l0, l1, l2;
-    g.tile_coords(T, t0, t1, t2);
+    g.tile_coords(T - I.tile0, t0, t1, t2);
     g.local_coords(l, l0, l1, l2);
     const int x0 = (t0 << g.tshift[0]) + l0, x1 = (t1 << g.tshift[1]) + l1, x2 = (t2 << g.tshift[2]) + l2;
     if (x0 >= g.dims[0] || x1 >= g.dims[1] || x2 >= g.dims[2]) {
@@ -736,9 +781,9 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd, const uint8_t *
         int o[3];
         bool nonzero;
         if (SHARE) {
-            const int8_t *oo = P.cls_off + ((long long)x2 * ND + k) * 3;
+            const int8_t *oo = P.cls_off + ((cls + x2) * ND + k) * 3;
             o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
-            nonzero = P.cls_w[(long long)x2 * ND + k] != Real(0);
+            nonzero = P.cls_w[(cls + x2) * ND + k] != Real(0);
         } else {
             const unsigned cd = P.code[k * P.ntc + c];
             o[0] = off_c(cd, 0); o[1] = off_c(cd, 1); o[2] = off_c(cd, 2);
@@ -749,7 +794,7 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd, const uint8_t *
             const int s = si == 0 ? 1 : -1;
             const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
             if (!nonzero) continue;
-            if (SHARE && !cls_enabled[(long long)x2 * (NFWD + 2 * NSYM) + slot]) continue;
+            if (SHARE && !cls_enabled[(cls + x2) * (NFWD + 2 * NSYM) + slot]) continue;
             int y0 = x0 + s * o[0], y1 = x1 + s * o[1], y2 = x2 + s * o[2];
             if (!g.wrap(y0, y1, y2)) continue;
             if (wd && !wall_visible(g, wd, y0, y1, y2, -s * o[0], -s * o[1], -s * o[2], x0, x1, x2)) continue;
@@ -763,15 +808,11 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd, const uint8_t *
 
 template <typename Real, bool SHARE>
 __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *val, int n) {
+    // idx: global cell indices
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const GridGeom &g = P.g;
     const long long x = idx[i];
-    const int x2 = (int)(x % g.dims[2]);
-    const long long r = x / g.dims[2];
-    const int x1 = (int)(r % g.dims[1]);
-    const int x0 = (int)(r / g.dims[1]);
-    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    const long long c = cell_ref(P.inst, P.ninst, x).c;
     P.values[x] = (Real)val[i];
     if (SHARE) P.vis[c] |= kShFixed;
     else P.code[c] |= kFixed;
@@ -791,15 +832,16 @@ __global__ void __launch_bounds__(kDepWarps * 32)
     __shared__ unsigned long long dmasks[kDepWarps][kDepCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long D = (long long)blockIdx.x * kDepWarps + warp;
-    if (D >= P.g.ntile) return;
+    if (D >= P.ntile) return;
     int *K = keys[warp];
     unsigned long long *M = masks[warp];
     unsigned long long *DM = dmasks[warp];
     for (int i = lane; i < kDepCap; i += 32) { K[i] = -1; M[i] = 0ull; DM[i] = 0ull; }
     __syncwarp();
-    const GridGeom &g = P.g;
+    const Inst &I = P.inst[P.tile_inst[D]];
+    const GridGeom &g = I.g;
     int t0, t1, t2;
-    g.tile_coords(D, t0, t1, t2);
+    g.tile_coords(D - I.tile0, t0, t1, t2);
     bool overflow = false;
     for (int j = 0; j < 2; ++j) {
         const int l = lane + 32 * j;
@@ -813,7 +855,7 @@ __global__ void __launch_bounds__(kDepWarps * 32)
             int o[3];
             unsigned bits;
             if (SHARE) {
-                const int8_t *oo = P.cls_off + ((long long)x2 * ND + k) * 3;
+                const int8_t *oo = P.cls_off + ((I.cls0 + x2) * ND + k) * 3;
                 o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
                 bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
             } else {
@@ -826,7 +868,7 @@ __global__ void __launch_bounds__(kDepWarps * 32)
                 const int s = si == 0 ? 1 : -1;
                 int y0 = x0 + s * o[0], y1 = x1 + s * o[1], y2 = x2 + s * o[2];
                 g.wrap(y0, y1, y2);
-                const int T = (int)g.tile_of(y0, y1, y2);
+                const int T = (int)(I.tile0 + g.tile_of(y0, y1, y2));
                 if (T == D) continue;
                 const int b = g.local_of(y0, y1, y2);
                 unsigned h = ((unsigned)T * 2654435761u) & (kDepCap - 1);
@@ -883,12 +925,15 @@ __global__ void dep_scatter_kernel(long long n, const int *src, const int *dst, 
 // Post-processing.
 
 template <typename Real>
-__global__ void count_finite_kernel(const Real *v, long long n, unsigned long long *out) {
-    unsigned long long cnt = 0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        cnt += (v[i] < Arith<Real>::inf()) ? 1ull : 0ull;
-    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+// Reached cells per instance (the reference's nAccepted).
+__global__ void count_finite_kernel(Dev<Real> P, unsigned long long *out) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool in = x < P.ncells;
+    const int i = in ? inst_of_cell(P.inst, P.ninst, x) : -1;
+    const bool fin = in && P.values[x] < Arith<Real>::inf();
+    const unsigned same = __match_any_sync(0xffffffffu, i);
+    const unsigned cnt = __popc(__ballot_sync(0xffffffffu, fin) & same);
+    if (in && cnt && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(out + i, (unsigned long long)cnt);
 }
 
 // activeNeighs bitsets in the reference layout (EulerianStencil.h:35-49): forward difference k
@@ -899,27 +944,26 @@ template <typename Real, int NFWD, int NSYM, bool SHARE>
 __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
     constexpr int ND = NFWD + NSYM;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const GridGeom &g = P.g;
-    if (x >= g.ncells) return;
-    const int x2 = (int)(x % g.dims[2]);
-    const long long r = x / g.dims[2];
-    const int x1 = (int)(r % g.dims[1]);
-    const int x0 = (int)(r / g.dims[1]);
-    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[R.i];
+    const int x0 = R.x0, x1 = R.x1, x2 = R.x2;
+    const long long c = R.c;
+    const long long cls = I.cls0 + x2;
     bool fixed, dead;
     cell_flags<Real, SHARE>(P, c, fixed, dead);
     unsigned long long bits = 0;
     if (!fixed && !dead) {
         unsigned used = 0, side = 0;
-        solve_cell<Real, NFWD, NSYM, SHARE>(P, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+        solve_cell<Real, NFWD, NSYM, SHARE>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
         for (int k = 0; k < ND; ++k) {
             if (!((used >> k) & 1u)) continue;
             if (k < NFWD) {
                 bits |= 1ull << k;
                 if (SHARE) {
-                    const int8_t *ok = P.cls_off + ((long long)x2 * ND + k) * 3;
+                    const int8_t *ok = P.cls_off + (cls * ND + k) * 3;
                     for (int k2 = 0; k2 < NFWD; ++k2) {
-                        const int8_t *o2 = P.cls_off + ((long long)x2 * ND + k2) * 3;
+                        const int8_t *o2 = P.cls_off + (cls * ND + k2) * 3;
                         if (o2[0] == ok[0] && o2[1] == ok[1] && o2[2] == ok[2]) bits |= 1ull << k2;
                     }
                 }
@@ -978,17 +1022,19 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
 
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
+    // the adjoint runs on a batch of one instance
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const GridGeom &g = P.g;
+    const Inst &I = P.inst[0];
+    const GridGeom &g = I.g;
     const long long N = g.ncells;
     if (x >= N) return;
     const int x2 = (int)(x % g.dims[2]);
     const long long r = x / g.dims[2];
     const int x1 = (int)(r % g.dims[1]);
     const int x0 = (int)(r / g.dims[1]);
-    const long long c = g.tile_of(x0, x1, x2) * 64 + g.local_of(x0, x1, x2);
+    const long long c = (I.tile0 + g.tile_of(x0, x1, x2)) * 64 + g.local_of(x0, x1, x2);
     bool fixed, dead;
     cell_flags<Real, SHARE>(P, c, fixed, dead);
     const double u = (double)P.values[x];
@@ -996,7 +1042,7 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
     var[x] = 0.0;
     if (fixed || dead || !(u < Arith<double>::inf())) return;
     unsigned used = 0, side = 0;
-    solve_cell<Real, NFWD, NSYM, SHARE>(P, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+    solve_cell<Real, NFWD, NSYM, SHARE>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
     double m = 1.0;
     if (SHARE) m = (double)P.mult[c];
     double ws = 0.0, v = 0.0;
@@ -1007,9 +1053,9 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
         int o0, o1, o2;
         double wb;
         if (SHARE) {
-            const int8_t *o = P.cls_off + ((long long)x2 * ND + k) * 3;
+            const int8_t *o = P.cls_off + ((I.cls0 + x2) * ND + k) * 3;
             o0 = o[0]; o1 = o[1]; o2 = o[2];
-            wb = A::mul((double)P.cls_w[(long long)x2 * ND + k], A::mul(m, m));
+            wb = A::mul((double)P.cls_w[(I.cls0 + x2) * ND + k], A::mul(m, m));
         } else {
             const unsigned cd = P.code[k * P.ntc + c];
             o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
@@ -1022,7 +1068,7 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
             else if (SHARE) {
                 for (int k2 = 0; k2 < NFWD; ++k2) {
                     if (!((used >> k2) & 1u)) continue;
-                    const int8_t *o2p = P.cls_off + ((long long)x2 * ND + k2) * 3;
+                    const int8_t *o2p = P.cls_off + ((I.cls0 + x2) * ND + k2) * 3;
                     if (o2p[0] == o0 && o2p[1] == o1 && o2p[2] == o2) { act = 1; break; }
                 }
             }
@@ -1146,11 +1192,10 @@ __global__ void adjoint_kernel(AdjDev A) {
 }
 
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-void run_adjoint(const Dev<Real> &P, const EulerProblem &p, EulerResult &res, DeviceBuffer<unsigned> &status,
-                 cudaStream_t s) {
+void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
+                 DeviceBuffer<unsigned> &status, cudaStream_t s) {
     constexpr int ND = NFWD + NSYM;
     constexpr int NF = 2 * ND > 32 ? 32 : 2 * ND;
-    const long long N = P.g.ncells;
     if (N >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large for the adjoint");
     DeviceBuffer<int> fidx((size_t)NF * N), indeg0(N), indeg(N);
     DeviceBuffer<double> fw((size_t)NF * N), var(N), acc(N), sens(N);
@@ -1236,35 +1281,78 @@ void run_adjoint(const Dev<Real> &P, const EulerProblem &p, EulerResult &res, De
 }
 
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-void run_impl(const EulerProblem &p, EulerResult &res) {
+void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
     constexpr int ND = NFWD + NSYM;
+    constexpr int NB = NFWD + 2 * NSYM;
     const auto wall_t0 = std::chrono::steady_clock::now();
     cudaStream_t s = current_stream();
-    const GridGeom g = make_geom(p.ndim, p.dims, p.periodic);
-    const long long N = g.ncells, ntc = g.ntile * 64;
-    if (g.ntile >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large");
+    const int ninst = (int)probs.size();
+    results.assign(ninst, EulerResult());
+    const EulerProblem &p0 = *probs[0];
+
+    // ---- batch layout: instance table, global tile space
+    std::vector<Inst> hinst(ninst);
+    long long ntile = 0, ncells = 0, nclass = 0, nmetric = 0;
+    bool any_walls = false, want_active = false, want_stencils = false;
+    for (int i = 0; i < ninst; ++i) {
+        const EulerProblem &p = *probs[i];
+        Inst &I = hinst[i];
+        std::memset(&I, 0, sizeof(I));
+        I.g = make_geom(p.ndim, p.dims, p.periodic);
+        I.tile0 = ntile;
+        I.cell0 = ncells;
+        I.cls0 = nclass;
+        I.metric0 = nmetric;
+        for (int a = 0; a < 3; ++a) I.h[a] = p.h[a];
+        I.dual = p.dual;
+        I.metric_const = p.metric_constant;
+        I.has_walls = (!p.walls.empty() || p.d_walls) ? 1 : 0;
+        ntile += I.g.ntile;
+        ncells += I.g.ncells;
+        nclass += SHARE ? p.nclass : 0;
+        if (!SHARE) nmetric += p.metric_constant ? 1 : I.g.ncells;
+        any_walls |= I.has_walls != 0;
+        want_active |= p.want_active;
+        want_stencils |= p.want_stencils;
+    }
+    if (ntile >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "batch too large");
+    if (ninst > 1)
+        for (const EulerProblem *q : probs)
+            if (!q->adjoint_index.empty()) throw Error(HFM_ERR_UNSUPPORTED, "the adjoint runs on single solves");
+    const long long N = ncells, ntc = ntile * 64, nt = ntile;
     Dev<Real> P{};
-    P.g = g;
+    P.ninst = ninst;
+    P.ncells = N;
+    P.ntile = nt;
     P.ntc = ntc;
-    HFM_TRACE("run_impl enter");
+    DeviceBuffer<Inst> dinst;
+    dinst.upload(hinst, s);
+    P.inst = dinst.get();
+    std::vector<int> htile_inst(nt);
+    for (int i = 0; i < ninst; ++i)
+        std::fill(htile_inst.begin() + hinst[i].tile0, htile_inst.begin() + hinst[i].tile0 + hinst[i].g.ntile, i);
+    DeviceBuffer<int> tile_inst;
+    tile_inst.upload(htile_inst, s);
+    P.tile_inst = tile_inst.get();
+    HFM_TRACE("batch layout");
     DeviceBuffer<unsigned> status(1);
     status.zero(s);
-    HFM_TRACE("status alloc");
     P.status = status.get();
     DeviceBuffer<Real> values(N);
     P.values = values.get();
-    launch(fill_kernel<Real>, nblocks(N, 256) > 4096 ? 4096 : nblocks(N, 256), 256, 0, s, values.get(), N, Arith<Real>::inf());
+    launch(fill_kernel<Real>, nblocks(N, 256) > 4096 ? 4096 : nblocks(N, 256), 256, 0, s, values.get(), N,
+           Arith<Real>::inf());
     EventTimer tm;
 
     // ---- stencils
     tm.start(s);
-    DeviceBuffer<unsigned> code, vis, maxw(1);
+    DeviceBuffer<unsigned> code, vis, maxw(ninst);
     DeviceBuffer<Real> weight, mult, cls_w;
     DeviceBuffer<int8_t> cls_off, plain_off;
     DeviceBuffer<uint8_t> cls_en;
     DeviceBuffer<double> metric, plain_w, mult_rm;
     maxw.zero(s);
-    int max_width = 0;
+    std::vector<unsigned> hmaxw(ninst, 0);
     if (!SHARE) {
         code.alloc(ND * ntc);
         code.zero(s);
@@ -1272,81 +1360,118 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         weight.zero(s);
         P.code = code.get();
         P.weight = weight.get();
-        const double *metric_ptr = p.d_metric;
-        if (!metric_ptr) {
-            if (p.metric_ptr) metric.upload(p.metric_ptr, p.metric_len, s);
-            else metric.upload(p.metric, s);
+        const int NS = p0.ndim * (p0.ndim + 1) / 2;
+        const double *metric_ptr = nullptr;
+        if (ninst == 1 && p0.d_metric) {
+            metric_ptr = p0.d_metric;
+        } else if (ninst == 1 && p0.metric_ptr) {
+            metric.upload(p0.metric_ptr, p0.metric_len, s);
+            metric_ptr = metric.get();
+        } else {
+            metric.alloc((size_t)nmetric * NS);
+            for (int i = 0; i < ninst; ++i) {
+                const EulerProblem &p = *probs[i];
+                const size_t rows = p.metric_constant ? 1 : (size_t)hinst[i].g.ncells;
+                const size_t bytes = rows * NS * sizeof(double);
+                double *dst = metric.get() + hinst[i].metric0 * NS;
+                if (p.d_metric) HFM_CUDA(cudaMemcpyAsync(dst, p.d_metric, bytes, cudaMemcpyDeviceToDevice, s));
+                else HFM_CUDA(cudaMemcpyAsync(dst, p.metric_ptr ? p.metric_ptr : p.metric.data(), bytes,
+                                              cudaMemcpyHostToDevice, s));
+            }
             metric_ptr = metric.get();
         }
-        if (p.want_stencils) {
+        if (want_stencils) {
             plain_off.alloc(N * ND * 3);
             plain_w.alloc(N * ND);
         }
-        if (p.ndim == 2)
-            launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, 
-                g, ntc, metric_ptr, p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
-                plain_off.get(), plain_w.get(), status.get());
+        if (p0.ndim == 2)
+            launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr, plain_off.get(),
+                   plain_w.get());
         else
-            launch(riemann_stencil_kernel<3, Real>, nblocks(N, 128), 128, 0, s, 
-                g, ntc, metric_ptr, p.metric_constant, p.dual, p.h[0], p.h[1], p.h[2], code.get(), weight.get(),
-                plain_off.get(), plain_w.get(), status.get());
+            launch(riemann_stencil_kernel<3, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr, plain_off.get(),
+                   plain_w.get());
         HFM_CUDA(cudaGetLastError());
         HFM_TRACE("stencil kernel");
         launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, P, maxw.get());
-        unsigned mw = 0;
-        maxw.download(&mw, 1, s);
+        maxw.download(hmaxw.data(), ninst, s);
         HFM_CUDA(cudaStreamSynchronize(s));
-        max_width = (int)mw;
     } else {
-        std::vector<Real> w(p.cls_w.size());
-        for (size_t i = 0; i < w.size(); ++i) w[i] = (Real)p.cls_w[i];
-        cls_w.upload(w, s);
-        cls_off.upload(p.cls_off, s);
-        cls_en.upload(p.cls_enabled, s);
+        std::vector<Real> hw;
+        std::vector<int8_t> ho;
+        std::vector<uint8_t> he;
+        std::vector<double> hm(N);
+        for (int i = 0; i < ninst; ++i) {
+            const EulerProblem &p = *probs[i];
+            for (double w : p.cls_w) hw.push_back((Real)w);
+            ho.insert(ho.end(), p.cls_off.begin(), p.cls_off.end());
+            he.insert(he.end(), p.cls_enabled.begin(), p.cls_enabled.end());
+            std::copy(p.mult.begin(), p.mult.end(), hm.begin() + hinst[i].cell0);
+            // width over the class tables, from each class centre (HFM_StencilShare.hxx:152-175)
+            int mw = 0;
+            for (int cl = 0; cl < p.nclass; ++cl)
+                for (int k = 0; k < ND; ++k) {
+                    if (p.cls_w[cl * ND + k] == 0.0) continue;
+                    const int8_t *o = &p.cls_off[(cl * ND + k) * 3];
+                    for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
+                        const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
+                        if (!p.cls_enabled[cl * NB + slot]) continue;
+                        mw = std::max(mw, std::abs(o[0]) + std::abs(o[1]) + std::abs(o[2]));
+                    }
+                }
+            hmaxw[i] = (unsigned)mw;
+        }
+        cls_w.upload(hw, s);
+        cls_off.upload(ho, s);
+        cls_en.upload(he, s);
+        maxw.upload(hmaxw, s);
         P.cls_w = cls_w.get();
         P.cls_off = cls_off.get();
         mult.alloc(ntc);
         mult.zero(s);
         P.mult = mult.get();
-        mult_rm.upload(p.mult, s);
-        launch(mult_layout_kernel<Real>, nblocks(N, 256), 256, 0, s, g, mult_rm.get(), mult.get());
+        mult_rm.upload(hm, s);
+        launch(mult_layout_kernel<Real>, nblocks(N, 256), 256, 0, s, P, mult_rm.get());
         vis.alloc(ntc);
         vis.zero(s);
         P.vis = vis.get();
-        // width over the class tables, from each class centre (HFM_StencilShare.hxx:152-175)
-        const int NB = NFWD + 2 * NSYM;
-        for (int cl = 0; cl < p.nclass; ++cl)
-            for (int k = 0; k < ND; ++k) {
-                if (p.cls_w[cl * ND + k] == 0.0) continue;
-                const int8_t *o = &p.cls_off[(cl * ND + k) * 3];
-                for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
-                    const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
-                    if (!p.cls_enabled[cl * NB + slot]) continue;
-                    max_width = std::max(max_width, std::abs(o[0]) + std::abs(o[1]) + std::abs(o[2]));
-                }
-            }
     }
-    res.max_stencil_width = max_width;
+    for (int i = 0; i < ninst; ++i) results[i].max_stencil_width = (int)hmaxw[i];
 
     // ---- walls and visibility
     DeviceBuffer<uint8_t> walls;
     DeviceBuffer<int> wdist;
     DeviceBuffer<int8_t> wd8;
-    const uint8_t *walls_ptr = p.d_walls;
-    if (!walls_ptr && !p.walls.empty()) {
-        walls.upload(p.walls, s);
-        walls_ptr = walls.get();
-    }
-    if (walls_ptr) {
+    if (any_walls) {
+        const uint8_t *walls_ptr = nullptr;
+        if (ninst == 1 && p0.d_walls) {
+            walls_ptr = p0.d_walls;
+        } else {
+            walls.alloc(N);
+            walls.zero(s);
+            for (int i = 0; i < ninst; ++i) {
+                const EulerProblem &p = *probs[i];
+                if (p.d_walls)
+                    HFM_CUDA(cudaMemcpyAsync(walls.get() + hinst[i].cell0, p.d_walls, hinst[i].g.ncells,
+                                             cudaMemcpyDeviceToDevice, s));
+                else if (!p.walls.empty())
+                    HFM_CUDA(cudaMemcpyAsync(walls.get() + hinst[i].cell0, p.walls.data(), hinst[i].g.ncells,
+                                             cudaMemcpyHostToDevice, s));
+            }
+            walls_ptr = walls.get();
+        }
         wdist.alloc(N);
         wd8.alloc(N);
         launch(wall_init_kernel, nblocks(N, 256), 256, 0, s, N, walls_ptr, wdist.get());
-        for (int a = 0; a < 3; ++a) {
-            if (g.dims[a] == 1) continue;
-            const long long nl = N / g.dims[a];
-            launch(wall_scan_kernel, nblocks(nl, 128), 128, 0, s, g, a, wdist.get());
+        for (int i = 0; i < ninst; ++i) {
+            if (!hinst[i].has_walls) continue;
+            const GridGeom &g = hinst[i].g;
+            for (int a = 0; a < 3; ++a) {
+                if (g.dims[a] == 1) continue;
+                const long long nl = g.ncells / g.dims[a];
+                launch(wall_scan_kernel, nblocks(nl, 128), 128, 0, s, g, a, wdist.get() + hinst[i].cell0);
+            }
         }
-        launch(wall_cap_kernel, nblocks(N, 256), 256, 0, s, N, wdist.get(), max_width, wd8.get());
+        launch(wall_cap_kernel<Real>, nblocks(N, 256), 256, 0, s, P, wdist.get(), maxw.get(), wd8.get());
         HFM_CUDA(cudaGetLastError());
     }
     HFM_TRACE("walls");
@@ -1355,40 +1480,65 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
     wdist.release();
     HFM_TRACE("visibility");
 
-    // ---- seeds
-    const int ns = (int)p.seed_index.size();
+    // ---- seeds (global cell indices) and their tiles
+    std::vector<long long> hsi;
+    std::vector<double> hsv;
+    std::vector<int> st;
+    std::vector<unsigned long long> sm;
+    for (int i = 0; i < ninst; ++i) {
+        const EulerProblem &p = *probs[i];
+        const GridGeom &g = hinst[i].g;
+        for (size_t k = 0; k < p.seed_index.size(); ++k) {
+            const long long x = p.seed_index[k];
+            hsi.push_back(hinst[i].cell0 + x);
+            hsv.push_back(p.seed_value[k]);
+            const int x2 = (int)(x % g.dims[2]);
+            const long long rr = x / g.dims[2];
+            const int x1 = (int)(rr % g.dims[1]), x0 = (int)(rr / g.dims[1]);
+            const int T = (int)(hinst[i].tile0 + g.tile_of(x0, x1, x2));
+            const int b = g.local_of(x0, x1, x2);
+            if (st.empty() || st.back() != T) {
+                auto it = std::find(st.begin(), st.end(), T);
+                if (it == st.end()) { st.push_back(T); sm.push_back(1ull << b); continue; }
+                sm[it - st.begin()] |= 1ull << b;
+            } else {
+                sm.back() |= 1ull << b;
+            }
+        }
+    }
+    const int ns = (int)hsi.size();
     DeviceBuffer<long long> sidx;
     DeviceBuffer<double> sval;
     if (ns) {
-        std::vector<long long> si(p.seed_index.begin(), p.seed_index.end());
-        sidx.upload(si, s);
-        sval.upload(p.seed_value, s);
+        sidx.upload(hsi, s);
+        sval.upload(hsv, s);
         launch(seeds_kernel<Real, SHARE>, nblocks(ns, 128), 128, 0, s, P, sidx.get(), sval.get(), ns);
     }
-
-    // ---- tile dependency graph (reverse CSR)
-    const long long nt = g.ntile;
     HFM_TRACE("seeds");
+
+    // ---- tile dependency graph (reverse CSR over the global tile space)
     DeviceBuffer<unsigned> dcnt(nt);
-    launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, 
-        P, 0, dcnt.get(), nullptr, nullptr, nullptr, nullptr, nullptr);
+    launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 0, dcnt.get(),
+           nullptr, nullptr, nullptr, nullptr, nullptr);
     HFM_CUDA(cudaGetLastError());
     DeviceBuffer<long long> doff(nt + 1), rptr(nt + 1);
+    std::vector<unsigned> hc(nt);
+    dcnt.download(hc.data(), nt, s);
+    HFM_CUDA(cudaStreamSynchronize(s));
+    std::vector<long long> ho(nt + 1, 0);
+    long long tot = 0;
+    for (long long t = 0; t < nt; ++t) { ho[t] = tot; tot += hc[t]; }
+    ho[nt] = tot;
+    doff.upload(ho, s);
+    const long long nE = tot;
+    DeviceBuffer<int> rtile(nE);
+    DeviceBuffer<unsigned long long> rmask(nE), rdmask(nE);
     {
-        std::vector<unsigned> hc(nt);
-        dcnt.download(hc.data(), nt, s);
-        HFM_CUDA(cudaStreamSynchronize(s));
-        std::vector<long long> ho(nt + 1, 0);
-        long long tot = 0;
-        for (long long t = 0; t < nt; ++t) { ho[t] = tot; tot += hc[t]; }
-        ho[nt] = tot;
-        doff.upload(ho, s);
-        const long long nE = tot;
         DeviceBuffer<int> esrc(nE), edst(nE);
         DeviceBuffer<unsigned long long> emsk(nE), edmsk(nE);
         if (nE)
-            launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s,
-                   P, 1, nullptr, doff.get(), esrc.get(), edst.get(), emsk.get(), edmsk.get());
+            launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 1, nullptr,
+                   doff.get(), esrc.get(), edst.get(), emsk.get(), edmsk.get());
         DeviceBuffer<unsigned> rcnt(nt), cursor(nt);
         rcnt.zero(s);
         cursor.zero(s);
@@ -1401,179 +1551,187 @@ void run_impl(const EulerProblem &p, EulerResult &res) {
         for (long long t = 0; t < nt; ++t) { hrp[t] = tot; tot += hr[t]; }
         hrp[nt] = tot;
         rptr.upload(hrp, s);
-        P.dep_ptr = rptr.get();
-        // reverse arrays live until the end of the solve
-        DeviceBuffer<int> rtile(nE);
-        DeviceBuffer<unsigned long long> rmask(nE), rdmask(nE);
         if (nE)
             launch(dep_scatter_kernel, nblocks(nE, 256), 256, 0, s, nE, esrc.get(), edst.get(), emsk.get(),
                    edmsk.get(), rptr.get(), cursor.get(), rtile.get(), rmask.get(), rdmask.get());
         HFM_CUDA(cudaGetLastError());
-        HFM_TRACE("deps");
-        P.dep_tile = rtile.get();
-        P.dep_mask = rmask.get();
-        P.dep_dmask = rdmask.get();
-        DeviceBuffer<unsigned long long> dirty(nt), key(nt), rstat(32);
-        dirty.zero(s);
-        P.dirty = dirty.get();
-        launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, key.get(), nt, 0x7ff0000000000000ull);
-        {
-            unsigned long long h[32];
-            for (int i = 0; i < 8; ++i) { h[4 * i] = 0x7ff0000000000000ull; h[4 * i + 1] = 0; h[4 * i + 2] = 0; h[4 * i + 3] = 0; }
-            rstat.upload(h, 32, s);
-        }
-        P.key = key.get();
-        P.rstat = rstat.get();
-        DeviceBuffer<unsigned long long> maxval(nt);
-        launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, maxval.get(), nt, 0x7ff0000000000000ull);
-        P.maxval = maxval.get();
-        res.t_stencil_ms = tm.stop(s);
-        check_status(status, "stencil");
+    }
+    HFM_TRACE("deps");
+    P.dep_ptr = rptr.get();
+    P.dep_tile = rtile.get();
+    P.dep_mask = rmask.get();
+    P.dep_dmask = rdmask.get();
+    DeviceBuffer<unsigned long long> dirty(nt), key(nt), rstat(32), maxval(nt);
+    dirty.zero(s);
+    P.dirty = dirty.get();
+    launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, key.get(), nt, 0x7ff0000000000000ull);
+    launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, maxval.get(), nt, 0x7ff0000000000000ull);
+    {
+        unsigned long long h[32];
+        for (int i = 0; i < 8; ++i) { h[4 * i] = 0x7ff0000000000000ull; h[4 * i + 1] = 0; h[4 * i + 2] = 0; h[4 * i + 3] = 0; }
+        rstat.upload(h, 32, s);
+    }
+    P.key = key.get();
+    P.rstat = rstat.get();
+    P.maxval = maxval.get();
+    const float t_stencil = tm.stop(s);
+    check_status(status, "stencil");
 
-        // ---- solve
-        DeviceBuffer<int> lists(3 * nt);
-        DeviceBuffer<unsigned> counters(16), flags(3 * nt);
-        counters.zero(s);
-        flags.zero(s);
-        DeviceBuffer<unsigned long long> stats(4);
-        stats.zero(s);
-        for (int i = 0; i < 3; ++i) {
-            P.list[i] = lists.get() + i * nt;
-            P.flag[i] = flags.get() + i * nt;
-            P.count[i] = counters.get() + i;
-            P.claim[i] = counters.get() + 3 + i;
-        }
-        P.bar_count = counters.get() + 6;
-        P.bar_gen = counters.get() + 7;
-        P.stats = stats.get();
-        P.max_rounds = p.max_rounds;
-        P.sweeps = p.sweeps_per_tile;
-        // seed tiles and the cells they hold
-        std::vector<int> st;
-        std::vector<unsigned long long> sm;
-        for (int i = 0; i < ns; ++i) {
-            const long long x = p.seed_index[i];
-            const int x2 = (int)(x % g.dims[2]);
-            const long long rr = x / g.dims[2];
-            const int x1 = (int)(rr % g.dims[1]), x0 = (int)(rr / g.dims[1]);
-            const int T = (int)g.tile_of(x0, x1, x2);
-            const int b = g.local_of(x0, x1, x2);
-            auto it = std::find(st.begin(), st.end(), T);
-            if (it == st.end()) { st.push_back(T); sm.push_back(1ull << b); }
-            else sm[it - st.begin()] |= 1ull << b;
-        }
-        DeviceBuffer<int> stile;
-        DeviceBuffer<unsigned long long> smask;
-        tm.start(s);
-        if (!st.empty()) {
-            stile.upload(st, s);
-            smask.upload(sm, s);
-            launch(init_lists_kernel<Real>, nblocks((long long)st.size() * 32, 128), 128, 0, s, P, stile.get(), smask.get(),
-                                                                                             (int)st.size());
-            HFM_CUDA(cudaGetLastError());
-            HFM_TRACE("init lists");
-            int dev = 0, nsm = 0, per_sm = 0;
-            HFM_CUDA(cudaGetDevice(&dev));
-            HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-            HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_kernel<Real, NFWD, NSYM, SHARE>,
-                                                                   kWarpsPerCta * 32, 0));
-            if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
-            const int grid = nsm * per_sm;
-            const double nwarps = (double)grid * kWarpsPerCta;
-            P.order_lo = p.ordered ? (unsigned)std::max(1.0, p.band_lo * nwarps) : 0u;
-            P.order_hi = p.ordered ? (unsigned)std::max(2.0, p.band_hi * nwarps) : 0u;
-            void *args[] = {&P};
-            count_launch();
-            HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, SHARE>, dim3(grid),
-                                                 dim3(kWarpsPerCta * 32), args, 0, s));
-        }
-        HFM_TRACE("fim kernel");
-        res.t_solve_ms = tm.stop(s);
-        check_status(status, "solver");
-        unsigned long long hs[4] = {0, 0, 0, 0};
-        stats.download(hs, 4, s);
-        DeviceBuffer<unsigned long long> nacc(1);
-        nacc.zero(s);
-        launch(count_finite_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 2048), 256, 0, s, values.get(), N, nacc.get());
-        unsigned long long hn = 0;
-        nacc.download(&hn, 1, s);
+    // ---- solve
+    DeviceBuffer<int> lists(3 * nt);
+    DeviceBuffer<unsigned> counters(16), flags(3 * nt);
+    counters.zero(s);
+    flags.zero(s);
+    DeviceBuffer<unsigned long long> stats(4);
+    stats.zero(s);
+    for (int i = 0; i < 3; ++i) {
+        P.list[i] = lists.get() + i * nt;
+        P.flag[i] = flags.get() + i * nt;
+        P.count[i] = counters.get() + i;
+        P.claim[i] = counters.get() + 3 + i;
+    }
+    P.bar_count = counters.get() + 6;
+    P.bar_gen = counters.get() + 7;
+    P.stats = stats.get();
+    P.max_rounds = p0.max_rounds;
+    P.sweeps = p0.sweeps_per_tile;
+    DeviceBuffer<int> stile;
+    DeviceBuffer<unsigned long long> smask;
+    tm.start(s);
+    if (!st.empty()) {
+        stile.upload(st, s);
+        smask.upload(sm, s);
+        launch(init_lists_kernel<Real>, nblocks((long long)st.size() * 32, 128), 128, 0, s, P, stile.get(),
+               smask.get(), (int)st.size());
+        HFM_CUDA(cudaGetLastError());
+        HFM_TRACE("init lists");
+        int dev = 0, nsm = 0, per_sm = 0;
+        HFM_CUDA(cudaGetDevice(&dev));
+        HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_kernel<Real, NFWD, NSYM, SHARE>,
+                                                               kWarpsPerCta * 32, 0));
+        if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
+        const int grid = nsm * per_sm;
+        const double nwarps = (double)grid * kWarpsPerCta;
+        // Keys are arrival times of one instance: the band ordering is used for single solves only.
+        const bool ordered = p0.ordered && ninst == 1;
+        P.order_lo = ordered ? (unsigned)std::max(1.0, p0.band_lo * nwarps) : 0u;
+        P.order_hi = ordered ? (unsigned)std::max(2.0, p0.band_hi * nwarps) : 0u;
+        void *args[] = {&P};
+        count_launch();
+        HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, SHARE>, dim3(grid),
+                                             dim3(kWarpsPerCta * 32), args, 0, s));
+    }
+    HFM_TRACE("fim kernel");
+    const float t_solve = tm.stop(s);
+    check_status(status, "solver");
+    unsigned long long hs[4] = {0, 0, 0, 0};
+    stats.download(hs, 4, s);
+    DeviceBuffer<unsigned long long> nacc(ninst);
+    nacc.zero(s);
+    launch(count_finite_kernel<Real>, nblocks(N, 256), 256, 0, s, P, nacc.get());
+    std::vector<unsigned long long> hn(ninst);
+    nacc.download(hn.data(), ninst, s);
+
+    // ---- outputs per instance
+    DeviceBuffer<double> vd;
+    if (!std::is_same<Real, double>::value) {
+        vd.alloc(N);
+        launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), vd.get(), N);
+    }
+    const double *vsrc = std::is_same<Real, double>::value ? reinterpret_cast<const double *>(values.get()) : vd.get();
+    DeviceBuffer<unsigned long long> act;
+    if (want_active) {
+        act.alloc(N);
+        launch(active_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, act.get());
+    }
+    for (int i = 0; i < ninst; ++i) {
+        const EulerProblem &p = *probs[i];
+        EulerResult &res = results[i];
+        const long long n = hinst[i].g.ncells, off = hinst[i].cell0;
         if (p.d_values_out) {
-            if (std::is_same<Real, double>::value)
-                HFM_CUDA(cudaMemcpyAsync(p.d_values_out, values.get(), N * sizeof(double), cudaMemcpyDeviceToDevice, s));
-            else
-                launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), p.d_values_out, N);
-            HFM_CUDA(cudaStreamSynchronize(s));
-        } else if (std::is_same<Real, double>::value) {
-            double *dst = p.h_values_out;
-            if (!dst) {
-                res.values.resize(N);
-                dst = res.values.data();
-            }
-            values.download(reinterpret_cast<Real *>(dst), N, s);
+            HFM_CUDA(cudaMemcpyAsync(p.d_values_out, vsrc + off, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         } else {
             double *dst = p.h_values_out;
             if (!dst) {
-                res.values.resize(N);
+                res.values.resize(n);
                 dst = res.values.data();
             }
-            DeviceBuffer<double> vd(N);
-            launch(to_double_kernel<Real>, std::min<unsigned>(nblocks(N, 256), 4096), 256, 0, s, values.get(), vd.get(), N);
-            vd.download(dst, N, s);
-            HFM_CUDA(cudaStreamSynchronize(s));
+            HFM_CUDA(cudaMemcpyAsync(dst, vsrc + off, n * sizeof(double), cudaMemcpyDeviceToHost, s));
         }
         if (p.want_active) {
-            DeviceBuffer<unsigned long long> act(N);
-            launch(active_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, act.get());
-            res.active.resize(N);
-            act.download(reinterpret_cast<unsigned long long *>(res.active.data()), N, s);
-        }
-        if (!p.adjoint_index.empty()) {
-            tm.start(s);
-            run_adjoint<Real, NFWD, NSYM, SHARE>(P, p, res, status, s);
-            res.t_adjoint_ms = tm.stop(s);
+            res.active.resize(n);
+            HFM_CUDA(cudaMemcpyAsync(res.active.data(), act.get() + off, n * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s));
         }
         if (p.want_stencils && !SHARE) {
-            res.stencil_off.resize(N * ND * 3);
-            res.stencil_w.resize(N * ND);
-            plain_off.download(res.stencil_off.data(), N * ND * 3, s);
-            plain_w.download(res.stencil_w.data(), N * ND, s);
+            res.stencil_off.resize(n * ND * 3);
+            res.stencil_w.resize(n * ND);
+            HFM_CUDA(cudaMemcpyAsync(res.stencil_off.data(), plain_off.get() + off * ND * 3, n * ND * 3,
+                                     cudaMemcpyDeviceToHost, s));
+            HFM_CUDA(cudaMemcpyAsync(res.stencil_w.data(), plain_w.get() + off * ND, n * ND * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s));
         }
-        HFM_CUDA(cudaStreamSynchronize(s));
-        HFM_CUDA(cudaGetLastError());
-        res.n_accepted = (int64_t)hn;
+        res.n_accepted = (int64_t)hn[i];
         res.rounds = (long long)hs[0];
         res.tile_activations = (long long)hs[1];
         res.local_solves = (long long)hs[2];
+        res.t_stencil_ms = t_stencil;
+        res.t_solve_ms = t_solve;
     }
-    res.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall_t0).count();
+    HFM_CUDA(cudaStreamSynchronize(s));
+    if (ninst == 1 && !p0.adjoint_index.empty()) {
+        tm.start(s);
+        run_adjoint<Real, NFWD, NSYM, SHARE>(P, N, p0, results[0], status, s);
+        results[0].t_adjoint_ms = tm.stop(s);
+    }
+    HFM_CUDA(cudaStreamSynchronize(s));
+    HFM_CUDA(cudaGetLastError());
+    const double total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall_t0).count();
+    for (EulerResult &r : results) r.t_total_ms = total;
 }
 
 }  // namespace detail
 
-using detail::run_impl;
+using detail::run_batch_impl;
 
-void solve_eulerian(const EulerProblem &p, EulerResult &r) {
+void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
+    if (probs.empty()) {
+        results.clear();
+        return;
+    }
+    const EulerProblem &p = *probs[0];
+    for (const EulerProblem *q : probs) {
+        if (q->kind != p.kind || q->ndim != p.ndim || q->nfwd != p.nfwd || q->nsym != p.nsym || q->fp64 != p.fp64)
+            throw Error(HFM_ERR_VALUE, "a batch must hold instances of one model family and one precision");
+    }
     if (p.kind == StencilKind::RiemannPerCell) {
         if (p.ndim == 2) {
-            if (p.fp64) run_impl<double, 0, 3, false>(p, r);
-            else run_impl<float, 0, 3, false>(p, r);
+            if (p.fp64) run_batch_impl<double, 0, 3, false>(probs, results);
+            else run_batch_impl<float, 0, 3, false>(probs, results);
         } else if (p.ndim == 3) {
-            if (p.fp64) run_impl<double, 0, 6, false>(p, r);
-            else run_impl<float, 0, 6, false>(p, r);
+            if (p.fp64) run_batch_impl<double, 0, 6, false>(probs, results);
+            else run_batch_impl<float, 0, 6, false>(probs, results);
         } else {
             throw Error(HFM_ERR_UNSUPPORTED, "Riemann models support dimensions 2 and 3");
         }
     } else {
         if (p.nfwd == 0 && p.nsym == 4) {
-            if (p.fp64) run_impl<double, 0, 4, true>(p, r);
-            else run_impl<float, 0, 4, true>(p, r);
+            if (p.fp64) run_batch_impl<double, 0, 4, true>(probs, results);
+            else run_batch_impl<float, 0, 4, true>(probs, results);
         } else if (p.nfwd == 27 && p.nsym == 0) {
-            if (p.fp64) run_impl<double, 27, 0, true>(p, r);
-            else run_impl<float, 27, 0, true>(p, r);
+            if (p.fp64) run_batch_impl<double, 27, 0, true>(probs, results);
+            else run_batch_impl<float, 27, 0, true>(probs, results);
         } else {
             throw Error(HFM_ERR_UNSUPPORTED, "unsupported shared stencil shape");
         }
     }
+}
+
+void solve_eulerian(const EulerProblem &p, EulerResult &r) {
+    std::vector<EulerResult> rs;
+    solve_eulerian_batch({&p}, rs);
+    r = std::move(rs[0]);
 }
 
 }  // namespace hfm

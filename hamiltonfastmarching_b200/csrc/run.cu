@@ -347,7 +347,18 @@ void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProble
     }
 }
 
-void run_model(Store &io, const std::string &model) {
+// A model read from its store, ready to solve (the part of Run before the solver loop).
+struct Prepared {
+    Param pm;
+    EulerProblem p;
+    bool export_values = false, export_active = false, skip = false;
+    std::vector<int64_t> dims;
+    double *values_dst = nullptr;
+};
+
+void prepare_model(Store &io, const std::string &model, Prepared &q) {
+    Param &pm = q.pm;
+    EulerProblem &p = q.p;
     // Run_SetupIO (HFMInterface.hxx:311-341)
     io.verbosity = (int)io.get_scalar("verbosity", io.verbosity);
     if (io.has_field("keyHelp")) io.get_string("keyHelp");
@@ -357,8 +368,6 @@ void run_model(Store &io, const std::string &model) {
     io.set_ordering(o);
     reject_unsupported(io);
 
-    Param pm;
-    EulerProblem p;
     const bool lifted = model == "ReedsShepp2" || model == "Elastica2";
     if (model == "Riemann2") setup_riemann(io, 2, pm, p);
     else if (model == "Riemann3") setup_riemann(io, 3, pm, p);
@@ -369,14 +378,15 @@ void run_model(Store &io, const std::string &model) {
     p.walls = read_walls(io, pm, lifted);
     read_seeds(io, pm, p, lifted);
 
-    const bool export_values = io.get_scalar("exportValues", 0.0, 2) != 0;
-    const bool export_active = io.get_scalar("exportActiveNeighs", 0.0, 3) != 0;
+    q.export_values = io.get_scalar("exportValues", 0.0, 2) != 0;
+    q.export_active = io.get_scalar("exportActiveNeighs", 0.0, 3) != 0;
     const bool inspect = io.has_field("inspectSensitivity");
-    p.want_active = export_active;
+    p.want_active = q.export_active;
 
-    std::vector<int64_t> dims(pm.dims, pm.dims + pm.ndim);
+    q.dims.assign(pm.dims, pm.dims + pm.ndim);
     if (p.seed_index.empty()) {
         io.warn("No seeds to run fast marching solver, and missing values or activeNeighs to compute geodesics.\n");
+        q.skip = true;
         return;
     }
     if (inspect) {
@@ -413,16 +423,13 @@ void run_model(Store &io, const std::string &model) {
         }
     }
     // the arrival times are downloaded straight into the output field when no reordering is needed
-    double *values_dst = export_values ? io.create_field("values", dims, 1) : nullptr;
-    p.h_values_out = values_dst;
-    EulerResult r;
-    try {
-        solve_eulerian(p, r);
-    } catch (...) {
-        if (values_dst) io.erase_field("values");
-        throw;
-    }
+    q.values_dst = q.export_values ? io.create_field("values", q.dims, 1) : nullptr;
+    p.h_values_out = q.values_dst;
+}
 
+void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
+    const Param &pm = q.pm;
+    const std::vector<int64_t> &dims = q.dims;
     // Outputs (Run_SetupSolver/Run_RunSolver/Run_ExportData, CommonStoppingCriteria::Finally)
     io.set_scalar("MaxStencilWidth", r.max_stencil_width);
     io.set_scalar("StencilCPUTime", r.t_stencil_ms * 1e-3);
@@ -438,8 +445,8 @@ void run_model(Store &io, const std::string &model) {
         m << "Fast marching solver completed in " << r.t_solve_ms * 1e-3 << " s.\n";
         io.msg(m.str());
     }
-    if (export_values && !values_dst) io.set_field("values", dims, 1, r.values.data());
-    if (export_active) {
+    if (q.export_values && !q.values_dst) io.set_field("values", dims, 1, r.values.data());
+    if (q.export_active) {
         std::vector<double> a(r.active.size());
         for (size_t i = 0; i < a.size(); ++i) a[i] = (double)r.active[i];
         io.set_field("activeNeighs", dims, 1, a.data());
@@ -463,6 +470,21 @@ void run_model(Store &io, const std::string &model) {
                       ss.data());
     }
     io.set_scalar("nAccepted", (double)r.n_accepted);
+}
+
+
+void run_model(Store &io, const std::string &model) {
+    Prepared q;
+    prepare_model(io, model, q);
+    if (q.skip) return;
+    EulerResult r;
+    try {
+        solve_eulerian(q.p, r);
+    } catch (...) {
+        if (q.values_dst) io.erase_field("values");
+        throw;
+    }
+    finish_model(io, q, r);
 }
 
 }  // namespace
@@ -608,6 +630,87 @@ int hfm_run(hfm_io *io, const char *expected_model) {
         hfm::run_model(st, model == "Elastica2_5" ? "Elastica2" : model);
         st.usage_report();
     });
+}
+
+int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *codes) {
+    if (n < 0 || (n > 0 && !ios)) return HFM_ERR_ARG;
+    for (int i = 0; i < n; ++i)
+        if (!ios[i]) return HFM_ERR_ARG;
+    std::vector<int> rc(n, HFM_OK);
+    std::vector<std::unique_ptr<hfm::Prepared>> qs(n);
+    for (int i = 0; i < n; ++i) ios[i]->store.current_setter = hfm::Setter::Compute;
+    // Reading: every instance on its own (errors stay with their instance).
+    for (int i = 0; i < n; ++i) {
+        rc[i] = guarded(ios[i], [&] {
+            hfm::Store &st = ios[i]->store;
+            const std::string model = st.get_string("model");
+            if (expected_model && model != expected_model)
+                throw Error(HFM_ERR_VALUE,
+                            std::string("Executable applies to ") + expected_model + ", not to " + model + ".");
+            auto q = std::make_unique<hfm::Prepared>();
+            hfm::prepare_model(st, model == "Elastica2_5" ? "Elastica2" : model, *q);
+            qs[i] = std::move(q);
+        });
+    }
+    // Solving: instances of one stencil family and precision share one launch sequence; sensitivity
+    // requests run on their own.
+    std::vector<char> done(n, 0);
+    for (int i = 0; i < n; ++i) {
+        if (rc[i] != HFM_OK || done[i] || qs[i]->skip) continue;
+        std::vector<int> grp{i};
+        done[i] = 1;
+        const hfm::EulerProblem &pi = qs[i]->p;
+        if (pi.adjoint_index.empty()) {
+            for (int j = i + 1; j < n; ++j) {
+                if (rc[j] != HFM_OK || done[j] || qs[j]->skip) continue;
+                const hfm::EulerProblem &pj = qs[j]->p;
+                if (pj.adjoint_index.empty() && pj.kind == pi.kind && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
+                    pj.nsym == pi.nsym && pj.fp64 == pi.fp64 && pj.sweeps_per_tile == pi.sweeps_per_tile &&
+                    pj.max_rounds == pi.max_rounds) {
+                    grp.push_back(j);
+                    done[j] = 1;
+                }
+            }
+        }
+        std::vector<const hfm::EulerProblem *> probs;
+        for (int j : grp) probs.push_back(&qs[j]->p);
+        std::vector<hfm::EulerResult> res;
+        hfm_io *lead = ios[grp[0]];
+        int code = guarded(lead, [&] { hfm::solve_eulerian_batch(probs, res); });
+        if (code != HFM_OK && code != HFM_ERR_CUDA && grp.size() > 1) {
+            // an invalid instance (e.g. a non-SPD metric) fails its whole group: solve the members
+            // one by one so that the error stays with its own store
+            res.assign(grp.size(), hfm::EulerResult());
+            for (size_t k = 0; k < grp.size(); ++k) {
+                const int j = grp[k];
+                rc[j] = guarded(ios[j], [&] { hfm::solve_eulerian(qs[j]->p, res[k]); });
+                if (rc[j] != HFM_OK && qs[j]->values_dst) ios[j]->store.erase_field("values");
+            }
+            for (size_t k = 0; k < grp.size(); ++k) {
+                const int j = grp[k];
+                if (rc[j] == HFM_OK) rc[j] = guarded(ios[j], [&] { hfm::finish_model(ios[j]->store, *qs[j], res[k]); });
+            }
+            continue;
+        }
+        for (size_t k = 0; k < grp.size(); ++k) {
+            const int j = grp[k];
+            if (code != HFM_OK) {
+                rc[j] = code;
+                ios[j]->last_error = lead->last_error;
+                if (qs[j]->values_dst) ios[j]->store.erase_field("values");
+                continue;
+            }
+            rc[j] = guarded(ios[j], [&] { hfm::finish_model(ios[j]->store, *qs[j], res[k]); });
+        }
+    }
+    int first = HFM_OK;
+    for (int i = 0; i < n; ++i) {
+        if (rc[i] == HFM_OK) rc[i] = guarded(ios[i], [&] { ios[i]->store.usage_report(); });
+        ios[i]->store.current_setter = hfm::Setter::User;
+        if (codes) codes[i] = rc[i];
+        if (first == HFM_OK) first = rc[i];
+    }
+    return first;
 }
 
 const char *hfm_io_last_error(hfm_io *io) { return io ? io->last_error.c_str() : "null hfm_io"; }

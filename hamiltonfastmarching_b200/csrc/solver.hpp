@@ -81,6 +81,9 @@ struct EulerResult {
 };
 
 void solve_eulerian(const EulerProblem &p, EulerResult &r);
+// One launch sequence for many instances of one model family and precision (a global tile space
+// over all instances, one persistent solver launch). Results are in the order of `probs`.
+void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results);
 
 // Curvature model stencil tables built on the host with the C library's cos/sin
 // (Headers/Specializations/Curvature2.h:48-66, 178-234, CommonTraits.h:118-161).

@@ -76,6 +76,16 @@ int hfm_io_computed_keys(hfm_io *io, char *buf, size_t cap, size_t *len);
  * single-model FileHFM_<Model> executables do (DispatchAndRun.h:227-233). */
 int hfm_run(hfm_io *io, const char *expected_model);
 
+/* Runs `n` stores as one batch: each is read as by hfm_run, then the instances of one stencil family
+ * and precision (and the same tileSweeps/maxRounds) are solved together — one global tile space
+ * over all of them, one persistent solver launch — and each store receives its own outputs.
+ * Stores with inspectSensitivity are solved on their own. `codes` (may be NULL) receives each
+ * store's status; the return value is the first non-zero status, or HFM_OK. The values are those
+ * hfm_run produces for each store alone (the fixed point of every instance is independent of its
+ * batch neighbours); solver statistics (solverRounds, tileActivations, executedUpdates,
+ * GPUSolveTime) are those of the whole batch. Extends the reference's one-instance Run(IO&). */
+int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *codes);
+
 /* Message of the last failure on `io` ("" if none). Valid until the next call on `io`. */
 const char *hfm_io_last_error(hfm_io *io);
 
