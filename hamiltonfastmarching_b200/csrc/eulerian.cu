@@ -47,7 +47,11 @@ void trace_step(const char *what) {
     static const bool registered = (std::atexit(trace_at_exit), true);
     (void)registered;
     const cudaError_t e = cudaDeviceSynchronize();
-    std::fprintf(stderr, "[hfm] %s: %s\n", what, cudaGetErrorString(e));
+    static auto last = std::chrono::steady_clock::now();
+    const auto now = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - last).count();
+    last = now;
+    std::fprintf(stderr, "[hfm] %s: %s (+%.3f ms)\n", what, cudaGetErrorString(e), ms);
     std::fflush(stderr);
 }
 
@@ -93,8 +97,10 @@ struct Inst {
     long long cell0;     // first global cell (RowMajor values of the instance start here)
     long long cls0;      // first class of its shared-stencil table
     long long metric0;   // first metric row
+    long long mult0;     // first entry of its compact speed-multiplier field
     double h[3];
-    int dual, metric_const, has_walls, pad;
+    int dual, metric_const, has_walls;
+    int mult_depth, mult_inverse, pad;
 };
 
 // Instance holding global cell x (binary search over the increasing cell0 offsets).
@@ -135,6 +141,9 @@ struct Dev {
     // decrease, so a stale entry is an upper bound
     unsigned long long *maxval;            // [ntile]
     unsigned long long *rstat;             // [8][4] per round slot: min key, max key, tiles solved, -
+    // per instance: key = value * kscale, so that the keys of a batch measure the progress of each
+    // instance's front on a common scale (nullptr: keys are the values)
+    const double *kscale;
     unsigned order_lo, order_hi;           // tiles solved per round kept in [lo, hi]; lo = 0: plain FIM
     // active-tile lists (triple buffered) and their dedupe flags
     int *list[3];
@@ -306,7 +315,8 @@ __device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bo
 // just claimed itself, sees them on its next activation.
 template <typename Real>
 __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int slot, int T, unsigned long long mask,
-                                                unsigned long long self_pending, unsigned long long mu, int lane) {
+                                                unsigned long long self_pending, unsigned long long mu,
+                                                unsigned long long kb, int lane) {
     bool any = false;
     if (mask) {
         const long long b = P.dep_ptr[T], e = P.dep_ptr[T + 1];
@@ -325,7 +335,7 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
                 }
                 if (want) {
                     atomicOr(P.dirty + D, P.dep_dmask[i]);
-                    atomicMin(P.key + D, mu);
+                    atomicMin(P.key + D, kb);
                 }
             }
             any |= __any_sync(0xffffffffu, want);
@@ -334,12 +344,12 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
     }
     if (self_pending && lane == 0) {
         atomicOr(P.dirty + T, self_pending);
-        atomicMin(P.key + T, mu);
+        atomicMin(P.key + T, kb);
     }
     push_tiles(P, li, T, self_pending != 0ull && lane == 0, lane);
     if ((any || self_pending) && lane == 0) {
-        atomicMin(P.rstat + slot * 4 + 0, mu);
-        atomicMax(P.rstat + slot * 4 + 1, mu);
+        atomicMin(P.rstat + slot * 4 + 0, kb);
+        atomicMax(P.rstat + slot * 4 + 1, kb);
     }
 }
 
@@ -476,7 +486,9 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 #pragma unroll
     for (int o = 16; o; o >>= 1) mu = fmin(mu, __shfl_xor_sync(0xffffffffu, mu, o));
     __threadfence();
-    push_dependents(P, li_next, slot, T, mask, pending, (unsigned long long)__double_as_longlong(mu), lane);
+    const double kv = P.kscale ? mu * P.kscale[P.tile_inst[T]] : mu;
+    push_dependents(P, li_next, slot, T, mask, pending, (unsigned long long)__double_as_longlong(mu),
+                    (unsigned long long)__double_as_longlong(kv), lane);
 }
 
 // Persistent cooperative solver: rounds over the triple-buffered active-tile lists. Round r solves
@@ -565,7 +577,7 @@ template <typename Real>
 __global__ void init_lists_kernel(Dev<Real> P, const int *seed_tiles, const unsigned long long *seed_masks, int n) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (wid >= n) return;
-    push_dependents(P, 0, 0, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, lane);
+    push_dependents(P, 0, 0, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, 0ull, lane);
 }
 
 // --------------------------------------------------------------------------------------------
@@ -654,12 +666,21 @@ __global__ void width_kernel(Dev<Real> P, unsigned *maxw) {
 }
 
 // Speed multiplier to the tile-major layout (shared stencils).
+// The compact field (depth 0: one value, 1: per angle, 2: per (x,y), 3: per cell) is broadcast
+// here; a cost is inverted in double precision (IEEE division, as the reference's 1./cost).
 template <typename Real>
-__global__ void mult_layout_kernel(Dev<Real> P, const double *mult_rm) {
+__global__ void mult_layout_kernel(Dev<Real> P, const double *src) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= P.ncells) return;
     const CellRef R = cell_ref(P.inst, P.ninst, x);
-    P.mult[R.c] = (Real)mult_rm[x];
+    const Inst &I = P.inst[R.i];
+    long long k = 0;
+    if (I.mult_depth == 3) k = R.xl;
+    else if (I.mult_depth == 2) k = (long long)R.x0 * I.g.dims[1] + R.x1;
+    else if (I.mult_depth == 1) k = R.x2;
+    double m = src[I.mult0 + k];
+    if (I.mult_inverse) m = 1.0 / m;
+    P.mult[R.c] = (Real)m;
 }
 
 // --------------------------------------------------------------------------------------------
@@ -923,6 +944,33 @@ __global__ void dep_scatter_kernel(long long n, const int *src, const int *dst, 
 
 // --------------------------------------------------------------------------------------------
 // Post-processing.
+
+// Per instance, the sum over cells of the norm scale of the Riemann metric: sqrt(tr(M)/d) for a
+// primal metric, sqrt(d/tr(D)) for a dual one (the key scale of batched ordering).
+template <int D, typename Real>
+__global__ void metric_scale_kernel(Dev<Real> P, const double *metric, double *out) {
+    constexpr int NS = D * (D + 1) / 2;
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool in = x < P.ncells;
+    int i = -1;
+    double v = 0.0;
+    if (in) {
+        i = inst_of_cell(P.inst, P.ninst, x);
+        const Inst &I = P.inst[i];
+        const double *m = metric + (I.metric0 + (I.metric_const ? 0 : x - I.cell0)) * NS;
+        const double tr = D == 2 ? m[0] + m[2] : m[0] + m[2] + m[5];
+        v = I.dual ? sqrt(D / tr) : sqrt(tr / D);
+        if (!(v < 1e300)) v = 0.0;
+    }
+    // segmented warp sum: the first lane of each instance adds the others' terms
+    const unsigned same = __match_any_sync(0xffffffffu, i);
+    const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+    for (int o = 0; o < 32; ++o) {
+        const double w = __shfl_sync(0xffffffffu, v, o);
+        if (lane == leader && o != lane && ((same >> o) & 1u)) v += w;
+    }
+    if (in && lane == leader) atomicAdd(out + i, v);
+}
 
 template <typename Real>
 // Reached cells per instance (the reference's nAccepted).
@@ -1292,7 +1340,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
 
     // ---- batch layout: instance table, global tile space
     std::vector<Inst> hinst(ninst);
-    long long ntile = 0, ncells = 0, nclass = 0, nmetric = 0;
+    long long ntile = 0, ncells = 0, nclass = 0, nmetric = 0, nmult = 0;
     bool any_walls = false, want_active = false, want_stencils = false;
     for (int i = 0; i < ninst; ++i) {
         const EulerProblem &p = *probs[i];
@@ -1311,6 +1359,13 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         ncells += I.g.ncells;
         nclass += SHARE ? p.nclass : 0;
         if (!SHARE) nmetric += p.metric_constant ? 1 : I.g.ncells;
+        I.mult0 = nmult;
+        I.mult_depth = p.mult_depth;
+        I.mult_inverse = p.mult_inverse ? 1 : 0;
+        if (SHARE) {
+            const long long nm[4] = {1, I.g.dims[2], (long long)I.g.dims[0] * I.g.dims[1], I.g.ncells};
+            nmult += nm[std::min(3, std::max(0, p.mult_depth))];
+        }
         any_walls |= I.has_walls != 0;
         want_active |= p.want_active;
         want_stencils |= p.want_stencils;
@@ -1350,7 +1405,8 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     DeviceBuffer<Real> weight, mult, cls_w;
     DeviceBuffer<int8_t> cls_off, plain_off;
     DeviceBuffer<uint8_t> cls_en;
-    DeviceBuffer<double> metric, plain_w, mult_rm;
+    DeviceBuffer<double> metric, plain_w, mult_rm, kscale;
+    std::vector<double> hscale;
     maxw.zero(s);
     std::vector<unsigned> hmaxw(ninst, 0);
     if (!SHARE) {
@@ -1380,6 +1436,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             }
             metric_ptr = metric.get();
         }
+        HFM_TRACE("metric upload");
         if (want_stencils) {
             plain_off.alloc(N * ND * 3);
             plain_w.alloc(N * ND);
@@ -1394,18 +1451,41 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_TRACE("stencil kernel");
         launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, P, maxw.get());
         maxw.download(hmaxw.data(), ninst, s);
+        if (ninst > 1 && p0.ordered) {
+            kscale.alloc(ninst);
+            kscale.zero(s);
+            if (p0.ndim == 2)
+                launch(metric_scale_kernel<2, Real>, nblocks(N, 256), 256, 0, s, P, metric_ptr, kscale.get());
+            else
+                launch(metric_scale_kernel<3, Real>, nblocks(N, 256), 256, 0, s, P, metric_ptr, kscale.get());
+            hscale.resize(ninst);
+            kscale.download(hscale.data(), ninst, s);
+        }
         HFM_CUDA(cudaStreamSynchronize(s));
     } else {
         std::vector<Real> hw;
         std::vector<int8_t> ho;
         std::vector<uint8_t> he;
-        std::vector<double> hm(N);
+        mult_rm.alloc(std::max(1ll, nmult));
         for (int i = 0; i < ninst; ++i) {
             const EulerProblem &p = *probs[i];
             for (double w : p.cls_w) hw.push_back((Real)w);
             ho.insert(ho.end(), p.cls_off.begin(), p.cls_off.end());
             he.insert(he.end(), p.cls_enabled.begin(), p.cls_enabled.end());
-            std::copy(p.mult.begin(), p.mult.end(), hm.begin() + hinst[i].cell0);
+            const long long len = (i + 1 < ninst ? hinst[i + 1].mult0 : nmult) - hinst[i].mult0;
+            const double *msrc = p.mult_ptr ? p.mult_ptr : p.mult.data();
+            if (!p.mult_ptr && (long long)p.mult.size() < len)
+                throw Error(HFM_ERR_VALUE, "speed multiplier field too short");
+            HFM_CUDA(cudaMemcpyAsync(mult_rm.get() + hinst[i].mult0, msrc, len * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+            if (ninst > 1 && p0.ordered) {  // time scale = mean cost over the (uniform) broadcast field
+                double t = 0.0;
+                for (long long k = 0; k < len; ++k) {
+                    const double m = msrc[k];
+                    t += p.mult_inverse ? m : (m > 0.0 ? 1.0 / m : 0.0);
+                }
+                hscale.push_back(t / (double)len * (double)hinst[i].g.ncells);
+            }
             // width over the class tables, from each class centre (HFM_StencilShare.hxx:152-175)
             int mw = 0;
             for (int cl = 0; cl < p.nclass; ++cl)
@@ -1420,6 +1500,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                 }
             hmaxw[i] = (unsigned)mw;
         }
+        HFM_TRACE("class tables and multipliers (host)");
         cls_w.upload(hw, s);
         cls_off.upload(ho, s);
         cls_en.upload(he, s);
@@ -1429,13 +1510,26 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         mult.alloc(ntc);
         mult.zero(s);
         P.mult = mult.get();
-        mult_rm.upload(hm, s);
         launch(mult_layout_kernel<Real>, nblocks(N, 256), 256, 0, s, P, mult_rm.get());
         vis.alloc(ntc);
         vis.zero(s);
         P.vis = vis.get();
     }
     for (int i = 0; i < ninst; ++i) results[i].max_stencil_width = (int)hmaxw[i];
+    if (!hscale.empty()) {
+        // key scale: 1 / (domain diameter x mean norm scale), a common progress measure of the
+        // instances' fronts for the value-ordered scheduling of a batch
+        for (int i = 0; i < ninst; ++i) {
+            const GridGeom &g = hinst[i].g;
+            const int nphys = SHARE ? 2 : probs[i]->ndim;
+            double d2 = 0.0;
+            for (int a = 0; a < nphys; ++a) d2 += (g.dims[a] * hinst[i].h[a]) * (g.dims[a] * hinst[i].h[a]);
+            const double t = std::sqrt(d2) * hscale[i] / (double)g.ncells;
+            hscale[i] = (t > 0.0 && t < 1e300) ? 1.0 / t : 1.0;
+        }
+        kscale.upload(hscale, s);
+        P.kscale = kscale.get();
+    }
 
     // ---- walls and visibility
     DeviceBuffer<uint8_t> walls;
@@ -1613,8 +1707,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
         const int grid = nsm * per_sm;
         const double nwarps = (double)grid * kWarpsPerCta;
-        // Keys are arrival times of one instance: the band ordering is used for single solves only.
-        const bool ordered = p0.ordered && ninst == 1;
+        const bool ordered = p0.ordered;
         P.order_lo = ordered ? (unsigned)std::max(1.0, p0.band_lo * nwarps) : 0u;
         P.order_hi = ordered ? (unsigned)std::max(2.0, p0.band_hi * nwarps) : 0u;
         void *args[] = {&P};
@@ -1680,6 +1773,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         res.t_solve_ms = t_solve;
     }
     HFM_CUDA(cudaStreamSynchronize(s));
+    HFM_TRACE("outputs");
     if (ninst == 1 && !p0.adjoint_index.empty()) {
         tm.start(s);
         run_adjoint<Real, NFWD, NSYM, SHARE>(P, N, p0, results[0], status, s);

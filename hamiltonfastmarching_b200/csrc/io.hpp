@@ -15,6 +15,7 @@
 #include <set>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace hfm {
@@ -50,6 +51,10 @@ struct BigAlloc {
         if (bytes >= kThreshold) munmap(p, bytes);
         else std::free(p);
     }
+    // resize() leaves new elements uninitialised (an output field is written in full by the solver,
+    // so zero-filling hundreds of MB first would only cost page faults and bandwidth)
+    template <typename U> void construct(U *p) { ::new ((void *)p) U; }
+    template <typename U, typename... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
     template <typename U> bool operator==(const BigAlloc<U> &) const { return true; }
     template <typename U> bool operator!=(const BigAlloc<U> &) const { return false; }
 };

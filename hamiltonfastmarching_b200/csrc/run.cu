@@ -156,32 +156,17 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
 }
 
 // A scalar field over the lifted grid given with depth 0 (constant), 3 (full), 2 (physical x,y)
-// or 1 (angle only) (HFMInterface.hxx:23-32).
-std::vector<double> read_lifted_scalar(Store &io, const std::string &key, const int *dims) {
+// or 1 (angle only) (HFMInterface.hxx:23-32), kept compact: the solver expands it on the device.
+// Returns the depth; `f` holds the field (a view into the store when no reordering is needed).
+int read_lifted_scalar(Store &io, const std::string &key, const int *dims, Field &f) {
     const std::vector<int64_t> dd = io.field_domain_dims(key, 1);
     const int depth = (int)dd.size();
-    const int64_t N = (int64_t)dims[0] * dims[1] * dims[2];
-    std::vector<double> out(N);
-    Field f = io.get_field(key, depth, 1);
-    if (depth == 0) {
-        std::fill(out.begin(), out.end(), f.ptr()[0]);
-    } else if (depth == 3) {
-        if (f.dims[0] != dims[0] || f.dims[1] != dims[1] || f.dims[2] != dims[2])
-            throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
-        out.assign(f.ptr(), f.ptr() + f.size());
-    } else if (depth == 2) {
-        if (f.dims[0] != dims[0] || f.dims[1] != dims[1])
-            throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
-        for (int64_t i = 0; i < (int64_t)dims[0] * dims[1]; ++i)
-            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.ptr()[i];
-    } else if (depth == 1) {
-        if (f.dims[0] != dims[2]) throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
-        for (int64_t i = 0; i < (int64_t)dims[0] * dims[1]; ++i)
-            for (int t = 0; t < dims[2]; ++t) out[i * dims[2] + t] = f.ptr()[t];
-    } else {
-        throw Error(HFM_ERR_VALUE, "Field " + key + " has incorrect depth.\n");
-    }
-    return out;
+    if (depth > 3) throw Error(HFM_ERR_VALUE, "Field " + key + " has incorrect depth.\n");
+    f = io.get_field(key, depth, 1);
+    if ((depth == 3 && (f.dims[0] != dims[0] || f.dims[1] != dims[1] || f.dims[2] != dims[2])) ||
+        (depth == 2 && (f.dims[0] != dims[0] || f.dims[1] != dims[1])) || (depth == 1 && f.dims[0] != dims[2]))
+        throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+    return depth;
 }
 
 std::vector<uint8_t> read_walls(Store &io, const Param &pm, bool lifted) {
@@ -190,8 +175,14 @@ std::vector<uint8_t> read_walls(Store &io, const Param &pm, bool lifted) {
     const int64_t N = (int64_t)pm.dims[0] * pm.dims[1] * pm.dims[2];
     w.resize(N);
     if (lifted) {
-        const std::vector<double> v = read_lifted_scalar(io, "walls", pm.dims);
-        for (int64_t i = 0; i < N; ++i) w[i] = v[i] != 0.0;  // GetIntegralField<bool>: (bool)double
+        Field f;
+        const int depth = read_lifted_scalar(io, "walls", pm.dims, f);
+        const double *v = f.ptr();
+        const int64_t nt = pm.dims[2];
+        for (int64_t i = 0; i < N; ++i) {  // GetIntegralField<bool>: (bool)double
+            const int64_t k = depth == 3 ? i : depth == 2 ? i / nt : depth == 1 ? i % nt : 0;
+            w[i] = v[k] != 0.0;
+        }
         return w;
     }
     const std::vector<int64_t> dd = io.field_domain_dims("walls", 1);
@@ -314,6 +305,8 @@ void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProble
     pm.origin[2] = -ds / 2.0;
     pm.scale[0] = pm.scale[1] = h;
     pm.scale[2] = ds;
+    p.h[0] = p.h[1] = h;  // the class tables carry the scales; h only sizes the domain
+    p.h[2] = ds;
     p.kind = StencilKind::SharedByTheta;
     p.nclass = dims[2];
     if (rs) {
@@ -338,12 +331,16 @@ void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProble
                 p.cls_enabled[c * NB + slot] = (y0 >= 0 && y0 < dims[0] && y1 >= 0 && y1 < dims[1]) ? 1 : 0;
             }
         }
-    if (io.has_field("speed")) {
-        p.mult = read_lifted_scalar(io, "speed", dims.data());
+    // speed, or cost inverted on the device (DataSource_Inverse, HFMInterface.hxx:131-150)
+    const bool has_speed = io.has_field("speed");
+    Field f;
+    p.mult_depth = read_lifted_scalar(io, has_speed ? "speed" : "cost", dims.data(), f);
+    p.mult_inverse = !has_speed;
+    if (f.view) {
+        p.mult_ptr = f.view;
     } else {
-        std::vector<double> cost = read_lifted_scalar(io, "cost", dims.data());
-        for (double &c : cost) c = 1. / c;  // DataSource_Inverse (HFMInterface.hxx:131-150)
-        p.mult = std::move(cost);
+        p.mult = std::move(f.data);
+        p.mult_ptr = nullptr;
     }
 }
 
@@ -652,6 +649,7 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
             qs[i] = std::move(q);
         });
     }
+    HFM_TRACE("batch: stores read");
     // Solving: instances of one stencil family and precision share one launch sequence; sensitivity
     // requests run on their own.
     std::vector<char> done(n, 0);
@@ -676,6 +674,7 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
         for (int j : grp) probs.push_back(&qs[j]->p);
         std::vector<hfm::EulerResult> res;
         hfm_io *lead = ios[grp[0]];
+        HFM_TRACE("batch: group formed");
         int code = guarded(lead, [&] { hfm::solve_eulerian_batch(probs, res); });
         if (code != HFM_OK && code != HFM_ERR_CUDA && grp.size() > 1) {
             // an invalid instance (e.g. a non-SPD metric) fails its whole group: solve the members
@@ -703,6 +702,7 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
             rc[j] = guarded(ios[j], [&] { hfm::finish_model(ios[j]->store, *qs[j], res[k]); });
         }
     }
+    HFM_TRACE("batch: solved and exported");
     int first = HFM_OK;
     for (int i = 0; i < n; ++i) {
         if (rc[i] == HFM_OK) rc[i] = guarded(ios[i], [&] { ios[i]->store.usage_report(); });

@@ -36,7 +36,14 @@ struct EulerProblem {
     std::vector<int8_t> cls_off;       // [nclass][nfwd+nsym][3]
     std::vector<double> cls_w;         // [nclass][nfwd+nsym]
     std::vector<uint8_t> cls_enabled;  // [nclass][nfwd+2*nsym] slot reachable from the class centre
-    std::vector<double> mult;          // [N] speed multiplier (RowMajor)
+    // Speed multiplier of the shared stencils, given compactly as in the reference's lifted scalar
+    // fields (HFMInterface.hxx:23-32): depth 0 (one value), 1 (per angle), 2 (per physical point
+    // x,y) or 3 (per cell), RowMajor at mult_ptr (host, not owned, or `mult` when null); the cost
+    // form (mult_inverse) is turned into a speed 1/cost on the device (DataSource_Inverse).
+    std::vector<double> mult;
+    const double *mult_ptr = nullptr;
+    int mult_depth = 3;
+    bool mult_inverse = false;
 
     std::vector<uint8_t> walls;        // [N] or empty
     // Device-resident alternatives (zero-copy path): used instead of `metric` / `walls` when set,

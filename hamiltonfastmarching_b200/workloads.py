@@ -222,3 +222,32 @@ def curvature2_case(n: int = 128, ntheta: int = 60, model: str = "ReedsShepp2", 
         "seeds": np.asarray(seed_points, dtype=float),
         "exportValues": 1.0,
     }
+
+
+def batched_mix(n_riemann: int = 384, n_lifted: int = 128, ntheta: int = 60, seed: int = 3,
+                side_range=(64, 1024), lifted_range=(64, 256), precision: str = "float32") -> list:
+    """Mixed batch: Riemann2 instances with log-uniform sides, anisotropy U[1,10] and smooth random
+    theta, plus ReedsShepp2 / Elastica2 lifted grids (half each) of N x N x ntheta points with the
+    tubular-image cost 1/(0.05+I), xi = 0.1, eps = 0.1. Each instance has one seed (centre for
+    Riemann2, random oriented point for the lifted models). Returns a list of hfmIn dictionaries.
+    """
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(side_range[0]), np.log(side_range[1])
+    sides = np.exp(rng.uniform(lo, hi, n_riemann)).round().astype(int)
+    anisos = rng.uniform(1.0, 10.0, n_riemann)
+    llo, lhi = np.log(lifted_range[0]), np.log(lifted_range[1])
+    lsides = np.exp(rng.uniform(llo, lhi, n_lifted)).round().astype(int)
+    cases = []
+    for k in range(n_riemann):
+        p = riemann2_case(int(sides[k]), aniso=float(anisos[k]), seed=int(seed * 100003 + k))
+        cases.append(p)
+    for k in range(n_lifted):
+        model = "ReedsShepp2" if k % 2 == 0 else "Elastica2"
+        p = curvature2_case(int(lsides[k]), ntheta, model, seed=int(seed * 100003 + n_riemann + k), xi=0.1,
+                            eps=0.1)
+        cases.append(p)
+    order = rng.permutation(len(cases))
+    cases = [cases[i] for i in order]
+    for p in cases:
+        p["solverPrecision"] = precision
+    return cases
