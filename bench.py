@@ -47,6 +47,9 @@ def parse_args(argv=None):
                     help="grid side of the bounded sample the reference CPU code is timed on")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-riemann", type=int, default=384, help="Riemann2 instances of the batched mix")
+    ap.add_argument("--batch-lifted", type=int, default=128, help="ReedsShepp2/Elastica2 instances of the mix")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-model leg")
     return ap.parse_args(argv)
 
 
@@ -149,6 +152,78 @@ def reference_cpu_sample(side, seed=1):
             "sample": f"FileHFM_Riemann3 on the same generator at {side}^3 ({int(out['nAccepted'])} reached cells); "
                       f"FMCPUTime {out['FMCPUTime']:.2f} s + StencilCPUTime {out['StencilCPUTime']:.2f} s "
                       f"(wall {wall:.1f} s incl. file IO)"}
+
+
+# ------------------------------------------------------------------------------- batched leg
+
+def batched_leg(args, rank, world):
+    """Batched mixed-model launch vs the plain one-at-a-time GPU solve of the same instances.
+
+    384 Riemann2 (sides log-uniform in [64,1024], anisotropy 1-10) + 128 lifted instances
+    (ReedsShepp2 / Elastica2, N x N x 60, N log-uniform in [64,256], tubular-image cost), FP32.
+    Both arms go through the public API from host arrays (hfm_run per store vs one hfm_run_batch
+    over all stores); stores are filled before the timed region. The FP32 values of a seeded 5%
+    sample are compared with the FP64 path (itself held to the reference at 1e-10 by the tests).
+    """
+    import hamiltonfastmarching_b200 as H
+    from hamiltonfastmarching_b200 import workloads as W
+    t0 = time.perf_counter()
+    cases = W.batched_mix(args.batch_riemann, args.batch_lifted, seed=3 + rank)
+    gen_s = time.perf_counter() - t0
+    cells = int(sum(int(np.prod(p["dims"])) for p in cases))
+    rng = np.random.default_rng(1234)
+    sample = sorted(rng.choice(len(cases), max(1, len(cases) // 20), replace=False).tolist())
+    sample_cases = {k: dict(cases[k], solverPrecision="float64", verbosity=0.0) for k in sample}
+    ios = []
+    for k in range(len(cases)):
+        io = H.HFMIO("RowMajor")
+        io.set_dict(cases[k])
+        io.set_scalar("verbosity", 0)
+        ios.append(io)
+        cases[k] = None  # the store holds its own copy: keep one copy of the inputs in host memory
+
+    def clear():
+        for io in ios:
+            if io.has_field("values"):
+                io.erase_field("values")
+
+    def batched():
+        codes = H.run_ios(ios)
+        if any(codes):
+            raise RuntimeError(f"batched solve failed: {sorted(set(codes))}")
+
+    def plain():
+        for io in ios:
+            io.run()
+
+    batched()  # warm-up of both paths (allocator pool, module load)
+    clear()
+    plain()
+    clear()
+    out = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        t0 = time.perf_counter()
+        fn()
+        el = time.perf_counter() - t0
+        reached = sum(io.get_scalar("nAccepted") for io in ios)
+        out[name] = {"seconds": el, "solves_per_s": len(ios) / el, "grid_updates_per_s": reached / el}
+        if name == "batched":
+            vals32 = {k: ios[k].get_array("values") for k in sample}
+        clear()
+    # FP64 on the sample
+    errs = []
+    res64 = H.run_batch([sample_cases[k] for k in sample])
+    for k, r in zip(sample, res64):
+        v64, v32 = r["values"], vals32[k]
+        fin = np.isfinite(v64)
+        errs.append(float(np.max(np.abs(v64[fin] - v32[fin])) / np.max(np.abs(v64[fin]))))
+    return {"workload": f"{args.batch_riemann} Riemann2 (64-1024 sides) + {args.batch_lifted} ReedsShepp2/Elastica2 "
+                        f"(N x N x 60, N 64-256), FP32, one hfm_run_batch",
+            "instances": len(ios), "cells": cells,
+            "batched": out["batched"], "plain_one_at_a_time": out["plain"],
+            "speedup_solves_per_s": out["batched"]["solves_per_s"] / out["plain"]["solves_per_s"],
+            "fp32_max_rel_err_vs_fp64": max(errs), "fp64_sample": len(sample), "input_generation_s": gen_s,
+            "path": "public API from host arrays (H2D/D2H inside both timings)"}
 
 
 # ------------------------------------------------------------------------------------- our arm
@@ -293,6 +368,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu_sample(args.cpu_sample_side)
+    batch = None
+    if not args.no_batch:
+        batch = batched_leg(args, rank, world)
 
     if rank == 0:
         line = {
@@ -310,6 +388,7 @@ def run_ours(args):
             "fp32": {"value": results[32]["value"], "ms_per_step": results[32]["ms_per_step"],
                      "solve_ms": results[32]["solve_ms"], "max_rel_err_vs_fp64": fp32_err,
                      "clocks": results[32]["clocks"]},
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

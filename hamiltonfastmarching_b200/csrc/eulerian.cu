@@ -1065,8 +1065,11 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
 // var(x) = (sum_i w_i (u - u_i)) / sum_i w_i (times the speed multiplier for shared stencils):
 // the same products and sums, in the same order, as ValueVariation. adjoint_kernel then sweeps
 // the upwind graph in reverse topological order: a cell is ready once every downwind cell that
-// reads it has pushed lambda * w into its accumulator (in-degree counters, atomics), which is the
-// order of the reference's decreasing-value traversal restricted to the actual dependencies.
+// reads it has been processed (in-degree counters), which is the order of the reference's
+// decreasing-value traversal restricted to the actual dependencies. A ready cell gathers
+// lambda = (its inspection weight) + sum of w * lambda(downwind) over a reverse adjacency sorted
+// by decreasing downwind value, the order in which the reference's traversal adds them
+// (FirstVariation.h:341-385): the result does not depend on the schedule.
 
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
@@ -1157,8 +1160,12 @@ struct AdjDev {
     const double *fw;
     const double *var;
     const uint8_t *nflow;
+    const long long *rptr;   // reverse adjacency: downwind cells reading y, sorted
+    const int *rx;
+    const double *rw;
+    double *lam;             // lambda of the processed cells
     int *indeg;
-    double *acc;
+    double *acc;             // inspection weights
     double *sens;
     int *list[3];
     unsigned *count[3];
@@ -1203,7 +1210,11 @@ __global__ void adjoint_kernel(AdjDev A) {
             double lam = 0.0;
             if (x >= 0) {
                 lam = __ldcg(A.acc + x);
+                for (long long k = A.rptr[x], e = A.rptr[x + 1]; k < e; ++k)
+                    lam = __dadd_rn(lam, __dmul_rn(A.rw[k], __ldcg(A.lam + A.rx[k])));
+                __stcg(A.lam + x, lam);
                 nf = A.nflow[x];
+                __threadfence();
                 if (lam != 0.0) {
                     A.sens[x] = lam * A.var[x];
                     if (nf == 0) {
@@ -1217,8 +1228,6 @@ __global__ void adjoint_kernel(AdjDev A) {
                 int y = 0;
                 if (j < nf) {
                     y = A.fidx[j * A.N + x];
-                    if (lam != 0.0) atomicAdd(A.acc + y, A.fw[j * A.N + x] * lam);
-                    __threadfence();
                     want = atomicSub(A.indeg + y, 1) == 1;
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, want);
@@ -1239,6 +1248,48 @@ __global__ void adjoint_kernel(AdjDev A) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *A.rounds = (unsigned long long)r;
 }
 
+// Reverse adjacency of the upwind graph: for every cell y, the (downwind cell, weight) pairs of
+// the cells whose final update read y.
+__global__ void flow_scatter_kernel(long long N, const int *fidx, const double *fw, const uint8_t *nflow,
+                                    const long long *rptr, unsigned *cursor, int *rx, double *rw) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    const int nf = nflow[x];
+    for (int j = 0; j < nf; ++j) {
+        const int y = fidx[j * N + x];
+        const long long pos = rptr[y] + atomicAdd(cursor + y, 1u);
+        rx[pos] = (int)x;
+        rw[pos] = fw[j * N + x];
+    }
+}
+
+// Sorts each cell's reverse adjacency by decreasing downwind value, then decreasing index, then
+// weight bits (a fixed order whatever the scatter order was).
+template <typename Real>
+__global__ void flow_sort_kernel(long long N, const long long *rptr, int *rx, double *rw, const Real *values) {
+    const long long y = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (y >= N) return;
+    const long long b = rptr[y], e = rptr[y + 1];
+    auto before = [&](int xa, double wa, int xb, double wb) {
+        const Real va = values[xa], vb = values[xb];
+        if (va != vb) return va > vb;
+        if (xa != xb) return xa > xb;
+        return __double_as_longlong(wa) > __double_as_longlong(wb);
+    };
+    for (long long i = b + 1; i < e; ++i) {
+        const int xi = rx[i];
+        const double wi = rw[i];
+        long long k = i - 1;
+        while (k >= b && before(xi, wi, rx[k], rw[k])) {
+            rx[k + 1] = rx[k];
+            rw[k + 1] = rw[k];
+            --k;
+        }
+        rx[k + 1] = xi;
+        rw[k + 1] = wi;
+    }
+}
+
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
                  DeviceBuffer<unsigned> &status, cudaStream_t s) {
@@ -1252,6 +1303,27 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     launch(flow_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, fidx.get(), fw.get(), var.get(),
                                                                           nflow.get(), indeg0.get());
     HFM_CUDA(cudaGetLastError());
+    // reverse adjacency (CSR over y, offsets scanned on the host)
+    DeviceBuffer<long long> rptr(N + 1);
+    std::vector<int> hdeg(N);
+    indeg0.download(hdeg.data(), N, s);
+    HFM_CUDA(cudaStreamSynchronize(s));
+    std::vector<long long> hrptr(N + 1);
+    long long ne = 0;
+    for (long long y = 0; y < N; ++y) { hrptr[y] = ne; ne += hdeg[y]; }
+    hrptr[N] = ne;
+    rptr.upload(hrptr, s);
+    DeviceBuffer<int> rx(std::max(1ll, ne));
+    DeviceBuffer<double> rw(std::max(1ll, ne)), lam(N);
+    {
+        DeviceBuffer<unsigned> cursor(N);
+        cursor.zero(s);
+        launch(flow_scatter_kernel, nblocks(N, 256), 256, 0, s, N, fidx.get(), fw.get(), nflow.get(), rptr.get(),
+               cursor.get(), rx.get(), rw.get());
+        launch(flow_sort_kernel<Real>, nblocks(N, 256), 256, 0, s, N, rptr.get(), rx.get(), rw.get(), P.values);
+        HFM_CUDA(cudaGetLastError());
+        HFM_CUDA(cudaStreamSynchronize(s));
+    }
     DeviceBuffer<int> lists(3 * N);
     DeviceBuffer<unsigned> counters(8);
     const unsigned seed_cap = 1u << 20;
@@ -1264,6 +1336,10 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     A.fw = fw.get();
     A.var = var.get();
     A.nflow = nflow.get();
+    A.rptr = rptr.get();
+    A.rx = rx.get();
+    A.rw = rw.get();
+    A.lam = lam.get();
     A.indeg = indeg.get();
     A.acc = acc.get();
     A.sens = sens.get();
