@@ -432,13 +432,17 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
     __syncwarp();
     bool converged = false;
     for (int sweep = 0; sweep < P.sweeps; ++sweep) {
-        Real nv[2];
+        Real nv[2] = {cur[0], cur[1]};
+        // one copy of the (large) local solve for both cells; the per-cell operands are selected,
+        // not indexed, so that they stay in registers
 #pragma unroll 1
         for (int j = 0; j < 2; ++j) {
-            nv[j] = cur[j];
-            if (todo[j]) {
-                nv[j] = solve_cell<Real, NFWD, NSYM, SHARE>(P, I, (long long)T * 64 + lane + 32 * j, xs[j][0], xs[j][1],
-                                                            xs[j][2], tx0, tx1, tx2, sv, nullptr, nullptr);
+            if (j ? todo[1] : todo[0]) {
+                const Real r = solve_cell<Real, NFWD, NSYM, SHARE>(
+                    P, I, (long long)T * 64 + lane + 32 * j, j ? xs[1][0] : xs[0][0], j ? xs[1][1] : xs[0][1],
+                    j ? xs[1][2] : xs[0][2], tx0, tx1, tx2, sv, nullptr, nullptr);
+                if (j) nv[1] = r;
+                else nv[0] = r;
                 ++n_solves;
             }
         }
@@ -496,8 +500,16 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 // the next list; delta_r doubles when a round solved fewer than order_lo tiles and halves above
 // order_hi, so the band follows the arrival front with enough tiles in flight. Every block derives
 // the same theta_r from the same round statistics read after the barrier.
+// Resident CTAs per SM requested from the register allocator (measured on B200: the solve is
+// latency-bound, and more resident warps beat the spills this costs, except for the 27-offset
+// Elastica stencil whose local solve needs the registers).
 template <typename Real, int NFWD, int NSYM, bool SHARE>
-__global__ void __launch_bounds__(kWarpsPerCta * 32) fim_kernel(Dev<Real> P) {
+constexpr int fim_min_blocks() {
+    return SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 6;
+}
+
+template <typename Real, int NFWD, int NSYM, bool SHARE>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD, NSYM, SHARE>())) fim_kernel(Dev<Real> P) {
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long kInfBits = 0x7ff0000000000000ull;
