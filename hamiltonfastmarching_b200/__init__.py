@@ -44,6 +44,7 @@ class HFMIO:
         self._L = _lib.load()
         if arrayOrdering not in _lib.ORDERINGS:
             raise ValueError(f"unknown array ordering {arrayOrdering}")
+        self._views = {}
         self._h = self._L.hfm_io_create(_lib.ORDERINGS[arrayOrdering])
         if not self._h:
             raise MemoryError("hfm_io_create failed")
@@ -85,6 +86,14 @@ class HFMIO:
         self._check(self._L.hfm_io_set_array(self._h, key.encode(), a.ctypes.data_as(ctypes.c_void_p), a.ndim,
                                              shape))
 
+    def set_array_view(self, key: str, value):
+        """Zero-copy ``set_array``: the store reads ``value`` in place (a reference is kept here)."""
+        a = np.ascontiguousarray(value, dtype=np.float64)
+        shape = (ctypes.c_int64 * max(a.ndim, 1))(*a.shape)
+        self._check(self._L.hfm_io_set_array_view(self._h, key.encode(), a.ctypes.data_as(ctypes.c_void_p), a.ndim,
+                                                  shape))
+        self._views[key] = a
+
     def get_array(self, key: str) -> np.ndarray:
         nd = ctypes.c_int()
         shape = (ctypes.c_int64 * 16)()
@@ -113,12 +122,15 @@ class HFMIO:
         return self._L.hfm_io_erase_field(self._h, key.encode()) == _lib.HFM_OK
 
     # ---- helpers
-    def set_dict(self, params: Dict):
+    def set_dict(self, params: Dict, views: bool = False):
+        """Sets every entry; with ``views`` arrays are referenced in place (set_array_view)."""
         for k, v in params.items():
             if isinstance(v, str):
                 self.set_string(k, v)
             elif np.isscalar(v) or (isinstance(v, np.ndarray) and v.ndim == 0):
                 self.set_scalar(k, float(v))
+            elif views:
+                self.set_array_view(k, v)
             else:
                 self.set_array(k, np.asarray(v, dtype=np.float64))
 

@@ -25,6 +25,7 @@ SIGNATURES = {
     "hfm_io_set_scalar": ([_P, _S, _D], _I),
     "hfm_io_set_string": ([_P, _S, _S], _I),
     "hfm_io_set_array": ([_P, _S, _P, _I, _I64P], _I),
+    "hfm_io_set_array_view": ([_P, _S, _P, _I, _I64P], _I),
     "hfm_io_get_scalar": ([_P, _S, ctypes.POINTER(_D)], _I),
     "hfm_io_get_string": ([_P, _S, _P, _SZ, ctypes.POINTER(_SZ)], _I),
     "hfm_io_get_array_info": ([_P, _S, ctypes.POINTER(_I), _I64P, _I], _I),
@@ -60,6 +61,28 @@ SIGNATURES["hfm_solve_riemann2_static_scratch"] = ([ctypes.c_int64, ctypes.c_int
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int)
 SIGNATURES["hfm_kernel_launches"] = ([ctypes.POINTER(ctypes.c_ulonglong)], ctypes.c_int)
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_ulonglong), ("completed", ctypes.c_ulonglong),
+                ("batches", ctypes.c_ulonglong), ("max_batch", ctypes.c_ulonglong),
+                ("queued", ctypes.c_ulonglong), ("running_batches", ctypes.c_ulonglong),
+                ("budget_bytes", ctypes.c_double), ("bytes_in_use", ctypes.c_double),
+                ("peak_bytes", ctypes.c_double)]
+
+
+SIGNATURES["hfm_server_create"] = ([ctypes.POINTER(ServerConfig)], ctypes.c_void_p)
+SIGNATURES["hfm_server_submit"] = ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int)
+SIGNATURES["hfm_server_wait"] = ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(ctypes.c_int)],
+                                 ctypes.c_int)
+SIGNATURES["hfm_server_release"] = ([ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)], ctypes.c_int)
+SIGNATURES["hfm_server_get_stats"] = ([ctypes.c_void_p, ctypes.POINTER(ServerStats)], ctypes.c_int)
+SIGNATURES["hfm_server_destroy"] = ([ctypes.c_void_p], None)
 
 _lib = None
 

@@ -23,7 +23,7 @@ BUILD = os.path.join(ROOT, "_build", "hfm_b200")
 LIB = os.path.join(HERE, "libhfm_b200.so")
 CLI = os.path.join(HERE, "bin", "FileHFM_b200")
 
-SOURCES = ["io.cpp", "run.cu", "eulerian.cu", "curvature.cu", "runtime.cu", "static_scratch.cu"]
+SOURCES = ["io.cpp", "run.cu", "eulerian.cu", "curvature.cu", "runtime.cu", "static_scratch.cu", "server.cu"]
 CLI_SOURCES = ["cli/FileHFM.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

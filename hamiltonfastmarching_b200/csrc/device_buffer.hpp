@@ -18,6 +18,9 @@ namespace hfm {
 
 // Stream on which the calling thread's solve runs (set by the orchestration).
 cudaStream_t &current_stream();
+// The calling thread's persistent solver kernels use 1/share of the device's resident CTAs (a
+// serving lane leaves the rest of the SMs to the lanes that run beside it).
+int &solver_share();
 void keep_pool_cached();
 // Kernel launches issued by this library (all threads), for launch accounting.
 void count_launch(unsigned n = 1);

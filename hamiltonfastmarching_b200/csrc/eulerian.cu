@@ -1391,7 +1391,9 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
         launch(adjoint_roots_kernel, nblocks(N, 256), 256, 0, s, A);
         void *args[] = {&A};
         count_launch();
-            HFM_CUDA(cudaLaunchCooperativeKernel((void *)adjoint_kernel, dim3(nsm * per_sm), dim3(256), args, 0, s));
+            HFM_CUDA(cudaLaunchCooperativeKernel((void *)adjoint_kernel,
+                                                 dim3(std::max(1, nsm * per_sm / std::max(1, solver_share()))),
+                                                 dim3(256), args, 0, s));
         check_status(status, "adjoint");
         AdjointResult ar;
         ar.sensitivity.resize(N);
@@ -1793,7 +1795,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_kernel<Real, NFWD, NSYM, SHARE>,
                                                                kWarpsPerCta * 32, 0));
         if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
-        const int grid = nsm * per_sm;
+        const int grid = std::max(1, nsm * per_sm / std::max(1, solver_share()));
         const double nwarps = (double)grid * kWarpsPerCta;
         const bool ordered = p0.ordered;
         P.order_lo = ordered ? (unsigned)std::max(1.0, p0.band_lo * nwarps) : 0u;

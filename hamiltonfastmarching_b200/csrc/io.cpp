@@ -60,7 +60,7 @@ RawElement &Store::create(const std::string &key) {
 
 std::string Store::get_string(const std::string &key) const {
     const RawElement &r = raw(key);
-    if (!r.data.empty()) throw Error(HFM_ERR_KEY, "BaseIO import error : field " + key + " is not a string.");
+    if (r.count() != 0) throw Error(HFM_ERR_KEY, "BaseIO import error : field " + key + " is not a string.");
     return r.str;
 }
 
@@ -80,6 +80,19 @@ void Store::set_array(const std::string &key, const double *data, const std::vec
     RawElement &r = create(key);
     r.dims = dims;
     r.data.assign(data, data + n);
+}
+
+void Store::set_array_view(const std::string &key, const double *data, const std::vector<int64_t> &dims) {
+    int64_t n = 1;
+    for (int64_t d : dims) {
+        if (d < 0) throw Error(HFM_ERR_VALUE, "negative extent for field " + key);
+        n *= d;
+    }
+    if (n > 0 && !data) throw Error(HFM_ERR_ARG, "null data for field " + key);
+    RawElement &r = create(key);  // a fresh element: no copied data
+    r.dims = dims;
+    r.ext = n > 0 ? data : nullptr;
+    r.ext_n = (size_t)n;
 }
 
 std::string Store::computed_keys() const {
@@ -143,7 +156,7 @@ double Store::get_scalar(const std::string &key) const {
     if (r.is_string()) throw Error(HFM_ERR_KEY, "IO error : key " + key + " is a string, not a numerical field.");
     if (!r.dims.empty())
         throw Error(HFM_ERR_KEY, "IO::Get error : Field " + key + " has incorrect dimensions for this object.");
-    return r.data[0];
+    return r.ptr()[0];
 }
 
 double Store::get_scalar(const std::string &key, double def, int verb) const {
@@ -177,7 +190,7 @@ std::vector<double> Store::get_vector(const std::string &key, int ncomp, int64_t
         throw Error(HFM_ERR_VALUE, "IO::GetArray error : Field " + key + " has depth " + std::to_string(dims.size()) +
                                        " instead of expected 1.");
     *count = dims[0];
-    return std::vector<double>(r.data.begin(), r.data.end());
+    return std::vector<double>(r.ptr(), r.ptr() + r.count());
 }
 
 // Element permutations of the four orderings (IO.hxx:87-110, 153-233).
@@ -248,7 +261,7 @@ Field Store::get_field(const std::string &key, int ndim, int ncomp) const {
     Field f;
     f.ncomp = ncomp;
     if (sd.empty()) {  // DataSource_Value
-        f.data.assign(r.data.begin(), r.data.begin() + ncomp);
+        f.data.assign(r.ptr(), r.ptr() + ncomp);
         return f;
     }
     if ((int)sd.size() != ndim)
@@ -261,21 +274,21 @@ Field Store::get_field(const std::string &key, int ndim, int ncomp) const {
         case Ordering::RowMajor:
             f.dims = sd;
             f.data.clear();
-            f.view = r.data.data();
+            f.view = r.ptr();
             break;
         case Ordering::YXZ_RowMajor:
             f.dims = transpose_dims(sd);
-            permute(r.data.data(), sd, f.dims, ncomp, f.data.data(),
+            permute(r.ptr(), sd, f.dims, ncomp, f.data.data(),
                     [](const std::vector<int64_t> &i) { return transpose_dims(i); });
             break;
         case Ordering::ColumnMajor:
             f.dims = reverse_dims(sd);
-            permute(r.data.data(), sd, f.dims, ncomp, f.data.data(),
+            permute(r.ptr(), sd, f.dims, ncomp, f.data.data(),
                     [](const std::vector<int64_t> &i) { return reverse_dims(i); });
             break;
         case Ordering::YXZ_ColumnMajor:
             f.dims = transpose_dims(reverse_dims(sd));
-            permute(r.data.data(), sd, f.dims, ncomp, f.data.data(),
+            permute(r.ptr(), sd, f.dims, ncomp, f.data.data(),
                     [](const std::vector<int64_t> &i) { return reverse_dims(transpose_dims(i)); });
             break;
     }

@@ -67,9 +67,14 @@ struct RawElement {
     std::string str;
     std::vector<int64_t> dims;
     DoubleArray data;
+    // an array referenced in the caller's memory instead of `data` (set_array_view)
+    const double *ext = nullptr;
+    size_t ext_n = 0;
     Setter setter = Setter::Unknown;
-    bool is_string() const { return data.empty() && dims.empty(); }
-    bool is_scalar() const { return !data.empty() && dims.empty(); }
+    const double *ptr() const { return ext ? ext : data.data(); }
+    size_t count() const { return ext ? ext_n : data.size(); }
+    bool is_string() const { return count() == 0 && dims.empty(); }
+    bool is_scalar() const { return count() != 0 && dims.empty(); }
 };
 
 // A domain field read from the store: RowMajor over `dims` (x, y, z order), `ncomp` components
@@ -104,6 +109,9 @@ public:
     void set_string(const std::string &key, const std::string &val);
     void set_scalar(const std::string &key, double v);
     void set_array(const std::string &key, const double *data, const std::vector<int64_t> &dims);
+    // Like set_array, without copying: the store reads `data` in place until the key is replaced
+    // or erased (the caller keeps it alive and unmodified meanwhile).
+    void set_array_view(const std::string &key, const double *data, const std::vector<int64_t> &dims);
     const RawElement &raw(const std::string &key, bool for_use = true) const;
     std::string computed_keys() const;
     void usage_report();

@@ -17,13 +17,9 @@
 
 #include "common.cuh"
 #include "io.hpp"
+#include "store_handle.hpp"
 #include "solver.hpp"
 
-struct hfm_io {
-    hfm::Store store;
-    std::string last_error;
-    explicit hfm_io(hfm::Ordering o) : store(o) {}
-};
 
 namespace hfm {
 namespace {
@@ -80,7 +76,7 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
     const RawElement &r = io.raw(key);
     if (r.dims.size() != 1 || r.dims[0] != n)
         throw Error(HFM_ERR_VALUE, "Field " + key + " must be a vector of " + std::to_string(n) + " entries");
-    return std::vector<double>(r.data.begin(), r.data.end());
+    return std::vector<double>(r.ptr(), r.ptr() + r.count());
 }
 
 void reject_unsupported(Store &io) {
@@ -547,6 +543,13 @@ int hfm_io_set_array(hfm_io *io, const char *key, const double *data, int ndim, 
     });
 }
 
+int hfm_io_set_array_view(hfm_io *io, const char *key, const double *data, int ndim, const int64_t *shape) {
+    return guarded(io, [&] {
+        if (!key || ndim < 0 || (ndim > 0 && !shape)) throw Error(HFM_ERR_ARG, "null argument");
+        io->store.set_array_view(key, data, std::vector<int64_t>(shape, shape + ndim));
+    });
+}
+
 int hfm_io_get_scalar(hfm_io *io, const char *key, double *value) {
     return guarded(io, [&] {
         if (!key || !value) throw Error(HFM_ERR_ARG, "null argument");
@@ -584,8 +587,8 @@ int hfm_io_get_array(hfm_io *io, const char *key, double *out, size_t count) {
         const hfm::RawElement &r = io->store.raw(key);
         if (r.is_string()) throw Error(HFM_ERR_KEY, "PythonIO error : field " + std::string(key) + " is a string, not an array");
         if (r.dims.empty()) throw Error(HFM_ERR_KEY, "PythonIO error : field " + std::string(key) + " is a scalar, not an array");
-        if (count != r.data.size()) throw Error(HFM_ERR_ARG, "buffer size does not match field " + std::string(key));
-        std::memcpy(out, r.data.data(), count * sizeof(double));
+        if (count != r.count()) throw Error(HFM_ERR_ARG, "buffer size does not match field " + std::string(key));
+        std::memcpy(out, r.ptr(), count * sizeof(double));
     });
 }
 

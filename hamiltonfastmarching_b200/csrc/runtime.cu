@@ -15,6 +15,11 @@ cudaStream_t &current_stream() {
     return s;
 }
 
+int &solver_share() {
+    thread_local int share = 1;
+    return share;
+}
+
 void keep_pool_cached() {
     // Once per device: keep freed blocks of the default pool cached instead of returning them at
     // every synchronisation, so repeated solves do not pay for new device mappings.

@@ -47,13 +47,20 @@ def smooth_field(rng: np.random.Generator, shape, h, K: int = 8, kmax: int = 4,
         k = rng.integers(-kmax, kmax + 1, size=d)
         amp = rng.standard_normal()
         phase = rng.uniform(0.0, 2.0 * math.pi)
-        # cos(sum_d a_d + phase) evaluated by broadcasting 1-D phase ramps
-        arg = np.full((1,) * d, phase, dtype=dtype)
-        for ax in range(d):
-            sh = [1] * d
-            sh[ax] = shape[ax]
-            arg = arg + (2.0 * math.pi * k[ax] * axes[ax]).reshape(sh).astype(dtype)
-        out += amp * np.cos(arg)
+        # cos(A + B) = cos A cos B - sin A sin B, A = phase + ramp of the first axis, B = the
+        # ramps of the other axes summed on their (lower-dimensional) grid
+        A = phase + 2.0 * math.pi * k[0] * axes[0]
+        if d == 1:
+            out += amp * np.cos(A).astype(dtype)
+            continue
+        B = np.zeros(shape[1:])
+        for ax in range(1, d):
+            sh = [1] * (d - 1)
+            sh[ax - 1] = shape[ax]
+            B = B + (2.0 * math.pi * k[ax] * axes[ax]).reshape(sh)
+        sh0 = (shape[0],) + (1,) * (d - 1)
+        cb, sb = np.cos(B)[None], np.sin(B)[None]
+        out += (amp * np.cos(A)).reshape(sh0).astype(dtype) * cb - (amp * np.sin(A)).reshape(sh0).astype(dtype) * sb
     out /= math.sqrt(K)
     return out
 
@@ -224,12 +231,27 @@ def curvature2_case(n: int = 128, ntheta: int = 60, model: str = "ReedsShepp2", 
     }
 
 
-def batched_mix(n_riemann: int = 384, n_lifted: int = 128, ntheta: int = 60, seed: int = 3,
-                side_range=(64, 1024), lifted_range=(64, 256), precision: str = "float32") -> list:
-    """Mixed batch: Riemann2 instances with log-uniform sides, anisotropy U[1,10] and smooth random
-    theta, plus ReedsShepp2 / Elastica2 lifted grids (half each) of N x N x ntheta points with the
-    tubular-image cost 1/(0.05+I), xi = 0.1, eps = 0.1. Each instance has one seed (centre for
-    Riemann2, random oriented point for the lifted models). Returns a list of hfmIn dictionaries.
+def _make(spec):
+    fn, kwargs = spec
+    return globals()[fn](**kwargs)
+
+
+def generate(specs, processes: int = 0) -> list:
+    """Builds the cases of a list of (generator name, keyword arguments) specs, in a pool of
+    ``processes`` worker processes (spawned, so it is safe after CUDA initialisation) when > 1."""
+    if processes and processes > 1 and len(specs) > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(min(processes, len(specs))) as pool:
+            return pool.map(_make, specs, chunksize=1)
+    return [_make(sp) for sp in specs]
+
+
+def batched_mix_specs(n_riemann: int = 384, n_lifted: int = 128, ntheta: int = 60, seed: int = 3,
+                      side_range=(64, 1024), lifted_range=(64, 256)) -> list:
+    """Specs of the mixed batch: Riemann2 instances with log-uniform sides, anisotropy U[1,10] and
+    smooth random theta, plus ReedsShepp2 / Elastica2 lifted grids (half each) of N x N x ntheta
+    points with the tubular-image cost 1/(0.05+I), xi = 0.1, eps = 0.1. One seed per instance
+    (centre for Riemann2, a random oriented point for the lifted models), in a seeded random order.
     """
     rng = np.random.default_rng(seed)
     lo, hi = np.log(side_range[0]), np.log(side_range[1])
@@ -237,17 +259,45 @@ def batched_mix(n_riemann: int = 384, n_lifted: int = 128, ntheta: int = 60, see
     anisos = rng.uniform(1.0, 10.0, n_riemann)
     llo, lhi = np.log(lifted_range[0]), np.log(lifted_range[1])
     lsides = np.exp(rng.uniform(llo, lhi, n_lifted)).round().astype(int)
-    cases = []
+    specs = []
     for k in range(n_riemann):
-        p = riemann2_case(int(sides[k]), aniso=float(anisos[k]), seed=int(seed * 100003 + k))
-        cases.append(p)
+        specs.append(("riemann2_case", dict(n=int(sides[k]), aniso=float(anisos[k]), seed=int(seed * 100003 + k))))
     for k in range(n_lifted):
         model = "ReedsShepp2" if k % 2 == 0 else "Elastica2"
-        p = curvature2_case(int(lsides[k]), ntheta, model, seed=int(seed * 100003 + n_riemann + k), xi=0.1,
-                            eps=0.1)
-        cases.append(p)
-    order = rng.permutation(len(cases))
-    cases = [cases[i] for i in order]
+        specs.append(("curvature2_case", dict(n=int(lsides[k]), ntheta=ntheta, model=model,
+                                              seed=int(seed * 100003 + n_riemann + k), xi=0.1, eps=0.1)))
+    order = rng.permutation(len(specs))
+    return [specs[i] for i in order]
+
+
+def batched_mix(n_riemann: int = 384, n_lifted: int = 128, ntheta: int = 60, seed: int = 3,
+                side_range=(64, 1024), lifted_range=(64, 256), precision: str = "float32",
+                processes: int = 0) -> list:
+    """The mixed batch of ``batched_mix_specs`` as a list of hfmIn dictionaries."""
+    cases = generate(batched_mix_specs(n_riemann, n_lifted, ntheta, seed, side_range, lifted_range), processes)
     for p in cases:
         p["solverPrecision"] = precision
     return cases
+
+
+def serving_specs(n_requests: int, seed: int = 5, ntheta: int = 60) -> list:
+    """Specs of a serving request mix: 60% Riemann2 (sides log-uniform 64-1024), 25% Riemann3
+    (sides 64-192, 40 spherical walls), 15% ReedsShepp2 (N x N x ntheta, N 64-256, tubular-image
+    cost, xi = 0.1); 1-4 random seeds each; every request has its own field seed."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k in range(n_requests):
+        u = rng.uniform()
+        ns = int(rng.integers(1, 5))
+        fs = int(seed * 1000003 + k)
+        if u < 0.60:
+            n = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+            specs.append(("riemann2_case", dict(n=n, aniso=float(rng.uniform(1, 10)), seed=fs, n_seeds=ns)))
+        elif u < 0.85:
+            n = int(round(np.exp(rng.uniform(np.log(64), np.log(192)))))
+            specs.append(("riemann3_case", dict(n=n, seed=fs, n_seeds=ns)))
+        else:
+            n = int(round(np.exp(rng.uniform(np.log(64), np.log(256)))))
+            specs.append(("curvature2_case", dict(n=n, ntheta=ntheta, model="ReedsShepp2", seed=fs, xi=0.1,
+                                                  n_seeds=ns)))
+    return specs

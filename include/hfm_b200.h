@@ -52,6 +52,10 @@ void hfm_io_destroy(hfm_io *io);
 int hfm_io_set_scalar(hfm_io *io, const char *key, double value);
 int hfm_io_set_string(hfm_io *io, const char *key, const char *value);
 int hfm_io_set_array(hfm_io *io, const char *key, const double *data, int ndim, const int64_t *shape);
+/* Zero-copy variant of hfm_io_set_array (an extension: the reference always copies): the store
+ * reads `data` in place, so the caller keeps it alive and unmodified until the key is replaced or
+ * erased, or the store destroyed. Used by request loops that hand large fields to a server. */
+int hfm_io_set_array_view(hfm_io *io, const char *key, const double *data, int ndim, const int64_t *shape);
 
 /* Getters: HFMIO::GetScalar / GetString / GetArray (main.cpp:17-21).
  * hfm_io_get_string copies at most `cap` bytes including the terminating NUL and stores the full
@@ -85,6 +89,42 @@ int hfm_run(hfm_io *io, const char *expected_model);
  * batch neighbours); solver statistics (solverRounds, tileActivations, executedUpdates,
  * GPUSolveTime) are those of the whole batch. Extends the reference's one-instance Run(IO&). */
 int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *codes);
+
+/* ---------------------------------------------------------------------------------------------
+ * Serving (an extension: the reference answers one Run(IO&) at a time). A server owns `lanes`
+ * worker threads, each with its own CUDA stream and 1/lanes of the SMs for the persistent solver.
+ * A free lane takes the waiting requests in arrival order while their estimated device footprint
+ * fits in the memory budget left by the running batches (at most max_batch of them) and solves
+ * them as one hfm_run_batch; requests arriving meanwhile are admitted by the next lane to free up,
+ * so batches overlap on the device (continuous batching). Each request's outputs are written into
+ * its own store, exactly as hfm_run would; the store must stay alive and untouched until the
+ * request is released.
+ */
+typedef struct hfm_server hfm_server;
+typedef struct {
+    int device;              /* CUDA device ordinal                                           */
+    int lanes;               /* concurrent batches (default 2)                                 */
+    int max_batch;           /* requests per batch at most (default 256)                       */
+    double hbm_budget_bytes; /* admission budget; <= 0: 80% of the free device memory          */
+} hfm_server_config;
+typedef struct {
+    unsigned long long submitted, completed, batches, max_batch, queued, running_batches;
+    double budget_bytes, bytes_in_use, peak_bytes;
+} hfm_server_stats;
+
+/* NULL on failure (no device, no memory). */
+hfm_server *hfm_server_create(const hfm_server_config *cfg);
+/* Queues `io` (filled as for hfm_run); HFM_ERR_NOMEM if it alone exceeds the budget. */
+int hfm_server_submit(hfm_server *s, hfm_io *io, uint64_t *ticket);
+/* Waits for a request (timeout_s < 0: no limit); *status receives its hfm_run status.
+ * Returns HFM_ERR_NOT_CONVERGED if the timeout expired first. */
+int hfm_server_wait(hfm_server *s, uint64_t ticket, double timeout_s, int *status);
+/* Forgets a completed request; times (may be NULL) receives submit, start and completion times in
+ * seconds since the server was created. */
+int hfm_server_release(hfm_server *s, uint64_t ticket, double *times);
+int hfm_server_get_stats(hfm_server *s, hfm_server_stats *stats);
+/* Finishes the queued and running requests, then stops the lanes. */
+void hfm_server_destroy(hfm_server *s);
 
 /* Message of the last failure on `io` ("" if none). Valid until the next call on `io`. */
 const char *hfm_io_last_error(hfm_io *io);

@@ -111,3 +111,27 @@ def test_no_host_path_exits_the_process():
     allowed = {"wall_visible"}
     bad = [c for c in callers if not any(a in c for a in allowed)]
     assert not bad, bad
+
+
+def test_server_without_device_fails_cleanly():
+    import ctypes
+    c = ctypes.c_int(0)
+    _lib.load().hfm_device_count(ctypes.byref(c))
+    if c.value > 0:
+        pytest.skip("a CUDA device is present")
+    from hamiltonfastmarching_b200.serving import Server
+    with pytest.raises(RuntimeError):
+        Server(lanes=2)
+
+
+def test_array_view_is_read_in_place():
+    io = H.HFMIO("RowMajor")
+    a = np.arange(12, dtype=np.float64).reshape(3, 4)
+    io.set_array_view("metric", a)
+    assert np.array_equal(io.get_array("metric"), a)
+    a[1, 2] = -7.0  # the store reads the caller's memory
+    assert io.get_array("metric")[1, 2] == -7.0
+    io.set_array("metric", np.zeros((2, 2)))  # replacing the key drops the view
+    assert np.array_equal(io.get_array("metric"), np.zeros((2, 2)))
+    io.set_array_view("empty", np.zeros((0, 3)))
+    assert io.get_array("empty").shape == (0, 3)
