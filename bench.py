@@ -50,6 +50,11 @@ def parse_args(argv=None):
     ap.add_argument("--batch-riemann", type=int, default=384, help="Riemann2 instances of the batched mix")
     ap.add_argument("--batch-lifted", type=int, default=128, help="ReedsShepp2/Elastica2 instances of the mix")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-model leg")
+    ap.add_argument("--serve-rates", default="50,200", help="Poisson arrival rates (req/s) of the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=200, help="requests per arrival rate")
+    ap.add_argument("--serve-pool", type=int, default=48, help="distinct request payloads the arrivals draw from")
+    ap.add_argument("--serve-lanes", type=int, default=2)
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     return ap.parse_args(argv)
 
 
@@ -168,7 +173,8 @@ def batched_leg(args, rank, world):
     import hamiltonfastmarching_b200 as H
     from hamiltonfastmarching_b200 import workloads as W
     t0 = time.perf_counter()
-    cases = W.batched_mix(args.batch_riemann, args.batch_lifted, seed=3 + rank)
+    cases = W.batched_mix(args.batch_riemann, args.batch_lifted, seed=3 + rank,
+                          processes=min(16, os.cpu_count() or 1))
     gen_s = time.perf_counter() - t0
     cells = int(sum(int(np.prod(p["dims"])) for p in cases))
     rng = np.random.default_rng(1234)
@@ -224,6 +230,101 @@ def batched_leg(args, rank, world):
             "speedup_solves_per_s": out["batched"]["solves_per_s"] / out["plain"]["solves_per_s"],
             "fp32_max_rel_err_vs_fp64": max(errs), "fp64_sample": len(sample), "input_generation_s": gen_s,
             "path": "public API from host arrays (H2D/D2H inside both timings)"}
+
+
+# ------------------------------------------------------------------------------- serving leg
+
+def serving_leg(args, rank, world):
+    """Continuous-batching server vs a plain one-at-a-time GPU solve loop on the same arrivals.
+
+    Requests: 60% Riemann2 (64-1024 sides), 25% Riemann3 (64-192, walls), 15% ReedsShepp2
+    (N x N x 60, N 64-256), 1-4 seeds, FP32, drawn from a pool of distinct seeded payloads;
+    Poisson arrivals at each rate. The served arm is hfm_server with `lanes` lanes (batches of the
+    waiting requests, admission by device memory); the plain arm is the same server with one lane
+    and batches of one request (one solve at a time on the whole GPU). Latency = completion - submit
+    (host clock of the server); throughput = requests / (last completion - first submit).
+    """
+    import threading
+    import hamiltonfastmarching_b200 as H
+    from hamiltonfastmarching_b200 import workloads as W
+    from hamiltonfastmarching_b200.serving import Server
+    t0 = time.perf_counter()
+    specs = W.serving_specs(args.serve_pool, seed=5 + rank)
+    pool = W.generate(specs, processes=min(16, os.cpu_count() or 1))
+    for p in pool:
+        p["solverPrecision"] = "float32"
+        p["verbosity"] = 0.0
+        p.pop("exportValues", None)
+        p["exportValues"] = 1.0
+    gen_s = time.perf_counter() - t0
+    cells = [int(np.prod(p["dims"])) for p in pool]
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+
+    def run_arm(lanes, max_batch, rate, seed):
+        rng = np.random.default_rng(seed)
+        picks = rng.integers(0, len(pool), args.serve_requests)
+        gaps = rng.exponential(1.0 / rate, args.serve_requests)
+        tickets = [None] * args.serve_requests
+        lat, done_t, sub_t = [], [], []
+        with Server(lanes=lanes, max_batch=max_batch) as srv:
+            def waiter():
+                for i in range(args.serve_requests):
+                    while tickets[i] is None:
+                        time.sleep(0.0005)
+                    t = tickets[i]
+                    t.wait()
+                    if t.status != 0:
+                        raise RuntimeError(f"request failed with status {t.status}")
+                    sub_t.append(t.times[0])
+                    done_t.append(t.times[2])
+                    lat.append(t.latency)
+                    tickets[i] = False  # drop the store (and its outputs)
+            th = threading.Thread(target=waiter)
+            th.start()
+            start = time.perf_counter()
+            due = start
+            for i in range(args.serve_requests):
+                due += gaps[i]
+                d = due - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets[i] = srv.submit(pool[picks[i]])
+            th.join()
+            st = srv.stats()
+        span = max(done_t) - min(sub_t)
+        ncell = float(sum(cells[k] for k in picks))
+        return {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "mean_ms": 1e3 * float(np.mean(lat)), "solves_per_s": args.serve_requests / span,
+                "cells_per_s": ncell / span, "batches": st["batches"], "max_batch": st["max_batch"],
+                "peak_bytes": st["peak_bytes"]}
+
+    # warm-up of both paths
+    with Server(lanes=args.serve_lanes) as srv:
+        for t in [srv.submit(pool[k]) for k in range(min(4, len(pool)))]:
+            t.wait()
+    out = []
+    for r in rates:
+        served = run_arm(args.serve_lanes, 256, r, seed=11 + int(r))
+        plain = run_arm(1, 1, r, seed=11 + int(r))
+        out.append({"rate_req_per_s": r, "served": served, "plain_one_at_a_time": plain,
+                    "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"],
+                    "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]})
+    # FP32 served results against the FP64 path on a 1% sample (at least 2) of the pool
+    errs = []
+    with Server(lanes=args.serve_lanes) as srv:
+        sample = list(range(0, len(pool), max(1, len(pool) // max(2, len(pool) // 100))))[:max(2, len(pool) // 100)]
+        t32 = [srv.submit(pool[k]) for k in sample]
+        t64 = [srv.submit(dict(pool[k], solverPrecision="float64")) for k in sample]
+        for a, b in zip(t32, t64):
+            v32, v64 = a.result()["values"], b.result()["values"]
+            fin = np.isfinite(v64)
+            errs.append(float(np.max(np.abs(v64[fin] - v32[fin])) / np.max(np.abs(v64[fin]))))
+    return {"workload": "60% Riemann2 (64-1024), 25% Riemann3 (64-192, walls), 15% ReedsShepp2 (N x N x 60, "
+                        "N 64-256), 1-4 seeds, FP32, Poisson arrivals",
+            "requests_per_rate": args.serve_requests, "pool_payloads": len(pool), "lanes": args.serve_lanes,
+            "rates": out, "fp32_max_rel_err_vs_fp64": max(errs), "fp64_sample": len(errs),
+            "input_generation_s": gen_s,
+            "path": "serving.Server (hfm_server C ABI) from host arrays, H2D/D2H inside the latency"}
 
 
 # ------------------------------------------------------------------------------------- our arm
@@ -371,6 +472,9 @@ def run_ours(args):
     batch = None
     if not args.no_batch:
         batch = batched_leg(args, rank, world)
+    serving = None
+    if not args.no_serve:
+        serving = serving_leg(args, rank, world)
 
     if rank == 0:
         line = {
@@ -389,6 +493,7 @@ def run_ours(args):
                      "solve_ms": results[32]["solve_ms"], "max_rel_err_vs_fp64": fp32_err,
                      "clocks": results[32]["clocks"]},
             "batch": batch,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -155,6 +155,7 @@ struct Dev {
     unsigned *status;
     unsigned long long *stats;  // rounds, tile activations, local solves
     int max_rounds;
+    int strict_after;  // rounds after which only decreasing values are accepted
     int sweeps;
 };
 
@@ -396,7 +397,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 // budget is spent (T re-queues itself with the cells still pending).
 template <typename Real, int NFWD, int NSYM, bool SHARE>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
-                                             unsigned long long &n_solves) {
+                                             unsigned long long &n_solves, bool strict) {
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
     int t0, t1, t2;
@@ -450,7 +451,12 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         bool now[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            now[j] = nv[j] != cur[j];
+            // Any change is taken, so that the converged field is the operator's exact fixed point
+            // (independent of the schedule). Rounding can make a recomputation land above the
+            // current value, and changes in both directions could then cycle; after
+            // P.strict_after rounds only decreases are taken, which must terminate (values then
+            // decrease in a finite set), leaving cells within an ulp of that fixed point.
+            now[j] = strict ? nv[j] < cur[j] : nv[j] != cur[j];
             if (now[j]) {
                 cur[j] = nv[j];
                 sv[lane + 32 * j] = nv[j];
@@ -550,7 +556,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
                 continue;
             }
             if (lane == 0) atomicExch(P.key + T, kInfBits);
-            process_tile<Real, NFWD, NSYM, SHARE>(P, T, s_vals[warp], lane, nxt, nslot, n_solves);
+            process_tile<Real, NFWD, NSYM, SHARE>(P, T, s_vals[warp], lane, nxt, nslot, n_solves,
+                                                  r >= P.strict_after);
             ++n_act;
             ++solved;
         }
@@ -1778,6 +1785,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     P.bar_gen = counters.get() + 7;
     P.stats = stats.get();
     P.max_rounds = p0.max_rounds;
+    P.strict_after = 1 << 14;
     P.sweeps = p0.sweeps_per_tile;
     DeviceBuffer<int> stile;
     DeviceBuffer<unsigned long long> smask;
