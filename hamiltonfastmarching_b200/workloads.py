@@ -231,6 +231,69 @@ def curvature2_case(n: int = 128, ntheta: int = 60, model: str = "ReedsShepp2", 
     }
 
 
+def thomsen_tti(vp, eps, delta, dip, azimuth) -> np.ndarray:
+    """TTI metric elements (..., 14) from Thomsen parameters and tilt angles.
+
+    The qP slowness surface is taken in Alkhalifah's acoustic approximation of transversely
+    isotropic media (Geophysics 63(2), 1998; 65(4), 2000): with p_h, p_v the slowness components
+    across and along the symmetry axis,
+        vh^2 p_h^2 + vv^2 p_v^2 - 2 eta vn^2 vv^2 p_h^2 p_v^2 = 1,
+    vv = vp, vh^2 = vp^2 (1 + 2 eps), vn^2 = vp^2 (1 + 2 delta), eta = (eps - delta) / (1 + 2 delta).
+    That is the reference's algebraic form <linear, q> + 1/2 <q, quadratic, q> = 1 with
+    q = (p_h^2, p_v^2): linear = (vh^2, vv^2), quadratic = (0, -2 vp^4 (eps - delta), 0). The
+    transform is the rotation whose last row is the symmetry axis (dip from the vertical, then
+    azimuth), so that its rows give (p_h components, p_v) of a slowness vector.
+    """
+    vp, eps, delta, dip, azimuth = np.broadcast_arrays(*(np.asarray(a, float) for a in (vp, eps, delta, dip, azimuth)))
+    out = np.zeros(vp.shape + (14,))
+    vp2 = vp * vp
+    out[..., 0] = vp2 * (1 + 2 * eps)
+    out[..., 1] = vp2
+    out[..., 2] = 0.0
+    out[..., 3] = -2.0 * vp2 * vp2 * (eps - delta)
+    out[..., 4] = 0.0
+    sd, cd, sa, ca = np.sin(dip), np.cos(dip), np.sin(azimuth), np.cos(azimuth)
+    # rows: e1 = (cd ca, cd sa, -sd), e2 = (-sa, ca, 0), n = (sd ca, sd sa, cd)
+    rows = [(cd * ca, cd * sa, -sd), (-sa, ca, 0 * sd), (sd * ca, sd * sa, cd)]
+    for i in range(3):  # transform(i, j) is element 5 + i + 3 j
+        for j in range(3):
+            out[..., 5 + i + 3 * j] = rows[i][j]
+    return out
+
+
+def tti3_case(n: int = 128, h: float = 0.01, seed: int = 4, vp_scale: float = 1.0, blob=None) -> Dict:
+    """TTI3 on an n^3 grid of spacing h (km): vp = 1.5 + 3 (1/2 + 1/2 tanh(smooth)) km/s,
+    Thomsen eps, delta in [0, 0.2] (delta <= eps) from smooth fields, tilt dip <= 30 degrees and
+    uniform azimuth from smooth fields; one source at the centre of the top face (z = 0).
+    ``blob`` = (centre (3,), radius, amplitude) multiplies vp by 1 + amplitude exp(-|x-c|^2/(2 r^2)).
+    """
+    rng = np.random.default_rng(seed)
+    shape = (n, n, n)
+    L = n * h
+    f = lambda: smooth_field(rng, shape, 1.0 / n)
+    vp = 1.5 + 3.0 * (0.5 + 0.5 * np.tanh(f()))
+    e = 0.2 * (0.5 + 0.5 * np.tanh(f()))
+    d = e * (0.5 + 0.5 * np.tanh(f()))
+    dip = (math.pi / 6) * (0.5 + 0.5 * np.tanh(f()))
+    az = math.pi * (1.0 + np.tanh(f()))
+    if blob is not None:
+        c, r, amp = blob
+        ax = _grid_axes(shape, h)
+        X, Y, Z = np.meshgrid(*ax, indexing="ij")
+        vp = vp * (1.0 + amp * np.exp(-((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) / (2 * r * r)))
+    vp = vp * vp_scale
+    return {
+        "model": "TTI3",
+        "arrayOrdering": "RowMajor",
+        "dims": np.array([n, n, n], dtype=float),
+        "gridScale": h,
+        "metric": thomsen_tti(vp, e, d, dip, az),
+        "seeds": np.array([[L / 2, L / 2, h / 2]]),
+        "exportValues": 1.0,
+        "_vp": vp,
+    }
+
+
 def _make(spec):
     fn, kwargs = spec
     return globals()[fn](**kwargs)

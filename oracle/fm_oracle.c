@@ -775,3 +775,556 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
     free(in_map);
     return nseeds;
 }
+
+/* ========================================================================================== */
+/* TTI3: tilted transversely anisotropic norm, semi-Lagrangian (Lag2) scheme.
+ * Norm: JMM_CPPLibs/JMM_CPPLibs/LinearAlgebra/TTINorm.h:19-28, Implementation/TTINorm.hxx:46-265.
+ * Selling path: JMM_CPPLibs/JMM_CPPLibs/LinearAlgebra/Implementation/BasisReduction.hpp:207-287.
+ * Local solve and neighbours: Headers/Experimental/Implementation/TTI.hpp:24-47, 67-92, 190-318.
+ * Fast marching with the Lag2 policy: a cell is re-solved from all its accepted neighbours
+ * whenever one of its path neighbours is accepted (Headers/Base/Implementation/
+ * HamiltonFastMarching.hxx:136-183, HFM_StencilLag2.hxx). */
+
+/* value, first and second derivative in t (the reference's Diff1 / AD2 types) */
+typedef struct { double v, d, dd; } dual2;
+static inline dual2 d2c(double v) { dual2 r = {v, 0.0, 0.0}; return r; }
+static inline dual2 d2add(dual2 a, dual2 b) { dual2 r = {a.v + b.v, a.d + b.d, a.dd + b.dd}; return r; }
+static inline dual2 d2sub(dual2 a, dual2 b) { dual2 r = {a.v - b.v, a.d - b.d, a.dd - b.dd}; return r; }
+static inline dual2 d2scale(dual2 a, double s) { dual2 r = {a.v * s, a.d * s, a.dd * s}; return r; }
+static inline dual2 d2mul(dual2 a, dual2 b) {
+    dual2 r = {a.v * b.v, a.d * b.v + a.v * b.d, a.dd * b.v + 2.0 * (a.d * b.d) + a.v * b.dd};
+    return r;
+}
+static inline dual2 d2div(dual2 a, dual2 b) {
+    const double q = a.v / b.v;
+    const double qd = (a.d - q * b.d) / b.v;
+    const double qdd = (a.dd - 2.0 * qd * b.d - q * b.dd) / b.v;
+    dual2 r = {q, qd, qdd};
+    return r;
+}
+static inline dual2 d2sqrt(dual2 a) {
+    const double s = sqrt(a.v);
+    const double sd = a.d / (2.0 * s);
+    const double sdd = (a.dd - 2.0 * sd * sd) / (2.0 * s);
+    dual2 r = {s, sd, sdd};
+    return r;
+}
+
+typedef struct {
+    double l0, l1, q00, q01, q11;   /* linear and quadratic coefficients */
+    double D0[6], D1[6];            /* packed symmetric matrices of the extremal ellipsoids */
+    double tmin, tmax;
+    int dir;                        /* optimDirection: -1 inf over t, +1 sup over t */
+} tti_norm;
+
+/* smallest positive s with 0.5 q s^2 + l s - 1 = 0 (TTINorm.hxx:46-60) */
+static double tti_spr(double l, double q) {
+    if (q == 0.0) return 1.0 / l;
+    const double delta = l * l + 2. * q;
+    const double sdelta = sqrt(delta);
+    const double rm = (-l - sdelta) / q, rp = (-l + sdelta) / q;
+    const double rmin = rm < rp ? rm : rp, rmax = rm < rp ? rp : rm;
+    return rmin > 0 ? rmin : rmax;
+}
+
+/* MakeNorm (TTI.hpp:24-34: transform columns scaled by the grid scales), the extremal matrices
+ * of Selling (TTINorm.hxx:89-97, Matrix::Inverse MatrixType.hxx:250-316) and Props
+ * (TTINorm.hxx:62-87). */
+static int tti_setup(const double *m, const double *h, tti_norm *n) {
+    n->l0 = m[0]; n->l1 = m[1];
+    n->q00 = m[2]; n->q01 = m[3]; n->q11 = m[4];
+    /* transform(i, j) is element 5 + i + 3 j of the 14 values: the order in which the reference's
+     * field reader fills its transform (pinned against the reference executable) */
+    double T[3][3], B[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) T[i][j] = m[5 + i + 3 * j] * h[j];
+    double det = 0.0;
+    for (int i = 0; i < 3; ++i)
+        det += T[i][0] * T[(i + 1) % 3][1] * T[(i + 2) % 3][2] - T[i][2] * T[(i + 1) % 3][1] * T[(i + 2) % 3][0];
+    if (!(det != 0.0)) return -1;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            B[j][i] = T[(i + 1) % 3][(j + 1) % 3] * T[(i + 2) % 3][(j + 2) % 3] -
+                      T[(i + 1) % 3][(j + 2) % 3] * T[(i + 2) % 3][(j + 1) % 3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] / det;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j) {
+            n->D0[sym_index(i, j)] = B[0][i] * B[0][j] + B[1][i] * B[1][j];
+            n->D1[sym_index(i, j)] = B[2][i] * B[2][j];
+        }
+    if (!(n->l0 >= 0 && n->l1 >= 0 && n->l0 + n->l1 > 0)) return -1;
+    const double root0 = tti_spr(n->l0, n->q00), root1 = tti_spr(n->l1, n->q11);
+    const double a0 = n->l0 + n->q00 * root0, a1 = n->l1 + n->q01 * root0;
+    const double b0 = n->l0 + n->q01 * root1, b1 = n->l1 + n->q11 * root1;
+    double tmin = a1 / (a0 + a1), tmax = b1 / (b0 + b1);
+    if (tmin < tmax) {
+        n->dir = -1;
+    } else {
+        const double s = tmin; tmin = tmax; tmax = s;
+        n->dir = 1;
+    }
+    n->tmin = tmin; n->tmax = tmax;
+    return (tmin == tmin && tmax == tmax) ? 0 : -1;
+}
+
+/* Multiplier(t): beta such that diag(1-t,t)/beta is tangent to the dual unit ball
+ * (TTINorm.hxx:165-226, general branch). */
+static dual2 tti_multiplier(const tti_norm *n, dual2 t) {
+    if (n->q00 == 0.0 && n->q01 == 0.0 && n->q11 == 0.0) return d2c(1. / (n->l0 + n->l1));
+    const double Q00 = n->q11, Q01 = -n->q01, Q11 = n->q00;   /* comatrix */
+    const double l0 = n->l0, l1 = n->l1;
+    const double Ql0 = Q00 * l0 + Q01 * l1, Ql1 = Q01 * l0 + Q11 * l1;
+    const double detQ = Q00 * Q11 - Q01 * Q01;
+    const double lQl = l0 * Ql0 + l1 * Ql1;
+    const dual2 v0 = d2sub(d2c(1.0), t), v1 = t;
+    const dual2 Qv0 = d2add(d2scale(v0, Q00), d2scale(v1, Q01));
+    const dual2 Qv1 = d2add(d2scale(v0, Q01), d2scale(v1, Q11));
+    const dual2 detVL = d2sub(d2scale(v0, l1), d2scale(v1, l0));
+    const dual2 lQv = d2add(d2scale(Qv0, l0), d2scale(Qv1, l1));
+    const dual2 vQv = d2add(d2mul(v0, Qv0), d2mul(v1, Qv1));
+    const dual2 num = d2add(d2mul(detVL, detVL), d2scale(vQv, 2.0));
+    const double signNum = num.v > 0 ? 1.0 : -1.0;
+    const dual2 delta = d2scale(vQv, 2 * detQ + lQl);
+    if (delta.v < 1e-10) return d2c(tti_spr(n->l0, n->q00) * v0.v);
+    const dual2 den = d2add(d2scale(d2sqrt(delta), signNum), lQv);
+    return d2div(num, den);
+}
+
+typedef struct {
+    int sb[4][3];
+    int off[6][3];
+    double w0[6], w1[6];
+} tti_path;
+
+static void tti_path_weights(const tti_norm *n, tti_path *P) {
+    for (int i = 0, r = 0; i < 4; ++i)
+        for (int j = i + 1; j < 4; ++j, ++r) {
+            P->w0[r] = -sym_scal_int(3, n->D0, P->sb[i], P->sb[j]);
+            P->w1[r] = -sym_scal_int(3, n->D1, P->sb[i], P->sb[j]);
+        }
+}
+
+static void tti_cross(const int *u, const int *v, int *o) {
+    for (int c = 0; c < 3; ++c) {
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        o[c] = u[c1] * v[c2] - u[c2] * v[c1];
+    }
+}
+
+static void tti_complement(int i, int j, int *k, int *l) {
+    int r = 0, kl[2] = {0, 0};
+    for (int q = 0; q < 4; ++q) if (q != i && q != j) kl[r++] = q;
+    *k = kl[0]; *l = kl[1];
+}
+
+static int tti_lin(int i, int j) {  /* LinearizeIndices (BasisReduction.hpp:181-192), i < j */
+    if (i > j) { const int s = i; i = j; j = s; }
+    int r = j - i - 1;
+    if (i == 1) r += 3;
+    else if (i == 2) r += 5;
+    return r;
+}
+
+/* SellingPath(D0, D1, t) (BasisReduction.hpp:213-233) */
+static int tti_path_init(const tti_norm *n, double t, tti_path *P) {
+    double D[6];
+    for (int k = 0; k < 6; ++k) D[k] = (1. - t) * n->D0[k] + t * n->D1[k];
+    if (obtuse_superbase(3, D, P->sb)) return -1;
+    tti_path_weights(n, P);
+    for (int i = 0, r = 0; i < 4; ++i)
+        for (int j = i + 1; j < 4; ++j, ++r) {
+            int k, l;
+            tti_complement(i, j, &k, &l);
+            tti_cross(P->sb[k], P->sb[l], P->off[r]);
+        }
+    return 0;
+}
+
+/* NextStep (BasisReduction.hpp:235-259): t receives the next breakpoint (inf if none). */
+static void tti_next_step(const tti_path *P, double *t, int *in, int *jn) {
+    *t = FMO_INF; *in = -1; *jn = -1;
+    for (int i = 0, r = 0; i < 4; ++i)
+        for (int j = i + 1; j < 4; ++j, ++r) {
+            const double s0 = P->w0[r], s1 = P->w1[r];
+            if (s1 >= s0) continue;
+            if (0 >= s0) continue;
+            const double tr = s0 / (s0 - s1);
+            if (tr >= *t) continue;
+            *t = tr; *in = i; *jn = j;
+        }
+}
+
+/* MakeStep (BasisReduction.hpp:261-285) */
+static void tti_make_step(const tti_norm *n, tti_path *P, int i, int j) {
+    int k, l;
+    tti_complement(i, j, &k, &l);
+    for (int c = 0; c < 3; ++c) {
+        P->sb[k][c] += P->sb[i][c];
+        P->sb[l][c] += P->sb[i][c];
+        P->sb[i][c] = -P->sb[i][c];
+    }
+    tti_cross(P->sb[k], P->sb[l], P->off[tti_lin(i, j)]);
+    int tmp[3];
+    memcpy(tmp, P->off[tti_lin(i, k)], sizeof tmp);
+    memcpy(P->off[tti_lin(i, k)], P->off[tti_lin(i, l)], sizeof tmp);
+    memcpy(P->off[tti_lin(i, l)], tmp, sizeof tmp);
+    tti_path_weights(n, P);
+}
+
+/* UpdateValue (TTINorm.hxx:99-163): sorted-prefix solve of a x^2 - 2 b x + c = 0 with weights
+ * interpolated at t; the scalar pass fixes the prefix, the derivative pass recomputes on it. */
+static dual2 tti_update_value(const tti_norm *n, dual2 t, const double *val, const tti_path *P, int with_ad) {
+    int idx[6];
+    for (int i = 0; i < 6; ++i) idx[i] = i;
+    for (int i = 1; i < 6; ++i) {   /* stable insertion sort by value */
+        const int x = idx[i];
+        int k = i - 1;
+        while (k >= 0 && val[idx[k]] > val[x]) { idx[k + 1] = idx[k]; --k; }
+        idx[k + 1] = x;
+    }
+    const double valMin = val[idx[0]];
+    if (valMin == FMO_INF) return d2c(FMO_INF);
+    const dual2 mult = tti_multiplier(n, t);
+    double a = 0, b = 0, c = -mult.v, sol = FMO_INF;
+    int r = 0;
+    for (; r < 6; ++r) {
+        const int i = idx[r];
+        const double v = val[i] - valMin;
+        if (v >= sol) break;
+        const double w_ = P->w0[i] + t.v * (P->w1[i] - P->w0[i]);
+        const double w = w_ > 0 ? w_ : 0.0, wv = w * v, wvv = wv * v;
+        a += w; b += wv; c += wvv;
+        if (a <= mult.v * 1e-10) continue;
+        const double delta = b * b - a * c;
+        sol = (b + sqrt(delta > 0 ? delta : 0.0)) / a;
+    }
+    if (!with_ad) return d2c(valMin + sol);
+    if (sol == FMO_INF) return d2c(FMO_INF);
+    dual2 A = d2c(0), B = d2c(0), C = d2scale(mult, -1.0);
+    for (int q = 0; q < r; ++q) {
+        const int i = idx[q];
+        const double v = val[i] - valMin;
+        const dual2 w = d2add(d2c(P->w0[i]), d2scale(t, P->w1[i] - P->w0[i]));
+        const dual2 wv = d2scale(w, v), wvv = d2scale(wv, v);
+        A = d2add(A, w); B = d2add(B, wv); C = d2add(C, wvv);
+    }
+    const dual2 delta = d2sub(d2mul(B, B), d2mul(A, C));
+    const dual2 s = d2div(d2add(B, d2sqrt(delta)), A);
+    return d2add(d2c(valMin), s);
+}
+
+/* Neighbour value of the Lag2 scheme: the accepted value, or +inf (TTI.hpp:203-211). */
+typedef double (*tti_getter)(void *ctx, int64_t cell, const int *off);
+
+/* HopfLaxUpdate with nmix = 0 (TTI.hpp:142-276): extremum over t in [tmin, tmax] of the
+ * Riemannian updates of the Selling path, interval by interval, with endpoint tests and a
+ * safeguarded Newton search inside. Returns the value; *t_active, *interior describe the
+ * extremum. Returns +inf if no neighbour is available. */
+static double tti_local_solve(const tti_norm *n, int64_t cell, tti_getter get, void *ctx, double *t_active,
+                              int *interior) {
+    tti_path P;
+    if (tti_path_init(n, n->tmin, &P)) return FMO_INF;
+    double values[6];
+    for (int r = 0; r < 6; ++r) values[r] = -FMO_INF;
+    double t0 = n->tmin;
+    const double objSign = -(double)n->dir;
+    double updateValue = FMO_INF, tAct = FMO_INF;
+    int isInt = 0;
+    for (int guard = 0; guard < 1000; ++guard) {
+        double t1;
+        int ni, nj;
+        tti_next_step(&P, &t1, &ni, &nj);
+        if (t1 > n->tmax) t1 = n->tmax;
+        do {
+            for (int r = 0; r < 6; ++r) {
+                if (values[r] == -FMO_INF) {
+                    int mo[3] = {-P.off[r][0], -P.off[r][1], -P.off[r][2]};
+                    const double vp = get(ctx, cell, P.off[r]), vm = get(ctx, cell, mo);
+                    values[r] = vp < vm ? vp : vm;
+                }
+            }
+            dual2 tt = {t0, 1.0, 0.0};
+            const dual2 val0 = d2scale(tti_update_value(n, tt, values, &P, 1), objSign);
+            if (val0.d >= 0 && val0.v < FMO_INF) {
+                if (val0.v < updateValue) { updateValue = val0.v; tAct = t0; isInt = 0; }
+                break;
+            }
+            tt.v = t1;
+            const dual2 val1 = d2scale(tti_update_value(n, tt, values, &P, 1), objSign);
+            if (val1.d <= 0 && val1.v < FMO_INF) {
+                if (val1.v < updateValue) { updateValue = val1.v; tAct = t1; isInt = 0; }
+                break;
+            }
+            if (isinf(val0.v) && isinf(val1.v)) break;
+            double x0 = t0, x1 = t1, x = (val1.d * t0 - val0.d * t1) / (val1.d - val0.d), xOld = FMO_INF;
+            for (int it = 0; fabs(xOld - x) > 100 * DBL_EPSILON && it < 200; ++it) {
+                xOld = x;
+                dual2 tx = {x, 1.0, 0.0};
+                const dual2 v = d2scale(tti_update_value(n, tx, values, &P, 1), objSign);
+                if (v.d <= 0) x0 = x;
+                else x1 = x;
+                if (v.dd > 0) {
+                    x -= v.d / v.dd;
+                    if (x0 < x && x < x1) continue;
+                }
+                x = (x0 + x1) / 2.;
+            }
+            const double v = objSign * tti_update_value(n, d2c(x), values, &P, 0).v;
+            if (v < updateValue) { updateValue = v; tAct = x; isInt = 1; }
+        } while (0);
+        if (t1 == n->tmax) break;
+        t0 = t1;
+        if (ni < 0) break;
+        tti_make_step(n, &P, ni, nj);
+        const int r = tti_lin(ni, nj);
+        values[r] = -FMO_INF;
+        int k, l;
+        tti_complement(ni, nj, &k, &l);
+        const double s = values[tti_lin(ni, k)];
+        values[tti_lin(ni, k)] = values[tti_lin(ni, l)];
+        values[tti_lin(ni, l)] = s;
+    }
+    if (t_active) *t_active = tAct;
+    if (interior) *interior = isInt;
+    return objSign * updateValue;
+}
+
+/* SetNeighbors (TTI.hpp:67-92): the Selling offsets at tmin and every offset entering along the
+ * path up to tmax (each with its opposite). Returns the number of offsets written (<= cap). */
+static int tti_neighbors(const tti_norm *n, int (*out)[3], int cap) {
+    tti_path P;
+    if (tti_path_init(n, n->tmin, &P)) return -1;
+    int cnt = 0;
+#define PUSH(o)                                                              \
+    do {                                                                     \
+        if (cnt + 2 > cap) return -1;                                        \
+        for (int c_ = 0; c_ < 3; ++c_) { out[cnt][c_] = (o)[c_]; out[cnt + 1][c_] = -(o)[c_]; } \
+        cnt += 2;                                                            \
+    } while (0)
+    for (int r = 0; r < 6; ++r) PUSH(P.off[r]);
+    if (n->tmax == n->tmin) return cnt;
+    double t = n->tmin;
+    for (int guard = 0; guard < 1000; ++guard) {
+        int i, j;
+        tti_next_step(&P, &t, &i, &j);
+        if (t >= n->tmax) break;
+        tti_make_step(n, &P, i, j);
+        PUSH(P.off[tti_lin(i, j)]);
+    }
+#undef PUSH
+    return cnt;
+}
+
+typedef struct {
+    const int64_t *dims;
+    const double *values;
+    const uint8_t *accepted;
+} tti_fm_ctx;
+
+static double tti_fm_get(void *vctx, int64_t cell, const int *off) {
+    const tti_fm_ctx *c = (const tti_fm_ctx *)vctx;
+    const int64_t n1 = c->dims[1], n2 = c->dims[2];
+    const int64_t x0 = cell / (n1 * n2), x1 = (cell / n2) % n1, x2 = cell % n2;
+    const int64_t y0 = x0 + off[0], y1 = x1 + off[1], y2 = x2 + off[2];
+    if (y0 < 0 || y0 >= c->dims[0] || y1 < 0 || y1 >= n1 || y2 < 0 || y2 >= n2) return FMO_INF;
+    const int64_t y = (y0 * n1 + y1) * n2 + y2;
+    return c->accepted[y] ? c->values[y] : FMO_INF;
+}
+
+int fmo_tti_norm(const double *metric, const double *h, double *out) {
+    tti_norm n;
+    if (tti_setup(metric, h, &n)) return -1;
+    out[0] = n.tmin; out[1] = n.tmax; out[2] = n.dir;
+    const dual2 m0 = tti_multiplier(&n, d2c(n.tmin)), m1 = tti_multiplier(&n, d2c(n.tmax));
+    out[3] = m0.v; out[4] = m1.v;
+    return 0;
+}
+
+int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double *metric, int nseeds,
+                              const int64_t *seed_index, const double *seed_value, double *values,
+                              double *t_active) {
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    tti_norm *norms = (tti_norm *)malloc(N * sizeof(tti_norm));
+    uint8_t *accepted = (uint8_t *)calloc(N, 1), *seed = (uint8_t *)calloc(N, 1);
+    enum { CAP = 64 };
+    int (*nb)[3] = (int (*)[3])malloc(sizeof(int) * 3 * CAP);
+    int64_t *rcount = (int64_t *)calloc(N + 1, sizeof(int64_t));
+    int64_t ret = -1;
+    heap_t h_ = {0};
+    int64_t *rcell = NULL;
+    if (!norms || !accepted || !seed || !nb || !rcount) goto done;
+    for (int64_t x = 0; x < N; ++x)
+        if (tti_setup(metric + 14 * x, h, &norms[x])) goto done;
+    /* reversed neighbours: y is re-solved when x = y + o is accepted */
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            for (int64_t x = 0; x < N; ++x) rcount[x + 1] += rcount[x];
+            rcell = (int64_t *)malloc((rcount[N] + 1) * sizeof(int64_t));
+            if (!rcell) goto done;
+        }
+        int64_t *cursor = pass == 1 ? (int64_t *)calloc(N, sizeof(int64_t)) : NULL;
+        for (int64_t y = 0; y < N; ++y) {
+            const int k = tti_neighbors(&norms[y], nb, CAP);
+            if (k < 0) { free(cursor); goto done; }
+            const int64_t y0 = y / (dims[1] * dims[2]), y1 = (y / dims[2]) % dims[1], y2 = y % dims[2];
+            for (int q = 0; q < k; ++q) {
+                const int64_t x0 = y0 + nb[q][0], x1 = y1 + nb[q][1], x2 = y2 + nb[q][2];
+                if (x0 < 0 || x0 >= dims[0] || x1 < 0 || x1 >= dims[1] || x2 < 0 || x2 >= dims[2]) continue;
+                const int64_t x = (x0 * dims[1] + x1) * dims[2] + x2;
+                if (pass == 0) rcount[x + 1]++;
+                else rcell[rcount[x] + cursor[x]++] = y;
+            }
+        }
+        free(cursor);
+    }
+    for (int64_t x = 0; x < N; ++x) { values[x] = FMO_INF; if (t_active) t_active[x] = FMO_INF; }
+    for (int s = 0; s < nseeds; ++s) {
+        values[seed_index[s]] = seed_value[s];
+        seed[seed_index[s]] = 1;
+        qelem q = {seed_index[s], seed_value[s]};
+        if (heap_push(&h_, q)) goto done;
+    }
+    tti_fm_ctx ctx = {dims, values, accepted};
+    int64_t nacc = 0;
+    while (h_.n > 0) {
+        const qelem top = heap_pop(&h_);
+        if (accepted[top.idx] || top.val != values[top.idx]) continue;
+        accepted[top.idx] = 1;
+        ++nacc;
+        for (int64_t k = rcount[top.idx]; k < rcount[top.idx + 1]; ++k) {
+            const int64_t y = rcell[k];
+            if (accepted[y] || seed[y]) continue;
+            if (values[y] <= top.val) continue;  /* ConditionalUpdate, HamiltonFastMarching.hxx:151 */
+            double ta = FMO_INF;
+            int interior = 0;
+            const double v = tti_local_solve(&norms[y], y, tti_fm_get, &ctx, &ta, &interior);
+            if (v < values[y]) {
+                values[y] = v;
+                if (t_active) t_active[y] = interior ? ta : -ta;
+                qelem q = {y, v};
+                if (heap_push(&h_, q)) goto done;
+            }
+        }
+    }
+    ret = nacc;
+done:
+    free(norms); free(accepted); free(seed); free(nb); free(rcount); free(rcell); free(h_.a);
+    return ret;
+}
+
+/* _HopfLaxRecompute at the stored extremum t (TTI.hpp:278-389, order 1): Riemannian update of the
+ * Selling decomposition at t, its value and the discrete flow (offset * sign, (sol - v) w). */
+static double tti_recompute(const tti_norm *n, const int64_t *dims, const double *values, int64_t x, double t,
+                            int64_t *nb, double *nbw, int *nn) {
+    tti_path P;
+    *nn = 0;
+    if (tti_path_init(n, t, &P)) return FMO_INF;
+    const int64_t n1 = dims[1], n2 = dims[2];
+    const int64_t x0 = x / (n1 * n2), x1 = (x / n2) % n1, x2 = x % n2;
+    double val[6];
+    int64_t cell[6];
+    for (int r = 0; r < 6; ++r) {
+        double vs[2] = {FMO_INF, FMO_INF};
+        int64_t cs[2] = {-1, -1};
+        for (int sg = 0; sg < 2; ++sg) {
+            const int s = sg ? -1 : 1;
+            const int64_t y0 = x0 + s * P.off[r][0], y1 = x1 + s * P.off[r][1], y2 = x2 + s * P.off[r][2];
+            if (y0 < 0 || y0 >= dims[0] || y1 < 0 || y1 >= n1 || y2 < 0 || y2 >= n2) continue;
+            cs[sg] = (y0 * n1 + y1) * n2 + y2;
+            vs[sg] = values[cs[sg]];
+        }
+        if (vs[0] < vs[1]) { val[r] = vs[0]; cell[r] = cs[0]; }
+        else { val[r] = vs[1]; cell[r] = cs[1]; }
+    }
+    int idx[6];
+    for (int i = 0; i < 6; ++i) idx[i] = i;
+    for (int i = 1; i < 6; ++i) {
+        const int q = idx[i];
+        int k = i - 1;
+        while (k >= 0 && val[idx[k]] > val[q]) { idx[k + 1] = idx[k]; --k; }
+        idx[k + 1] = q;
+    }
+    const double valMin = val[idx[0]];
+    if (!(valMin < FMO_INF)) return FMO_INF;
+    double a = 0, b = 0, c = -tti_multiplier(n, d2c(t)).v, sol = FMO_INF;
+    int r = 0;
+    for (; r < 6; ++r) {
+        const int i = idx[r];
+        const double v = val[i] - valMin;
+        if (v >= sol) break;
+        const double w = (1 - t) * P.w0[i] + t * P.w1[i];
+        const double wv = w * v, wvv = wv * v;
+        a += w; b += wv; c += wvv;
+        if (a <= 100 * fabs(c) * DBL_EPSILON) continue;
+        const double delta = b * b - a * c;
+        sol = (b + sqrt(delta)) / a;
+    }
+    for (int q = 0; q < r; ++q) {
+        const int i = idx[q];
+        const double v = val[i] - valMin;
+        const double w0 = (1 - t) * P.w0[i] + t * P.w1[i];
+        const double d = (sol - v) * w0;
+        nb[*nn] = cell[i];
+        nbw[*nn] = d > 0 ? d : 0.0;
+        ++*nn;
+    }
+    return sol + valMin;
+}
+
+int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const double *metric,
+                                   const double *values, const double *t_active, int npts,
+                                   const int64_t *pt_index, const double *pt_weight, double *sensitivity,
+                                   int64_t max_seeds, int64_t *seed_out_index, double *seed_out_weight) {
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    double *pend = (double *)calloc(N, sizeof(double));
+    uint8_t *in_map = (uint8_t *)calloc(N, 1);
+    bheap_t hp = {0};
+    if (!pend || !in_map) { free(pend); free(in_map); return -1; }
+    for (int64_t x = 0; x < N; ++x) sensitivity[x] = 0.0;
+    for (int i = 0; i < npts; ++i) {
+        const int64_t x = pt_index[i];
+        if (x < 0 || x >= N || in_map[x]) continue;
+        in_map[x] = 1; pend[x] = pt_weight[i];
+        bheap_push(&hp, (bkey){values[x], x});
+    }
+    int64_t nseeds = 0, nb[6];
+    double nbw[6];
+    while (hp.n > 0) {
+        const bkey k = bheap_pop(&hp);
+        const int64_t x = k.idx;
+        if (!in_map[x]) continue;
+        in_map[x] = 0;
+        const double weight = pend[x];
+        pend[x] = 0.0;
+        if (weight == 0.0) continue;
+        /* ValueVariation, semi-Lagrangian branch (FirstVariation.h:169-196); Recompute returns the
+         * stored value and no flow where no update was recorded (HamiltonFastMarching.hxx:194-195) */
+        int nn = 0;
+        double rec = values[x];
+        if (t_active[x] < FMO_INF) {
+            tti_norm n;
+            if (tti_setup(metric + 14 * x, h, &n)) { nn = 0; }
+            else rec = tti_recompute(&n, dims, values, x, fabs(t_active[x]), nb, nbw, &nn);
+        }
+        double ws = 0.0;
+        for (int j = 0; j < nn; ++j) ws += nbw[j];
+        double valueDiff = rec;
+        for (int j = 0; j < nn; ++j) {
+            nbw[j] = nbw[j] / ws;
+            valueDiff -= nbw[j] * values[nb[j]];
+        }
+        if (nn == 0) {
+            if (nseeds < max_seeds) { seed_out_index[nseeds] = x; seed_out_weight[nseeds] = weight; }
+            ++nseeds;
+        }
+        sensitivity[x] = weight * valueDiff;
+        for (int j = 0; j < nn; ++j) {
+            const int64_t y = nb[j];
+            if (in_map[y]) pend[y] += nbw[j] * weight;
+            else { in_map[y] = 1; pend[y] = nbw[j] * weight; bheap_push(&hp, (bkey){values[y], y}); }
+        }
+    }
+    free(hp.a); free(pend); free(in_map);
+    return nseeds;
+}

@@ -69,6 +69,22 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
  * visible[N][nfwd + 2*nsym] receives 1 if the neighbour (x+e) may update x. */
 int fmo_visibility(const fmo_problem *p, int max_width, uint8_t *visible);
 
+/* TTI3 (semi-Lagrangian, nmix = 0): metric[N][14] = linear(2), quadratic (xx,xy,yy), transform
+ * 3x3 with transform(i, j) at element 5 + i + 3 j; h[3] grid scales. values[N] out, t_active[N] (may be NULL) receives the
+ * reference's activeNeighs encoding (t of the extremum, negative at an interval endpoint).
+ * Returns the accepted count, or -1. */
+int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double *metric, int nseeds,
+                              const int64_t *seed_index, const double *seed_value, double *values,
+                              double *t_active);
+/* Reverse first variation of the TTI3 solve (semi-Lagrangian ValueVariation), from the values and
+ * t_active of fmo_tti_fast_marching. Returns the number of sensitive seeds, or -1. */
+int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const double *metric,
+                                   const double *values, const double *t_active, int npts,
+                                   const int64_t *pt_index, const double *pt_weight, double *sensitivity,
+                                   int64_t max_seeds, int64_t *seed_out_index, double *seed_out_weight);
+/* Properties of one TTI norm: out = {tmin, tmax, optimDirection, Multiplier(tmin), Multiplier(tmax)}. */
+int fmo_tti_norm(const double *metric, const double *h, double *out);
+
 #ifdef __cplusplus
 }
 #endif

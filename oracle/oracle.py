@@ -70,6 +70,12 @@ def lib():
                                              _P, ctypes.c_int64, _P, _P]
         L.fmo_backward_variation.restype = ctypes.c_int64
         L.fmo_visibility.argtypes = [ctypes.POINTER(_Problem), ctypes.c_int, _P]
+        L.fmo_tti_fast_marching.argtypes = [_P, _P, _P, ctypes.c_int, _P, _P, _P, _P]
+        L.fmo_tti_fast_marching.restype = ctypes.c_int64
+        L.fmo_tti_norm.argtypes = [_P, _P, _P]
+        L.fmo_tti_backward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int64,
+                                                 _P, _P]
+        L.fmo_tti_backward_variation.restype = ctypes.c_int64
         _lib = L
     return _lib
 
@@ -310,3 +316,60 @@ def visibility(params: Dict, max_width: int):
     if lib().fmo_visibility(ctypes.byref(P.struct), max_width, _ptr(vis)):
         raise RuntimeError("oracle visibility failed")
     return vis
+
+
+def tti_norm(metric, h):
+    """{tmin, tmax, optimDirection, Multiplier(tmin), Multiplier(tmax)} of one TTI metric element
+    (14 values) at grid scales h (``TTINorm.hxx:62-87, 165-226``)."""
+    m = np.ascontiguousarray(metric, np.float64)
+    hh = np.ascontiguousarray(np.broadcast_to(np.asarray(h, float), (3,)))
+    out = np.zeros(5)
+    if lib().fmo_tti_norm(_ptr(m), _ptr(hh), _ptr(out)) != 0:
+        raise ValueError("invalid TTI metric")
+    return out
+
+
+def tti_solve(params: Dict) -> Dict:
+    """Semi-Lagrangian fast marching of a TTI3 ``params`` dictionary (RowMajor arrays)."""
+    dims = tuple(int(round(d)) for d in np.asarray(params["dims"]).ravel())
+    hs = np.asarray(params.get("gridScales", [params.get("gridScale", 1.0)] * 3), float)
+    hs = np.ascontiguousarray(np.broadcast_to(hs, (3,)))
+    origin = np.asarray(params.get("origin", np.zeros(3)), float)
+    metric = np.ascontiguousarray(np.broadcast_to(np.asarray(params["metric"], float), dims + (14,)))
+    sidx, sval = _seed_indices(params, lambda p: (np.asarray(p) - origin) / hs, dims, [0, 0, 0])
+    n = int(np.prod(dims))
+    values = np.empty(n)
+    tact = np.empty(n)
+    d = np.array(dims, np.int64)
+    nacc = lib().fmo_tti_fast_marching(_ptr(d), _ptr(hs), _ptr(metric), len(sidx), _ptr(sidx), _ptr(sval),
+                                       _ptr(values), _ptr(tact))
+    if nacc < 0:
+        raise RuntimeError("oracle TTI fast marching failed")
+    return {"values": values.reshape(dims), "activeNeighs": tact.reshape(dims), "nAccepted": int(nacc),
+            "_tti": (d, hs, metric, origin)}
+
+
+def tti_backward_variation(res: Dict, points, weights=None):
+    """Reverse first variation of a :func:`tti_solve` result from weighted physical points.
+    Returns (costSensitivity, seed indices, seed weights)."""
+    d, hs, metric, origin = res["_tti"]
+    dims = tuple(int(x) for x in d)
+    pts = np.atleast_2d(np.asarray(points, float))
+    w = np.ones(len(pts)) if weights is None else np.asarray(weights, float).ravel()
+    idx = []
+    for q in pts:
+        i = np.floor((q - origin) / hs).astype(np.int64)
+        idx.append(int(np.ravel_multi_index(tuple(i), dims)) if np.all((i >= 0) & (i < dims)) else -1)
+    idx = np.asarray(idx, np.int64)
+    values = np.ascontiguousarray(res["values"].ravel())
+    tact = np.ascontiguousarray(res["activeNeighs"].ravel())
+    sens = np.empty(values.size)
+    cap = 1 << 16
+    si = np.empty(cap, np.int64)
+    sw = np.empty(cap)
+    ns = lib().fmo_tti_backward_variation(_ptr(d), _ptr(hs), _ptr(metric), _ptr(values), _ptr(tact), len(idx),
+                                          _ptr(idx), _ptr(np.ascontiguousarray(w)), _ptr(sens), cap, _ptr(si),
+                                          _ptr(sw))
+    if ns < 0:
+        raise RuntimeError("oracle TTI backward variation failed")
+    return sens.reshape(dims), si[:ns], sw[:ns]

@@ -147,5 +147,19 @@ def main():
                   (pts[:2], rng.uniform(0.5, 2.0, 2)))
 
 
+def tti_fixtures():
+    """TTI3 16^3 (Thomsen parameters, tilted axis) with 6 weighted receivers on the top face."""
+    p = W.tti3_case(16, h=0.01, seed=4)
+    p.pop("_vp")
+    rng = np.random.default_rng(77)
+    pts = np.c_[rng.uniform(0.0, 0.16, (6, 2)), np.full((6, 1), 0.005)]
+    solve_fixture("tti3_16", p, (pts, rng.uniform(0.5, 2.0, 6)))
+
+
 if __name__ == "__main__":
-    main()
+    # `make_golden.py tti` regenerates only the TTI3 fixture
+    if sys.argv[1:] == ["tti"]:
+        tti_fixtures()
+    else:
+        main()
+        tti_fixtures()

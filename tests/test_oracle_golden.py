@@ -49,3 +49,23 @@ def test_oracle_stencils_match_reference(name):
     ref_w = extra["stencil_weights_6digits"]
     np.testing.assert_array_equal(off[..., :ndim].astype(np.int64), ref_off)
     np.testing.assert_allclose(w, ref_w, rtol=5e-6, atol=0)
+
+
+def test_tti_oracle_matches_reference():
+    """TTI3 (semi-Lagrangian, interval-wise Newton over the Selling path): values within 1e-14 and
+    the reverse first variation within 1e-12 of the reference executable (the extremum over t is
+    found by an iterative search whose last digits depend on the order of operations)."""
+    params, ref, _ = load_golden("tti3_16")
+    res = O.tti_solve(params)
+    a, b = ref["values"], res["values"]
+    assert np.array_equal(np.isinf(a), np.isinf(b))
+    fin = np.isfinite(a)
+    assert np.max(np.abs(a[fin] - b[fin])) <= 1e-14 * np.max(np.abs(a[fin]))
+    assert np.mean(a[fin] == b[fin]) > 0.3
+    assert int(ref["nAccepted"]) == res["nAccepted"]
+    sens, si, sw = O.tti_backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
+    rs = ref["costSensitivity_0"]
+    assert np.max(np.abs(sens - rs)) <= 1e-12 * np.max(np.abs(rs))
+    seeds = ref["seedSensitivity_0"]
+    assert len(seeds) == len(si)
+    np.testing.assert_allclose(seeds[:, -1], sw, rtol=1e-12)
