@@ -80,6 +80,9 @@ namespace detail {
 constexpr unsigned kVisPlus = 1u << 24, kVisMinus = 1u << 25, kFixed = 1u << 28, kDead = 1u << 29;
 constexpr unsigned kShFixed = 1u << 30, kShDead = 1u << 31;
 constexpr int kWarpsPerCta = 4;
+// Stencil families of the solver kernels (the KIND template parameter): per-cell Riemann
+// stencils, shared per-angle stencils (curvature models), per-cell TTI Selling paths.
+constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2;
 constexpr int kDepWarps = 2;
 constexpr int kDepCap = 1024;
 constexpr unsigned long long kBarrierPolls = 1ull << 25;
@@ -218,9 +221,10 @@ __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real 
 // Local solve at one cell. `sv` holds the current values of the warp's tile (nullptr: read all
 // neighbours from global memory). `side` receives, per symmetric difference, 1 if the -e
 // neighbour provided the candidate.
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1, int x2,
                                            int tx0, int tx1, int tx2, const Real *sv, unsigned *used, unsigned *side) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     using A = Arith<Real>;
     const Real INF = A::inf();
@@ -284,8 +288,9 @@ __device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, lo
     return hopf_lax_sorted<Real, ND>(v, w, used);
 }
 
-template <typename Real, bool SHARE>
+template <typename Real, int KIND>
 __device__ __forceinline__ void cell_flags(const Dev<Real> &P, long long c, bool &fixed, bool &dead) {
+    constexpr bool SHARE = KIND == kKindShare;
     if (SHARE) {
         const unsigned f = P.vis[c];
         fixed = f & kShFixed;
@@ -355,9 +360,10 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
 }
 
 // Cells of the warp's tile that the cell at (x0,x1,x2) reads through its visible stencil entries.
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, const Inst &I, long long c, int x0,
                                                            int x1, int x2, int tx0, int tx1, int tx2) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     const GridGeom &g = I.g;
     unsigned long long m = 0;
@@ -395,9 +401,10 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 // One activation of tile T: solve the dirty cells, then, sweep after sweep, the cells reading an
 // in-tile cell that changed in the previous sweep, until nothing changes (warp vote) or the sweep
 // budget is spent (T re-queues itself with the cells still pending).
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves, bool strict) {
+    constexpr bool SHARE = KIND == kKindShare;
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
     int t0, t1, t2;
@@ -422,11 +429,11 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         const bool valid = xs[j][0] < g.dims[0] && xs[j][1] < g.dims[1] && xs[j][2] < g.dims[2];
         bool fixed = true, dead = true;
         const long long c = (long long)T * 64 + l;
-        if (valid) cell_flags<Real, SHARE>(P, c, fixed, dead);
+        if (valid) cell_flags<Real, KIND>(P, c, fixed, dead);
         gi[j] = valid ? I.cell0 + g.lin(xs[j][0], xs[j][1], xs[j][2]) : 0;
         cur[j] = (valid && !dead) ? __ldcg(P.values + gi[j]) : INF;
         upd[j] = valid && !dead && !fixed;
-        if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, SHARE>(P, I, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
+        if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, KIND>(P, I, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
         todo[j] = upd[j] && ((dirty >> l) & 1ull);
         sv[l] = cur[j];
     }
@@ -439,7 +446,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 #pragma unroll 1
         for (int j = 0; j < 2; ++j) {
             if (j ? todo[1] : todo[0]) {
-                const Real r = solve_cell<Real, NFWD, NSYM, SHARE>(
+                const Real r = solve_cell<Real, NFWD, NSYM, KIND>(
                     P, I, (long long)T * 64 + lane + 32 * j, j ? xs[1][0] : xs[0][0], j ? xs[1][1] : xs[0][1],
                     j ? xs[1][2] : xs[0][2], tx0, tx1, tx2, sv, nullptr, nullptr);
                 if (j) nv[1] = r;
@@ -509,13 +516,15 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 // Resident CTAs per SM requested from the register allocator (measured on B200: the solve is
 // latency-bound, and more resident warps beat the spills this costs, except for the 27-offset
 // Elastica stencil whose local solve needs the registers).
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 constexpr int fim_min_blocks() {
+    constexpr bool SHARE = KIND == kKindShare;
     return SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 6;
 }
 
-template <typename Real, int NFWD, int NSYM, bool SHARE>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD, NSYM, SHARE>())) fim_kernel(Dev<Real> P) {
+template <typename Real, int NFWD, int NSYM, int KIND>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD, NSYM, KIND>())) fim_kernel(Dev<Real> P) {
+    constexpr bool SHARE = KIND == kKindShare;
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long kInfBits = 0x7ff0000000000000ull;
@@ -556,7 +565,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
                 continue;
             }
             if (lane == 0) atomicExch(P.key + T, kInfBits);
-            process_tile<Real, NFWD, NSYM, SHARE>(P, T, s_vals[warp], lane, nxt, nslot, n_solves,
+            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves,
                                                   r >= P.strict_after);
             ++n_act;
             ++solved;
@@ -796,8 +805,9 @@ __device__ bool wall_visible(const GridGeom &g, const int8_t *wd, int b0, int b1
 // Visibility bits of every (cell, neighbour slot): the neighbour y = x + s e may update x iff the
 // difference has non-zero weight, y lies in the domain, and Visible(y, -s e, x) holds
 // (ConditionalUpdate, HamiltonFastMarching.hxx:136-154). Also marks padding cells dead.
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8_t *cls_enabled) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= P.ntc) return;
@@ -846,8 +856,9 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
     if (SHARE) P.vis[c] = visw;
 }
 
-template <typename Real, bool SHARE>
+template <typename Real, int KIND>
 __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *val, int n) {
+    constexpr bool SHARE = KIND == kKindShare;
     // idx: global cell indices
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -862,10 +873,11 @@ __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *va
 // Tile dependency graph. Pass 0 counts, pass 1 writes, for every tile D, the distinct source
 // tiles T != D its visible stencil entries read, with the 64-bit mask of the cells read in T.
 
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void __launch_bounds__(kDepWarps * 32)
     deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
                 unsigned long long *msk, unsigned long long *dmsk) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     __shared__ int keys[kDepWarps][kDepCap];
     __shared__ unsigned long long masks[kDepWarps][kDepCap];
@@ -1007,8 +1019,9 @@ __global__ void count_finite_kernel(Dev<Real> P, unsigned long long *out) {
 // at bit k, symmetric difference j at bits nfwd+2j (+e) and nfwd+2j+1 (-e). A used forward
 // difference also marks the other forward differences with the same offset, as the reference's
 // update adds every difference matching the accepted offset (EulerianStencil.hxx:114-123).
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= P.ncells) return;
@@ -1018,11 +1031,11 @@ __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
     const long long c = R.c;
     const long long cls = I.cls0 + x2;
     bool fixed, dead;
-    cell_flags<Real, SHARE>(P, c, fixed, dead);
+    cell_flags<Real, KIND>(P, c, fixed, dead);
     unsigned long long bits = 0;
     if (!fixed && !dead) {
         unsigned used = 0, side = 0;
-        solve_cell<Real, NFWD, NSYM, SHARE>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+        solve_cell<Real, NFWD, NSYM, KIND>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
         for (int k = 0; k < ND; ++k) {
             if (!((used >> k) & 1u)) continue;
             if (k < NFWD) {
@@ -1090,8 +1103,9 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
 // by decreasing downwind value, the order in which the reference's traversal adds them
 // (FirstVariation.h:341-385): the result does not depend on the schedule.
 
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
+    constexpr bool SHARE = KIND == kKindShare;
     // the adjoint runs on a batch of one instance
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
@@ -1106,13 +1120,13 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
     const int x0 = (int)(r / g.dims[1]);
     const long long c = (I.tile0 + g.tile_of(x0, x1, x2)) * 64 + g.local_of(x0, x1, x2);
     bool fixed, dead;
-    cell_flags<Real, SHARE>(P, c, fixed, dead);
+    cell_flags<Real, KIND>(P, c, fixed, dead);
     const double u = (double)P.values[x];
     nflow[x] = 0;
     var[x] = 0.0;
     if (fixed || dead || !(u < Arith<double>::inf())) return;
     unsigned used = 0, side = 0;
-    solve_cell<Real, NFWD, NSYM, SHARE>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+    solve_cell<Real, NFWD, NSYM, KIND>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
     double m = 1.0;
     if (SHARE) m = (double)P.mult[c];
     double ws = 0.0, v = 0.0;
@@ -1309,9 +1323,10 @@ __global__ void flow_sort_kernel(long long N, const long long *rptr, int *rx, do
     }
 }
 
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
                  DeviceBuffer<unsigned> &status, cudaStream_t s) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     constexpr int NF = 2 * ND > 32 ? 32 : 2 * ND;
     if (N >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large for the adjoint");
@@ -1319,7 +1334,7 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     DeviceBuffer<double> fw((size_t)NF * N), var(N), acc(N), sens(N);
     DeviceBuffer<uint8_t> nflow(N);
     indeg0.zero(s);
-    launch(flow_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, fidx.get(), fw.get(), var.get(),
+    launch(flow_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, P, fidx.get(), fw.get(), var.get(),
                                                                           nflow.get(), indeg0.get());
     HFM_CUDA(cudaGetLastError());
     // reverse adjacency (CSR over y, offsets scanned on the host)
@@ -1425,8 +1440,9 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     }
 }
 
-template <typename Real, int NFWD, int NSYM, bool SHARE>
+template <typename Real, int NFWD, int NSYM, int KIND>
 void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
+    constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     constexpr int NB = NFWD + 2 * NSYM;
     const auto wall_t0 = std::chrono::steady_clock::now();
@@ -1666,7 +1682,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_CUDA(cudaGetLastError());
     }
     HFM_TRACE("walls");
-    launch(visibility_kernel<Real, NFWD, NSYM, SHARE>, nblocks(ntc, 128), 128, 0, s, P, wd8.get(), cls_en.get());
+    launch(visibility_kernel<Real, NFWD, NSYM, KIND>, nblocks(ntc, 128), 128, 0, s, P, wd8.get(), cls_en.get());
     HFM_CUDA(cudaGetLastError());
     wdist.release();
     HFM_TRACE("visibility");
@@ -1703,13 +1719,13 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     if (ns) {
         sidx.upload(hsi, s);
         sval.upload(hsv, s);
-        launch(seeds_kernel<Real, SHARE>, nblocks(ns, 128), 128, 0, s, P, sidx.get(), sval.get(), ns);
+        launch(seeds_kernel<Real, KIND>, nblocks(ns, 128), 128, 0, s, P, sidx.get(), sval.get(), ns);
     }
     HFM_TRACE("seeds");
 
     // ---- tile dependency graph (reverse CSR over the global tile space)
     DeviceBuffer<unsigned> dcnt(nt);
-    launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 0, dcnt.get(),
+    launch(deps_kernel<Real, NFWD, NSYM, KIND>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 0, dcnt.get(),
            nullptr, nullptr, nullptr, nullptr, nullptr);
     HFM_CUDA(cudaGetLastError());
     DeviceBuffer<long long> doff(nt + 1), rptr(nt + 1);
@@ -1728,7 +1744,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         DeviceBuffer<int> esrc(nE), edst(nE);
         DeviceBuffer<unsigned long long> emsk(nE), edmsk(nE);
         if (nE)
-            launch(deps_kernel<Real, NFWD, NSYM, SHARE>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 1, nullptr,
+            launch(deps_kernel<Real, NFWD, NSYM, KIND>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 1, nullptr,
                    doff.get(), esrc.get(), edst.get(), emsk.get(), edmsk.get());
         DeviceBuffer<unsigned> rcnt(nt), cursor(nt);
         rcnt.zero(s);
@@ -1800,7 +1816,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         int dev = 0, nsm = 0, per_sm = 0;
         HFM_CUDA(cudaGetDevice(&dev));
         HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_kernel<Real, NFWD, NSYM, SHARE>,
+        HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_kernel<Real, NFWD, NSYM, KIND>,
                                                                kWarpsPerCta * 32, 0));
         if (per_sm < 1) throw Error(HFM_ERR_CUDA, "solver kernel cannot be resident");
         const int grid = std::max(1, nsm * per_sm / std::max(1, solver_share()));
@@ -1810,7 +1826,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         P.order_hi = ordered ? (unsigned)std::max(2.0, p0.band_hi * nwarps) : 0u;
         void *args[] = {&P};
         count_launch();
-        HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, SHARE>, dim3(grid),
+        HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, KIND>, dim3(grid),
                                              dim3(kWarpsPerCta * 32), args, 0, s));
     }
     HFM_TRACE("fim kernel");
@@ -1834,7 +1850,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     DeviceBuffer<unsigned long long> act;
     if (want_active) {
         act.alloc(N);
-        launch(active_kernel<Real, NFWD, NSYM, SHARE>, nblocks(N, 128), 128, 0, s, P, act.get());
+        launch(active_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, P, act.get());
     }
     for (int i = 0; i < ninst; ++i) {
         const EulerProblem &p = *probs[i];
@@ -1874,7 +1890,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     HFM_TRACE("outputs");
     if (ninst == 1 && !p0.adjoint_index.empty()) {
         tm.start(s);
-        run_adjoint<Real, NFWD, NSYM, SHARE>(P, N, p0, results[0], status, s);
+        run_adjoint<Real, NFWD, NSYM, KIND>(P, N, p0, results[0], status, s);
         results[0].t_adjoint_ms = tm.stop(s);
     }
     HFM_CUDA(cudaStreamSynchronize(s));
@@ -1899,21 +1915,21 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
     }
     if (p.kind == StencilKind::RiemannPerCell) {
         if (p.ndim == 2) {
-            if (p.fp64) run_batch_impl<double, 0, 3, false>(probs, results);
-            else run_batch_impl<float, 0, 3, false>(probs, results);
+            if (p.fp64) run_batch_impl<double, 0, 3, detail::kKindRiemann>(probs, results);
+            else run_batch_impl<float, 0, 3, detail::kKindRiemann>(probs, results);
         } else if (p.ndim == 3) {
-            if (p.fp64) run_batch_impl<double, 0, 6, false>(probs, results);
-            else run_batch_impl<float, 0, 6, false>(probs, results);
+            if (p.fp64) run_batch_impl<double, 0, 6, detail::kKindRiemann>(probs, results);
+            else run_batch_impl<float, 0, 6, detail::kKindRiemann>(probs, results);
         } else {
             throw Error(HFM_ERR_UNSUPPORTED, "Riemann models support dimensions 2 and 3");
         }
     } else {
         if (p.nfwd == 0 && p.nsym == 4) {
-            if (p.fp64) run_batch_impl<double, 0, 4, true>(probs, results);
-            else run_batch_impl<float, 0, 4, true>(probs, results);
+            if (p.fp64) run_batch_impl<double, 0, 4, detail::kKindShare>(probs, results);
+            else run_batch_impl<float, 0, 4, detail::kKindShare>(probs, results);
         } else if (p.nfwd == 27 && p.nsym == 0) {
-            if (p.fp64) run_batch_impl<double, 27, 0, true>(probs, results);
-            else run_batch_impl<float, 27, 0, true>(probs, results);
+            if (p.fp64) run_batch_impl<double, 27, 0, detail::kKindShare>(probs, results);
+            else run_batch_impl<float, 27, 0, detail::kKindShare>(probs, results);
         } else {
             throw Error(HFM_ERR_UNSUPPORTED, "unsupported shared stencil shape");
         }

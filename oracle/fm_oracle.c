@@ -1328,3 +1328,24 @@ int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const d
     free(hp.a); free(pend); free(in_map);
     return nseeds;
 }
+
+/* Number of distinct offsets (up to sign) of SetNeighbors for each cell; -1 if invalid. */
+int fmo_tti_neighbor_counts(int64_t n, const double *metric, const double *h, int *counts) {
+    int nb[64][3];
+    for (int64_t x = 0; x < n; ++x) {
+        tti_norm nm;
+        if (tti_setup(metric + 14 * x, h, &nm)) { counts[x] = -1; continue; }
+        const int k = tti_neighbors(&nm, nb, 64);
+        if (k < 0) { counts[x] = -1; continue; }
+        int distinct = 0;
+        for (int q = 0; q < k; q += 2) {
+            int dup = 0;
+            for (int r = 0; r < q; r += 2)
+                if ((nb[r][0] == nb[q][0] && nb[r][1] == nb[q][1] && nb[r][2] == nb[q][2]) ||
+                    (nb[r][0] == -nb[q][0] && nb[r][1] == -nb[q][1] && nb[r][2] == -nb[q][2])) dup = 1;
+            distinct += !dup;
+        }
+        counts[x] = distinct;
+    }
+    return 0;
+}
