@@ -12,6 +12,11 @@ Cost semantics follow the reference:
 * Riemann2/Riemann3: ``cost`` is a positive local multiplier rho(x) of the norm, the metric used
   being rho^2 * metric; the reference's costSensitivity is the derivative with respect to a relative
   change of the local norm, so d/d(rho) = costSensitivity / rho.
+* TTI3: ``cost`` is a positive local multiplier c(x) of the norm (c = vp_ref / vp for a velocity
+  change at fixed anisotropy and tilt): the dual unit ball <l, q> + 1/2 <q, Q q> = 1 becomes
+  <l / c^2, q> + 1/2 <q, Q / c^4 q> = 1. The reference's costSensitivity (semi-Lagrangian
+  ValueVariation, FirstVariation.h:169-196) is the derivative with respect to c at c = 1; here the
+  multiplier is applied to the metric, so d/dc = costSensitivity / c.
 
 Sensitivities are exact for the discrete scheme (piecewise linear in the cost); the gradient is
 that of the discrete arrival times.
@@ -31,13 +36,19 @@ _CURVATURE = ("ReedsShepp2", "Elastica2")
 
 
 def _with_cost(params: Dict, cost: np.ndarray) -> Dict:
-    p = dict(params)
+    p = {k: v for k, v in params.items() if not k.startswith("_")}
     p.setdefault("arrayOrdering", "RowMajor")
     p["verbosity"] = 0.0
     p["exportValues"] = 1.0
     if p["model"] in _CURVATURE:
         p["cost"] = cost
         p.pop("speed", None)
+    elif p["model"] == "TTI3":
+        metric = np.array(p["metric"], dtype=np.float64)
+        c2 = (cost * cost)[..., None]
+        metric[..., 0:2] /= c2
+        metric[..., 2:5] /= c2 * c2
+        p["metric"] = metric
     else:
         metric = np.asarray(p["metric"], dtype=np.float64)
         p["metric"] = metric * (cost[..., None] ** 2)

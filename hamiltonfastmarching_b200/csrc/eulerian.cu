@@ -30,6 +30,7 @@
 
 #include "device_buffer.hpp"
 #include "selling.cuh"
+#include "tti.cuh"
 #include "solver.hpp"
 
 namespace hfm {
@@ -147,6 +148,7 @@ struct Dev {
     // per instance: key = value * kscale, so that the keys of a batch measure the progress of each
     // instance's front on a common scale (nullptr: keys are the values)
     const double *kscale;
+    const TTICell *tti;                    // [ntc] TTI norms (TTI kind)
     unsigned order_lo, order_hi;           // tiles solved per round kept in [lo, hi]; lo = 0: plain FIM
     // active-tile lists (triple buffered) and their dedupe flags
     int *list[3];
@@ -222,9 +224,10 @@ __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real 
 // neighbours from global memory). `side` receives, per symmetric difference, 1 if the -e
 // neighbour provided the candidate.
 template <typename Real, int NFWD, int NSYM, int KIND>
-__device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1, int x2,
-                                           int tx0, int tx1, int tx2, const Real *sv, unsigned *used, unsigned *side) {
-    constexpr bool SHARE = KIND == kKindShare;
+__device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1,
+                                                   int x2, int tx0, int tx1, int tx2, const Real *sv, unsigned *used,
+                                                   unsigned *side) {
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     using A = Arith<Real>;
     const Real INF = A::inf();
@@ -288,9 +291,44 @@ __device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, lo
     return hopf_lax_sorted<Real, ND>(v, w, used);
 }
 
+// TTI local solve at one cell (FP64): neighbour values from the tile in shared memory or global
+// memory, +inf outside the domain.
+template <typename Real>
+__device__ __forceinline__ Real solve_cell_tti(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1, int x2,
+                                               int tx0, int tx1, int tx2, const Real *sv, double *t_act,
+                                               bool *interior) {
+    const GridGeom &g = I.g;
+    const Real *values = P.values + I.cell0;
+    auto get = [&](int o0, int o1, int o2) -> double {
+        const int n0 = x0 + o0, n1 = x1 + o1, n2 = x2 + o2;
+        if ((unsigned)n0 >= (unsigned)g.dims[0] || (unsigned)n1 >= (unsigned)g.dims[1] ||
+            (unsigned)n2 >= (unsigned)g.dims[2])
+            return Arith<double>::inf();
+        if (sv) {
+            const unsigned l0 = n0 - tx0, l1 = n1 - tx1, l2 = n2 - tx2;
+            if (l0 < (1u << g.tshift[0]) && l1 < (1u << g.tshift[1]) && l2 < (1u << g.tshift[2]))
+                return (double)sv[((l0 << g.tshift[1] | l1) << g.tshift[2]) | l2];
+        }
+        return (double)__ldcg(values + g.lin(n0, n1, n2));
+    };
+    return (Real)tti_solve(P.tti[c], get, t_act, interior);
+}
+
+template <typename Real, int NFWD, int NSYM, int KIND>
+__device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1, int x2,
+                                           int tx0, int tx1, int tx2, const Real *sv, unsigned *used, unsigned *side) {
+    if constexpr (KIND == kKindTTI) {
+        if (used) *used = 0;
+        if (side) *side = 0;
+        return solve_cell_tti<Real>(P, I, c, x0, x1, x2, tx0, tx1, tx2, sv, nullptr, nullptr);
+    } else {
+        return solve_cell_stencil<Real, NFWD, NSYM, KIND>(P, I, c, x0, x1, x2, tx0, tx1, tx2, sv, used, side);
+    }
+}
+
 template <typename Real, int KIND>
 __device__ __forceinline__ void cell_flags(const Dev<Real> &P, long long c, bool &fixed, bool &dead) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     if (SHARE) {
         const unsigned f = P.vis[c];
         fixed = f & kShFixed;
@@ -363,7 +401,7 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, const Inst &I, long long c, int x0,
                                                            int x1, int x2, int tx0, int tx1, int tx2) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     const GridGeom &g = I.g;
     unsigned long long m = 0;
@@ -404,7 +442,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves, bool strict) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
     int t0, t1, t2;
@@ -518,13 +556,13 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 // Elastica stencil whose local solve needs the registers).
 template <typename Real, int NFWD, int NSYM, int KIND>
 constexpr int fim_min_blocks() {
-    constexpr bool SHARE = KIND == kKindShare;
-    return SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 6;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    return KIND == kKindTTI ? 1 : SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 6;
 }
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD, NSYM, KIND>())) fim_kernel(Dev<Real> P) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long kInfBits = 0x7ff0000000000000ull;
@@ -669,6 +707,58 @@ __global__ void riemann_stencil_kernel(Dev<Real> P, const double *metric, int8_t
     }
 }
 
+// One thread per cell: the TTI norm (tile-major) and the distinct offsets of its Selling path as
+// the cell's stencil slots (weight 1; unused slots weight 0), for the visibility and dependency
+// passes. Invalid norms set kErrSelling; paths with more than NSYM offsets kErrTableOverflow.
+template <int NSYM, typename Real>
+__global__ void tti_setup_kernel(Dev<Real> P, const double *metric) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[R.i];
+    double m[14];
+    const double *src = metric + (I.metric0 + (I.metric_const ? 0 : R.xl)) * 14;
+#pragma unroll
+    for (int k = 0; k < 14; ++k) m[k] = src[k];
+    TTICell cell;
+    int off[NSYM][3];
+    int n = -1;
+    if (tti_setup(m, I.h, cell)) n = tti_neighbors(cell, off, NSYM);
+    else atomicOr(P.status, (unsigned)kErrSelling);
+    if (n < 0 && (P.status[0] & kErrSelling) == 0) atomicOr(P.status, (unsigned)kErrTableOverflow);
+    ((TTICell *)P.tti)[R.c] = cell;
+#pragma unroll
+    for (int k = 0; k < NSYM; ++k) {
+        const bool on = k < n && abs(off[k][0]) < 128 && abs(off[k][1]) < 128 && abs(off[k][2]) < 128;
+        P.code[k * P.ntc + R.c] = on ? pack_off(off[k][0], off[k][1], off[k][2]) : 0u;
+        P.weight[k * P.ntc + R.c] = on ? Real(1) : Real(0);
+    }
+}
+
+// Per instance, the sum over cells of 1 / sqrt((l0 + l1) / 2) of the TTI norms (a slowness scale:
+// the key scale of batched ordering).
+template <typename Real>
+__global__ void tti_scale_kernel(Dev<Real> P, const double *metric, double *out) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool in = x < P.ncells;
+    int i = -1;
+    double v = 0.0;
+    if (in) {
+        i = inst_of_cell(P.inst, P.ninst, x);
+        const Inst &I = P.inst[i];
+        const double *m = metric + (I.metric0 + (I.metric_const ? 0 : x - I.cell0)) * 14;
+        const double s = 0.5 * (m[0] + m[1]);
+        v = s > 0 ? 1.0 / sqrt(s) : 0.0;
+    }
+    const unsigned same = __match_any_sync(0xffffffffu, i);
+    const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+    for (int o = 0; o < 32; ++o) {
+        const double w = __shfl_sync(0xffffffffu, v, o);
+        if (lane == leader && o != lane && ((same >> o) & 1u)) v += w;
+    }
+    if (in && lane == leader) atomicAdd(out + i, v);
+}
+
 // Largest L1 norm of a non-zero-weight offset whose target lies in the domain (MaxStencilWidth,
 // HamiltonFastMarching.hxx:36-45 over the reversed offsets of HFM_StencilRecompute.hxx:91-116),
 // per instance.
@@ -807,7 +897,7 @@ __device__ bool wall_visible(const GridGeom &g, const int8_t *wd, int b0, int b1
 // (ConditionalUpdate, HamiltonFastMarching.hxx:136-154). Also marks padding cells dead.
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8_t *cls_enabled) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= P.ntc) return;
@@ -858,7 +948,7 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
 
 template <typename Real, int KIND>
 __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *val, int n) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     // idx: global cell indices
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -877,7 +967,7 @@ template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void __launch_bounds__(kDepWarps * 32)
     deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
                 unsigned long long *msk, unsigned long long *dmsk) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     __shared__ int keys[kDepWarps][kDepCap];
     __shared__ unsigned long long masks[kDepWarps][kDepCap];
@@ -1021,10 +1111,14 @@ __global__ void count_finite_kernel(Dev<Real> P, unsigned long long *out) {
 // update adds every difference matching the accepted offset (EulerianStencil.hxx:114-123).
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= P.ncells) return;
+    if constexpr (KIND == kKindTTI) {  // no bitset for the semi-Lagrangian scheme
+        active[x] = 0ull;
+        return;
+    }
     const CellRef R = cell_ref(P.inst, P.ninst, x);
     const Inst &I = P.inst[R.i];
     const int x0 = R.x0, x1 = R.x1, x2 = R.x2;
@@ -1105,7 +1199,7 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     // the adjoint runs on a batch of one instance
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
@@ -1124,6 +1218,86 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
     const double u = (double)P.values[x];
     nflow[x] = 0;
     var[x] = 0.0;
+    if constexpr (KIND == kKindTTI) {
+        // semi-Lagrangian ValueVariation (FirstVariation.h:169-196): the update recomputed at the
+        // extremum t (TTI.hpp:278-389), flow weights (sol - v) w(t), and the local derivative
+        // value - sum of the normalised weights times the neighbour values. A seed has no flow
+        // and the derivative is its value (HamiltonFastMarching.hxx:194-195).
+        if (fixed) var[x] = u;
+        if (fixed || dead || !(u < Arith<double>::inf())) return;
+        double ta = 0.0;
+        bool inner = false;
+        solve_cell_tti<Real>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &ta, &inner);
+        if (!(ta < Arith<double>::inf())) return;
+        const TTICell &tc = P.tti[c];
+        TTIPath path;
+        if (!tti_path_at(tc, ta, path)) return;
+        double vals[6];
+        int cell[6];
+        for (int r = 0; r < 6; ++r) {
+            double vs[2] = {Arith<double>::inf(), Arith<double>::inf()};
+            int cs[2] = {-1, -1};
+            for (int si = 0; si < 2; ++si) {
+                const int s = si ? -1 : 1;
+                const int y0 = x0 + s * path.off[r][0], y1 = x1 + s * path.off[r][1], y2 = x2 + s * path.off[r][2];
+                if ((unsigned)y0 >= (unsigned)g.dims[0] || (unsigned)y1 >= (unsigned)g.dims[1] ||
+                    (unsigned)y2 >= (unsigned)g.dims[2])
+                    continue;
+                cs[si] = (int)g.lin(y0, y1, y2);
+                vs[si] = (double)P.values[cs[si]];
+            }
+            const int pick = vs[0] < vs[1] ? 0 : 1;  // the +e neighbour only when strictly smaller
+            vals[r] = vs[pick];
+            cell[r] = cs[pick];
+        }
+        int idx[6] = {0, 1, 2, 3, 4, 5};
+        for (int i = 1; i < 6; ++i) {
+            const int q = idx[i];
+            int k = i - 1;
+            while (k >= 0 && vals[idx[k]] > vals[q]) { idx[k + 1] = idx[k]; --k; }
+            idx[k + 1] = q;
+        }
+        const double vmin = vals[idx[0]];
+        if (!(vmin < Arith<double>::inf())) return;
+        double a = 0, b = 0, cc = -tti_multiplier(tc, dconst(ta)).v, sol = Arith<double>::inf();
+        int r = 0;
+        for (; r < 6; ++r) {
+            const int i = idx[r];
+            const double v = vals[i] - vmin;
+            if (v >= sol) break;
+            const double w = (1 - ta) * path.w0[i] + ta * path.w1[i];
+            a += w;
+            b += w * v;
+            cc += (w * v) * v;
+            if (a <= 100 * fabs(cc) * 2.220446049250313e-16) continue;
+            sol = (b + sqrt(b * b - a * cc)) / a;
+        }
+        double wd[6], ws = 0.0;
+        int n = 0, ys[6];
+        for (int q = 0; q < r; ++q) {
+            const int i = idx[q];
+            const double v = vals[i] - vmin;
+            const double w0 = (1 - ta) * path.w0[i] + ta * path.w1[i];
+            const double d = (sol - v) * w0;
+            wd[n] = d > 0 ? d : 0.0;
+            ys[n] = cell[i];
+            ws += wd[n];
+            ++n;
+        }
+        double vd = sol + vmin;
+        for (int j = 0; j < n; ++j) {
+            wd[j] = wd[j] / ws;
+            vd -= wd[j] * (double)P.values[ys[j]];
+        }
+        var[x] = vd;
+        nflow[x] = (uint8_t)n;
+        for (int j = 0; j < n; ++j) {
+            fidx[j * N + x] = ys[j];
+            fw[j * N + x] = wd[j];
+            atomicAdd(indeg + ys[j], 1);
+        }
+        return;
+    }
     if (fixed || dead || !(u < Arith<double>::inf())) return;
     unsigned used = 0, side = 0;
     solve_cell<Real, NFWD, NSYM, KIND>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
@@ -1326,7 +1500,7 @@ __global__ void flow_sort_kernel(long long N, const long long *rptr, int *rx, do
 template <typename Real, int NFWD, int NSYM, int KIND>
 void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
                  DeviceBuffer<unsigned> &status, cudaStream_t s) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     constexpr int NF = 2 * ND > 32 ? 32 : 2 * ND;
     if (N >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large for the adjoint");
@@ -1442,7 +1616,7 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
-    constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     constexpr int ND = NFWD + NSYM;
     constexpr int NB = NFWD + 2 * NSYM;
     const auto wall_t0 = std::chrono::steady_clock::now();
@@ -1519,6 +1693,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     DeviceBuffer<int8_t> cls_off, plain_off;
     DeviceBuffer<uint8_t> cls_en;
     DeviceBuffer<double> metric, plain_w, mult_rm, kscale;
+    DeviceBuffer<TTICell> ttibuf;
     std::vector<double> hscale;
     maxw.zero(s);
     std::vector<unsigned> hmaxw(ninst, 0);
@@ -1529,7 +1704,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         weight.zero(s);
         P.code = code.get();
         P.weight = weight.get();
-        const int NS = p0.ndim * (p0.ndim + 1) / 2;
+        const int NS = KIND == kKindTTI ? 14 : p0.ndim * (p0.ndim + 1) / 2;
         const double *metric_ptr = nullptr;
         if (ninst == 1 && p0.d_metric) {
             metric_ptr = p0.d_metric;
@@ -1550,16 +1725,22 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             metric_ptr = metric.get();
         }
         HFM_TRACE("metric upload");
-        if (want_stencils) {
+        if (want_stencils && KIND != kKindTTI) {
             plain_off.alloc(N * ND * 3);
             plain_w.alloc(N * ND);
         }
-        if (p0.ndim == 2)
+        if constexpr (KIND == kKindTTI) {
+            ttibuf.alloc(ntc);
+            ttibuf.zero(s);
+            P.tti = ttibuf.get();
+            launch(tti_setup_kernel<NSYM, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr);
+        } else if (p0.ndim == 2) {
             launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr, plain_off.get(),
                    plain_w.get());
-        else
+        } else {
             launch(riemann_stencil_kernel<3, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr, plain_off.get(),
                    plain_w.get());
+        }
         HFM_CUDA(cudaGetLastError());
         HFM_TRACE("stencil kernel");
         launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, P, maxw.get());
@@ -1567,7 +1748,9 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         if (ninst > 1 && p0.ordered) {
             kscale.alloc(ninst);
             kscale.zero(s);
-            if (p0.ndim == 2)
+            if (KIND == kKindTTI)
+                launch(tti_scale_kernel<Real>, nblocks(N, 256), 256, 0, s, P, metric_ptr, kscale.get());
+            else if (p0.ndim == 2)
                 launch(metric_scale_kernel<2, Real>, nblocks(N, 256), 256, 0, s, P, metric_ptr, kscale.get());
             else
                 launch(metric_scale_kernel<3, Real>, nblocks(N, 256), 256, 0, s, P, metric_ptr, kscale.get());
@@ -1913,7 +2096,11 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
         if (q->kind != p.kind || q->ndim != p.ndim || q->nfwd != p.nfwd || q->nsym != p.nsym || q->fp64 != p.fp64)
             throw Error(HFM_ERR_VALUE, "a batch must hold instances of one model family and one precision");
     }
-    if (p.kind == StencilKind::RiemannPerCell) {
+    if (p.kind == StencilKind::TTI) {
+        if (p.ndim != 3 || !p.fp64 || p.nsym != kTTISlots)
+            throw Error(HFM_ERR_UNSUPPORTED, "TTI3 is solved in FP64 on 3D grids");
+        run_batch_impl<double, 0, kTTISlots, detail::kKindTTI>(probs, results);
+    } else if (p.kind == StencilKind::RiemannPerCell) {
         if (p.ndim == 2) {
             if (p.fp64) run_batch_impl<double, 0, 3, detail::kKindRiemann>(probs, results);
             else run_batch_impl<float, 0, 3, detail::kKindRiemann>(probs, results);

@@ -252,6 +252,54 @@ void setup_riemann(Store &io, int ndim, Param &pm, EulerProblem &p) {
     }
 }
 
+// TTI3 (Headers/Experimental/TTI.h:18-33, Implementation/TTI.hpp:11-21): a 14-component metric
+// per point (linear 2, quadratic 3, transform 9), grid scales as for Riemann3, `nmix` (0: the
+// Newton-like optimisation, the only one on the GPU path).
+void setup_tti(Store &io, Param &pm, EulerProblem &p) {
+    const int ndim = 3;
+    const std::vector<int> dims = read_dims(io, ndim);
+    pm.ndim = ndim;
+    for (int a = 0; a < ndim; ++a) pm.dims[a] = dims[a];
+    const std::vector<double> origin = read_point(io, "origin", ndim, std::vector<double>(ndim, 0.0));
+    std::vector<double> hs(ndim);
+    if (io.has_field("gridScales")) {
+        hs = read_point(io, "gridScales", ndim, hs);
+    } else {
+        const double h = io.get_scalar("gridScale");
+        std::fill(hs.begin(), hs.end(), h);
+    }
+    for (int a = 0; a < ndim; ++a) {
+        if (!(hs[a] > 0)) throw Error(HFM_ERR_VALUE, "Parametrization error : gridscales should be positive");
+        pm.origin[a] = origin[a];
+        pm.scale[a] = hs[a];
+        p.h[a] = hs[a];
+        p.dims[a] = dims[a];
+    }
+    if (io.has_field("nmix") && io.get_scalar("nmix") != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, "TTI3 with nmix > 0 (finite envelope) is not supported by the GPU solve path");
+    if (io.has_field("walls"))
+        throw Error(HFM_ERR_UNSUPPORTED, "TTI3 with walls is not supported by the GPU solve path");
+    if (io.get_scalar("exportActiveNeighs", 0.0, 3) != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, "activeNeighs export is not supported for TTI3 by the GPU solve path");
+    p.ndim = ndim;
+    p.kind = StencilKind::TTI;
+    p.nfwd = 0;
+    p.nsym = kTTISlots;
+    const std::vector<int64_t> dd = io.field_domain_dims("metric", 14);
+    Field f = io.get_field("metric", dd.empty() ? 0 : ndim, 14);
+    if (!f.constant()) {
+        for (int a = 0; a < ndim; ++a)
+            if (f.dims[a] != dims[a]) throw Error(HFM_ERR_VALUE, "Error : Field metric has inconsistent dimensions.");
+    }
+    p.metric_constant = f.constant();
+    if (f.view) {
+        p.metric_ptr = f.view;
+        p.metric_len = f.size();
+    } else {
+        p.metric = std::move(f.data);
+    }
+}
+
 void setup_isotropic2(Store &io, Param &pm, EulerProblem &p) {
     // Isotropic2 solved as the Riemann metric cost^2 Id: its 4-point stencil is what Selling returns
     // for a multiple of the identity, so values match the reference's isotropic scheme.
@@ -366,6 +414,7 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     else if (model == "Riemann3") setup_riemann(io, 3, pm, p);
     else if (model == "Isotropic2") setup_isotropic2(io, pm, p);
     else if (lifted) setup_curvature(io, model, pm, p);
+    else if (model == "TTI3") setup_tti(io, pm, p);
     else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);
     set_common_solver_options(io, p);
     p.walls = read_walls(io, pm, lifted);

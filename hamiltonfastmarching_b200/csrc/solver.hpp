@@ -14,7 +14,12 @@ namespace hfm {
 enum class StencilKind {
     RiemannPerCell,   // Selling stencil of a metric at every cell (Recomp policy)
     SharedByTheta,    // one stencil per index of the last axis times a speed multiplier (Share policy)
+    TTI,              // TTI3 norm per cell, semi-Lagrangian Selling-path update (Lag2 policy); metric has 14 values
 };
+
+// Stencil slots of a TTI3 cell: the distinct offsets of its Selling path (at most 8 were met on
+// Thomsen media with eps, delta <= 0.2; a longer path is reported as an error).
+constexpr int kTTISlots = 10;
 
 struct EulerProblem {
     int ndim = 2;

@@ -64,3 +64,41 @@ def test_reedsshepp2_cost_gradient_matches_finite_differences():
     g = c.grad.numpy().reshape(-1)
     cells = np.flatnonzero(np.abs(g) > 1e-3 * np.abs(g).max())[::13][:8]
     _fd_check(p, cost, receivers, cells, rel_tol=2e-3)
+
+
+def test_tti3_velocity_gradient_matches_finite_differences():
+    """d loss / d vp with loss = sum over top-face receivers of (T - T_obs)^2, T_obs from a perturbed
+    vp (Gaussian blob), through the TTI3 adjoint; vp enters as the norm multiplier vp_ref / vp."""
+    import torch
+    from hamiltonfastmarching_b200.autograd import arrival_times
+    n, h = 24, 0.01
+    p = W.tti3_case(n, h=h, seed=4)
+    vp0 = p.pop("_vp")
+    obs = W.tti3_case(n, h=h, seed=4, blob=((0.12, 0.12, 0.12), 0.04, 0.05))
+    vp_obs = obs.pop("_vp")
+    rng = np.random.default_rng(5)
+    rx = rng.integers(0, n, (16, 2))
+    receivers = np.ravel_multi_index((rx[:, 0], rx[:, 1], np.zeros(16, int)), (n, n, n))
+    with torch.no_grad():
+        t_obs = arrival_times(p, torch.from_numpy(vp0 / vp_obs)).reshape(-1)[receivers]
+
+    def loss_of(vp):
+        T = arrival_times(p, torch.from_numpy(vp0) / vp)
+        return ((T.reshape(-1)[receivers] - t_obs) ** 2).sum()
+
+    vp = torch.from_numpy(vp0.copy()).requires_grad_(True)
+    loss_of(vp).backward()
+    g = vp.grad.numpy().reshape(-1)
+    assert np.all(np.isfinite(g)) and np.abs(g).max() > 0
+    cells = np.flatnonzero(np.abs(g) > 1e-2 * np.abs(g).max())
+    cells = rng.choice(cells, min(8, len(cells)), replace=False)
+    for cell in cells:
+        d = 1e-6 * vp0.reshape(-1)[cell]
+        vpp, vpm = vp0.copy().reshape(-1), vp0.copy().reshape(-1)
+        vpp[cell] += d
+        vpm[cell] -= d
+        with torch.no_grad():
+            fd = (loss_of(torch.from_numpy(vpp.reshape(vp0.shape))) -
+                  loss_of(torch.from_numpy(vpm.reshape(vp0.shape)))).item() / (2 * d)
+        scale = max(abs(fd), 1e-3 * np.abs(g).max())
+        assert abs(g[cell] - fd) <= 5e-3 * scale, (cell, g[cell], fd)
