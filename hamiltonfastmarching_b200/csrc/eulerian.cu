@@ -1232,8 +1232,12 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
         const TTICell &tc = P.tti[c];
         TTIPath path;
         if (!tti_path_at(tc, ta, path)) return;
-        double vals[6];
-        int cell[6];
+        // candidates (value, weights at both ends, cell), sorted by value: the sort moves whole
+        // records, so no array is read through an index array
+        struct Cand {
+            double v, wa, wb;
+            int cell;
+        } cand[6];
         for (int r = 0; r < 6; ++r) {
             double vs[2] = {Arith<double>::inf(), Arith<double>::inf()};
             int cs[2] = {-1, -1};
@@ -1246,26 +1250,23 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
                 cs[si] = (int)g.lin(y0, y1, y2);
                 vs[si] = (double)P.values[cs[si]];
             }
-            const int pick = vs[0] < vs[1] ? 0 : 1;  // the +e neighbour only when strictly smaller
-            vals[r] = vs[pick];
-            cell[r] = cs[pick];
+            const bool plus = vs[0] < vs[1];  // the +e neighbour only when strictly smaller
+            Cand cd{plus ? vs[0] : vs[1], path.w0[r], path.w1[r], plus ? cs[0] : cs[1]};
+            int k = r - 1;
+            while (k >= 0 && cand[k].v > cd.v) {
+                cand[k + 1] = cand[k];
+                --k;
+            }
+            cand[k + 1] = cd;
         }
-        int idx[6] = {0, 1, 2, 3, 4, 5};
-        for (int i = 1; i < 6; ++i) {
-            const int q = idx[i];
-            int k = i - 1;
-            while (k >= 0 && vals[idx[k]] > vals[q]) { idx[k + 1] = idx[k]; --k; }
-            idx[k + 1] = q;
-        }
-        const double vmin = vals[idx[0]];
+        const double vmin = cand[0].v;
         if (!(vmin < Arith<double>::inf())) return;
         double a = 0, b = 0, cc = -tti_multiplier(tc, dconst(ta)).v, sol = Arith<double>::inf();
         int r = 0;
         for (; r < 6; ++r) {
-            const int i = idx[r];
-            const double v = vals[i] - vmin;
+            const double v = cand[r].v - vmin;
             if (v >= sol) break;
-            const double w = (1 - ta) * path.w0[i] + ta * path.w1[i];
+            const double w = (1 - ta) * cand[r].wa + ta * cand[r].wb;
             a += w;
             b += w * v;
             cc += (w * v) * v;
@@ -1273,28 +1274,25 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
             sol = (b + sqrt(b * b - a * cc)) / a;
         }
         double wd[6], ws = 0.0;
-        int n = 0, ys[6];
-        for (int q = 0; q < r; ++q) {
-            const int i = idx[q];
-            const double v = vals[i] - vmin;
-            const double w0 = (1 - ta) * path.w0[i] + ta * path.w1[i];
+        const int n = r;
+        for (int q = 0; q < n; ++q) {
+            const double v = cand[q].v - vmin;
+            const double w0 = (1 - ta) * cand[q].wa + ta * cand[q].wb;
             const double d = (sol - v) * w0;
-            wd[n] = d > 0 ? d : 0.0;
-            ys[n] = cell[i];
-            ws += wd[n];
-            ++n;
+            wd[q] = d > 0 ? d : 0.0;
+            ws += wd[q];
         }
         double vd = sol + vmin;
         for (int j = 0; j < n; ++j) {
             wd[j] = wd[j] / ws;
-            vd -= wd[j] * (double)P.values[ys[j]];
+            vd -= wd[j] * (double)P.values[cand[j].cell];
         }
         var[x] = vd;
         nflow[x] = (uint8_t)n;
         for (int j = 0; j < n; ++j) {
-            fidx[j * N + x] = ys[j];
+            fidx[j * N + x] = cand[j].cell;
             fw[j * N + x] = wd[j];
-            atomicAdd(indeg + ys[j], 1);
+            atomicAdd(indeg + cand[j].cell, 1);
         }
         return;
     }
