@@ -84,6 +84,8 @@ constexpr int kWarpsPerCta = 4;
 // Stencil families of the solver kernels (the KIND template parameter): per-cell Riemann
 // stencils, shared per-angle stencils (curvature models), per-cell TTI Selling paths.
 constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2;
+// Value increases a tile may take before it accepts decreases only (termination guard).
+constexpr unsigned kUpBudget = 128;
 constexpr int kDepWarps = 2;
 constexpr int kDepCap = 1024;
 constexpr unsigned long long kBarrierPolls = 1ull << 25;
@@ -149,6 +151,7 @@ struct Dev {
     // instance's front on a common scale (nullptr: keys are the values)
     const double *kscale;
     const TTICell *tti;                    // [ntc] TTI norms (TTI kind)
+    unsigned *tile_up;                     // [ntile] value increases taken by each tile
     unsigned order_lo, order_hi;           // tiles solved per round kept in [lo, hi]; lo = 0: plain FIM
     // active-tile lists (triple buffered) and their dedupe flags
     int *list[3];
@@ -160,7 +163,6 @@ struct Dev {
     unsigned *status;
     unsigned long long *stats;  // rounds, tile activations, local solves
     int max_rounds;
-    int strict_after;  // rounds after which only decreasing values are accepted
     int sweeps;
 };
 
@@ -441,7 +443,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 // budget is spent (T re-queues itself with the cells still pending).
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
-                                             unsigned long long &n_solves, bool strict) {
+                                             unsigned long long &n_solves) {
     [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
@@ -477,6 +479,10 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
     }
     __syncwarp();
     bool converged = false;
+    unsigned ups = 0;  // increases taken by this lane in this activation
+    unsigned tile_ups = 0;
+    if (lane == 0) tile_ups = __ldcg(P.tile_up + T);
+    const bool strict = __shfl_sync(0xffffffffu, tile_ups, 0) >= kUpBudget;
     for (int sweep = 0; sweep < P.sweeps; ++sweep) {
         Real nv[2] = {cur[0], cur[1]};
         // one copy of the (large) local solve for both cells; the per-cell operands are selected,
@@ -496,12 +502,16 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         bool now[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            // Any change is taken, so that the converged field is the operator's exact fixed point
-            // (independent of the schedule). Rounding can make a recomputation land above the
-            // current value, and changes in both directions could then cycle; after
-            // P.strict_after rounds only decreases are taken, which must terminate (values then
-            // decrease in a finite set), leaving cells within an ulp of that fixed point.
+            // Any change is taken, so that the field converges to the exact fixed point of the
+            // local solves (what fast marching computes from the final neighbour values, whatever
+            // the schedule). Rounding can make a recomputation land an ulp above the current value
+            // and such increases can cycle (observed on TTI3, whose extremum over t is found
+            // iteratively): a tile that has taken kUpBudget increases takes only decreases from
+            // then on, so the iteration terminates (values then decrease in a finite set); its
+            // cells keep the smallest value they were computed at (fast marching's own rule,
+            // HamiltonFastMarching.hxx:151-176), equal to the fixed point up to rounding.
             now[j] = strict ? nv[j] < cur[j] : nv[j] != cur[j];
+            ups += (now[j] && nv[j] > cur[j]) ? 1u : 0u;
             if (now[j]) {
                 cur[j] = nv[j];
                 sv[lane + 32 * j] = nv[j];
@@ -515,6 +525,9 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 #pragma unroll
         for (int j = 0; j < 2; ++j) todo[j] = upd[j] && (reads[j] & C) != 0ull;
     }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) ups += __shfl_xor_sync(0xffffffffu, ups, o);
+    if (lane == 0 && ups) __stcg(P.tile_up + T, tile_ups + ups);
     unsigned long long pending = 0;
     if (!converged)
         pending = (unsigned long long)__ballot_sync(0xffffffffu, todo[0]) |
@@ -603,8 +616,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
                 continue;
             }
             if (lane == 0) atomicExch(P.key + T, kInfBits);
-            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves,
-                                                  r >= P.strict_after);
+            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves);
             ++n_act;
             ++solved;
         }
@@ -1950,6 +1962,9 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     P.dep_mask = rmask.get();
     P.dep_dmask = rdmask.get();
     DeviceBuffer<unsigned long long> dirty(nt), key(nt), rstat(32), maxval(nt);
+    DeviceBuffer<unsigned> tile_up(nt);
+    tile_up.zero(s);
+    P.tile_up = tile_up.get();
     dirty.zero(s);
     P.dirty = dirty.get();
     launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, key.get(), nt, 0x7ff0000000000000ull);
@@ -1982,7 +1997,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     P.bar_gen = counters.get() + 7;
     P.stats = stats.get();
     P.max_rounds = p0.max_rounds;
-    P.strict_after = 1 << 14;
     P.sweeps = p0.sweeps_per_tile;
     DeviceBuffer<int> stile;
     DeviceBuffer<unsigned long long> smask;
