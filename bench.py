@@ -55,6 +55,9 @@ def parse_args(argv=None):
     ap.add_argument("--serve-pool", type=int, default=48, help="distinct request payloads the arrivals draw from")
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--tti-side", type=int, default=128, help="grid side of the TTI3 differentiation leg")
+    ap.add_argument("--tti-fd-voxels", type=int, default=8, help="voxels checked by central differences")
+    ap.add_argument("--no-diff", action="store_true", help="skip the TTI3 differentiation leg")
     return ap.parse_args(argv)
 
 
@@ -327,6 +330,66 @@ def serving_leg(args, rank, world):
             "path": "serving.Server (hfm_server C ABI) from host arrays, H2D/D2H inside the latency"}
 
 
+# ------------------------------------------------------------------------------- differentiation leg
+
+def differentiation_leg(args):
+    """TTI3 128^3 (10 m spacing, Thomsen vp/eps/delta and tilt), one source at the top-face centre,
+    loss = sum over 64 top-face receivers of (T - T_obs)^2 with T_obs from vp with a +5% Gaussian
+    blob; d loss / d vp through the torch.autograd.Function over the GPU adjoint, checked by
+    central differences (step 1e-4 vp) at voxels drawn among those with a gradient."""
+    import torch
+    import hamiltonfastmarching_b200 as H
+    from hamiltonfastmarching_b200 import workloads as W
+    from hamiltonfastmarching_b200.autograd import arrival_times
+    n, h = args.tti_side, 0.01
+    p = W.tti3_case(n, h=h, seed=4)
+    vp0 = p.pop("_vp")
+    L = n * h
+    obs = W.tti3_case(n, h=h, seed=4, blob=((0.5 * L, 0.5 * L, 0.35 * L), 0.12 * L, 0.05))
+    vp_obs = obs.pop("_vp")
+    rng = np.random.default_rng(7)
+    rx = rng.integers(0, n, (64, 2))
+    receivers = np.ravel_multi_index((rx[:, 0], rx[:, 1], np.zeros(64, int)), (n, n, n))
+    q = dict(p, verbosity=0.0)
+    H.run(q)  # warm-up
+    t0 = time.perf_counter()
+    out = H.run(q)
+    fwd_s = time.perf_counter() - t0
+    with torch.no_grad():
+        t_obs = arrival_times(p, torch.from_numpy(vp0 / vp_obs)).reshape(-1)[receivers]
+
+    def loss_of(vp):
+        T = arrival_times(p, torch.from_numpy(vp0) / vp)
+        return ((T.reshape(-1)[receivers] - t_obs) ** 2).sum()
+
+    vp = torch.from_numpy(vp0.copy()).requires_grad_(True)
+    t0 = time.perf_counter()
+    loss = loss_of(vp)
+    t1 = time.perf_counter()
+    loss.backward()
+    t2 = time.perf_counter()
+    g = vp.grad.numpy().reshape(-1)
+    cand = np.flatnonzero(np.abs(g) > 1e-2 * np.abs(g).max())
+    cells = rng.choice(cand, min(args.tti_fd_voxels, len(cand)), replace=False) if len(cand) else []
+    errs = []
+    for cell in cells:
+        d = 1e-4 * vp0.reshape(-1)[cell]
+        vpp, vpm = vp0.copy().reshape(-1), vp0.copy().reshape(-1)
+        vpp[cell] += d
+        vpm[cell] -= d
+        with torch.no_grad():
+            fd = (loss_of(torch.from_numpy(vpp.reshape(vp0.shape))) -
+                  loss_of(torch.from_numpy(vpm.reshape(vp0.shape)))).item() / (2 * d)
+        errs.append(abs(g[cell] - fd) / max(abs(fd), 1e-12))
+    return {"workload": f"TTI3 {n}^3, h = 10 m, Thomsen vp in [1.5,4.5] km/s, eps/delta in [0,0.2], dip <= 30 deg; "
+                        f"64 top-face receivers, T_obs from vp with a +5% Gaussian blob",
+            "forward_solve_s": fwd_s, "gpu_solve_s": out["GPUSolveTime"], "n_accepted": out["nAccepted"],
+            "grid_updates_per_s": out["nAccepted"] / fwd_s,
+            "loss": float(loss.item()), "autograd_forward_s": t1 - t0, "autograd_backward_s": t2 - t1,
+            "fd_voxels": len(errs), "fd_max_rel_err": max(errs) if errs else None,
+            "fd_step": "1e-4 vp, central", "dtype": "f64"}
+
+
 # ------------------------------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -475,6 +538,9 @@ def run_ours(args):
     serving = None
     if not args.no_serve:
         serving = serving_leg(args, rank, world)
+    diff = None
+    if not args.no_diff and rank == 0:
+        diff = differentiation_leg(args)
 
     if rank == 0:
         line = {
@@ -494,6 +560,7 @@ def run_ours(args):
                      "clocks": results[32]["clocks"]},
             "batch": batch,
             "serving": serving,
+            "differentiation": diff,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
