@@ -114,7 +114,8 @@ struct GridGeom {
     }
 };
 
-GridGeom make_geom(int ndim, const int *dims, const int *periodic);
+// Tiles of 64 cells: log2 extents `shift` (summing to 6, unused axes 0), or 8x8 / 4x4x4 if null.
+GridGeom make_geom(int ndim, const int *dims, const int *periodic, const int *shift = nullptr);
 
 // Bounded sense-reversing barrier across all CTAs of a cooperative launch. Every wait gives up
 // after `limit` polls, sets kErrBarrierTimeout in *status and lets the caller return.

@@ -56,13 +56,14 @@ void trace_step(const char *what) {
     std::fflush(stderr);
 }
 
-GridGeom make_geom(int ndim, const int *dims, const int *periodic) {
+GridGeom make_geom(int ndim, const int *dims, const int *periodic, const int *shift) {
     GridGeom g{};
     for (int a = 0; a < 3; ++a) {
         g.dims[a] = a < ndim ? dims[a] : 1;
         g.periodic[a] = a < ndim ? periodic[a] : 0;
     }
-    if (ndim == 2) { g.tshift[0] = 3; g.tshift[1] = 3; g.tshift[2] = 0; }
+    if (shift) { for (int a = 0; a < 3; ++a) g.tshift[a] = a < ndim ? shift[a] : 0; }
+    else if (ndim == 2) { g.tshift[0] = 3; g.tshift[1] = 3; g.tshift[2] = 0; }
     else { g.tshift[0] = 2; g.tshift[1] = 2; g.tshift[2] = 2; }
     g.ncells = 1;
     g.ntile = 1;
@@ -1643,7 +1644,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         const EulerProblem &p = *probs[i];
         Inst &I = hinst[i];
         std::memset(&I, 0, sizeof(I));
-        I.g = make_geom(p.ndim, p.dims, p.periodic);
+        I.g = make_geom(p.ndim, p.dims, p.periodic, p.tile_shift[0] >= 0 ? p.tile_shift : nullptr);
         I.tile0 = ntile;
         I.cell0 = ncells;
         I.cls0 = nclass;

@@ -206,6 +206,22 @@ void set_common_solver_options(Store &io, EulerProblem &p) {
     p.band_lo = io.get_scalar("bandLo", p.band_lo, 3);
     p.band_hi = io.get_scalar("bandHi", p.band_hi, 3);
     if (!(p.band_lo > 0) || !(p.band_hi > p.band_lo)) throw Error(HFM_ERR_VALUE, "bandLo/bandHi must satisfy 0 < bandLo < bandHi");
+    if (io.has_field("tileShape")) {
+        // tile extents per axis (x, y[, z|theta]): powers of two whose product is 64
+        int64_t n = 0;
+        const std::vector<double> e = io.get_vector("tileShape", 1, &n);
+        if (n != p.ndim) throw Error(HFM_ERR_VALUE, "tileShape must give one extent per axis");
+        int sum = 0;
+        for (int a = 0; a < p.ndim; ++a) {
+            const int v = (int)e[a];
+            if (v < 1 || v != e[a] || (v & (v - 1))) throw Error(HFM_ERR_VALUE, "tileShape extents must be powers of two");
+            int sh = 0;
+            while ((1 << sh) < v) ++sh;
+            p.tile_shift[a] = sh;
+            sum += sh;
+        }
+        if (sum != 6) throw Error(HFM_ERR_VALUE, "tileShape must hold 64 cells");
+    }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -65,6 +65,7 @@ struct EulerProblem {
     std::vector<std::vector<int64_t>> adjoint_index;
     std::vector<std::vector<double>> adjoint_weight;
     bool want_stencils = false;        // export per-cell offsets/weights (RiemannPerCell)
+    int tile_shift[3] = {-1, -1, -1};  // log2 tile extents per axis (sum 6); -1: 8x8 / 4x4x4
     int sweeps_per_tile = 4;           // local Jacobi sweeps before a tile re-queues itself
     int max_rounds = 1 << 20;
     // Value-ordered scheduling: a round solves the tiles whose wake-up key is within a band above

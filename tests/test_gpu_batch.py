@@ -128,3 +128,24 @@ def test_batch_with_sensitivity_request_runs_it_alone():
     assert _same(out[1]["values"], ref["values"])
     assert _rel(out[1]["costSensitivity_0"], ref["costSensitivity_0"]) <= 1e-10
     assert _same(out[0]["values"], _alone(p))
+
+
+def test_autotuner_picks_a_valid_schedule_and_values_do_not_change():
+    """Tile shape, sweeps and queue policy change the speed, not the fixed point."""
+    from hamiltonfastmarching_b200.autotune import Autotuner
+    cases = [_ragged_riemann2(n, n, seed=70 + n) for n in (64, 96, 80)]
+    for p in cases:
+        p["solverPrecision"] = "float32"
+    at = Autotuner(repeats=1, device="test")
+    res = at.tune(cases, sweeps=1)
+    assert np.isfinite(res["seconds"]) and res["seconds"] <= res["default_seconds"]
+    assert len(at.trials) >= 8
+    for p in cases:
+        q = at.apply(p)
+        assert "tileShape" in q
+        assert _rel(hfm.run(q)["values"], _alone(p)) <= SAME["float32"]
+    # a non-default tile shape on each domain kind gives the same values
+    for p, shape in ((cases[0], [16, 4]), (W.riemann3_case(24, seed=3, n_spheres=3), [2, 4, 8]),
+                     (W.curvature2_case(32, 24, "ReedsShepp2", seed=4, n_curves=4), [2, 2, 16])):
+        assert _same(hfm.run(dict(p, tileShape=np.array(shape, float)))["values"], _alone(p),
+                     p.get("solverPrecision", "float64"))
