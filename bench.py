@@ -228,8 +228,8 @@ def batched_leg(args, rank, world):
     for k in range(len(ios)):
         fams.setdefault(ios[k].get_string("model"), []).append(k)
     for fam, ks in fams.items():
-        sample = [cases[k] for k in ks[:: max(1, len(ks) // 8)][:8]]
-        tuned[fam] = at.tune(sample, sweeps=1)
+        tune_sample = [cases[k] for k in ks[:: max(1, len(ks) // 8)][:8]]
+        tuned[fam] = at.tune(tune_sample, sweeps=1)
     tune_s = time.perf_counter() - t0
     for k, io in enumerate(ios):
         t = at.lookup(cases[k])
