@@ -24,7 +24,7 @@ __all__ = ["Autotuner", "family_key", "SPACE"]
 
 # Candidates per parameter; tile shapes per domain kind (extents per axis, 64 cells).
 SPACE = {
-    "tileSweeps": [2, 3, 4, 6, 8],
+    "tileSweeps": [1, 2, 3, 4, 6],
     "queue": [("band", 1.0, 4.0), ("band", 2.0, 8.0), ("band", 4.0, 16.0), ("fifo", None, None)],
     "tileShape": {
         "2d": [(8, 8), (16, 4), (4, 16)],
@@ -32,7 +32,15 @@ SPACE = {
         "lifted": [(4, 4, 4), (8, 8, 1), (2, 2, 16), (8, 4, 2)],
     },
 }
-DEFAULT = {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)}
+# The library's default schedule per model (default_schedule in the solver), the search's start.
+DEFAULT = {
+    "Riemann3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
+    "Riemann2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
+    "Isotropic2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
+    "ReedsShepp2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
+    "Elastica2": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
+    "TTI3": {"tileSweeps": 1, "queue": ("band", 1.0, 4.0)},
+}
 _LIFTED = ("ReedsShepp2", "Elastica2")
 
 
@@ -103,7 +111,7 @@ class Autotuner:
         """Coordinate search over tile shape, sweeps and queue policy on a sample of instances of one
         family; returns (and records) the best configuration and its time against the defaults."""
         kind = _domain_kind(cases[0])
-        cfg = dict(DEFAULT, tileShape=SPACE["tileShape"][kind][0])
+        cfg = dict(DEFAULT[cases[0]["model"]], tileShape=SPACE["tileShape"][kind][0])
         base = self.measure(cases, cfg)
         best_t = base
         for _ in range(sweeps):

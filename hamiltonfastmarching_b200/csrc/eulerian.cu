@@ -2136,6 +2136,14 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
     }
 }
 
+void default_schedule(EulerProblem &p) {
+    if (p.kind == StencilKind::TTI) { p.sweeps_per_tile = 1; p.band_lo = 1; p.band_hi = 4; }
+    else if (p.kind == StencilKind::SharedByTheta && p.nfwd > 0) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
+    else if (p.kind == StencilKind::SharedByTheta) { p.sweeps_per_tile = 4; p.band_lo = 2; p.band_hi = 8; }
+    else if (p.ndim == 3) { p.sweeps_per_tile = 2; p.band_lo = 1; p.band_hi = 4; }
+    else { p.sweeps_per_tile = 3; p.band_lo = 2; p.band_hi = 8; }
+}
+
 void solve_eulerian(const EulerProblem &p, EulerResult &r) {
     std::vector<EulerResult> rs;
     solve_eulerian_batch({&p}, rs);

@@ -199,7 +199,8 @@ void set_common_solver_options(Store &io, EulerProblem &p) {
     if (prec == "float64") p.fp64 = true;
     else if (prec == "float32") p.fp64 = false;
     else throw Error(HFM_ERR_VALUE, "solverPrecision must be float64 or float32");
-    p.sweeps_per_tile = (int)io.get_scalar("tileSweeps", 4, 3);
+    default_schedule(p);
+    p.sweeps_per_tile = (int)io.get_scalar("tileSweeps", p.sweeps_per_tile, 3);
     if (p.sweeps_per_tile < 1 || p.sweeps_per_tile > 1024) throw Error(HFM_ERR_VALUE, "tileSweeps out of range");
     p.max_rounds = (int)io.get_scalar("maxRounds", (double)(1 << 20), 3);
     p.ordered = io.get_scalar("tileOrdering", 1.0, 3) != 0;

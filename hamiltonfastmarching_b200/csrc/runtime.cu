@@ -90,6 +90,7 @@ int hfm_solve_riemann_device(const hfm_riemann_device_args *a, hfm_solve_stats *
         p.d_metric = a->metric;
         p.d_walls = a->walls;
         p.d_values_out = a->values;
+        hfm::default_schedule(p);
         if (a->sweeps_per_tile > 0) p.sweeps_per_tile = a->sweeps_per_tile;
         std::vector<std::pair<int64_t, double>> seeds;
         for (int64_t i = 0; i < a->nseeds; ++i) {

@@ -94,6 +94,10 @@ struct EulerResult {
 };
 
 void solve_eulerian(const EulerProblem &p, EulerResult &r);
+// Default schedule of a family (local sweeps per activation and band limits), measured on B200:
+// Riemann3 2 sweeps, band [1,4]; Riemann2 3, [2,8]; ReedsShepp2 4, [2,8]; Elastica2 2, [4,16];
+// TTI3 1, [1,4]. Callers override it with tileSweeps / bandLo / bandHi (or the autotuner).
+void default_schedule(EulerProblem &p);
 // One launch sequence for many instances of one model family and precision (a global tile space
 // over all instances, one persistent solver launch). Results are in the order of `probs`.
 void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results);
