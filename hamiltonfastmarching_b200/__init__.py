@@ -94,7 +94,25 @@ class HFMIO:
                                                   shape))
         self._views[key] = a
 
-    def get_array(self, key: str) -> np.ndarray:
+    def get_array(self, key: str, copy: bool = True) -> np.ndarray:
+        """The array `key`; with ``copy=False`` a read-only view of the store's memory, which keeps
+        this store alive (valid while the key is not replaced or erased)."""
+        if not copy:
+            ptr, nd = ctypes.c_void_p(), ctypes.c_int()
+            shape = (ctypes.c_int64 * 16)()
+            self._check(self._L.hfm_io_get_array_ptr(self._h, key.encode(), ctypes.byref(ptr), ctypes.byref(nd),
+                                                     shape, 16))
+            if nd.value == 0:
+                raise PyExp(1, f"PythonIO error : field {key} is a scalar, not an array")
+            dims = tuple(shape[i] for i in range(nd.value))
+            n = int(np.prod(dims))
+            if n == 0:
+                return np.empty(dims, np.float64)
+            buf = (ctypes.c_double * n).from_address(ptr.value)
+            buf.owner = self  # the store outlives the view
+            a = np.frombuffer(buf, dtype=np.float64).reshape(dims)
+            a.flags.writeable = False
+            return a
         nd = ctypes.c_int()
         shape = (ctypes.c_int64 * 16)()
         self._check(self._L.hfm_io_get_array_info(self._h, key.encode(), ctypes.byref(nd), shape, 16))
@@ -134,20 +152,20 @@ class HFMIO:
             else:
                 self.set_array(k, np.asarray(v, dtype=np.float64))
 
-    def get_computed(self) -> Dict:
+    def get_computed(self, copy: bool = True) -> Dict:
         out = {}
         for key, kind in ast.literal_eval(self.computed_keys()):
             out[key] = (self.get_string(key) if kind == "string" else
-                        self.get_scalar(key) if kind == "float" else self.get_array(key))
+                        self.get_scalar(key) if kind == "float" else self.get_array(key, copy))
         return out
 
 
 def run(params: Dict, arrayOrdering: str = "RowMajor", expected_model: str = None) -> Dict:
     """Solve an ``hfmIn`` dictionary on the GPU and return the computed ``hfmOut`` dictionary."""
     io = HFMIO(arrayOrdering)
-    io.set_dict(params)
+    io.set_dict(params, views=True)  # the call is synchronous: the caller's arrays are read in place
     io.run(expected_model)
-    return io.get_computed()
+    return io.get_computed(copy=False)  # read-only views of the result store
 
 
 def run_ios(ios, expected_model: str = None):

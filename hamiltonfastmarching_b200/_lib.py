@@ -30,6 +30,7 @@ SIGNATURES = {
     "hfm_io_get_string": ([_P, _S, _P, _SZ, ctypes.POINTER(_SZ)], _I),
     "hfm_io_get_array_info": ([_P, _S, ctypes.POINTER(_I), _I64P, _I], _I),
     "hfm_io_get_array": ([_P, _S, _P, _SZ], _I),
+    "hfm_io_get_array_ptr": ([_P, _S, ctypes.POINTER(_P), ctypes.POINTER(_I), _I64P, _I], _I),
     "hfm_io_has_field": ([_P, _S], _I),
     "hfm_io_erase_field": ([_P, _S], _I),
     "hfm_io_computed_keys": ([_P, _P, _SZ, ctypes.POINTER(_SZ)], _I),

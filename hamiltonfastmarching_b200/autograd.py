@@ -80,7 +80,7 @@ class EikonalSolve(torch.autograd.Function):
         out = _run(_with_cost(params, c))
         ctx.params = params
         ctx.save_for_backward(cost)
-        return torch.from_numpy(out["values"]).to(device=cost.device, dtype=cost.dtype)
+        return torch.from_numpy(np.array(out["values"])).to(device=cost.device, dtype=cost.dtype)
 
     @staticmethod
     def backward(ctx, grad: torch.Tensor):
@@ -102,7 +102,7 @@ class EikonalSolve(torch.autograd.Function):
                 gc = gc.sum(axis=2)
         else:
             gc = sens / c
-        return torch.from_numpy(np.ascontiguousarray(gc)).to(device=cost.device, dtype=cost.dtype), None
+        return torch.from_numpy(np.array(gc)).to(device=cost.device, dtype=cost.dtype), None
 
 
 def arrival_times(params: Dict, cost: torch.Tensor) -> torch.Tensor:

@@ -25,6 +25,15 @@ void keep_pool_cached();
 // Kernel launches issued by this library (all threads), for launch accounting.
 void count_launch(unsigned n = 1);
 
+// Large host<->device copies of pageable memory: through two page-locked staging buffers of the
+// calling thread, the host-side copies split over a pool of worker threads and overlapped with the
+// DMA of the previous chunk. Copies below kStagedMin bytes go straight through cudaMemcpyAsync.
+// staged_upload returns once the host source has been read (the DMA may still be in flight on `s`);
+// staged_download returns once the destination is written.
+constexpr size_t kStagedMin = size_t(8) << 20;
+void staged_upload(void *dst_dev, const void *src_host, size_t bytes, cudaStream_t s);
+void staged_download(void *dst_host, const void *src_dev, size_t bytes, cudaStream_t s);
+
 // Counted kernel launch: launch(kernel, grid, block, shared_bytes, stream, args...).
 template <typename... KArgs, typename... Args>
 inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
@@ -36,7 +45,6 @@ inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
 template <typename T>
 class DeviceBuffer {
 public:
-    static constexpr size_t kPinThreshold = size_t(64) << 20;
     DeviceBuffer() = default;
     explicit DeviceBuffer(size_t n) { alloc(n); }
     ~DeviceBuffer() { release(); }
@@ -66,20 +74,7 @@ public:
     void upload(const T *h, size_t n, cudaStream_t s = current_stream()) {
         if (n > n_) alloc(n);
         if (!n) return;
-        // Large pageable sources are page-locked for the transfer (DMA at full link speed instead
-        // of staged copies); if locking is refused the copy proceeds from pageable memory.
-        const size_t bytes = n * sizeof(T);
-        if (bytes >= kPinThreshold &&
-            cudaHostRegister(const_cast<T *>(h), bytes, cudaHostRegisterReadOnly) == cudaSuccess) {
-            const cudaError_t e = cudaMemcpyAsync(p_, h, bytes, cudaMemcpyHostToDevice, s);
-            const cudaError_t e2 = cudaStreamSynchronize(s);
-            cudaHostUnregister(const_cast<T *>(h));
-            HFM_CUDA(e);
-            HFM_CUDA(e2);
-            return;
-        }
-        cudaGetLastError();
-        HFM_CUDA(cudaMemcpyAsync(p_, h, bytes, cudaMemcpyHostToDevice, s));
+        staged_upload(p_, h, n * sizeof(T), s);
     }
     void upload(const std::vector<T> &v, cudaStream_t s = current_stream()) { upload(v.data(), v.size(), s); }
     void download(T *h, size_t n, cudaStream_t s = current_stream()) const {

@@ -1730,8 +1730,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                 const size_t bytes = rows * NS * sizeof(double);
                 double *dst = metric.get() + hinst[i].metric0 * NS;
                 if (p.d_metric) HFM_CUDA(cudaMemcpyAsync(dst, p.d_metric, bytes, cudaMemcpyDeviceToDevice, s));
-                else HFM_CUDA(cudaMemcpyAsync(dst, p.metric_ptr ? p.metric_ptr : p.metric.data(), bytes,
-                                              cudaMemcpyHostToDevice, s));
+                else staged_upload(dst, p.metric_ptr ? p.metric_ptr : p.metric.data(), bytes, s);
             }
             metric_ptr = metric.get();
         }
@@ -1783,8 +1782,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             const double *msrc = p.mult_ptr ? p.mult_ptr : p.mult.data();
             if (!p.mult_ptr && (long long)p.mult.size() < len)
                 throw Error(HFM_ERR_VALUE, "speed multiplier field too short");
-            HFM_CUDA(cudaMemcpyAsync(mult_rm.get() + hinst[i].mult0, msrc, len * sizeof(double),
-                                     cudaMemcpyHostToDevice, s));
+            staged_upload(mult_rm.get() + hinst[i].mult0, msrc, len * sizeof(double), s);
             if (ninst > 1 && p0.ordered) {  // time scale = mean cost over the (uniform) broadcast field
                 double t = 0.0;
                 for (long long k = 0; k < len; ++k) {
@@ -1855,8 +1853,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                     HFM_CUDA(cudaMemcpyAsync(walls.get() + hinst[i].cell0, p.d_walls, hinst[i].g.ncells,
                                              cudaMemcpyDeviceToDevice, s));
                 else if (!p.walls.empty())
-                    HFM_CUDA(cudaMemcpyAsync(walls.get() + hinst[i].cell0, p.walls.data(), hinst[i].g.ncells,
-                                             cudaMemcpyHostToDevice, s));
+                    staged_upload(walls.get() + hinst[i].cell0, p.walls.data(), hinst[i].g.ncells, s);
             }
             walls_ptr = walls.get();
         }
@@ -2060,7 +2057,8 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                 res.values.resize(n);
                 dst = res.values.data();
             }
-            HFM_CUDA(cudaMemcpyAsync(dst, vsrc + off, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            if (n * sizeof(double) >= kStagedMin) staged_download(dst, vsrc + off, n * sizeof(double), s);
+            else HFM_CUDA(cudaMemcpyAsync(dst, vsrc + off, n * sizeof(double), cudaMemcpyDeviceToHost, s));
         }
         if (p.want_active) {
             res.active.resize(n);

@@ -658,6 +658,19 @@ int hfm_io_get_array(hfm_io *io, const char *key, double *out, size_t count) {
     });
 }
 
+int hfm_io_get_array_ptr(hfm_io *io, const char *key, const double **data, int *ndim, int64_t *shape,
+                         int max_ndim) {
+    return guarded(io, [&] {
+        if (!key || !data || !ndim) throw Error(HFM_ERR_ARG, "null argument");
+        const hfm::RawElement &r = io->store.raw(key);
+        if (r.is_string()) throw Error(HFM_ERR_KEY, "PythonIO error : field " + std::string(key) + " is a string, not an array");
+        *ndim = (int)r.dims.size();
+        if (shape)
+            for (int i = 0; i < *ndim && i < max_ndim; ++i) shape[i] = r.dims[i];
+        *data = r.ptr();
+    });
+}
+
 int hfm_io_has_field(hfm_io *io, const char *key) {
     if (!io || !key) return -HFM_ERR_ARG;
     return io->store.has_field(key) ? 1 : 0;

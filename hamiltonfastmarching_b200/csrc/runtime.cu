@@ -2,8 +2,11 @@
 // device-resident entry point of the C ABI.
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstring>
 #include <mutex>
+#include <thread>
+#include <vector>
 
 #include "device_buffer.hpp"
 #include "solver.hpp"
@@ -35,6 +38,152 @@ void keep_pool_cached() {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     done[dev] = true;
+}
+
+// ---- staged transfers
+namespace {
+
+// Worker threads for the host-side parts of staged copies (one pool per process).
+class CopyPool {
+public:
+    CopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        nworkers_ = std::max(1u, std::min(16u, hw ? hw / 2 : 4u));
+        for (unsigned i = 0; i + 1 < nworkers_; ++i) threads_.emplace_back([this, i] { work(i + 1); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread &t : threads_) t.join();
+    }
+    // dst[0:n) = src[0:n), split in nworkers_ parts; the caller copies part 0.
+    void copy(char *dst, const char *src, size_t n) {
+        std::unique_lock<std::mutex> call(call_mu_);  // one parallel copy at a time
+        const size_t part = (n + nworkers_ - 1) / nworkers_;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = dst; src_ = src; n_ = n; part_ = part;
+            pending_ = nworkers_ - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        std::memcpy(dst, src, std::min(part, n));
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+private:
+    void work(unsigned idx) {
+        unsigned long long seen = 0;
+        for (;;) {
+            char *d;
+            const char *s;
+            size_t n, part;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                d = dst_; s = src_; n = n_; part = part_;
+            }
+            const size_t b = std::min(n, (size_t)idx * part), e = std::min(n, b + part);
+            if (e > b) std::memcpy(d + b, s + b, e - b);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (--pending_ == 0) done_cv_.notify_all();
+            }
+        }
+    }
+    unsigned nworkers_ = 1;
+    std::vector<std::thread> threads_;
+    std::mutex mu_, call_mu_;
+    std::condition_variable cv_, done_cv_;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t n_ = 0, part_ = 0;
+    unsigned pending_ = 0;
+    unsigned long long gen_ = 0;
+    bool stop_ = false;
+};
+
+CopyPool &copy_pool() {
+    static CopyPool *pool = new CopyPool();  // lives until exit (workers are never joined late)
+    return *pool;
+}
+
+constexpr size_t kChunk = size_t(32) << 20;
+
+// Two page-locked chunks and their completion events, per thread (kept for the thread's life).
+struct Staging {
+    char *buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool used[2] = {false, false};
+    bool ok = false;
+    Staging() {
+        ok = cudaHostAlloc((void **)&buf[0], kChunk, cudaHostAllocDefault) == cudaSuccess &&
+             cudaHostAlloc((void **)&buf[1], kChunk, cudaHostAllocDefault) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+    }
+};
+
+Staging &staging() {
+    thread_local Staging *st = new Staging();  // released with the process
+    return *st;
+}
+
+}  // namespace
+
+void staged_upload(void *dst_dev, const void *src_host, size_t bytes, cudaStream_t s) {
+    Staging &st = staging();
+    if (bytes < kStagedMin || !st.ok) {
+        HFM_CUDA(cudaMemcpyAsync(dst_dev, src_host, bytes, cudaMemcpyHostToDevice, s));
+        return;
+    }
+    const char *src = static_cast<const char *>(src_host);
+    char *dst = static_cast<char *>(dst_dev);
+    for (size_t off = 0, i = 0; off < bytes; off += kChunk, ++i) {
+        const int b = (int)(i & 1);
+        const size_t len = std::min(kChunk, bytes - off);
+        if (st.used[b]) HFM_CUDA(cudaEventSynchronize(st.ev[b]));  // the chunk's previous DMA is done
+        copy_pool().copy(st.buf[b], src + off, len);
+        HFM_CUDA(cudaMemcpyAsync(dst + off, st.buf[b], len, cudaMemcpyHostToDevice, s));
+        HFM_CUDA(cudaEventRecord(st.ev[b], s));
+        st.used[b] = true;
+    }
+}
+
+void staged_download(void *dst_host, const void *src_dev, size_t bytes, cudaStream_t s) {
+    Staging &st = staging();
+    if (bytes < kStagedMin || !st.ok) {
+        HFM_CUDA(cudaMemcpyAsync(dst_host, src_dev, bytes, cudaMemcpyDeviceToHost, s));
+        HFM_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    const char *src = static_cast<const char *>(src_dev);
+    char *dst = static_cast<char *>(dst_host);
+    const size_t nchunks = (bytes + kChunk - 1) / kChunk;
+    auto issue = [&](size_t i) {
+        const int b = (int)(i & 1);
+        const size_t off = i * kChunk, len = std::min(kChunk, bytes - off);
+        if (st.used[b]) HFM_CUDA(cudaEventSynchronize(st.ev[b]));
+        HFM_CUDA(cudaMemcpyAsync(st.buf[b], src + off, len, cudaMemcpyDeviceToHost, s));
+        HFM_CUDA(cudaEventRecord(st.ev[b], s));
+        st.used[b] = true;
+    };
+    issue(0);
+    for (size_t i = 0; i < nchunks; ++i) {
+        const int b = (int)(i & 1);
+        const size_t off = i * kChunk, len = std::min(kChunk, bytes - off);
+        HFM_CUDA(cudaEventSynchronize(st.ev[b]));
+        if (i + 1 < nchunks) issue(i + 1);  // the next chunk's DMA overlaps this chunk's host copy
+        copy_pool().copy(dst + off, st.buf[b], len);
+        st.used[b] = false;
+    }
 }
 
 static std::atomic<unsigned long long> g_launches{0};

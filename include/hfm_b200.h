@@ -65,6 +65,10 @@ int hfm_io_get_scalar(hfm_io *io, const char *key, double *value);
 int hfm_io_get_string(hfm_io *io, const char *key, char *buf, size_t cap, size_t *len);
 int hfm_io_get_array_info(hfm_io *io, const char *key, int *ndim, int64_t *shape, int max_ndim);
 int hfm_io_get_array(hfm_io *io, const char *key, double *out, size_t count);
+/* Zero-copy read of an array (an extension): *data points into the store, valid until the key is
+ * replaced or erased or the store destroyed; *ndim and shape[:max_ndim] receive its extents. */
+int hfm_io_get_array_ptr(hfm_io *io, const char *key, const double **data, int *ndim, int64_t *shape,
+                         int max_ndim);
 
 /* Field inspection: HFMIO::HasField / EraseField / GetComputedKeys (main.cpp:25-27,
  * BaseIO.hxx:38-47, PythonIO.hxx:37-48). has_field returns 1/0 (negative on a null argument). */
