@@ -819,6 +819,11 @@ __global__ void mult_layout_kernel(Dev<Real> P, const double *src) {
 // Headers/ExtraAlgorithms/WallObstructionTest.h:48-88, which on a box grid is the L1 distance,
 // computed here by separable forward/backward scans per axis), capped at the stencil width.
 
+__global__ void walls_from_f64_kernel(long long n, const double *src, uint8_t *dst) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < n) dst[x] = src[x] != 0.0 ? 1 : 0;
+}
+
 __global__ void wall_init_kernel(long long n, const uint8_t *walls, int *d) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x < n) d[x] = walls[x] ? 0 : (1 << 29);
@@ -1652,7 +1657,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         for (int a = 0; a < 3; ++a) I.h[a] = p.h[a];
         I.dual = p.dual;
         I.metric_const = p.metric_constant;
-        I.has_walls = (!p.walls.empty() || p.d_walls) ? 1 : 0;
+        I.has_walls = (!p.walls.empty() || p.d_walls || p.walls_f64) ? 1 : 0;
         ntile += I.g.ntile;
         ncells += I.g.ncells;
         nclass += SHARE ? p.nclass : 0;
@@ -1854,6 +1859,12 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                                              cudaMemcpyDeviceToDevice, s));
                 else if (!p.walls.empty())
                     staged_upload(walls.get() + hinst[i].cell0, p.walls.data(), hinst[i].g.ncells, s);
+                else if (p.walls_f64) {
+                    DeviceBuffer<double> wf(hinst[i].g.ncells);
+                    staged_upload(wf.get(), p.walls_f64, hinst[i].g.ncells * sizeof(double), s);
+                    launch(walls_from_f64_kernel, nblocks(hinst[i].g.ncells, 256), 256, 0, s, hinst[i].g.ncells,
+                           wf.get(), walls.get() + hinst[i].cell0);
+                }
             }
             walls_ptr = walls.get();
         }

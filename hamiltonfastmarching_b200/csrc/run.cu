@@ -165,33 +165,41 @@ int read_lifted_scalar(Store &io, const std::string &key, const int *dims, Field
     return depth;
 }
 
-std::vector<uint8_t> read_walls(Store &io, const Param &pm, bool lifted) {
-    std::vector<uint8_t> w;
-    if (!io.has_field("walls")) return w;
+// Walls (GetIntegralField<bool>: (bool)double). A full RowMajor field stored in the store is
+// handed to the solver as a view (converted on the device); other shapes are converted here.
+void read_walls(Store &io, const Param &pm, bool lifted, EulerProblem &p) {
+    std::vector<uint8_t> &w = p.walls;
+    w.clear();
+    p.walls_f64 = nullptr;
+    if (!io.has_field("walls")) return;
     const int64_t N = (int64_t)pm.dims[0] * pm.dims[1] * pm.dims[2];
-    w.resize(N);
     if (lifted) {
+        w.resize(N);
         Field f;
         const int depth = read_lifted_scalar(io, "walls", pm.dims, f);
         const double *v = f.ptr();
         const int64_t nt = pm.dims[2];
-        for (int64_t i = 0; i < N; ++i) {  // GetIntegralField<bool>: (bool)double
+        for (int64_t i = 0; i < N; ++i) {
             const int64_t k = depth == 3 ? i : depth == 2 ? i / nt : depth == 1 ? i % nt : 0;
             w[i] = v[k] != 0.0;
         }
-        return w;
+        return;
     }
     const std::vector<int64_t> dd = io.field_domain_dims("walls", 1);
     Field f = io.get_field("walls", dd.empty() ? 0 : pm.ndim, 1);
     if (f.constant()) {
-        std::fill(w.begin(), w.end(), f.ptr()[0] != 0.0);
-        return w;
+        w.assign(N, f.ptr()[0] != 0.0);
+        return;
     }
     for (int a = 0; a < pm.ndim; ++a)
         if (f.dims[a] != pm.dims[a]) throw Error(HFM_ERR_VALUE, "Error : walls have inconsistent dims");
+    if (f.view) {
+        p.walls_f64 = f.view;
+        return;
+    }
+    w.resize(N);
     const double *v = f.ptr();
     for (int64_t i = 0; i < N; ++i) w[i] = v[i] != 0.0;
-    return w;
 }
 
 void set_common_solver_options(Store &io, EulerProblem &p) {
@@ -434,7 +442,7 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     else if (model == "TTI3") setup_tti(io, pm, p);
     else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);
     set_common_solver_options(io, p);
-    p.walls = read_walls(io, pm, lifted);
+    read_walls(io, pm, lifted, p);
     read_seeds(io, pm, p, lifted);
 
     q.export_values = io.get_scalar("exportValues", 0.0, 2) != 0;

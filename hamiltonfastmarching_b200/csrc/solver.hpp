@@ -51,6 +51,7 @@ struct EulerProblem {
     bool mult_inverse = false;
 
     std::vector<uint8_t> walls;        // [N] or empty
+    const double *walls_f64 = nullptr; // [N] host view of a full walls field (nonzero = wall), instead of `walls`
     // Device-resident alternatives (zero-copy path): used instead of `metric` / `walls` when set,
     // and `d_values_out` receives the FP64 arrival times instead of EulerResult::values.
     const double *d_metric = nullptr;
