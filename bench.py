@@ -228,9 +228,9 @@ def batched_leg(args, rank, world):
     for k in range(len(ios)):
         fams.setdefault(ios[k].get_string("model"), []).append(k)
     for fam, ks in fams.items():
-        # a quarter of the family's instances (every fourth): a batch large enough to load the GPU
-        # as the full batch does, at a quarter of the tuning time
-        tuned[fam] = at.tune([cases[k] for k in ks[::4]], sweeps=1)
+        # on the family's own batch (the schedule is tuned for the batch it will run), over sweeps
+        # and queue policy (tile shapes seldom win on these grids and double the search)
+        tuned[fam] = at.tune([cases[k] for k in ks], sweeps=1, params=("tileSweeps", "queue"))
     tune_s = time.perf_counter() - t0
     for k, io in enumerate(ios):
         t = at.lookup(cases[k])

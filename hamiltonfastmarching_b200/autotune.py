@@ -107,9 +107,10 @@ class Autotuner:
                             "seconds": best})
         return best
 
-    def tune(self, cases: List[Dict], sweeps: int = 2) -> Dict:
-        """Coordinate search over tile shape, sweeps and queue policy on a sample of instances of one
-        family; returns (and records) the best configuration and its time against the defaults."""
+    def tune(self, cases: List[Dict], sweeps: int = 2, params=("tileShape", "tileSweeps", "queue")) -> Dict:
+        """Coordinate search over `params` (of tile shape, sweeps and queue policy) on a sample of
+        instances of one family; returns (and records) the best configuration and its time against
+        the defaults. A candidate replaces the incumbent only if it is 2% faster."""
         kind = _domain_kind(cases[0])
         cfg = dict(DEFAULT[cases[0]["model"]], tileShape=SPACE["tileShape"][kind][0])
         base = self.measure(cases, cfg)
@@ -118,6 +119,8 @@ class Autotuner:
             improved = False
             for name, values in (("tileShape", SPACE["tileShape"][kind]), ("tileSweeps", SPACE["tileSweeps"]),
                                  ("queue", SPACE["queue"])):
+                if name not in params:
+                    continue
                 for v in values:
                     if v == cfg[name]:
                         continue
