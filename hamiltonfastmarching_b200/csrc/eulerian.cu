@@ -778,22 +778,33 @@ __global__ void tti_scale_kernel(Dev<Real> P, const double *metric, double *out)
 template <typename Real, int NSYM>
 __global__ void width_kernel(Dev<Real> P, unsigned *maxw) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (x >= P.ncells) return;
-    const CellRef R = cell_ref(P.inst, P.ninst, x);
-    const GridGeom &g = P.inst[R.i].g;
-    int best = 0;
+    const bool in = x < P.ncells;
+    int i = -1;
+    unsigned best = 0;
+    if (in) {
+        const CellRef R = cell_ref(P.inst, P.ninst, x);
+        i = R.i;
+        const GridGeom &g = P.inst[R.i].g;
 #pragma unroll
-    for (int k = 0; k < NSYM; ++k) {
-        if (P.weight[k * P.ntc + R.c] == Real(0)) continue;
-        const unsigned cd = P.code[k * P.ntc + R.c];
-        const int o0 = off_c(cd, 0), o1 = off_c(cd, 1), o2 = off_c(cd, 2);
-        const int l1 = abs(o0) + abs(o1) + abs(o2);
-        for (int s = 1; s >= -1; s -= 2) {
-            int n0 = R.x0 + s * o0, n1 = R.x1 + s * o1, n2 = R.x2 + s * o2;
-            if (g.wrap(n0, n1, n2) && l1 > best) best = l1;
+        for (int k = 0; k < NSYM; ++k) {
+            if (P.weight[k * P.ntc + R.c] == Real(0)) continue;
+            const unsigned cd = P.code[k * P.ntc + R.c];
+            const int o0 = off_c(cd, 0), o1 = off_c(cd, 1), o2 = off_c(cd, 2);
+            const unsigned l1 = abs(o0) + abs(o1) + abs(o2);
+            for (int s = 1; s >= -1; s -= 2) {
+                int n0 = R.x0 + s * o0, n1 = R.x1 + s * o1, n2 = R.x2 + s * o2;
+                if (g.wrap(n0, n1, n2) && l1 > best) best = l1;
+            }
         }
     }
-    if (best) atomicMax(maxw + R.i, (unsigned)best);
+    // one atomic per (warp, instance) instead of one per cell on a single word
+    const unsigned same = __match_any_sync(0xffffffffu, i);
+    const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+    for (int o = 0; o < 32; ++o) {
+        const unsigned w = __shfl_sync(0xffffffffu, best, o);
+        if (lane == leader && ((same >> o) & 1u) && w > best) best = w;
+    }
+    if (in && lane == leader && best) atomicMax(maxw + i, best);
 }
 
 // Speed multiplier to the tile-major layout (shared stencils).
