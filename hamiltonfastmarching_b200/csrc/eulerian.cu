@@ -87,8 +87,10 @@ constexpr int kWarpsPerCta = 4;
 constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2;
 // Value increases a tile may take before it accepts decreases only (termination guard).
 constexpr unsigned kUpBudget = 128;
-constexpr int kDepWarps = 2;
-constexpr int kDepCap = 1024;
+// Tile dependency tables: a small hash table per warp first (fast, high occupancy), the large one
+// only for grids whose tiles read more distinct tiles (detected by the overflow status).
+constexpr int kDepCapSmall = 128, kDepWarpsSmall = 4;
+constexpr int kDepCapLarge = 1024, kDepWarpsLarge = 2;
 constexpr unsigned long long kBarrierPolls = 1ull << 25;
 
 __host__ __device__ __forceinline__ unsigned pack_off(int o0, int o1, int o2) {
@@ -992,7 +994,7 @@ __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *va
 // Tile dependency graph. Pass 0 counts, pass 1 writes, for every tile D, the distinct source
 // tiles T != D its visible stencil entries read, with the 64-bit mask of the cells read in T.
 
-template <typename Real, int NFWD, int NSYM, int KIND>
+template <typename Real, int NFWD, int NSYM, int KIND, int kDepCap, int kDepWarps>
 __global__ void __launch_bounds__(kDepWarps * 32)
     deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
                 unsigned long long *msk, unsigned long long *dmsk) {
@@ -1938,9 +1940,29 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
 
     // ---- tile dependency graph (reverse CSR over the global tile space)
     DeviceBuffer<unsigned> dcnt(nt);
-    launch(deps_kernel<Real, NFWD, NSYM, KIND>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 0, dcnt.get(),
-           nullptr, nullptr, nullptr, nullptr, nullptr);
-    HFM_CUDA(cudaGetLastError());
+    auto deps_pass = [&](bool large, int pass, const long long *offs, int *src, int *dst, unsigned long long *msk,
+                         unsigned long long *dmsk) {
+        if (large)
+            launch(deps_kernel<Real, NFWD, NSYM, KIND, kDepCapLarge, kDepWarpsLarge>, nblocks(nt, kDepWarpsLarge),
+                   kDepWarpsLarge * 32, 0, s, P, pass, dcnt.get(), offs, src, dst, msk, dmsk);
+        else
+            launch(deps_kernel<Real, NFWD, NSYM, KIND, kDepCapSmall, kDepWarpsSmall>, nblocks(nt, kDepWarpsSmall),
+                   kDepWarpsSmall * 32, 0, s, P, pass, dcnt.get(), offs, src, dst, msk, dmsk);
+        HFM_CUDA(cudaGetLastError());
+    };
+    bool large_deps = false;
+    deps_pass(false, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
+    {
+        unsigned st = 0;
+        status.download(&st, 1, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        if (st & kErrTableOverflow) {  // some tile reads more distinct tiles than the small table holds
+            const unsigned keep = st & ~(unsigned)kErrTableOverflow;
+            HFM_CUDA(cudaMemcpyAsync(status.get(), &keep, sizeof(unsigned), cudaMemcpyHostToDevice, s));
+            large_deps = true;
+            deps_pass(true, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
+        }
+    }
     DeviceBuffer<long long> doff(nt + 1), rptr(nt + 1);
     std::vector<unsigned> hc(nt);
     dcnt.download(hc.data(), nt, s);
@@ -1956,9 +1978,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     {
         DeviceBuffer<int> esrc(nE), edst(nE);
         DeviceBuffer<unsigned long long> emsk(nE), edmsk(nE);
-        if (nE)
-            launch(deps_kernel<Real, NFWD, NSYM, KIND>, nblocks(nt, kDepWarps), kDepWarps * 32, 0, s, P, 1, nullptr,
-                   doff.get(), esrc.get(), edst.get(), emsk.get(), edmsk.get());
+        if (nE) deps_pass(large_deps, 1, doff.get(), esrc.get(), edst.get(), emsk.get(), edmsk.get());
         DeviceBuffer<unsigned> rcnt(nt), cursor(nt);
         rcnt.zero(s);
         cursor.zero(s);
