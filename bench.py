@@ -446,12 +446,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from hamiltonfastmarching_b200.replicas import max_over_ranks
 
     L = _lib.load()
     n = args.side
