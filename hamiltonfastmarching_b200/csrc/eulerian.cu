@@ -573,7 +573,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 template <typename Real, int NFWD, int NSYM, int KIND>
 constexpr int fim_min_blocks() {
     [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
-    return KIND == kKindTTI ? 1 : SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 6;
+    return KIND == kKindTTI ? 1 : SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 8;
 }
 
 template <typename Real, int NFWD, int NSYM, int KIND>
