@@ -50,7 +50,7 @@ def parse_args(argv=None):
     ap.add_argument("--batch-riemann", type=int, default=384, help="Riemann2 instances of the batched mix")
     ap.add_argument("--batch-lifted", type=int, default=128, help="ReedsShepp2/Elastica2 instances of the mix")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-model leg")
-    ap.add_argument("--serve-rates", default="50,200", help="Poisson arrival rates (req/s) of the serving leg")
+    ap.add_argument("--serve-rates", default="50,200,1000", help="Poisson arrival rates (req/s) of the serving leg")
     ap.add_argument("--serve-requests", type=int, default=200, help="requests per arrival rate")
     ap.add_argument("--serve-pool", type=int, default=48, help="distinct request payloads the arrivals draw from")
     ap.add_argument("--serve-lanes", type=int, default=2)

@@ -1,8 +1,8 @@
 // Request loop for serving solves: continuous batching over lanes, admission by device memory.
 //
 // The reference answers one Run(IO&) at a time (Headers/DispatchAndRun.h:224-244). Here a client
-// submits filled stores; `lanes` worker threads each own a CUDA stream and 1/lanes of the SMs for
-// the persistent solver kernel. A lane that is free takes, in arrival order, the waiting requests
+// submits filled stores; `lanes` worker threads each own a CUDA stream; a batch started while
+// others run gives its persistent solver 1/lanes of the SMs, a batch started alone the whole GPU. A lane that is free takes, in arrival order, the waiting requests
 // whose estimated device footprint fits in what the running batches leave of the memory budget
 // (up to max_batch of them) and solves them as one batch (hfm_run_batch: instances of a family
 // share a launch sequence). Requests that arrive while other batches are on the device are
@@ -89,7 +89,6 @@ struct hfm_server {
         const bool ok = cudaSetDevice(cfg.device) == cudaSuccess &&
                         cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess;
         hfm::current_stream() = stream;
-        hfm::solver_share() = cfg.lanes;
         std::vector<Request *> batch;
         std::vector<hfm_io *> ios;
         std::vector<int> codes;
@@ -111,6 +110,10 @@ struct hfm_server {
                 in_use += bytes;
                 peak = std::max(peak, in_use);
                 ++running;
+                // SM share of this batch's persistent solver: the whole GPU when it runs alone (low
+                // load: the latency of a plain solve), 1/lanes when other batches are on the device
+                // (their solvers then run side by side)
+                hfm::solver_share() = running > 1 ? cfg.lanes : 1;
                 const double t = now();
                 for (Request *r : batch) r->t_start = t;
                 if (!queue.empty()) cv_work.notify_one();  // leave the rest to another free lane

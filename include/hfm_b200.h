@@ -96,7 +96,8 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
 
 /* ---------------------------------------------------------------------------------------------
  * Serving (an extension: the reference answers one Run(IO&) at a time). A server owns `lanes`
- * worker threads, each with its own CUDA stream and 1/lanes of the SMs for the persistent solver.
+ * worker threads, each with its own CUDA stream; a batch's persistent solver takes the whole GPU
+ * when it starts alone and 1/lanes of the SMs when other batches are running.
  * A free lane takes the waiting requests in arrival order while their estimated device footprint
  * fits in the memory budget left by the running batches (at most max_batch of them) and solves
  * them as one hfm_run_batch; requests arriving meanwhile are admitted by the next lane to free up,
