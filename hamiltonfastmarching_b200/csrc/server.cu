@@ -2,7 +2,8 @@
 //
 // The reference answers one Run(IO&) at a time (Headers/DispatchAndRun.h:224-244). Here a client
 // submits filled stores; `lanes` worker threads each own a CUDA stream; a batch started while
-// others run gives its persistent solver 1/lanes of the SMs, a batch started alone the whole GPU. A lane that is free takes, in arrival order, the waiting requests
+// others run gives its persistent solver 1/lanes of the SMs, a batch started alone the whole GPU.
+// A lane that is free takes, in arrival order, the waiting requests
 // whose estimated device footprint fits in what the running batches leave of the memory budget
 // (up to max_batch of them) and solves them as one batch (hfm_run_batch: instances of a family
 // share a launch sequence). Requests that arrive while other batches are on the device are
