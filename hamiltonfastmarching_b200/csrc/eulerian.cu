@@ -1146,8 +1146,22 @@ __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
     constexpr int ND = NFWD + NSYM;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= P.ncells) return;
-    if constexpr (KIND == kKindTTI) {  // no bitset for the semi-Lagrangian scheme
-        active[x] = 0ull;
+    if constexpr (KIND == kKindTTI) {
+        // the semi-Lagrangian scheme records the extremum t instead of a bitset (TTI.h:45-60):
+        // t at an interior extremum, -t at an interval endpoint, +inf where no update was made;
+        // the bits of that double are stored
+        const CellRef R = cell_ref(P.inst, P.ninst, x);
+        const Inst &I = P.inst[R.i];
+        bool fixed, dead;
+        cell_flags<Real, KIND>(P, R.c, fixed, dead);
+        double code = Arith<double>::inf();
+        if (!fixed && !dead && (double)P.values[x] < Arith<double>::inf()) {
+            double ta = Arith<double>::inf();
+            bool inner = false;
+            solve_cell_tti<Real>(P, I, R.c, R.x0, R.x1, R.x2, 0, 0, 0, nullptr, &ta, &inner);
+            code = inner ? ta : -ta;
+        }
+        active[x] = (unsigned long long)__double_as_longlong(code);
         return;
     }
     const CellRef R = cell_ref(P.inst, P.ninst, x);

@@ -304,8 +304,6 @@ void setup_tti(Store &io, Param &pm, EulerProblem &p) {
         throw Error(HFM_ERR_UNSUPPORTED, "TTI3 with nmix > 0 (finite envelope) is not supported by the GPU solve path");
     if (io.has_field("walls"))
         throw Error(HFM_ERR_UNSUPPORTED, "TTI3 with walls is not supported by the GPU solve path");
-    if (io.get_scalar("exportActiveNeighs", 0.0, 3) != 0)
-        throw Error(HFM_ERR_UNSUPPORTED, "activeNeighs export is not supported for TTI3 by the GPU solve path");
     p.ndim = ndim;
     p.kind = StencilKind::TTI;
     p.nfwd = 0;
@@ -515,7 +513,10 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
     if (q.export_values && !q.values_dst) io.set_field("values", dims, 1, r.values.data());
     if (q.export_active) {
         std::vector<double> a(r.active.size());
-        for (size_t i = 0; i < a.size(); ++i) a[i] = (double)r.active[i];
+        if (q.p.kind == StencilKind::TTI)  // the extremum t, stored as the bits of a double
+            std::memcpy(a.data(), r.active.data(), a.size() * sizeof(double));
+        else
+            for (size_t i = 0; i < a.size(); ++i) a[i] = (double)r.active[i];
         io.set_field("activeNeighs", dims, 1, a.data());
     }
     for (size_t gi = 0; gi < r.adjoints.size(); ++gi) {

@@ -149,3 +149,14 @@ def test_autotuner_picks_a_valid_schedule_and_values_do_not_change():
                      (W.curvature2_case(32, 24, "ReedsShepp2", seed=4, n_curves=4), [2, 2, 16])):
         assert _same(hfm.run(dict(p, tileShape=np.array(shape, float)))["values"], _alone(p),
                      p.get("solverPrecision", "float64"))
+
+
+def test_batch_tti3_instances_equal_alone():
+    cases = []
+    for n, seed in ((16, 1), (24, 2), (12, 3)):
+        p = W.tti3_case(n, h=0.01, seed=seed)
+        p.pop("_vp")
+        cases.append(p)
+    out = hfm.run_batch(cases)
+    for p, o in zip(cases, out):
+        assert _same(o["values"], _alone(p))

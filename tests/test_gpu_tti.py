@@ -45,6 +45,19 @@ def test_tti_matches_oracle(n, seed):
     assert int(out["nAccepted"]) == ref["nAccepted"]
 
 
+def test_tti_active_neighs_encoding():
+    """activeNeighs of TTI3: the extremum t (negative at an interval endpoint), as the reference
+    exports it; flat extrema make the endpoint/interior label and t agree only to rounding on a
+    few cells."""
+    params, ref, _ = load_golden("tti3_16")
+    out = hfm.run(dict(params, exportActiveNeighs=1.0))
+    a, b = out["activeNeighs"], ref["activeNeighs"]
+    assert np.array_equal(np.isinf(a), np.isinf(b))
+    fin = np.isfinite(b)
+    assert np.mean(np.abs(np.abs(a[fin]) - np.abs(b[fin])) < 1e-6) > 0.95
+    assert np.mean(np.abs(a[fin] - b[fin]) < 1e-6) > 0.9
+
+
 def test_tti_rejects_what_the_gpu_path_does_not_do():
     p = W.tti3_case(8, h=0.01, seed=1)
     p.pop("_vp")
