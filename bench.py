@@ -343,7 +343,7 @@ def serving_leg(args, rank, world):
             t.wait()
     out = []
     for r in rates:
-        served = run_arm(args.serve_lanes, 256, r, seed=11 + int(r))
+        served = run_arm(args.serve_lanes, 64, r, seed=11 + int(r))
         plain = run_arm(1, 1, r, seed=11 + int(r))
         out.append({"rate_req_per_s": r, "served": served, "plain_one_at_a_time": plain,
                     "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"],

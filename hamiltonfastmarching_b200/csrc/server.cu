@@ -156,7 +156,7 @@ hfm_server *hfm_server_create(const hfm_server_config *cfg) {
         auto s = std::make_unique<hfm_server>();
         if (cfg) s->cfg = *cfg;
         if (s->cfg.lanes <= 0) s->cfg.lanes = 2;
-        if (s->cfg.max_batch <= 0) s->cfg.max_batch = 256;
+        if (s->cfg.max_batch <= 0) s->cfg.max_batch = 64;
         if (cudaSetDevice(s->cfg.device) != cudaSuccess) return nullptr;
         hfm::keep_pool_cached();
         size_t free_b = 0, total_b = 0;

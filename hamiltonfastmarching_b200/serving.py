@@ -52,7 +52,7 @@ class Ticket:
 
 
 class Server:
-    def __init__(self, lanes: int = 2, max_batch: int = 256, hbm_budget_bytes: float = 0.0, device: int = 0):
+    def __init__(self, lanes: int = 2, max_batch: int = 64, hbm_budget_bytes: float = 0.0, device: int = 0):
         self._L = _lib.load()
         cfg = _lib.ServerConfig(device, lanes, max_batch, float(hbm_budget_bytes))
         self._h = self._L.hfm_server_create(ctypes.byref(cfg))

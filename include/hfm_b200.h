@@ -109,7 +109,7 @@ typedef struct hfm_server hfm_server;
 typedef struct {
     int device;              /* CUDA device ordinal                                           */
     int lanes;               /* concurrent batches (default 2)                                 */
-    int max_batch;           /* requests per batch at most (default 256)                       */
+    int max_batch;           /* requests per batch at most (default 64)                        */
     double hbm_budget_bytes; /* admission budget; <= 0: 80% of the free device memory          */
 } hfm_server_config;
 typedef struct {
