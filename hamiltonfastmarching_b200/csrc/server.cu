@@ -102,7 +102,10 @@ struct hfm_server {
                 });
                 if (queue.empty()) break;  // stopping
                 batch.clear();
-                while (!queue.empty() && (int)batch.size() < cfg.max_batch &&
+                // leave a fair share of the waiting requests to the other free lanes
+                const int free_lanes = std::max(1, cfg.lanes - running);
+                const int limit = std::min<int>(cfg.max_batch, ((int)queue.size() + free_lanes - 1) / free_lanes);
+                while (!queue.empty() && (int)batch.size() < limit &&
                        in_use + bytes + queue.front()->bytes <= budget) {
                     bytes += queue.front()->bytes;
                     batch.push_back(queue.front());
