@@ -82,7 +82,7 @@ __host__ __device__ __forceinline__ void sym_inverse(const double *m, double *ou
 // Returns false if the matrix is rejected or Selling does not terminate within 200 sweeps.
 template <int D>
 __host__ __device__ bool tensor_decomposition(const double *d, int off[6][3], double w[6]) {
-    if (sym_det<D>(d) <= 0.0 || sym_trace<D>(d) <= 0.0) return false;
+    if (!(sym_det<D>(d) > 0.0) || !(sym_trace<D>(d) > 0.0)) return false;  // NaN too
     int sb[4][3];
 #pragma unroll
     for (int i = 0; i <= D; ++i)
