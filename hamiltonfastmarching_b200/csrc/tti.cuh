@@ -119,7 +119,7 @@ __host__ __device__ inline bool tti_setup(const double *m, const double *h, TTIC
     // obtuse superbase of D(tmin), from the canonical one
     double D[6];
     for (int k = 0; k < 6; ++k) D[k] = (1. - tmin) * n.D0[k] + tmin * n.D1[k];
-    if (sym_det<3>(D) <= 0.0 || sym_trace<3>(D) <= 0.0) return false;
+    if (!(sym_det<3>(D) > 0.0) || !(sym_trace<3>(D) > 0.0)) return false;  // NaN too
     int sb[4][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {-1, -1, -1}};
     bool reduced = true;
     for (int it = 0; reduced && it < 200; ++it) {
@@ -377,7 +377,7 @@ __host__ __device__ inline int tti_neighbors(const TTICell &n, int (*out)[3], in
 __host__ __device__ inline bool tti_path_at(const TTICell &n, double t, TTIPath &P) {
     double D[6];
     for (int k = 0; k < 6; ++k) D[k] = (1. - t) * n.D0[k] + t * n.D1[k];
-    if (sym_det<3>(D) <= 0.0 || sym_trace<3>(D) <= 0.0) return false;
+    if (!(sym_det<3>(D) > 0.0) || !(sym_trace<3>(D) > 0.0)) return false;  // NaN too
     int sb[4][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {-1, -1, -1}};
     bool reduced = true;
     for (int it = 0; reduced && it < 200; ++it) {
