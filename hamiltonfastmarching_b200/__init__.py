@@ -62,6 +62,11 @@ class HFMIO:
     def run(self, expected_model: str = None):
         self._check(self._L.hfm_run(self._h, expected_model.encode() if expected_model else None))
 
+    def run_sensitivity(self):
+        """Reverse first variation for the inspectSensitivity keys now set, from the device state
+        of the last ``run`` with ``retainState = 1`` (no new solve); fills costSensitivity_i."""
+        self._check(self._L.hfm_run_sensitivity(self._h))
+
     def set_scalar(self, key: str, value: float):
         self._check(self._L.hfm_io_set_scalar(self._h, key.encode(), float(value)))
 

@@ -36,6 +36,7 @@ SIGNATURES = {
     "hfm_io_computed_keys": ([_P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
     "hfm_run": ([_P, _S], _I),
     "hfm_run_batch": ([_P, _I, _S, ctypes.POINTER(_I)], _I),
+    "hfm_run_sensitivity": ([_P], _I),
     "hfm_io_last_error": ([_P], _S),
     "hfm_version": ([], _S),
     "hfm_device_count": ([ctypes.POINTER(_I)], _I),

@@ -28,7 +28,7 @@ from typing import Dict
 import numpy as np
 import torch
 
-from . import run as _run
+from . import HFMIO
 
 __all__ = ["EikonalSolve", "arrival_times"]
 
@@ -72,30 +72,36 @@ def _cell_centres(params: Dict, idx: np.ndarray) -> np.ndarray:
 
 
 class EikonalSolve(torch.autograd.Function):
-    """values = solve(params, cost); backward through the GPU adjoint."""
+    """values = solve(params, cost); backward through the GPU adjoint. The forward solve keeps its
+    device state (retainState), so the backward pass is one reverse sweep, not a second solve."""
 
     @staticmethod
     def forward(ctx, cost: torch.Tensor, params: Dict):
         c = cost.detach().to("cpu", torch.float64).numpy()
-        out = _run(_with_cost(params, c))
-        ctx.params = params
+        io = HFMIO("RowMajor")
+        io.set_dict(_with_cost(params, c), views=True)
+        io.set_scalar("retainState", 1.0)
+        io.run()
+        values = io.get_array("values")
+        ctx.params, ctx.io = params, io
         ctx.save_for_backward(cost)
-        return torch.from_numpy(np.array(out["values"])).to(device=cost.device, dtype=cost.dtype)
+        return torch.from_numpy(values).to(device=cost.device, dtype=cost.dtype)
 
     @staticmethod
     def backward(ctx, grad: torch.Tensor):
         (cost,) = ctx.saved_tensors
-        params = ctx.params
+        params, io = ctx.params, ctx.io
+        ctx.io = None  # the device state is released with the store
         c = cost.detach().to("cpu", torch.float64).numpy()
         g = grad.detach().to("cpu", torch.float64).numpy().ravel()
         idx = np.flatnonzero(g)
         if idx.size == 0:
             return torch.zeros_like(cost), None
-        p = _with_cost(params, c)
-        p["inspectSensitivity"] = _cell_centres(params, idx)
-        p["inspectSensitivityWeights"] = g[idx]
-        p["inspectSensitivityLengths"] = np.array([float(idx.size)])
-        sens = _run(p)["costSensitivity_0"]
+        io.set_array("inspectSensitivity", _cell_centres(params, idx))
+        io.set_array("inspectSensitivityWeights", g[idx])
+        io.set_array("inspectSensitivityLengths", np.array([float(idx.size)]))
+        io.run_sensitivity()
+        sens = io.get_array("costSensitivity_0")
         if params["model"] in _CURVATURE:
             gc = sens
             if gc.shape != c.shape:  # physical (x, y) cost field: sum over the angular axis

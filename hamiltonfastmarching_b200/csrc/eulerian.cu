@@ -1657,6 +1657,36 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     }
 }
 
+// The device state that the reverse sweep reads (RetainedSolve of a single-instance solve).
+template <typename Real, int NFWD, int NSYM, int KIND>
+struct Retained final : RetainedSolve {
+    Dev<Real> P{};
+    long long N = 0;
+    DeviceBuffer<Inst> dinst;
+    DeviceBuffer<int> tile_inst;
+    DeviceBuffer<unsigned> status, code, vis;
+    DeviceBuffer<Real> values, weight, mult, cls_w;
+    DeviceBuffer<int8_t> cls_off;
+    DeviceBuffer<TTICell> tti;
+    void adjoint(const EulerProblem &p, EulerResult &res) override {
+        cudaStream_t s = current_stream();
+        // arrival times (RowMajor, FP64) for the ordering of the sensitive seeds
+        std::vector<Real> v(N);
+        values.download(v.data(), N, s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+        res.values.assign(v.begin(), v.end());
+        EulerProblem q;
+        q.adjoint_index = p.adjoint_index;
+        q.adjoint_weight = p.adjoint_weight;
+        status.zero(s);
+        EventTimer tm;
+        tm.start(s);
+        run_adjoint<Real, NFWD, NSYM, KIND>(P, N, q, res, status, s);
+        res.t_adjoint_ms = tm.stop(s);
+        HFM_CUDA(cudaStreamSynchronize(s));
+    }
+};
+
 template <typename Real, int NFWD, int NSYM, int KIND>
 void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
     [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
@@ -2145,6 +2175,23 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     HFM_CUDA(cudaStreamSynchronize(s));
     HFM_CUDA(cudaGetLastError());
+    if (ninst == 1 && p0.retain) {
+        auto r = std::make_shared<Retained<Real, NFWD, NSYM, KIND>>();
+        r->P = P;
+        r->N = N;
+        r->dinst = std::move(dinst);
+        r->tile_inst = std::move(tile_inst);
+        r->status = std::move(status);
+        r->code = std::move(code);
+        r->vis = std::move(vis);
+        r->values = std::move(values);
+        r->weight = std::move(weight);
+        r->mult = std::move(mult);
+        r->cls_w = std::move(cls_w);
+        r->cls_off = std::move(cls_off);
+        r->tti = std::move(ttibuf);
+        results[0].retained = r;
+    }
     const double total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall_t0).count();
     for (EulerResult &r : results) r.t_total_ms = total;
 }

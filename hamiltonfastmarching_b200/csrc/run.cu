@@ -411,6 +411,43 @@ void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProble
     }
 }
 
+// inspectSensitivity groups (FirstVariation::Finally, FirstVariation.h:60-102): weighted points.
+void read_inspect(Store &io, const Param &pm, EulerProblem &p) {
+    p.adjoint_index.clear();
+    p.adjoint_weight.clear();
+    // FirstVariation::Finally (FirstVariation.h:60-102): groups of weighted points
+    int64_t n = 0;
+    const std::vector<double> pts = io.get_vector("inspectSensitivity", pm.ndim, &n);
+    std::vector<double> lengths(n, 1.0);
+    if (io.has_field("inspectSensitivityLengths")) {
+        int64_t nl = 0;
+        lengths = io.get_vector("inspectSensitivityLengths", 1, &nl);
+        double tot = 0;
+        for (double l : lengths) tot += l;
+        if (tot != (double)n) throw Error(HFM_ERR_VALUE, "Error : inconsistent inspectSensitivityLengths");
+    }
+    std::vector<double> weights(n, 1.0);
+    if (io.has_field("inspectSensitivityWeights")) {
+        int64_t nw = 0;
+        weights = io.get_vector("inspectSensitivityWeights", 1, &nw);
+        if (nw != n) throw Error(HFM_ERR_VALUE, "Error: Inconsistent inspectSensitivityWeights size");
+    }
+    int64_t pos = 0;
+    for (size_t gi = 0; gi < lengths.size(); ++gi) {
+        std::vector<int64_t> idx;
+        std::vector<double> wts;
+        for (int64_t k = 0; k < (int64_t)lengths[gi]; ++k, ++pos) {
+            int64_t lin;
+            if (!pm.index_of(&pts[pos * pm.ndim], &lin))
+                throw Error(HFM_ERR_VALUE, "Error : inspectSensitivity data points are out of range");
+            idx.push_back(lin);
+            wts.push_back(weights[pos]);
+        }
+        p.adjoint_index.push_back(std::move(idx));
+        p.adjoint_weight.push_back(std::move(wts));
+    }
+}
+
 // A model read from its store, ready to solve (the part of Run before the solver loop).
 struct Prepared {
     Param pm;
@@ -444,6 +481,7 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     read_seeds(io, pm, p, lifted);
 
     q.export_values = io.get_scalar("exportValues", 0.0, 2) != 0;
+    p.retain = io.get_scalar("retainState", 0.0, 3) != 0;
     q.export_active = io.get_scalar("exportActiveNeighs", 0.0, 3) != 0;
     const bool inspect = io.has_field("inspectSensitivity");
     p.want_active = q.export_active;
@@ -454,42 +492,33 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
         q.skip = true;
         return;
     }
-    if (inspect) {
-        // FirstVariation::Finally (FirstVariation.h:60-102): groups of weighted points
-        int64_t n = 0;
-        const std::vector<double> pts = io.get_vector("inspectSensitivity", pm.ndim, &n);
-        std::vector<double> lengths(n, 1.0);
-        if (io.has_field("inspectSensitivityLengths")) {
-            int64_t nl = 0;
-            lengths = io.get_vector("inspectSensitivityLengths", 1, &nl);
-            double tot = 0;
-            for (double l : lengths) tot += l;
-            if (tot != (double)n) throw Error(HFM_ERR_VALUE, "Error : inconsistent inspectSensitivityLengths");
-        }
-        std::vector<double> weights(n, 1.0);
-        if (io.has_field("inspectSensitivityWeights")) {
-            int64_t nw = 0;
-            weights = io.get_vector("inspectSensitivityWeights", 1, &nw);
-            if (nw != n) throw Error(HFM_ERR_VALUE, "Error: Inconsistent inspectSensitivityWeights size");
-        }
-        int64_t pos = 0;
-        for (size_t gi = 0; gi < lengths.size(); ++gi) {
-            std::vector<int64_t> idx;
-            std::vector<double> wts;
-            for (int64_t k = 0; k < (int64_t)lengths[gi]; ++k, ++pos) {
-                int64_t lin;
-                if (!pm.index_of(&pts[pos * pm.ndim], &lin))
-                    throw Error(HFM_ERR_VALUE, "Error : inspectSensitivity data points are out of range");
-                idx.push_back(lin);
-                wts.push_back(weights[pos]);
-            }
-            p.adjoint_index.push_back(std::move(idx));
-            p.adjoint_weight.push_back(std::move(wts));
-        }
-    }
+    if (inspect) read_inspect(io, pm, p);
     // the arrival times are downloaded straight into the output field when no reordering is needed
     q.values_dst = q.export_values ? io.create_field("values", q.dims, 1) : nullptr;
     p.h_values_out = q.values_dst;
+}
+
+// costSensitivity_i and seedSensitivity_i (point, weight) of each inspection group.
+void export_sensitivities(Store &io, const Param &pm, const std::vector<int64_t> &dims,
+                          const std::vector<AdjointResult> &adjoints) {
+    for (size_t gi = 0; gi < adjoints.size(); ++gi) {
+        const AdjointResult &ar = adjoints[gi];
+        io.set_field("costSensitivity_" + std::to_string(gi), dims, 1, ar.sensitivity.data());
+        std::vector<double> ss;
+        for (size_t k = 0; k < ar.seed_index.size(); ++k) {
+            int64_t x = ar.seed_index[k];
+            double q[3];
+            for (int a = pm.ndim - 1; a >= 0; --a) {
+                const int64_t i = x % pm.dims[a];
+                x /= pm.dims[a];
+                q[a] = (i + 0.5) * pm.scale[a] + pm.origin[a];  // ReDim(PointFromIndex)
+            }
+            for (int a = 0; a < pm.ndim; ++a) ss.push_back(q[a]);
+            ss.push_back(ar.seed_weight[k]);
+        }
+        io.set_vector("seedSensitivity_" + std::to_string(gi), (int64_t)ar.seed_index.size(), pm.ndim + 1,
+                      ss.data());
+    }
 }
 
 void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
@@ -519,29 +548,19 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
             for (size_t i = 0; i < a.size(); ++i) a[i] = (double)r.active[i];
         io.set_field("activeNeighs", dims, 1, a.data());
     }
-    for (size_t gi = 0; gi < r.adjoints.size(); ++gi) {
-        const AdjointResult &ar = r.adjoints[gi];
-        io.set_field("costSensitivity_" + std::to_string(gi), dims, 1, ar.sensitivity.data());
-        std::vector<double> ss;
-        for (size_t k = 0; k < ar.seed_index.size(); ++k) {
-            int64_t x = ar.seed_index[k];
-            double q[3];
-            for (int a = pm.ndim - 1; a >= 0; --a) {
-                const int64_t i = x % pm.dims[a];
-                x /= pm.dims[a];
-                q[a] = (i + 0.5) * pm.scale[a] + pm.origin[a];  // ReDim(PointFromIndex)
-            }
-            for (int a = 0; a < pm.ndim; ++a) ss.push_back(q[a]);
-            ss.push_back(ar.seed_weight[k]);
-        }
-        io.set_vector("seedSensitivity_" + std::to_string(gi), (int64_t)ar.seed_index.size(), pm.ndim + 1,
-                      ss.data());
-    }
+    export_sensitivities(io, pm, dims, r.adjoints);
     io.set_scalar("nAccepted", (double)r.n_accepted);
 }
 
 
-void run_model(Store &io, const std::string &model) {
+// The device state of the last retainState solve of a store, with its grid description.
+struct RetainedCtx {
+    std::shared_ptr<RetainedSolve> solve;
+    Param pm;
+    std::vector<int64_t> dims;
+};
+
+void run_model(Store &io, const std::string &model, std::shared_ptr<void> *retained) {
     Prepared q;
     prepare_model(io, model, q);
     if (q.skip) return;
@@ -553,6 +572,30 @@ void run_model(Store &io, const std::string &model) {
         throw;
     }
     finish_model(io, q, r);
+    if (retained) {
+        if (r.retained) {
+            auto ctx = std::make_shared<RetainedCtx>();
+            ctx->solve = r.retained;
+            ctx->pm = q.pm;
+            ctx->dims = q.dims;
+            *retained = ctx;
+        } else {
+            retained->reset();
+        }
+    }
+}
+
+// Reverse first variation of the retained solve for the inspectSensitivity keys now in the store.
+void run_sensitivity(Store &io, const std::shared_ptr<void> &retained) {
+    if (!retained) throw Error(HFM_ERR_ARG, "no retained solve on this store (run it with retainState = 1)");
+    const RetainedCtx &ctx = *static_cast<const RetainedCtx *>(retained.get());
+    if (!io.has_field("inspectSensitivity")) throw Error(HFM_ERR_KEY, "BaseIO import error : field inspectSensitivity not found.");
+    EulerProblem p;
+    read_inspect(io, ctx.pm, p);
+    EulerResult r;
+    ctx.solve->adjoint(p, r);
+    export_sensitivities(io, ctx.pm, ctx.dims, r.adjoints);
+    io.set_scalar("GPUAdjointTime", r.t_adjoint_ms * 1e-3);
 }
 
 }  // namespace
@@ -715,7 +758,7 @@ int hfm_run(hfm_io *io, const char *expected_model) {
             hfm::Store &s;
             ~Restore() { s.current_setter = hfm::Setter::User; }
         } restore{st};
-        hfm::run_model(st, model == "Elastica2_5" ? "Elastica2" : model);
+        hfm::run_model(st, model == "Elastica2_5" ? "Elastica2" : model, &io->retained);
         st.usage_report();
     });
 }
@@ -737,6 +780,7 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
                             std::string("Executable applies to ") + expected_model + ", not to " + model + ".");
             auto q = std::make_unique<hfm::Prepared>();
             hfm::prepare_model(st, model == "Elastica2_5" ? "Elastica2" : model, *q);
+            q->p.retain = false;  // device state is retained by hfm_run only
             qs[i] = std::move(q);
         });
     }
@@ -802,6 +846,18 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
         if (first == HFM_OK) first = rc[i];
     }
     return first;
+}
+
+int hfm_run_sensitivity(hfm_io *io) {
+    return guarded(io, [&] {
+        hfm::Store &st = io->store;
+        st.current_setter = hfm::Setter::Compute;
+        struct Restore {
+            hfm::Store &s;
+            ~Restore() { s.current_setter = hfm::Setter::User; }
+        } restore{st};
+        hfm::run_sensitivity(st, io->retained);
+    });
 }
 
 const char *hfm_io_last_error(hfm_io *io) { return io ? io->last_error.c_str() : "null hfm_io"; }

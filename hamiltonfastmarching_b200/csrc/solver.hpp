@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <string>
+#include <memory>
 #include <vector>
 
 namespace hfm {
@@ -65,7 +66,8 @@ struct EulerProblem {
     // Reverse first variation: groups of (linear index, weight) points (inspectSensitivity).
     std::vector<std::vector<int64_t>> adjoint_index;
     std::vector<std::vector<double>> adjoint_weight;
-    bool want_stencils = false;        // export per-cell offsets/weights (RiemannPerCell)
+    bool want_stencils = false;
+    bool retain = false;               // keep the device state for later reverse sweeps (single instance)        // export per-cell offsets/weights (RiemannPerCell)
     int tile_shift[3] = {-1, -1, -1};  // log2 tile extents per axis (sum 6); -1: 8x8 / 4x4x4
     int sweeps_per_tile = 4;           // local Jacobi sweeps before a tile re-queues itself
     int max_rounds = 1 << 20;
@@ -82,6 +84,17 @@ struct AdjointResult {
     std::vector<double> seed_weight;
 };
 
+struct EulerResult;
+
+// Device state of a solve kept for later reverse sweeps (EulerProblem::retain): the stencils and
+// arrival times stay in device memory, so a sensitivity for new inspection weights costs one
+// reverse sweep instead of a new solve.
+struct RetainedSolve {
+    virtual ~RetainedSolve() = default;
+    // Reverse first variation of the retained solve for the groups of p.adjoint_index.
+    virtual void adjoint(const EulerProblem &p, EulerResult &res) = 0;
+};
+
 struct EulerResult {
     std::vector<double> values;        // RowMajor, +inf where unreached
     std::vector<uint64_t> active;      // activeNeighs bitsets (if requested)
@@ -92,6 +105,7 @@ struct EulerResult {
     std::vector<AdjointResult> adjoints;
     double t_stencil_ms = 0, t_solve_ms = 0, t_adjoint_ms = 0, t_total_ms = 0;
     long long rounds = 0, tile_activations = 0, local_solves = 0;
+    std::shared_ptr<RetainedSolve> retained;  // set when EulerProblem::retain (single instance)
 };
 
 void solve_eulerian(const EulerProblem &p, EulerResult &r);

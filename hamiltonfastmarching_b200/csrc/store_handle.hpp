@@ -2,6 +2,7 @@
 // its last failure.
 #pragma once
 
+#include <memory>
 #include <string>
 
 #include "io.hpp"
@@ -9,5 +10,6 @@
 struct hfm_io {
     hfm::Store store;
     std::string last_error;
+    std::shared_ptr<void> retained;  // device state of the last solve run with retainState = 1
     explicit hfm_io(hfm::Ordering o) : store(o) {}
 };

@@ -84,6 +84,13 @@ int hfm_io_computed_keys(hfm_io *io, char *buf, size_t cap, size_t *len);
  * single-model FileHFM_<Model> executables do (DispatchAndRun.h:227-233). */
 int hfm_run(hfm_io *io, const char *expected_model);
 
+/* Reverse first variation for the inspectSensitivity keys now in `io`, from the device state of
+ * the last hfm_run on `io` that had the key retainState = 1 (an extension: the reference
+ * differentiates inside Run). Writes costSensitivity_i and seedSensitivity_i as hfm_run does,
+ * without solving again; HFM_ERR_ARG if no solve was retained. The retained device memory is
+ * released with the store or by the next hfm_run. */
+int hfm_run_sensitivity(hfm_io *io);
+
 /* Runs `n` stores as one batch: each is read as by hfm_run, then the instances of one stencil family
  * and precision (and the same tileSweeps/maxRounds) are solved together — one global tile space
  * over all of them, one persistent solver launch — and each store receives its own outputs.

@@ -102,3 +102,31 @@ def test_tti3_velocity_gradient_matches_finite_differences():
                   loss_of(torch.from_numpy(vpm.reshape(vp0.shape)))).item() / (2 * d)
         scale = max(abs(fd), 1e-3 * np.abs(g).max())
         assert abs(g[cell] - fd) <= 5e-3 * scale, (cell, g[cell], fd)
+
+
+def test_retained_solve_sensitivity_equals_one_shot():
+    """hfm_run with retainState then hfm_run_sensitivity gives what one hfm_run with the inspection
+    keys gives (same solve, deterministic reverse sweep), and matches the reference fixture."""
+    import hamiltonfastmarching_b200 as H
+    from conftest import load_golden
+    params, ref, _ = load_golden("riemann2_64")
+    keys = ("inspectSensitivity", "inspectSensitivityWeights", "inspectSensitivityLengths")
+    base = {k: v for k, v in params.items() if k not in keys and k != "exportActiveNeighs"}
+    io = H.HFMIO("RowMajor")
+    io.set_dict(dict(base, retainState=1.0, verbosity=0.0))
+    io.run()
+    for k in keys:
+        io.set_array(k, params[k])
+    io.run_sensitivity()
+    s1 = io.get_array("costSensitivity_0")
+    one = H.run(dict(base, **{k: params[k] for k in keys}))["costSensitivity_0"]
+    assert np.array_equal(s1, one)
+    rs = ref["costSensitivity_0"]
+    assert np.max(np.abs(s1 - rs)) <= 1e-10 * np.max(np.abs(rs))
+    io2 = H.HFMIO("RowMajor")
+    io2.set_dict(dict(base, verbosity=0.0))
+    io2.run()
+    for k in keys:
+        io2.set_array(k, params[k])
+    with pytest.raises(H.PyExp):
+        io2.run_sensitivity()
