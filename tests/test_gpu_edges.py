@@ -16,7 +16,9 @@ RTOL = 1e-10
 def _rel(a, b):
     fin = np.isfinite(b)
     assert np.array_equal(np.isfinite(a), fin)
-    return float(np.max(np.abs(a[fin] - b[fin])) / np.max(np.abs(b[fin])))
+    if not fin.any():
+        return 0.0
+    return float(np.max(np.abs(a[fin] - b[fin])) / max(np.max(np.abs(b[fin])), 1e-300))
 
 
 def test_seed_outside_domain_is_ignored_and_colliding_seeds_keep_the_first():
