@@ -1349,3 +1349,359 @@ int fmo_tti_neighbor_counts(int64_t n, const double *metric, const double *h, in
     }
     return 0;
 }
+
+/* ========================================================================================== */
+/* Geodesic backtracking and the geodesic flow.
+ * Discrete solver: Headers/Base/Implementation/GeodesicDiscreteSolver.hxx:41-211 (Run with its
+ * restarts, GeodesicDiscrete); flow: HamiltonFastMarching.hxx:187-272 (Recompute, order 1) with
+ * EulerianStencil.hxx:157-229 (HopfLaxRecompute) and :363-378 (GeodesicFlow). Points are in the
+ * reference's dimensionless coordinates (cell i spans [i, i+1)); the caller applies ReDim. */
+
+#define GEO_MAXF 64
+
+typedef int (*geo_flow_fn)(void *ctx, int64_t x, int (*off)[3], double *fw, double *value, double *width);
+
+/* Order-1 Recompute at cell x for Eulerian stencils: the active differences in stencil order (the
+ * forward ones, then the +e and -e sides of each symmetric one), the quadratic update over them and
+ * the flow weights w_i max(0, value - u_i); width = sum of flow weights / sum of w_i. */
+typedef struct { const fmo_problem *p; const double *values; const uint64_t *active; } eul_ctx;
+
+static int eul_recompute(void *vctx, int64_t x, int (*off)[3], double *fw, double *value, double *width) {
+    const eul_ctx *E = (const eul_ctx *)vctx;
+    const fmo_problem *p = E->p;
+    const int nd = p->nfwd + p->nsym;
+    const uint64_t act = E->active[x];
+    *width = 0.0;
+    *value = E->values[x];
+    if (act == 0) return 0;
+    int64_t idx[3], nidx[3];
+    index_of(p, x, idx);
+    const int64_t sid = stencil_id(p, idx, x);
+    const int8_t *O = p->off + sid * nd * 3;
+    const double *W = p->w + sid * nd;
+    double nv[GEO_MAXF], wts[GEO_MAXF];
+    int n = 0, bit = 0;
+    for (int k = 0; k < nd; ++k) {
+        for (int sg = 1; sg >= -1; sg -= 2) {
+            if (sg == -1 && k < p->nfwd) break;
+            const int b = k < p->nfwd ? bit : bit + (sg == 1 ? 0 : 1);
+            if (!(act & (1ULL << b)) || n >= GEO_MAXF) continue;
+            for (int a = 0; a < 3; ++a) off[n][a] = a < p->ndim ? sg * O[3 * k + a] : 0;
+            for (int a = 0; a < p->ndim; ++a) nidx[a] = idx[a] + off[n][a];
+            periodize(p, nidx);
+            nv[n] = E->values[linear_of(p, nidx)];
+            wts[n] = diff_weight(p, W[k], x);
+            ++n;
+        }
+        bit += k < p->nfwd ? 1 : 2;
+    }
+    quad_t q = {FMO_INF, 0.0, 0.0, -1.0, 1};  /* QuadraticMax<ScalarType, 1>: a = b = 0, c = -1 */
+    for (int i = 0; i < n; ++i) q.minVal = nv[i] < q.minVal ? nv[i] : q.minVal;
+    for (int i = 0; i < n; ++i) quad_add(&q, nv[i], wts[i]);
+    const double val = quad_solve(&q);
+    double wsum = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double d = val - nv[i];
+        fw[i] = wts[i] * (0.0 < d ? d : 0.0);
+        *width += fw[i];
+    }
+    for (int i = 0; i < n; ++i) wsum += wts[i];
+    if (wsum > 0) *width /= wsum;
+    *value = val;
+    return n;
+}
+
+/* TTI3 (Lag2) Recompute at the stored extremum t: offsets of the used Selling-path cells. */
+typedef struct { const int64_t *dims; const double *h; const double *metric; const double *values;
+                 const double *t_active; } tti_ctx;
+
+static int tti_flow(void *vctx, int64_t x, int (*off)[3], double *fw, double *value, double *width) {
+    const tti_ctx *T = (const tti_ctx *)vctx;
+    *width = 0.0;
+    *value = T->values[x];
+    if (!(T->t_active[x] < FMO_INF)) return 0;
+    tti_norm nm;
+    if (tti_setup(T->metric + 14 * x, T->h, &nm)) return 0;
+    int64_t nb[6];
+    double nbw[6];
+    int nn = 0;
+    *value = tti_recompute(&nm, T->dims, T->values, x, fabs(T->t_active[x]), nb, nbw, &nn);
+    const int64_t n1 = T->dims[1], n2 = T->dims[2];
+    const int64_t x0 = x / (n1 * n2), x1 = (x / n2) % n1, x2 = x % n2;
+    for (int j = 0; j < nn; ++j) {
+        const int64_t y = nb[j];
+        off[j][0] = (int)(y / (n1 * n2) - x0);
+        off[j][1] = (int)((y / n2) % n1 - x1);
+        off[j][2] = (int)(y % n2 - x2);
+        fw[j] = nbw[j];
+    }
+    return nn;
+}
+
+typedef struct { double val; int64_t ind[3]; double w; } geo_entry;
+
+typedef struct {
+    const fmo_problem *p;   /* grid (dims, periodic axes) */
+    const double *values;
+    geo_flow_fn flow;
+    void *ctx;
+    double step, threshold;
+    double *pts;            /* [cap][ndim] */
+    int64_t n, cap;
+    int overflow;
+} geo_run;
+
+static void geo_push(geo_run *G, const double *pt) {
+    const int D = G->p->ndim;
+    if (G->n >= G->cap) { G->overflow = 1; return; }
+    for (int a = 0; a < D; ++a) G->pts[G->n * D + a] = pt[a];
+    ++G->n;
+}
+
+/* weightSum, indexSum and covSum of the entries (UpdateSums, GeodesicDiscreteSolver.hxx:71-76) */
+typedef struct { double ws, is[3], cs[3][3]; } geo_sums;
+
+static void geo_add(geo_sums *S, int D, double w, const int64_t *ind) {
+    S->ws += w;
+    for (int i = 0; i < D; ++i) S->is[i] += w * (double)ind[i];
+    for (int i = 0; i < D; ++i)
+        for (int j = 0; j <= i; ++j) S->cs[i][j] += w * ((double)ind[i] * (double)ind[j]);
+}
+
+static int geo_greater(const geo_entry *a, const geo_entry *b, int D) {
+    if (a->val != b->val) return a->val > b->val;
+    for (int i = 0; i < D; ++i)
+        if (a->ind[i] != b->ind[i]) return a->ind[i] > b->ind[i];
+    return 0;
+}
+
+/* One pass of GeodesicDiscrete from the last point; returns 1 if a restart is needed, -1 on
+ * allocation failure. */
+static int geo_discrete_pass(geo_run *G, double vbound) {
+    const fmo_problem *p = G->p;
+    const int D = p->ndim;
+    geo_entry *set = NULL;
+    int64_t ns = 0, scap = 0;
+    double *sv = NULL, (*sd)[3] = NULL;
+    int64_t nst = 0, stcap = 0;
+    geo_sums S;
+    memset(&S, 0, sizeof(S));
+    double avg[3] = {0, 0, 0}, base[3] = {0, 0, 0}, stepNorm = 0.0;
+    int ret = 0;
+    double tip[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) tip[a] = G->pts[(G->n - 1) * D + a];
+    int64_t ref[3];
+    double pref[3];
+    for (int a = 0; a < D; ++a) { ref[a] = (int64_t)floor(tip[a]); pref[a] = (double)ref[a] + 0.5; }
+    /* unit mass split among the 2^D grid neighbours of the tip */
+    for (int i = 0; i < (1 << D); ++i) {
+        double weight = 1.0;
+        int64_t ind[3] = {0, 0, 0}, per[3];
+        for (int j = 0; j < D; ++j) {
+            const double diff = tip[j] - pref[j];
+            ind[j] = ref[j];
+            if (i & (1 << j)) { ind[j] += diff > 0 ? 1 : -1; weight *= fabs(diff); }
+            else weight *= 1. - fabs(diff);
+        }
+        for (int j = 0; j < D; ++j) per[j] = ind[j];
+        if (!periodize(p, per)) continue;
+        if (ns == scap) { scap = scap ? 2 * scap : 64; set = (geo_entry *)realloc(set, scap * sizeof(geo_entry)); if (!set) return -1; }
+        set[ns].val = G->values[linear_of(p, per)];
+        for (int j = 0; j < 3; ++j) set[ns].ind[j] = ind[j];
+        set[ns].w = weight;
+        ++ns;
+        geo_add(&S, D, weight, ind);
+    }
+    if (S.ws == 0) goto done;
+    for (int a = 0; a < D; ++a) { avg[a] = S.is[a] / S.ws; base[a] = avg[a]; }
+    while (ns > 0 && S.ws > 1e-5) {
+        int64_t best = 0;
+        for (int64_t k = 1; k < ns; ++k)
+            if (geo_greater(&set[k], &set[best], D)) best = k;
+        const geo_entry e = set[best];
+        set[best] = set[--ns];
+        if (e.w == 0) continue;
+        geo_add(&S, D, -e.w, e.ind);
+        int64_t per[3] = {e.ind[0], e.ind[1], e.ind[2]};
+        periodize(p, per);
+        int off[GEO_MAXF][3];
+        double fw[GEO_MAXF], rval, rwidth;
+        const int nf = G->flow(G->ctx, linear_of(p, per), off, fw, &rval, &rwidth);
+        double wSum = 0;
+        for (int f = 0; f < nf; ++f) wSum += fw[f];
+        if (wSum == 0) continue;
+        for (int f = 0; f < nf; ++f) {
+            const double w = e.w * fw[f] / wSum;
+            int64_t ind[3] = {0, 0, 0}, q[3];
+            for (int a = 0; a < D; ++a) { ind[a] = e.ind[a] + off[f][a]; q[a] = ind[a]; }
+            periodize(p, q);
+            const double val = G->values[linear_of(p, q)];
+            int64_t k = -1;
+            for (int64_t m = 0; m < ns; ++m) {
+                int same = set[m].val == val;
+                for (int a = 0; a < D && same; ++a) same = set[m].ind[a] == ind[a];
+                if (same) { k = m; break; }
+            }
+            if (k < 0) {
+                if (w < S.ws * G->threshold) continue;
+                if (ns == scap) { scap = scap ? 2 * scap : 64; set = (geo_entry *)realloc(set, scap * sizeof(geo_entry)); if (!set) return -1; }
+                set[ns].val = val;
+                for (int a = 0; a < 3; ++a) set[ns].ind[a] = ind[a];
+                set[ns].w = w;
+                ++ns;
+            } else {
+                set[k].w += w;
+            }
+            geo_add(&S, D, w, ind);
+        }
+        if (S.ws <= 0) {
+            double pt[3];
+            for (int a = 0; a < D; ++a) pt[a] = avg[a] + 0.5;
+            geo_push(G, pt);
+            goto done;
+        }
+        double step[3] = {0, 0, 0}, sq = 0.0;
+        for (int a = 0; a < D; ++a) {
+            const double old = avg[a];
+            avg[a] = S.is[a] / S.ws;
+            step[a] = avg[a] - old;
+        }
+        for (int a = 0; a < D; ++a) sq += step[a] * step[a];
+        if (nst == stcap) {
+            stcap = stcap ? 2 * stcap : 64;
+            sv = (double *)realloc(sv, stcap * sizeof(double));
+            sd = (double (*)[3])realloc(sd, stcap * sizeof(*sd));
+            if (!sv || !sd) { ret = -1; goto done; }
+        }
+        sv[nst] = e.val;
+        for (int a = 0; a < 3; ++a) sd[nst][a] = step[a];
+        ++nst;
+        stepNorm += sqrt(sq);
+        if (ns == 1) {  /* mass concentrated at one point (seed or wall corner) */
+            if (nf == 0) break;
+            double pt[3];
+            for (int a = 0; a < D; ++a) { pt[a] = avg[a] + 0.5; base[a] = avg[a]; }
+            geo_push(G, pt);
+            stepNorm = 0; nst = 0;
+            continue;
+        }
+        if (stepNorm < G->step && ns > 1) continue;
+        const double valInc = sv[0] - e.val;
+        if (valInc <= 0) continue;
+        const double delta = valInc / D;
+        double pt[3];
+        for (int a = 0; a < D; ++a) pt[a] = base[a];
+        for (int64_t k = 0; k < nst; ++k)
+            for (int a = 0; a < D; ++a) pt[a] += sd[k][a] * (sv[k] - e.val + delta) / (valInc + delta);
+        for (int a = 0; a < D; ++a) { pt[a] += 0.5; base[a] = avg[a]; }
+        geo_push(G, pt);
+        stepNorm = 0; nst = 0;
+        /* spread of the mass: det(covariance + Id) against the squared volume bound */
+        double V[3][3];
+        for (int i = 0; i < D; ++i)
+            for (int j = 0; j <= i; ++j) {
+                V[i][j] = S.cs[i][j] / S.ws - (S.is[i] / S.ws) * (S.is[j] / S.ws) + (i == j ? 1.0 : 0.0);
+                V[j][i] = V[i][j];
+            }
+        double det;
+        if (D == 2) det = V[0][0] * V[1][1] - V[1][0] * V[0][1];
+        else det = V[0][0] * (V[1][1] * V[2][2] - V[1][2] * V[2][1]) - V[0][1] * (V[1][0] * V[2][2] - V[1][2] * V[2][0]) +
+                   V[0][2] * (V[1][0] * V[2][1] - V[1][1] * V[2][0]);
+        if (det > vbound * vbound) {
+            for (int a = 0; a < D; ++a) pt[a] = avg[a] + 0.5;
+            geo_push(G, pt);
+            ret = 1;
+            goto done;
+        }
+    }
+done:
+    free(set); free(sv); free(sd);
+    return ret;
+}
+
+/* Run (GeodesicDiscreteSolver.hxx:41-55): restarts from the last point while the mass spreads too
+ * much; after 5 restarts the volume bound grows by 1.3 per restart; 50 restarts mean failure. */
+static int64_t geo_discrete_all(const fmo_problem *grid, const double *values, geo_flow_fn flow, void *ctx,
+                                int ntips, const double *tips, double step, double threshold, double volume_bound,
+                                int64_t max_points, double *points, int64_t *lengths, int *failed) {
+    const int D = grid->ndim;
+    int64_t total = 0;
+    for (int t = 0; t < ntips; ++t) {
+        geo_run G = {grid, values, flow, ctx, step, threshold, points + total * D, 0, max_points - total, 0};
+        geo_push(&G, tips + (int64_t)t * D);
+        int restarts = 0;
+        double vb = volume_bound;
+        while (restarts < 50 && !G.overflow) {
+            const int r = geo_discrete_pass(&G, vb);
+            if (r < 0) return -1;
+            if (!r) break;
+            ++restarts;
+            if (restarts >= 5) vb *= 1.3;
+        }
+        if (G.overflow) return -2;
+        lengths[t] = G.n;
+        failed[t] = restarts == 50;
+        total += G.n;
+    }
+    return total;
+}
+
+int64_t fmo_geodesic_discrete(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
+                              const double *tips, double step, double threshold, double volume_bound,
+                              int64_t max_points, double *points, int64_t *lengths, int *failed) {
+    eul_ctx E = {p, values, active};
+    return geo_discrete_all(p, values, eul_recompute, &E, ntips, tips, step, threshold, volume_bound, max_points,
+                            points, lengths, failed);
+}
+
+int64_t fmo_tti_geodesic_discrete(const int64_t *dims, const double *h, const double *metric, const double *values,
+                                  const double *t_active, int ntips, const double *tips, double step,
+                                  double threshold, double volume_bound, int64_t max_points, double *points,
+                                  int64_t *lengths, int *failed) {
+    fmo_problem g;
+    memset(&g, 0, sizeof(g));
+    g.ndim = 3;
+    for (int a = 0; a < 3; ++a) g.dims[a] = dims[a];
+    tti_ctx T = {dims, h, metric, values, t_active};
+    return geo_discrete_all(&g, values, tti_flow, &T, ntips, tips, step, threshold, volume_bound, max_points, points,
+                            lengths, failed);
+}
+
+/* GeodesicFlow at every cell: flow[x] = sum of weight * offset over the Recompute flow (dimensionless;
+ * the export is -ReDim of it), value and width of the Recompute. */
+static void geo_flow_all(const fmo_problem *grid, geo_flow_fn flow, void *ctx, double *out, double *value,
+                         double *width) {
+    const int D = grid->ndim;
+    const int64_t N = ncells(grid);
+    int off[GEO_MAXF][3];
+    double fw[GEO_MAXF];
+    for (int64_t x = 0; x < N; ++x) {
+        double v, wd;
+        const int nf = flow(ctx, x, off, fw, &v, &wd);
+        for (int a = 0; a < D; ++a) {
+            double s = 0.0;
+            for (int f = 0; f < nf; ++f) s += fw[f] * (double)off[f][a];
+            out[x * D + a] = s;
+        }
+        if (value) value[x] = v;
+        if (width) width[x] = wd;
+    }
+}
+
+int fmo_geodesic_flow(const fmo_problem *p, const double *values, const uint64_t *active, double *flow,
+                      double *value, double *width) {
+    eul_ctx E = {p, values, active};
+    geo_flow_all(p, eul_recompute, &E, flow, value, width);
+    return 0;
+}
+
+int fmo_tti_geodesic_flow(const int64_t *dims, const double *h, const double *metric, const double *values,
+                          const double *t_active, double *flow, double *value, double *width) {
+    fmo_problem g;
+    memset(&g, 0, sizeof(g));
+    g.ndim = 3;
+    for (int a = 0; a < 3; ++a) g.dims[a] = dims[a];
+    tti_ctx T = {dims, h, metric, values, t_active};
+    geo_flow_all(&g, tti_flow, &T, flow, value, width);
+    return 0;
+}

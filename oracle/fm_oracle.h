@@ -85,6 +85,25 @@ int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const d
 /* Properties of one TTI norm: out = {tmin, tmax, optimDirection, Multiplier(tmin), Multiplier(tmax)}. */
 int fmo_tti_norm(const double *metric, const double *h, double *out);
 
+/* Discrete geodesic backtracking from ntips tips (dimensionless coordinates: cell i spans [i, i+1)),
+ * from the values and activeNeighs of fmo_fast_marching. points[max_points][ndim] receive the
+ * concatenated geodesics (dimensionless), lengths[ntips] their lengths, failed[ntips] 1 where the
+ * restart limit was reached. Returns the total number of points, -1 on allocation failure, -2 if
+ * max_points is too small. */
+int64_t fmo_geodesic_discrete(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
+                              const double *tips, double step, double threshold, double volume_bound,
+                              int64_t max_points, double *points, int64_t *lengths, int *failed);
+int64_t fmo_tti_geodesic_discrete(const int64_t *dims, const double *h, const double *metric, const double *values,
+                                  const double *t_active, int ntips, const double *tips, double step,
+                                  double threshold, double volume_bound, int64_t max_points, double *points,
+                                  int64_t *lengths, int *failed);
+/* Geodesic flow per cell (sum of Recompute weight * offset, dimensionless) with the Recompute value
+ * and width (value, width may be NULL). */
+int fmo_geodesic_flow(const fmo_problem *p, const double *values, const uint64_t *active, double *flow,
+                      double *value, double *width);
+int fmo_tti_geodesic_flow(const int64_t *dims, const double *h, const double *metric, const double *values,
+                          const double *t_active, double *flow, double *value, double *width);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,14 @@ def lib():
         L.fmo_tti_backward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int64,
                                                  _P, _P]
         L.fmo_tti_backward_variation.restype = ctypes.c_int64
+        L.fmo_geodesic_discrete.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_int64, _P, _P, _P]
+        L.fmo_geodesic_discrete.restype = ctypes.c_int64
+        L.fmo_tti_geodesic_discrete.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double, ctypes.c_int64, _P, _P, _P]
+        L.fmo_tti_geodesic_discrete.restype = ctypes.c_int64
+        L.fmo_geodesic_flow.argtypes = [ctypes.POINTER(_Problem), _P, _P, _P, _P, _P]
+        L.fmo_tti_geodesic_flow.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -196,6 +204,7 @@ class Problem:
                     metric = np.broadcast_to(metric, dims + (ns,))
             off, w = riemann_stencils(np.ascontiguousarray(metric), hs, dual)
             nfwd, nsym, share = 0, off.shape[1], 0
+            scale = hs
             adim = lambda p: (np.asarray(p, float) - origin) / hs
         elif model in ("ReedsShepp2", "Elastica2"):
             periodic = [0, 0, 1]
@@ -242,6 +251,7 @@ class Problem:
         self.walls = walls
         self.seed_index, self.seed_value = _seed_indices(params, adim, dims, periodic)
         self._adim = adim
+        self.origin, self.scale = np.asarray(origin, float), np.asarray(scale, float)
         s = _Problem()
         s.ndim = ndim
         for a in range(3):
@@ -373,3 +383,97 @@ def tti_backward_variation(res: Dict, points, weights=None):
     if ns < 0:
         raise RuntimeError("oracle TTI backward variation failed")
     return sens.reshape(dims), si[:ns], sw[:ns]
+
+
+def _geo_params(params: Dict, ndim: int):
+    """geodesicStep, geodesicWeightThreshold, geodesicVolumeBound with the reference's defaults
+    (``GeodesicDiscreteSolver.h:17-19``)."""
+    return (float(_get(params, "geodesicStep", 0.25)), float(_get(params, "geodesicWeightThreshold", 0.001)),
+            float(_get(params, "geodesicVolumeBound", 5.0 * 1.3 ** ndim)))
+
+
+def _unoriented_tips(values, adim, dims, tips_u):
+    """tips_Unoriented -> oriented dimensionless tips: among the angles at the cell centres, the one
+    of smallest value, the last one on ties (``HFMInterface.hxx:499-521`` with ``:56-90``)."""
+    out = []
+    for q in np.atleast_2d(np.asarray(tips_u, float)):
+        base = adim(np.array([q[0], q[1], 0.0]))
+        best, vmin = None, math.inf
+        for t in range(dims[2]):
+            p = np.array([base[0], base[1], t + 0.5])
+            i, j = int(math.floor(p[0])), int(math.floor(p[1]))
+            if best is None:
+                best = p
+            if not (0 <= i < dims[0] and 0 <= j < dims[1]):
+                continue
+            v = values[i, j, t]
+            if vmin < v:
+                continue
+            best, vmin = p, v
+        out.append(best)
+    return np.array(out)
+
+
+def _run_discrete(fn, args, tips, step, thr, vb, ndim):
+    tips = np.ascontiguousarray(np.atleast_2d(tips), np.float64)
+    cap = 1 << 16
+    while True:
+        pts = np.empty((cap, ndim))
+        lens = np.zeros(len(tips), np.int64)
+        failed = np.zeros(len(tips), np.int32)
+        n = fn(*args, len(tips), _ptr(tips), step, thr, vb, cap, _ptr(pts), _ptr(lens), _ptr(failed))
+        if n == -2:
+            cap *= 4
+            continue
+        if n < 0:
+            raise RuntimeError("oracle geodesic extraction failed")
+        return pts[:n].copy(), lens, failed
+
+
+def geodesics(res: Dict, params: Dict) -> Dict:
+    """Discrete geodesics of a :func:`solve` or :func:`tti_solve` result for the ``tips`` and
+    ``tips_Unoriented`` keys of ``params``: geodesicPoints[_Unoriented] (physical coordinates,
+    concatenated), geodesicLengths[_Unoriented] and the failure flags."""
+    out = {}
+    if "_tti" in res:
+        d, hs, metric, origin = res["_tti"]
+        ndim, scale, adim = 3, hs, (lambda p: (np.asarray(p, float) - origin) / hs)
+        values = np.ascontiguousarray(res["values"].ravel())
+        tact = np.ascontiguousarray(res["activeNeighs"].ravel())
+        fn, args = lib().fmo_tti_geodesic_discrete, (_ptr(d), _ptr(hs), _ptr(metric), _ptr(values), _ptr(tact))
+        dims = tuple(int(x) for x in d)
+    else:
+        P: Problem = res["problem"]
+        ndim, scale, origin, adim, dims = P.ndim, P.scale, P.origin, P._adim, P.dims
+        values = np.ascontiguousarray(res["values"].ravel())
+        fn, args = lib().fmo_geodesic_discrete, (ctypes.byref(P.struct), _ptr(values), _ptr(res["activeNeighs"]))
+    step, thr, vb = _geo_params(params, ndim)
+    groups = []
+    if "tips" in params:
+        groups.append(("", np.array([adim(p) for p in np.atleast_2d(np.asarray(params["tips"], float))])))
+    if "tips_Unoriented" in params and ndim == 3 and "_tti" not in res:
+        groups.append(("_Unoriented", _unoriented_tips(res["values"], adim, dims, params["tips_Unoriented"])))
+    for suffix, tips in groups:
+        pts, lens, failed = _run_discrete(fn, args, tips, step, thr, vb, ndim)
+        out["geodesicPoints" + suffix] = pts * scale + origin
+        out["geodesicLengths" + suffix] = lens.astype(float)
+        out["geodesicFailed" + suffix] = failed
+    return out
+
+
+def geodesic_flow(res: Dict) -> np.ndarray:
+    """exportGeodesicFlow of a solve result: -ReDim of the Recompute flow at every cell, dims + (ndim,)."""
+    if "_tti" in res:
+        d, hs, metric, origin = res["_tti"]
+        dims, scale = tuple(int(x) for x in d), hs
+        values = np.ascontiguousarray(res["values"].ravel())
+        tact = np.ascontiguousarray(res["activeNeighs"].ravel())
+        flow = np.empty((values.size, 3))
+        lib().fmo_tti_geodesic_flow(_ptr(d), _ptr(hs), _ptr(metric), _ptr(values), _ptr(tact), _ptr(flow), None, None)
+    else:
+        P: Problem = res["problem"]
+        dims, scale = P.dims, P.scale
+        values = np.ascontiguousarray(res["values"].ravel())
+        flow = np.empty((values.size, P.ndim))
+        lib().fmo_geodesic_flow(ctypes.byref(P.struct), _ptr(values), _ptr(res["activeNeighs"]), _ptr(flow), None, None)
+    return (-(flow * scale)).reshape(dims + (len(dims),))

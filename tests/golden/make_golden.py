@@ -104,7 +104,8 @@ def save(name, params, out, **extra):
     for k, v in params.items():
         blob["in_" + k] = np.asarray(v) if not isinstance(v, str) else np.array(v)
     for k in ("values", "activeNeighs", "nAccepted", "MaxStencilWidth", "costSensitivity_0",
-              "seedSensitivity_0", "spreadedSeeds", "spreadedSeedValues"):
+              "seedSensitivity_0", "spreadedSeeds", "spreadedSeedValues", "geodesicPoints", "geodesicLengths",
+              "geodesicPoints_Unoriented", "geodesicLengths_Unoriented", "geodesicFlow"):
         if k in out:
             blob["out_" + k] = np.asarray(out[k])
     blob.update(extra)
@@ -156,10 +157,39 @@ def tti_fixtures():
     solve_fixture("tti3_16", p, (pts, rng.uniform(0.5, 2.0, 6)))
 
 
+def geodesic_fixtures():
+    """Discrete geodesics (tips, tips_Unoriented) and the geodesic flow of every model family."""
+    rng = np.random.default_rng(2024)
+    p = W.riemann2_case(48, aniso=10.0, seed=21)
+    p["walls"] = np.zeros((48, 48))
+    p["walls"][20, 6:40] = 1.0
+    p["tips"] = rng.uniform(0.05, 0.95, (6, 2))
+    p["exportGeodesicFlow"] = 1.0
+    solve_fixture("geo_riemann2_48_walls", p)
+    p = W.riemann3_case(16, n_spheres=3, n_seeds=2, rmin=0.1, rmax=0.2, seed=22)
+    p["tips"] = rng.uniform(0.05, 0.95, (4, 3))
+    p["exportGeodesicFlow"] = 1.0
+    solve_fixture("geo_riemann3_16_walls", p)
+    for model, name in (("ReedsShepp2", "geo_reedsshepp2_24x16"), ("Elastica2", "geo_elastica2_24x16")):
+        p = W.curvature2_case(24, 16, model, seed=23, n_curves=4)
+        p["tips"] = np.c_[rng.uniform(0.1, 0.9, (3, 2)), rng.uniform(0, 6.2, (3, 1))]
+        p["tips_Unoriented"] = rng.uniform(0.1, 0.9, (3, 2))
+        p["exportGeodesicFlow"] = 1.0
+        solve_fixture(name, p)
+    p = W.tti3_case(12, h=0.01, seed=24)
+    p.pop("_vp")
+    p["tips"] = np.c_[rng.uniform(0.0, 0.12, (3, 2)), rng.uniform(0.03, 0.12, (3, 1))]
+    p["exportGeodesicFlow"] = 1.0
+    solve_fixture("geo_tti3_12", p)
+
+
 if __name__ == "__main__":
-    # `make_golden.py tti` regenerates only the TTI3 fixture
+    # `make_golden.py tti` / `make_golden.py geodesic` regenerate only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
+    elif sys.argv[1:] == ["geodesic"]:
+        geodesic_fixtures()
     else:
         main()
         tti_fixtures()
+        geodesic_fixtures()

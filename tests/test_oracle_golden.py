@@ -69,3 +69,28 @@ def test_tti_oracle_matches_reference():
     seeds = ref["seedSensitivity_0"]
     assert len(seeds) == len(si)
     np.testing.assert_allclose(seeds[:, -1], sw, rtol=1e-12)
+
+
+GOLDEN_GEODESICS = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
+                    "geo_tti3_12"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_GEODESICS)
+def test_geodesic_oracle_matches_reference(name):
+    """Discrete geodesics (tips, tips_Unoriented) and the geodesic flow of the oracle against the
+    reference executable: same lengths, points within 1e-12 (relative to the domain size), flow
+    within 1e-12 of its largest entry."""
+    params, ref, _ = load_golden(name)
+    res = O.tti_solve(params) if params["model"] == "TTI3" else O.solve(params)
+    geo = O.geodesics(res, params)
+    for suffix in ("", "_Unoriented"):
+        if "geodesicPoints" + suffix not in ref:
+            continue
+        np.testing.assert_array_equal(geo["geodesicLengths" + suffix], ref["geodesicLengths" + suffix])
+        scale = np.max(np.abs(ref["geodesicPoints" + suffix]))
+        assert np.max(np.abs(geo["geodesicPoints" + suffix] - ref["geodesicPoints" + suffix])) <= 1e-12 * scale
+        assert not geo["geodesicFailed" + suffix].any()
+    flow, rflow = O.geodesic_flow(res), ref["geodesicFlow"]
+    fin = np.isfinite(rflow)
+    assert np.array_equal(fin, np.isfinite(flow))
+    assert np.max(np.abs(flow[fin] - rflow[fin])) <= 1e-12 * np.max(np.abs(rflow[fin]))
