@@ -1404,6 +1404,8 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
     }
 }
 
+#include "geodesic.cuh"
+
 struct AdjDev {
     long long N;
     const int *fidx;
@@ -2168,6 +2170,8 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     HFM_CUDA(cudaStreamSynchronize(s));
     HFM_TRACE("outputs");
+    run_geodesics<Real, NFWD, NSYM, KIND>(P, hinst, probs, results, s);
+    HFM_TRACE("geodesics");
     if (ninst == 1 && !p0.adjoint_index.empty()) {
         tm.start(s);
         run_adjoint<Real, NFWD, NSYM, KIND>(P, N, p0, results[0], status, s);

@@ -1,0 +1,690 @@
+// Geodesic backtracking and the geodesic flow on the device.
+//
+// Included by eulerian.cu inside namespace hfm::detail, after the solver kernels (it uses Dev,
+// Inst, solve_cell, cell_flags and the TTI path helpers).
+//
+// The reference extracts geodesics one tip at a time on the host with a std::map keyed by
+// (value, index) (Headers/Base/Implementation/GeodesicDiscreteSolver.hxx:59-211). Tips are
+// independent, so here one warp follows one tip: the pending (value, index, weight) entries of
+// its tip live in the warp's shared memory, the largest one is found with a warp reduction, the
+// Recompute of the extracted cell is done on the device from the arrival times still resident in
+// HBM, and children are matched against the entries with a warp ballot. Running sums and the step
+// bookkeeping are warp-uniform; the arithmetic keeps the reference's order and rounds every
+// product and sum on its own (no contraction), so a geodesic follows the reference's to rounding.
+// Warps loop over the tips of all instances of a batch (persistent grid).
+
+constexpr int kGeoMaxFlow = 32;      // flow entries of one Recompute (two per difference, capped)
+constexpr int kGeoWarps = 4;         // warps per CTA of the geodesic kernel
+constexpr int kGeoCap = 256, kGeoStepCap = 64;          // shared-memory set / step list
+constexpr int kGeoCapBig = 8192, kGeoStepCapBig = 512;  // global-memory rerun of overflowed tips
+constexpr long long kGeoIndexBias = 1ll << 20;          // unwrapped indices packed as 3 x 21 bits
+
+// Per-tip status bits.
+enum : int {
+    kGeoFailed = 1,         // the restart limit was reached (the reference's "extraction failed")
+    kGeoPointOverflow = 2,  // more points than the tip's output capacity (rerun with more room)
+    kGeoSetOverflow = 4,    // more pending entries than the warp's set holds (rerun in global memory)
+    kGeoIterCap = 8,        // iteration limit of one pass reached
+    kGeoRange = 16,         // an unwrapped index left the packable range
+};
+
+struct GeoTip {
+    double p[3];        // dimensionless tip (cell i spans [i, i+1)); unoriented: (x, y) only
+    double step, thr, vbound;  // geodesicStep, geodesicWeightThreshold, geodesicVolumeBound
+    long long out0;     // first point slot of this tip in the output
+    int inst;           // instance of the batch
+    int cap;            // output capacity in points
+    int ndim;           // model dimension (2 or 3)
+    int unoriented;     // choose the angle of smallest value (tips_Unoriented)
+};
+
+struct GeoOut {
+    int len;            // points written
+    int status;         // kGeo* bits
+    int restarts;       // restarts of the discrete solver
+    int pad;
+};
+
+template <int CAP, int SCAP>
+struct GeoSet {
+    double val[CAP];
+    double w[CAP];
+    long long key[CAP];
+    double sv[SCAP];        // step list: value of the extracted entry and the step of the mean
+    double sd[SCAP][3];
+    unsigned foff[kGeoMaxFlow];
+    double fw[kGeoMaxFlow];
+};
+
+__device__ __forceinline__ long long geo_pack(const int *ind) {
+    return ((ind[0] + kGeoIndexBias) << 42) | ((ind[1] + kGeoIndexBias) << 21) | (ind[2] + kGeoIndexBias);
+}
+__device__ __forceinline__ void geo_unpack(long long k, int *ind) {
+    const long long m = (1ll << 21) - 1;
+    ind[0] = (int)(((k >> 42) & m) - kGeoIndexBias);
+    ind[1] = (int)(((k >> 21) & m) - kGeoIndexBias);
+    ind[2] = (int)((k & m) - kGeoIndexBias);
+}
+__device__ __forceinline__ bool geo_packable(const int *ind) {
+    return ind[0] > -kGeoIndexBias && ind[0] < kGeoIndexBias && ind[1] > -kGeoIndexBias &&
+           ind[1] < kGeoIndexBias && ind[2] > -kGeoIndexBias && ind[2] < kGeoIndexBias;
+}
+
+// Order-1 Recompute at cell (x0, x1, x2) of instance I (HamiltonFastMarching.hxx:187-272): the
+// flow entries (packed offset, weight) in the reference's order, the recomputed value and the
+// width. Stencils: the active differences (forward ones, then the +e / -e side of each symmetric
+// one, as the activeNeighs bits), the quadratic update over them, weights w_i max(0, value - u_i)
+// (EulerianStencil.hxx:157-229). TTI3: the Selling path at the extremum t, weights
+// (sol - v) w(t) (TTI.hpp:278-389). Seeds, walls and unreached cells have no flow.
+template <typename Real, int NFWD, int NSYM, int KIND>
+__device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1, int x2, unsigned *foff, double *fw,
+                              double *value, double *width) {
+    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    constexpr int ND = NFWD + NSYM;
+    using A = Arith<double>;
+    const GridGeom &g = I.g;
+    const long long c = (I.tile0 + g.tile_of(x0, x1, x2)) * 64 + g.local_of(x0, x1, x2);
+    const Real *values = P.values + I.cell0;
+    const double u = (double)values[g.lin(x0, x1, x2)];
+    *value = u;
+    *width = 0.0;
+    bool fixed, dead;
+    cell_flags<Real, KIND>(P, c, fixed, dead);
+    if (fixed || dead || !(u < A::inf())) return 0;
+    if constexpr (KIND == kKindTTI) {
+        double ta = 0.0;
+        bool inner = false;
+        solve_cell_tti<Real>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &ta, &inner);
+        if (!(ta < A::inf())) return 0;
+        const TTICell &tc = P.tti[c];
+        TTIPath path;
+        if (!tti_path_at(tc, ta, path)) return 0;
+        struct Cand {
+            double v, wa, wb;
+            unsigned off;
+        } cand[6];
+        for (int r = 0; r < 6; ++r) {
+            double vs[2] = {A::inf(), A::inf()};
+            for (int si = 0; si < 2; ++si) {
+                const int s = si ? -1 : 1;
+                const int y0 = x0 + s * path.off[r][0], y1 = x1 + s * path.off[r][1], y2 = x2 + s * path.off[r][2];
+                if ((unsigned)y0 >= (unsigned)g.dims[0] || (unsigned)y1 >= (unsigned)g.dims[1] ||
+                    (unsigned)y2 >= (unsigned)g.dims[2])
+                    continue;
+                vs[si] = (double)values[g.lin(y0, y1, y2)];
+            }
+            const bool plus = vs[0] < vs[1];  // the +e neighbour only when strictly smaller
+            const int s = plus ? 1 : -1;
+            Cand cd{plus ? vs[0] : vs[1], path.w0[r], path.w1[r],
+                    pack_off(s * path.off[r][0], s * path.off[r][1], s * path.off[r][2])};
+            int k = r - 1;
+            while (k >= 0 && cand[k].v > cd.v) {
+                cand[k + 1] = cand[k];
+                --k;
+            }
+            cand[k + 1] = cd;
+        }
+        const double vmin = cand[0].v;
+        if (!(vmin < A::inf())) return 0;
+        double a = 0, b = 0, cc = -tti_multiplier(tc, dconst(ta)).v, sol = A::inf();
+        int r = 0;
+        for (; r < 6; ++r) {
+            const double v = A::sub(cand[r].v, vmin);
+            if (v >= sol) break;
+            const double w = A::add(A::mul(A::sub(1.0, ta), cand[r].wa), A::mul(ta, cand[r].wb));
+            const double wv = A::mul(w, v);
+            a = A::add(a, w);
+            b = A::add(b, wv);
+            cc = A::add(cc, A::mul(wv, v));
+            if (a <= 100 * fabs(cc) * 2.220446049250313e-16) continue;
+            sol = A::div(A::add(b, A::sqrt(A::sub(A::mul(b, b), A::mul(a, cc)))), a);
+        }
+        for (int q = 0; q < r; ++q) {
+            const double v = A::sub(cand[q].v, vmin);
+            const double w0 = A::add(A::mul(A::sub(1.0, ta), cand[q].wa), A::mul(ta, cand[q].wb));
+            const double d = A::mul(A::sub(sol, v), w0);
+            foff[q] = cand[q].off;
+            fw[q] = d > 0 ? d : 0.0;
+        }
+        *value = A::add(sol, vmin);
+        return r;
+    } else {
+        unsigned used = 0, side = 0;
+        solve_cell<Real, NFWD, NSYM, KIND>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
+        double m = 1.0;
+        if (SHARE) m = (double)P.mult[c];
+        double nv[kGeoMaxFlow], wts[kGeoMaxFlow];
+        int n = 0;
+        for (int k = 0; k < ND; ++k) {
+            int o0, o1, o2;
+            double wb;
+            if (SHARE) {
+                const int8_t *o = P.cls_off + ((I.cls0 + x2) * ND + k) * 3;
+                o0 = o[0]; o1 = o[1]; o2 = o[2];
+                wb = A::mul((double)P.cls_w[(I.cls0 + x2) * ND + k], A::mul(m, m));
+            } else {
+                const unsigned cd = P.code[k * P.ntc + c];
+                o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
+                wb = (double)P.weight[k * P.ntc + c];
+            }
+            // active sides of this difference, as the activeNeighs bits (active_kernel)
+            unsigned act = 0;  // bit0: +e, bit1: -e
+            if (k < NFWD) {
+                if ((used >> k) & 1u) act = 1;
+                else if (SHARE) {
+                    for (int k2 = 0; k2 < NFWD; ++k2) {
+                        if (!((used >> k2) & 1u)) continue;
+                        const int8_t *o2p = P.cls_off + ((I.cls0 + x2) * ND + k2) * 3;
+                        if (o2p[0] == o0 && o2p[1] == o1 && o2p[2] == o2) { act = 1; break; }
+                    }
+                }
+            } else if ((used >> k) & 1u) {
+                act = ((side >> (k - NFWD)) & 1u) ? 2u : 1u;
+            }
+            for (int si = 0; si < 2; ++si) {
+                if (!((act >> si) & 1u) || n >= kGeoMaxFlow) continue;
+                const int s = si ? -1 : 1;
+                int y0 = x0 + s * o0, y1 = x1 + s * o1, y2 = x2 + s * o2;
+                g.wrap(y0, y1, y2);
+                nv[n] = (double)values[g.lin(y0, y1, y2)];
+                wts[n] = wb;
+                foff[n] = pack_off(s * o0, s * o1, s * o2);
+                ++n;
+            }
+        }
+        if (n == 0) return 0;
+        // QuadraticMax over the active neighbours in this order (minVal = their smallest value)
+        double mn = A::inf();
+        for (int i = 0; i < n; ++i) mn = nv[i] < mn ? nv[i] : mn;
+        double a = 0, b = 0, cc = -1;
+        for (int i = 0; i < n; ++i) {
+            const double v = A::sub(nv[i], mn);
+            const double wv = A::mul(wts[i], v);
+            a = A::add(a, wts[i]);
+            b = A::add(b, wv);
+            cc = A::add(cc, A::mul(wv, v));
+        }
+        double val = A::inf();
+        if (a != 0.0) {
+            const double d2 = A::sub(A::mul(b, b), A::mul(a, cc));
+            val = A::add(mn, A::div(A::add(b, A::sqrt(0.0 < d2 ? d2 : 0.0)), a));
+        }
+        double wid = 0.0, wsum = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double d = A::sub(val, nv[i]);
+            fw[i] = A::mul(wts[i], 0.0 < d ? d : 0.0);
+            wid = A::add(wid, fw[i]);
+        }
+        for (int i = 0; i < n; ++i) wsum = A::add(wsum, wts[i]);
+        if (wsum > 0) wid = A::div(wid, wsum);
+        *value = val;
+        *width = wid;
+        return n;
+    }
+}
+
+// Geodesic flow of every cell of a batch: sum of weight * offset over the Recompute flow
+// (HamiltonFastMarching.hxx:363-378), dimensionless, [cell][ndim] at cell0 * ndim of each instance
+// (the export is -ReDim of it, HFMInterface.hxx:541-553).
+template <typename Real, int NFWD, int NSYM, int KIND>
+__global__ void geodesic_flow_kernel(Dev<Real> P, int ndim, double *out) {
+    using A = Arith<double>;
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells) return;
+    const int ii = inst_of_cell(P.inst, P.ninst, x);
+    const Inst &I = P.inst[ii];
+    const GridGeom &g = I.g;
+    const long long l = x - I.cell0;
+    const int x2 = (int)(l % g.dims[2]);
+    const long long r = l / g.dims[2];
+    const int x1 = (int)(r % g.dims[1]);
+    const int x0 = (int)(r / g.dims[1]);
+    unsigned foff[kGeoMaxFlow];
+    double fw[kGeoMaxFlow], v, wd;
+    const int nf = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, x0, x1, x2, foff, fw, &v, &wd);
+    for (int a = 0; a < ndim; ++a) {
+        double s = 0.0;
+        for (int f = 0; f < nf; ++f) s = A::add(s, A::mul(fw[f], (double)off_c(foff[f], a)));
+        out[x * ndim + a] = s;
+    }
+}
+
+// Unit mass split among the 2^D grid neighbours of the tip, the extraction loop and the emission of
+// points (GeodesicDiscreteSolver.hxx:59-211). Warp-uniform except where lane 0 writes. Returns 1
+// if the mass spread beyond the volume bound (restart from the last point), 0 otherwise.
+template <typename Real, int NFWD, int NSYM, int KIND, int CAP, int SCAP>
+__device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, int D, GeoSet<CAP, SCAP> &S, double *out,
+                             int cap, int &len, int &status, double step, double thr, double vbound,
+                             long long iter_cap) {
+    using A = Arith<double>;
+    const int lane = threadIdx.x & 31;
+    const GridGeom &g = I.g;
+    const Real *values = P.values + I.cell0;
+    int n = 0;
+    double ws = 0.0, is[3] = {0, 0, 0}, cs[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    auto sums = [&](double w, const int *ind) {
+        ws = A::add(ws, w);
+        for (int i = 0; i < D; ++i) is[i] = A::add(is[i], A::mul(w, (double)ind[i]));
+        for (int i = 0; i < D; ++i)
+            for (int j = 0; j <= i; ++j) cs[i][j] = A::add(cs[i][j], A::mul(w, A::mul((double)ind[i], (double)ind[j])));
+    };
+    auto emit = [&](const double *pt) -> bool {
+        if (len >= cap) {
+            status |= kGeoPointOverflow;
+            return false;
+        }
+        if (lane == 0)
+            for (int a = 0; a < D; ++a) out[(long long)len * D + a] = pt[a];
+        ++len;
+        return true;
+    };
+    double tip[3] = {0, 0, 0};
+    __syncwarp();
+    for (int a = 0; a < D; ++a) tip[a] = out[(long long)(len - 1) * D + a];
+    int ref[3] = {0, 0, 0};
+    double pref[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) {
+        ref[a] = (int)floor(tip[a]);
+        pref[a] = A::add((double)ref[a], 0.5);
+    }
+    for (int i = 0; i < (1 << D); ++i) {
+        double weight = 1.0;
+        int ind[3] = {0, 0, 0};
+        for (int j = 0; j < D; ++j) {
+            const double diff = A::sub(tip[j], pref[j]);
+            ind[j] = ref[j];
+            if (i & (1 << j)) {
+                ind[j] += diff > 0 ? 1 : -1;
+                weight = A::mul(weight, fabs(diff));
+            } else {
+                weight = A::mul(weight, A::sub(1.0, fabs(diff)));
+            }
+        }
+        int q0 = ind[0], q1 = ind[1], q2 = ind[2];
+        if (!g.wrap(q0, q1, q2)) continue;
+        if (!geo_packable(ind)) { status |= kGeoRange; return 0; }
+        if (lane == 0) {
+            S.val[n] = (double)values[g.lin(q0, q1, q2)];
+            S.key[n] = geo_pack(ind);
+            S.w[n] = weight;
+        }
+        ++n;
+        sums(weight, ind);
+    }
+    __syncwarp();
+    if (ws == 0) return 0;
+    double avg[3] = {0, 0, 0}, base[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) { avg[a] = A::div(is[a], ws); base[a] = avg[a]; }
+    double stepNorm = 0.0;
+    int nst = 0;
+    double f0[3] = {0, 0, 0}, f1[3] = {0, 0, 0};  // steps beyond the list: sum of s and of s * value
+    long long iters = 0;
+    while (n > 0 && ws > 1e-5) {
+        if (++iters > iter_cap) { status |= kGeoIterCap; return 0; }
+        // entry of largest (value, index): lanes scan their slots, then a butterfly reduction
+        double bv = -A::inf();
+        long long bk = 0;
+        int bs = -1;
+        for (int j = lane; j < n; j += 32) {
+            const double v = S.val[j];
+            const long long k = S.key[j];
+            if (bs < 0 || v > bv || (v == bv && k > bk)) { bv = v; bk = k; bs = j; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const long long ok = __shfl_xor_sync(0xffffffffu, bk, o);
+            const int os = __shfl_xor_sync(0xffffffffu, bs, o);
+            if (os >= 0 && (bs < 0 || ov > bv || (ov == bv && ok > bk))) { bv = ov; bk = ok; bs = os; }
+        }
+        const double ew = S.w[bs];
+        __syncwarp();
+        if (lane == 0) {
+            S.val[bs] = S.val[n - 1];
+            S.key[bs] = S.key[n - 1];
+            S.w[bs] = S.w[n - 1];
+        }
+        --n;
+        __syncwarp();
+        if (ew == 0) continue;
+        int ind[3];
+        geo_unpack(bk, ind);
+        sums(-ew, ind);
+        int q0 = ind[0], q1 = ind[1], q2 = ind[2];
+        g.wrap(q0, q1, q2);
+        int nf = 0;
+        if (lane == 0) {
+            double rv, rw;
+            nf = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, q0, q1, q2, S.foff, S.fw, &rv, &rw);
+        }
+        nf = __shfl_sync(0xffffffffu, nf, 0);
+        __syncwarp();
+        double wSum = 0.0;
+        for (int f = 0; f < nf; ++f) wSum = A::add(wSum, S.fw[f]);
+        if (wSum == 0) continue;
+        for (int f = 0; f < nf; ++f) {
+            const double w = A::div(A::mul(ew, S.fw[f]), wSum);
+            const unsigned oc = S.foff[f];
+            int c[3] = {ind[0] + off_c(oc, 0), ind[1] + off_c(oc, 1), ind[2] + off_c(oc, 2)};
+            if (!geo_packable(c)) { status |= kGeoRange; return 0; }
+            const long long key = geo_pack(c);
+            int found = -1;
+            for (int j = lane; j < n; j += 32)
+                if (S.key[j] == key) found = j;
+            const unsigned ball = __ballot_sync(0xffffffffu, found >= 0);
+            if (ball) {
+                if (lane == __ffs(ball) - 1) S.w[found] = A::add(S.w[found], w);
+            } else {
+                if (w < A::mul(ws, thr)) continue;
+                if (n >= CAP) { status |= kGeoSetOverflow; return 0; }
+                int p0 = c[0], p1 = c[1], p2 = c[2];
+                g.wrap(p0, p1, p2);
+                if (lane == 0) {
+                    S.val[n] = (double)values[g.lin(p0, p1, p2)];
+                    S.key[n] = key;
+                    S.w[n] = w;
+                }
+                ++n;
+            }
+            __syncwarp();
+            sums(w, c);
+        }
+        if (ws <= 0) {
+            double pt[3];
+            for (int a = 0; a < D; ++a) pt[a] = A::add(avg[a], 0.5);
+            emit(pt);
+            return 0;
+        }
+        double stp[3] = {0, 0, 0}, sq = 0.0;
+        for (int a = 0; a < D; ++a) {
+            const double old = avg[a];
+            avg[a] = A::div(is[a], ws);
+            stp[a] = A::sub(avg[a], old);
+        }
+        for (int a = 0; a < D; ++a) sq = A::add(sq, A::mul(stp[a], stp[a]));
+        if (nst < SCAP) {
+            if (lane == 0) {
+                S.sv[nst] = bv;
+                for (int a = 0; a < 3; ++a) S.sd[nst][a] = stp[a];
+            }
+        } else {
+            for (int a = 0; a < D; ++a) { f0[a] = A::add(f0[a], stp[a]); f1[a] = A::add(f1[a], A::mul(stp[a], bv)); }
+        }
+        ++nst;
+        __syncwarp();
+        stepNorm = A::add(stepNorm, A::sqrt(sq));
+        if (n == 1) {  // mass concentrated at one point (a seed, or around a wall corner)
+            if (nf == 0) break;
+            double pt[3];
+            for (int a = 0; a < D; ++a) { pt[a] = A::add(avg[a], 0.5); base[a] = avg[a]; }
+            if (!emit(pt)) return 0;
+            stepNorm = 0;
+            nst = 0;
+            for (int a = 0; a < 3; ++a) { f0[a] = 0; f1[a] = 0; }
+            continue;
+        }
+        if (stepNorm < step && n > 1) continue;
+        const double valInc = A::sub(S.sv[0], bv);
+        if (valInc <= 0) continue;
+        const double delta = A::div(valInc, (double)D);
+        const double den = A::add(valInc, delta);
+        double pt[3];
+        for (int a = 0; a < D; ++a) pt[a] = base[a];
+        const int nl = nst < SCAP ? nst : SCAP;
+        for (int k = 0; k < nl; ++k) {
+            const double cf = A::add(A::sub(S.sv[k], bv), delta);
+            for (int a = 0; a < D; ++a) pt[a] = A::add(pt[a], A::div(A::mul(S.sd[k][a], cf), den));
+        }
+        if (nst > SCAP)  // steps past the list, summed: sum s (v - value + delta) / den
+            for (int a = 0; a < D; ++a)
+                pt[a] = A::add(pt[a], A::div(A::add(f1[a], A::mul(A::sub(delta, bv), f0[a])), den));
+        for (int a = 0; a < D; ++a) { pt[a] = A::add(pt[a], 0.5); base[a] = avg[a]; }
+        if (!emit(pt)) return 0;
+        stepNorm = 0;
+        nst = 0;
+        for (int a = 0; a < 3; ++a) { f0[a] = 0; f1[a] = 0; }
+        // spread of the mass: det(covariance + Id) against the squared volume bound
+        double V[3][3];
+        for (int i = 0; i < D; ++i)
+            for (int j = 0; j <= i; ++j) {
+                V[i][j] = A::add(A::sub(A::div(cs[i][j], ws), A::mul(A::div(is[i], ws), A::div(is[j], ws))),
+                                 i == j ? 1.0 : 0.0);
+                V[j][i] = V[i][j];
+            }
+        double det;
+        if (D == 2) {
+            det = A::sub(A::mul(V[0][0], V[1][1]), A::mul(V[1][0], V[0][1]));
+        } else {
+            const double m0 = A::sub(A::mul(V[1][1], V[2][2]), A::mul(V[1][2], V[2][1]));
+            const double m1 = A::sub(A::mul(V[1][0], V[2][2]), A::mul(V[1][2], V[2][0]));
+            const double m2 = A::sub(A::mul(V[1][0], V[2][1]), A::mul(V[1][1], V[2][0]));
+            det = A::add(A::sub(A::mul(V[0][0], m0), A::mul(V[0][1], m1)), A::mul(V[0][2], m2));
+        }
+        if (det > A::mul(vbound, vbound)) {
+            for (int a = 0; a < D; ++a) pt[a] = A::add(avg[a], 0.5);
+            emit(pt);
+            return 1;
+        }
+    }
+    return 0;
+}
+
+// One warp per tip, warps looping over the tips (GeodesicDiscreteSolver.hxx:41-55 for the restarts:
+// after 5 restarts the volume bound grows by 1.3 per restart, 50 restarts mean failure). With
+// GLOBAL the warps' sets live in `gsets` (one per warp of the grid) instead of shared memory.
+template <typename Real, int NFWD, int NSYM, int KIND, int CAP, int SCAP, bool GLOBAL>
+__global__ void __launch_bounds__(kGeoWarps * 32)
+geodesic_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut *outs, GeoSet<CAP, SCAP> *gsets) {
+    using A = Arith<double>;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * kGeoWarps + wib, nw = (long long)gridDim.x * kGeoWarps;
+    GeoSet<CAP, SCAP> *S;
+    if constexpr (GLOBAL) {
+        S = gsets + gw;
+    } else {
+        __shared__ GeoSet<CAP, SCAP> sets[kGeoWarps];
+        S = sets + wib;
+    }
+    for (long long t = gw; t < ntips; t += nw) {
+        const GeoTip tp = tips[t];
+        const Inst &I = P.inst[tp.inst];
+        const GridGeom &g = I.g;
+        const int D = tp.ndim;
+        double *out = pts + tp.out0 * D;
+        double tip[3] = {tp.p[0], tp.p[1], tp.p[2]};
+        if (tp.unoriented) {
+            // the angle (cell centre) of smallest value at the point (x, y); the last one on ties
+            // (HFMInterface.hxx:499-521); the first angle if (x, y) is outside the grid
+            const Real *values = P.values + I.cell0;
+            const double fx = floor(tip[0]), fy = floor(tip[1]);
+            const bool inside = fx >= 0 && fy >= 0 && fx < g.dims[0] && fy < g.dims[1];
+            double bv = A::inf();
+            int bt = -1;
+            if (inside)
+                for (int th = lane; th < g.dims[2]; th += 32) {
+                    const double v = (double)values[g.lin((int)fx, (int)fy, th)];
+                    if (v <= bv) { bv = v; bt = th; }
+                }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int ot = __shfl_xor_sync(0xffffffffu, bt, o);
+                if (ot >= 0 && (bt < 0 || ov < bv || (ov == bv && ot > bt))) { bv = ov; bt = ot; }
+            }
+            tip[2] = A::add((double)(bt < 0 ? 0 : bt), 0.5);
+        }
+        int len = 0, status = 0, restarts = 0;
+        if (tp.cap < 1) {
+            status |= kGeoPointOverflow;
+        } else {
+            if (lane == 0)
+                for (int a = 0; a < D; ++a) out[a] = tip[a];
+            len = 1;
+            double vb = tp.vbound;
+            const long long iter_cap = 64 * g.ncells + 4096;
+            while (restarts < 50) {
+                const int r = geodesic_pass<Real, NFWD, NSYM, KIND, CAP, SCAP>(P, I, D, *S, out, tp.cap, len, status,
+                                                                              tp.step, tp.thr, vb, iter_cap);
+                if (!r || status) break;
+                ++restarts;
+                if (restarts >= 5) vb = A::mul(vb, 1.3);
+            }
+            if (restarts == 50) status |= kGeoFailed;
+        }
+        if (lane == 0) outs[t] = GeoOut{len, status, restarts, 0};
+        __syncwarp();
+    }
+}
+
+// Gathers the points of each tip (len points of ndim values at out0) into a compact array.
+__global__ void geodesic_compact_kernel(const double *pts, const GeoTip *tips, const GeoOut *outs,
+                                        const long long *dst0, int ntips, double *dst) {
+    for (int t = blockIdx.x; t < ntips; t += gridDim.x) {
+        const long long n = (long long)outs[t].len * tips[t].ndim;
+        const double *src = pts + tips[t].out0 * tips[t].ndim;
+        double *d = dst + dst0[t];
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+    }
+}
+
+// Geodesics of the tips of every instance of a batch, on the arrival times resident in P.values,
+// and the geodesic flow fields that were requested. A tip whose points or pending entries
+// overflowed is run again with 8x the room (its set in global memory); three attempts at most.
+template <typename Real, int NFWD, int NSYM, int KIND>
+void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std::vector<const EulerProblem *> &probs,
+                   std::vector<EulerResult> &results, cudaStream_t s) {
+    const int ninst = (int)probs.size();
+    bool any_flow = false;
+    std::vector<GeoTip> tips;
+    std::vector<int> group;  // 0: tips, 1: tips_Unoriented
+    long long slots = 0;
+    int ndim = 2;
+    for (int i = 0; i < ninst; ++i) {
+        const EulerProblem &p = *probs[i];
+        ndim = p.ndim;
+        any_flow |= p.want_geodesic_flow;
+        long long extent = 0;
+        for (int a = 0; a < p.ndim; ++a) extent += p.dims[a];
+        const int cap = (int)std::min<long long>(1 << 24, std::max<long long>(256, (long long)(2.0 * extent / p.geo_step)));
+        for (int gi = 0; gi < 2; ++gi) {
+            const std::vector<double> &src = gi ? p.geo_tips_unoriented : p.geo_tips;
+            const int w = gi ? 2 : p.ndim;
+            for (size_t k = 0; k + w <= src.size(); k += w) {
+                GeoTip t{};
+                for (int a = 0; a < w; ++a) t.p[a] = src[k + a];
+                t.step = p.geo_step;
+                t.thr = p.geo_threshold;
+                t.vbound = p.geo_volume_bound;
+                t.out0 = slots;
+                t.inst = i;
+                t.cap = cap;
+                t.ndim = p.ndim;
+                t.unoriented = gi;
+                slots += cap;
+                tips.push_back(t);
+                group.push_back(gi);
+            }
+        }
+    }
+    const int ntips = (int)tips.size();
+    if (ntips == 0 && !any_flow) return;
+    EventTimer tm;
+    tm.start(s);
+    int dev = 0, nsm = 0;
+    HFM_CUDA(cudaGetDevice(&dev));
+    HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (any_flow) {
+        DeviceBuffer<double> flow(P.ncells * ndim);
+        launch(geodesic_flow_kernel<Real, NFWD, NSYM, KIND>, nblocks(P.ncells, 128), 128, 0, s, P, ndim, flow.get());
+        HFM_CUDA(cudaGetLastError());
+        for (int i = 0; i < ninst; ++i) {
+            if (!probs[i]->want_geodesic_flow) continue;
+            const long long n = hinst[i].g.ncells * ndim;
+            results[i].geodesic_flow.resize(n);
+            HFM_CUDA(cudaMemcpyAsync(results[i].geodesic_flow.data(), flow.get() + hinst[i].cell0 * ndim,
+                                     n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        HFM_CUDA(cudaStreamSynchronize(s));
+    }
+    if (ntips > 0) {
+        std::vector<GeoOut> houts(ntips);
+        std::vector<int> todo(ntips);
+        for (int t = 0; t < ntips; ++t) todo[t] = t;
+        std::vector<std::vector<double>> tip_pts(ntips);
+        for (int attempt = 0; attempt < 3 && !todo.empty(); ++attempt) {
+            bool big = false;
+            if (attempt > 0) {
+                long long sl = 0;
+                for (int t : todo) {
+                    big |= (houts[t].status & kGeoSetOverflow) != 0;
+                    if (houts[t].status & kGeoPointOverflow) tips[t].cap = (int)std::min<long long>(1 << 27, 8ll * tips[t].cap);
+                    tips[t].out0 = sl;
+                    sl += tips[t].cap;
+                }
+                slots = sl;
+            }
+            std::vector<GeoTip> sub(todo.size());
+            for (size_t k = 0; k < todo.size(); ++k) sub[k] = tips[todo[k]];
+            const int nsub = (int)sub.size();
+            DeviceBuffer<GeoTip> dtips(nsub);
+            dtips.upload(sub.data(), nsub, s);
+            DeviceBuffer<GeoOut> douts(nsub);
+            DeviceBuffer<double> pts(slots * ndim);
+            const int want_blocks = (nsub + kGeoWarps - 1) / kGeoWarps;
+            if (!big) {
+                auto kern = geodesic_kernel<Real, NFWD, NSYM, KIND, kGeoCap, kGeoStepCap, false>;
+                int per_sm = 0;
+                HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGeoWarps * 32, 0));
+                const int grid = std::max(1, std::min(want_blocks, nsm * std::max(1, per_sm)));
+                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), nsub, pts.get(), douts.get(),
+                       (GeoSet<kGeoCap, kGeoStepCap> *)nullptr);
+            } else {
+                auto kern = geodesic_kernel<Real, NFWD, NSYM, KIND, kGeoCapBig, kGeoStepCapBig, true>;
+                const int grid = std::max(1, std::min(want_blocks, 2 * nsm));
+                DeviceBuffer<GeoSet<kGeoCapBig, kGeoStepCapBig>> gsets((size_t)grid * kGeoWarps);
+                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), nsub, pts.get(), douts.get(), gsets.get());
+                HFM_CUDA(cudaStreamSynchronize(s));
+            }
+            HFM_CUDA(cudaGetLastError());
+            std::vector<GeoOut> o(nsub);
+            douts.download(o.data(), nsub, s);
+            HFM_CUDA(cudaStreamSynchronize(s));
+            // compact the finished tips of this attempt and bring their points back
+            std::vector<long long> d0(nsub, 0);
+            long long tot = 0;
+            for (int k = 0; k < nsub; ++k) {
+                d0[k] = tot;
+                tot += (long long)o[k].len * ndim;
+            }
+            DeviceBuffer<long long> dd0(nsub);
+            dd0.upload(d0.data(), nsub, s);
+            DeviceBuffer<double> cpt(std::max<long long>(tot, 1));
+            launch(geodesic_compact_kernel, std::min(nsub, 4 * nsm), 128, 0, s, pts.get(), dtips.get(), douts.get(),
+                   dd0.get(), nsub, cpt.get());
+            HFM_CUDA(cudaGetLastError());
+            std::vector<double> hp(tot);
+            if (tot) cpt.download(hp.data(), tot, s);
+            HFM_CUDA(cudaStreamSynchronize(s));
+            std::vector<int> again;
+            for (int k = 0; k < nsub; ++k) {
+                const int t = todo[k];
+                houts[t] = o[k];
+                const bool rerun = (o[k].status & (kGeoPointOverflow | kGeoSetOverflow)) != 0;
+                if (rerun && attempt < 2) {
+                    again.push_back(t);
+                    continue;
+                }
+                tip_pts[t].assign(hp.begin() + d0[k], hp.begin() + d0[k] + (long long)o[k].len * ndim);
+            }
+            todo.swap(again);
+        }
+        for (int t = 0; t < ntips; ++t) {  // in the order of the tips
+            EulerResult &r = results[tips[t].inst];
+            const int gi = group[t];
+            r.geo_points[gi].insert(r.geo_points[gi].end(), tip_pts[t].begin(), tip_pts[t].end());
+            r.geo_lengths[gi].push_back(houts[t].len);
+            r.geo_status[gi].push_back(houts[t].status);
+            r.geo_restarts[gi].push_back(houts[t].restarts);
+        }
+    }
+    const float ms = tm.stop(s);
+    for (int i = 0; i < ninst; ++i) results[i].t_geodesic_ms = ms;
+}

@@ -80,7 +80,7 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
 }
 
 void reject_unsupported(Store &io) {
-    static const char *keys[] = {"tips", "tips_Unoriented", "factoringValues", "speed_times", "cost_times",
+    static const char *keys[] = {"factoringValues", "speed_times", "cost_times",
                                  "metric_times", "dualMetric_times", "stopAtDistance", "nMaxAccepted",
                                  "stopWhenAnyAccepted", "stopWhenAllAccepted", "stopWhenAnyAccepted_Unoriented",
                                  "stopWhenAllAccepted_Unoriented", "costVariation", "seedValueVariation",
@@ -93,8 +93,8 @@ void reject_unsupported(Store &io) {
         throw Error(HFM_ERR_UNSUPPORTED, "option 'factoringRadius' (static factoring) is not supported by the GPU solve path");
     if (io.has_field("order") && io.get_scalar("order") != 1)
         throw Error(HFM_ERR_UNSUPPORTED, "only order=1 is supported by the GPU solve path");
-    if (io.get_scalar("exportGeodesicFlow", 0.0, 2) != 0 || io.get_scalar("exportActiveOffsets", 0.0, 3) != 0)
-        throw Error(HFM_ERR_UNSUPPORTED, "geodesic flow exports are not supported by the GPU solve path");
+    if (io.get_scalar("exportActiveOffsets", 0.0, 3) != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, "exportActiveOffsets is not supported by the GPU solve path");
     if (io.get_scalar("refineStencilAtWallBoundary", 0.0, 3) != 0)
         throw Error(HFM_ERR_UNSUPPORTED, "refineStencilAtWallBoundary is not supported by the GPU solve path");
 }
@@ -448,10 +448,44 @@ void read_inspect(Store &io, const Param &pm, EulerProblem &p) {
     }
 }
 
+// Geodesic keys (HFMInterface.hxx:452-523, GeodesicDiscreteSolver.hxx:8-15): tips and, on the
+// lifted models, tips_Unoriented, made dimensionless; the discrete solver's parameters. Returns
+// which of the two tip keys are present.
+void read_geodesics(Store &io, const Param &pm, bool lifted, EulerProblem &p, bool has[2]) {
+    has[0] = io.has_field("tips");
+    has[1] = lifted && io.has_field("tips_Unoriented");
+    if (has[0] || has[1]) {
+        const std::string solver = io.get_string("geodesicSolver", "Discrete");
+        if (solver == "ODE")
+            throw Error(HFM_ERR_UNSUPPORTED, "geodesicSolver 'ODE' is not supported by the GPU solve path");
+        if (solver != "Discrete") throw Error(HFM_ERR_VALUE, "Error : Unrecognized geodesic solver " + solver + ".\n");
+        p.geo_step = io.get_scalar("geodesicStep", 0.25);
+        p.geo_threshold = io.get_scalar("geodesicWeightThreshold", 0.001);
+        p.geo_volume_bound = io.get_scalar("geodesicVolumeBound", 5. * std::pow(1.3, pm.ndim));
+    }
+    if (has[0]) {
+        int64_t n = 0;
+        const std::vector<double> t = io.get_vector("tips", pm.ndim, &n);
+        p.geo_tips.resize(n * pm.ndim);
+        for (int64_t i = 0; i < n; ++i)
+            for (int a = 0; a < pm.ndim; ++a)
+                p.geo_tips[i * pm.ndim + a] = (t[i * pm.ndim + a] - pm.origin[a]) / pm.scale[a];  // ADim
+    }
+    if (has[1]) {
+        int64_t n = 0;
+        const std::vector<double> t = io.get_vector("tips_Unoriented", 2, &n);
+        p.geo_tips_unoriented.resize(n * 2);
+        for (int64_t i = 0; i < n; ++i)
+            for (int a = 0; a < 2; ++a) p.geo_tips_unoriented[i * 2 + a] = (t[i * 2 + a] - pm.origin[a]) / pm.scale[a];
+    }
+    p.want_geodesic_flow = io.get_scalar("exportGeodesicFlow", 0.0, 2) != 0;
+}
+
 // A model read from its store, ready to solve (the part of Run before the solver loop).
 struct Prepared {
     Param pm;
     EulerProblem p;
+    bool geo_keys[2] = {false, false};  // tips, tips_Unoriented present
     bool export_values = false, export_active = false, skip = false;
     std::vector<int64_t> dims;
     double *values_dst = nullptr;
@@ -480,6 +514,7 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     read_walls(io, pm, lifted, p);
     read_seeds(io, pm, p, lifted);
 
+    read_geodesics(io, pm, lifted, p, q.geo_keys);
     q.export_values = io.get_scalar("exportValues", 0.0, 2) != 0;
     p.retain = io.get_scalar("retainState", 0.0, 3) != 0;
     q.export_active = io.get_scalar("exportActiveNeighs", 0.0, 3) != 0;
@@ -521,6 +556,49 @@ void export_sensitivities(Store &io, const Param &pm, const std::vector<int64_t>
     }
 }
 
+// geodesicPoints / geodesicLengths (suffix _Unoriented for tips_Unoriented) in physical
+// coordinates (ReDim), the reference's messages for failed tips (GeodesicDiscreteSolver.hxx:17-34),
+// and geodesicFlow = -ReDim(flow) (HFMInterface.hxx:452-485, 541-553).
+void export_geodesics(Store &io, const Prepared &q, const EulerResult &r) {
+    const Param &pm = q.pm;
+    const int D = pm.ndim;
+    for (int gi = 0; gi < 2; ++gi) {
+        if (!q.geo_keys[gi]) continue;
+        const std::string suffix = gi ? "_Unoriented" : "";
+        std::vector<double> pts(r.geo_points[gi]);
+        for (size_t k = 0; k < pts.size(); ++k) pts[k] = pts[k] * pm.scale[k % D] + pm.origin[k % D];
+        std::vector<double> lens(r.geo_lengths[gi].begin(), r.geo_lengths[gi].end());
+        size_t first = 0;
+        for (size_t t = 0; t < lens.size(); ++t) {
+            std::ostringstream tip;
+            tip << "{";
+            for (int a = 0; a < D; ++a) tip << (a ? "," : "") << pts[first * D + a];
+            tip << "}";
+            const int st = r.geo_status[gi][t];
+            if (st & 1) io.msg("Geodesic extraction failed for tip " + tip.str() + "\n");
+            else if (r.geo_restarts[gi][t] > 5) {
+                double vb = q.p.geo_volume_bound;
+                for (int k = 5; k <= r.geo_restarts[gi][t]; ++k) vb *= 1.3;
+                std::ostringstream m;
+                m << "Tip " << tip.str() << " yields " << r.geo_restarts[gi][t] << " restarts, "
+                  << "geodesicVolumeBound increased to " << vb;
+                io.msg(m.str());
+            }
+            if (st & ~1)
+                io.warn("Geodesic extraction for tip " + tip.str() + " stopped early (" +
+                        ((st & 6) ? std::string("out of room") : (st & 8) ? std::string("iteration limit") : std::string("index range")) + ")\n");
+            first += (size_t)lens[t];
+        }
+        io.set_vector("geodesicPoints" + suffix, (int64_t)(pts.size() / D), D, pts.data());
+        io.set_vector("geodesicLengths" + suffix, (int64_t)lens.size(), 1, lens.data());
+    }
+    if (q.p.want_geodesic_flow && !r.geodesic_flow.empty()) {
+        std::vector<double> f(r.geodesic_flow.size());
+        for (size_t k = 0; k < f.size(); ++k) f[k] = -(r.geodesic_flow[k] * pm.scale[k % D]);
+        io.set_field("geodesicFlow", q.dims, D, f.data());
+    }
+}
+
 void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
     const Param &pm = q.pm;
     const std::vector<int64_t> &dims = q.dims;
@@ -528,7 +606,7 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
     io.set_scalar("MaxStencilWidth", r.max_stencil_width);
     io.set_scalar("StencilCPUTime", r.t_stencil_ms * 1e-3);
     io.set_scalar("FMCPUTime", r.t_solve_ms * 1e-3);
-    io.set_scalar("GeodesicCPUTime", 0.0);
+    io.set_scalar("GeodesicCPUTime", r.t_geodesic_ms * 1e-3);
     io.set_scalar("GPUStencilTime", r.t_stencil_ms * 1e-3);
     io.set_scalar("GPUSolveTime", r.t_solve_ms * 1e-3);
     io.set_scalar("solverRounds", (double)r.rounds);
@@ -549,6 +627,7 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
         io.set_field("activeNeighs", dims, 1, a.data());
     }
     export_sensitivities(io, pm, dims, r.adjoints);
+    export_geodesics(io, q, r);
     io.set_scalar("nAccepted", (double)r.n_accepted);
 }
 

@@ -66,8 +66,14 @@ struct EulerProblem {
     // Reverse first variation: groups of (linear index, weight) points (inspectSensitivity).
     std::vector<std::vector<int64_t>> adjoint_index;
     std::vector<std::vector<double>> adjoint_weight;
-    bool want_stencils = false;
-    bool retain = false;               // keep the device state for later reverse sweeps (single instance)        // export per-cell offsets/weights (RiemannPerCell)
+    bool want_stencils = false;        // export per-cell offsets/weights (RiemannPerCell)
+    bool retain = false;               // keep the device state for later reverse sweeps (single instance)
+    // Geodesic backtracking (tips, tips_Unoriented) from the solved arrival times, in dimensionless
+    // coordinates (cell i spans [i, i+1) on every axis): geo_tips [n][ndim]; geo_tips_unoriented
+    // [n][2] (x, y) whose angle is chosen on the device; the discrete solver's parameters.
+    std::vector<double> geo_tips, geo_tips_unoriented;
+    double geo_step = 0.25, geo_threshold = 1e-3, geo_volume_bound = 8.45;
+    bool want_geodesic_flow = false;   // exportGeodesicFlow
     int tile_shift[3] = {-1, -1, -1};  // log2 tile extents per axis (sum 6); -1: 8x8 / 4x4x4
     int sweeps_per_tile = 4;           // local Jacobi sweeps before a tile re-queues itself
     int max_rounds = 1 << 20;
@@ -103,7 +109,14 @@ struct EulerResult {
     int64_t n_accepted = 0;
     int max_stencil_width = 0;
     std::vector<AdjointResult> adjoints;
-    double t_stencil_ms = 0, t_solve_ms = 0, t_adjoint_ms = 0, t_total_ms = 0;
+    // Geodesics of geo_tips ([0]) and geo_tips_unoriented ([1]): concatenated dimensionless points,
+    // the length, status bits (1: restart limit reached; 2, 4: overflow; 8: iteration limit;
+    // 16: index range) and restarts of each.
+    std::vector<double> geo_points[2];
+    std::vector<int64_t> geo_lengths[2];
+    std::vector<int> geo_status[2], geo_restarts[2];
+    std::vector<double> geodesic_flow;  // [N][ndim] sum of Recompute weight * offset (dimensionless)
+    double t_stencil_ms = 0, t_solve_ms = 0, t_adjoint_ms = 0, t_geodesic_ms = 0, t_total_ms = 0;
     long long rounds = 0, tile_activations = 0, local_solves = 0;
     std::shared_ptr<RetainedSolve> retained;  // set when EulerProblem::retain (single instance)
 };

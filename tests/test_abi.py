@@ -68,7 +68,7 @@ def test_store_errors_raise_not_crash():
         io.run()               # no model key: reported, not a segfault
 
 
-@pytest.mark.parametrize("key,val", [("tips", np.zeros((1, 2))), ("order", 2.0), ("factoringRadius", 5.0),
+@pytest.mark.parametrize("key,val", [("exportActiveOffsets", 1.0), ("order", 2.0), ("factoringRadius", 5.0),
                                      ("stopAtDistance", 1.0), ("seedRadius", 2.0)])
 def test_unsupported_options_rejected_before_gpu_work(key, val):
     p = {"model": "Riemann2", "arrayOrdering": "RowMajor", "dims": np.array([8., 8.]), "gridScale": 0.125,
@@ -76,6 +76,16 @@ def test_unsupported_options_rejected_before_gpu_work(key, val):
     with pytest.raises(H.PyExp) as e:
         H.run(p)
     assert e.value.code == 3, str(e.value)
+
+
+@pytest.mark.parametrize("solver,code", [("ODE", 3), ("Runge", 2)])
+def test_geodesic_solver_choice_checked_before_gpu_work(solver, code):
+    p = {"model": "Riemann2", "arrayOrdering": "RowMajor", "dims": np.array([8., 8.]), "gridScale": 0.125,
+         "metric": np.array([1., 0., 1.]), "seeds": np.array([[0.5, 0.5]]), "verbosity": 0.0,
+         "tips": np.array([[0.1, 0.1]]), "geodesicSolver": solver}
+    with pytest.raises(H.PyExp) as e:
+        H.run(p)
+    assert e.value.code == code, str(e.value)
 
 
 def test_model_mismatch_is_reported():

@@ -1,0 +1,154 @@
+"""Geodesic backtracking on the GPU (tips, tips_Unoriented, exportGeodesicFlow).
+
+Two checks per case:
+- against the oracle run on the GPU's own arrival times and activeNeighs: the discrete solver and
+  the Recompute are then fed the same inputs, so the geodesics agree to rounding (same lengths,
+  points within 1e-11 of the domain size, flow within 1e-11 of its largest entry);
+- against the reference's golden fixtures end to end: the arrival times differ from the
+  reference's by at most 1e-10 (relative), which moves the geodesics by about as much: same
+  lengths, points within 1e-7 of the domain size, flow within 1e-7 of its largest entry.
+"""
+import numpy as np
+import pytest
+
+import hamiltonfastmarching_b200 as hfm
+from conftest import load_golden
+from hamiltonfastmarching_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
+          "geo_tti3_12"]
+
+
+def _oracle_on(out, params):
+    """Oracle geodesics and flow computed from the GPU's values and activeNeighs."""
+    if params["model"] == "TTI3":
+        res = O.tti_solve(params)  # for the grid description; values / activeNeighs replaced below
+        res["values"] = np.ascontiguousarray(out["values"])
+        res["activeNeighs"] = np.ascontiguousarray(out["activeNeighs"])
+    else:
+        P = O.Problem(params)
+        res = {"values": np.ascontiguousarray(out["values"]),
+               "activeNeighs": np.ascontiguousarray(out["activeNeighs"].astype(np.uint64).ravel()), "problem": P}
+    return O.geodesics(res, params), O.geodesic_flow(res)
+
+
+def _check(out, ref, keys, tol_pts, tol_flow):
+    for suffix in keys:
+        np.testing.assert_array_equal(out["geodesicLengths" + suffix], ref["geodesicLengths" + suffix])
+        a, b = out["geodesicPoints" + suffix], ref["geodesicPoints" + suffix]
+        assert a.shape == b.shape
+        assert np.max(np.abs(a - b)) <= tol_pts * max(1.0, np.max(np.abs(b))), suffix
+    if "geodesicFlow" in ref:
+        f, g = out["geodesicFlow"], ref["geodesicFlow"]
+        fin = np.isfinite(g)
+        assert np.array_equal(np.isfinite(f), fin)
+        assert np.max(np.abs(f[fin] - g[fin])) <= tol_flow * np.max(np.abs(g[fin]))
+
+
+def _suffixes(params):
+    return [s for s, k in (("", "tips"), ("_Unoriented", "tips_Unoriented")) if k in params]
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_geodesics_match_oracle_on_gpu_values(name):
+    params, _, _ = load_golden(name)
+    params = dict(params, exportValues=1.0, exportActiveNeighs=1.0, exportGeodesicFlow=1.0)
+    out = hfm.run(params)
+    geo, flow = _oracle_on(out, params)
+    _check(out, dict(geo, geodesicFlow=flow), _suffixes(params), 1e-11, 1e-11)
+    assert out["GeodesicCPUTime"] > 0
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_geodesics_match_reference(name):
+    params, ref, _ = load_golden(name)
+    params = dict(params)
+    params.pop("exportActiveNeighs", None)
+    out = hfm.run(params)
+    _check(out, ref, _suffixes(params), 1e-7, 1e-7)
+
+
+def test_many_tips_one_launch():
+    """400 tips on a 192^2 Riemann2 grid with walls: every geodesic as the oracle's."""
+    p = W.riemann2_case(192, aniso=8.0, seed=31)
+    rng = np.random.default_rng(5)
+    p["walls"] = np.zeros((192, 192))
+    p["walls"][60, 20:170] = 1.0
+    p["walls"][130, 30:192] = 1.0
+    p["tips"] = rng.uniform(0.02, 0.98, (400, 2))
+    params = dict(p, exportValues=1.0, exportActiveNeighs=1.0)
+    out = hfm.run(params)
+    geo, _ = _oracle_on(out, params)
+    _check(out, geo, [""], 1e-11, 0)
+
+
+def test_point_overflow_rerun():
+    """A serpentine corridor makes the geodesic (1188 points) longer than the first output
+    allocation (2 * 128 / 0.25 = 1024 points): the tip is run again with more room."""
+    n = 64
+    walls = np.zeros((n, n))
+    for k, row in enumerate(range(4, n - 2, 4)):
+        if k % 2 == 0:
+            walls[row, 0:n - 4] = 1.0
+        else:
+            walls[row, 4:n] = 1.0
+    p = {"model": "Isotropic2", "arrayOrdering": "RowMajor", "dims": np.array([n, n], float), "gridScale": 1.0 / n,
+         "cost": 1.0, "walls": walls, "seeds": np.array([[0.5 / n, 0.5 / n]]), "tips": np.array([[0.97, 0.97]]),
+         "exportValues": 1.0, "exportActiveNeighs": 1.0, "verbosity": 0.0}
+    out = hfm.run(p)
+    geo, _ = _oracle_on(out, p)
+    assert geo["geodesicLengths"][0] > 1024
+    _check(out, geo, [""], 1e-11, 0)
+
+
+def test_set_overflow_rerun():
+    """A tiny weight threshold and no restarts keep up to 880 entries pending on a 32^3 grid (more
+    than the warp's shared-memory set holds) and 471 steps between two points: the tip is run again
+    with its set in global memory."""
+    m = 32
+    p = {"model": "Riemann3", "arrayOrdering": "RowMajor", "dims": np.array([m] * 3, float), "gridScale": 1.0 / m,
+         "metric": np.array([1., 0., 1., 0., 0., 1.]), "seeds": np.array([[0.5 / m] * 3]),
+         "tips": np.array([[0.97, 0.97, 0.97]]), "geodesicWeightThreshold": 1e-12, "geodesicVolumeBound": 1e9,
+         "exportValues": 1.0, "exportActiveNeighs": 1.0, "verbosity": 0.0}
+    out = hfm.run(p)
+    geo, _ = _oracle_on(out, p)
+    _check(out, geo, [""], 1e-11, 0)
+
+
+def test_batch_of_instances_with_tips_matches_single_runs():
+    cases = []
+    for k in range(3):
+        p = W.riemann2_case(64 + 16 * k, aniso=6.0, seed=40 + k)
+        p["tips"] = np.random.default_rng(k).uniform(0.05, 0.95, (5, 2))
+        cases.append(p)
+    c = W.curvature2_case(24, 16, "ReedsShepp2", seed=3, n_curves=3)
+    c["tips_Unoriented"] = np.array([[0.2, 0.3], [0.8, 0.7]])
+    singles = [hfm.run(dict(q)) for q in cases]
+    batch = hfm.run_batch([dict(q) for q in cases])
+    # a batch reaches the same fixed point up to rounding (the schedule differs)
+    for a, b in zip(singles, batch):
+        np.testing.assert_array_equal(a["geodesicLengths"], b["geodesicLengths"])
+        np.testing.assert_allclose(a["geodesicPoints"], b["geodesicPoints"], rtol=0, atol=1e-9)
+    one = hfm.run(dict(c))
+    two = hfm.run_batch([dict(c), dict(c)])
+    for r in two:
+        np.testing.assert_array_equal(one["geodesicLengths_Unoriented"], r["geodesicLengths_Unoriented"])
+        np.testing.assert_allclose(one["geodesicPoints_Unoriented"], r["geodesicPoints_Unoriented"], rtol=0,
+                                   atol=1e-9)
+
+
+def test_fp32_geodesics_close_to_fp64():
+    params, ref, _ = load_golden("geo_riemann2_48_walls")
+    params = dict(params, solverPrecision="float32")
+    params.pop("exportActiveNeighs", None)
+    out = hfm.run(params)
+    lens = out["geodesicLengths"]
+    assert len(lens) == len(ref["geodesicLengths"])
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(int)
+    rstarts = np.concatenate([[0], np.cumsum(ref["geodesicLengths"])[:-1]]).astype(int)
+    for s, rs, ln, rl in zip(starts, rstarts, lens, ref["geodesicLengths"]):
+        a, b = out["geodesicPoints"][int(s + ln - 1)], ref["geodesicPoints"][int(rs + rl - 1)]
+        assert np.max(np.abs(a - b)) < 0.05   # both end at the seed
