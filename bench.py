@@ -58,6 +58,10 @@ def parse_args(argv=None):
     ap.add_argument("--tti-side", type=int, default=128, help="grid side of the TTI3 differentiation leg")
     ap.add_argument("--tti-fd-voxels", type=int, default=8, help="voxels checked by central differences")
     ap.add_argument("--no-diff", action="store_true", help="skip the TTI3 differentiation leg")
+    ap.add_argument("--geo-side", type=int, default=1024, help="grid side of the geodesic leg (Riemann2)")
+    ap.add_argument("--geo-tips", type=int, default=4096, help="tips of the geodesic leg")
+    ap.add_argument("--geo-cpu-tips", type=int, default=64, help="tips timed on the reference CPU build")
+    ap.add_argument("--no-geo", action="store_true", help="skip the geodesic leg")
     return ap.parse_args(argv)
 
 
@@ -426,6 +430,48 @@ def differentiation_leg(args):
             "fd_step": "1e-4 vp, central", "dtype": "f64"}
 
 
+def geodesic_leg(args):
+    """Geodesic backtracking throughput: Riemann2 1024^2 (anisotropy 8, smooth random orientation,
+    two wall segments, one seed at the centre) with --geo-tips random tips. GPU: the geodesic stage
+    of one run (CUDA events around the warp-per-tip kernel and its copies, `GeodesicCPUTime`), and
+    the whole run through the public call. CPU: the reference's FileHFM_Riemann2 on the same input
+    with --geo-cpu-tips of the tips (its own `GeodesicCPUTime`, one core)."""
+    import hamiltonfastmarching_b200 as H
+    from hamiltonfastmarching_b200 import workloads as W
+    n = args.geo_side
+    p = W.riemann2_case(n, aniso=8.0, seed=11, seed_points=np.array([[0.5, 0.5]]))
+    p["walls"] = np.zeros((n, n))
+    p["walls"][n // 4, n // 8: 7 * n // 8] = 1.0
+    p["walls"][3 * n // 4, 0: 5 * n // 8] = 1.0
+    rng = np.random.default_rng(12)
+    tips = rng.uniform(0.01, 0.99, (args.geo_tips, 2))
+    q = dict(p, tips=tips, verbosity=0.0, exportValues=0.0)
+    H.run(q)  # warm-up
+    t0 = time.perf_counter()
+    out = H.run(q)
+    run_s = time.perf_counter() - t0
+    gpu_s = float(out["GeodesicCPUTime"])
+    npts = int(np.sum(out["geodesicLengths"]))
+    res = {"workload": f"Riemann2 {n}^2, anisotropy 8, 2 wall segments, 1 seed; {len(tips)} random tips",
+           "tips": len(tips), "points": npts, "mean_points_per_tip": npts / len(tips),
+           "gpu_geodesic_s": gpu_s, "tips_per_s": len(tips) / gpu_s, "run_s": run_s,
+           "gpu_solve_s": float(out["GPUSolveTime"]), "dtype": "f64"}
+    from oracle.refrun import have_reference, run_reference
+    if not args.no_cpu_baseline and have_reference("Riemann2") and args.geo_cpu_tips > 0:
+        k = min(args.geo_cpu_tips, len(tips))
+        ref = run_reference(dict(p, tips=tips[:k], verbosity=0.0, exportValues=0.0))
+        if ref.get("retcode") == 0:
+            cpu_s = float(ref["GeodesicCPUTime"])
+            res["cpu_baseline"] = {"tips_per_s": k / cpu_s, "cores": 1, "kind": "reference",
+                                   "sample": f"FileHFM_Riemann2 on the same input with the first {k} tips: "
+                                             f"GeodesicCPUTime {cpu_s:.3f} s"}
+            gk = int(np.sum(out["geodesicLengths"][:k]))
+            rk = int(np.sum(ref["geodesicLengths"]))
+            res["cpu_baseline"]["points_same_tips"] = {"gpu": gk, "reference": rk}
+            res["speedup_tips_per_s_vs_1_core"] = res["tips_per_s"] / (k / cpu_s)
+    return res
+
+
 # ------------------------------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -572,6 +618,9 @@ def run_ours(args):
     diff = None
     if not args.no_diff and rank == 0:
         diff = differentiation_leg(args)
+    geo = None
+    if not args.no_geo and rank == 0:
+        geo = geodesic_leg(args)
 
     if rank == 0:
         line = {
@@ -592,6 +641,7 @@ def run_ours(args):
             "batch": batch,
             "serving": serving,
             "differentiation": diff,
+            "geodesics": geo,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -52,8 +52,10 @@ struct GeoSet {
     long long key[CAP];
     double sv[SCAP];        // step list: value of the extracted entry and the step of the mean
     double sd[SCAP][3];
-    unsigned foff[kGeoMaxFlow];
+    unsigned foff[kGeoMaxFlow];  // flow of the extracted cell
     double fw[kGeoMaxFlow];
+    long long ckey[kGeoMaxFlow]; // its children: packed unwrapped index, pending slot or -1
+    int cfound[kGeoMaxFlow];
 };
 
 __device__ __forceinline__ long long geo_pack(const int *ind) {
@@ -185,7 +187,7 @@ __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1,
                 if (!((act >> si) & 1u) || n >= kGeoMaxFlow) continue;
                 const int s = si ? -1 : 1;
                 int y0 = x0 + s * o0, y1 = x1 + s * o1, y2 = x2 + s * o2;
-                g.wrap(y0, y1, y2);
+                if (!g.wrap(y0, y1, y2)) continue;  // active neighbours are inside; kept as a guard
                 nv[n] = (double)values[g.lin(y0, y1, y2)];
                 wts[n] = wb;
                 foff[n] = pack_off(s * o0, s * o1, s * o2);
@@ -361,31 +363,55 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, int D, GeoSet<CA
         double wSum = 0.0;
         for (int f = 0; f < nf; ++f) wSum = A::add(wSum, S.fw[f]);
         if (wSum == 0) continue;
+        // children: lane f computes the index, key and value of child f (their loads overlap), one
+        // pass over the pending entries finds those already there; they are then added in flow
+        // order, as the reference does (the insertion threshold depends on the running sum)
+        long long ckey = 0;
+        double cval = 0.0;
+        bool cok = true;
+        if (lane < nf) {
+            const unsigned oc = S.foff[lane];
+            int c[3] = {ind[0] + off_c(oc, 0), ind[1] + off_c(oc, 1), ind[2] + off_c(oc, 2)};
+            cok = geo_packable(c);
+            if (cok) {
+                ckey = geo_pack(c);
+                cok = g.wrap(c[0], c[1], c[2]);  // flow neighbours are inside; kept as a guard
+                if (cok) cval = (double)values[g.lin(c[0], c[1], c[2])];
+            }
+            S.ckey[lane] = ckey;
+            S.cfound[lane] = -1;
+        }
+        if (__any_sync(0xffffffffu, !cok)) { status |= kGeoRange; return 0; }
+        __syncwarp();
+        for (int j = lane; j < n; j += 32) {
+            const long long k = S.key[j];
+            for (int f = 0; f < nf; ++f)
+                if (S.ckey[f] == k) S.cfound[f] = j;
+        }
+        __syncwarp();
         for (int f = 0; f < nf; ++f) {
             const double w = A::div(A::mul(ew, S.fw[f]), wSum);
-            const unsigned oc = S.foff[f];
-            int c[3] = {ind[0] + off_c(oc, 0), ind[1] + off_c(oc, 1), ind[2] + off_c(oc, 2)};
-            if (!geo_packable(c)) { status |= kGeoRange; return 0; }
-            const long long key = geo_pack(c);
-            int found = -1;
-            for (int j = lane; j < n; j += 32)
-                if (S.key[j] == key) found = j;
-            const unsigned ball = __ballot_sync(0xffffffffu, found >= 0);
-            if (ball) {
-                if (lane == __ffs(ball) - 1) S.w[found] = A::add(S.w[found], w);
+            const long long key = __shfl_sync(0xffffffffu, ckey, f);
+            const double val = __shfl_sync(0xffffffffu, cval, f);
+            const int found = S.cfound[f];
+            __syncwarp();
+            if (found >= 0) {
+                if (lane == 0) S.w[found] = A::add(S.w[found], w);
             } else {
                 if (w < A::mul(ws, thr)) continue;
                 if (n >= CAP) { status |= kGeoSetOverflow; return 0; }
-                int p0 = c[0], p1 = c[1], p2 = c[2];
-                g.wrap(p0, p1, p2);
                 if (lane == 0) {
-                    S.val[n] = (double)values[g.lin(p0, p1, p2)];
+                    S.val[n] = val;
                     S.key[n] = key;
                     S.w[n] = w;
                 }
+                // a later child with the same offset (repeated forward differences) adds to it
+                if (lane > f && lane < nf && ckey == key) S.cfound[lane] = n;
                 ++n;
             }
             __syncwarp();
+            int c[3];
+            geo_unpack(key, c);
             sums(w, c);
         }
         if (ws <= 0) {
