@@ -695,12 +695,52 @@ static bkey bheap_pop(bheap_t *h) {
     return top;
 }
 
+/* ValueVariation for Eulerian stencils (FirstVariation.h:198-251): the active neighbours in
+ * stencil order with weights w max(0, value - u_neighbour) normalised by their sum, and the local
+ * derivative (sum of w valueDiff) / sum (times the speed multiplier of shared stencils). */
+static double eul_value_variation(const fmo_problem *p, const double *values, const uint64_t *active, int64_t x,
+                                  int64_t *nb_idx, double *nb_w, int *nn_out) {
+    const int nd = p->nfwd + p->nsym;
+    int64_t idx[3], nidx[3];
+    index_of(p, x, idx);
+    const double value = values[x];
+    const int64_t sid = stencil_id(p, idx, x);
+    const int8_t *O = p->off + sid * nd * 3;
+    const double *W = p->w + sid * nd;
+    const uint64_t act = active[x];
+    double var = 0.0, weightSum = 0.0;
+    int nn = 0;
+    int bit = 0;
+    for (int k2 = 0; k2 < nd; ++k2) {
+        for (int sg = 1; sg >= -1; sg -= 2) {
+            if (sg == -1 && k2 < p->nfwd) break;
+            const int b = (k2 < p->nfwd) ? bit : bit + (sg == 1 ? 0 : 1);
+            if (act & (1ULL << b)) {
+                for (int a = 0; a < p->ndim; ++a) nidx[a] = idx[a] + sg * O[3 * k2 + a];
+                periodize(p, nidx);
+                const int64_t y = linear_of(p, nidx);
+                const double d = value - values[y];
+                const double valueDiff = 0.0 < d ? d : 0.0;
+                const double w = diff_weight(p, W[k2], x) * valueDiff;
+                weightSum += w;
+                nb_idx[nn] = y; nb_w[nn] = w; ++nn;
+                var += w * valueDiff;
+            }
+        }
+        bit += (k2 < p->nfwd) ? 1 : 2;
+    }
+    *nn_out = nn;
+    if (weightSum == 0.0) return var;
+    const double inv = 1.0 / weightSum;
+    for (int j = 0; j < nn; ++j) nb_w[j] *= inv;
+    return p->mult ? inv * (p->mult[x] * var) : inv * var;
+}
+
 int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const uint64_t *active,
                                int npts, const int64_t *pt_index, const double *pt_weight,
                                double *sensitivity, int64_t max_seeds, int64_t *seed_out_index,
                                double *seed_out_weight) {
     const int64_t N = ncells(p);
-    const int nd = p->nfwd + p->nsym;
     /* pending weight per cell; in_map marks membership of (values[x], x) in the ordered set */
     double *pend = (double *)calloc(N, sizeof(double));
     uint8_t *in_map = (uint8_t *)calloc(N, 1);
@@ -715,7 +755,6 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
         bheap_push(&h, (bkey){values[x], x});
     }
     int64_t nseeds = 0;
-    int64_t idx[3], nidx[3];
     int64_t nb_idx[64];
     double nb_w[64];
     while (h.n > 0) {
@@ -726,42 +765,11 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
         const double weight = pend[x];
         pend[x] = 0.0;
         if (weight == 0.0) continue;
-        /* ValueVariation */
-        index_of(p, x, idx);
-        const double value = values[x];
-        const int64_t sid = stencil_id(p, idx, x);
-        const int8_t *O = p->off + sid * nd * 3;
-        const double *W = p->w + sid * nd;
-        const uint64_t act = active[x];
-        double var = 0.0, weightSum = 0.0;
         int nn = 0;
-        int bit = 0;
-        for (int k2 = 0; k2 < nd; ++k2) {
-            for (int sg = 1; sg >= -1; sg -= 2) {
-                if (sg == -1 && k2 < p->nfwd) break;
-                const int b = (k2 < p->nfwd) ? bit : bit + (sg == 1 ? 0 : 1);
-                if (act & (1ULL << b)) {
-                    for (int a = 0; a < p->ndim; ++a) nidx[a] = idx[a] + sg * O[3 * k2 + a];
-                    periodize(p, nidx);
-                    const int64_t y = linear_of(p, nidx);
-                    const double d = value - values[y];
-                    const double valueDiff = 0.0 < d ? d : 0.0;
-                    const double w = diff_weight(p, W[k2], x) * valueDiff;
-                    weightSum += w;
-                    nb_idx[nn] = y; nb_w[nn] = w; ++nn;
-                    var += w * valueDiff;
-                }
-            }
-            bit += (k2 < p->nfwd) ? 1 : 2;
-        }
+        const double var = eul_value_variation(p, values, active, x, nb_idx, nb_w, &nn);
         if (nn == 0) {
             if (nseeds < max_seeds) { seed_out_index[nseeds] = x; seed_out_weight[nseeds] = weight; }
             ++nseeds;
-        }
-        if (weightSum != 0.0) {
-            const double inv = 1.0 / weightSum;
-            for (int j = 0; j < nn; ++j) nb_w[j] *= inv;
-            var = p->mult ? inv * (p->mult[x] * var) : inv * var;
         }
         sensitivity[x] = weight * var;
         for (int j = 0; j < nn; ++j) {
@@ -1703,5 +1711,84 @@ int fmo_tti_geodesic_flow(const int64_t *dims, const double *h, const double *me
     for (int a = 0; a < 3; ++a) g.dims[a] = dims[a];
     tti_ctx T = {dims, h, metric, values, t_active};
     geo_flow_all(&g, tti_flow, &T, flow, value, width);
+    return 0;
+}
+
+
+/* ========================================================================================== */
+/* Forward first variation (Headers/ExtraAlgorithms/FirstVariation.h:389-429, inputs :103-124):
+ * cells in increasing (value, index) order; result(x, k) += ValueVariation(x) * costVariation(x, k),
+ * then += w_i result(neighbour_i, k) over the normalised flow. `result` [N][nvar] holds the seed
+ * value variations on entry (zero elsewhere); cost_var [N][nvar] may be NULL (no cost variation). */
+typedef struct { double val; int64_t idx; } vkey;
+
+static int vkey_cmp(const void *a, const void *b) {
+    const vkey *x = (const vkey *)a, *y = (const vkey *)b;
+    if (x->val < y->val) return -1;
+    if (x->val > y->val) return 1;
+    return x->idx < y->idx ? -1 : (x->idx > y->idx ? 1 : 0);
+}
+
+static vkey *sorted_cells(const double *values, int64_t N) {
+    vkey *o = (vkey *)malloc((size_t)N * sizeof(vkey));
+    if (!o) return NULL;
+    for (int64_t x = 0; x < N; ++x) { o[x].val = values[x]; o[x].idx = x; }
+    qsort(o, (size_t)N, sizeof(vkey), vkey_cmp);
+    return o;
+}
+
+int fmo_forward_variation(const fmo_problem *p, const double *values, const uint64_t *active, int nvar,
+                          const double *cost_var, double *result) {
+    const int64_t N = ncells(p);
+    vkey *order = sorted_cells(values, N);
+    if (!order) return -1;
+    int64_t nb_idx[64];
+    double nb_w[64];
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t x = order[i].idx;
+        int nn = 0;
+        const double var = eul_value_variation(p, values, active, x, nb_idx, nb_w, &nn);
+        for (int k = 0; k < nvar; ++k) {
+            double r = result[x * nvar + k];
+            r += var * (cost_var ? cost_var[x * nvar + k] : 0.0);
+            for (int j = 0; j < nn; ++j) r += nb_w[j] * result[nb_idx[j] * nvar + k];
+            result[x * nvar + k] = r;
+        }
+    }
+    free(order);
+    return 0;
+}
+
+int fmo_tti_forward_variation(const int64_t *dims, const double *h, const double *metric, const double *values,
+                              const double *t_active, int nvar, const double *cost_var, double *result) {
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    vkey *order = sorted_cells(values, N);
+    if (!order) return -1;
+    int64_t nb[6];
+    double nbw[6];
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t x = order[i].idx;
+        /* semi-Lagrangian ValueVariation (FirstVariation.h:169-196), as in the backward sweep */
+        int nn = 0;
+        double rec = values[x];
+        if (t_active[x] < FMO_INF) {
+            tti_norm n;
+            if (!tti_setup(metric + 14 * x, h, &n)) rec = tti_recompute(&n, dims, values, x, fabs(t_active[x]), nb, nbw, &nn);
+        }
+        double ws = 0.0;
+        for (int j = 0; j < nn; ++j) ws += nbw[j];
+        double var = rec;
+        for (int j = 0; j < nn; ++j) {
+            nbw[j] = nbw[j] / ws;
+            var -= nbw[j] * values[nb[j]];
+        }
+        for (int k = 0; k < nvar; ++k) {
+            double r = result[x * nvar + k];
+            r += var * (cost_var ? cost_var[x * nvar + k] : 0.0);
+            for (int j = 0; j < nn; ++j) r += nbw[j] * result[nb[j] * nvar + k];
+            result[x * nvar + k] = r;
+        }
+    }
+    free(order);
     return 0;
 }

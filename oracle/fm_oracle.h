@@ -101,6 +101,12 @@ int64_t fmo_tti_geodesic_discrete(const int64_t *dims, const double *h, const do
  * and width (value, width may be NULL). */
 int fmo_geodesic_flow(const fmo_problem *p, const double *values, const uint64_t *active, double *flow,
                       double *value, double *width);
+/* Forward first variation: result [N][nvar] holds the seed value variations on entry and the
+ * valueVariation on return; cost_var [N][nvar] or NULL. Returns 0, or -1 on allocation failure. */
+int fmo_forward_variation(const fmo_problem *p, const double *values, const uint64_t *active, int nvar,
+                          const double *cost_var, double *result);
+int fmo_tti_forward_variation(const int64_t *dims, const double *h, const double *metric, const double *values,
+                              const double *t_active, int nvar, const double *cost_var, double *result);
 int fmo_tti_geodesic_flow(const int64_t *dims, const double *h, const double *metric, const double *values,
                           const double *t_active, double *flow, double *value, double *width);
 

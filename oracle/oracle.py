@@ -83,6 +83,8 @@ def lib():
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_int64, _P, _P, _P]
         L.fmo_tti_geodesic_discrete.restype = ctypes.c_int64
         L.fmo_geodesic_flow.argtypes = [ctypes.POINTER(_Problem), _P, _P, _P, _P, _P]
+        L.fmo_forward_variation.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, _P]
+        L.fmo_tti_forward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P]
         L.fmo_tti_geodesic_flow.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
@@ -477,3 +479,51 @@ def geodesic_flow(res: Dict) -> np.ndarray:
         flow = np.empty((values.size, P.ndim))
         lib().fmo_geodesic_flow(ctypes.byref(P.struct), _ptr(values), _ptr(res["activeNeighs"]), _ptr(flow), None, None)
     return (-(flow * scale)).reshape(dims + (len(dims),))
+
+
+def forward_variation(res: Dict, params: Dict) -> np.ndarray:
+    """valueVariation of a :func:`solve` or :func:`tti_solve` result for the ``costVariation`` and
+    ``seedValueVariation`` keys of ``params`` (RowMajor): dims + (nVar,)
+    (``FirstVariation.h:103-124, 389-429``)."""
+    tti = "_tti" in res
+    if tti:
+        d, hs, metric, origin = res["_tti"]
+        dims = tuple(int(x) for x in d)
+        adim = lambda q: (np.asarray(q, float) - origin) / hs
+        periodic = [0, 0, 0]
+    else:
+        P: Problem = res["problem"]
+        dims, adim, periodic = P.dims, P._adim, P.periodic
+    n = int(np.prod(dims))
+    cost = None
+    nvar = 0
+    if "costVariation" in params:
+        cost = np.ascontiguousarray(np.asarray(params["costVariation"], float).reshape(n, -1))
+        nvar = cost.shape[1]
+    seedvar = None
+    if "seedValueVariation" in params:
+        seedvar = np.atleast_2d(np.asarray(params["seedValueVariation"], float))
+        nvar = max(nvar, seedvar.shape[0])
+    result = np.zeros((n, nvar))
+    if seedvar is not None:
+        seeds = np.atleast_2d(np.asarray(params["seeds"], float))
+        if seeds.shape[0] != seedvar.shape[1]:
+            raise ValueError("Error : Inconsistent size of seedValueVariation")
+        for i, q in enumerate(seeds):
+            idx = [int(math.floor(c)) for c in adim(q)]
+            for a, m in enumerate(dims):
+                if periodic[a]:
+                    idx[a] %= m
+            if all(0 <= idx[a] < dims[a] for a in range(len(dims))):
+                result[np.ravel_multi_index(tuple(idx), dims)] = seedvar[:, i]
+    values = np.ascontiguousarray(res["values"].ravel())
+    if tti:
+        tact = np.ascontiguousarray(res["activeNeighs"].ravel())
+        rc = lib().fmo_tti_forward_variation(_ptr(d), _ptr(hs), _ptr(metric), _ptr(values), _ptr(tact), nvar,
+                                             _ptr(cost), _ptr(result))
+    else:
+        rc = lib().fmo_forward_variation(ctypes.byref(P.struct), _ptr(values), _ptr(res["activeNeighs"]), nvar,
+                                         _ptr(cost), _ptr(result))
+    if rc != 0:
+        raise RuntimeError("oracle forward variation failed")
+    return result.reshape(dims + (nvar,))

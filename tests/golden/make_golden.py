@@ -105,7 +105,7 @@ def save(name, params, out, **extra):
         blob["in_" + k] = np.asarray(v) if not isinstance(v, str) else np.array(v)
     for k in ("values", "activeNeighs", "nAccepted", "MaxStencilWidth", "costSensitivity_0",
               "seedSensitivity_0", "spreadedSeeds", "spreadedSeedValues", "geodesicPoints", "geodesicLengths",
-              "geodesicPoints_Unoriented", "geodesicLengths_Unoriented", "geodesicFlow"):
+              "geodesicPoints_Unoriented", "geodesicLengths_Unoriented", "geodesicFlow", "valueVariation"):
         if k in out:
             blob["out_" + k] = np.asarray(out[k])
     blob.update(extra)
@@ -183,13 +183,38 @@ def geodesic_fixtures():
     solve_fixture("geo_tti3_12", p)
 
 
+def variation_fixtures():
+    """Forward first variation (costVariation, seedValueVariation -> valueVariation)."""
+    rng = np.random.default_rng(2025)
+    p = W.riemann2_case(40, aniso=6.0, seed=5, n_seeds=3)
+    p["costVariation"] = rng.standard_normal((40, 40, 2))
+    p["seedValueVariation"] = rng.standard_normal((2, 3))
+    solve_fixture("fwd_riemann2_40_seeds", p)
+    p = W.riemann3_case(16, n_spheres=3, n_seeds=2, rmin=0.1, rmax=0.2, seed=9)
+    p["costVariation"] = rng.standard_normal((16, 16, 16, 2))
+    solve_fixture("fwd_riemann3_16_walls", p)
+    for model, name in (("ReedsShepp2", "fwd_reedsshepp2_20x12"), ("Elastica2", "fwd_elastica2_20x12")):
+        p = W.curvature2_case(20, 12, model, seed=4, n_curves=3)
+        p["costVariation"] = rng.standard_normal((20, 20, 12, 1))
+        p["seedValueVariation"] = np.array([[0.7]])
+        solve_fixture(name, p)
+    p = W.tti3_case(12, h=0.01, seed=2)
+    p.pop("_vp")
+    p["costVariation"] = rng.standard_normal((12, 12, 12, 2))
+    p["seedValueVariation"] = rng.standard_normal((2, 1))
+    solve_fixture("fwd_tti3_12", p)
+
+
 if __name__ == "__main__":
-    # `make_golden.py tti` / `make_golden.py geodesic` regenerate only those fixtures
+    # `make_golden.py tti|geodesic|variation` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
         geodesic_fixtures()
+    elif sys.argv[1:] == ["variation"]:
+        variation_fixtures()
     else:
         main()
         tti_fixtures()
         geodesic_fixtures()
+        variation_fixtures()

@@ -94,3 +94,21 @@ def test_geodesic_oracle_matches_reference(name):
     fin = np.isfinite(rflow)
     assert np.array_equal(fin, np.isfinite(flow))
     assert np.max(np.abs(flow[fin] - rflow[fin])) <= 1e-12 * np.max(np.abs(rflow[fin]))
+
+
+GOLDEN_VARIATIONS = ["fwd_riemann2_40_seeds", "fwd_riemann3_16_walls", "fwd_reedsshepp2_20x12", "fwd_elastica2_20x12",
+                     "fwd_tti3_12"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_VARIATIONS)
+def test_forward_variation_oracle_matches_reference(name):
+    """valueVariation (costVariation, seedValueVariation): bit for bit on the Eulerian models,
+    within 1e-14 of its max on TTI3."""
+    params, ref, _ = load_golden(name)
+    res = O.tti_solve(params) if params["model"] == "TTI3" else O.solve(params)
+    v, r = O.forward_variation(res, params), ref["valueVariation"]
+    assert v.shape == r.shape
+    if params["model"] == "TTI3":
+        assert np.max(np.abs(v - r)) <= 1e-14 * np.max(np.abs(r))
+    else:
+        np.testing.assert_array_equal(v, r)
