@@ -1542,41 +1542,69 @@ __global__ void flow_sort_kernel(long long N, const long long *rptr, int *rx, do
     }
 }
 
+// Upwind flow graph of a solved single instance: per cell its normalised flow (fidx, fw, nflow)
+// and local derivative (var), and the reverse adjacency (rptr, rx, rw: the downwind cells that
+// read each cell, sorted) with the reverse degrees (indeg0).
+struct FlowGraph {
+    long long N = 0, ne = 0;
+    DeviceBuffer<int> fidx, indeg0, rx;
+    DeviceBuffer<double> fw, var, rw;
+    DeviceBuffer<uint8_t> nflow;
+    DeviceBuffer<long long> rptr;
+};
+
 template <typename Real, int NFWD, int NSYM, int KIND>
-void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
-                 DeviceBuffer<unsigned> &status, cudaStream_t s) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+void build_flow_graph(const Dev<Real> &P, long long N, FlowGraph &G, cudaStream_t s) {
     constexpr int ND = NFWD + NSYM;
     constexpr int NF = 2 * ND > 32 ? 32 : 2 * ND;
-    if (N >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large for the adjoint");
-    DeviceBuffer<int> fidx((size_t)NF * N), indeg0(N), indeg(N);
-    DeviceBuffer<double> fw((size_t)NF * N), var(N), acc(N), sens(N);
-    DeviceBuffer<uint8_t> nflow(N);
-    indeg0.zero(s);
-    launch(flow_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, P, fidx.get(), fw.get(), var.get(),
-                                                                          nflow.get(), indeg0.get());
+    if (N >= (1ll << 31)) throw Error(HFM_ERR_UNSUPPORTED, "grid too large for the first variation");
+    G.N = N;
+    G.fidx.alloc((size_t)NF * N);
+    G.indeg0.alloc(N);
+    G.fw.alloc((size_t)NF * N);
+    G.var.alloc(N);
+    G.nflow.alloc(N);
+    G.indeg0.zero(s);
+    launch(flow_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, P, G.fidx.get(), G.fw.get(), G.var.get(),
+           G.nflow.get(), G.indeg0.get());
     HFM_CUDA(cudaGetLastError());
     // reverse adjacency (CSR over y, offsets scanned on the host)
-    DeviceBuffer<long long> rptr(N + 1);
+    G.rptr.alloc(N + 1);
     std::vector<int> hdeg(N);
-    indeg0.download(hdeg.data(), N, s);
+    G.indeg0.download(hdeg.data(), N, s);
     HFM_CUDA(cudaStreamSynchronize(s));
     std::vector<long long> hrptr(N + 1);
     long long ne = 0;
     for (long long y = 0; y < N; ++y) { hrptr[y] = ne; ne += hdeg[y]; }
     hrptr[N] = ne;
-    rptr.upload(hrptr, s);
-    DeviceBuffer<int> rx(std::max(1ll, ne));
-    DeviceBuffer<double> rw(std::max(1ll, ne)), lam(N);
-    {
-        DeviceBuffer<unsigned> cursor(N);
-        cursor.zero(s);
-        launch(flow_scatter_kernel, nblocks(N, 256), 256, 0, s, N, fidx.get(), fw.get(), nflow.get(), rptr.get(),
-               cursor.get(), rx.get(), rw.get());
-        launch(flow_sort_kernel<Real>, nblocks(N, 256), 256, 0, s, N, rptr.get(), rx.get(), rw.get(), P.values);
-        HFM_CUDA(cudaGetLastError());
-        HFM_CUDA(cudaStreamSynchronize(s));
+    G.ne = ne;
+    G.rptr.upload(hrptr, s);
+    G.rx.alloc(std::max(1ll, ne));
+    G.rw.alloc(std::max(1ll, ne));
+    DeviceBuffer<unsigned> cursor(N);
+    cursor.zero(s);
+    launch(flow_scatter_kernel, nblocks(N, 256), 256, 0, s, N, G.fidx.get(), G.fw.get(), G.nflow.get(), G.rptr.get(),
+           cursor.get(), G.rx.get(), G.rw.get());
+    launch(flow_sort_kernel<Real>, nblocks(N, 256), 256, 0, s, N, G.rptr.get(), G.rx.get(), G.rw.get(), P.values);
+    HFM_CUDA(cudaGetLastError());
+    HFM_CUDA(cudaStreamSynchronize(s));
+}
+
+template <typename Real, int NFWD, int NSYM, int KIND>
+void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
+                 DeviceBuffer<unsigned> &status, cudaStream_t s, FlowGraph *graph = nullptr) {
+    FlowGraph own;
+    if (!graph) {
+        build_flow_graph<Real, NFWD, NSYM, KIND>(P, N, own, s);
+        graph = &own;
     }
+    FlowGraph &G = *graph;
+    DeviceBuffer<int> indeg(N);
+    DeviceBuffer<double> acc(N), sens(N), lam(N);
+    DeviceBuffer<int> &fidx = G.fidx, &indeg0 = G.indeg0, &rx = G.rx;
+    DeviceBuffer<double> &fw = G.fw, &var = G.var, &rw = G.rw;
+    DeviceBuffer<uint8_t> &nflow = G.nflow;
+    DeviceBuffer<long long> &rptr = G.rptr;
     DeviceBuffer<int> lists(3 * N);
     DeviceBuffer<unsigned> counters(8);
     const unsigned seed_cap = 1u << 20;
@@ -1657,6 +1685,159 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
         for (size_t k : order) { ar.seed_index.push_back(si[k]); ar.seed_weight.push_back(sw[k]); }
         res.adjoints.push_back(std::move(ar));
     }
+}
+
+// Forward first variation (FirstVariation.h:389-429): cells in upwind-to-downwind order, each
+// pulling result(x, k) = result(x, k) + var(x) cost(x, k) + sum_j w_j result(y_j, k) over its
+// normalised flow, in the flow's order (so the sums are those of the reference, whatever the
+// schedule). A cell is ready once the cells it reads are done: a counter of pending upwind cells,
+// decremented through the reverse adjacency; rounds of ready lists in one cooperative launch.
+struct FwdDev {
+    long long N;
+    int nvar;
+    const int *fidx;
+    const double *fw;
+    const double *var;
+    const uint8_t *nflow;
+    const long long *rptr;
+    const int *rx;
+    const double *cost;  // [N][nvar] or null
+    double *res;         // [N][nvar]: seed value variations on entry
+    int *cnt;            // upwind cells not yet done
+    int *list[3];
+    unsigned *count[3];
+    unsigned *bar_count;
+    unsigned *bar_gen;
+    unsigned *status;
+    unsigned long long *rounds;
+    long long max_rounds;
+};
+
+__global__ void forward_roots_kernel(FwdDev F) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool want = x < F.N && F.cnt[x] == 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, want);
+    if (!bal) return;
+    unsigned base = 0;
+    if (lane == __ffs(bal) - 1) base = atomicAdd(F.count[0], (unsigned)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+    if (want) F.list[0][base + __popc(bal & ((1u << lane) - 1u))] = (int)x;
+}
+
+__global__ void forward_kernel(FwdDev F) {
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nth = (long long)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    long long r = 0;
+    bool ok = true;
+    for (; r < F.max_rounds; ++r) {
+        const int cur = (int)(r % 3), nxt = (int)((r + 1) % 3), old = (int)((r + 2) % 3);
+        if (blockIdx.x == 0 && threadIdx.x == 0) *F.count[old] = 0;
+        const long long n = *(volatile unsigned *)F.count[cur];
+        const long long nround = (n + 31) / 32 * 32;
+        for (long long i = tid; i < nround; i += nth) {
+            int x = -1;
+            if (i < n) x = F.list[cur][i];
+            long long e = 0, ee = 0;
+            if (x >= 0) {
+                const int nf = F.nflow[x];
+                const double v = F.var[x];
+                for (int k = 0; k < F.nvar; ++k) {
+                    double acc = __ldcg(F.res + (long long)x * F.nvar + k);
+                    acc = __dadd_rn(acc, __dmul_rn(v, F.cost ? F.cost[(long long)x * F.nvar + k] : 0.0));
+                    for (int j = 0; j < nf; ++j) {
+                        const long long y = F.fidx[j * F.N + x];
+                        acc = __dadd_rn(acc, __dmul_rn(F.fw[j * F.N + x], __ldcg(F.res + y * F.nvar + k)));
+                    }
+                    __stcg(F.res + (long long)x * F.nvar + k, acc);
+                }
+                __threadfence();
+                e = F.rptr[x];
+                ee = F.rptr[x + 1];
+            }
+            // downwind cells whose last pending input this was join the next round
+            while (__any_sync(0xffffffffu, e < ee)) {
+                bool want = false;
+                int z = 0;
+                if (e < ee) {
+                    z = F.rx[e];
+                    want = atomicSub(F.cnt + z, 1) == 1;
+                    ++e;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, want);
+                if (bal) {
+                    unsigned base = 0;
+                    if (lane == __ffs(bal) - 1) base = atomicAdd(F.count[nxt], (unsigned)__popc(bal));
+                    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+                    if (want) F.list[nxt][base + __popc(bal & ((1u << lane) - 1u))] = z;
+                }
+            }
+        }
+        ok = grid_barrier(F.bar_count, F.bar_gen, gridDim.x, F.status, kBarrierPolls);
+        if (!ok) break;
+        if (*(volatile unsigned *)F.count[nxt] == 0u) { ++r; break; }
+    }
+    if (ok && r >= F.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(F.status, (unsigned)kErrRoundCap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *F.rounds = (unsigned long long)r;
+}
+
+__global__ void nflow_to_count_kernel(long long N, const uint8_t *nflow, int *cnt) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < N) cnt[x] = nflow[x];
+}
+
+template <typename Real, int NFWD, int NSYM, int KIND>
+void run_forward(const Dev<Real> &P, long long N, const EulerProblem &p, EulerResult &res,
+                 DeviceBuffer<unsigned> &status, cudaStream_t s, FlowGraph &G) {
+    const int nvar = p.fwd_nvar;
+    DeviceBuffer<double> cost, out((size_t)N * nvar);
+    out.zero(s);
+    for (size_t i = 0; i < p.fwd_seed_cell.size(); ++i)
+        HFM_CUDA(cudaMemcpyAsync(out.get() + p.fwd_seed_cell[i] * nvar, p.fwd_seed_value.data() + i * nvar,
+                                 nvar * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (!p.fwd_cost.empty()) {
+        cost.alloc((size_t)N * nvar);
+        cost.upload(p.fwd_cost.data(), (size_t)N * nvar, s);
+    }
+    DeviceBuffer<int> cnt(N), lists(3 * N);
+    DeviceBuffer<unsigned> counters(8);
+    DeviceBuffer<unsigned long long> rounds(1);
+    counters.zero(s);
+    launch(nflow_to_count_kernel, nblocks(N, 256), 256, 0, s, N, G.nflow.get(), cnt.get());
+    FwdDev F{};
+    F.N = N;
+    F.nvar = nvar;
+    F.fidx = G.fidx.get();
+    F.fw = G.fw.get();
+    F.var = G.var.get();
+    F.nflow = G.nflow.get();
+    F.rptr = G.rptr.get();
+    F.rx = G.rx.get();
+    F.cost = p.fwd_cost.empty() ? nullptr : cost.get();
+    F.res = out.get();
+    F.cnt = cnt.get();
+    for (int i = 0; i < 3; ++i) { F.list[i] = lists.get() + i * N; F.count[i] = counters.get() + i; }
+    F.bar_count = counters.get() + 4;
+    F.bar_gen = counters.get() + 5;
+    F.status = status.get();
+    F.rounds = rounds.get();
+    F.max_rounds = N + 2;
+    int dev = 0, nsm = 0, per_sm = 0;
+    HFM_CUDA(cudaGetDevice(&dev));
+    HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_kernel, 256, 0));
+    if (per_sm < 1) throw Error(HFM_ERR_CUDA, "forward variation kernel cannot be resident");
+    launch(forward_roots_kernel, nblocks(N, 256), 256, 0, s, F);
+    void *args[] = {&F};
+    count_launch();
+    HFM_CUDA(cudaLaunchCooperativeKernel((void *)forward_kernel,
+                                         dim3(std::max(1, nsm * per_sm / std::max(1, solver_share()))), dim3(256),
+                                         args, 0, s));
+    check_status(status, "forward variation");
+    res.value_variation.resize((size_t)N * nvar);
+    out.download(res.value_variation.data(), (size_t)N * nvar, s);
+    HFM_CUDA(cudaStreamSynchronize(s));
 }
 
 // The device state that the reverse sweep reads (RetainedSolve of a single-instance solve).
@@ -2172,9 +2353,12 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     HFM_TRACE("outputs");
     run_geodesics<Real, NFWD, NSYM, KIND>(P, hinst, probs, results, s);
     HFM_TRACE("geodesics");
-    if (ninst == 1 && !p0.adjoint_index.empty()) {
+    if (ninst == 1 && (!p0.adjoint_index.empty() || p0.fwd_nvar > 0)) {
         tm.start(s);
-        run_adjoint<Real, NFWD, NSYM, KIND>(P, N, p0, results[0], status, s);
+        FlowGraph G;
+        build_flow_graph<Real, NFWD, NSYM, KIND>(P, N, G, s);
+        if (!p0.adjoint_index.empty()) run_adjoint<Real, NFWD, NSYM, KIND>(P, N, p0, results[0], status, s, &G);
+        if (p0.fwd_nvar > 0) run_forward<Real, NFWD, NSYM, KIND>(P, N, p0, results[0], status, s, G);
         results[0].t_adjoint_ms = tm.stop(s);
     }
     HFM_CUDA(cudaStreamSynchronize(s));

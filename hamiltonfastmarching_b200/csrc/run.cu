@@ -83,7 +83,7 @@ void reject_unsupported(Store &io) {
     static const char *keys[] = {"factoringValues", "speed_times", "cost_times",
                                  "metric_times", "dualMetric_times", "stopAtDistance", "nMaxAccepted",
                                  "stopWhenAnyAccepted", "stopWhenAllAccepted", "stopWhenAnyAccepted_Unoriented",
-                                 "stopWhenAllAccepted_Unoriented", "costVariation", "seedValueVariation",
+                                 "stopWhenAllAccepted_Unoriented",
                                  "euclideanScale", "seedFlags", "getStencils", "activeNeighs", "values",
                                  "factoringPointChoice"};
     for (const char *k : keys)
@@ -481,6 +481,45 @@ void read_geodesics(Store &io, const Param &pm, bool lifted, EulerProblem &p, bo
     p.want_geodesic_flow = io.get_scalar("exportGeodesicFlow", 0.0, 2) != 0;
 }
 
+// costVariation (dims + (nVar,), the store's ordering applied to all axes) and seedValueVariation
+// ((nVar, nSeeds), RowMajor whatever the ordering) of the forward first variation
+// (FirstVariation.h:103-124, 389-396).
+void read_forward_variation(Store &io, const Param &pm, EulerProblem &p) {
+    const bool cost = io.has_field("costVariation"), seed = io.has_field("seedValueVariation");
+    if (!cost && !seed) return;
+    int64_t ncells = 1;
+    for (int a = 0; a < pm.ndim; ++a) ncells *= pm.dims[a];
+    int kc = 0, ks = 0;
+    if (cost) {
+        const Field f = io.get_field("costVariation", pm.ndim + 1, 1);
+        bool ok = (int)f.dims.size() == pm.ndim + 1;
+        for (int a = 0; ok && a < pm.ndim; ++a) ok = f.dims[a] == pm.dims[a];
+        if (!ok) throw Error(HFM_ERR_VALUE, "Forward variation error : inconsistent input sizes");
+        kc = (int)f.dims[pm.ndim];
+        p.fwd_cost.assign(f.ptr(), f.ptr() + ncells * kc);
+    }
+    if (seed) {
+        const RawElement &r = io.raw("seedValueVariation");
+        if (r.is_string() || r.dims.size() != 2)
+            throw Error(HFM_ERR_VALUE, "IO::GetArray error : Field seedValueVariation has depth " +
+                                           std::to_string(r.dims.size()) + " instead of expected 2.");
+        int64_t ns = 0;
+        const std::vector<double> pts = io.get_vector("seeds", pm.ndim, &ns);
+        if (ns != r.dims[1]) throw Error(HFM_ERR_VALUE, "Error : Inconsistent size of seedValueVariation");
+        ks = (int)r.dims[0];
+        const double *sv = r.ptr();
+        for (int64_t i = 0; i < ns; ++i) {
+            int64_t lin;
+            if (!pm.index_of(&pts[i * pm.ndim], &lin)) continue;
+            p.fwd_seed_cell.push_back(lin);
+            for (int k = 0; k < ks; ++k) p.fwd_seed_value.push_back(sv[k * ns + i]);
+        }
+    }
+    if (cost && seed && kc != ks) throw Error(HFM_ERR_VALUE, "Forward variation error : inconsistent input sizes");
+    p.fwd_nvar = cost ? kc : ks;
+    if (p.fwd_nvar <= 0) throw Error(HFM_ERR_VALUE, "Forward variation error : inconsistent input sizes");
+}
+
 // A model read from its store, ready to solve (the part of Run before the solver loop).
 struct Prepared {
     Param pm;
@@ -528,6 +567,7 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
         return;
     }
     if (inspect) read_inspect(io, pm, p);
+    read_forward_variation(io, pm, p);
     // the arrival times are downloaded straight into the output field when no reordering is needed
     q.values_dst = q.export_values ? io.create_field("values", q.dims, 1) : nullptr;
     p.h_values_out = q.values_dst;
@@ -627,6 +667,11 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
         io.set_field("activeNeighs", dims, 1, a.data());
     }
     export_sensitivities(io, pm, dims, r.adjoints);
+    if (q.p.fwd_nvar > 0) {
+        std::vector<int64_t> vd(dims);
+        vd.push_back(q.p.fwd_nvar);
+        io.set_field("valueVariation", vd, 1, r.value_variation.data());
+    }
     export_geodesics(io, q, r);
     io.set_scalar("nAccepted", (double)r.n_accepted);
 }
@@ -864,19 +909,19 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
         });
     }
     HFM_TRACE("batch: stores read");
-    // Solving: instances of one stencil family and precision share one launch sequence; sensitivity
-    // requests run on their own.
+    // Solving: instances of one stencil family and precision share one launch sequence; first
+    // variation requests (inspectSensitivity, costVariation, seedValueVariation) run on their own.
     std::vector<char> done(n, 0);
     for (int i = 0; i < n; ++i) {
         if (rc[i] != HFM_OK || done[i] || qs[i]->skip) continue;
         std::vector<int> grp{i};
         done[i] = 1;
         const hfm::EulerProblem &pi = qs[i]->p;
-        if (pi.adjoint_index.empty()) {
+        if (pi.adjoint_index.empty() && pi.fwd_nvar == 0) {
             for (int j = i + 1; j < n; ++j) {
                 if (rc[j] != HFM_OK || done[j] || qs[j]->skip) continue;
                 const hfm::EulerProblem &pj = qs[j]->p;
-                if (pj.adjoint_index.empty() && pj.kind == pi.kind && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
+                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && pj.kind == pi.kind && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
                     pj.nsym == pi.nsym && pj.fp64 == pi.fp64 && pj.sweeps_per_tile == pi.sweeps_per_tile &&
                     pj.max_rounds == pi.max_rounds) {
                     grp.push_back(j);

@@ -74,6 +74,13 @@ struct EulerProblem {
     std::vector<double> geo_tips, geo_tips_unoriented;
     double geo_step = 0.25, geo_threshold = 1e-3, geo_volume_bound = 8.45;
     bool want_geodesic_flow = false;   // exportGeodesicFlow
+    // Forward first variation (costVariation, seedValueVariation): fwd_nvar variations; fwd_cost
+    // [N][nvar] RowMajor or empty; seed cells and their value variations [n][nvar], later entries
+    // overwriting earlier ones.
+    int fwd_nvar = 0;
+    std::vector<double> fwd_cost;
+    std::vector<int64_t> fwd_seed_cell;
+    std::vector<double> fwd_seed_value;
     int tile_shift[3] = {-1, -1, -1};  // log2 tile extents per axis (sum 6); -1: 8x8 / 4x4x4
     int sweeps_per_tile = 4;           // local Jacobi sweeps before a tile re-queues itself
     int max_rounds = 1 << 20;
@@ -116,6 +123,7 @@ struct EulerResult {
     std::vector<int64_t> geo_lengths[2];
     std::vector<int> geo_status[2], geo_restarts[2];
     std::vector<double> geodesic_flow;  // [N][ndim] sum of Recompute weight * offset (dimensionless)
+    std::vector<double> value_variation;  // [N][fwd_nvar] forward first variation
     double t_stencil_ms = 0, t_solve_ms = 0, t_adjoint_ms = 0, t_geodesic_ms = 0, t_total_ms = 0;
     long long rounds = 0, tile_activations = 0, local_solves = 0;
     std::shared_ptr<RetainedSolve> retained;  // set when EulerProblem::retain (single instance)

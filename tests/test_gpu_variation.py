@@ -1,0 +1,106 @@
+"""Forward first variation on the GPU (costVariation, seedValueVariation -> valueVariation).
+
+- Against the oracle run on the GPU's own arrival times and activeNeighs: same flows, same sums in
+  the same order, so within 1e-12 of the largest entry.
+- Against the reference's golden fixtures: the arrival times differ by at most 1e-10 (relative),
+  so the variations agree within 1e-8 of the largest entry.
+- Size-independent identity at full size: with the seed values as seedValueVariation and
+  costVariation = 1 (per-cell stencils, TTI3) or the cost, i.e. 1 / speed multiplier (shared
+  stencils, whose local derivative carries the multiplier), the forward variation telescopes to
+  the arrival times themselves (var(x) = m (u(x) - sum_i w_i u(y_i)) along the normalised flow).
+"""
+import numpy as np
+import pytest
+
+import hamiltonfastmarching_b200 as hfm
+from conftest import load_golden
+from hamiltonfastmarching_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = ["fwd_riemann2_40_seeds", "fwd_riemann3_16_walls", "fwd_reedsshepp2_20x12", "fwd_elastica2_20x12",
+          "fwd_tti3_12"]
+
+
+def _oracle_on(out, params):
+    if params["model"] == "TTI3":
+        res = O.tti_solve(params)
+        res["values"] = np.ascontiguousarray(out["values"])
+        res["activeNeighs"] = np.ascontiguousarray(out["activeNeighs"])
+    else:
+        res = {"values": np.ascontiguousarray(out["values"]),
+               "activeNeighs": np.ascontiguousarray(out["activeNeighs"].astype(np.uint64).ravel()),
+               "problem": O.Problem(params)}
+    return O.forward_variation(res, params)
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_forward_variation_matches_oracle_on_gpu_values(name):
+    params, _, _ = load_golden(name)
+    params = dict(params, exportValues=1.0, exportActiveNeighs=1.0)
+    out = hfm.run(params)
+    ref = _oracle_on(out, params)
+    v = out["valueVariation"]
+    assert v.shape == ref.shape
+    assert np.max(np.abs(v - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_forward_variation_matches_reference(name):
+    params, ref, _ = load_golden(name)
+    params = dict(params)
+    params.pop("exportActiveNeighs", None)
+    out = hfm.run(params)
+    v, r = out["valueVariation"], ref["valueVariation"]
+    assert v.shape == r.shape
+    assert np.max(np.abs(v - r)) <= 1e-8 * np.max(np.abs(r))
+
+
+@pytest.mark.parametrize("case", ["riemann3_96", "reedsshepp2_96", "tti3_48"])
+def test_unit_cost_variation_telescopes_to_values(case):
+    if case == "riemann3_96":
+        p = W.riemann3_case(96, n_spheres=12, n_seeds=4)
+    elif case == "reedsshepp2_96":
+        p = W.curvature2_case(96, 36, "ReedsShepp2", n_curves=8)
+    else:
+        p = W.tti3_case(48, h=0.01, seed=3)
+        p.pop("_vp")
+    dims = tuple(int(d) for d in p["dims"])
+    nseeds = len(np.atleast_2d(p["seeds"]))
+    seed_values = np.asarray(p.get("seedValues", np.zeros(nseeds)), float)
+    if p["model"] == "ReedsShepp2":
+        cost = np.asarray(p["cost"], float)
+        cv = np.broadcast_to(cost[:, :, None] if cost.ndim == 2 else cost, dims)[..., None]
+    else:
+        cv = np.ones(dims + (1,))
+    q = dict(p, costVariation=np.ascontiguousarray(cv), seedValueVariation=seed_values[None, :], exportValues=1.0,
+             verbosity=0.0)
+    out = hfm.run(q)
+    u, v = out["values"], out["valueVariation"][..., 0]
+    fin = np.isfinite(u)
+    assert np.max(np.abs(v[fin] - u[fin])) <= 1e-12 * np.max(np.abs(u[fin]))
+    assert np.all(v[~fin] == 0)
+
+
+def test_linearity_and_channels():
+    p = W.riemann2_case(128, aniso=6.0, seed=8, n_seeds=2)
+    rng = np.random.default_rng(4)
+    a, b = rng.standard_normal((128, 128)), rng.standard_normal((128, 128))
+    out = hfm.run(dict(p, costVariation=np.stack([a, b, a + b], axis=-1), verbosity=0.0))
+    v = out["valueVariation"]
+    scale = np.max(np.abs(v))
+    assert np.max(np.abs(v[..., 0] + v[..., 1] - v[..., 2])) <= 1e-12 * scale
+    # a second solve reaches the same fixed point up to rounding (the schedule may differ)
+    one = hfm.run(dict(p, costVariation=a[..., None], verbosity=0.0))["valueVariation"]
+    assert np.max(np.abs(one[..., 0] - v[..., 0])) <= 1e-10 * scale
+
+
+def test_inconsistent_variation_sizes_rejected():
+    p = W.riemann2_case(32, seed=1, n_seeds=2)
+    with pytest.raises(hfm.PyExp):
+        hfm.run(dict(p, costVariation=np.ones((32, 32, 2)), seedValueVariation=np.ones((3, 2)), verbosity=0.0))
+    with pytest.raises(hfm.PyExp):
+        hfm.run(dict(p, seedValueVariation=np.ones((1, 3)), verbosity=0.0))
+    with pytest.raises(hfm.PyExp):
+        hfm.run(dict(p, costVariation=np.ones((16, 32, 1)), verbosity=0.0))
