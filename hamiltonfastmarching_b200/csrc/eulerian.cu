@@ -2071,7 +2071,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         // instances' fronts for the value-ordered scheduling of a batch
         for (int i = 0; i < ninst; ++i) {
             const GridGeom &g = hinst[i].g;
-            const int nphys = SHARE ? 2 : probs[i]->ndim;
+            const int nphys = SHARE && probs[i]->angular ? 2 : probs[i]->ndim;
             double d2 = 0.0;
             for (int a = 0; a < nphys; ++a) d2 += (g.dims[a] * hinst[i].h[a]) * (g.dims[a] * hinst[i].h[a]);
             const double t = std::sqrt(d2) * hscale[i] / (double)g.ncells;
@@ -2416,6 +2416,12 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
         if (p.nfwd == 0 && p.nsym == 4) {
             if (p.fp64) run_batch_impl<double, 0, 4, detail::kKindShare>(probs, results);
             else run_batch_impl<float, 0, 4, detail::kKindShare>(probs, results);
+        } else if (p.nfwd == 0 && p.nsym == 2) {
+            if (p.fp64) run_batch_impl<double, 0, 2, detail::kKindShare>(probs, results);
+            else run_batch_impl<float, 0, 2, detail::kKindShare>(probs, results);
+        } else if (p.nfwd == 0 && p.nsym == 3) {
+            if (p.fp64) run_batch_impl<double, 0, 3, detail::kKindShare>(probs, results);
+            else run_batch_impl<float, 0, 3, detail::kKindShare>(probs, results);
         } else if (p.nfwd == 27 && p.nsym == 0) {
             if (p.fp64) run_batch_impl<double, 27, 0, detail::kKindShare>(probs, results);
             else run_batch_impl<float, 27, 0, detail::kKindShare>(probs, results);
@@ -2427,8 +2433,8 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
 
 void default_schedule(EulerProblem &p) {
     if (p.kind == StencilKind::TTI) { p.sweeps_per_tile = 1; p.band_lo = 1; p.band_hi = 4; }
-    else if (p.kind == StencilKind::SharedByTheta && p.nfwd > 0) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
-    else if (p.kind == StencilKind::SharedByTheta) { p.sweeps_per_tile = 4; p.band_lo = 2; p.band_hi = 8; }
+    else if (p.kind == StencilKind::SharedByTheta && p.angular && p.nfwd > 0) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
+    else if (p.kind == StencilKind::SharedByTheta && p.angular) { p.sweeps_per_tile = 4; p.band_lo = 2; p.band_hi = 8; }
     else if (p.ndim == 3) { p.sweeps_per_tile = 2; p.band_lo = 1; p.band_hi = 4; }
     else { p.sweeps_per_tile = 3; p.band_lo = 2; p.band_hi = 8; }
 }

@@ -323,33 +323,56 @@ void setup_tti(Store &io, Param &pm, EulerProblem &p) {
     }
 }
 
-void setup_isotropic2(Store &io, Param &pm, EulerProblem &p) {
-    // Isotropic2 solved as the Riemann metric cost^2 Id: its 4-point stencil is what Selling returns
-    // for a multiple of the identity, so values match the reference's isotropic scheme.
-    const std::vector<int> dims = read_dims(io, 2);
-    pm.ndim = 2;
-    p.ndim = 2;
-    const std::vector<double> origin = read_point(io, "origin", 2, {0.0, 0.0});
-    const double h = io.get_scalar("gridScale");
-    for (int a = 0; a < 2; ++a) {
+// Isotropic2 / Isotropic3 (Headers/Specializations/Isotropic.h:11-59): one symmetric difference
+// per axis, base weight 1 / h_i^2, times the squared speed of the cell (speed, or 1 / cost). Solved
+// as a shared stencil (the same table on every index of the last axis) with the speed as the
+// per-cell multiplier, so that activeNeighs, sensitivities and variations follow the reference's
+// multiplier semantics.
+void setup_isotropic(Store &io, int ndim, Param &pm, EulerProblem &p) {
+    const std::vector<int> dims = read_dims(io, ndim);
+    pm.ndim = ndim;
+    p.ndim = ndim;
+    const std::vector<double> origin = read_point(io, "origin", ndim, std::vector<double>(ndim, 0.0));
+    std::vector<double> hs(ndim);
+    if (io.has_field("gridScales")) {
+        hs = read_point(io, "gridScales", ndim, hs);
+    } else {
+        const double h = io.get_scalar("gridScale");
+        std::fill(hs.begin(), hs.end(), h);
+    }
+    for (int a = 0; a < ndim; ++a) {
+        if (!(hs[a] > 0)) throw Error(HFM_ERR_VALUE, "Parametrization error : gridscales should be positive");
         pm.dims[a] = p.dims[a] = dims[a];
         pm.origin[a] = origin[a];
-        pm.scale[a] = p.h[a] = h;
+        pm.scale[a] = p.h[a] = hs[a];
     }
-    p.kind = StencilKind::RiemannPerCell;
-    const int64_t N = (int64_t)dims[0] * dims[1];
-    std::vector<double> speed;
-    const char *key = io.has_field("speed") ? "speed" : "cost";
+    p.kind = StencilKind::SharedByTheta;
+    p.angular = false;
+    p.nfwd = 0;
+    p.nsym = ndim;
+    p.nclass = ndim == 3 ? dims[2] : 1;
+    p.cls_off.assign((size_t)p.nclass * ndim * 3, 0);
+    p.cls_w.assign((size_t)p.nclass * ndim, 0.0);
+    p.cls_enabled.assign((size_t)p.nclass * 2 * ndim, 1);
+    for (int c = 0; c < p.nclass; ++c)
+        for (int i = 0; i < ndim; ++i) {
+            p.cls_off[(c * ndim + i) * 3 + i] = 1;
+            p.cls_w[c * ndim + i] = 1. / (hs[i] * hs[i]);
+        }
+    const bool has_speed = io.has_field("speed");
+    const char *key = has_speed ? "speed" : "cost";
     const std::vector<int64_t> dd = io.field_domain_dims(key, 1);
-    Field f = io.get_field(key, dd.empty() ? 0 : 2, 1);
-    p.metric.resize(f.constant() ? 3 : N * 3);
-    p.metric_constant = f.constant();
-    const size_t nf = f.size();
-    for (size_t i = 0; i < nf; ++i) {
-        const double c = (std::string(key) == "speed") ? 1.0 / f.ptr()[i] : f.ptr()[i];
-        p.metric[3 * i] = c * c;
-        p.metric[3 * i + 1] = 0.0;
-        p.metric[3 * i + 2] = c * c;
+    Field f = io.get_field(key, dd.empty() ? 0 : ndim, 1);
+    if (!f.constant())
+        for (int a = 0; a < ndim; ++a)
+            if (f.dims[a] != dims[a]) throw Error(HFM_ERR_VALUE, std::string("Error : Field ") + key + " has inconsistent dimensions.");
+    p.mult_depth = f.constant() ? 0 : 3;
+    p.mult_inverse = !has_speed;
+    if (f.view) {
+        p.mult_ptr = f.view;
+    } else {
+        p.mult = std::move(f.data);
+        p.mult_ptr = nullptr;
     }
 }
 
@@ -545,7 +568,8 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     const bool lifted = model == "ReedsShepp2" || model == "Elastica2";
     if (model == "Riemann2") setup_riemann(io, 2, pm, p);
     else if (model == "Riemann3") setup_riemann(io, 3, pm, p);
-    else if (model == "Isotropic2") setup_isotropic2(io, pm, p);
+    else if (model == "Isotropic2") setup_isotropic(io, 2, pm, p);
+    else if (model == "Isotropic3") setup_isotropic(io, 3, pm, p);
     else if (lifted) setup_curvature(io, model, pm, p);
     else if (model == "TTI3") setup_tti(io, pm, p);
     else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);

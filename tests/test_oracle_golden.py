@@ -112,3 +112,23 @@ def test_forward_variation_oracle_matches_reference(name):
         assert np.max(np.abs(v - r)) <= 1e-14 * np.max(np.abs(r))
     else:
         np.testing.assert_array_equal(v, r)
+
+
+@pytest.mark.parametrize("name", ["iso2_40x36_walls", "iso3_14x12x10_walls"])
+def test_isotropic_oracle_matches_reference(name):
+    """Isotropic2 / Isotropic3 (one difference per axis, speed multiplier): values, activeNeighs,
+    costSensitivity, valueVariation, geodesics and flow bit for bit (points within 1e-15)."""
+    params, ref, _ = load_golden(name)
+    res = O.solve(params)
+    np.testing.assert_array_equal(res["values"], ref["values"])
+    np.testing.assert_array_equal(res["activeNeighs"].reshape(res["values"].shape).astype(float), ref["activeNeighs"])
+    assert res["nAccepted"] == int(ref["nAccepted"])
+    assert res["MaxStencilWidth"] == int(ref["MaxStencilWidth"])
+    sens, _, _ = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
+    np.testing.assert_array_equal(sens, ref["costSensitivity_0"])
+    np.testing.assert_array_equal(O.forward_variation(res, params), ref["valueVariation"])
+    geo = O.geodesics(res, params)
+    np.testing.assert_array_equal(geo["geodesicLengths"], ref["geodesicLengths"])
+    assert np.max(np.abs(geo["geodesicPoints"] - ref["geodesicPoints"])) <= 1e-15
+    fin = np.isfinite(ref["geodesicFlow"])
+    np.testing.assert_array_equal(O.geodesic_flow(res)[fin], ref["geodesicFlow"][fin])
