@@ -37,6 +37,9 @@ DEFAULT = {
     "Riemann3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
     "Riemann2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
     "Isotropic2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
+    "Isotropic3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
+    "Diagonal2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
+    "Diagonal3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
     "ReedsShepp2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
     "Elastica2": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
     "TTI3": {"tileSweeps": 1, "queue": ("band", 1.0, 4.0)},

@@ -722,6 +722,33 @@ __global__ void riemann_stencil_kernel(Dev<Real> P, const double *metric, int8_t
     }
 }
 
+// Diagonal2 / Diagonal3 (Headers/Specializations/Isotropic.h:61-115): one symmetric difference
+// per axis, weight baseWeight * speed_i^2 with baseWeight = 1 / h_i^2 (EulerianStencil.h:79-81), the
+// speed vector per cell (or the inverse of the cost vector, component-wise).
+template <typename Real>
+__global__ void diagonal_stencil_kernel(Dev<Real> P, int D, const double *speed, int8_t *plain_off, double *plain_w) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[R.i];
+    const double *src = speed + (I.metric0 + (I.metric_const ? 0 : R.xl)) * D;
+    for (int k = 0; k < D; ++k) {
+        double sp = src[k];
+        if (I.mult_inverse) sp = 1.0 / sp;
+        const double base = 1. / (I.h[k] * I.h[k]);
+        const double w = base * (sp * sp);
+        int o[3] = {0, 0, 0};
+        o[k] = 1;
+        P.code[k * P.ntc + R.c] = pack_off(o[0], o[1], o[2]);
+        P.weight[k * P.ntc + R.c] = (Real)w;
+        if (plain_off) {
+            for (int a = 0; a < 3; ++a) plain_off[(x * D + k) * 3 + a] = (int8_t)o[a];
+            plain_w[x * D + k] = w;
+        }
+        if (!(w >= 0.0) || !(w < Arith<double>::inf())) atomicOr(P.status, (unsigned)kErrSelling);
+    }
+}
+
 // One thread per cell: the TTI norm (tile-major) and the distinct offsets of its Selling path as
 // the cell's stencil slots (weight 1; unused slots weight 0), for the visibility and dependency
 // passes. Invalid norms set kErrSelling; paths with more than NSYM offsets kErrTableOverflow.
@@ -1960,7 +1987,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         weight.zero(s);
         P.code = code.get();
         P.weight = weight.get();
-        const int NS = KIND == kKindTTI ? 14 : p0.ndim * (p0.ndim + 1) / 2;
+        const int NS = KIND == kKindTTI ? 14 : p0.diagonal ? p0.ndim : p0.ndim * (p0.ndim + 1) / 2;
         const double *metric_ptr = nullptr;
         if (ninst == 1 && p0.d_metric) {
             metric_ptr = p0.d_metric;
@@ -1989,6 +2016,9 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             ttibuf.zero(s);
             P.tti = ttibuf.get();
             launch(tti_setup_kernel<NSYM, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr);
+        } else if (p0.diagonal) {
+            launch(diagonal_stencil_kernel<Real>, nblocks(N, 128), 128, 0, s, P, p0.ndim, metric_ptr, plain_off.get(),
+                   plain_w.get());
         } else if (p0.ndim == 2) {
             launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr, plain_off.get(),
                    plain_w.get());
@@ -2000,7 +2030,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_TRACE("stencil kernel");
         launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, P, maxw.get());
         maxw.download(hmaxw.data(), ninst, s);
-        if (ninst > 1 && p0.ordered) {
+        if (ninst > 1 && p0.ordered && !p0.diagonal) {
             kscale.alloc(ninst);
             kscale.zero(s);
             if (KIND == kKindTTI)
@@ -2395,13 +2425,24 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
     }
     const EulerProblem &p = *probs[0];
     for (const EulerProblem *q : probs) {
-        if (q->kind != p.kind || q->ndim != p.ndim || q->nfwd != p.nfwd || q->nsym != p.nsym || q->fp64 != p.fp64)
+        if (q->kind != p.kind || q->ndim != p.ndim || q->nfwd != p.nfwd || q->nsym != p.nsym || q->fp64 != p.fp64 ||
+            q->diagonal != p.diagonal)
             throw Error(HFM_ERR_VALUE, "a batch must hold instances of one model family and one precision");
     }
     if (p.kind == StencilKind::TTI) {
         if (p.ndim != 3 || !p.fp64 || p.nsym != kTTISlots)
             throw Error(HFM_ERR_UNSUPPORTED, "TTI3 is solved in FP64 on 3D grids");
         run_batch_impl<double, 0, kTTISlots, detail::kKindTTI>(probs, results);
+    } else if (p.kind == StencilKind::RiemannPerCell && p.diagonal) {
+        if (p.ndim == 2) {
+            if (p.fp64) run_batch_impl<double, 0, 2, detail::kKindRiemann>(probs, results);
+            else run_batch_impl<float, 0, 2, detail::kKindRiemann>(probs, results);
+        } else if (p.ndim == 3) {
+            if (p.fp64) run_batch_impl<double, 0, 3, detail::kKindRiemann>(probs, results);
+            else run_batch_impl<float, 0, 3, detail::kKindRiemann>(probs, results);
+        } else {
+            throw Error(HFM_ERR_UNSUPPORTED, "Diagonal models support dimensions 2 and 3");
+        }
     } else if (p.kind == StencilKind::RiemannPerCell) {
         if (p.ndim == 2) {
             if (p.fp64) run_batch_impl<double, 0, 3, detail::kKindRiemann>(probs, results);

@@ -376,6 +376,48 @@ void setup_isotropic(Store &io, int ndim, Param &pm, EulerProblem &p) {
     }
 }
 
+// Diagonal2 / Diagonal3 (Headers/Specializations/Isotropic.h:61-115): a speed (or cost) vector
+// per point, one symmetric difference per axis of weight speed_i^2 / h_i^2.
+void setup_diagonal(Store &io, int ndim, Param &pm, EulerProblem &p) {
+    const std::vector<int> dims = read_dims(io, ndim);
+    pm.ndim = ndim;
+    p.ndim = ndim;
+    const std::vector<double> origin = read_point(io, "origin", ndim, std::vector<double>(ndim, 0.0));
+    std::vector<double> hs(ndim);
+    if (io.has_field("gridScales")) {
+        hs = read_point(io, "gridScales", ndim, hs);
+    } else {
+        const double h = io.get_scalar("gridScale");
+        std::fill(hs.begin(), hs.end(), h);
+    }
+    for (int a = 0; a < ndim; ++a) {
+        if (!(hs[a] > 0)) throw Error(HFM_ERR_VALUE, "Parametrization error : gridscales should be positive");
+        pm.dims[a] = p.dims[a] = dims[a];
+        pm.origin[a] = origin[a];
+        pm.scale[a] = p.h[a] = hs[a];
+    }
+    p.kind = StencilKind::RiemannPerCell;
+    p.diagonal = true;
+    const bool has_speed = io.has_field("speed");
+    const std::string key = has_speed ? "speed" : "cost";
+    const std::vector<int64_t> dd = io.field_domain_dims(key, ndim);
+    Field f = io.get_field(key, dd.empty() ? 0 : ndim, ndim);
+    if (!f.constant())
+        for (int a = 0; a < ndim; ++a)
+            if (f.dims[a] != dims[a]) throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+    p.metric_constant = f.constant();
+    p.mult_inverse = !has_speed;
+    if (f.view) {
+        p.metric_ptr = f.view;
+        p.metric_len = f.size();
+    } else {
+        p.metric = std::move(f.data);
+    }
+    // the reference's first variation of these models is per axis (a vector multiplier)
+    if (io.has_field("inspectSensitivity") || io.has_field("costVariation"))
+        throw Error(HFM_ERR_UNSUPPORTED, "first variations of the Diagonal models are not supported by the GPU solve path");
+}
+
 void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProblem &p) {
     const std::vector<int> dims = read_dims(io, 3);
     pm.ndim = 3;
@@ -570,6 +612,8 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     else if (model == "Riemann3") setup_riemann(io, 3, pm, p);
     else if (model == "Isotropic2") setup_isotropic(io, 2, pm, p);
     else if (model == "Isotropic3") setup_isotropic(io, 3, pm, p);
+    else if (model == "Diagonal2") setup_diagonal(io, 2, pm, p);
+    else if (model == "Diagonal3") setup_diagonal(io, 3, pm, p);
     else if (lifted) setup_curvature(io, model, pm, p);
     else if (model == "TTI3") setup_tti(io, pm, p);
     else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);
@@ -945,7 +989,7 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
             for (int j = i + 1; j < n; ++j) {
                 if (rc[j] != HFM_OK || done[j] || qs[j]->skip) continue;
                 const hfm::EulerProblem &pj = qs[j]->p;
-                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && pj.kind == pi.kind && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
+                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && pj.kind == pi.kind && pj.diagonal == pi.diagonal && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
                     pj.nsym == pi.nsym && pj.fp64 == pi.fp64 && pj.sweeps_per_tile == pi.sweeps_per_tile &&
                     pj.max_rounds == pi.max_rounds) {
                     grp.push_back(j);

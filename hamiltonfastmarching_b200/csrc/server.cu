@@ -62,8 +62,10 @@ size_t estimate_bytes(const hfm::Store &st) {
     const size_t r = fp64 ? 8 : 4;
     size_t per_cell;
     if (model == "Riemann3") per_cell = 48 + 6 * (4 + r) + r + 8 + 8 + 16;
-    else if (model == "Riemann2" || model == "Isotropic2") per_cell = 24 + 3 * (4 + r) + r + 8 + 8 + 16;
-    else per_cell = 4 + r + r + 8 + 8 + 16;  // lifted models: visibility, multiplier, values
+    else if (model == "Riemann2") per_cell = 24 + 3 * (4 + r) + r + 8 + 8 + 16;
+    else if (model == "Diagonal2" || model == "Diagonal3") per_cell = 24 + 3 * (4 + r) + r + 8 + 8 + 16;
+    else if (model == "TTI3") per_cell = 112 + 200 + r + 8 + 8 + 16;
+    else per_cell = 4 + r + r + 8 + 8 + 16;  // shared stencils: visibility, multiplier, values
     return cells * per_cell + (size_t(4) << 20);
 }
 

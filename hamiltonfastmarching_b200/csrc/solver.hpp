@@ -35,6 +35,9 @@ struct EulerProblem {
     size_t metric_len = 0;
     bool metric_constant = false;
     bool dual = false;
+    // Diagonal2/3: `metric` holds ndim speeds (or costs, mult_inverse) per cell instead of a
+    // packed matrix; the stencil is one symmetric difference per axis.
+    bool diagonal = false;
     double h[3] = {1, 1, 1};
 
     // SharedByTheta: nclass stencils of nfwd forward + nsym symmetric differences, one per index of

@@ -209,6 +209,28 @@ class Problem:
                 sp = 1.0 / np.asarray(params["cost"], float)
             mult = np.ascontiguousarray(np.broadcast_to(sp, dims), dtype=np.float64)
             adim = lambda p: (np.asarray(p, float) - origin) / hs
+        elif model in ("Diagonal2", "Diagonal3"):
+            # one symmetric difference per axis, weight (1/h_i^2) * speed_i^2 per cell
+            # (Headers/Specializations/Isotropic.h:61-115, EulerianStencil.h:79-81)
+            origin = np.asarray(_get(params, "origin", np.zeros(ndim)), float)
+            if "gridScales" in params:
+                hs = np.asarray(params["gridScales"], float).ravel()
+            else:
+                hs = np.full(ndim, float(params["gridScale"]))
+            scale = hs
+            if "speed" in params:
+                sp = np.asarray(params["speed"], float)
+            else:
+                sp = 1.0 / np.asarray(params["cost"], float)
+            sp = np.broadcast_to(sp, dims + (ndim,)).reshape(-1, ndim)
+            n = sp.shape[0]
+            off = np.zeros((n, ndim, 3), np.int8)
+            w = np.zeros((n, ndim))
+            for i in range(ndim):
+                off[:, i, i] = 1
+                w[:, i] = (1.0 / (hs[i] * hs[i])) * (sp[:, i] * sp[:, i])
+            nfwd, nsym, share = 0, ndim, 0
+            adim = lambda p: (np.asarray(p, float) - origin) / hs
         elif model in ("Riemann2", "Riemann3"):
             origin = np.asarray(_get(params, "origin", np.zeros(ndim)), float)
             if "gridScales" in params:

@@ -206,8 +206,8 @@ def variation_fixtures():
 
 
 def isotropic_fixtures():
-    """Isotropic2 / Isotropic3 with walls, two seeds, distinct grid scales: values, activeNeighs,
-    costSensitivity, valueVariation, geodesics and the geodesic flow."""
+    """Isotropic2 / Isotropic3 and Diagonal2 / Diagonal3 with walls, two seeds, distinct grid scales:
+    values, activeNeighs, costSensitivity (isotropic), valueVariation, geodesics and the geodesic flow."""
     rng = np.random.default_rng(2026)
     for model, dims, name in (("Isotropic2", (40, 36), "iso2_40x36_walls"), ("Isotropic3", (14, 12, 10), "iso3_14x12x10_walls")):
         nd = len(dims)
@@ -219,6 +219,17 @@ def isotropic_fixtures():
              "costVariation": rng.standard_normal(dims + (2,)), "tips": rng.uniform(0.0, 0.3, (3, nd)),
              "exportGeodesicFlow": 1.0, "exportValues": 1.0}
         solve_fixture(name, p, (rng.uniform(0.05, 0.25, (3, nd)), np.array([1.0, 2.0, 0.5])))
+    # Diagonal2 / Diagonal3: a speed vector per point (no first variation of the multiplier here)
+    for model, dims, name in (("Diagonal2", (40, 36), "diag2_40x36_walls"), ("Diagonal3", (14, 12, 10), "diag3_14x12x10_walls")):
+        nd = len(dims)
+        walls = np.zeros(dims)
+        walls[dims[0] // 2, 2:] = 1.0
+        p = {"model": model, "arrayOrdering": "RowMajor", "dims": np.array(dims, float),
+             "gridScales": np.linspace(0.02, 0.03, nd), "speed": 0.5 + rng.random(dims + (nd,)), "walls": walls,
+             "seeds": np.array([[0.3] * nd, [0.1] * nd]), "seedValues": np.array([0.0, 0.05]),
+             "seedValueVariation": rng.standard_normal((2, 2)), "tips": rng.uniform(0.0, 0.3, (3, nd)),
+             "exportGeodesicFlow": 1.0, "exportValues": 1.0}
+        solve_fixture(name, p)
 
 
 if __name__ == "__main__":

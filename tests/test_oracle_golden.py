@@ -114,18 +114,21 @@ def test_forward_variation_oracle_matches_reference(name):
         np.testing.assert_array_equal(v, r)
 
 
-@pytest.mark.parametrize("name", ["iso2_40x36_walls", "iso3_14x12x10_walls"])
+@pytest.mark.parametrize("name", ["iso2_40x36_walls", "iso3_14x12x10_walls", "diag2_40x36_walls",
+                                  "diag3_14x12x10_walls"])
 def test_isotropic_oracle_matches_reference(name):
-    """Isotropic2 / Isotropic3 (one difference per axis, speed multiplier): values, activeNeighs,
-    costSensitivity, valueVariation, geodesics and flow bit for bit (points within 1e-15)."""
+    """Isotropic2/3 (one difference per axis, speed multiplier) and Diagonal2/3 (a speed per axis):
+    values, activeNeighs, costSensitivity, valueVariation, geodesics and flow bit for bit (points
+    within 1e-15)."""
     params, ref, _ = load_golden(name)
     res = O.solve(params)
     np.testing.assert_array_equal(res["values"], ref["values"])
     np.testing.assert_array_equal(res["activeNeighs"].reshape(res["values"].shape).astype(float), ref["activeNeighs"])
     assert res["nAccepted"] == int(ref["nAccepted"])
     assert res["MaxStencilWidth"] == int(ref["MaxStencilWidth"])
-    sens, _, _ = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
-    np.testing.assert_array_equal(sens, ref["costSensitivity_0"])
+    if "inspectSensitivity" in params:
+        sens, _, _ = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
+        np.testing.assert_array_equal(sens, ref["costSensitivity_0"])
     np.testing.assert_array_equal(O.forward_variation(res, params), ref["valueVariation"])
     geo = O.geodesics(res, params)
     np.testing.assert_array_equal(geo["geodesicLengths"], ref["geodesicLengths"])
