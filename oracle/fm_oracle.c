@@ -1224,7 +1224,7 @@ done:
 /* _HopfLaxRecompute at the stored extremum t (TTI.hpp:278-389, order 1): Riemannian update of the
  * Selling decomposition at t, its value and the discrete flow (offset * sign, (sol - v) w). */
 static double tti_recompute(const tti_norm *n, const int64_t *dims, const double *values, int64_t x, double t,
-                            int64_t *nb, double *nbw, int *nn) {
+                            int64_t *nb, double *nbw, int *nn, double *width) {
     tti_path P;
     *nn = 0;
     if (tti_path_init(n, t, &P)) return FMO_INF;
@@ -1268,15 +1268,19 @@ static double tti_recompute(const tti_norm *n, const int64_t *dims, const double
         const double delta = b * b - a * c;
         sol = (b + sqrt(delta)) / a;
     }
+    double wsum = 0.0, wd = 0.0;
     for (int q = 0; q < r; ++q) {
         const int i = idx[q];
         const double v = val[i] - valMin;
         const double w0 = (1 - t) * P.w0[i] + t * P.w1[i];
         const double d = (sol - v) * w0;
+        wsum += w0;
         nb[*nn] = cell[i];
         nbw[*nn] = d > 0 ? d : 0.0;
+        wd += nbw[*nn];
         ++*nn;
     }
+    if (width) *width = wd / wsum;  /* TTI.hpp:372-388 */
     return sol + valMin;
 }
 
@@ -1313,7 +1317,7 @@ int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const d
         if (t_active[x] < FMO_INF) {
             tti_norm n;
             if (tti_setup(metric + 14 * x, h, &n)) { nn = 0; }
-            else rec = tti_recompute(&n, dims, values, x, fabs(t_active[x]), nb, nbw, &nn);
+            else rec = tti_recompute(&n, dims, values, x, fabs(t_active[x]), nb, nbw, &nn, NULL);
         }
         double ws = 0.0;
         for (int j = 0; j < nn; ++j) ws += nbw[j];
@@ -1433,7 +1437,7 @@ static int tti_flow(void *vctx, int64_t x, int (*off)[3], double *fw, double *va
     int64_t nb[6];
     double nbw[6];
     int nn = 0;
-    *value = tti_recompute(&nm, T->dims, T->values, x, fabs(T->t_active[x]), nb, nbw, &nn);
+    *value = tti_recompute(&nm, T->dims, T->values, x, fabs(T->t_active[x]), nb, nbw, &nn, width);
     const int64_t n1 = T->dims[1], n2 = T->dims[2];
     const int64_t x0 = x / (n1 * n2), x1 = (x / n2) % n1, x2 = x % n2;
     for (int j = 0; j < nn; ++j) {
@@ -1773,7 +1777,7 @@ int fmo_tti_forward_variation(const int64_t *dims, const double *h, const double
         double rec = values[x];
         if (t_active[x] < FMO_INF) {
             tti_norm n;
-            if (!tti_setup(metric + 14 * x, h, &n)) rec = tti_recompute(&n, dims, values, x, fabs(t_active[x]), nb, nbw, &nn);
+            if (!tti_setup(metric + 14 * x, h, &n)) rec = tti_recompute(&n, dims, values, x, fabs(t_active[x]), nb, nbw, &nn, NULL);
         }
         double ws = 0.0;
         for (int j = 0; j < nn; ++j) ws += nbw[j];
@@ -1791,4 +1795,225 @@ int fmo_tti_forward_variation(const int64_t *dims, const double *h, const double
     }
     free(order);
     return 0;
+}
+
+/* ========================================================================================== */
+/* ODE geodesic solver (Headers/Base/Implementation/GeodesicODESolver.hxx): a midpoint scheme on
+ * the geodesic flow interpolated from the 2^D cells around the point, stopping when the L-infinity
+ * distance to the seeds (capped at 6) stops decreasing, or failing when a cell is revisited too
+ * often (stationarity). For unit offsets the wall test of VisibleOffset reduces to "the target is
+ * not a wall" (WallObstructionTest.h:95-150 with vMax = 1). */
+
+typedef struct { int64_t key; int count; double flow[3], value, width; } ode_slot;
+typedef struct { ode_slot *a; int64_t cap, n; } ode_map;
+
+static ode_slot *ode_find(ode_map *m, int64_t key, int *fresh) {
+    if (2 * (m->n + 1) > m->cap) {
+        const int64_t nc = m->cap ? 2 * m->cap : 1024;
+        ode_slot *na = (ode_slot *)malloc((size_t)nc * sizeof(ode_slot));
+        if (!na) return NULL;
+        for (int64_t i = 0; i < nc; ++i) na[i].key = -1;
+        for (int64_t i = 0; i < m->cap; ++i) {
+            if (m->a[i].key < 0) continue;
+            int64_t h = (m->a[i].key * 0x9E3779B97F4A7C15ULL) & (nc - 1);
+            while (na[h].key >= 0) h = (h + 1) & (nc - 1);
+            na[h] = m->a[i];
+        }
+        free(m->a);
+        m->a = na;
+        m->cap = nc;
+    }
+    int64_t h = (key * 0x9E3779B97F4A7C15ULL) & (m->cap - 1);
+    while (m->a[h].key >= 0 && m->a[h].key != key) h = (h + 1) & (m->cap - 1);
+    *fresh = m->a[h].key < 0;
+    if (*fresh) { m->a[h].key = key; m->a[h].count = 0; ++m->n; }
+    return &m->a[h];
+}
+
+/* LInfDistance (GeodesicODESolver.hxx:225-258): breadth-first distance over the 3^D - 1 neighbours
+ * through visible offsets, capped: cells at the cap are reached but not expanded. */
+static int16_t *linf_distance(const fmo_problem *p, const int64_t *seeds, int nseeds, int cap) {
+    const int64_t N = ncells(p);
+    int16_t *d = (int16_t *)malloc((size_t)N * sizeof(int16_t));
+    int64_t *q = (int64_t *)malloc((size_t)N * sizeof(int64_t));
+    if (!d || !q) { free(d); free(q); return NULL; }
+    for (int64_t x = 0; x < N; ++x) d[x] = 32767;
+    int64_t head = 0, tail = 0;
+    for (int s = 0; s < nseeds; ++s) {
+        if (d[seeds[s]] != 0) { d[seeds[s]] = 0; q[tail++] = seeds[s]; }
+    }
+    int64_t idx[3], nb[3];
+    const int D = p->ndim;
+    while (head < tail) {
+        const int64_t x = q[head++];
+        if (d[x] >= cap) continue;
+        index_of(p, x, idx);
+        int n3 = 1;
+        for (int a = 0; a < D; ++a) n3 *= 3;
+        for (int c = 0; c < n3; ++c) {
+            int cc = c, zero = 1;
+            for (int a = 0; a < D; ++a) { const int o = cc % 3 - 1; cc /= 3; nb[a] = idx[a] + o; zero &= o == 0; }
+            if (zero || !periodize(p, nb)) continue;
+            const int64_t y = linear_of(p, nb);
+            if (p->walls && p->walls[y]) continue;
+            if (d[y] <= d[x] + 1) continue;
+            d[y] = (int16_t)(d[x] + 1);
+            q[tail++] = y;
+        }
+    }
+    free(q);
+    return d;
+}
+
+typedef struct { double flow[3]; int nstat, tol; } ode_flow;
+
+static int ode_flow_at(const fmo_problem *p, geo_flow_fn flow, void *ctx, const int16_t *target, ode_map *cache,
+                       double causality, const double *pt, ode_flow *out) {
+    const int D = p->ndim;
+    int64_t pi[3] = {0, 0, 0};
+    double w[3] = {0, 0, 0};
+    int sg[3] = {0, 0, 0};
+    for (int j = 0; j < D; ++j) {
+        pi[j] = (int64_t)floor(pt[j]);
+        w[j] = pt[j] - (double)pi[j] - 0.5;
+        sg[j] = w[j] > 0 ? 1 : -1;
+        w[j] = fabs(w[j]);
+    }
+    ode_slot *slots[8];
+    double wt[8];
+    int mintol = 2147483647, maxstat = 0;
+    for (int i = 0; i < (1 << D); ++i) {
+        slots[i] = NULL;
+        wt[i] = 0.0;
+        int64_t q[3] = {0, 0, 0};
+        for (int j = 0; j < D; ++j) q[j] = pi[j] + (((i >> j) & 1) ? sg[j] : 0);
+        if (!periodize(p, q)) continue;
+        const int64_t y = linear_of(p, q);
+        if (p->walls && p->walls[y]) continue;
+        if (target[y] < mintol) mintol = target[y];
+        int fresh = 0;
+        ode_slot *s = ode_find(cache, y, &fresh);
+        if (!s) return -1;
+        if (fresh) {
+            int off[GEO_MAXF][3];
+            double fw[GEO_MAXF];
+            const int nf = flow(ctx, y, off, fw, &s->value, &s->width);
+            for (int a = 0; a < 3; ++a) {
+                double acc = 0.0;
+                for (int f = 0; f < nf; ++f) acc += fw[f] * (double)off[f][a];
+                s->flow[a] = acc;
+            }
+        }
+        double weight = 1;
+        for (int j = 0; j < D; ++j) weight *= ((i >> j) & 1) ? w[j] : (1 - w[j]);
+        slots[i] = s;
+        wt[i] = weight;
+        if (s->count > maxstat) maxstat = s->count;
+        ++s->count;
+    }
+    out->nstat = maxstat;
+    out->tol = mintol;
+    out->flow[0] = out->flow[1] = out->flow[2] = 0.0;
+    double minVal = FMO_INF;
+    int imin = -1;
+    for (int i = 0; i < (1 << D); ++i)
+        if (wt[i] > 0 && slots[i]->value < minVal) { minVal = slots[i]->value; imin = i; }
+    if (minVal == FMO_INF) return 0;
+    const double thr = minVal + causality * slots[imin]->width;
+    double ws = 0.0;
+    for (int i = 0; i < (1 << D); ++i) {
+        if (wt[i] <= 0) continue;
+        if (slots[i]->value <= thr) {
+            ws += wt[i];
+            for (int a = 0; a < D; ++a) out->flow[a] += wt[i] * slots[i]->flow[a];
+        }
+    }
+    if (ws > 0)
+        for (int a = 0; a < D; ++a) out->flow[a] /= ws;
+    return 0;
+}
+
+/* Run (GeodesicODESolver.hxx:159-212) for one tip; returns 0 (reached the seeds or a seed), 1
+ * (stalled: the reference's failure), -1 on allocation failure, -2 if the output is full. */
+static int ode_run(const fmo_problem *p, geo_flow_fn flow, void *ctx, const int16_t *target, double step,
+                   double causality, double *pts, int64_t cap, int64_t *len) {
+    const int D = p->ndim;
+    ode_map cache = {NULL, 0, 0};
+    const int nstat_max = (int)(6 * sqrt((double)D) / step);
+    int nh = 0;
+    for (int i = 0; i < sqrt((double)D) / step; ++i) ++nh;
+    int *hist = (int *)malloc((size_t)(nh > 0 ? nh : 1) * sizeof(int));
+    if (!hist) return -1;
+    for (int i = 0; i < nh; ++i) hist[i] = 2147483647;
+    int head = 0, ret = 0;
+    for (;;) {
+        const double *pt = pts + (*len - 1) * D;
+        ode_flow fd;
+        if (ode_flow_at(p, flow, ctx, target, &cache, causality, pt, &fd)) { ret = -1; break; }
+        int old = 2147483647;
+        if (nh > 0) { old = hist[head]; hist[head] = fd.tol; head = (head + 1) % nh; }
+        else old = fd.tol;  /* an empty history compares the front of the pushed value */
+        if (old < fd.tol) break;
+        if (fd.nstat > nstat_max) { ret = 1; break; }
+        double nrm = 0.0;
+        for (int a = 0; a < D; ++a) nrm += fd.flow[a] * fd.flow[a];
+        nrm = sqrt(nrm);
+        if (nrm == 0) break;
+        double q[3];
+        for (int a = 0; a < D; ++a) q[a] = pt[a] + 0.5 * step * fd.flow[a] / nrm;
+        if (ode_flow_at(p, flow, ctx, target, &cache, causality, q, &fd)) { ret = -1; break; }
+        nrm = 0.0;
+        for (int a = 0; a < D; ++a) nrm += fd.flow[a] * fd.flow[a];
+        nrm = sqrt(nrm);
+        if (nrm == 0) break;
+        if (*len >= cap) { ret = -2; break; }
+        for (int a = 0; a < D; ++a) pts[*len * D + a] = pt[a] + step * fd.flow[a] / nrm;
+        ++*len;
+    }
+    free(hist);
+    free(cache.a);
+    return ret;
+}
+
+static int64_t ode_all(const fmo_problem *grid, geo_flow_fn flow, void *ctx, const int64_t *seeds, int nseeds,
+                       int ntips, const double *tips, double step, double causality, int64_t max_points,
+                       double *points, int64_t *lengths, int *failed) {
+    const int D = grid->ndim;
+    int16_t *target = linf_distance(grid, seeds, nseeds, 6);
+    if (!target) return -1;
+    int64_t total = 0;
+    for (int t = 0; t < ntips; ++t) {
+        if (total >= max_points) { free(target); return -2; }
+        double *pts = points + total * D;
+        for (int a = 0; a < D; ++a) pts[a] = tips[(int64_t)t * D + a];
+        int64_t len = 1;
+        const int r = ode_run(grid, flow, ctx, target, step, causality, pts, max_points - total, &len);
+        if (r == -1 || r == -2) { free(target); return r; }
+        lengths[t] = len;
+        failed[t] = r == 1;
+        total += len;
+    }
+    free(target);
+    return total;
+}
+
+int64_t fmo_geodesic_ode(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
+                         const double *tips, double step, double causality, int64_t max_points, double *points,
+                         int64_t *lengths, int *failed) {
+    eul_ctx E = {p, values, active};
+    return ode_all(p, eul_recompute, &E, p->seed_index, p->nseeds, ntips, tips, step, causality, max_points, points,
+                   lengths, failed);
+}
+
+int64_t fmo_tti_geodesic_ode(const int64_t *dims, const double *h, const double *metric, const double *values,
+                             const double *t_active, int nseeds, const int64_t *seed_index, int ntips,
+                             const double *tips, double step, double causality, int64_t max_points, double *points,
+                             int64_t *lengths, int *failed) {
+    fmo_problem g;
+    memset(&g, 0, sizeof(g));
+    g.ndim = 3;
+    for (int a = 0; a < 3; ++a) g.dims[a] = dims[a];
+    tti_ctx T = {dims, h, metric, values, t_active};
+    return ode_all(&g, tti_flow, &T, seed_index, nseeds, ntips, tips, step, causality, max_points, points, lengths,
+                   failed);
 }

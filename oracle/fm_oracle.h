@@ -107,6 +107,17 @@ int fmo_forward_variation(const fmo_problem *p, const double *values, const uint
                           const double *cost_var, double *result);
 int fmo_tti_forward_variation(const int64_t *dims, const double *h, const double *metric, const double *values,
                               const double *t_active, int nvar, const double *cost_var, double *result);
+/* ODE geodesic solver (midpoint scheme on the interpolated flow) from the same inputs as
+ * fmo_geodesic_discrete; causality = geodesicCausalityTolerance. failed[t] = 1 where the solver
+ * stalled. Returns the total number of points, -1 on allocation failure, -2 if max_points is too
+ * small. The TTI variant takes the seed cells explicitly. */
+int64_t fmo_geodesic_ode(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
+                         const double *tips, double step, double causality, int64_t max_points, double *points,
+                         int64_t *lengths, int *failed);
+int64_t fmo_tti_geodesic_ode(const int64_t *dims, const double *h, const double *metric, const double *values,
+                             const double *t_active, int nseeds, const int64_t *seed_index, int ntips,
+                             const double *tips, double step, double causality, int64_t max_points, double *points,
+                             int64_t *lengths, int *failed);
 int fmo_tti_geodesic_flow(const int64_t *dims, const double *h, const double *metric, const double *values,
                           const double *t_active, double *flow, double *value, double *width);
 

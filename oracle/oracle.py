@@ -84,6 +84,12 @@ def lib():
         L.fmo_tti_geodesic_discrete.restype = ctypes.c_int64
         L.fmo_geodesic_flow.argtypes = [ctypes.POINTER(_Problem), _P, _P, _P, _P, _P]
         L.fmo_forward_variation.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, _P]
+        L.fmo_geodesic_ode.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int64, _P, _P, _P]
+        L.fmo_geodesic_ode.restype = ctypes.c_int64
+        L.fmo_tti_geodesic_ode.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int64, _P, _P, _P]
+        L.fmo_tti_geodesic_ode.restype = ctypes.c_int64
         L.fmo_tti_forward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P]
         L.fmo_tti_geodesic_flow.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
         _lib = L
@@ -461,7 +467,8 @@ def _run_discrete(fn, args, tips, step, thr, vb, ndim):
         pts = np.empty((cap, ndim))
         lens = np.zeros(len(tips), np.int64)
         failed = np.zeros(len(tips), np.int32)
-        n = fn(*args, len(tips), _ptr(tips), step, thr, vb, cap, _ptr(pts), _ptr(lens), _ptr(failed))
+        extra = (step, thr) if vb is None else (step, thr, vb)
+        n = fn(*args, len(tips), _ptr(tips), *extra, cap, _ptr(pts), _ptr(lens), _ptr(failed))
         if n == -2:
             cap *= 4
             continue
@@ -488,6 +495,17 @@ def geodesics(res: Dict, params: Dict) -> Dict:
         values = np.ascontiguousarray(res["values"].ravel())
         fn, args = lib().fmo_geodesic_discrete, (ctypes.byref(P.struct), _ptr(values), _ptr(res["activeNeighs"]))
     step, thr, vb = _geo_params(params, ndim)
+    if params.get("geodesicSolver", "Discrete") == "ODE":
+        # GeodesicODESolver.hxx:17-23: geodesicStep, geodesicCausalityTolerance (the target
+        # tolerance of 6 is fixed when the solver is built, before the keys are read)
+        caus = float(_get(params, "geodesicCausalityTolerance", 4.0))
+        if "_tti" in res:
+            sidx, _ = _seed_indices(params, adim, dims, [0, 0, 0])
+            sidx = np.ascontiguousarray(sidx, np.int64)
+            fn, args = lib().fmo_tti_geodesic_ode, args + (len(sidx), _ptr(sidx))
+        else:
+            fn = lib().fmo_geodesic_ode
+        thr, vb = caus, None
     groups = []
     if "tips" in params:
         groups.append(("", np.array([adim(p) for p in np.atleast_2d(np.asarray(params["tips"], float))])))

@@ -183,6 +183,39 @@ def geodesic_fixtures():
     solve_fixture("geo_tti3_12", p)
 
 
+def ode_fixtures():
+    """ODE geodesic solver (geodesicSolver = 'ODE') on every family; one Riemann3 tip stalls (the
+    reference's failure message)."""
+    rng = np.random.default_rng(1)
+    n = 48
+    m = np.zeros((n, n, 3))
+    m[..., 0] = 1 + rng.random((n, n))
+    m[..., 2] = 1 + rng.random((n, n))
+    m[..., 1] = 0.4 * (rng.random((n, n)) - 0.5)
+    walls = np.zeros((n, n))
+    walls[20, 5:40] = 1.0
+    tips = rng.random((6, 2))
+    solve_fixture("ode_riemann2_48_walls", {"model": "Riemann2", "arrayOrdering": "RowMajor", "dims": np.array([n, n], float),
+                                            "gridScale": 1.0 / n, "metric": m, "seeds": np.array([[0.5, 0.3]]),
+                                            "tips": tips, "walls": walls, "geodesicSolver": "ODE"})
+    rng.random((n, n))  # keeps the generator sequence of the fixtures below
+    p = W.riemann3_case(16, n_spheres=3, n_seeds=2, rmin=0.1, rmax=0.2, seed=22)
+    p["tips"] = rng.uniform(0.05, 0.95, (4, 3))
+    p["geodesicSolver"] = "ODE"
+    solve_fixture("ode_riemann3_16_walls", p)
+    for model, name in (("ReedsShepp2", "ode_reedsshepp2_24x16"), ("Elastica2", "ode_elastica2_24x16")):
+        p = W.curvature2_case(24, 16, model, seed=23, n_curves=4)
+        p["tips"] = np.c_[rng.uniform(0.1, 0.9, (3, 2)), rng.uniform(0, 6.2, (3, 1))]
+        p["tips_Unoriented"] = rng.uniform(0.1, 0.9, (3, 2))
+        p["geodesicSolver"] = "ODE"
+        solve_fixture(name, p)
+    p = W.tti3_case(12, h=0.01, seed=24)
+    p.pop("_vp")
+    p["tips"] = np.c_[rng.uniform(0.0, 0.12, (3, 2)), rng.uniform(0.03, 0.12, (3, 1))]
+    p["geodesicSolver"] = "ODE"
+    solve_fixture("ode_tti3_12", p)
+
+
 def variation_fixtures():
     """Forward first variation (costVariation, seedValueVariation -> valueVariation)."""
     rng = np.random.default_rng(2025)
@@ -233,7 +266,7 @@ def isotropic_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic|ode` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
@@ -242,9 +275,12 @@ if __name__ == "__main__":
         variation_fixtures()
     elif sys.argv[1:] == ["isotropic"]:
         isotropic_fixtures()
+    elif sys.argv[1:] == ["ode"]:
+        ode_fixtures()
     else:
         main()
         tti_fixtures()
         geodesic_fixtures()
         variation_fixtures()
         isotropic_fixtures()
+        ode_fixtures()

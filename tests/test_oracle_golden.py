@@ -72,14 +72,15 @@ def test_tti_oracle_matches_reference():
 
 
 GOLDEN_GEODESICS = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
-                    "geo_tti3_12"]
+                    "geo_tti3_12", "ode_riemann2_48_walls", "ode_riemann3_16_walls", "ode_reedsshepp2_24x16",
+                    "ode_elastica2_24x16", "ode_tti3_12"]
 
 
 @pytest.mark.parametrize("name", GOLDEN_GEODESICS)
 def test_geodesic_oracle_matches_reference(name):
-    """Discrete geodesics (tips, tips_Unoriented) and the geodesic flow of the oracle against the
-    reference executable: same lengths, points within 1e-12 (relative to the domain size), flow
-    within 1e-12 of its largest entry."""
+    """Geodesics (discrete and ODE solvers; tips, tips_Unoriented) and the geodesic flow of the
+    oracle against the reference executable: same lengths, points within 1e-12 (relative to the
+    domain size), flow within 1e-12 of its largest entry."""
     params, ref, _ = load_golden(name)
     res = O.tti_solve(params) if params["model"] == "TTI3" else O.solve(params)
     geo = O.geodesics(res, params)
@@ -89,7 +90,10 @@ def test_geodesic_oracle_matches_reference(name):
         np.testing.assert_array_equal(geo["geodesicLengths" + suffix], ref["geodesicLengths" + suffix])
         scale = np.max(np.abs(ref["geodesicPoints" + suffix]))
         assert np.max(np.abs(geo["geodesicPoints" + suffix] - ref["geodesicPoints" + suffix])) <= 1e-12 * scale
-        assert not geo["geodesicFailed" + suffix].any()
+        if name != "ode_riemann3_16_walls":  # its last tip stalls, for the reference too
+            assert not geo["geodesicFailed" + suffix].any()
+    if "geodesicFlow" not in ref:
+        return
     flow, rflow = O.geodesic_flow(res), ref["geodesicFlow"]
     fin = np.isfinite(rflow)
     assert np.array_equal(fin, np.isfinite(flow))
