@@ -2381,7 +2381,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     HFM_CUDA(cudaStreamSynchronize(s));
     HFM_TRACE("outputs");
-    run_geodesics<Real, NFWD, NSYM, KIND>(P, hinst, probs, results, s);
+    run_geodesics<Real, NFWD, NSYM, KIND>(P, hinst, probs, results, any_walls ? wd8.get() : nullptr, s);
     HFM_TRACE("geodesics");
     if (ninst == 1 && (!p0.adjoint_index.empty() || p0.fwd_nvar > 0)) {
         tm.start(s);

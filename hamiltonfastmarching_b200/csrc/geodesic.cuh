@@ -31,11 +31,16 @@ enum : int {
 struct GeoTip {
     double p[3];        // dimensionless tip (cell i spans [i, i+1)); unoriented: (x, y) only
     double step, thr, vbound;  // geodesicStep, geodesicWeightThreshold, geodesicVolumeBound
+    double causality;   // geodesicCausalityTolerance (ODE solver)
     long long out0;     // first point slot of this tip in the output
     int inst;           // instance of the batch
     int cap;            // output capacity in points
     int ndim;           // model dimension (2 or 3)
     int unoriented;     // choose the angle of smallest value (tips_Unoriented)
+    int ode;            // geodesicSolver 'ODE' instead of 'Discrete'
+    int nstat_max;      // ODE: stationarity limit, int(6 sqrt(D) / step)
+    int nhist;          // ODE: length of the target-distance history, ceil(sqrt(D) / step)
+    int table_log2;     // ODE: log2 of the per-tip visit-count table
 };
 
 struct GeoOut {
@@ -141,14 +146,18 @@ __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1,
             if (a <= 100 * fabs(cc) * 2.220446049250313e-16) continue;
             sol = A::div(A::add(b, A::sqrt(A::sub(A::mul(b, b), A::mul(a, cc)))), a);
         }
+        double wsum = 0.0, wid = 0.0;
         for (int q = 0; q < r; ++q) {
             const double v = A::sub(cand[q].v, vmin);
             const double w0 = A::add(A::mul(A::sub(1.0, ta), cand[q].wa), A::mul(ta, cand[q].wb));
             const double d = A::mul(A::sub(sol, v), w0);
             foff[q] = cand[q].off;
             fw[q] = d > 0 ? d : 0.0;
+            wsum = A::add(wsum, w0);
+            wid = A::add(wid, fw[q]);
         }
         *value = A::add(sol, vmin);
+        *width = A::div(wid, wsum);  // TTI.hpp:372-388
         return r;
     } else {
         unsigned used = 0, side = 0;
@@ -494,6 +503,36 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, int D, GeoSet<CA
     return 0;
 }
 
+// First point of a tip (warp-wide). tips_Unoriented: the angle (cell centre) of smallest value at
+// the point (x, y), the last one on ties (HFMInterface.hxx:499-521); the first angle if (x, y) is
+// outside the grid.
+template <typename Real>
+__device__ void geo_tip_start(const Dev<Real> &P, const Inst &I, const GeoTip &tp, double *tip) {
+    using A = Arith<double>;
+    const int lane = threadIdx.x & 31;
+    const GridGeom &g = I.g;
+    tip[0] = tp.p[0];
+    tip[1] = tp.p[1];
+    tip[2] = tp.p[2];
+    if (!tp.unoriented) return;
+    const Real *values = P.values + I.cell0;
+    const double fx = floor(tip[0]), fy = floor(tip[1]);
+    const bool inside = fx >= 0 && fy >= 0 && fx < g.dims[0] && fy < g.dims[1];
+    double bv = A::inf();
+    int bt = -1;
+    if (inside)
+        for (int th = lane; th < g.dims[2]; th += 32) {
+            const double v = (double)values[g.lin((int)fx, (int)fy, th)];
+            if (v <= bv) { bv = v; bt = th; }
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int ot = __shfl_xor_sync(0xffffffffu, bt, o);
+        if (ot >= 0 && (bt < 0 || ov < bv || (ov == bv && ot > bt))) { bv = ov; bt = ot; }
+    }
+    tip[2] = A::add((double)(bt < 0 ? 0 : bt), 0.5);
+}
+
 // One warp per tip, warps looping over the tips (GeodesicDiscreteSolver.hxx:41-55 for the restarts:
 // after 5 restarts the volume bound grows by 1.3 per restart, 50 restarts mean failure). With
 // GLOBAL the warps' sets live in `gsets` (one per warp of the grid) instead of shared memory.
@@ -516,27 +555,8 @@ geodesic_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut 
         const GridGeom &g = I.g;
         const int D = tp.ndim;
         double *out = pts + tp.out0 * D;
-        double tip[3] = {tp.p[0], tp.p[1], tp.p[2]};
-        if (tp.unoriented) {
-            // the angle (cell centre) of smallest value at the point (x, y); the last one on ties
-            // (HFMInterface.hxx:499-521); the first angle if (x, y) is outside the grid
-            const Real *values = P.values + I.cell0;
-            const double fx = floor(tip[0]), fy = floor(tip[1]);
-            const bool inside = fx >= 0 && fy >= 0 && fx < g.dims[0] && fy < g.dims[1];
-            double bv = A::inf();
-            int bt = -1;
-            if (inside)
-                for (int th = lane; th < g.dims[2]; th += 32) {
-                    const double v = (double)values[g.lin((int)fx, (int)fy, th)];
-                    if (v <= bv) { bv = v; bt = th; }
-                }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                const int ot = __shfl_xor_sync(0xffffffffu, bt, o);
-                if (ot >= 0 && (bt < 0 || ov < bv || (ov == bv && ot > bt))) { bv = ov; bt = ot; }
-            }
-            tip[2] = A::add((double)(bt < 0 ? 0 : bt), 0.5);
-        }
+        double tip[3];
+        geo_tip_start<Real>(P, I, tp, tip);
         int len = 0, status = 0, restarts = 0;
         if (tp.cap < 1) {
             status |= kGeoPointOverflow;
@@ -560,6 +580,213 @@ geodesic_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// ODE geodesic solver (Headers/Base/Implementation/GeodesicODESolver.hxx): a midpoint scheme on the
+// geodesic flow interpolated from the 2^D cells around the point. It stops when the L-infinity
+// distance to the seeds (capped at 6) is larger than it was ceil(sqrt(D)/step) steps before, and
+// fails when a cell has been used more than int(6 sqrt(D)/step) times (stationarity). The counts
+// live in a per-tip hash table in global memory (one per warp of the grid); the flow data of a
+// cell is recomputed where the reference caches it (the same values). For the unit offsets used
+// here the wall test of VisibleOffset reduces to "the target cell is not a wall".
+
+constexpr short kOdeFar = 32767;
+constexpr int kOdeTargetCap = 6;
+constexpr int kOdeHistCap = 256;
+
+// L-infinity distance to the seeds (LInfDistance, GeodesicODESolver.hxx:225-258): 0 at the seeds.
+template <typename Real, int KIND>
+__global__ void ode_target_init_kernel(Dev<Real> P, short *target) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    bool fixed, dead;
+    cell_flags<Real, KIND>(P, R.c, fixed, dead);
+    target[x] = fixed ? (short)0 : kOdeFar;
+}
+
+// One breadth-first level: an unassigned cell that is not a wall takes k + 1 if one of its 3^D - 1
+// neighbours is at k (cells at the cap are not expanded).
+template <typename Real>
+__global__ void ode_target_step_kernel(Dev<Real> P, const int8_t *wd, int k, short *target) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells || target[x] != kOdeFar) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[R.i];
+    const GridGeom &g = I.g;
+    if (wd && I.has_walls && wd[x] == 0) return;
+    for (int o = 0; o < 27; ++o) {
+        if (o == 13) continue;
+        int y0 = R.x0 - (o / 9 - 1), y1 = R.x1 - ((o / 3) % 3 - 1), y2 = R.x2 - (o % 3 - 1);
+        if (!g.wrap(y0, y1, y2)) continue;
+        if (target[I.cell0 + g.lin(y0, y1, y2)] == (short)k) {
+            target[x] = (short)(k + 1);
+            return;
+        }
+    }
+}
+
+// GeodesicFlow at a point (GeodesicODESolver.hxx:53-154), warp-wide; lanes < 2^D each take one of
+// the cells around the point. Returns the interpolated flow (uniform), the largest use count
+// before this call among the cells (nstat) and their smallest target distance (tol).
+template <typename Real, int NFWD, int NSYM, int KIND>
+__device__ void ode_flow_at(const Dev<Real> &P, const Inst &I, int D, const int8_t *wd, const short *target,
+                            unsigned long long *keys, int *counts, int tmask, double causality, const double *pt,
+                            double *flow, int &nstat, int &tol, int &status) {
+    using A = Arith<double>;
+    const int lane = threadIdx.x & 31;
+    const GridGeom &g = I.g;
+    int pi[3] = {0, 0, 0}, sg[3] = {0, 0, 0};
+    double w[3] = {0, 0, 0};
+    for (int j = 0; j < D; ++j) {
+        pi[j] = (int)floor(pt[j]);
+        w[j] = A::sub(A::sub(pt[j], (double)pi[j]), 0.5);
+        sg[j] = w[j] > 0 ? 1 : -1;
+        w[j] = fabs(w[j]);
+    }
+    bool valid = false;
+    int ltol = 2147483647, lstat = 0;
+    double val = A::inf(), wid = 0.0, fl[3] = {0, 0, 0}, weight = 0.0;
+    if (lane < (1 << D)) {
+        int q[3] = {pi[0], pi[1], pi[2]};
+        for (int j = 0; j < D; ++j)
+            if ((lane >> j) & 1) q[j] += sg[j];
+        valid = g.wrap(q[0], q[1], q[2]);
+        const long long y = valid ? g.lin(q[0], q[1], q[2]) : 0;
+        if (valid && wd && I.has_walls && wd[I.cell0 + y] == 0) valid = false;
+        if (valid) {
+            ltol = target[I.cell0 + y];
+            unsigned foff[kGeoMaxFlow];
+            double fw[kGeoMaxFlow];
+            const int nf = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, q[0], q[1], q[2], foff, fw, &val, &wid);
+            for (int a = 0; a < D; ++a) {
+                double acc = 0.0;
+                for (int f = 0; f < nf; ++f) acc = A::add(acc, A::mul(fw[f], (double)off_c(foff[f], a)));
+                fl[a] = acc;
+            }
+            // use count of the cell in this tip's table (open addressing, linear probing)
+            unsigned h = (unsigned)((unsigned long long)(y + 1) * 0x9E3779B97F4A7C15ull >> 32) & (unsigned)tmask;
+            int probes = 0;
+            for (;;) {
+                const unsigned long long prev = atomicCAS(keys + h, ~0ull, (unsigned long long)y);
+                if (prev == ~0ull || prev == (unsigned long long)y) break;
+                h = (h + 1) & (unsigned)tmask;
+                if (++probes > (tmask >> 1)) { status |= kGeoSetOverflow; break; }
+            }
+            if (probes <= (tmask >> 1)) lstat = atomicAdd(counts + h, 1);
+            weight = 1.0;
+            for (int j = 0; j < D; ++j) weight = A::mul(weight, ((lane >> j) & 1) ? w[j] : A::sub(1.0, w[j]));
+        }
+    }
+    status |= __reduce_or_sync(0xffffffffu, (unsigned)status);
+    // reductions in the order of the cells (the reference's loops over i)
+    tol = 2147483647;
+    nstat = 0;
+    double minVal = A::inf(), minWidth = 0.0;
+    for (int i = 0; i < (1 << D); ++i) {
+        const bool vi = __shfl_sync(0xffffffffu, valid, i);
+        if (!vi) continue;
+        tol = min(tol, __shfl_sync(0xffffffffu, ltol, i));
+        nstat = max(nstat, __shfl_sync(0xffffffffu, lstat, i));
+        const double wi = __shfl_sync(0xffffffffu, weight, i), v = __shfl_sync(0xffffffffu, val, i);
+        const double wd_i = __shfl_sync(0xffffffffu, wid, i);
+        if (wi > 0 && v < minVal) { minVal = v; minWidth = wd_i; }
+    }
+    flow[0] = flow[1] = flow[2] = 0.0;
+    if (!(minVal < A::inf())) return;  // in a wall
+    const double thr = A::add(minVal, A::mul(causality, minWidth));
+    double ws = 0.0;
+    for (int i = 0; i < (1 << D); ++i) {
+        const bool vi = __shfl_sync(0xffffffffu, valid, i);
+        const double wi = __shfl_sync(0xffffffffu, weight, i), v = __shfl_sync(0xffffffffu, val, i);
+        double f[3];
+        for (int a = 0; a < 3; ++a) f[a] = __shfl_sync(0xffffffffu, fl[a], i);
+        if (!vi || !(wi > 0)) continue;
+        if (v <= thr) {
+            ws = A::add(ws, wi);
+            for (int a = 0; a < D; ++a) flow[a] = A::add(flow[a], A::mul(wi, f[a]));
+        }
+    }
+    if (ws > 0)
+        for (int a = 0; a < D; ++a) flow[a] = A::div(flow[a], ws);
+}
+
+// One warp per ODE tip (Run, GeodesicODESolver.hxx:159-212); the warp's count table has
+// 2^table_log2 entries at keys/counts + warp * 2^table_log2.
+template <typename Real, int NFWD, int NSYM, int KIND>
+__global__ void __launch_bounds__(kGeoWarps * 32)
+geodesic_ode_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut *outs, const int8_t *wd,
+                    const short *target, unsigned long long *tkeys, int *tcounts, int table_log2) {
+    using A = Arith<double>;
+    __shared__ int hist_s[kGeoWarps][kOdeHistCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * kGeoWarps + wib, nw = (long long)gridDim.x * kGeoWarps;
+    int *hist = hist_s[wib];
+    for (long long t = gw; t < ntips; t += nw) {
+        const GeoTip tp = tips[t];
+        const Inst &I = P.inst[tp.inst];
+        const int D = tp.ndim;
+        double *out = pts + tp.out0 * D;
+        double tip[3];
+        geo_tip_start<Real>(P, I, tp, tip);
+        int len = 0, status = 0, failed = 0;
+        const int tl2 = min(tp.table_log2, table_log2);
+        const int tmask = (1 << tl2) - 1;
+        unsigned long long *keys = tkeys + (gw << table_log2);
+        int *counts = tcounts + (gw << table_log2);
+        for (int i = lane; i <= tmask; i += 32) { keys[i] = ~0ull; counts[i] = 0; }
+        for (int i = lane; i < tp.nhist; i += 32) hist[i] = 2147483647;
+        __syncwarp();
+        __threadfence_block();
+        if (tp.cap < 1 || tp.nhist > kOdeHistCap) {
+            status |= kGeoPointOverflow;
+        } else {
+            if (lane == 0)
+                for (int a = 0; a < D; ++a) out[a] = tip[a];
+            len = 1;
+            int head = 0;
+            double p[3] = {tip[0], tip[1], tip[2]};
+            for (;;) {
+                double f[3];
+                int nstat, tol;
+                ode_flow_at<Real, NFWD, NSYM, KIND>(P, I, D, wd, target, keys, counts, tmask, tp.causality, p, f,
+                                                    nstat, tol, status);
+                if (status) break;
+                int old = tol;
+                if (tp.nhist > 0) {
+                    __syncwarp();
+                    old = hist[head];
+                    __syncwarp();
+                    if (lane == 0) hist[head] = tol;
+                    head = head + 1 == tp.nhist ? 0 : head + 1;
+                }
+                if (old < tol) break;  // moving away from the seeds: done
+                if (nstat > tp.nstat_max) { failed = 1; break; }
+                double nrm = 0.0;
+                for (int a = 0; a < D; ++a) nrm = A::add(nrm, A::mul(f[a], f[a]));
+                nrm = A::sqrt(nrm);
+                if (nrm == 0) break;  // at a seed
+                const double half = A::mul(0.5, tp.step);
+                double q[3] = {p[0], p[1], p[2]};
+                for (int a = 0; a < D; ++a) q[a] = A::add(p[a], A::div(A::mul(half, f[a]), nrm));
+                ode_flow_at<Real, NFWD, NSYM, KIND>(P, I, D, wd, target, keys, counts, tmask, tp.causality, q, f,
+                                                    nstat, tol, status);
+                if (status) break;
+                nrm = 0.0;
+                for (int a = 0; a < D; ++a) nrm = A::add(nrm, A::mul(f[a], f[a]));
+                nrm = A::sqrt(nrm);
+                if (nrm == 0) break;
+                if (len >= tp.cap) { status |= kGeoPointOverflow; break; }
+                for (int a = 0; a < D; ++a) p[a] = A::add(p[a], A::div(A::mul(tp.step, f[a]), nrm));
+                if (lane == 0)
+                    for (int a = 0; a < D; ++a) out[(long long)len * D + a] = p[a];
+                ++len;
+            }
+        }
+        if (lane == 0) outs[t] = GeoOut{len, status | (failed ? kGeoFailed : 0), 0, 0};
+        __syncwarp();
+    }
+}
+
 // Gathers the points of each tip (len points of ndim values at out0) into a compact array.
 __global__ void geodesic_compact_kernel(const double *pts, const GeoTip *tips, const GeoOut *outs,
                                         const long long *dst0, int ntips, double *dst) {
@@ -576,7 +803,7 @@ __global__ void geodesic_compact_kernel(const double *pts, const GeoTip *tips, c
 // overflowed is run again with 8x the room (its set in global memory); three attempts at most.
 template <typename Real, int NFWD, int NSYM, int KIND>
 void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std::vector<const EulerProblem *> &probs,
-                   std::vector<EulerResult> &results, cudaStream_t s) {
+                   std::vector<EulerResult> &results, const int8_t *wd, cudaStream_t s) {
     const int ninst = (int)probs.size();
     bool any_flow = false;
     std::vector<GeoTip> tips;
@@ -604,6 +831,21 @@ void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std
                 t.cap = cap;
                 t.ndim = p.ndim;
                 t.unoriented = gi;
+                t.ode = p.geo_ode ? 1 : 0;
+                t.causality = p.geo_causality;
+                if (p.geo_ode) {
+                    const double sd = std::sqrt((double)p.ndim);
+                    t.nstat_max = (int)(6 * sd / p.geo_step);
+                    const double hl = sd / p.geo_step;
+                    if (!(hl < kOdeHistCap))
+                        throw Error(HFM_ERR_UNSUPPORTED, "geodesicStep too small for the ODE geodesic solver");
+                    int nh = 0;
+                    while (nh < hl) ++nh;
+                    t.nhist = nh;
+                    int l2 = 12;
+                    while (l2 < 24 && (1ll << l2) < 2ll * cap) ++l2;
+                    t.table_log2 = l2;
+                }
                 slots += cap;
                 tips.push_back(t);
                 group.push_back(gi);
@@ -635,38 +877,66 @@ void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std
         std::vector<int> todo(ntips);
         for (int t = 0; t < ntips; ++t) todo[t] = t;
         std::vector<std::vector<double>> tip_pts(ntips);
+        DeviceBuffer<short> target;  // L-infinity distance to the seeds (ODE tips)
         for (int attempt = 0; attempt < 3 && !todo.empty(); ++attempt) {
             bool big = false;
             if (attempt > 0) {
                 long long sl = 0;
                 for (int t : todo) {
-                    big |= (houts[t].status & kGeoSetOverflow) != 0;
+                    const bool set_over = (houts[t].status & kGeoSetOverflow) != 0;
+                    big |= set_over && !tips[t].ode;
+                    if (set_over && tips[t].ode) tips[t].table_log2 = std::min(27, tips[t].table_log2 + 3);
                     if (houts[t].status & kGeoPointOverflow) tips[t].cap = (int)std::min<long long>(1 << 27, 8ll * tips[t].cap);
                     tips[t].out0 = sl;
                     sl += tips[t].cap;
                 }
                 slots = sl;
             }
+            // discrete tips first, then ODE tips (one launch each)
+            std::stable_partition(todo.begin(), todo.end(), [&](int t) { return !tips[t].ode; });
             std::vector<GeoTip> sub(todo.size());
             for (size_t k = 0; k < todo.size(); ++k) sub[k] = tips[todo[k]];
             const int nsub = (int)sub.size();
+            int ndisc = 0;
+            while (ndisc < nsub && !sub[ndisc].ode) ++ndisc;
+            const int node = nsub - ndisc;
             DeviceBuffer<GeoTip> dtips(nsub);
             dtips.upload(sub.data(), nsub, s);
             DeviceBuffer<GeoOut> douts(nsub);
             DeviceBuffer<double> pts(slots * ndim);
-            const int want_blocks = (nsub + kGeoWarps - 1) / kGeoWarps;
-            if (!big) {
+            if (node > 0) {
+                if (!target.get()) {
+                    target.alloc(P.ncells);
+                    launch(ode_target_init_kernel<Real, KIND>, nblocks(P.ncells, 256), 256, 0, s, P, target.get());
+                    for (int k = 0; k < kOdeTargetCap; ++k)
+                        launch(ode_target_step_kernel<Real>, nblocks(P.ncells, 256), 256, 0, s, P, wd, k, target.get());
+                    HFM_CUDA(cudaGetLastError());
+                }
+                int l2 = 0;
+                for (int k = ndisc; k < nsub; ++k) l2 = std::max(l2, sub[k].table_log2);
+                const int grid = std::max(1, std::min((node + kGeoWarps - 1) / kGeoWarps, nsm));
+                const size_t entries = ((size_t)grid * kGeoWarps) << l2;
+                DeviceBuffer<unsigned long long> tkeys(entries);
+                DeviceBuffer<int> tcounts(entries);
+                launch(geodesic_ode_kernel<Real, NFWD, NSYM, KIND>, grid, kGeoWarps * 32, 0, s, P, dtips.get() + ndisc,
+                       node, pts.get(), douts.get() + ndisc, wd, (const short *)target.get(), tkeys.get(), tcounts.get(),
+                       l2);
+                HFM_CUDA(cudaGetLastError());
+                HFM_CUDA(cudaStreamSynchronize(s));
+            }
+            const int want_blocks = (ndisc + kGeoWarps - 1) / kGeoWarps;
+            if (ndisc > 0 && !big) {
                 auto kern = geodesic_kernel<Real, NFWD, NSYM, KIND, kGeoCap, kGeoStepCap, false>;
                 int per_sm = 0;
                 HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGeoWarps * 32, 0));
                 const int grid = std::max(1, std::min(want_blocks, nsm * std::max(1, per_sm)));
-                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), nsub, pts.get(), douts.get(),
+                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), ndisc, pts.get(), douts.get(),
                        (GeoSet<kGeoCap, kGeoStepCap> *)nullptr);
-            } else {
+            } else if (ndisc > 0) {
                 auto kern = geodesic_kernel<Real, NFWD, NSYM, KIND, kGeoCapBig, kGeoStepCapBig, true>;
                 const int grid = std::max(1, std::min(want_blocks, 2 * nsm));
                 DeviceBuffer<GeoSet<kGeoCapBig, kGeoStepCapBig>> gsets((size_t)grid * kGeoWarps);
-                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), nsub, pts.get(), douts.get(), gsets.get());
+                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), ndisc, pts.get(), douts.get(), gsets.get());
                 HFM_CUDA(cudaStreamSynchronize(s));
             }
             HFM_CUDA(cudaGetLastError());

@@ -521,12 +521,20 @@ void read_geodesics(Store &io, const Param &pm, bool lifted, EulerProblem &p, bo
     has[1] = lifted && io.has_field("tips_Unoriented");
     if (has[0] || has[1]) {
         const std::string solver = io.get_string("geodesicSolver", "Discrete");
-        if (solver == "ODE")
-            throw Error(HFM_ERR_UNSUPPORTED, "geodesicSolver 'ODE' is not supported by the GPU solve path");
-        if (solver != "Discrete") throw Error(HFM_ERR_VALUE, "Error : Unrecognized geodesic solver " + solver + ".\n");
+        if (solver != "Discrete" && solver != "ODE")
+            throw Error(HFM_ERR_VALUE, "Error : Unrecognized geodesic solver " + solver + ".\n");
+        p.geo_ode = solver == "ODE";
         p.geo_step = io.get_scalar("geodesicStep", 0.25);
-        p.geo_threshold = io.get_scalar("geodesicWeightThreshold", 0.001);
-        p.geo_volume_bound = io.get_scalar("geodesicVolumeBound", 5. * std::pow(1.3, pm.ndim));
+        if (!(p.geo_step > 0)) throw Error(HFM_ERR_VALUE, "geodesicStep must be positive");
+        if (p.geo_ode) {
+            // GeodesicODESolver.hxx:17-23; the target tolerance is read but the distances to the
+            // seeds are capped at 6 when the solver is built, before the keys are read
+            p.geo_causality = io.get_scalar("geodesicCausalityTolerance", 4.0);
+            io.get_scalar("geodesicTargetTolerance", 6.0);
+        } else {
+            p.geo_threshold = io.get_scalar("geodesicWeightThreshold", 0.001);
+            p.geo_volume_bound = io.get_scalar("geodesicVolumeBound", 5. * std::pow(1.3, pm.ndim));
+        }
     }
     if (has[0]) {
         int64_t n = 0;
@@ -683,7 +691,8 @@ void export_geodesics(Store &io, const Prepared &q, const EulerResult &r) {
             for (int a = 0; a < D; ++a) tip << (a ? "," : "") << pts[first * D + a];
             tip << "}";
             const int st = r.geo_status[gi][t];
-            if (st & 1) io.msg("Geodesic extraction failed for tip " + tip.str() + "\n");
+            if ((st & 1) && q.p.geo_ode) io.msg("Geodesic ODE solver seems to have failed for tip " + tip.str() + ".\n");
+            else if (st & 1) io.msg("Geodesic extraction failed for tip " + tip.str() + "\n");
             else if (r.geo_restarts[gi][t] > 5) {
                 double vb = q.p.geo_volume_bound;
                 for (int k = 5; k <= r.geo_restarts[gi][t]; ++k) vb *= 1.3;

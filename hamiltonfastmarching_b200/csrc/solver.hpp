@@ -79,6 +79,8 @@ struct EulerProblem {
     // [n][2] (x, y) whose angle is chosen on the device; the discrete solver's parameters.
     std::vector<double> geo_tips, geo_tips_unoriented;
     double geo_step = 0.25, geo_threshold = 1e-3, geo_volume_bound = 8.45;
+    bool geo_ode = false;              // geodesicSolver 'ODE' instead of 'Discrete'
+    double geo_causality = 4.0;        // geodesicCausalityTolerance (ODE)
     bool want_geodesic_flow = false;   // exportGeodesicFlow
     // Forward first variation (costVariation, seedValueVariation): fwd_nvar variations; fwd_cost
     // [N][nvar] RowMajor or empty; seed cells and their value variations [n][nvar], later entries

@@ -78,7 +78,7 @@ def test_unsupported_options_rejected_before_gpu_work(key, val):
     assert e.value.code == 3, str(e.value)
 
 
-@pytest.mark.parametrize("solver,code", [("ODE", 3), ("Runge", 2)])
+@pytest.mark.parametrize("solver,code", [("Runge", 2)])
 def test_geodesic_solver_choice_checked_before_gpu_work(solver, code):
     p = {"model": "Riemann2", "arrayOrdering": "RowMajor", "dims": np.array([8., 8.]), "gridScale": 0.125,
          "metric": np.array([1., 0., 1.]), "seeds": np.array([[0.5, 0.5]]), "verbosity": 0.0,

@@ -20,6 +20,9 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
           "geo_tti3_12"]
+# geodesicSolver = 'ODE' (the Riemann3 fixture has a tip whose solver stalls, as in the reference)
+GOLDEN_ODE = ["ode_riemann2_48_walls", "ode_riemann3_16_walls", "ode_reedsshepp2_24x16", "ode_elastica2_24x16",
+              "ode_tti3_12"]
 
 
 def _oracle_on(out, params):
@@ -160,3 +163,26 @@ def test_fp32_geodesics_close_to_fp64():
     for s, rs, ln, rl in zip(starts, rstarts, lens, ref["geodesicLengths"]):
         a, b = out["geodesicPoints"][int(s + ln - 1)], ref["geodesicPoints"][int(rs + rl - 1)]
         assert np.max(np.abs(a - b)) < 0.05   # both end at the seed
+
+
+@pytest.mark.parametrize("name", GOLDEN_ODE)
+def test_ode_geodesics_match_oracle_and_reference(name):
+    """ODE solver: against the oracle on the GPU's values and activeNeighs (same lengths, points
+    within 1e-11) and against the reference executable (same lengths, points within 1e-7)."""
+    params, ref, _ = load_golden(name)
+    params = dict(params, exportValues=1.0, exportActiveNeighs=1.0)
+    out = hfm.run(params)
+    geo, _ = _oracle_on(out, params)
+    _check(out, geo, _suffixes(params), 1e-11, 0)
+    _check(out, {k: v for k, v in ref.items() if k != "geodesicFlow"}, _suffixes(params), 1e-7, 0)
+
+
+def test_ode_many_tips_with_walls():
+    p = W.riemann2_case(128, aniso=6.0, seed=33)
+    p["walls"] = np.zeros((128, 128))
+    p["walls"][40, 10:110] = 1.0
+    p["tips"] = np.random.default_rng(6).uniform(0.02, 0.98, (200, 2))
+    params = dict(p, geodesicSolver="ODE", exportValues=1.0, exportActiveNeighs=1.0, verbosity=0.0)
+    out = hfm.run(params)
+    geo, _ = _oracle_on(out, params)
+    _check(out, geo, [""], 1e-11, 0)
