@@ -260,11 +260,37 @@ __global__ void geodesic_flow_kernel(Dev<Real> P, int ndim, double *out) {
     }
 }
 
+// Recompute flow of every cell of a batch, computed once before the geodesic launch (the
+// discrete solver reads it at every extraction): nf[x] entries, entry f at foff/fw[f * N + x].
+struct GeoRec {
+    long long N;
+    const uint8_t *nf;
+    const unsigned *foff;
+    const double *fw;
+};
+
+template <typename Real, int NFWD, int NSYM, int KIND>
+__global__ void geo_rec_kernel(Dev<Real> P, int maxf, uint8_t *nf, unsigned *foff, double *fw) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells) return;
+    const CellRef C = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[C.i];
+    unsigned o[kGeoMaxFlow];
+    double w[kGeoMaxFlow], v, wd;
+    int n = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, C.x0, C.x1, C.x2, o, w, &v, &wd);
+    n = n < maxf ? n : maxf;
+    nf[x] = (uint8_t)n;
+    for (int f = 0; f < n; ++f) {
+        foff[f * P.ncells + x] = o[f];
+        fw[f * P.ncells + x] = w[f];
+    }
+}
+
 // Unit mass split among the 2^D grid neighbours of the tip, the extraction loop and the emission of
 // points (GeodesicDiscreteSolver.hxx:59-211). Warp-uniform except where lane 0 writes. Returns 1
 // if the mass spread beyond the volume bound (restart from the last point), 0 otherwise.
-template <typename Real, int NFWD, int NSYM, int KIND, int CAP, int SCAP>
-__device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, int D, GeoSet<CAP, SCAP> &S, double *out,
+template <typename Real, int CAP, int SCAP, int D>
+__device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, const GeoRec &R, GeoSet<CAP, SCAP> &S, double *out,
                              int cap, int &len, int &status, double step, double thr, double vbound,
                              long long iter_cap) {
     using A = Arith<double>;
@@ -362,12 +388,13 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, int D, GeoSet<CA
         sums(-ew, ind);
         int q0 = ind[0], q1 = ind[1], q2 = ind[2];
         g.wrap(q0, q1, q2);
-        int nf = 0;
-        if (lane == 0) {
-            double rv, rw;
-            nf = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, q0, q1, q2, S.foff, S.fw, &rv, &rw);
+        // the extracted cell's flow, from the records computed for every cell before the launch
+        const long long gx = I.cell0 + g.lin(q0, q1, q2);
+        const int nf = R.nf[gx];
+        if (lane < nf) {
+            S.foff[lane] = R.foff[lane * R.N + gx];
+            S.fw[lane] = R.fw[lane * R.N + gx];
         }
-        nf = __shfl_sync(0xffffffffu, nf, 0);
         __syncwarp();
         double wSum = 0.0;
         for (int f = 0; f < nf; ++f) wSum = A::add(wSum, S.fw[f]);
@@ -536,9 +563,10 @@ __device__ void geo_tip_start(const Dev<Real> &P, const Inst &I, const GeoTip &t
 // One warp per tip, warps looping over the tips (GeodesicDiscreteSolver.hxx:41-55 for the restarts:
 // after 5 restarts the volume bound grows by 1.3 per restart, 50 restarts mean failure). With
 // GLOBAL the warps' sets live in `gsets` (one per warp of the grid) instead of shared memory.
-template <typename Real, int NFWD, int NSYM, int KIND, int CAP, int SCAP, bool GLOBAL>
+template <typename Real, int CAP, int SCAP, bool GLOBAL, int D>
 __global__ void __launch_bounds__(kGeoWarps * 32)
-geodesic_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut *outs, GeoSet<CAP, SCAP> *gsets) {
+geodesic_kernel(Dev<Real> P, GeoRec R, const GeoTip *tips, int ntips, double *pts, GeoOut *outs,
+                GeoSet<CAP, SCAP> *gsets) {
     using A = Arith<double>;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long gw = (long long)blockIdx.x * kGeoWarps + wib, nw = (long long)gridDim.x * kGeoWarps;
@@ -553,7 +581,6 @@ geodesic_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut 
         const GeoTip tp = tips[t];
         const Inst &I = P.inst[tp.inst];
         const GridGeom &g = I.g;
-        const int D = tp.ndim;
         double *out = pts + tp.out0 * D;
         double tip[3];
         geo_tip_start<Real>(P, I, tp, tip);
@@ -567,8 +594,8 @@ geodesic_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut 
             double vb = tp.vbound;
             const long long iter_cap = 64 * g.ncells + 4096;
             while (restarts < 50) {
-                const int r = geodesic_pass<Real, NFWD, NSYM, KIND, CAP, SCAP>(P, I, D, *S, out, tp.cap, len, status,
-                                                                              tp.step, tp.thr, vb, iter_cap);
+                const int r = geodesic_pass<Real, CAP, SCAP, D>(P, I, R, *S, out, tp.cap, len, status, tp.step,
+                                                               tp.thr, vb, iter_cap);
                 if (!r || status) break;
                 ++restarts;
                 if (restarts >= 5) vb = A::mul(vb, 1.3);
@@ -604,6 +631,29 @@ __global__ void ode_target_init_kernel(Dev<Real> P, short *target) {
     target[x] = fixed ? (short)0 : kOdeFar;
 }
 
+// The flow data the ODE solver reads at a cell (the reference's GeodesicFlow, cached per tip):
+// rec[x][0..D) = sum of weight * offset over the Recompute flow, rec[x][D] = value, rec[x][D+1] =
+// width. Computed once for every cell of the batch.
+template <typename Real, int NFWD, int NSYM, int KIND>
+__global__ void ode_cell_kernel(Dev<Real> P, int D, double *rec) {
+    using A = Arith<double>;
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= P.ncells) return;
+    const CellRef R = cell_ref(P.inst, P.ninst, x);
+    const Inst &I = P.inst[R.i];
+    unsigned foff[kGeoMaxFlow];
+    double fw[kGeoMaxFlow], v, wd;
+    const int nf = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, R.x0, R.x1, R.x2, foff, fw, &v, &wd);
+    double *o = rec + x * (D + 2);
+    for (int a = 0; a < D; ++a) {
+        double acc = 0.0;
+        for (int f = 0; f < nf; ++f) acc = A::add(acc, A::mul(fw[f], (double)off_c(foff[f], a)));
+        o[a] = acc;
+    }
+    o[D] = v;
+    o[D + 1] = wd;
+}
+
 // One breadth-first level: an unassigned cell that is not a wall takes k + 1 if one of its 3^D - 1
 // neighbours is at k (cells at the cap are not expanded).
 template <typename Real>
@@ -628,10 +678,10 @@ __global__ void ode_target_step_kernel(Dev<Real> P, const int8_t *wd, int k, sho
 // GeodesicFlow at a point (GeodesicODESolver.hxx:53-154), warp-wide; lanes < 2^D each take one of
 // the cells around the point. Returns the interpolated flow (uniform), the largest use count
 // before this call among the cells (nstat) and their smallest target distance (tol).
-template <typename Real, int NFWD, int NSYM, int KIND>
+template <typename Real>
 __device__ void ode_flow_at(const Dev<Real> &P, const Inst &I, int D, const int8_t *wd, const short *target,
-                            unsigned long long *keys, int *counts, int tmask, double causality, const double *pt,
-                            double *flow, int &nstat, int &tol, int &status) {
+                            const double *rec, unsigned long long *keys, int *counts, int tmask, double causality,
+                            const double *pt, double *flow, int &nstat, int &tol, int &status) {
     using A = Arith<double>;
     const int lane = threadIdx.x & 31;
     const GridGeom &g = I.g;
@@ -655,14 +705,10 @@ __device__ void ode_flow_at(const Dev<Real> &P, const Inst &I, int D, const int8
         if (valid && wd && I.has_walls && wd[I.cell0 + y] == 0) valid = false;
         if (valid) {
             ltol = target[I.cell0 + y];
-            unsigned foff[kGeoMaxFlow];
-            double fw[kGeoMaxFlow];
-            const int nf = recompute_flow<Real, NFWD, NSYM, KIND>(P, I, q[0], q[1], q[2], foff, fw, &val, &wid);
-            for (int a = 0; a < D; ++a) {
-                double acc = 0.0;
-                for (int f = 0; f < nf; ++f) acc = A::add(acc, A::mul(fw[f], (double)off_c(foff[f], a)));
-                fl[a] = acc;
-            }
+            const double *r = rec + (I.cell0 + y) * (D + 2);
+            for (int a = 0; a < D; ++a) fl[a] = r[a];
+            val = r[D];
+            wid = r[D + 1];
             // use count of the cell in this tip's table (open addressing, linear probing)
             unsigned h = (unsigned)((unsigned long long)(y + 1) * 0x9E3779B97F4A7C15ull >> 32) & (unsigned)tmask;
             int probes = 0;
@@ -712,10 +758,10 @@ __device__ void ode_flow_at(const Dev<Real> &P, const Inst &I, int D, const int8
 
 // One warp per ODE tip (Run, GeodesicODESolver.hxx:159-212); the warp's count table has
 // 2^table_log2 entries at keys/counts + warp * 2^table_log2.
-template <typename Real, int NFWD, int NSYM, int KIND>
+template <typename Real>
 __global__ void __launch_bounds__(kGeoWarps * 32)
 geodesic_ode_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, GeoOut *outs, const int8_t *wd,
-                    const short *target, unsigned long long *tkeys, int *tcounts, int table_log2) {
+                    const short *target, const double *rec, unsigned long long *tkeys, int *tcounts, int table_log2) {
     using A = Arith<double>;
     __shared__ int hist_s[kGeoWarps][kOdeHistCap];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -748,8 +794,8 @@ geodesic_ode_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, Geo
             for (;;) {
                 double f[3];
                 int nstat, tol;
-                ode_flow_at<Real, NFWD, NSYM, KIND>(P, I, D, wd, target, keys, counts, tmask, tp.causality, p, f,
-                                                    nstat, tol, status);
+                ode_flow_at<Real>(P, I, D, wd, target, rec, keys, counts, tmask, tp.causality, p, f, nstat, tol,
+                                  status);
                 if (status) break;
                 int old = tol;
                 if (tp.nhist > 0) {
@@ -768,8 +814,8 @@ geodesic_ode_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, Geo
                 const double half = A::mul(0.5, tp.step);
                 double q[3] = {p[0], p[1], p[2]};
                 for (int a = 0; a < D; ++a) q[a] = A::add(p[a], A::div(A::mul(half, f[a]), nrm));
-                ode_flow_at<Real, NFWD, NSYM, KIND>(P, I, D, wd, target, keys, counts, tmask, tp.causality, q, f,
-                                                    nstat, tol, status);
+                ode_flow_at<Real>(P, I, D, wd, target, rec, keys, counts, tmask, tp.causality, q, f, nstat, tol,
+                                  status);
                 if (status) break;
                 nrm = 0.0;
                 for (int a = 0; a < D; ++a) nrm = A::add(nrm, A::mul(f[a], f[a]));
@@ -796,6 +842,17 @@ __global__ void geodesic_compact_kernel(const double *pts, const GeoTip *tips, c
         double *d = dst + dst0[t];
         for (long long i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
     }
+}
+
+// Model dimensions a stencil family can have (the discrete kernel is compiled per dimension):
+// two symmetric per-cell differences are Diagonal2, three Riemann2 or Diagonal3, six Riemann3; two
+// shared axis differences are Isotropic2; every other family is three-dimensional.
+template <int NFWD, int NSYM, int KIND>
+constexpr bool geo_dim_ok(int d) {
+    if (KIND == kKindRiemann && NFWD == 0 && NSYM == 2) return d == 2;
+    if (KIND == kKindRiemann && NFWD == 0 && NSYM == 3) return true;
+    if (KIND == kKindShare && NFWD == 0 && NSYM == 2) return d == 2;
+    return d == 3;
 }
 
 // Geodesics of the tips of every instance of a batch, on the arrival times resident in P.values,
@@ -878,6 +935,13 @@ void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std
         for (int t = 0; t < ntips; ++t) todo[t] = t;
         std::vector<std::vector<double>> tip_pts(ntips);
         DeviceBuffer<short> target;  // L-infinity distance to the seeds (ODE tips)
+        DeviceBuffer<double> orec;   // per-cell flow, value and width (ODE tips)
+        // per-cell Recompute flow (discrete tips): at most one entry per forward difference and one
+        // side per symmetric difference
+        const int maxf = std::min(kGeoMaxFlow, KIND == kKindTTI ? 6 : NFWD + NSYM);
+        DeviceBuffer<uint8_t> rnf;
+        DeviceBuffer<unsigned> rfoff;
+        DeviceBuffer<double> rfw;
         for (int attempt = 0; attempt < 3 && !todo.empty(); ++attempt) {
             bool big = false;
             if (attempt > 0) {
@@ -910,6 +974,8 @@ void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std
                     launch(ode_target_init_kernel<Real, KIND>, nblocks(P.ncells, 256), 256, 0, s, P, target.get());
                     for (int k = 0; k < kOdeTargetCap; ++k)
                         launch(ode_target_step_kernel<Real>, nblocks(P.ncells, 256), 256, 0, s, P, wd, k, target.get());
+                    orec.alloc((size_t)P.ncells * (ndim + 2));
+                    launch(ode_cell_kernel<Real, NFWD, NSYM, KIND>, nblocks(P.ncells, 128), 128, 0, s, P, ndim, orec.get());
                     HFM_CUDA(cudaGetLastError());
                 }
                 int l2 = 0;
@@ -918,25 +984,49 @@ void run_geodesics(const Dev<Real> &P, const std::vector<Inst> &hinst, const std
                 const size_t entries = ((size_t)grid * kGeoWarps) << l2;
                 DeviceBuffer<unsigned long long> tkeys(entries);
                 DeviceBuffer<int> tcounts(entries);
-                launch(geodesic_ode_kernel<Real, NFWD, NSYM, KIND>, grid, kGeoWarps * 32, 0, s, P, dtips.get() + ndisc,
-                       node, pts.get(), douts.get() + ndisc, wd, (const short *)target.get(), tkeys.get(), tcounts.get(),
-                       l2);
+                launch(geodesic_ode_kernel<Real>, grid, kGeoWarps * 32, 0, s, P, dtips.get() + ndisc, node, pts.get(),
+                       douts.get() + ndisc, wd, (const short *)target.get(), (const double *)orec.get(), tkeys.get(),
+                       tcounts.get(), l2);
                 HFM_CUDA(cudaGetLastError());
                 HFM_CUDA(cudaStreamSynchronize(s));
             }
             const int want_blocks = (ndisc + kGeoWarps - 1) / kGeoWarps;
+            if (ndisc > 0 && !rnf.get()) {
+                rnf.alloc(P.ncells);
+                rfoff.alloc((size_t)maxf * P.ncells);
+                rfw.alloc((size_t)maxf * P.ncells);
+                launch(geo_rec_kernel<Real, NFWD, NSYM, KIND>, nblocks(P.ncells, 128), 128, 0, s, P, maxf, rnf.get(),
+                       rfoff.get(), rfw.get());
+                HFM_CUDA(cudaGetLastError());
+            }
+            const GeoRec R{P.ncells, rnf.get(), rfoff.get(), rfw.get()};
             if (ndisc > 0 && !big) {
-                auto kern = geodesic_kernel<Real, NFWD, NSYM, KIND, kGeoCap, kGeoStepCap, false>;
-                int per_sm = 0;
-                HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGeoWarps * 32, 0));
-                const int grid = std::max(1, std::min(want_blocks, nsm * std::max(1, per_sm)));
-                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), ndisc, pts.get(), douts.get(),
-                       (GeoSet<kGeoCap, kGeoStepCap> *)nullptr);
+                auto run = [&](auto kern) {
+                    int per_sm = 0;
+                    HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGeoWarps * 32, 0));
+                    const int grid = std::max(1, std::min(want_blocks, nsm * std::max(1, per_sm)));
+                    launch(kern, grid, kGeoWarps * 32, 0, s, P, R, dtips.get(), ndisc, pts.get(), douts.get(),
+                           (GeoSet<kGeoCap, kGeoStepCap> *)nullptr);
+                };
+                if (ndim == 2) {
+                    if constexpr (geo_dim_ok<NFWD, NSYM, KIND>(2))
+                        run(geodesic_kernel<Real, kGeoCap, kGeoStepCap, false, 2>);
+                } else if constexpr (geo_dim_ok<NFWD, NSYM, KIND>(3)) {
+                    run(geodesic_kernel<Real, kGeoCap, kGeoStepCap, false, 3>);
+                }
             } else if (ndisc > 0) {
-                auto kern = geodesic_kernel<Real, NFWD, NSYM, KIND, kGeoCapBig, kGeoStepCapBig, true>;
                 const int grid = std::max(1, std::min(want_blocks, 2 * nsm));
                 DeviceBuffer<GeoSet<kGeoCapBig, kGeoStepCapBig>> gsets((size_t)grid * kGeoWarps);
-                launch(kern, grid, kGeoWarps * 32, 0, s, P, dtips.get(), ndisc, pts.get(), douts.get(), gsets.get());
+                auto run = [&](auto kern) {
+                    launch(kern, grid, kGeoWarps * 32, 0, s, P, R, dtips.get(), ndisc, pts.get(), douts.get(),
+                           gsets.get());
+                };
+                if (ndim == 2) {
+                    if constexpr (geo_dim_ok<NFWD, NSYM, KIND>(2))
+                        run(geodesic_kernel<Real, kGeoCapBig, kGeoStepCapBig, true, 2>);
+                } else if constexpr (geo_dim_ok<NFWD, NSYM, KIND>(3)) {
+                    run(geodesic_kernel<Real, kGeoCapBig, kGeoStepCapBig, true, 3>);
+                }
                 HFM_CUDA(cudaStreamSynchronize(s));
             }
             HFM_CUDA(cudaGetLastError());
