@@ -553,13 +553,38 @@ int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active
     }
     int64_t nAccepted = 0;
     int64_t aidx[3], uidx[3];
+    /* stopWhenAllAccepted sets: targets not yet accepted (duplicates count once) */
+    uint8_t *all_left = NULL, *all_left_u = NULL;
+    int64_t n_all = 0, n_all_u = 0;
+    if (p->nstop_all > 0) {
+        all_left = (uint8_t *)calloc(N, 1);
+        for (int i = 0; i < p->nstop_all; ++i)
+            if (!all_left[p->stop_all[i]]) { all_left[p->stop_all[i]] = 1; ++n_all; }
+    }
+    if (p->nstop_all_u > 0) {
+        all_left_u = (uint8_t *)calloc(p->dims[0] * p->dims[1], 1);
+        for (int i = 0; i < p->nstop_all_u; ++i)
+            if (!all_left_u[p->stop_all_u[i]]) { all_left_u[p->stop_all_u[i]] = 1; ++n_all_u; }
+    }
     while (heap.n > 0) {
         /* RunOnce (HamiltonFastMarching.hxx:86-112) */
         const qelem top = heap_pop(&heap);
         if (accepted[top.idx]) continue;
         ++nAccepted;
-        accepted[top.idx] = 1;
         index_of(p, top.idx, aidx);
+        /* CommonStoppingCriteria::PostProcess (CommonStoppingCriteria.h:58-93): the cell that
+         * triggers a criterion is counted but not accepted */
+        {
+            int stop = p->n_max_accepted > 0 && nAccepted >= p->n_max_accepted;
+            for (int i = 0; !stop && i < p->nstop_any; ++i) stop = p->stop_any[i] == top.idx;
+            if (!stop && all_left && all_left[top.idx]) { all_left[top.idx] = 0; stop = --n_all == 0; }
+            const int64_t xy = aidx[0] * p->dims[1] + aidx[1];
+            for (int i = 0; !stop && i < p->nstop_any_u; ++i) stop = p->stop_any_u[i] == xy;
+            if (!stop && all_left_u && all_left_u[xy]) { all_left_u[xy] = 0; stop = --n_all_u == 0; }
+            if (!stop && p->has_stop_at_distance && values[top.idx] > p->stop_at_distance) stop = 1;
+            if (stop) break;
+        }
+        accepted[top.idx] = 1;
         const int64_t key = p->share ? aidx[p->ndim - 1] : top.idx;
         for (int64_t r = rc.split[key]; r < rc.split[key + 1]; ++r) {
             const int8_t *e = rc.off[r];
@@ -612,6 +637,8 @@ int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active
     free(heap.a);
     free(quads);
     free(accepted);
+    free(all_left);
+    free(all_left_u);
     if (!active) free(act);
     free(wd);
     free(rc.split);

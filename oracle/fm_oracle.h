@@ -50,10 +50,20 @@ typedef struct {
     int nseeds;
     const int64_t *seed_index; /* row-major linear indices */
     const double *seed_value;
+    /* stopping criteria (Headers/ExtraAlgorithms/CommonStoppingCriteria.h:58-93); a zeroed field
+     * is no criterion: stop_at_distance is used when has_stop_at_distance, n_max_accepted when > 0;
+     * stop_any / stop_all are cells, the _u variants (x, y) pairs packed as x * dims[1] + y. */
+    int has_stop_at_distance;
+    double stop_at_distance;
+    int64_t n_max_accepted;
+    int nstop_any, nstop_all, nstop_any_u, nstop_all_u;
+    const int64_t *stop_any, *stop_all, *stop_any_u, *stop_all_u;
 } fmo_problem;
 
 /* Fast marching. values[N] out; active[N] out (bitset, forward bits then symmetric +/- pairs,
- * as the reference's ActiveNeighFlagType) may be NULL. Returns accepted count, or -1. */
+ * as the reference's ActiveNeighFlagType) may be NULL. Returns the number of cells popped from the
+ * queue and examined (the reference's nAccepted: with a stopping criterion this counts the cell
+ * that stopped the run, which is not accepted), or -1. */
 int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active,
                           int *max_stencil_width);
 

@@ -41,6 +41,17 @@ class _Problem(ctypes.Structure):
         ("nseeds", ctypes.c_int),
         ("seed_index", _P),
         ("seed_value", _P),
+        ("has_stop_at_distance", ctypes.c_int),
+        ("stop_at_distance", ctypes.c_double),
+        ("n_max_accepted", ctypes.c_int64),
+        ("nstop_any", ctypes.c_int),
+        ("nstop_all", ctypes.c_int),
+        ("nstop_any_u", ctypes.c_int),
+        ("nstop_all_u", ctypes.c_int),
+        ("stop_any", _P),
+        ("stop_all", _P),
+        ("stop_any_u", _P),
+        ("stop_all_u", _P),
     ]
 
 
@@ -309,6 +320,33 @@ class Problem:
         s.walls = _ptr(self.walls)
         s.nseeds = len(self.seed_index)
         s.seed_index, s.seed_value = _ptr(self.seed_index), _ptr(self.seed_value)
+        # stopping criteria (CommonStoppingCriteria.h:95-147): target points out of range are dropped
+        if "stopAtDistance" in params:
+            s.has_stop_at_distance, s.stop_at_distance = 1, float(params["stopAtDistance"])
+        if "nMaxAccepted" in params:
+            s.n_max_accepted = int(params["nMaxAccepted"])
+        self._stops = {}
+        for key, fld, unoriented in (("stopWhenAnyAccepted", "stop_any", False),
+                                     ("stopWhenAllAccepted", "stop_all", False),
+                                     ("stopWhenAnyAccepted_Unoriented", "stop_any_u", True),
+                                     ("stopWhenAllAccepted_Unoriented", "stop_all_u", True)):
+            if key not in params:
+                continue
+            cells = []
+            for q in np.atleast_2d(np.asarray(params[key], float)):
+                if unoriented:
+                    i = self.index_of_point(np.array([q[0], q[1], 0.0]))
+                    if i is not None:
+                        idx = np.unravel_index(i, dims)
+                        cells.append(idx[0] * dims[1] + idx[1])
+                else:
+                    i = self.index_of_point(q)
+                    if i is not None:
+                        cells.append(i)
+            arr = np.ascontiguousarray(cells, np.int64)
+            self._stops[fld] = arr
+            setattr(s, "n" + fld, len(arr))
+            setattr(s, fld, _ptr(arr))
         self.struct = s
 
     def index_of_point(self, p):

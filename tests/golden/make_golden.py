@@ -216,6 +216,20 @@ def ode_fixtures():
     solve_fixture("ode_tti3_12", p)
 
 
+def stopping_fixtures():
+    """Stopping criteria: the run stops at the first cell popped that meets one (that cell is
+    counted in nAccepted but not accepted); the other cells keep their tentative values."""
+    p = W.riemann2_case(48, aniso=6.0, seed=5, n_seeds=2)
+    solve_fixture("stop_riemann2_distance", dict(p, stopAtDistance=0.12))
+    solve_fixture("stop_riemann2_nmax", dict(p, nMaxAccepted=700.0))
+    solve_fixture("stop_riemann2_any_all", dict(p, stopWhenAnyAccepted=np.array([[0.9, 0.9], [0.1, 0.8]]),
+                                                stopWhenAllAccepted=np.array([[0.7, 0.2], [0.3, 0.35]])))
+    p3 = W.riemann3_case(16, n_spheres=3, n_seeds=2, rmin=0.1, rmax=0.2, seed=22)
+    solve_fixture("stop_riemann3_walls_nmax", dict(p3, stopAtDistance=0.5, nMaxAccepted=2500.0))
+    c = W.curvature2_case(24, 16, "ReedsShepp2", seed=23, n_curves=4)
+    solve_fixture("stop_reedsshepp2_unoriented", dict(c, stopWhenAnyAccepted_Unoriented=np.array([[0.8, 0.2]])))
+
+
 def variation_fixtures():
     """Forward first variation (costVariation, seedValueVariation -> valueVariation)."""
     rng = np.random.default_rng(2025)
@@ -266,7 +280,7 @@ def isotropic_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
@@ -277,6 +291,8 @@ if __name__ == "__main__":
         isotropic_fixtures()
     elif sys.argv[1:] == ["ode"]:
         ode_fixtures()
+    elif sys.argv[1:] == ["stopping"]:
+        stopping_fixtures()
     else:
         main()
         tti_fixtures()
@@ -284,3 +300,4 @@ if __name__ == "__main__":
         variation_fixtures()
         isotropic_fixtures()
         ode_fixtures()
+        stopping_fixtures()

@@ -139,3 +139,18 @@ def test_isotropic_oracle_matches_reference(name):
     assert np.max(np.abs(geo["geodesicPoints"] - ref["geodesicPoints"])) <= 1e-15
     fin = np.isfinite(ref["geodesicFlow"])
     np.testing.assert_array_equal(O.geodesic_flow(res)[fin], ref["geodesicFlow"][fin])
+
+
+GOLDEN_STOPPING = ["stop_riemann2_distance", "stop_riemann2_nmax", "stop_riemann2_any_all", "stop_riemann3_walls_nmax",
+                   "stop_reedsshepp2_unoriented"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_STOPPING)
+def test_stopping_criteria_oracle_matches_reference(name):
+    """stopAtDistance, nMaxAccepted, stopWhenAny/AllAccepted (and _Unoriented): values (accepted
+    and tentative), activeNeighs and nAccepted bit for bit."""
+    params, ref, _ = load_golden(name)
+    res = O.solve(params)
+    np.testing.assert_array_equal(res["values"], ref["values"])
+    np.testing.assert_array_equal(res["activeNeighs"].reshape(res["values"].shape).astype(float), ref["activeNeighs"])
+    assert res["nAccepted"] == int(ref["nAccepted"])
