@@ -1432,6 +1432,7 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
 }
 
 #include "geodesic.cuh"
+#include "stopping.cuh"
 
 struct AdjDev {
     long long N;
@@ -2326,6 +2327,14 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     check_status(status, "solver");
     unsigned long long hs[4] = {0, 0, 0, 0};
     stats.download(hs, 4, s);
+    Stopped<Real> stopped;
+    bool stopping = false;
+    if constexpr (KIND != kKindTTI) {
+        if (ninst == 1 && p0.has_stopping()) {
+            apply_stopping<Real, NFWD, NSYM, KIND>(P, N, p0, values.get(), stopped, s);
+            stopping = true;
+        }
+    }
     DeviceBuffer<unsigned long long> nacc(ninst);
     nacc.zero(s);
     launch(count_finite_kernel<Real>, nblocks(N, 256), 256, 0, s, P, nacc.get());
@@ -2343,6 +2352,15 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     if (want_active) {
         act.alloc(N);
         launch(active_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, P, act.get());
+        if (stopped.on) {  // cells not accepted: the neighbours that were accepted
+            DeviceBuffer<unsigned long long> act2(N);
+            Dev<Real> PM = P;
+            PM.values = stopped.vmask.get();
+            launch(active_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, PM, act2.get());
+            launch(stop_select_kernel, nblocks(N, 256), 256, 0, s, N, (const uint8_t *)stopped.acc.get(),
+                   (const unsigned long long *)act2.get(), act.get());
+            HFM_CUDA(cudaStreamSynchronize(s));
+        }
     }
     for (int i = 0; i < ninst; ++i) {
         const EulerProblem &p = *probs[i];
@@ -2372,7 +2390,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             HFM_CUDA(cudaMemcpyAsync(res.stencil_w.data(), plain_w.get() + off * ND, n * ND * sizeof(double),
                                      cudaMemcpyDeviceToHost, s));
         }
-        res.n_accepted = (int64_t)hn[i];
+        res.n_accepted = stopping ? (int64_t)stopped.count : (int64_t)hn[i];
         res.rounds = (long long)hs[0];
         res.tile_activations = (long long)hs[1];
         res.local_solves = (long long)hs[2];

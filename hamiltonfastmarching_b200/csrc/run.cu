@@ -81,9 +81,7 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
 
 void reject_unsupported(Store &io) {
     static const char *keys[] = {"factoringValues", "speed_times", "cost_times",
-                                 "metric_times", "dualMetric_times", "stopAtDistance", "nMaxAccepted",
-                                 "stopWhenAnyAccepted", "stopWhenAllAccepted", "stopWhenAnyAccepted_Unoriented",
-                                 "stopWhenAllAccepted_Unoriented",
+                                 "metric_times", "dualMetric_times",
                                  "euclideanScale", "seedFlags", "getStencils", "activeNeighs", "values",
                                  "factoringPointChoice"};
     for (const char *k : keys)
@@ -593,6 +591,43 @@ void read_forward_variation(Store &io, const Param &pm, EulerProblem &p) {
     if (p.fwd_nvar <= 0) throw Error(HFM_ERR_VALUE, "Forward variation error : inconsistent input sizes");
 }
 
+// Stopping criteria (CommonStoppingCriteria.h:95-147): targets out of range are dropped with the
+// reference's warning; the _Unoriented forms exist on the lifted models only.
+void read_stopping(Store &io, const Param &pm, bool lifted, EulerProblem &p) {
+    if (io.has_field("nMaxAccepted")) p.stop_n_max = (int64_t)io.get_scalar("nMaxAccepted");
+    auto targets = [&](const char *key, std::vector<int64_t> &out) {
+        if (!io.has_field(key)) return;
+        int64_t n = 0;
+        const std::vector<double> pts = io.get_vector(key, pm.ndim, &n);
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t lin;
+            if (pm.index_of(&pts[i * pm.ndim], &lin)) out.push_back(lin);
+            else io.msg("Warning : target is out of range.");
+        }
+    };
+    targets("stopWhenAnyAccepted", p.stop_any);
+    targets("stopWhenAllAccepted", p.stop_all);
+    auto targets_u = [&](const char *key, std::vector<int64_t> &out) {
+        if (!lifted || !io.has_field(key)) return;
+        int64_t n = 0;
+        const std::vector<double> pts = io.get_vector(key, 2, &n);
+        for (int64_t i = 0; i < n; ++i) {
+            const double q[3] = {pts[2 * i], pts[2 * i + 1], pm.origin[2] + 0.5 * pm.scale[2]};
+            int64_t lin;
+            if (pm.index_of(q, &lin)) out.push_back(lin / pm.dims[2]);
+            else io.msg("Warning : unoriented target is out of range.");
+        }
+    };
+    targets_u("stopWhenAnyAccepted_Unoriented", p.stop_any_u);
+    targets_u("stopWhenAllAccepted_Unoriented", p.stop_all_u);
+    if (io.has_field("stopAtDistance")) {
+        p.has_stop_distance = true;
+        p.stop_distance = io.get_scalar("stopAtDistance");
+    }
+    if (p.has_stopping() && p.kind == StencilKind::TTI)
+        throw Error(HFM_ERR_UNSUPPORTED, "stopping criteria of TTI3 are not supported by the GPU solve path");
+}
+
 // A model read from its store, ready to solve (the part of Run before the solver loop).
 struct Prepared {
     Param pm;
@@ -629,6 +664,7 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     read_walls(io, pm, lifted, p);
     read_seeds(io, pm, p, lifted);
 
+    read_stopping(io, pm, lifted, p);
     read_geodesics(io, pm, lifted, p, q.geo_keys);
     q.export_values = io.get_scalar("exportValues", 0.0, 2) != 0;
     p.retain = io.get_scalar("retainState", 0.0, 3) != 0;
@@ -691,14 +727,17 @@ void export_geodesics(Store &io, const Prepared &q, const EulerResult &r) {
             for (int a = 0; a < D; ++a) tip << (a ? "," : "") << pts[first * D + a];
             tip << "}";
             const int st = r.geo_status[gi][t];
-            if ((st & 1) && q.p.geo_ode) io.msg("Geodesic ODE solver seems to have failed for tip " + tip.str() + ".\n");
-            else if (st & 1) io.msg("Geodesic extraction failed for tip " + tip.str() + "\n");
-            else if (r.geo_restarts[gi][t] > 5) {
+            if (io.verbosity < 1) {
+            } else if ((st & 1) && q.p.geo_ode) {
+                io.msg("Geodesic ODE solver seems to have failed for tip " + tip.str() + ".\n");
+            } else if (st & 1) {
+                io.msg("Geodesic extraction failed for tip " + tip.str() + "\n");
+            } else if (r.geo_restarts[gi][t] > 5) {
                 double vb = q.p.geo_volume_bound;
                 for (int k = 5; k <= r.geo_restarts[gi][t]; ++k) vb *= 1.3;
                 std::ostringstream m;
                 m << "Tip " << tip.str() << " yields " << r.geo_restarts[gi][t] << " restarts, "
-                  << "geodesicVolumeBound increased to " << vb;
+                  << "geodesicVolumeBound increased to " << vb << "\n";
                 io.msg(m.str());
             }
             if (st & ~1)
@@ -994,11 +1033,11 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
         std::vector<int> grp{i};
         done[i] = 1;
         const hfm::EulerProblem &pi = qs[i]->p;
-        if (pi.adjoint_index.empty() && pi.fwd_nvar == 0) {
+        if (pi.adjoint_index.empty() && pi.fwd_nvar == 0 && !pi.has_stopping()) {
             for (int j = i + 1; j < n; ++j) {
                 if (rc[j] != HFM_OK || done[j] || qs[j]->skip) continue;
                 const hfm::EulerProblem &pj = qs[j]->p;
-                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && pj.kind == pi.kind && pj.diagonal == pi.diagonal && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
+                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && !pj.has_stopping() && pj.kind == pi.kind && pj.diagonal == pi.diagonal && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
                     pj.nsym == pi.nsym && pj.fp64 == pi.fp64 && pj.sweeps_per_tile == pi.sweeps_per_tile &&
                     pj.max_rounds == pi.max_rounds) {
                     grp.push_back(j);

@@ -85,6 +85,16 @@ struct EulerProblem {
     // Forward first variation (costVariation, seedValueVariation): fwd_nvar variations; fwd_cost
     // [N][nvar] RowMajor or empty; seed cells and their value variations [n][nvar], later entries
     // overwriting earlier ones.
+    // Stopping criteria (stopAtDistance, nMaxAccepted, stopWhenAny/AllAccepted; the _Unoriented
+    // forms give (x, y) columns packed as x * dims[1] + y); single instances of Eulerian models.
+    bool has_stop_distance = false;
+    double stop_distance = 0.0;
+    int64_t stop_n_max = 0;
+    std::vector<int64_t> stop_any, stop_all, stop_any_u, stop_all_u;
+    bool has_stopping() const {
+        return has_stop_distance || stop_n_max > 0 || !stop_any.empty() || !stop_all.empty() ||
+               !stop_any_u.empty() || !stop_all_u.empty();
+    }
     int fwd_nvar = 0;
     std::vector<double> fwd_cost;
     std::vector<int64_t> fwd_seed_cell;
