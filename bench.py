@@ -432,10 +432,11 @@ def differentiation_leg(args):
 
 def geodesic_leg(args):
     """Geodesic backtracking throughput: Riemann2 1024^2 (anisotropy 8, smooth random orientation,
-    two wall segments, one seed at the centre) with --geo-tips random tips. GPU: the geodesic stage
-    of one run (CUDA events around the warp-per-tip kernel and its copies, `GeodesicCPUTime`), and
-    the whole run through the public call. CPU: the reference's FileHFM_Riemann2 on the same input
-    with --geo-cpu-tips of the tips (its own `GeodesicCPUTime`, one core)."""
+    two wall segments, one seed at the centre) with --geo-tips random tips, discrete solver, then the
+    same tips with the ODE solver. GPU: the geodesic stage of one run (CUDA events around the
+    warp-per-tip kernels and their copies, `GeodesicCPUTime`), and the whole run through the public
+    call. CPU: the reference's FileHFM_Riemann2 on the same input with --geo-cpu-tips of the tips
+    (its own `GeodesicCPUTime`, one core)."""
     import hamiltonfastmarching_b200 as H
     from hamiltonfastmarching_b200 import workloads as W
     n = args.geo_side
@@ -469,6 +470,21 @@ def geodesic_leg(args):
             rk = int(np.sum(ref["geodesicLengths"]))
             res["cpu_baseline"]["points_same_tips"] = {"gpu": gk, "reference": rk}
             res["speedup_tips_per_s_vs_1_core"] = res["tips_per_s"] / (k / cpu_s)
+    # the same tips with the ODE solver (geodesicSolver = 'ODE')
+    qo = dict(q, geodesicSolver="ODE")
+    H.run(qo)
+    out = H.run(qo)
+    ode = {"gpu_geodesic_s": float(out["GeodesicCPUTime"]), "points": int(np.sum(out["geodesicLengths"]))}
+    ode["tips_per_s"] = len(tips) / ode["gpu_geodesic_s"]
+    if "cpu_baseline" in res:
+        ref = run_reference(dict(p, tips=tips[:k], geodesicSolver="ODE", verbosity=0.0, exportValues=0.0))
+        if ref.get("retcode") == 0:
+            cpu_s = float(ref["GeodesicCPUTime"])
+            ode["cpu_baseline"] = {"tips_per_s": k / cpu_s, "cores": 1, "kind": "reference",
+                                   "sample": f"FileHFM_Riemann2, geodesicSolver ODE, first {k} tips: "
+                                             f"GeodesicCPUTime {cpu_s:.3f} s"}
+            ode["speedup_tips_per_s_vs_1_core"] = ode["tips_per_s"] / (k / cpu_s)
+    res["ode"] = ode
     return res
 
 
