@@ -351,7 +351,12 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, const GeoRec &R,
     __syncwarp();
     if (ws == 0) return 0;
     double avg[3] = {0, 0, 0}, base[3] = {0, 0, 0};
-    for (int a = 0; a < D; ++a) { avg[a] = A::div(is[a], ws); base[a] = avg[a]; }
+    // a vector divided by a scalar is multiplied by the reciprocal, as in the reference's vector
+    // types (FriendOperators.h:35, VectorType.h:37-41)
+    {
+        const double iw = A::div(1.0, ws);
+        for (int a = 0; a < D; ++a) { avg[a] = A::mul(is[a], iw); base[a] = avg[a]; }
+    }
     double stepNorm = 0.0;
     int nst = 0;
     double f0[3] = {0, 0, 0}, f1[3] = {0, 0, 0};  // steps beyond the list: sum of s and of s * value
@@ -457,9 +462,10 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, const GeoRec &R,
             return 0;
         }
         double stp[3] = {0, 0, 0}, sq = 0.0;
+        const double iw = A::div(1.0, ws);
         for (int a = 0; a < D; ++a) {
             const double old = avg[a];
-            avg[a] = A::div(is[a], ws);
+            avg[a] = A::mul(is[a], iw);
             stp[a] = A::sub(avg[a], old);
         }
         for (int a = 0; a < D; ++a) sq = A::add(sq, A::mul(stp[a], stp[a]));
@@ -488,17 +494,17 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, const GeoRec &R,
         const double valInc = A::sub(S.sv[0], bv);
         if (valInc <= 0) continue;
         const double delta = A::div(valInc, (double)D);
-        const double den = A::add(valInc, delta);
+        const double rden = A::div(1.0, A::add(valInc, delta));
         double pt[3];
         for (int a = 0; a < D; ++a) pt[a] = base[a];
         const int nl = nst < SCAP ? nst : SCAP;
         for (int k = 0; k < nl; ++k) {
             const double cf = A::add(A::sub(S.sv[k], bv), delta);
-            for (int a = 0; a < D; ++a) pt[a] = A::add(pt[a], A::div(A::mul(S.sd[k][a], cf), den));
+            for (int a = 0; a < D; ++a) pt[a] = A::add(pt[a], A::mul(A::mul(S.sd[k][a], cf), rden));
         }
         if (nst > SCAP)  // steps past the list, summed: sum s (v - value + delta) / den
             for (int a = 0; a < D; ++a)
-                pt[a] = A::add(pt[a], A::div(A::add(f1[a], A::mul(A::sub(delta, bv), f0[a])), den));
+                pt[a] = A::add(pt[a], A::mul(A::add(f1[a], A::mul(A::sub(delta, bv), f0[a])), rden));
         for (int a = 0; a < D; ++a) { pt[a] = A::add(pt[a], 0.5); base[a] = avg[a]; }
         if (!emit(pt)) return 0;
         stepNorm = 0;
@@ -508,7 +514,7 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, const GeoRec &R,
         double V[3][3];
         for (int i = 0; i < D; ++i)
             for (int j = 0; j <= i; ++j) {
-                V[i][j] = A::add(A::sub(A::div(cs[i][j], ws), A::mul(A::div(is[i], ws), A::div(is[j], ws))),
+                V[i][j] = A::add(A::sub(A::mul(cs[i][j], iw), A::mul(A::mul(is[i], iw), A::mul(is[j], iw))),
                                  i == j ? 1.0 : 0.0);
                 V[j][i] = V[i][j];
             }
@@ -752,8 +758,10 @@ __device__ void ode_flow_at(const Dev<Real> &P, const Inst &I, int D, const int8
             for (int a = 0; a < D; ++a) flow[a] = A::add(flow[a], A::mul(wi, f[a]));
         }
     }
-    if (ws > 0)
-        for (int a = 0; a < D; ++a) flow[a] = A::div(flow[a], ws);
+    if (ws > 0) {
+        const double iw = A::div(1.0, ws);
+        for (int a = 0; a < D; ++a) flow[a] = A::mul(flow[a], iw);
+    }
 }
 
 // One warp per ODE tip (Run, GeodesicODESolver.hxx:159-212); the warp's count table has
@@ -813,7 +821,8 @@ geodesic_ode_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, Geo
                 if (nrm == 0) break;  // at a seed
                 const double half = A::mul(0.5, tp.step);
                 double q[3] = {p[0], p[1], p[2]};
-                for (int a = 0; a < D; ++a) q[a] = A::add(p[a], A::div(A::mul(half, f[a]), nrm));
+                const double inv = A::div(1.0, nrm);
+                for (int a = 0; a < D; ++a) q[a] = A::add(p[a], A::mul(A::mul(half, f[a]), inv));
                 ode_flow_at<Real>(P, I, D, wd, target, rec, keys, counts, tmask, tp.causality, q, f, nstat, tol,
                                   status);
                 if (status) break;
@@ -822,7 +831,8 @@ geodesic_ode_kernel(Dev<Real> P, const GeoTip *tips, int ntips, double *pts, Geo
                 nrm = A::sqrt(nrm);
                 if (nrm == 0) break;
                 if (len >= tp.cap) { status |= kGeoPointOverflow; break; }
-                for (int a = 0; a < D; ++a) p[a] = A::add(p[a], A::div(A::mul(tp.step, f[a]), nrm));
+                const double inv2 = A::div(1.0, nrm);
+                for (int a = 0; a < D; ++a) p[a] = A::add(p[a], A::mul(A::mul(tp.step, f[a]), inv2));
                 if (lane == 0)
                     for (int a = 0; a < D; ++a) out[(long long)len * D + a] = p[a];
                 ++len;

@@ -13,6 +13,8 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <limits>
+#include <set>
 #include <sstream>
 
 #include "common.cuh"
@@ -97,7 +99,130 @@ void reject_unsupported(Store &io) {
         throw Error(HFM_ERR_UNSUPPORTED, "refineStencilAtWallBoundary is not supported by the GPU solve path");
 }
 
-// Seeds: points -> unique indices (first value kept), sorted; seedRadius must be 0.
+// Distance guess of the seed spreading (StaticFactoring.hxx:285-346): the model's norm at a cell,
+// or interpolated at a point over its 2^D grid neighbours with the reference's unnormalised
+// weights (BaseGrid.h:79-101, PeriodicGrid.hxx Neighbors, MapWeightedSum.h): a symmetric matrix
+// in grid units for Riemann metrics (Riemannian.h:62-71: the metric, inverted if dual, times
+// h_i h_j), a diagonal d_i = h_i / speed_i for the isotropic and diagonal models (Isotropic.h).
+struct SeedGuess {
+    const EulerProblem &p;
+    const Param &pm;
+    int ns() const { return p.kind == StencilKind::RiemannPerCell && !p.diagonal ? pm.ndim * (pm.ndim + 1) / 2 : pm.ndim; }
+    // raw model data at a cell: packed metric, speed vector (diagonal) or speed (isotropic)
+    void raw(int64_t cell, double *out) const {
+        const int D = pm.ndim;
+        if (p.kind == StencilKind::RiemannPerCell) {
+            const int n = ns();
+            const double *src = p.metric_ptr ? p.metric_ptr : p.metric.data();
+            const double *m = src + (p.metric_constant ? 0 : cell * n);
+            for (int k = 0; k < n; ++k) out[k] = (p.diagonal && p.mult_inverse) ? 1.0 / m[k] : m[k];
+        } else {
+            const double *src = p.mult_ptr ? p.mult_ptr : p.mult.data();
+            const double v = src[p.mult_depth == 0 ? 0 : cell];
+            out[0] = p.mult_inverse ? 1.0 / v : v;
+            (void)D;
+        }
+    }
+    // the norm from interpolated or cell data: Riemann matrices rescaled to grid units
+    void finish(const double *in, double *norm) const {
+        const int D = pm.ndim;
+        if (p.kind == StencilKind::RiemannPerCell && !p.diagonal) {
+            double m[6];
+            for (int k = 0; k < ns(); ++k) m[k] = in[k];
+            if (p.dual) {  // Inverse = Comatrix / Determinant (SymmetricMatrixType.hxx:201-242)
+                auto c = [&](int i, int j) { return i >= j ? m[i * (i + 1) / 2 + j] : m[j * (j + 1) / 2 + i]; };
+                double co[6], det;
+                if (D == 2) {
+                    co[0] = c(1, 1); co[1] = -c(1, 0); co[2] = c(0, 0);
+                    det = c(0, 0) * c(1, 1) - c(1, 0) * c(0, 1);
+                } else {
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j <= i; ++j) {
+                            const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                            co[i * (i + 1) / 2 + j] = c(i1, j1) * c(i2, j2) - c(i1, j2) * c(i2, j1);
+                        }
+                    det = c(0, 0) * (c(1, 1) * c(2, 2) - c(1, 2) * c(2, 1)) +
+                          c(0, 1) * (2. * c(1, 2) * c(2, 0) - c(1, 0) * c(2, 2)) - c(0, 2) * (c(1, 1) * c(2, 0));
+                }
+                const double idet = 1. / det;  // matrix / scalar multiplies by the reciprocal
+                for (int k = 0; k < ns(); ++k) m[k] = co[k] * idet;
+            }
+            for (int i = 0; i < D; ++i)
+                for (int j = 0; j <= i; ++j) m[i * (i + 1) / 2 + j] *= pm.scale[i] * pm.scale[j];
+            for (int k = 0; k < ns(); ++k) norm[k] = m[k];
+        } else if (p.diagonal) {
+            for (int i = 0; i < D; ++i) norm[i] = pm.scale[i] / in[i];
+        } else {
+            for (int i = 0; i < D; ++i) norm[i] = pm.scale[i] / in[0];
+        }
+    }
+    double apply(const double *norm, const double *v) const {
+        const int D = pm.ndim;
+        if (p.kind == StencilKind::RiemannPerCell && !p.diagonal) {  // sqrt(<v, M v>)
+            auto c = [&](int i, int j) { return i >= j ? norm[i * (i + 1) / 2 + j] : norm[j * (j + 1) / 2 + i]; };
+            double sum = 0.;
+            for (int i = 0; i < D; ++i) {
+                double si = 0.;
+                for (int j = 0; j < D; ++j) si += c(i, j) * v[j];
+                sum += v[i] * si;
+            }
+            return std::sqrt(sum);
+        }
+        double s = 0.;
+        for (int i = 0; i < D; ++i) s += (norm[i] * v[i]) * (norm[i] * v[i]);
+        return std::sqrt(s);
+    }
+    bool cell_of(const int64_t *idx, int64_t *lin) const {
+        int64_t r = 0;
+        for (int a = 0; a < pm.ndim; ++a) {
+            if (idx[a] < 0 || idx[a] >= pm.dims[a]) return false;
+            r = r * pm.dims[a] + idx[a];
+        }
+        *lin = r;
+        return true;
+    }
+    void at_cell(const int64_t *idx, double *norm) const {
+        int64_t lin;
+        cell_of(idx, &lin);
+        double d[6];
+        raw(lin, d);
+        finish(d, norm);
+    }
+    void at_point(const double *q, double *norm) const {
+        const int D = pm.ndim, n = ns();
+        int64_t nearest[3];
+        int dir[3];
+        double w[3];
+        for (int i = 0; i < D; ++i) {
+            nearest[i] = (int64_t)std::floor(q[i]);
+            const double diff = q[i] - nearest[i] - 0.5;
+            dir[i] = diff > 0 ? 1 : -1;
+            w[i] = std::abs(diff);
+        }
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < (1 << D); ++i) {
+            int64_t idx[3];
+            double wt = 1.;
+            for (int j = 0; j < D; ++j) {
+                idx[j] = nearest[j];
+                if ((i >> j) & 1) { wt *= w[j]; idx[j] += dir[j]; }
+                else wt *= 1. - w[j];
+            }
+            int64_t lin = 0;
+            const bool inside = cell_of(idx, &lin);
+            if (!inside) wt = 0.;
+            if (i > 0 && wt == 0) continue;  // the first term is always evaluated (MapWeightedSum.h)
+            double d[6] = {0, 0, 0, 0, 0, 0};
+            if (inside) raw(lin, d);
+            for (int k = 0; k < n; ++k) acc[k] = i == 0 ? wt * d[k] : acc[k] + wt * d[k];
+        }
+        finish(acc, norm);
+    }
+};
+
+// Seeds: points -> unique indices (first value kept), sorted; with seedRadius > 0 each seed is
+// spread to the cells whose centre lies within that many cells of it (StaticFactoring.hxx:242-346).
+
 void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_allowed) {
     std::map<int64_t, double> seeds;
     std::vector<double> pts;
@@ -111,7 +236,53 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
             if (nv != n) throw Error(HFM_ERR_VALUE, "Error : Inconsistent size of seedValues.");
         }
         const double radius = io.get_scalar("seedRadius", 0.0);
-        if (radius != 0) throw Error(HFM_ERR_UNSUPPORTED, "seedRadius != 0 is not supported by the GPU solve path");
+        if (radius < 0)
+            throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 (stencil-step spreading) is not supported by the GPU solve path");
+        if (radius > 0) {
+            const bool guessable = p.kind == StencilKind::RiemannPerCell ||
+                                   (p.kind == StencilKind::SharedByTheta && !p.angular);
+            if (!guessable)
+                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius > 0 is supported for the Riemann, Isotropic and Diagonal models only");
+            const int D = pm.ndim;
+            SeedGuess G{p, pm};
+            std::vector<double> npts, nvals;
+            const int bd = 1 + (int)std::ceil(radius);
+            const int side = 1 + 2 * bd;
+            int64_t box = 1;
+            for (int a = 0; a < D; ++a) box *= side;
+            for (int64_t i = 0; i < n; ++i) {
+                double q[3];
+                for (int a = 0; a < D; ++a) q[a] = (pts[i * D + a] - pm.origin[a]) / pm.scale[a];  // ADim
+                std::set<std::vector<int64_t>> seen;
+                double distp[6];
+                G.at_point(q, distp);
+                auto insert = [&](const int64_t *index, double rad) {
+                    double v[3], nn = 0.;
+                    for (int a = 0; a < D; ++a) { v[a] = q[a] - ((double)index[a] + 0.5); nn += v[a] * v[a]; }
+                    if (std::sqrt(nn) >= rad) return;
+                    if (!seen.insert(std::vector<int64_t>(index, index + D)).second) return;
+                    int64_t lin;
+                    if (!G.cell_of(index, &lin)) return;
+                    double distq[6];
+                    G.at_cell(index, distq);
+                    for (int a = 0; a < D; ++a) npts.push_back(((double)index[a] + 0.5) * pm.scale[a] + pm.origin[a]);
+                    nvals.push_back(vals[i] + 0.5 * (G.apply(distp, v) + G.apply(distq, v)));
+                };
+                int64_t pidx[3];
+                for (int a = 0; a < D; ++a) pidx[a] = (int64_t)std::floor(q[a]);
+                insert(pidx, std::numeric_limits<double>::infinity());
+                for (int64_t k = 0; k < box; ++k) {  // the box of offsets, RowMajor
+                    int64_t idx[3], r = k;
+                    for (int a = D - 1; a >= 0; --a) { idx[a] = pidx[a] + (r % side) - bd; r /= side; }
+                    insert(idx, radius);
+                }
+            }
+            io.set_vector("spreadedSeeds", (int64_t)nvals.size(), D, npts.data());
+            io.set_vector("spreadedSeedValues", (int64_t)nvals.size(), 1, nvals.data());
+            pts.swap(npts);
+            vals.swap(nvals);
+            n = (int64_t)vals.size();
+        }
         for (int64_t i = 0; i < n; ++i) {
             int64_t lin;
             if (!pm.index_of(&pts[i * pm.ndim], &lin)) {

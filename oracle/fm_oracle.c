@@ -1552,7 +1552,8 @@ static int geo_discrete_pass(geo_run *G, double vbound) {
         geo_add(&S, D, weight, ind);
     }
     if (S.ws == 0) goto done;
-    for (int a = 0; a < D; ++a) { avg[a] = S.is[a] / S.ws; base[a] = avg[a]; }
+    /* vector / scalar multiplies by the reciprocal (FriendOperators.h:35, VectorType.h:37-41) */
+    { const double iw = 1.0 / S.ws; for (int a = 0; a < D; ++a) { avg[a] = S.is[a] * iw; base[a] = avg[a]; } }
     while (ns > 0 && S.ws > 1e-5) {
         int64_t best = 0;
         for (int64_t k = 1; k < ns; ++k)
@@ -1600,9 +1601,10 @@ static int geo_discrete_pass(geo_run *G, double vbound) {
             goto done;
         }
         double step[3] = {0, 0, 0}, sq = 0.0;
+        const double iw = 1.0 / S.ws;
         for (int a = 0; a < D; ++a) {
             const double old = avg[a];
-            avg[a] = S.is[a] / S.ws;
+            avg[a] = S.is[a] * iw;
             step[a] = avg[a] - old;
         }
         for (int a = 0; a < D; ++a) sq += step[a] * step[a];
@@ -1628,10 +1630,11 @@ static int geo_discrete_pass(geo_run *G, double vbound) {
         const double valInc = sv[0] - e.val;
         if (valInc <= 0) continue;
         const double delta = valInc / D;
+        const double rden = 1.0 / (valInc + delta);
         double pt[3];
         for (int a = 0; a < D; ++a) pt[a] = base[a];
         for (int64_t k = 0; k < nst; ++k)
-            for (int a = 0; a < D; ++a) pt[a] += sd[k][a] * (sv[k] - e.val + delta) / (valInc + delta);
+            for (int a = 0; a < D; ++a) pt[a] += (sd[k][a] * (sv[k] - e.val + delta)) * rden;
         for (int a = 0; a < D; ++a) { pt[a] += 0.5; base[a] = avg[a]; }
         geo_push(G, pt);
         stepNorm = 0; nst = 0;
@@ -1639,7 +1642,7 @@ static int geo_discrete_pass(geo_run *G, double vbound) {
         double V[3][3];
         for (int i = 0; i < D; ++i)
             for (int j = 0; j <= i; ++j) {
-                V[i][j] = S.cs[i][j] / S.ws - (S.is[i] / S.ws) * (S.is[j] / S.ws) + (i == j ? 1.0 : 0.0);
+                V[i][j] = S.cs[i][j] * iw - (S.is[i] * iw) * (S.is[j] * iw) + (i == j ? 1.0 : 0.0);
                 V[j][i] = V[i][j];
             }
         double det;
@@ -1956,7 +1959,10 @@ static int ode_flow_at(const fmo_problem *p, geo_flow_fn flow, void *ctx, const 
         }
     }
     if (ws > 0)
-        for (int a = 0; a < D; ++a) out->flow[a] /= ws;
+    {
+        const double iw = 1.0 / ws;
+        for (int a = 0; a < D; ++a) out->flow[a] *= iw;
+    }
     return 0;
 }
 
@@ -1987,14 +1993,16 @@ static int ode_run(const fmo_problem *p, geo_flow_fn flow, void *ctx, const int1
         nrm = sqrt(nrm);
         if (nrm == 0) break;
         double q[3];
-        for (int a = 0; a < D; ++a) q[a] = pt[a] + 0.5 * step * fd.flow[a] / nrm;
+        const double inv = 1.0 / nrm;
+        for (int a = 0; a < D; ++a) q[a] = pt[a] + (0.5 * step * fd.flow[a]) * inv;
         if (ode_flow_at(p, flow, ctx, target, &cache, causality, q, &fd)) { ret = -1; break; }
         nrm = 0.0;
         for (int a = 0; a < D; ++a) nrm += fd.flow[a] * fd.flow[a];
         nrm = sqrt(nrm);
         if (nrm == 0) break;
         if (*len >= cap) { ret = -2; break; }
-        for (int a = 0; a < D; ++a) pts[*len * D + a] = pt[a] + step * fd.flow[a] / nrm;
+        const double inv2 = 1.0 / nrm;
+        for (int a = 0; a < D; ++a) pts[*len * D + a] = pt[a] + (step * fd.flow[a]) * inv2;
         ++*len;
     }
     free(hist);

@@ -230,6 +230,26 @@ def stopping_fixtures():
     solve_fixture("stop_reedsshepp2_unoriented", dict(c, stopWhenAnyAccepted_Unoriented=np.array([[0.8, 0.2]])))
 
 
+def spreading_fixtures():
+    """seedRadius > 0: seeds spread to the cells within that many cells, with values from the
+    model's norm at the seed and at the cell (spreadedSeeds, spreadedSeedValues)."""
+    rng = np.random.default_rng(4)
+    p = W.riemann2_case(40, aniso=6.0, seed=5, n_seeds=2)
+    m = p.pop("metric")
+    solve_fixture("spread_riemann2_dual", dict(p, dualMetric=m, seedRadius=1.5))
+    p3 = W.riemann3_case(16, n_spheres=2, n_seeds=2, rmin=0.1, rmax=0.2, seed=22)
+    solve_fixture("spread_riemann3_walls", dict(p3, seedRadius=2.0))
+    n = 30
+    solve_fixture("spread_isotropic2", {"model": "Isotropic2", "arrayOrdering": "RowMajor",
+                                        "dims": np.array([n, n], float), "gridScale": 1.0 / n,
+                                        "cost": 1 + rng.random((n, n)), "seeds": np.array([[0.31, 0.52], [0.01, 0.5]]),
+                                        "seedRadius": 3.0, "exportValues": 1.0})
+    solve_fixture("spread_diagonal3", {"model": "Diagonal3", "arrayOrdering": "RowMajor",
+                                       "dims": np.array([12, 10, 8], float), "gridScales": np.array([0.1, 0.12, 0.15]),
+                                       "speed": 0.5 + rng.random((12, 10, 8, 3)), "seeds": np.array([[0.55, 0.61, 0.33]]),
+                                       "seedRadius": 2.2, "exportValues": 1.0})
+
+
 def variation_fixtures():
     """Forward first variation (costVariation, seedValueVariation -> valueVariation)."""
     rng = np.random.default_rng(2025)
@@ -280,7 +300,7 @@ def isotropic_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
@@ -293,6 +313,8 @@ if __name__ == "__main__":
         ode_fixtures()
     elif sys.argv[1:] == ["stopping"]:
         stopping_fixtures()
+    elif sys.argv[1:] == ["spreading"]:
+        spreading_fixtures()
     else:
         main()
         tti_fixtures()
@@ -301,3 +323,4 @@ if __name__ == "__main__":
         isotropic_fixtures()
         ode_fixtures()
         stopping_fixtures()
+        spreading_fixtures()

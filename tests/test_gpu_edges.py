@@ -64,3 +64,17 @@ def test_full_size_riemann2_1024_matches_oracle():
 def test_full_size_reedsshepp2_128x60_matches_oracle():
     p = W.curvature2_case(128, 60, "ReedsShepp2", seed=2)
     assert _rel(hfm.run(p)["values"], O.solve(p, with_active=False)["values"]) <= RTOL
+
+
+@pytest.mark.parametrize("name", ["spread_riemann2_dual", "spread_riemann3_walls", "spread_isotropic2",
+                                  "spread_diagonal3"])
+def test_spread_seeds_solve_matches_reference(name):
+    """Solve from seeds spread by seedRadius: values within 1e-10 of the reference's."""
+    from conftest import load_golden
+    params, ref, _ = load_golden(name)
+    out = hfm.run(dict(params))
+    a, b = out["values"], ref["values"]
+    fin = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), fin)
+    assert np.max(np.abs(a[fin] - b[fin])) <= 1e-10 * np.max(np.abs(b[fin]))
+    assert int(out["nAccepted"]) == int(ref["nAccepted"])

@@ -79,8 +79,8 @@ GOLDEN_GEODESICS = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reeds
 @pytest.mark.parametrize("name", GOLDEN_GEODESICS)
 def test_geodesic_oracle_matches_reference(name):
     """Geodesics (discrete and ODE solvers; tips, tips_Unoriented) and the geodesic flow of the
-    oracle against the reference executable: same lengths, points within 1e-12 (relative to the
-    domain size), flow within 1e-12 of its largest entry."""
+    oracle against the reference executable: same lengths, points bit for bit (TTI3 within 1e-14 of
+    the domain size), flow within 1e-12 of its largest entry."""
     params, ref, _ = load_golden(name)
     res = O.tti_solve(params) if params["model"] == "TTI3" else O.solve(params)
     geo = O.geodesics(res, params)
@@ -88,8 +88,11 @@ def test_geodesic_oracle_matches_reference(name):
         if "geodesicPoints" + suffix not in ref:
             continue
         np.testing.assert_array_equal(geo["geodesicLengths" + suffix], ref["geodesicLengths" + suffix])
-        scale = np.max(np.abs(ref["geodesicPoints" + suffix]))
-        assert np.max(np.abs(geo["geodesicPoints" + suffix] - ref["geodesicPoints" + suffix])) <= 1e-12 * scale
+        if params["model"] == "TTI3":  # the extremum over t comes from an iterative search
+            scale = np.max(np.abs(ref["geodesicPoints" + suffix]))
+            assert np.max(np.abs(geo["geodesicPoints" + suffix] - ref["geodesicPoints" + suffix])) <= 1e-14 * scale
+        else:
+            np.testing.assert_array_equal(geo["geodesicPoints" + suffix], ref["geodesicPoints" + suffix])
         if name != "ode_riemann3_16_walls":  # its last tip stalls, for the reference too
             assert not geo["geodesicFailed" + suffix].any()
     if "geodesicFlow" not in ref:

@@ -1,0 +1,37 @@
+"""seedRadius > 0 (StaticFactoring.hxx:242-346): the library spreads each seed to the cells whose
+centre lies within seedRadius cells of it, with values from the model's norm at the seed
+(interpolated) and at the cell. The spreading is host work done while the store is read, before
+any device work, so it is checked here on the CPU against the reference's spreadedSeeds and
+spreadedSeedValues, bit for bit; the GPU solve from the spread seeds is in test_gpu_edges.py."""
+import numpy as np
+import pytest
+
+import hamiltonfastmarching_b200 as H
+from conftest import load_golden
+
+SPREAD = ["spread_riemann2_dual", "spread_riemann3_walls", "spread_isotropic2", "spread_diagonal3"]
+
+
+@pytest.mark.parametrize("name", SPREAD)
+def test_spread_seeds_match_reference(name):
+    params, ref, _ = load_golden(name)
+    io = H.HFMIO("RowMajor")
+    io.set_dict(dict(params, verbosity=0.0))
+    try:
+        io.run()  # on a machine without a GPU the solve fails after the seeds were spread
+    except H.PyExp:
+        pass
+    np.testing.assert_array_equal(io.get_array("spreadedSeeds"), ref["spreadedSeeds"])
+    np.testing.assert_array_equal(io.get_array("spreadedSeedValues"), ref["spreadedSeedValues"])
+
+
+def test_negative_radius_and_lifted_models_refused():
+    params, _, _ = load_golden("spread_isotropic2")
+    with pytest.raises(H.PyExp) as e:
+        H.run(dict(params, seedRadius=-2.0, verbosity=0.0))
+    assert e.value.code == 3
+    p = {"model": "ReedsShepp2", "dims": np.array([8., 8., 8.]), "gridScale": 0.125, "cost": 1.0,
+         "seeds": np.array([[0.5, 0.5, 0.0]]), "seedRadius": 2.0, "verbosity": 0.0}
+    with pytest.raises(H.PyExp) as e:
+        H.run(p)
+    assert e.value.code == 3
