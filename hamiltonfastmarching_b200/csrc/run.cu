@@ -84,7 +84,7 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
 void reject_unsupported(Store &io) {
     static const char *keys[] = {"factoringValues", "speed_times", "cost_times",
                                  "metric_times", "dualMetric_times",
-                                 "euclideanScale", "seedFlags", "getStencils", "activeNeighs", "values",
+                                 "euclideanScale", "seedFlags", "getStencils",
                                  "factoringPointChoice"};
     for (const char *k : keys)
         if (io.has_field(k))
@@ -844,7 +844,33 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     p.want_active = q.export_active;
 
     q.dims.assign(pm.dims, pm.dims + pm.ndim);
-    if (p.seed_index.empty()) {
+    // values and activeNeighs given: the solve is bypassed (HFMInterface.hxx:399-427); the cells
+    // without an active neighbour (the seeds of the run that produced them) are fixed, since the
+    // reference's Recompute gives them no flow
+    if (io.has_field("values") || io.has_field("activeNeighs")) {
+        if (!(io.has_field("values") && io.has_field("activeNeighs")))
+            throw Error(HFM_ERR_UNSUPPORTED, "values without activeNeighs (or the converse) is not supported by the GPU solve path");
+        const Field fv = io.get_field("values", pm.ndim, 1), fa = io.get_field("activeNeighs", pm.ndim, 1);
+        for (int a = 0; a < pm.ndim; ++a)
+            if (fv.dims[a] != pm.dims[a] || fa.dims[a] != pm.dims[a])
+                throw Error(HFM_ERR_VALUE, "values and activeNeighs must have the domain's dims");
+        const size_t n = fv.size();
+        p.bypass = true;
+        p.bypass_values.assign(fv.ptr(), fv.ptr() + n);
+        p.seed_index.clear();
+        p.seed_value.clear();
+        const double *act = fa.ptr();
+        const bool tti = p.kind == StencilKind::TTI;
+        for (size_t x = 0; x < n; ++x) {
+            const bool none = tti ? !(act[x] < std::numeric_limits<double>::infinity()) : act[x] == 0.0;
+            if (none && p.bypass_values[x] < std::numeric_limits<double>::infinity()) {
+                p.seed_index.push_back((int64_t)x);
+                p.seed_value.push_back(p.bypass_values[x]);
+            }
+        }
+        if (io.verbosity >= 1) io.msg("Bypassing fast marching solver based on cached data.\n");
+    }
+    if (p.seed_index.empty() && !p.bypass) {
         io.warn("No seeds to run fast marching solver, and missing values or activeNeighs to compute geodesics.\n");
         q.skip = true;
         return;
@@ -1204,11 +1230,12 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
         std::vector<int> grp{i};
         done[i] = 1;
         const hfm::EulerProblem &pi = qs[i]->p;
-        if (pi.adjoint_index.empty() && pi.fwd_nvar == 0 && !pi.has_stopping()) {
+        if (pi.adjoint_index.empty() && pi.fwd_nvar == 0 && !pi.has_stopping() && !pi.bypass) {
             for (int j = i + 1; j < n; ++j) {
                 if (rc[j] != HFM_OK || done[j] || qs[j]->skip) continue;
                 const hfm::EulerProblem &pj = qs[j]->p;
-                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && !pj.has_stopping() && pj.kind == pi.kind && pj.diagonal == pi.diagonal && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
+                if (pj.adjoint_index.empty() && pj.fwd_nvar == 0 && !pj.has_stopping() && !pj.bypass &&
+                    pj.kind == pi.kind && pj.diagonal == pi.diagonal && pj.ndim == pi.ndim && pj.nfwd == pi.nfwd &&
                     pj.nsym == pi.nsym && pj.fp64 == pi.fp64 && pj.sweeps_per_tile == pi.sweeps_per_tile &&
                     pj.max_rounds == pi.max_rounds) {
                     grp.push_back(j);

@@ -95,6 +95,10 @@ struct EulerProblem {
         return has_stop_distance || stop_n_max > 0 || !stop_any.empty() || !stop_all.empty() ||
                !stop_any_u.empty() || !stop_all_u.empty();
     }
+    // Bypass of the solve (values and activeNeighs given, HFMInterface.hxx:399-427): the arrival
+    // times are taken as given [N] (geodesics and first variations are computed from them).
+    bool bypass = false;
+    std::vector<double> bypass_values;
     int fwd_nvar = 0;
     std::vector<double> fwd_cost;
     std::vector<int64_t> fwd_seed_cell;

@@ -59,3 +59,18 @@ def test_stopping_edge_cases_match_oracle():
         assert np.array_equal(np.isfinite(a), fin)
         if fin.any():
             assert np.max(np.abs(a[fin] - b[fin])) <= 1e-10 * max(1.0, np.max(np.abs(b[fin])))
+
+
+@pytest.mark.parametrize("solver", ["Discrete", "ODE"])
+def test_bypass_from_previous_values(solver):
+    """values and activeNeighs of a previous run given back (the reference's bypass of the solve,
+    HFMInterface.hxx:399-427): the geodesics equal those computed in the run itself."""
+    p = dict(_case(), exportValues=1.0, exportActiveNeighs=1.0, verbosity=0.0)
+    tips = np.array([[0.9, 0.1], [0.15, 0.85], [0.6, 0.95]])
+    first = hfm.run(dict(p, tips=tips, geodesicSolver=solver))
+    q = {k: v for k, v in p.items() if k not in ("seeds", "exportActiveNeighs")}
+    again = hfm.run(dict(q, values=np.array(first["values"]), activeNeighs=np.array(first["activeNeighs"]),
+                         tips=tips, geodesicSolver=solver))
+    np.testing.assert_array_equal(again["geodesicLengths"], first["geodesicLengths"])
+    np.testing.assert_array_equal(again["geodesicPoints"], first["geodesicPoints"])
+    np.testing.assert_array_equal(again["values"], first["values"])
