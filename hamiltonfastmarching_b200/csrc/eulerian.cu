@@ -2344,11 +2344,9 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     stats.download(hs, 4, s);
     Stopped<Real> stopped;
     bool stopping = false;
-    if constexpr (KIND != kKindTTI) {
-        if (ninst == 1 && p0.has_stopping()) {
-            apply_stopping<Real, NFWD, NSYM, KIND>(P, N, p0, values.get(), stopped, s);
-            stopping = true;
-        }
+    if (ninst == 1 && p0.has_stopping()) {
+        apply_stopping<Real, NFWD, NSYM, KIND>(P, N, p0, values.get(), stopped, s);
+        stopping = true;
     }
     DeviceBuffer<unsigned long long> nacc(ninst);
     nacc.zero(s);

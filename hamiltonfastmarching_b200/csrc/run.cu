@@ -795,8 +795,6 @@ void read_stopping(Store &io, const Param &pm, bool lifted, EulerProblem &p) {
         p.has_stop_distance = true;
         p.stop_distance = io.get_scalar("stopAtDistance");
     }
-    if (p.has_stopping() && p.kind == StencilKind::TTI)
-        throw Error(HFM_ERR_UNSUPPORTED, "stopping criteria of TTI3 are not supported by the GPU solve path");
 }
 
 // A model read from its store, ready to solve (the part of Run before the solver loop).

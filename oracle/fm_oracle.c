@@ -1176,10 +1176,23 @@ int fmo_tti_norm(const double *metric, const double *h, double *out) {
     return 0;
 }
 
+int64_t fmo_tti_fast_marching_stop(const int64_t *dims, const double *h, const double *metric, int nseeds,
+                                   const int64_t *seed_index, const double *seed_value, double *values,
+                                   double *t_active, const fmo_problem *stop);
+
 int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double *metric, int nseeds,
                               const int64_t *seed_index, const double *seed_value, double *values,
                               double *t_active) {
+    return fmo_tti_fast_marching_stop(dims, h, metric, nseeds, seed_index, seed_value, values, t_active, NULL);
+}
+
+/* With the stopping criteria of `stop` (its stop_* fields only; NULL: none), as the Eulerian loop. */
+int64_t fmo_tti_fast_marching_stop(const int64_t *dims, const double *h, const double *metric, int nseeds,
+                                   const int64_t *seed_index, const double *seed_value, double *values,
+                                   double *t_active, const fmo_problem *stop) {
     const int64_t N = dims[0] * dims[1] * dims[2];
+    uint8_t *all_left = NULL;
+    int64_t n_all = 0;
     tti_norm *norms = (tti_norm *)malloc(N * sizeof(tti_norm));
     uint8_t *accepted = (uint8_t *)calloc(N, 1), *seed = (uint8_t *)calloc(N, 1);
     enum { CAP = 64 };
@@ -1222,11 +1235,24 @@ int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double
     }
     tti_fm_ctx ctx = {dims, values, accepted};
     int64_t nacc = 0;
+    if (stop && stop->nstop_all > 0) {
+        all_left = (uint8_t *)calloc(N, 1);
+        if (!all_left) goto done;
+        for (int i = 0; i < stop->nstop_all; ++i)
+            if (!all_left[stop->stop_all[i]]) { all_left[stop->stop_all[i]] = 1; ++n_all; }
+    }
     while (h_.n > 0) {
         const qelem top = heap_pop(&h_);
         if (accepted[top.idx] || top.val != values[top.idx]) continue;
-        accepted[top.idx] = 1;
         ++nacc;
+        if (stop) {  /* CommonStoppingCriteria::PostProcess (CommonStoppingCriteria.h:58-93) */
+            int halt = stop->n_max_accepted > 0 && nacc >= stop->n_max_accepted;
+            for (int i = 0; !halt && i < stop->nstop_any; ++i) halt = stop->stop_any[i] == top.idx;
+            if (!halt && all_left && all_left[top.idx]) { all_left[top.idx] = 0; halt = --n_all == 0; }
+            if (!halt && stop->has_stop_at_distance && values[top.idx] > stop->stop_at_distance) halt = 1;
+            if (halt) break;
+        }
+        accepted[top.idx] = 1;
         for (int64_t k = rcount[top.idx]; k < rcount[top.idx + 1]; ++k) {
             const int64_t y = rcell[k];
             if (accepted[y] || seed[y]) continue;
@@ -1244,7 +1270,7 @@ int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double
     }
     ret = nacc;
 done:
-    free(norms); free(accepted); free(seed); free(nb); free(rcount); free(rcell); free(h_.a);
+    free(norms); free(accepted); free(seed); free(nb); free(rcount); free(rcell); free(h_.a); free(all_left);
     return ret;
 }
 

@@ -86,6 +86,10 @@ int fmo_visibility(const fmo_problem *p, int max_width, uint8_t *visible);
 int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double *metric, int nseeds,
                               const int64_t *seed_index, const double *seed_value, double *values,
                               double *t_active);
+/* The same with stopping criteria: the stop_* fields of `stop` (NULL: none). */
+int64_t fmo_tti_fast_marching_stop(const int64_t *dims, const double *h, const double *metric, int nseeds,
+                                   const int64_t *seed_index, const double *seed_value, double *values,
+                                   double *t_active, const fmo_problem *stop);
 /* Reverse first variation of the TTI3 solve (semi-Lagrangian ValueVariation), from the values and
  * t_active of fmo_tti_fast_marching. Returns the number of sensitive seeds, or -1. */
 int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const double *metric,

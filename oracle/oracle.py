@@ -83,6 +83,8 @@ def lib():
         L.fmo_visibility.argtypes = [ctypes.POINTER(_Problem), ctypes.c_int, _P]
         L.fmo_tti_fast_marching.argtypes = [_P, _P, _P, ctypes.c_int, _P, _P, _P, _P]
         L.fmo_tti_fast_marching.restype = ctypes.c_int64
+        L.fmo_tti_fast_marching_stop.argtypes = [_P, _P, _P, ctypes.c_int, _P, _P, _P, _P, ctypes.POINTER(_Problem)]
+        L.fmo_tti_fast_marching_stop.restype = ctypes.c_int64
         L.fmo_tti_norm.argtypes = [_P, _P, _P]
         L.fmo_tti_backward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int64,
                                                  _P, _P]
@@ -435,8 +437,27 @@ def tti_solve(params: Dict) -> Dict:
     values = np.empty(n)
     tact = np.empty(n)
     d = np.array(dims, np.int64)
-    nacc = lib().fmo_tti_fast_marching(_ptr(d), _ptr(hs), _ptr(metric), len(sidx), _ptr(sidx), _ptr(sval),
-                                       _ptr(values), _ptr(tact))
+    # stopping criteria (CommonStoppingCriteria.h:95-147) in a problem structure of their own
+    stop, keep = _Problem(), []
+    has_stop = False
+    if "stopAtDistance" in params:
+        stop.has_stop_at_distance, stop.stop_at_distance, has_stop = 1, float(params["stopAtDistance"]), True
+    if "nMaxAccepted" in params:
+        stop.n_max_accepted, has_stop = int(params["nMaxAccepted"]), True
+    for key, fld in (("stopWhenAnyAccepted", "stop_any"), ("stopWhenAllAccepted", "stop_all")):
+        if key in params:
+            cells = []
+            for q in np.atleast_2d(np.asarray(params[key], float)):
+                i = np.floor((q - origin) / hs).astype(np.int64)
+                if np.all((i >= 0) & (i < d)):
+                    cells.append(int(np.ravel_multi_index(tuple(i), dims)))
+            arr = np.ascontiguousarray(cells, np.int64)
+            keep.append(arr)
+            setattr(stop, "n" + fld, len(arr))
+            setattr(stop, fld, _ptr(arr))
+            has_stop = True
+    nacc = lib().fmo_tti_fast_marching_stop(_ptr(d), _ptr(hs), _ptr(metric), len(sidx), _ptr(sidx), _ptr(sval),
+                                            _ptr(values), _ptr(tact), ctypes.byref(stop) if has_stop else None)
     if nacc < 0:
         raise RuntimeError("oracle TTI fast marching failed")
     return {"values": values.reshape(dims), "activeNeighs": tact.reshape(dims), "nAccepted": int(nacc),

@@ -228,6 +228,10 @@ def stopping_fixtures():
     solve_fixture("stop_riemann3_walls_nmax", dict(p3, stopAtDistance=0.5, nMaxAccepted=2500.0))
     c = W.curvature2_case(24, 16, "ReedsShepp2", seed=23, n_curves=4)
     solve_fixture("stop_reedsshepp2_unoriented", dict(c, stopWhenAnyAccepted_Unoriented=np.array([[0.8, 0.2]])))
+    t = W.tti3_case(14, h=0.01, seed=5)
+    t.pop("_vp")
+    solve_fixture("stop_tti3_distance", dict(t, stopAtDistance=0.02))
+    solve_fixture("stop_tti3_all", dict(t, stopWhenAllAccepted=np.array([[0.02, 0.03, 0.12], [0.11, 0.1, 0.1]])))
 
 
 def spreading_fixtures():

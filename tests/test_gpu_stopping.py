@@ -12,7 +12,7 @@ from conftest import load_golden
 pytestmark = pytest.mark.gpu
 
 GOLDEN = ["stop_riemann2_distance", "stop_riemann2_nmax", "stop_riemann2_any_all", "stop_riemann3_walls_nmax",
-          "stop_reedsshepp2_unoriented"]
+          "stop_reedsshepp2_unoriented", "stop_tti3_distance", "stop_tti3_all"]
 
 
 @pytest.mark.parametrize("name", GOLDEN)
@@ -24,7 +24,8 @@ def test_stopping_matches_reference(name):
     fin = np.isfinite(b)
     assert np.array_equal(np.isfinite(a), fin)
     assert np.max(np.abs(a[fin] - b[fin])) <= 1e-10 * np.max(np.abs(b[fin]))
-    assert np.mean(out["activeNeighs"] == ref["activeNeighs"]) > 0.99
+    if params["model"] != "TTI3":  # TTI3 activeNeighs hold the extremum t (see test_gpu_tti.py)
+        assert np.mean(out["activeNeighs"] == ref["activeNeighs"]) > 0.99
 
 
 def test_distance_beyond_every_value_accepts_all():
