@@ -725,9 +725,10 @@ static bkey bheap_pop(bheap_t *h) {
 /* ValueVariation for Eulerian stencils (FirstVariation.h:198-251): the active neighbours in
  * stencil order with weights w max(0, value - u_neighbour) normalised by their sum, and the local
  * derivative (sum of w valueDiff) / sum (times the speed multiplier of shared stencils). */
-static double eul_value_variation(const fmo_problem *p, const double *values, const uint64_t *active, int64_t x,
-                                  int64_t *nb_idx, double *nb_w, int *nn_out) {
+static void eul_value_variation(const fmo_problem *p, const double *values, const uint64_t *active, int64_t x,
+                                int64_t *nb_idx, double *nb_w, int *nn_out, double *var) {
     const int nd = p->nfwd + p->nsym;
+    const int vd = p->var_dim > 1 ? p->var_dim : 1;
     int64_t idx[3], nidx[3];
     index_of(p, x, idx);
     const double value = values[x];
@@ -735,7 +736,8 @@ static double eul_value_variation(const fmo_problem *p, const double *values, co
     const int8_t *O = p->off + sid * nd * 3;
     const double *W = p->w + sid * nd;
     const uint64_t act = active[x];
-    double var = 0.0, weightSum = 0.0;
+    double weightSum = 0.0;
+    for (int i = 0; i < vd; ++i) var[i] = 0.0;
     int nn = 0;
     int bit = 0;
     for (int k2 = 0; k2 < nd; ++k2) {
@@ -751,16 +753,22 @@ static double eul_value_variation(const fmo_problem *p, const double *values, co
                 const double w = diff_weight(p, W[k2], x) * valueDiff;
                 weightSum += w;
                 nb_idx[nn] = y; nb_w[nn] = w; ++nn;
-                var += w * valueDiff;
+                /* DiffHelper::Elem: the component of the difference's multiplier (its axis for the
+                 * diagonal models, whose difference k is along axis k) */
+                var[vd > 1 ? k2 : 0] += w * valueDiff;
             }
         }
         bit += (k2 < p->nfwd) ? 1 : 2;
     }
     *nn_out = nn;
-    if (weightSum == 0.0) return var;
+    if (weightSum == 0.0) return;
     const double inv = 1.0 / weightSum;
     for (int j = 0; j < nn; ++j) nb_w[j] *= inv;
-    return p->mult ? inv * (p->mult[x] * var) : inv * var;
+    if (vd > 1) {
+        for (int i = 0; i < vd; ++i) var[i] = inv * (p->mult_vec[x * vd + i] * var[i]);
+    } else {
+        var[0] = p->mult ? inv * (p->mult[x] * var[0]) : inv * var[0];
+    }
 }
 
 int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const uint64_t *active,
@@ -773,7 +781,8 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
     uint8_t *in_map = (uint8_t *)calloc(N, 1);
     bheap_t h = {0};
     if (!pend || !in_map) return -1;
-    for (int64_t x = 0; x < N; ++x) sensitivity[x] = 0.0;
+    const int vd = p->var_dim > 1 ? p->var_dim : 1;
+    for (int64_t x = 0; x < N * vd; ++x) sensitivity[x] = 0.0;
     for (int i = 0; i < npts; ++i) {
         const int64_t x = pt_index[i];
         if (x < 0 || x >= N) continue;
@@ -793,12 +802,13 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
         pend[x] = 0.0;
         if (weight == 0.0) continue;
         int nn = 0;
-        const double var = eul_value_variation(p, values, active, x, nb_idx, nb_w, &nn);
+        double var[3];
+        eul_value_variation(p, values, active, x, nb_idx, nb_w, &nn, var);
         if (nn == 0) {
             if (nseeds < max_seeds) { seed_out_index[nseeds] = x; seed_out_weight[nseeds] = weight; }
             ++nseeds;
         }
-        sensitivity[x] = weight * var;
+        for (int i = 0; i < vd; ++i) sensitivity[x * vd + i] = weight * var[i];
         for (int j = 0; j < nn; ++j) {
             const int64_t y = nb_idx[j];
             if (in_map[y]) pend[y] += nb_w[j] * weight;
@@ -1807,10 +1817,15 @@ int fmo_forward_variation(const fmo_problem *p, const double *values, const uint
     for (int64_t i = 0; i < N; ++i) {
         const int64_t x = order[i].idx;
         int nn = 0;
-        const double var = eul_value_variation(p, values, active, x, nb_idx, nb_w, &nn);
+        double var[3];
+        eul_value_variation(p, values, active, x, nb_idx, nb_w, &nn, var);
+        const int vd = p->var_dim > 1 ? p->var_dim : 1;
         for (int k = 0; k < nvar; ++k) {
             double r = result[x * nvar + k];
-            r += var * (cost_var ? cost_var[x * nvar + k] : 0.0);
+            /* DiffHelper::Scal: sum of the products of the components */
+            double sc = 0.0;
+            for (int i = 0; i < vd; ++i) sc += var[i] * (cost_var ? cost_var[(x * nvar + k) * vd + i] : 0.0);
+            r += sc;
             for (int j = 0; j < nn; ++j) r += nb_w[j] * result[nb_idx[j] * nvar + k];
             result[x * nvar + k] = r;
         }

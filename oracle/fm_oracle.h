@@ -58,6 +58,10 @@ typedef struct {
     int64_t n_max_accepted;
     int nstop_any, nstop_all, nstop_any_u, nstop_all_u;
     const int64_t *stop_any, *stop_all, *stop_any_u, *stop_all_u;
+    /* Diagonal models: the first variation is per axis (a speed vector per cell): var_dim = ndim
+     * and mult_vec[N][var_dim] the speeds; 0 (or 1) and NULL otherwise. */
+    int var_dim;
+    const double *mult_vec;
 } fmo_problem;
 
 /* Fast marching. values[N] out; active[N] out (bitset, forward bits then symmetric +/- pairs,
@@ -67,7 +71,7 @@ typedef struct {
 int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active,
                           int *max_stencil_width);
 
-/* Reverse first variation from weighted points (linear indices). sensitivity[N] out;
+/* Reverse first variation from weighted points (linear indices). sensitivity[N][max(1, var_dim)] out;
  * seed_out_index/seed_out_weight receive up to max_seeds sensitive seeds. Returns the number of
  * sensitive seeds, or -1. */
 int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const uint64_t *active,
@@ -116,7 +120,8 @@ int64_t fmo_tti_geodesic_discrete(const int64_t *dims, const double *h, const do
 int fmo_geodesic_flow(const fmo_problem *p, const double *values, const uint64_t *active, double *flow,
                       double *value, double *width);
 /* Forward first variation: result [N][nvar] holds the seed value variations on entry and the
- * valueVariation on return; cost_var [N][nvar] or NULL. Returns 0, or -1 on allocation failure. */
+ * valueVariation on return; cost_var [N][nvar][max(1, var_dim)] or NULL. Returns 0, or -1 on
+ * allocation failure. */
 int fmo_forward_variation(const fmo_problem *p, const double *values, const uint64_t *active, int nvar,
                           const double *cost_var, double *result);
 int fmo_tti_forward_variation(const int64_t *dims, const double *h, const double *metric, const double *values,

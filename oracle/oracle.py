@@ -52,6 +52,8 @@ class _Problem(ctypes.Structure):
         ("stop_all", _P),
         ("stop_any_u", _P),
         ("stop_all_u", _P),
+        ("var_dim", ctypes.c_int),
+        ("mult_vec", _P),
     ]
 
 
@@ -249,6 +251,7 @@ class Problem:
                 off[:, i, i] = 1
                 w[:, i] = (1.0 / (hs[i] * hs[i])) * (sp[:, i] * sp[:, i])
             nfwd, nsym, share = 0, ndim, 0
+            self._mult_vec = np.ascontiguousarray(sp, np.float64)  # per-axis first variations
             adim = lambda p: (np.asarray(p, float) - origin) / hs
         elif model in ("Riemann2", "Riemann3"):
             origin = np.asarray(_get(params, "origin", np.zeros(ndim)), float)
@@ -322,6 +325,10 @@ class Problem:
         s.walls = _ptr(self.walls)
         s.nseeds = len(self.seed_index)
         s.seed_index, s.seed_value = _ptr(self.seed_index), _ptr(self.seed_value)
+        self.var_dim = 1
+        if getattr(self, "_mult_vec", None) is not None:
+            self.var_dim = ndim
+            s.var_dim, s.mult_vec = ndim, _ptr(self._mult_vec)
         # stopping criteria (CommonStoppingCriteria.h:95-147): target points out of range are dropped
         if "stopAtDistance" in params:
             s.has_stop_at_distance, s.stop_at_distance = 1, float(params["stopAtDistance"])
@@ -390,7 +397,7 @@ def backward_variation(res: Dict, points, weights=None):
         idx.append(i)
     idx = np.array(idx, np.int64)
     n = int(np.prod(P.dims))
-    sens = np.zeros(n, np.float64)
+    sens = np.zeros(n * P.var_dim, np.float64)
     max_seeds = max(16, len(P.seed_index) + 16)
     so_i = np.zeros(max_seeds, np.int64)
     so_w = np.zeros(max_seeds, np.float64)
@@ -401,7 +408,8 @@ def backward_variation(res: Dict, points, weights=None):
     if ns < 0:
         raise RuntimeError("oracle backward variation failed")
     ns = min(int(ns), max_seeds)
-    return sens.reshape(P.dims), so_i[:ns].copy(), so_w[:ns].copy()
+    shape = P.dims + ((P.var_dim,) if P.var_dim > 1 else ())
+    return sens.reshape(shape), so_i[:ns].copy(), so_w[:ns].copy()
 
 
 def visibility(params: Dict, max_width: int):
@@ -612,9 +620,10 @@ def forward_variation(res: Dict, params: Dict) -> np.ndarray:
     n = int(np.prod(dims))
     cost = None
     nvar = 0
+    vd = 1 if tti else P.var_dim
     if "costVariation" in params:
         cost = np.ascontiguousarray(np.asarray(params["costVariation"], float).reshape(n, -1))
-        nvar = cost.shape[1]
+        nvar = cost.shape[1] // vd
     seedvar = None
     if "seedValueVariation" in params:
         seedvar = np.atleast_2d(np.asarray(params["seedValueVariation"], float))

@@ -254,6 +254,22 @@ def spreading_fixtures():
                                        "seedRadius": 2.2, "exportValues": 1.0})
 
 
+def diagonal_variation_fixtures():
+    """First variations of the Diagonal models, per axis: costSensitivity dims + (D,), costVariation
+    dims + (nVar, D)."""
+    rng = np.random.default_rng(7)
+    for model, dims, name in (("Diagonal2", (30, 26), "fv_diag2_30x26"), ("Diagonal3", (12, 10, 8), "fv_diag3_12x10x8")):
+        nd = len(dims)
+        walls = np.zeros(dims)
+        walls[dims[0] // 2, 2:] = 1.0
+        p = {"model": model, "arrayOrdering": "RowMajor", "dims": np.array(dims, float),
+             "gridScales": np.linspace(0.02, 0.03, nd), "speed": 0.5 + rng.random(dims + (nd,)), "walls": walls,
+             "seeds": np.array([[0.3] * nd, [0.1] * nd]), "seedValues": np.array([0.0, 0.05]),
+             "costVariation": rng.standard_normal(dims + (2, nd)), "seedValueVariation": rng.standard_normal((2, 2)),
+             "exportValues": 1.0}
+        solve_fixture(name, p, (rng.uniform(0.05, 0.25, (3, nd)), np.array([1.0, 2.0, 0.5])))
+
+
 def variation_fixtures():
     """Forward first variation (costVariation, seedValueVariation -> valueVariation)."""
     rng = np.random.default_rng(2025)
@@ -304,7 +320,7 @@ def isotropic_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
@@ -319,6 +335,8 @@ if __name__ == "__main__":
         stopping_fixtures()
     elif sys.argv[1:] == ["spreading"]:
         spreading_fixtures()
+    elif sys.argv[1:] == ["diagvar"]:
+        diagonal_variation_fixtures()
     else:
         main()
         tti_fixtures()
@@ -328,3 +346,4 @@ if __name__ == "__main__":
         ode_fixtures()
         stopping_fixtures()
         spreading_fixtures()
+        diagonal_variation_fixtures()

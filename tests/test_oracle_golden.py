@@ -173,3 +173,14 @@ def test_stopping_criteria_oracle_matches_reference(name):
     np.testing.assert_array_equal(res["values"], ref["values"])
     np.testing.assert_array_equal(res["activeNeighs"].reshape(res["values"].shape).astype(float), ref["activeNeighs"])
     assert res["nAccepted"] == int(ref["nAccepted"])
+
+
+@pytest.mark.parametrize("name", ["fv_diag2_30x26", "fv_diag3_12x10x8"])
+def test_diagonal_first_variations_oracle_matches_reference(name):
+    """Diagonal models: the reverse (costSensitivity, one component per axis) and forward
+    (costVariation with one component per axis) first variations bit for bit."""
+    params, ref, _ = load_golden(name)
+    res = O.solve(params)
+    sens, _, _ = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
+    np.testing.assert_array_equal(sens, ref["costSensitivity_0"])
+    np.testing.assert_array_equal(O.forward_variation(res, params), ref["valueVariation"])
