@@ -155,6 +155,11 @@ struct Dev {
     const double *kscale;
     const TTICell *tti;                    // [ntc] TTI norms (TTI kind)
     unsigned *tile_up;                     // [ntile] value increases taken by each tile
+    // Diagonal models (a single instance): the speed (or cost) vector per cell, for the first
+    // variations, which have one component per axis (var_dim = ndim; 1 elsewhere)
+    const double *diag_src;
+    int diag_inverse;
+    int var_dim;
     unsigned order_lo, order_hi;           // tiles solved per round kept in [lo, hi]; lo = 0: plain FIM
     // active-tile lists (triple buffered) and their dedupe flags
     int *list[3];
@@ -1295,7 +1300,7 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
     cell_flags<Real, KIND>(P, c, fixed, dead);
     const double u = (double)P.values[x];
     nflow[x] = 0;
-    var[x] = 0.0;
+    var[x * (P.var_dim > 1 ? P.var_dim : 1)] = 0.0;
     if constexpr (KIND == kKindTTI) {
         // semi-Lagrangian ValueVariation (FirstVariation.h:169-196): the update recomputed at the
         // extremum t (TTI.hpp:278-389), flow weights (sol - v) w(t), and the local derivative
@@ -1374,12 +1379,15 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
         }
         return;
     }
+    const int vdim = P.var_dim > 1 ? P.var_dim : 1;
+    for (int i = 1; i < vdim; ++i) var[x * vdim + i] = 0.0;
     if (fixed || dead || !(u < Arith<double>::inf())) return;
     unsigned used = 0, side = 0;
     solve_cell<Real, NFWD, NSYM, KIND>(P, I, c, x0, x1, x2, 0, 0, 0, nullptr, &used, &side);
     double m = 1.0;
     if (SHARE) m = (double)P.mult[c];
     double ws = 0.0, v = 0.0;
+    double vv[3] = {0.0, 0.0, 0.0};  // per axis (Diagonal models: difference k is along axis k)
     int n = 0;
     int ys[2 * ND > 32 ? 32 : 2 * ND];
     double ww[2 * ND > 32 ? 32 : 2 * ND];
@@ -1420,6 +1428,7 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
             const double w = A::mul(wb, vd);
             ws = A::add(ws, w);
             v = A::add(v, A::mul(w, vd));
+            if (vdim > 1 && k < 3) vv[k] = A::add(vv[k], A::mul(w, vd));
             if (n < 32) { ys[n] = (int)y; ww[n] = w; ++n; }
         }
     }
@@ -1427,8 +1436,19 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
         const double inv = A::div(1.0, ws);
         for (int j = 0; j < n; ++j) ww[j] = A::mul(ww[j], inv);
         v = SHARE ? A::mul(inv, A::mul(m, v)) : A::mul(inv, v);
+        if (vdim > 1) {  // inv * (speed_i * var_i) (FirstVariation.h:243-247 with the vector multiplier)
+            const double *sp = P.diag_src + (I.metric0 + (I.metric_const ? 0 : x)) * vdim;
+            for (int i = 0; i < vdim && i < 3; ++i) {
+                const double si = P.diag_inverse ? A::div(1.0, sp[i]) : sp[i];
+                vv[i] = A::mul(inv, A::mul(si, vv[i]));
+            }
+        }
     }
-    var[x] = v;
+    if (vdim > 1) {
+        for (int i = 0; i < vdim && i < 3; ++i) var[x * vdim + i] = vv[i];
+    } else {
+        var[x] = v;
+    }
     nflow[x] = (uint8_t)n;
     for (int j = 0; j < n; ++j) {
         fidx[j * N + x] = ys[j];
@@ -1453,6 +1473,7 @@ struct AdjDev {
     int *indeg;
     double *acc;             // inspection weights
     double *sens;
+    int var_dim;             // components of var / sens per cell
     int *list[3];
     unsigned *count[3];
     long long *seed_idx;
@@ -1502,7 +1523,7 @@ __global__ void adjoint_kernel(AdjDev A) {
                 nf = A.nflow[x];
                 __threadfence();
                 if (lam != 0.0) {
-                    A.sens[x] = lam * A.var[x];
+                    for (int i = 0; i < A.var_dim; ++i) A.sens[(long long)x * A.var_dim + i] = lam * A.var[(long long)x * A.var_dim + i];
                     if (nf == 0) {
                         const unsigned si = atomicAdd(A.seed_count, 1u);
                         if (si < A.seed_cap) { A.seed_idx[si] = x; A.seed_w[si] = lam; }
@@ -1596,7 +1617,7 @@ void build_flow_graph(const Dev<Real> &P, long long N, FlowGraph &G, cudaStream_
     G.fidx.alloc((size_t)NF * N);
     G.indeg0.alloc(N);
     G.fw.alloc((size_t)NF * N);
-    G.var.alloc(N);
+    G.var.alloc((size_t)N * (P.var_dim > 1 ? P.var_dim : 1));
     G.nflow.alloc(N);
     G.indeg0.zero(s);
     launch(flow_kernel<Real, NFWD, NSYM, KIND>, nblocks(N, 128), 128, 0, s, P, G.fidx.get(), G.fw.get(), G.var.get(),
@@ -1634,7 +1655,8 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     }
     FlowGraph &G = *graph;
     DeviceBuffer<int> indeg(N);
-    DeviceBuffer<double> acc(N), sens(N), lam(N);
+    const int vdim = P.var_dim > 1 ? P.var_dim : 1;
+    DeviceBuffer<double> acc(N), sens((size_t)N * vdim), lam(N);
     DeviceBuffer<int> &fidx = G.fidx, &indeg0 = G.indeg0, &rx = G.rx;
     DeviceBuffer<double> &fw = G.fw, &var = G.var, &rw = G.rw;
     DeviceBuffer<uint8_t> &nflow = G.nflow;
@@ -1658,6 +1680,7 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     A.indeg = indeg.get();
     A.acc = acc.get();
     A.sens = sens.get();
+    A.var_dim = vdim;
     for (int i = 0; i < 3; ++i) { A.list[i] = lists.get() + i * N; A.count[i] = counters.get() + i; }
     A.seed_count = counters.get() + 3;
     A.bar_count = counters.get() + 4;
@@ -1699,8 +1722,8 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
                                                  dim3(256), args, 0, s));
         check_status(status, "adjoint");
         AdjointResult ar;
-        ar.sensitivity.resize(N);
-        sens.download(ar.sensitivity.data(), N, s);
+        ar.sensitivity.resize((size_t)N * vdim);
+        sens.download(ar.sensitivity.data(), (size_t)N * vdim, s);
         unsigned hc[8];
         counters.download(hc, 8, s);
         HFM_CUDA(cudaStreamSynchronize(s));
@@ -1735,7 +1758,8 @@ struct FwdDev {
     const uint8_t *nflow;
     const long long *rptr;
     const int *rx;
-    const double *cost;  // [N][nvar] or null
+    const double *cost;  // [N][nvar][var_dim] or null
+    int var_dim;         // components of var per cell
     double *res;         // [N][nvar]: seed value variations on entry
     int *cnt;            // upwind cells not yet done
     int *list[3];
@@ -1776,10 +1800,15 @@ __global__ void forward_kernel(FwdDev F) {
             long long e = 0, ee = 0;
             if (x >= 0) {
                 const int nf = F.nflow[x];
-                const double v = F.var[x];
+                const int vd = F.var_dim;
                 for (int k = 0; k < F.nvar; ++k) {
                     double acc = __ldcg(F.res + (long long)x * F.nvar + k);
-                    acc = __dadd_rn(acc, __dmul_rn(v, F.cost ? F.cost[(long long)x * F.nvar + k] : 0.0));
+                    // the local derivative paired with the cost variation (DiffHelper::Scal)
+                    double sc = 0.0;
+                    for (int i = 0; i < vd; ++i)
+                        sc = __dadd_rn(sc, __dmul_rn(F.var[(long long)x * vd + i],
+                                                     F.cost ? F.cost[((long long)x * F.nvar + k) * vd + i] : 0.0));
+                    acc = __dadd_rn(acc, sc);
                     for (int j = 0; j < nf; ++j) {
                         const long long y = F.fidx[j * F.N + x];
                         acc = __dadd_rn(acc, __dmul_rn(F.fw[j * F.N + x], __ldcg(F.res + y * F.nvar + k)));
@@ -1830,9 +1859,10 @@ void run_forward(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     for (size_t i = 0; i < p.fwd_seed_cell.size(); ++i)
         HFM_CUDA(cudaMemcpyAsync(out.get() + p.fwd_seed_cell[i] * nvar, p.fwd_seed_value.data() + i * nvar,
                                  nvar * sizeof(double), cudaMemcpyHostToDevice, s));
+    const int vdim = P.var_dim > 1 ? P.var_dim : 1;
     if (!p.fwd_cost.empty()) {
-        cost.alloc((size_t)N * nvar);
-        cost.upload(p.fwd_cost.data(), (size_t)N * nvar, s);
+        cost.alloc((size_t)N * nvar * vdim);
+        cost.upload(p.fwd_cost.data(), (size_t)N * nvar * vdim, s);
     }
     DeviceBuffer<int> cnt(N), lists(3 * N);
     DeviceBuffer<unsigned> counters(8);
@@ -1849,6 +1879,7 @@ void run_forward(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     F.rptr = G.rptr.get();
     F.rx = G.rx.get();
     F.cost = p.fwd_cost.empty() ? nullptr : cost.get();
+    F.var_dim = vdim;
     F.res = out.get();
     F.cnt = cnt.get();
     for (int i = 0; i < 3; ++i) { F.list[i] = lists.get() + i * N; F.count[i] = counters.get() + i; }
@@ -2026,6 +2057,11 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         } else if (p0.diagonal) {
             launch(diagonal_stencil_kernel<Real>, nblocks(N, 128), 128, 0, s, P, p0.ndim, metric_ptr, plain_off.get(),
                    plain_w.get());
+            if (ninst == 1) {  // first variations read the speeds again (the metric buffer lives on)
+                P.diag_src = metric_ptr;
+                P.diag_inverse = p0.mult_inverse ? 1 : 0;
+                P.var_dim = p0.ndim;
+            }
         } else if (p0.ndim == 2) {
             launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr, plain_off.get(),
                    plain_w.get());
@@ -2424,7 +2460,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     HFM_CUDA(cudaStreamSynchronize(s));
     HFM_CUDA(cudaGetLastError());
-    if (ninst == 1 && p0.retain) {
+    if (ninst == 1 && p0.retain && !p0.diagonal) {  // (the speeds of a Diagonal model are not retained)
         auto r = std::make_shared<Retained<Real, NFWD, NSYM, KIND>>();
         r->P = P;
         r->N = N;

@@ -582,9 +582,6 @@ void setup_diagonal(Store &io, int ndim, Param &pm, EulerProblem &p) {
     } else {
         p.metric = std::move(f.data);
     }
-    // the reference's first variation of these models is per axis (a vector multiplier)
-    if (io.has_field("inspectSensitivity") || io.has_field("costVariation"))
-        throw Error(HFM_ERR_UNSUPPORTED, "first variations of the Diagonal models are not supported by the GPU solve path");
 }
 
 void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProblem &p) {
@@ -733,12 +730,14 @@ void read_forward_variation(Store &io, const Param &pm, EulerProblem &p) {
     for (int a = 0; a < pm.ndim; ++a) ncells *= pm.dims[a];
     int kc = 0, ks = 0;
     if (cost) {
-        const Field f = io.get_field("costVariation", pm.ndim + 1, 1);
+        // one component per axis for the Diagonal models (their multiplier is a speed vector)
+        const int comp = p.diagonal ? pm.ndim : 1;
+        const Field f = io.get_field("costVariation", pm.ndim + 1, comp);
         bool ok = (int)f.dims.size() == pm.ndim + 1;
         for (int a = 0; ok && a < pm.ndim; ++a) ok = f.dims[a] == pm.dims[a];
         if (!ok) throw Error(HFM_ERR_VALUE, "Forward variation error : inconsistent input sizes");
         kc = (int)f.dims[pm.ndim];
-        p.fwd_cost.assign(f.ptr(), f.ptr() + ncells * kc);
+        p.fwd_cost.assign(f.ptr(), f.ptr() + ncells * kc * comp);
     }
     if (seed) {
         const RawElement &r = io.raw("seedValueVariation");
@@ -880,12 +879,19 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     p.h_values_out = q.values_dst;
 }
 
+size_t n_cells(const std::vector<int64_t> &dims) {
+    size_t n = 1;
+    for (int64_t d : dims) n *= (size_t)d;
+    return n;
+}
+
 // costSensitivity_i and seedSensitivity_i (point, weight) of each inspection group.
 void export_sensitivities(Store &io, const Param &pm, const std::vector<int64_t> &dims,
                           const std::vector<AdjointResult> &adjoints) {
     for (size_t gi = 0; gi < adjoints.size(); ++gi) {
         const AdjointResult &ar = adjoints[gi];
-        io.set_field("costSensitivity_" + std::to_string(gi), dims, 1, ar.sensitivity.data());
+        const int comp = (int)(ar.sensitivity.size() / std::max<size_t>(1, n_cells(dims)));
+        io.set_field("costSensitivity_" + std::to_string(gi), dims, comp, ar.sensitivity.data());
         std::vector<double> ss;
         for (size_t k = 0; k < ar.seed_index.size(); ++k) {
             int64_t x = ar.seed_index[k];

@@ -51,8 +51,13 @@ def test_isotropic3_matches_oracle_at_64():
     assert int(out["nAccepted"]) == ref["nAccepted"]
 
 
-def test_diagonal_first_variation_of_the_multiplier_refused():
-    params, _, _ = load_golden("diag2_40x36_walls")
-    with pytest.raises(hfm.PyExp) as e:
-        hfm.run(dict(params, costVariation=np.ones((40, 36, 1))))
-    assert e.value.code == 3
+@pytest.mark.parametrize("name", ["fv_diag2_30x26", "fv_diag3_12x10x8"])
+def test_diagonal_first_variations_match_reference(name):
+    """Diagonal models: costSensitivity (one component per axis) and valueVariation (a cost
+    variation with one component per axis) within 1e-8 of the reference's largest entry."""
+    params, ref, _ = load_golden(name)
+    out = hfm.run(dict(params))
+    for key in ("costSensitivity_0", "valueVariation"):
+        a, b = out[key], ref[key]
+        assert a.shape == b.shape, key
+        assert np.max(np.abs(a - b)) <= 1e-8 * np.max(np.abs(b)), key
