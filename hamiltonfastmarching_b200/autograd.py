@@ -7,8 +7,10 @@ group whose ``costSensitivity_0`` is the vector-Jacobian product.
 
 Cost semantics follow the reference:
 
-* curvature models (ReedsShepp2, Elastica2): ``cost`` is the model's cost field (the reference's
-  ``cost`` key, speed = 1/cost); the reference's costSensitivity is d(values)/d(cost).
+* curvature models (ReedsShepp2, Elastica2) and Isotropic2/3: ``cost`` is the model's cost field (the
+  reference's ``cost`` key, speed = 1/cost); the reference's costSensitivity is d(values)/d(cost).
+* Diagonal2/3: ``cost`` is the per-axis cost field, shape dims + (ndim,) (speed_i = 1/cost_i), and the
+  costSensitivity holds d(values)/d(cost_i).
 * Riemann2/Riemann3: ``cost`` is a positive local multiplier rho(x) of the norm, the metric used
   being rho^2 * metric; the reference's costSensitivity is the derivative with respect to a relative
   change of the local norm, so d/d(rho) = costSensitivity / rho.
@@ -33,6 +35,7 @@ from . import HFMIO
 __all__ = ["EikonalSolve", "arrival_times"]
 
 _CURVATURE = ("ReedsShepp2", "Elastica2")
+_COST_KEY = _CURVATURE + ("Isotropic2", "Isotropic3", "Diagonal2", "Diagonal3")
 
 
 def _with_cost(params: Dict, cost: np.ndarray) -> Dict:
@@ -40,7 +43,7 @@ def _with_cost(params: Dict, cost: np.ndarray) -> Dict:
     p.setdefault("arrayOrdering", "RowMajor")
     p["verbosity"] = 0.0
     p["exportValues"] = 1.0
-    if p["model"] in _CURVATURE:
+    if p["model"] in _COST_KEY:
         p["cost"] = cost
         p.pop("speed", None)
     elif p["model"] == "TTI3":
@@ -102,7 +105,7 @@ class EikonalSolve(torch.autograd.Function):
         io.set_array("inspectSensitivityLengths", np.array([float(idx.size)]))
         io.run_sensitivity()
         sens = io.get_array("costSensitivity_0")
-        if params["model"] in _CURVATURE:
+        if params["model"] in _COST_KEY:
             gc = sens
             if gc.shape != c.shape:  # physical (x, y) cost field: sum over the angular axis
                 gc = gc.sum(axis=2)

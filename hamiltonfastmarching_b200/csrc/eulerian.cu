@@ -1916,6 +1916,7 @@ struct Retained final : RetainedSolve {
     DeviceBuffer<Real> values, weight, mult, cls_w;
     DeviceBuffer<int8_t> cls_off;
     DeviceBuffer<TTICell> tti;
+    DeviceBuffer<double> diag;  // per-axis speeds of a Diagonal model (P.diag_src points here)
     void adjoint(const EulerProblem &p, EulerResult &res) override {
         cudaStream_t s = current_stream();
         // arrival times (RowMajor, FP64) for the ordering of the sensitive seeds
@@ -2460,7 +2461,8 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     HFM_CUDA(cudaStreamSynchronize(s));
     HFM_CUDA(cudaGetLastError());
-    if (ninst == 1 && p0.retain && !p0.diagonal) {  // (the speeds of a Diagonal model are not retained)
+    // A Diagonal model's speeds stay in the metric buffer, which the retained state then owns.
+    if (ninst == 1 && p0.retain && (!p0.diagonal || !p0.d_metric)) {
         auto r = std::make_shared<Retained<Real, NFWD, NSYM, KIND>>();
         r->P = P;
         r->N = N;
@@ -2475,6 +2477,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         r->cls_w = std::move(cls_w);
         r->cls_off = std::move(cls_off);
         r->tti = std::move(ttibuf);
+        if (p0.diagonal) r->diag = std::move(metric);
         results[0].retained = r;
     }
     const double total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall_t0).count();
