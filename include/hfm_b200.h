@@ -26,7 +26,7 @@ extern "C" {
 #define HFM_OK 0
 #define HFM_ERR_KEY 1           /* missing key, wrong field kind (string/scalar/array)            */
 #define HFM_ERR_VALUE 2         /* invalid value: shape mismatch, non-SPD metric, bad ordering    */
-#define HFM_ERR_UNSUPPORTED 3   /* a reference option this build does not implement              */
+#define HFM_ERR_UNSUPPORTED 3   /* a reference option this library does not implement            */
 #define HFM_ERR_CUDA 4          /* CUDA runtime failure (message carries cudaGetErrorString)      */
 #define HFM_ERR_NOT_CONVERGED 5 /* solver iteration cap reached, or a bounded device wait expired */
 #define HFM_ERR_NOMEM 6         /* device or host allocation failure                              */
