@@ -7,8 +7,9 @@ group whose ``costSensitivity_0`` is the vector-Jacobian product.
 
 Cost semantics follow the reference:
 
-* curvature models (ReedsShepp2, Elastica2) and Isotropic2/3: ``cost`` is the model's cost field (the
-  reference's ``cost`` key, speed = 1/cost); the reference's costSensitivity is d(values)/d(cost).
+* curvature models (ReedsShepp2, ReedsSheppForward2, Elastica2) and Isotropic2/3: ``cost`` is the
+  model's cost field (the reference's ``cost`` key, speed = 1/cost); the reference's
+  costSensitivity is d(values)/d(cost).
 * Diagonal2/3: ``cost`` is the per-axis cost field, shape dims + (ndim,) (speed_i = 1/cost_i), and the
   costSensitivity holds d(values)/d(cost_i).
 * Riemann2/Riemann3: ``cost`` is a positive local multiplier rho(x) of the norm, the metric used
@@ -34,7 +35,7 @@ from . import HFMIO
 
 __all__ = ["EikonalSolve", "arrival_times"]
 
-_CURVATURE = ("ReedsShepp2", "Elastica2")
+_CURVATURE = ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")
 _COST_KEY = _CURVATURE + ("Isotropic2", "Isotropic3", "Diagonal2", "Diagonal3")
 
 

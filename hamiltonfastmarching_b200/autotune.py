@@ -41,10 +41,11 @@ DEFAULT = {
     "Diagonal2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
     "Diagonal3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
     "ReedsShepp2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
+    "ReedsSheppForward2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
     "Elastica2": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
     "TTI3": {"tileSweeps": 1, "queue": ("band", 1.0, 4.0)},
 }
-_LIFTED = ("ReedsShepp2", "Elastica2")
+_LIFTED = ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")
 
 
 def _domain_kind(params: Dict) -> str:

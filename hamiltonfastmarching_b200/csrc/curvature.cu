@@ -5,6 +5,7 @@
 // angle index, Headers/Base/Implementation/HFM_StencilShare.hxx:132-181). The arithmetic follows:
 //   Voronoi1Vec (relaxed rank-one tensor, tolerances, reorientation)  CommonTraits.h:118-161
 //   StencilReedsShepp2::SetStencil                                      Curvature2.h:48-66
+//   StencilReedsSheppForward2::SetStencil                               Curvature2.h:86-100
 //   StencilElastica2<5>::SetStencil and its Fejer weights               Curvature2.h:178-234
 #include <cmath>
 
@@ -59,6 +60,26 @@ void reedsshepp2_table(int ntheta, double h, double xi, double eps, bool project
         off[t * 12 + 10] = 0;
         off[t * 12 + 11] = 1;
         const double xd = xi * ds;
+        w[t * 4 + 3] = 1.0 / (xd * xd);
+    }
+}
+
+// Forward-only car: per angle, the 3 forward differences of the 2D Voronoi1Vec of (cos, sin)/h
+// followed by one symmetric angular difference, offset (0, 0, -1), weight 1/(xi dtheta)^2.
+void reedssheppforward2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,
+                              std::vector<double> &w) {
+    off.assign((size_t)ntheta * 4 * 3, 0);
+    w.assign((size_t)ntheta * 4, 0.0);
+    const double ds = 2.0 * kPi / (double)ntheta;
+    const double ih = 1.0 / h;
+    const double xd = xi * ds;
+    for (int t = 0; t < ntheta; ++t) {
+        const double theta = (double)t * ds;
+        const double v[2] = {std::cos(theta) * ih, std::sin(theta) * ih};
+        voronoi1vec<2>(v, eps, &off[t * 12], &w[t * 4]);
+        off[t * 12 + 9] = 0;
+        off[t * 12 + 10] = 0;
+        off[t * 12 + 11] = -1;
         w[t * 4 + 3] = 1.0 / (xd * xd);
     }
 }

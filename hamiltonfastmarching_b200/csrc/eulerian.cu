@@ -578,7 +578,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 template <typename Real, int NFWD, int NSYM, int KIND>
 constexpr int fim_min_blocks() {
     [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
-    return KIND == kKindTTI ? 1 : SHARE ? (NFWD > 0 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 8;
+    return KIND == kKindTTI ? 1 : SHARE ? (NFWD + NSYM > 8 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 8;
 }
 
 template <typename Real, int NFWD, int NSYM, int KIND>
@@ -2533,6 +2533,9 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
         } else if (p.nfwd == 0 && p.nsym == 3) {
             if (p.fp64) run_batch_impl<double, 0, 3, detail::kKindShare>(probs, results);
             else run_batch_impl<float, 0, 3, detail::kKindShare>(probs, results);
+        } else if (p.nfwd == 3 && p.nsym == 1) {
+            if (p.fp64) run_batch_impl<double, 3, 1, detail::kKindShare>(probs, results);
+            else run_batch_impl<float, 3, 1, detail::kKindShare>(probs, results);
         } else if (p.nfwd == 27 && p.nsym == 0) {
             if (p.fp64) run_batch_impl<double, 27, 0, detail::kKindShare>(probs, results);
             else run_batch_impl<float, 27, 0, detail::kKindShare>(probs, results);
@@ -2544,7 +2547,7 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
 
 void default_schedule(EulerProblem &p) {
     if (p.kind == StencilKind::TTI) { p.sweeps_per_tile = 1; p.band_lo = 1; p.band_hi = 4; }
-    else if (p.kind == StencilKind::SharedByTheta && p.angular && p.nfwd > 0) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
+    else if (p.kind == StencilKind::SharedByTheta && p.angular && p.nfwd + p.nsym > 4) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
     else if (p.kind == StencilKind::SharedByTheta && p.angular) { p.sweeps_per_tile = 4; p.band_lo = 2; p.band_hi = 8; }
     else if (p.ndim == 3) { p.sweeps_per_tile = 2; p.band_lo = 1; p.band_hi = 4; }
     else { p.sweeps_per_tile = 3; p.band_lo = 2; p.band_hi = 8; }

@@ -161,10 +161,12 @@ void default_schedule(EulerProblem &p);
 void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results);
 
 // Curvature model stencil tables built on the host with the C library's cos/sin
-// (Headers/Specializations/Curvature2.h:48-66, 178-234, CommonTraits.h:118-161).
+// (Headers/Specializations/Curvature2.h:48-66, 86-100, 178-234, CommonTraits.h:118-161).
 void reedsshepp2_table(int ntheta, double h, double xi, double eps, bool projective,
                        std::vector<int8_t> &off, std::vector<double> &w);
 void elastica2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,
                      std::vector<double> &w);
+void reedssheppforward2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,
+                              std::vector<double> &w);
 
 }  // namespace hfm

@@ -229,6 +229,25 @@ int fmo_reedsshepp2_table(int ntheta, double h, double xi, double eps, int proje
     return 0;
 }
 
+/* StencilReedsSheppForward2::SetStencil (Curvature2.h:86-100): 3 forward differences from the
+ * 2D Voronoi1Vec of (cos, sin)(theta) / h, then one symmetric angular difference, offset (0,0,-1),
+ * weight 1/(xi dtheta)^2. Layout per angle: forward first, then the symmetric one. */
+int fmo_reedssheppforward2_table(int ntheta, double h, double xi, double eps,
+                                 int8_t *offsets, double *weights) {
+    const double ds = (2.0 * kPi) / (double)ntheta;
+    const double ih = 1.0 / h;
+    for (int t = 0; t < ntheta; ++t) {
+        const double theta = (double)t * ds;
+        const double v[2] = {cos(theta) * ih, sin(theta) * ih};
+        if (fmo_voronoi1vec(2, v, eps, offsets + t * 12, weights + t * 4)) return -1;
+        int8_t *o = offsets + t * 12 + 9;
+        o[0] = 0; o[1] = 0; o[2] = -1;
+        const double xd = xi * ds;
+        weights[t * 4 + 3] = 1.0 / (xd * xd);
+    }
+    return 0;
+}
+
 /* StencilElastica2<5>::SetStencil (Curvature2.h:178-234): Fejer quadrature over 5 points; for
  * l = 0,1 a 3D Voronoi1Vec (6 offsets) and its mirror in theta, then a 2D one (3 offsets). */
 int fmo_elastica2_table(int ntheta, double h, double xi, double eps,

@@ -36,6 +36,9 @@ int fmo_reedsshepp2_table(int ntheta, double h, double xi, double eps, int proje
                           int8_t *offsets, double *weights);
 int fmo_elastica2_table(int ntheta, double h, double xi, double eps,
                         int8_t *offsets, double *weights);
+/* ReedsSheppForward2: 3 forward differences then 1 symmetric (angular) per angle. */
+int fmo_reedssheppforward2_table(int ntheta, double h, double xi, double eps,
+                                 int8_t *offsets, double *weights);
 
 typedef struct {
     int ndim;

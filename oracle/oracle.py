@@ -77,6 +77,8 @@ def lib():
                                             ctypes.c_double, ctypes.c_int, _P, _P]
         L.fmo_elastica2_table.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, _P, _P]
+        L.fmo_reedssheppforward2_table.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                   ctypes.c_double, _P, _P]
         L.fmo_fast_marching.argtypes = [ctypes.POINTER(_Problem), _P, _P, _P]
         L.fmo_fast_marching.restype = ctypes.c_int64
         L.fmo_backward_variation.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, _P,
@@ -152,6 +154,10 @@ def curvature2_table(model: str, ntheta: int, h: float, xi: float, eps: float, p
         off = np.zeros((ntheta, 4, 3), np.int8)
         w = np.zeros((ntheta, 4), np.float64)
         rc = L.fmo_reedsshepp2_table(ntheta, h, xi, eps, int(projective), _ptr(off), _ptr(w))
+    elif model == "ReedsSheppForward2":
+        off = np.zeros((ntheta, 4, 3), np.int8)
+        w = np.zeros((ntheta, 4), np.float64)
+        rc = L.fmo_reedssheppforward2_table(ntheta, h, xi, eps, _ptr(off), _ptr(w))
     elif model == "Elastica2":
         off = np.zeros((ntheta, 27, 3), np.int8)
         w = np.zeros((ntheta, 27), np.float64)
@@ -268,7 +274,7 @@ class Problem:
             nfwd, nsym, share = 0, off.shape[1], 0
             scale = hs
             adim = lambda p: (np.asarray(p, float) - origin) / hs
-        elif model in ("ReedsShepp2", "Elastica2"):
+        elif model in ("ReedsShepp2", "ReedsSheppForward2", "Elastica2"):
             periodic = [0, 0, 1]
             h = float(params["gridScale"])
             xi = float(_get(params, "xi", 1.0))
@@ -279,6 +285,8 @@ class Problem:
             off, w = curvature2_table(model, nth, h, xi, eps, projective)
             if model == "ReedsShepp2":
                 nfwd, nsym = 0, 4
+            elif model == "ReedsSheppForward2":
+                nfwd, nsym = 3, 1
             else:
                 nfwd, nsym = 27, 0
             share = 1

@@ -37,7 +37,7 @@ def load_golden(name):
 
 
 GOLDEN_SOLVES = ["riemann2_64", "riemann2_48_seeds", "riemann3_16_walls", "reedsshepp2_32x24",
-                 "reedsshepp2_24x16_walls", "elastica2_24x16"]
+                 "reedsshepp2_24x16_walls", "elastica2_24x16", "rsf2_32x24", "rsf2_24x16_walls"]
 GOLDEN_STENCILS = ["selling2_32", "selling2_dual_24", "selling3_10"]
 
 

@@ -319,8 +319,26 @@ def isotropic_fixtures():
         solve_fixture(name, p)
 
 
+def forward_curvature_fixtures():
+    """ReedsSheppForward2 (3 forward differences and 1 symmetric angular one per angle): values,
+    activeNeighs, costSensitivity; with walls, geodesics (tips, tips_Unoriented), the geodesic flow
+    and a forward variation."""
+    rng = np.random.default_rng(2027)
+    pts = np.c_[rng.uniform(0.1, 0.9, (4, 2)), rng.uniform(0, 6, (4, 1))]
+    solve_fixture("rsf2_32x24", W.curvature2_case(32, 24, "ReedsSheppForward2", seed=11, n_curves=6),
+                  (pts, rng.uniform(0.5, 2.0, 4)))
+    p = W.curvature2_case(24, 16, "ReedsSheppForward2", seed=12, n_curves=4)
+    p["walls"] = (np.random.default_rng(13).uniform(size=(24, 24)) < 0.06).astype(float)
+    p["tips"] = np.c_[rng.uniform(0.1, 0.9, (3, 2)), rng.uniform(0, 6.2, (3, 1))]
+    p["tips_Unoriented"] = rng.uniform(0.1, 0.9, (3, 2))
+    p["exportGeodesicFlow"] = 1.0
+    p["costVariation"] = rng.standard_normal((24, 24, 16, 1))
+    p["seedValueVariation"] = np.array([[0.7]])
+    solve_fixture("rsf2_24x16_walls", p)
+
+
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2` regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
@@ -337,6 +355,8 @@ if __name__ == "__main__":
         spreading_fixtures()
     elif sys.argv[1:] == ["diagvar"]:
         diagonal_variation_fixtures()
+    elif sys.argv[1:] == ["rsf2"]:
+        forward_curvature_fixtures()
     else:
         main()
         tti_fixtures()

@@ -19,7 +19,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 GOLDEN = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
-          "geo_tti3_12"]
+          "geo_tti3_12", "rsf2_24x16_walls"]
 # geodesicSolver = 'ODE' (the Riemann3 fixture has a tip whose solver stalls, as in the reference)
 GOLDEN_ODE = ["ode_riemann2_48_walls", "ode_riemann3_16_walls", "ode_reedsshepp2_24x16", "ode_elastica2_24x16",
               "ode_tti3_12"]

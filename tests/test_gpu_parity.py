@@ -64,7 +64,7 @@ def test_golden_sensitivity(name):
     np.testing.assert_allclose(so, sr, rtol=1e-10, atol=0)
 
 
-@pytest.mark.parametrize("case", ["riemann2_256", "riemann3_40_walls", "rs2_64x36", "elastica2_48x30"])
+@pytest.mark.parametrize("case", ["riemann2_256", "riemann3_40_walls", "rs2_64x36", "elastica2_48x30", "rsf2_64x36"])
 def test_oracle_parity_larger(case):
     if case == "riemann2_256":
         p = W.riemann2_case(256)
@@ -72,6 +72,8 @@ def test_oracle_parity_larger(case):
         p = W.riemann3_case(40)
     elif case == "rs2_64x36":
         p = W.curvature2_case(64, 36, "ReedsShepp2")
+    elif case == "rsf2_64x36":
+        p = W.curvature2_case(64, 36, "ReedsSheppForward2")
     else:
         p = W.curvature2_case(48, 30, "Elastica2")
     ora = O.solve(p)

@@ -20,7 +20,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 GOLDEN = ["fwd_riemann2_40_seeds", "fwd_riemann3_16_walls", "fwd_reedsshepp2_20x12", "fwd_elastica2_20x12",
-          "fwd_tti3_12"]
+          "fwd_tti3_12", "rsf2_24x16_walls"]
 
 
 def _oracle_on(out, params):
@@ -51,8 +51,10 @@ def test_forward_variation_matches_reference(name):
     """Where the two sides of a symmetric difference hold exactly equal values, the reference's
     flow takes the side its heap accepted first, this solver the +e side: the values are the same
     but the variations of the cells downstream differ. The ReedsShepp2 fixture has two such cells
-    (angle 0, next to the seed's row), which move 370 of its 4800 cells; everywhere else the
-    variations agree within 1e-8."""
+    (angle 0, next to the seed's row), which move 370 of its 4800 cells; the ReedsSheppForward2
+    one has an exact tie on its angular difference where the reference took the -e side (the
+    oracle, given the reference's activeNeighs with that tie moved to +e, differs from the reference
+    on 1 of 9216 cells). Everywhere else the variations agree within 1e-8."""
     params, ref, _ = load_golden(name)
     params = dict(params)
     params.pop("exportActiveNeighs", None)
@@ -60,7 +62,7 @@ def test_forward_variation_matches_reference(name):
     v, r = out["valueVariation"], ref["valueVariation"]
     assert v.shape == r.shape
     close = np.abs(v - r) <= 1e-8 * np.max(np.abs(r))
-    if name == "fwd_reedsshepp2_20x12":
+    if name in ("fwd_reedsshepp2_20x12", "rsf2_24x16_walls"):
         assert np.mean(close) > 0.9
     else:
         assert close.all()

@@ -73,7 +73,7 @@ def test_tti_oracle_matches_reference():
 
 GOLDEN_GEODESICS = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
                     "geo_tti3_12", "ode_riemann2_48_walls", "ode_riemann3_16_walls", "ode_reedsshepp2_24x16",
-                    "ode_elastica2_24x16", "ode_tti3_12"]
+                    "ode_elastica2_24x16", "ode_tti3_12", "rsf2_24x16_walls"]
 
 
 @pytest.mark.parametrize("name", GOLDEN_GEODESICS)
@@ -104,7 +104,7 @@ def test_geodesic_oracle_matches_reference(name):
 
 
 GOLDEN_VARIATIONS = ["fwd_riemann2_40_seeds", "fwd_riemann3_16_walls", "fwd_reedsshepp2_20x12", "fwd_elastica2_20x12",
-                     "fwd_tti3_12"]
+                     "fwd_tti3_12", "rsf2_24x16_walls"]
 
 
 @pytest.mark.parametrize("name", GOLDEN_VARIATIONS)
@@ -184,3 +184,26 @@ def test_diagonal_first_variations_oracle_matches_reference(name):
     sens, _, _ = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
     np.testing.assert_array_equal(sens, ref["costSensitivity_0"])
     np.testing.assert_array_equal(O.forward_variation(res, params), ref["valueVariation"])
+
+
+def test_rsf2_exact_angular_tie_moves_one_cell():
+    """ReedsSheppForward2 fixture: the cells whose angular neighbours (offset (0,0,-1) and its
+    opposite) hold exactly equal values. The reference took the -e side on one of them; with that
+    tie moved to the +e side (the GPU solver's rule) the forward variation of the oracle differs
+    from the reference's on that one cell, and with the reference's activeNeighs on none."""
+    params, ref, _ = load_golden("rsf2_24x16_walls")
+    u = ref["values"]
+    act = ref["activeNeighs"].astype(np.uint64)
+    plus, minus = np.roll(u, 1, axis=2), np.roll(u, -1, axis=2)
+    tie = np.isfinite(u) & np.isfinite(plus) & (plus == minus)
+    took_minus = tie & (((act >> np.uint64(4)) & np.uint64(1)) == 1)
+    assert int(took_minus.sum()) == 1
+    moved = act.copy()
+    moved[took_minus] = (moved[took_minus] & ~np.uint64(1 << 4)) | np.uint64(1 << 3)
+    res = {"values": np.ascontiguousarray(u), "activeNeighs": np.ascontiguousarray(moved.ravel()),
+           "problem": O.Problem(params)}
+    r = ref["valueVariation"]
+    far = np.abs(O.forward_variation(res, params) - r) > 1e-8 * np.max(np.abs(r))
+    assert int(far.sum()) == 1
+    res["activeNeighs"] = np.ascontiguousarray(act.ravel())
+    np.testing.assert_array_equal(O.forward_variation(res, params), r)
