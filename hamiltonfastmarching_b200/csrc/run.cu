@@ -103,15 +103,23 @@ void reject_unsupported(Store &io) {
 // or interpolated at a point over its 2^D grid neighbours with the reference's unnormalised
 // weights (BaseGrid.h:79-101, PeriodicGrid.hxx Neighbors, MapWeightedSum.h): a symmetric matrix
 // in grid units for Riemann metrics (Riemannian.h:62-71: the metric, inverted if dual, times
-// h_i h_j), a diagonal d_i = h_i / speed_i for the isotropic and diagonal models (Isotropic.h).
+// h_i h_j), a diagonal d_i = h_i / speed_i for the isotropic and diagonal models (Isotropic.h),
+// the 14 TTI3 metric elements with the transform's columns scaled by h_j (TTI.hpp:22-46).
 struct SeedGuess {
     const EulerProblem &p;
     const Param &pm;
-    int ns() const { return p.kind == StencilKind::RiemannPerCell && !p.diagonal ? pm.ndim * (pm.ndim + 1) / 2 : pm.ndim; }
+    int ns() const {
+        if (p.kind == StencilKind::TTI) return 14;
+        return p.kind == StencilKind::RiemannPerCell && !p.diagonal ? pm.ndim * (pm.ndim + 1) / 2 : pm.ndim;
+    }
     // raw model data at a cell: packed metric, speed vector (diagonal) or speed (isotropic)
     void raw(int64_t cell, double *out) const {
         const int D = pm.ndim;
-        if (p.kind == StencilKind::RiemannPerCell) {
+        if (p.kind == StencilKind::TTI) {
+            const double *src = p.metric_ptr ? p.metric_ptr : p.metric.data();
+            const double *m = src + (p.metric_constant ? 0 : cell * 14);
+            for (int k = 0; k < 14; ++k) out[k] = m[k];
+        } else if (p.kind == StencilKind::RiemannPerCell) {
             const int n = ns();
             const double *src = p.metric_ptr ? p.metric_ptr : p.metric.data();
             const double *m = src + (p.metric_constant ? 0 : cell * n);
@@ -126,7 +134,11 @@ struct SeedGuess {
     // the norm from interpolated or cell data: Riemann matrices rescaled to grid units
     void finish(const double *in, double *norm) const {
         const int D = pm.ndim;
-        if (p.kind == StencilKind::RiemannPerCell && !p.diagonal) {
+        if (p.kind == StencilKind::TTI) {  // linear (2), quadratic (3), transform(i, j) at 5 + 3 i + j
+            for (int k = 0; k < 14; ++k) norm[k] = in[k];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) norm[5 + 3 * i + j] *= pm.scale[j];
+        } else if (p.kind == StencilKind::RiemannPerCell && !p.diagonal) {
             double m[6];
             for (int k = 0; k < ns(); ++k) m[k] = in[k];
             if (p.dual) {  // Inverse = Comatrix / Determinant (SymmetricMatrixType.hxx:201-242)
@@ -158,6 +170,7 @@ struct SeedGuess {
     }
     double apply(const double *norm, const double *v) const {
         const int D = pm.ndim;
+        if (p.kind == StencilKind::TTI) return tti_norm(norm, v);
         if (p.kind == StencilKind::RiemannPerCell && !p.diagonal) {  // sqrt(<v, M v>)
             auto c = [&](int i, int j) { return i >= j ? norm[i * (i + 1) / 2 + j] : norm[j * (j + 1) / 2 + i]; };
             double sum = 0.;
@@ -172,6 +185,61 @@ struct SeedGuess {
         for (int i = 0; i < D; ++i) s += (norm[i] * v[i]) * (norm[i] * v[i]);
         return std::sqrt(s);
     }
+    // TTINorm::Norm (TTINorm.hxx:331-336) = <Gradient(v), v>, the gradient from the optimized
+    // variant of TTINorm::Gradient (TTINorm.hxx:268-329): in the plane (|(Av)_xy|, (Av)_z) of the
+    // transformed vector, maximise <q, p> subject to the level 1 - <l, (x^2, y^2)> - 1/2 <(x^2, y^2),
+    // Q (x^2, y^2)> >= 0 by 8 steps of sequential quadratic programming (AD2::SQP, AD2.h:124-140:
+    // h = lambda H^-1 q - H^-1 g, lambda = -sqrt((<H^-1 g, g> - 2 f) / <H^-1 q, q>)), the first one
+    // in closed form; then map back through the transposed transform. Sums start from 0 and
+    // divisions of vectors and matrices multiply by the reciprocal, as in the reference's algebra.
+    static double tti_norm(const double *m, const double *v) {
+        if (v[0] == 0. && v[1] == 0. && v[2] == 0.) return 0.;
+        const double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4];
+        auto A = [&](int i, int j) { return m[5 + 3 * i + j]; };  // the guess reads the transform row by row
+        double q1[3];
+        for (int i = 0; i < 3; ++i) {
+            q1[i] = 0.;
+            for (int j = 0; j < 3; ++j) q1[i] += A(i, j) * v[j];
+        }
+        const double q[2] = {std::sqrt(q1[0] * q1[0] + q1[1] * q1[1]), q1[2]};
+        const double q0a = q[0] / a, q1b = q[1] / b;
+        const double r0 = 1. / std::sqrt(q[0] * q0a + q[1] * q1b);
+        double pp[2] = {q0a * r0, q1b * r0};
+        for (int it = 1; it < 8; ++it) {
+            const double x = pp[0], y = pp[1];
+            const double x2 = x * x, y2 = y * y, cx2 = c * x2, ey2 = e * y2, dx2 = d * x2, dy2 = d * y2;
+            const double f = 1. - (a * x2 + b * y2 + 0.5 * (cx2 * x2 + 2. * dx2 * y2 + ey2 * y2));
+            const double g[2] = {-2. * (x * (a + cx2 + dy2)), -2. * (y * (b + dx2 + ey2))};
+            const double h[3] = {-2. * (a + 3. * cx2 + dy2), -2. * (2. * d * x * y), -2. * (b + dx2 + 3. * ey2)};
+            const double det = h[0] * h[2] - h[1] * h[1];
+            const double idet = 1. / det;  // Comatrix / Determinant
+            const double hi[3] = {h[2] * idet, -h[1] * idet, h[0] * idet};
+            double hg[2], hq[2];
+            for (int i = 0; i < 2; ++i) {
+                hg[i] = 0.;
+                hq[i] = 0.;
+                for (int j = 0; j < 2; ++j) {
+                    const double hij = hi[i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i];
+                    hg[i] += hij * g[j];
+                    hq[i] += hij * q[j];
+                }
+            }
+            double num = 0., den = 0.;
+            for (int i = 0; i < 2; ++i) { num += hg[i] * g[i]; den += hq[i] * q[i]; }
+            num -= 2. * f;
+            const double lambda = -std::sqrt(num / den);
+            for (int i = 0; i < 2; ++i) pp[i] += lambda * hq[i] - hg[i];
+        }
+        const double n01 = q[0];
+        const double w[3] = {n01 == 0. ? 0. : pp[0] * q1[0] / n01, n01 == 0. ? 0. : pp[0] * q1[1] / n01, pp[1]};
+        double norm = 0.;
+        for (int i = 0; i < 3; ++i) {
+            double gi = 0.;
+            for (int j = 0; j < 3; ++j) gi += A(j, i) * w[j];
+            norm += gi * v[i];
+        }
+        return norm;
+    }
     bool cell_of(const int64_t *idx, int64_t *lin) const {
         int64_t r = 0;
         for (int a = 0; a < pm.ndim; ++a) {
@@ -184,7 +252,7 @@ struct SeedGuess {
     void at_cell(const int64_t *idx, double *norm) const {
         int64_t lin;
         cell_of(idx, &lin);
-        double d[6];
+        double d[14];
         raw(lin, d);
         finish(d, norm);
     }
@@ -199,7 +267,7 @@ struct SeedGuess {
             dir[i] = diff > 0 ? 1 : -1;
             w[i] = std::abs(diff);
         }
-        double acc[6] = {0, 0, 0, 0, 0, 0};
+        double acc[14] = {};
         for (int i = 0; i < (1 << D); ++i) {
             int64_t idx[3];
             double wt = 1.;
@@ -212,7 +280,7 @@ struct SeedGuess {
             const bool inside = cell_of(idx, &lin);
             if (!inside) wt = 0.;
             if (i > 0 && wt == 0) continue;  // the first term is always evaluated (MapWeightedSum.h)
-            double d[6] = {0, 0, 0, 0, 0, 0};
+            double d[14] = {};
             if (inside) raw(lin, d);
             for (int k = 0; k < n; ++k) acc[k] = i == 0 ? wt * d[k] : acc[k] + wt * d[k];
         }
@@ -239,10 +307,10 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
         if (radius < 0)
             throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 (stencil-step spreading) is not supported by the GPU solve path");
         if (radius > 0) {
-            const bool guessable = p.kind == StencilKind::RiemannPerCell ||
+            const bool guessable = p.kind == StencilKind::RiemannPerCell || p.kind == StencilKind::TTI ||
                                    (p.kind == StencilKind::SharedByTheta && !p.angular);
             if (!guessable)
-                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius > 0 is supported for the Riemann, Isotropic and Diagonal models only");
+                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius > 0 is supported for the Riemann, Isotropic, Diagonal and TTI3 models only");
             const int D = pm.ndim;
             SeedGuess G{p, pm};
             std::vector<double> npts, nvals;
@@ -254,7 +322,7 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
                 double q[3];
                 for (int a = 0; a < D; ++a) q[a] = (pts[i * D + a] - pm.origin[a]) / pm.scale[a];  // ADim
                 std::set<std::vector<int64_t>> seen;
-                double distp[6];
+                double distp[14];
                 G.at_point(q, distp);
                 auto insert = [&](const int64_t *index, double rad) {
                     double v[3], nn = 0.;
@@ -263,7 +331,7 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
                     if (!seen.insert(std::vector<int64_t>(index, index + D)).second) return;
                     int64_t lin;
                     if (!G.cell_of(index, &lin)) return;
-                    double distq[6];
+                    double distq[14];
                     G.at_cell(index, distq);
                     for (int a = 0; a < D; ++a) npts.push_back(((double)index[a] + 0.5) * pm.scale[a] + pm.origin[a]);
                     nvals.push_back(vals[i] + 0.5 * (G.apply(distp, v) + G.apply(distq, v)));

@@ -78,15 +78,17 @@ __host__ __device__ __forceinline__ void tti_cross(const int *u, const int *v, i
     o[2] = u[0] * v[1] - u[1] * v[0];
 }
 
-// Norm set-up from the 14 metric values (linear 2, quadratic xx,xy,yy, transform with entry
-// 5 + i + 3 j = transform(i, j), the order in which the reference's field reader fills it), the
-// grid scales and the obtuse superbase at tmin. False if the element is not a valid TTI norm.
+// Norm set-up from the 14 metric values (linear 2, quadratic xx,xy,yy, then the transform, which
+// the reference reads row by row: element 5 + 3 i + j is its transform(i, j)), the grid scales and
+// the obtuse superbase at tmin. T below holds that transform transposed, T(i, j) = element
+// 5 + i + 3 j; MakeNorm scales column j of the transform by h_j (TTI.hpp:24-34), i.e. row i of T by
+// h_i. False if the element is not a valid TTI norm.
 __host__ __device__ inline bool tti_setup(const double *m, const double *h, TTICell &n) {
     n.l0 = m[0]; n.l1 = m[1];
     n.q00 = m[2]; n.q01 = m[3]; n.q11 = m[4];
     double T[3][3], B[3][3];
     for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) T[i][j] = m[5 + i + 3 * j] * h[j];
+        for (int j = 0; j < 3; ++j) T[i][j] = m[5 + i + 3 * j] * h[i];
     double det = 0.0;
     for (int i = 0; i < 3; ++i)
         det += T[i][0] * T[(i + 1) % 3][1] * T[(i + 2) % 3][2] - T[i][2] * T[(i + 1) % 3][1] * T[(i + 2) % 3][0];

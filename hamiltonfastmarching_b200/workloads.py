@@ -255,7 +255,10 @@ def thomsen_tti(vp, eps, delta, dip, azimuth) -> np.ndarray:
     sd, cd, sa, ca = np.sin(dip), np.cos(dip), np.sin(azimuth), np.cos(azimuth)
     # rows: e1 = (cd ca, cd sa, -sd), e2 = (-sa, ca, 0), n = (sd ca, sd sa, cd)
     rows = [(cd * ca, cd * sa, -sd), (-sa, ca, 0 * sd), (sd * ca, sd * sa, cd)]
-    for i in range(3):  # transform(i, j) is element 5 + i + 3 j
+    # element 5 + i + 3 j holds rows[i][j]; the reference reads the transform row by row, so its
+    # transform is this rotation transposed, whose inverse transpose (the map its dual unit ball
+    # applies to a slowness vector) is this rotation again
+    for i in range(3):
         for j in range(3):
             out[..., 5 + i + 3 * j] = rows[i][j]
     return out

@@ -897,11 +897,13 @@ static double tti_spr(double l, double q) {
 static int tti_setup(const double *m, const double *h, tti_norm *n) {
     n->l0 = m[0]; n->l1 = m[1];
     n->q00 = m[2]; n->q01 = m[3]; n->q11 = m[4];
-    /* transform(i, j) is element 5 + i + 3 j of the 14 values: the order in which the reference's
-     * field reader fills its transform (pinned against the reference executable) */
+    /* the reference reads the transform row by row (element 5 + 3 i + j is its transform(i, j));
+     * T holds it transposed, T(i, j) = element 5 + i + 3 j, and MakeNorm's scaling of column j by
+     * h_j is a scaling of row i of T by h_i (pinned against the reference executable, non-uniform
+     * grid scales included) */
     double T[3][3], B[3][3];
     for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) T[i][j] = m[5 + i + 3 * j] * h[j];
+        for (int j = 0; j < 3; ++j) T[i][j] = m[5 + i + 3 * j] * h[i];
     double det = 0.0;
     for (int i = 0; i < 3; ++i)
         det += T[i][0] * T[(i + 1) % 3][1] * T[(i + 2) % 3][2] - T[i][2] * T[(i + 1) % 3][1] * T[(i + 2) % 3][0];

@@ -87,7 +87,7 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
 int fmo_visibility(const fmo_problem *p, int max_width, uint8_t *visible);
 
 /* TTI3 (semi-Lagrangian, nmix = 0): metric[N][14] = linear(2), quadratic (xx,xy,yy), transform
- * 3x3 with transform(i, j) at element 5 + i + 3 j; h[3] grid scales. values[N] out, t_active[N] (may be NULL) receives the
+ * 3x3 read row by row (transform(i, j) at element 5 + 3 i + j); h[3] grid scales. values[N] out, t_active[N] (may be NULL) receives the
  * reference's activeNeighs encoding (t of the extremum, negative at an interval endpoint).
  * Returns the accepted count, or -1. */
 int64_t fmo_tti_fast_marching(const int64_t *dims, const double *h, const double *metric, int nseeds,

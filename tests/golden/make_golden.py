@@ -254,6 +254,18 @@ def spreading_fixtures():
                                        "seedRadius": 2.2, "exportValues": 1.0})
 
 
+def tti_spreading_fixtures():
+    """seedRadius > 0 on TTI3: the guess is the TTI norm of the metric interpolated at the seed and
+    of the metric at the cell (the transform's columns scaled by the grid scales)."""
+    p = W.tti3_case(12, h=0.01, seed=6)
+    p.pop("_vp")
+    solve_fixture("spread_tti3", dict(p, seeds=np.array([[0.043, 0.061, 0.052], [0.021, 0.093, 0.011]]),
+                                      seedRadius=2.0))
+    q = {k: v for k, v in W.tti3_case(10, h=0.01, seed=7).items() if k not in ("_vp", "gridScale")}
+    solve_fixture("spread_tti3_scales", dict(q, gridScales=np.array([0.01, 0.012, 0.009]),
+                                             seeds=np.array([[0.0512, 0.0433, 0.0017]]), seedRadius=1.5))
+
+
 def diagonal_variation_fixtures():
     """First variations of the Diagonal models, per axis: costSensitivity dims + (D,), costVariation
     dims + (nVar, D)."""
@@ -338,7 +350,8 @@ def forward_curvature_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2` regenerates only those fixtures
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread`
+    # regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
     elif sys.argv[1:] == ["geodesic"]:
@@ -357,6 +370,8 @@ if __name__ == "__main__":
         diagonal_variation_fixtures()
     elif sys.argv[1:] == ["rsf2"]:
         forward_curvature_fixtures()
+    elif sys.argv[1:] == ["ttispread"]:
+        tti_spreading_fixtures()
     else:
         main()
         tti_fixtures()

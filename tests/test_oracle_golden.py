@@ -207,3 +207,19 @@ def test_rsf2_exact_angular_tie_moves_one_cell():
     assert int(far.sum()) == 1
     res["activeNeighs"] = np.ascontiguousarray(act.ravel())
     np.testing.assert_array_equal(O.forward_variation(res, params), r)
+
+
+@pytest.mark.parametrize("name", ["spread_tti3", "spread_tti3_scales"])
+def test_tti_oracle_from_spread_seeds_matches_reference(name):
+    """TTI3 solved from the reference's spreadedSeeds / spreadedSeedValues: the reference's values
+    within 1e-14 (relative) and its nAccepted, also with distinct grid scales per axis, where the
+    transform's scaling axis matters."""
+    params, ref, _ = load_golden(name)
+    q = {k: v for k, v in params.items() if k != "seedRadius"}
+    q["seeds"], q["seedValues"] = ref["spreadedSeeds"], ref["spreadedSeedValues"]
+    res = O.tti_solve(q)
+    a, b = res["values"], ref["values"]
+    fin = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), fin)
+    assert np.max(np.abs(a[fin] - b[fin])) <= 1e-14 * np.max(np.abs(b[fin]))
+    assert res["nAccepted"] == int(ref["nAccepted"])

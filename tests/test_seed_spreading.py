@@ -9,7 +9,8 @@ import pytest
 import hamiltonfastmarching_b200 as H
 from conftest import load_golden
 
-SPREAD = ["spread_riemann2_dual", "spread_riemann3_walls", "spread_isotropic2", "spread_diagonal3"]
+SPREAD = ["spread_riemann2_dual", "spread_riemann3_walls", "spread_isotropic2", "spread_diagonal3", "spread_tti3",
+          "spread_tti3_scales"]
 
 
 @pytest.mark.parametrize("name", SPREAD)
