@@ -248,6 +248,28 @@ int fmo_reedssheppforward2_table(int ntheta, double h, double xi, double eps,
     return 0;
 }
 
+/* StencilDubins2::SetStencil (Curvature2.h:119-140): per angle two stencils of 6 forward
+ * differences, the first from the 3D Voronoi1Vec of (cos/h, sin/h, 1/(xi dtheta)), the second the
+ * same with the angular component of each offset negated. Layout per angle: 12 forward
+ * differences, stencil 0 then stencil 1. */
+int fmo_dubins2_table(int ntheta, double h, double xi, double eps, int8_t *offsets, double *weights) {
+    const double ds = (2.0 * kPi) / (double)ntheta;
+    for (int t = 0; t < ntheta; ++t) {
+        const double theta = (double)t * ds;
+        const double v[3] = {cos(theta) / h, sin(theta) / h, 1. / (xi * ds)};
+        int8_t *O = offsets + t * 36;
+        double *W = weights + t * 12;
+        if (fmo_voronoi1vec(3, v, eps, O, W)) return -1;
+        for (int i = 0; i < 6; ++i) {
+            W[6 + i] = W[i];
+            O[(6 + i) * 3 + 0] = O[i * 3 + 0];
+            O[(6 + i) * 3 + 1] = O[i * 3 + 1];
+            O[(6 + i) * 3 + 2] = (int8_t)(-O[i * 3 + 2]);
+        }
+    }
+    return 0;
+}
+
 /* StencilElastica2<5>::SetStencil (Curvature2.h:178-234): Fejer quadrature over 5 points; for
  * l = 0,1 a 3D Voronoi1Vec (6 offsets) and its mirror in theta, then a 2D one (3 offsets). */
 int fmo_elastica2_table(int ntheta, double h, double xi, double eps,
@@ -559,7 +581,9 @@ int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active
 
     uint8_t *accepted = (uint8_t *)calloc(N, 1);
     uint64_t *act = active ? active : (uint64_t *)calloc(N, sizeof(uint64_t));
-    quad_t *quads = (quad_t *)calloc(N, sizeof(quad_t));
+    const int nq = p->nmax == 2 ? 2 : 1;
+    if (nq == 2 && (p->nsym != 0 || p->nfwd % 2)) return -1;
+    quad_t *quads = (quad_t *)calloc(N * nq, sizeof(quad_t));
     heap_t heap = {0};
     if (!accepted || !act || !quads) return -1;
     if (active) memset(active, 0, N * sizeof(uint64_t));
@@ -620,8 +644,10 @@ int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active
             if (values[u] <= top.val) continue;
             /* Update + HopfLaxUpdate (HFM_StencilRecompute.hxx:48-57, HFM_StencilShare.hxx:74-84,
              * EulerianStencil.hxx:104-153) */
-            quad_t *q = &quads[u];
-            if (!q->used) { q->used = 1; q->minVal = top.val; q->a = 0; q->b = 0; q->c = -1; }
+            quad_t *q = &quads[u * nq];
+            if (!q->used) {
+                for (int i = 0; i < nq; ++i) { q[i].used = 1; q[i].minVal = top.val; q[i].a = 0; q[i].b = 0; q[i].c = -1; }
+            }
             const int64_t sid = stencil_id(p, uidx, u);
             const int8_t *O = p->off + sid * nd * 3;
             const double *W = p->w + sid * nd;
@@ -630,7 +656,7 @@ int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active
                 const int8_t *o = O + 3 * k;
                 if (o[0] == e[0] && o[1] == e[1] && o[2] == e[2]) {
                     act[u] |= (1ULL << bit);
-                    quad_add(q, top.val, diff_weight(p, W[k], u));
+                    quad_add(q + (nq == 2 && k >= p->nfwd / 2), top.val, diff_weight(p, W[k], u));
                 }
             }
             for (int k = p->nfwd; k < nd; ++k, bit += 2) {
@@ -648,7 +674,26 @@ int64_t fmo_fast_marching(const fmo_problem *p, double *values, uint64_t *active
                     }
                 }
             }
-            const double val = quad_solve(q);
+            double val;
+            if (nq == 2) {
+                /* QuadraticMax<., 2>::Solve (EulerianStencil.hxx:30-50): the smaller root, the first
+                 * stencil on ties; SetIMax records it in the bit after the differences */
+                int imin = 0;
+                double res = FMO_INF;
+                for (int i = 0; i < 2; ++i) {
+                    if (q[i].a == 0.0) continue;
+                    const double delta2 = q[i].b * q[i].b - q[i].a * q[i].c;
+                    const double r = (q[i].b + sqrt(0.0 < delta2 ? delta2 : 0.0)) / q[i].a;
+                    if (r >= res) continue;
+                    imin = i;
+                    res = r;
+                }
+                val = q[0].minVal + res;
+                if (imin) act[u] |= (1ULL << p->nfwd);
+                else act[u] &= ~(1ULL << p->nfwd);
+            } else {
+                val = quad_solve(q);
+            }
             values[u] = val;
             heap_push(&heap, (qelem){u, val});
         }
@@ -794,6 +839,7 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
                                int npts, const int64_t *pt_index, const double *pt_weight,
                                double *sensitivity, int64_t max_seeds, int64_t *seed_out_index,
                                double *seed_out_weight) {
+    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     const int64_t N = ncells(p);
     /* pending weight per cell; in_map marks membership of (values[x], x) in the ordered set */
     double *pend = (double *)calloc(N, sizeof(double));
@@ -1748,6 +1794,7 @@ static int64_t geo_discrete_all(const fmo_problem *grid, const double *values, g
 int64_t fmo_geodesic_discrete(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
                               const double *tips, double step, double threshold, double volume_bound,
                               int64_t max_points, double *points, int64_t *lengths, int *failed) {
+    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     eul_ctx E = {p, values, active};
     return geo_discrete_all(p, values, eul_recompute, &E, ntips, tips, step, threshold, volume_bound, max_points,
                             points, lengths, failed);
@@ -1789,6 +1836,7 @@ static void geo_flow_all(const fmo_problem *grid, geo_flow_fn flow, void *ctx, d
 
 int fmo_geodesic_flow(const fmo_problem *p, const double *values, const uint64_t *active, double *flow,
                       double *value, double *width) {
+    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     eul_ctx E = {p, values, active};
     geo_flow_all(p, eul_recompute, &E, flow, value, width);
     return 0;
@@ -1830,6 +1878,7 @@ static vkey *sorted_cells(const double *values, int64_t N) {
 
 int fmo_forward_variation(const fmo_problem *p, const double *values, const uint64_t *active, int nvar,
                           const double *cost_var, double *result) {
+    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     const int64_t N = ncells(p);
     vkey *order = sorted_cells(values, N);
     if (!order) return -1;
@@ -2097,6 +2146,7 @@ static int64_t ode_all(const fmo_problem *grid, geo_flow_fn flow, void *ctx, con
 int64_t fmo_geodesic_ode(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
                          const double *tips, double step, double causality, int64_t max_points, double *points,
                          int64_t *lengths, int *failed) {
+    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     eul_ctx E = {p, values, active};
     return ode_all(p, eul_recompute, &E, p->seed_index, p->nseeds, ntips, tips, step, causality, max_points, points,
                    lengths, failed);

@@ -36,7 +36,9 @@ int fmo_reedsshepp2_table(int ntheta, double h, double xi, double eps, int proje
                           int8_t *offsets, double *weights);
 int fmo_elastica2_table(int ntheta, double h, double xi, double eps,
                         int8_t *offsets, double *weights);
-/* ReedsSheppForward2: 3 forward differences then 1 symmetric (angular) per angle. */
+/* ReedsSheppForward2: 3 forward differences then 1 symmetric (angular) per angle.
+ * Dubins2: 12 forward differences per angle, two stencils of 6 (nmax = 2). */
+int fmo_dubins2_table(int ntheta, double h, double xi, double eps, int8_t *offsets, double *weights);
 int fmo_reedssheppforward2_table(int ntheta, double h, double xi, double eps,
                                  int8_t *offsets, double *weights);
 
@@ -65,6 +67,11 @@ typedef struct {
      * and mult_vec[N][var_dim] the speeds; 0 (or 1) and NULL otherwise. */
     int var_dim;
     const double *mult_vec;
+    /* nmax = 2: the forward differences form two stencils of nfwd / 2 each and the value is the
+     * smaller of their two solutions (EulerianStencil<.., nMax = 2>, EulerianStencil.hxx:13-50,
+     * 104-153); activeNeighs bit nfwd records which one. 0 or 1: one stencil. Only
+     * fmo_fast_marching supports nmax = 2. */
+    int nmax;
 } fmo_problem;
 
 /* Fast marching. values[N] out; active[N] out (bitset, forward bits then symmetric +/- pairs,

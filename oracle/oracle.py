@@ -54,6 +54,7 @@ class _Problem(ctypes.Structure):
         ("stop_all_u", _P),
         ("var_dim", ctypes.c_int),
         ("mult_vec", _P),
+        ("nmax", ctypes.c_int),
     ]
 
 
@@ -79,6 +80,7 @@ def lib():
                                           ctypes.c_double, _P, _P]
         L.fmo_reedssheppforward2_table.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                    ctypes.c_double, _P, _P]
+        L.fmo_dubins2_table.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _P]
         L.fmo_fast_marching.argtypes = [ctypes.POINTER(_Problem), _P, _P, _P]
         L.fmo_fast_marching.restype = ctypes.c_int64
         L.fmo_backward_variation.argtypes = [ctypes.POINTER(_Problem), _P, _P, ctypes.c_int, _P, _P,
@@ -158,6 +160,10 @@ def curvature2_table(model: str, ntheta: int, h: float, xi: float, eps: float, p
         off = np.zeros((ntheta, 4, 3), np.int8)
         w = np.zeros((ntheta, 4), np.float64)
         rc = L.fmo_reedssheppforward2_table(ntheta, h, xi, eps, _ptr(off), _ptr(w))
+    elif model == "Dubins2":
+        off = np.zeros((ntheta, 12, 3), np.int8)
+        w = np.zeros((ntheta, 12), np.float64)
+        rc = L.fmo_dubins2_table(ntheta, h, xi, eps, _ptr(off), _ptr(w))
     elif model == "Elastica2":
         off = np.zeros((ntheta, 27, 3), np.int8)
         w = np.zeros((ntheta, 27), np.float64)
@@ -274,7 +280,7 @@ class Problem:
             nfwd, nsym, share = 0, off.shape[1], 0
             scale = hs
             adim = lambda p: (np.asarray(p, float) - origin) / hs
-        elif model in ("ReedsShepp2", "ReedsSheppForward2", "Elastica2"):
+        elif model in ("ReedsShepp2", "ReedsSheppForward2", "Elastica2", "Dubins2"):
             periodic = [0, 0, 1]
             h = float(params["gridScale"])
             xi = float(_get(params, "xi", 1.0))
@@ -287,6 +293,8 @@ class Problem:
                 nfwd, nsym = 0, 4
             elif model == "ReedsSheppForward2":
                 nfwd, nsym = 3, 1
+            elif model == "Dubins2":  # two stencils of 6 forward differences (nmax = 2)
+                nfwd, nsym = 12, 0
             else:
                 nfwd, nsym = 27, 0
             share = 1
@@ -328,6 +336,7 @@ class Problem:
             s.dims[a] = dims[a] if a < ndim else 1
             s.periodic[a] = periodic[a]
         s.nfwd, s.nsym, s.share = nfwd, nsym, share
+        s.nmax = 2 if model == "Dubins2" else 1
         s.off, s.w = _ptr(self.off), _ptr(self.w)
         s.mult = _ptr(self.mult)
         s.walls = _ptr(self.walls)

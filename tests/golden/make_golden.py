@@ -254,6 +254,15 @@ def spreading_fixtures():
                                        "seedRadius": 2.2, "exportValues": 1.0})
 
 
+def dubins_fixtures():
+    """Dubins2 (two stencils of 6 forward differences, the value the smaller of their solutions):
+    values, activeNeighs (with the bit naming the stencil), nAccepted, MaxStencilWidth."""
+    solve_fixture("dubins2_32x24", W.curvature2_case(32, 24, "Dubins2", seed=14, n_curves=6))
+    p = W.curvature2_case(24, 16, "Dubins2", seed=15, n_curves=4)
+    p["walls"] = (np.random.default_rng(16).uniform(size=(24, 24)) < 0.06).astype(float)
+    solve_fixture("dubins2_24x16_walls", p)
+
+
 def tti_spreading_fixtures():
     """seedRadius > 0 on TTI3: the guess is the TTI norm of the metric interpolated at the seed and
     of the metric at the cell (the transform's columns scaled by the grid scales)."""
@@ -350,7 +359,7 @@ def forward_curvature_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread`
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread|dubins`
     # regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
@@ -372,6 +381,8 @@ if __name__ == "__main__":
         forward_curvature_fixtures()
     elif sys.argv[1:] == ["ttispread"]:
         tti_spreading_fixtures()
+    elif sys.argv[1:] == ["dubins"]:
+        dubins_fixtures()
     else:
         main()
         tti_fixtures()

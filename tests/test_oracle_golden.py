@@ -223,3 +223,19 @@ def test_tti_oracle_from_spread_seeds_matches_reference(name):
     assert np.array_equal(np.isfinite(a), fin)
     assert np.max(np.abs(a[fin] - b[fin])) <= 1e-14 * np.max(np.abs(b[fin]))
     assert res["nAccepted"] == int(ref["nAccepted"])
+
+
+@pytest.mark.parametrize("name", ["dubins2_32x24", "dubins2_24x16_walls"])
+def test_dubins2_oracle_bit_exact(name):
+    """Dubins2 (two stencils of 6 forward differences, the value the smaller of their solutions):
+    values, activeNeighs with the bit naming the stencil, nAccepted and MaxStencilWidth as the
+    reference's, bit for bit."""
+    params, ref, _ = load_golden(name)
+    res = O.solve(params)
+    a, b = ref["values"], res["values"]
+    assert np.array_equal(np.isinf(a), np.isinf(b))
+    fin = np.isfinite(a)
+    assert np.array_equal(a[fin], b[fin])
+    assert int(ref["nAccepted"]) == res["nAccepted"]
+    assert int(ref["MaxStencilWidth"]) == res["MaxStencilWidth"]
+    assert np.array_equal(ref["activeNeighs"].ravel().astype(np.uint64), res["activeNeighs"])
