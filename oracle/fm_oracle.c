@@ -789,6 +789,15 @@ static bkey bheap_pop(bheap_t *h) {
 /* ValueVariation for Eulerian stencils (FirstVariation.h:198-251): the active neighbours in
  * stencil order with weights w max(0, value - u_neighbour) normalised by their sum, and the local
  * derivative (sum of w valueDiff) / sum (times the speed multiplier of shared stencils). */
+/* The differences of a Recompute (EulerianStencil.hxx:155-229): every active one, or with two
+ * stencils (nmax = 2) the active ones of the stencil named by bit nfwd (GetIMax). */
+static inline uint64_t recompute_active(const fmo_problem *p, uint64_t act) {
+    if (p->nmax != 2) return act;
+    const int half = p->nfwd / 2;
+    const int imax = (int)((act >> p->nfwd) & 1ULL);
+    return act & (((1ULL << half) - 1ULL) << (imax * half));
+}
+
 static void eul_value_variation(const fmo_problem *p, const double *values, const uint64_t *active, int64_t x,
                                 int64_t *nb_idx, double *nb_w, int *nn_out, double *var) {
     const int nd = p->nfwd + p->nsym;
@@ -799,7 +808,7 @@ static void eul_value_variation(const fmo_problem *p, const double *values, cons
     const int64_t sid = stencil_id(p, idx, x);
     const int8_t *O = p->off + sid * nd * 3;
     const double *W = p->w + sid * nd;
-    const uint64_t act = active[x];
+    const uint64_t act = recompute_active(p, active[x]);
     double weightSum = 0.0;
     for (int i = 0; i < vd; ++i) var[i] = 0.0;
     int nn = 0;
@@ -839,7 +848,6 @@ int64_t fmo_backward_variation(const fmo_problem *p, const double *values, const
                                int npts, const int64_t *pt_index, const double *pt_weight,
                                double *sensitivity, int64_t max_seeds, int64_t *seed_out_index,
                                double *seed_out_weight) {
-    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     const int64_t N = ncells(p);
     /* pending weight per cell; in_map marks membership of (values[x], x) in the ordered set */
     double *pend = (double *)calloc(N, sizeof(double));
@@ -1512,7 +1520,7 @@ static int eul_recompute(void *vctx, int64_t x, int (*off)[3], double *fw, doubl
     const eul_ctx *E = (const eul_ctx *)vctx;
     const fmo_problem *p = E->p;
     const int nd = p->nfwd + p->nsym;
-    const uint64_t act = E->active[x];
+    const uint64_t act = recompute_active(p, E->active[x]);
     *width = 0.0;
     *value = E->values[x];
     if (act == 0) return 0;
@@ -1794,7 +1802,6 @@ static int64_t geo_discrete_all(const fmo_problem *grid, const double *values, g
 int64_t fmo_geodesic_discrete(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
                               const double *tips, double step, double threshold, double volume_bound,
                               int64_t max_points, double *points, int64_t *lengths, int *failed) {
-    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     eul_ctx E = {p, values, active};
     return geo_discrete_all(p, values, eul_recompute, &E, ntips, tips, step, threshold, volume_bound, max_points,
                             points, lengths, failed);
@@ -1836,7 +1843,6 @@ static void geo_flow_all(const fmo_problem *grid, geo_flow_fn flow, void *ctx, d
 
 int fmo_geodesic_flow(const fmo_problem *p, const double *values, const uint64_t *active, double *flow,
                       double *value, double *width) {
-    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     eul_ctx E = {p, values, active};
     geo_flow_all(p, eul_recompute, &E, flow, value, width);
     return 0;
@@ -1878,7 +1884,6 @@ static vkey *sorted_cells(const double *values, int64_t N) {
 
 int fmo_forward_variation(const fmo_problem *p, const double *values, const uint64_t *active, int nvar,
                           const double *cost_var, double *result) {
-    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     const int64_t N = ncells(p);
     vkey *order = sorted_cells(values, N);
     if (!order) return -1;
@@ -2146,7 +2151,6 @@ static int64_t ode_all(const fmo_problem *grid, geo_flow_fn flow, void *ctx, con
 int64_t fmo_geodesic_ode(const fmo_problem *p, const double *values, const uint64_t *active, int ntips,
                          const double *tips, double step, double causality, int64_t max_points, double *points,
                          int64_t *lengths, int *failed) {
-    if (p->nmax == 2) return -1;  /* two-stencil (Dubins2) Recompute not restated */
     eul_ctx E = {p, values, active};
     return ode_all(p, eul_recompute, &E, p->seed_index, p->nseeds, ntips, tips, step, causality, max_points, points,
                    lengths, failed);

@@ -69,8 +69,8 @@ typedef struct {
     const double *mult_vec;
     /* nmax = 2: the forward differences form two stencils of nfwd / 2 each and the value is the
      * smaller of their two solutions (EulerianStencil<.., nMax = 2>, EulerianStencil.hxx:13-50,
-     * 104-153); activeNeighs bit nfwd records which one. 0 or 1: one stencil. Only
-     * fmo_fast_marching supports nmax = 2. */
+     * 104-153); activeNeighs bit nfwd records which one, and a Recompute (geodesics, first
+     * variations) uses that stencil only. 0 or 1: one stencil. */
     int nmax;
 } fmo_problem;
 

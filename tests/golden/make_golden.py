@@ -256,11 +256,21 @@ def spreading_fixtures():
 
 def dubins_fixtures():
     """Dubins2 (two stencils of 6 forward differences, the value the smaller of their solutions):
-    values, activeNeighs (with the bit naming the stencil), nAccepted, MaxStencilWidth."""
+    values, activeNeighs (with the bit naming the stencil), nAccepted, MaxStencilWidth; the last
+    one also geodesics, the geodesic flow and both first variations."""
     solve_fixture("dubins2_32x24", W.curvature2_case(32, 24, "Dubins2", seed=14, n_curves=6))
     p = W.curvature2_case(24, 16, "Dubins2", seed=15, n_curves=4)
     p["walls"] = (np.random.default_rng(16).uniform(size=(24, 24)) < 0.06).astype(float)
     solve_fixture("dubins2_24x16_walls", p)
+    rng = np.random.default_rng(17)
+    p = W.curvature2_case(24, 16, "Dubins2", seed=18, n_curves=4)
+    p["tips"] = np.c_[rng.uniform(0.1, 0.9, (3, 2)), rng.uniform(0, 6.2, (3, 1))]
+    p["tips_Unoriented"] = rng.uniform(0.1, 0.9, (3, 2))
+    p["exportGeodesicFlow"] = 1.0
+    p["costVariation"] = rng.standard_normal((24, 24, 16, 1))
+    p["seedValueVariation"] = np.array([[0.7]])
+    pts = np.c_[rng.uniform(0.1, 0.9, (3, 2)), rng.uniform(0, 6, (3, 1))]
+    solve_fixture("dubins2_24x16_geo", p, (pts, rng.uniform(0.5, 2.0, 3)))
 
 
 def tti_spreading_fixtures():

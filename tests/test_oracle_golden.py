@@ -73,7 +73,7 @@ def test_tti_oracle_matches_reference():
 
 GOLDEN_GEODESICS = ["geo_riemann2_48_walls", "geo_riemann3_16_walls", "geo_reedsshepp2_24x16", "geo_elastica2_24x16",
                     "geo_tti3_12", "ode_riemann2_48_walls", "ode_riemann3_16_walls", "ode_reedsshepp2_24x16",
-                    "ode_elastica2_24x16", "ode_tti3_12", "rsf2_24x16_walls"]
+                    "ode_elastica2_24x16", "ode_tti3_12", "rsf2_24x16_walls", "dubins2_24x16_geo"]
 
 
 @pytest.mark.parametrize("name", GOLDEN_GEODESICS)
@@ -104,7 +104,7 @@ def test_geodesic_oracle_matches_reference(name):
 
 
 GOLDEN_VARIATIONS = ["fwd_riemann2_40_seeds", "fwd_riemann3_16_walls", "fwd_reedsshepp2_20x12", "fwd_elastica2_20x12",
-                     "fwd_tti3_12", "rsf2_24x16_walls"]
+                     "fwd_tti3_12", "rsf2_24x16_walls", "dubins2_24x16_geo"]
 
 
 @pytest.mark.parametrize("name", GOLDEN_VARIATIONS)
@@ -225,11 +225,11 @@ def test_tti_oracle_from_spread_seeds_matches_reference(name):
     assert res["nAccepted"] == int(ref["nAccepted"])
 
 
-@pytest.mark.parametrize("name", ["dubins2_32x24", "dubins2_24x16_walls"])
+@pytest.mark.parametrize("name", ["dubins2_32x24", "dubins2_24x16_walls", "dubins2_24x16_geo"])
 def test_dubins2_oracle_bit_exact(name):
     """Dubins2 (two stencils of 6 forward differences, the value the smaller of their solutions):
-    values, activeNeighs with the bit naming the stencil, nAccepted and MaxStencilWidth as the
-    reference's, bit for bit."""
+    values, activeNeighs with the bit naming the stencil, nAccepted, MaxStencilWidth and the
+    reverse first variation (Recompute on the named stencil) as the reference's, bit for bit."""
     params, ref, _ = load_golden(name)
     res = O.solve(params)
     a, b = ref["values"], res["values"]
