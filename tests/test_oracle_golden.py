@@ -239,3 +239,7 @@ def test_dubins2_oracle_bit_exact(name):
     assert int(ref["nAccepted"]) == res["nAccepted"]
     assert int(ref["MaxStencilWidth"]) == res["MaxStencilWidth"]
     assert np.array_equal(ref["activeNeighs"].ravel().astype(np.uint64), res["activeNeighs"])
+    if "costSensitivity_0" in ref:
+        sens, _, sw = O.backward_variation(res, params["inspectSensitivity"], params["inspectSensitivityWeights"])
+        assert np.array_equal(ref["costSensitivity_0"], sens)
+        np.testing.assert_array_equal(ref["seedSensitivity_0"][:, -1], sw)
