@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "common.cuh"
 #include "io.hpp"
+#include "selling.cuh"
 #include "store_handle.hpp"
 #include "solver.hpp"
 
@@ -288,6 +290,75 @@ struct SeedGuess {
     }
 };
 
+// Reversed offsets of a cell x of a Riemann model (HFM_StencilRecompute.hxx:85-124): the offsets e,
+// sorted and without repeats, such that e or -e is a difference of nonzero weight of the Selling
+// stencil of y = x - e, y in the domain (no walls, no periodic axes here). The stencils scanned are
+// those of the cells within `width` (the largest offset component of the domain's stencils) of x.
+void riemann_cell_stencil(const EulerProblem &p, const Param &pm, int64_t lin, int off[6][3], double w[6]) {
+    SeedGuess G{p, pm};
+    double m[6];
+    G.raw(lin, m);
+    const bool ok = pm.ndim == 2 ? riemann_stencil<2>(m, p.dual, p.h, off, w) : riemann_stencil<3>(m, p.dual, p.h, off, w);
+    if (!ok) throw Error(HFM_ERR_VALUE, "Error : metric is not positive definite");
+}
+
+int riemann_max_width(const EulerProblem &p, const Param &pm) {
+    int64_t ncell = 1;
+    for (int a = 0; a < pm.ndim; ++a) ncell *= pm.dims[a];
+    int width = 0;
+    for (int64_t lin = 0; lin < ncell; ++lin) {
+        int off[6][3];
+        double w[6];
+        riemann_cell_stencil(p, pm, lin, off, w);
+        for (int k = 0; k < (pm.ndim == 2 ? 3 : 6); ++k)
+            for (int a = 0; a < pm.ndim; ++a) width = std::max(width, std::abs(off[k][a]));
+        if (p.metric_constant) break;
+    }
+    return width;
+}
+
+std::vector<std::array<int, 3>> reversed_offsets(const EulerProblem &p, const Param &pm, const int64_t *x, int width) {
+    const int D = pm.ndim;
+    SeedGuess G{p, pm};
+    const int nk = D == 2 ? 3 : 6;
+    for (int a = 0; a < D; ++a)
+        if (x[a] < 0 || x[a] >= pm.dims[a])
+            throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 with a seed closer to the domain boundary than the radius "
+                                             "is not supported by the GPU solve path");
+    std::set<std::array<int, 3>> out;
+    const int side = 2 * width + 1;
+    int64_t box = 1;
+    for (int a = 0; a < D; ++a) box *= side;
+    for (int64_t b = 0; b < box; ++b) {
+        int64_t y[3] = {0, 0, 0}, r = b;
+        bool inside = true;
+        for (int a = D - 1; a >= 0; --a) {
+            y[a] = x[a] + (r % side) - width;
+            r /= side;
+            inside = inside && y[a] >= 0 && y[a] < pm.dims[a];
+        }
+        if (!inside) continue;
+        int64_t lin = 0;
+        G.cell_of(y, &lin);
+        int off[6][3];
+        double w[6];
+        riemann_cell_stencil(p, pm, lin, off, w);
+        for (int k = 0; k < nk; ++k) {
+            if (w[k] == 0.) continue;
+            for (int sgn = 1; sgn >= -1; sgn -= 2) {
+                std::array<int, 3> e = {0, 0, 0};
+                bool hit = true;
+                for (int a = 0; a < D; ++a) {
+                    e[a] = sgn * off[k][a];
+                    hit = hit && y[a] + e[a] == x[a];
+                }
+                if (hit) out.insert(e);
+            }
+        }
+    }
+    return std::vector<std::array<int, 3>>(out.begin(), out.end());
+}
+
 // Seeds: points -> unique indices (first value kept), sorted; with seedRadius > 0 each seed is
 // spread to the cells whose centre lies within that many cells of it (StaticFactoring.hxx:242-346).
 
@@ -303,9 +374,16 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
             vals = io.get_vector("seedValues", 1, &nv);
             if (nv != n) throw Error(HFM_ERR_VALUE, "Error : Inconsistent size of seedValues.");
         }
-        const double radius = io.get_scalar("seedRadius", 0.0);
-        if (radius < 0)
-            throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 (stencil-step spreading) is not supported by the GPU solve path");
+        // seedRadius < 0: spread to |seedRadius|, then one step of the reversed stencils
+        const double radius_in = io.get_scalar("seedRadius", 0.0);
+        const bool stencil_step = radius_in < 0;
+        const double radius = std::abs(radius_in);
+        if (stencil_step) {
+            if (p.kind != StencilKind::RiemannPerCell || p.diagonal)
+                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 (stencil-step spreading) is supported for the Riemann models only");
+            if (io.has_field("walls") || pm.periodic[0] || pm.periodic[1] || pm.periodic[2])
+                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 with walls or periodic axes is not supported by the GPU solve path");
+        }
         if (radius > 0) {
             const bool guessable = p.kind == StencilKind::RiemannPerCell || p.kind == StencilKind::TTI ||
                                    (p.kind == StencilKind::SharedByTheta && !p.angular);
@@ -318,6 +396,7 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
             const int side = 1 + 2 * bd;
             int64_t box = 1;
             for (int a = 0; a < D; ++a) box *= side;
+            int width = -1;  // largest stencil offset component, computed on first use
             for (int64_t i = 0; i < n; ++i) {
                 double q[3];
                 for (int a = 0; a < D; ++a) q[a] = (pts[i * D + a] - pm.origin[a]) / pm.scale[a];  // ADim
@@ -343,6 +422,17 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
                     int64_t idx[3], r = k;
                     for (int a = D - 1; a >= 0; --a) { idx[a] = pidx[a] + (r % side) - bd; r /= side; }
                     insert(idx, radius);
+                }
+                if (stencil_step) {  // every index seen so far, in index order, plus its reversed offsets
+                    if (width < 0) width = riemann_max_width(p, pm);
+                    const std::set<std::vector<int64_t>> base = seen;
+                    for (const std::vector<int64_t> &x : base) {
+                        for (const std::array<int, 3> &e : reversed_offsets(p, pm, x.data(), width)) {
+                            int64_t idx[3];
+                            for (int a = 0; a < D; ++a) idx[a] = x[a] + e[a];
+                            insert(idx, std::numeric_limits<double>::infinity());
+                        }
+                    }
                 }
             }
             io.set_vector("spreadedSeeds", (int64_t)nvals.size(), D, npts.data());

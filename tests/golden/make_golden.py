@@ -273,6 +273,15 @@ def dubins_fixtures():
     solve_fixture("dubins2_24x16_geo", p, (pts, rng.uniform(0.5, 2.0, 3)))
 
 
+def stencil_step_spreading_fixtures():
+    """seedRadius < 0 on Riemann models: the spread cells plus one step of the reversed stencils."""
+    p = W.riemann2_case(40, aniso=6.0, seed=9, n_seeds=1)
+    solve_fixture("spread_riemann2_step", dict(p, seeds=np.array([[0.41, 0.57], [0.62, 0.33]]), seedRadius=-1.5))
+    p3 = W.riemann3_case(14, n_spheres=1, n_seeds=1, rmin=0.05, rmax=0.08, seed=23)
+    p3.pop("walls", None)
+    solve_fixture("spread_riemann3_step", dict(p3, seeds=np.array([[0.52, 0.47, 0.55]]), seedRadius=-1.0))
+
+
 def tti_spreading_fixtures():
     """seedRadius > 0 on TTI3: the guess is the TTI norm of the metric interpolated at the seed and
     of the metric at the cell (the transform's columns scaled by the grid scales)."""
@@ -369,7 +378,8 @@ def forward_curvature_fixtures():
 
 
 if __name__ == "__main__":
-    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread|dubins`
+    # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread|dubins|
+    # spreadstep`
     # regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
@@ -393,6 +403,8 @@ if __name__ == "__main__":
         tti_spreading_fixtures()
     elif sys.argv[1:] == ["dubins"]:
         dubins_fixtures()
+    elif sys.argv[1:] == ["spreadstep"]:
+        stencil_step_spreading_fixtures()
     else:
         main()
         tti_fixtures()

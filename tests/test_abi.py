@@ -69,7 +69,7 @@ def test_store_errors_raise_not_crash():
 
 
 @pytest.mark.parametrize("key,val", [("exportActiveOffsets", 1.0), ("order", 2.0), ("factoringRadius", 5.0),
-                                     ("speed_times", np.zeros(3)), ("seedRadius", -2.0)])
+                                     ("speed_times", np.zeros(3))])
 def test_unsupported_options_rejected_before_gpu_work(key, val):
     p = {"model": "Riemann2", "arrayOrdering": "RowMajor", "dims": np.array([8., 8.]), "gridScale": 0.125,
          "metric": np.array([1., 0., 1.]), "seeds": np.array([[0.5, 0.5]]), "verbosity": 0.0, key: val}

@@ -10,7 +10,7 @@ import hamiltonfastmarching_b200 as H
 from conftest import load_golden
 
 SPREAD = ["spread_riemann2_dual", "spread_riemann3_walls", "spread_isotropic2", "spread_diagonal3", "spread_tti3",
-          "spread_tti3_scales"]
+          "spread_tti3_scales", "spread_riemann2_step", "spread_riemann3_step"]
 
 
 @pytest.mark.parametrize("name", SPREAD)
@@ -35,4 +35,17 @@ def test_negative_radius_and_lifted_models_refused():
          "seeds": np.array([[0.5, 0.5, 0.0]]), "seedRadius": 2.0, "verbosity": 0.0}
     with pytest.raises(H.PyExp) as e:
         H.run(p)
+    assert e.value.code == 3
+
+
+def test_stencil_step_refusals():
+    """seedRadius < 0 on a Riemann model is refused (HFM_ERR_UNSUPPORTED, before any device work)
+    with walls, and for a seed whose spread cells reach outside the domain."""
+    params, _, _ = load_golden("spread_riemann2_step")
+    n = int(params["dims"][0])
+    with pytest.raises(H.PyExp) as e:
+        H.run(dict(params, walls=np.zeros((n, n)), verbosity=0.0))
+    assert e.value.code == 3
+    with pytest.raises(H.PyExp) as e:
+        H.run(dict(params, seeds=np.array([[0.01, 0.5]]), verbosity=0.0))
     assert e.value.code == 3
