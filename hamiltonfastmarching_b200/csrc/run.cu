@@ -378,9 +378,11 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
         const double radius_in = io.get_scalar("seedRadius", 0.0);
         const bool stencil_step = radius_in < 0;
         const double radius = std::abs(radius_in);
+        const bool shared_axes = p.diagonal || (p.kind == StencilKind::SharedByTheta && !p.angular);
         if (stencil_step) {
-            if (p.kind != StencilKind::RiemannPerCell || p.diagonal)
-                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 (stencil-step spreading) is supported for the Riemann models only");
+            if (p.kind != StencilKind::RiemannPerCell && !shared_axes)
+                throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 (stencil-step spreading) is supported for the Riemann, "
+                                                 "Isotropic and Diagonal models only");
             if (io.has_field("walls") || pm.periodic[0] || pm.periodic[1] || pm.periodic[2])
                 throw Error(HFM_ERR_UNSUPPORTED, "seedRadius < 0 with walls or periodic axes is not supported by the GPU solve path");
         }
@@ -424,10 +426,27 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
                     insert(idx, radius);
                 }
                 if (stencil_step) {  // every index seen so far, in index order, plus its reversed offsets
-                    if (width < 0) width = riemann_max_width(p, pm);
+                    // Isotropic and Diagonal models share one stencil, +-e_i with nonzero base weights,
+                    // whose reversed offsets the reference takes once, from the domain's centre
+                    // (HFM_StencilShare.hxx:104-180): the same sorted list for every cell.
+                    std::vector<std::array<int, 3>> shared;
+                    if (shared_axes) {
+                        std::set<std::array<int, 3>> acc;
+                        for (int a = 0; a < D; ++a)
+                            for (int sgn = -1; sgn <= 1; sgn += 2) {
+                                const int64_t c = pm.dims[a] / 2 + sgn;
+                                if (c < 0 || c >= pm.dims[a]) continue;
+                                std::array<int, 3> e = {0, 0, 0};
+                                e[a] = sgn;
+                                acc.insert(e);
+                            }
+                        shared.assign(acc.begin(), acc.end());
+                    } else if (width < 0) {
+                        width = riemann_max_width(p, pm);
+                    }
                     const std::set<std::vector<int64_t>> base = seen;
                     for (const std::vector<int64_t> &x : base) {
-                        for (const std::array<int, 3> &e : reversed_offsets(p, pm, x.data(), width)) {
+                        for (const std::array<int, 3> &e : shared_axes ? shared : reversed_offsets(p, pm, x.data(), width)) {
                             int64_t idx[3];
                             for (int a = 0; a < D; ++a) idx[a] = x[a] + e[a];
                             insert(idx, std::numeric_limits<double>::infinity());

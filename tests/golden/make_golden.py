@@ -280,6 +280,16 @@ def stencil_step_spreading_fixtures():
     p3 = W.riemann3_case(14, n_spheres=1, n_seeds=1, rmin=0.05, rmax=0.08, seed=23)
     p3.pop("walls", None)
     solve_fixture("spread_riemann3_step", dict(p3, seeds=np.array([[0.52, 0.47, 0.55]]), seedRadius=-1.0))
+    rng = np.random.default_rng(31)
+    n = 30
+    solve_fixture("spread_isotropic2_step", {"model": "Isotropic2", "arrayOrdering": "RowMajor",
+                                             "dims": np.array([n, n], float), "gridScale": 1.0 / n,
+                                             "cost": 1 + rng.random((n, n)), "seeds": np.array([[0.31, 0.52], [0.02, 0.5]]),
+                                             "seedRadius": -2.0, "exportValues": 1.0})
+    solve_fixture("spread_diagonal3_step", {"model": "Diagonal3", "arrayOrdering": "RowMajor",
+                                            "dims": np.array([12, 10, 8], float), "gridScales": np.array([0.1, 0.12, 0.15]),
+                                            "speed": 0.5 + rng.random((12, 10, 8, 3)),
+                                            "seeds": np.array([[0.55, 0.61, 0.33]]), "seedRadius": -1.2, "exportValues": 1.0})
 
 
 def tti_spreading_fixtures():

@@ -10,7 +10,8 @@ import hamiltonfastmarching_b200 as H
 from conftest import load_golden
 
 SPREAD = ["spread_riemann2_dual", "spread_riemann3_walls", "spread_isotropic2", "spread_diagonal3", "spread_tti3",
-          "spread_tti3_scales", "spread_riemann2_step", "spread_riemann3_step"]
+          "spread_tti3_scales", "spread_riemann2_step", "spread_riemann3_step", "spread_isotropic2_step",
+          "spread_diagonal3_step"]
 
 
 @pytest.mark.parametrize("name", SPREAD)
@@ -27,7 +28,7 @@ def test_spread_seeds_match_reference(name):
 
 
 def test_negative_radius_and_lifted_models_refused():
-    params, _, _ = load_golden("spread_isotropic2")
+    params, _, _ = load_golden("spread_tti3")  # seedRadius < 0 on TTI3 (Lag2 reversed offsets)
     with pytest.raises(H.PyExp) as e:
         H.run(dict(params, seedRadius=-2.0, verbosity=0.0))
     assert e.value.code == 3
