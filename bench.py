@@ -43,8 +43,6 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--side", type=int, default=192, help="grid side of the benchmarked instance")
-    ap.add_argument("--cpu-sample-side", type=int, default=128,
-                    help="grid side of the bounded sample the reference CPU code is timed on")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-riemann", type=int, default=384, help="Riemann2 instances of the batched mix")
@@ -56,7 +54,7 @@ def parse_args(argv=None):
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--tti-side", type=int, default=128, help="grid side of the TTI3 differentiation leg")
-    ap.add_argument("--tti-fd-voxels", type=int, default=8, help="voxels checked by central differences")
+    ap.add_argument("--tti-fd-voxels", type=int, default=32, help="voxels checked by central differences")
     ap.add_argument("--no-diff", action="store_true", help="skip the TTI3 differentiation leg")
     ap.add_argument("--geo-side", type=int, default=1024, help="grid side of the geodesic leg (Riemann2)")
     ap.add_argument("--geo-tips", type=int, default=4096, help="tips of the geodesic leg")
@@ -145,9 +143,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def bench_config(n):
+    """The workload description, identical in both arms of the benchmark."""
+    return {"workload": WORKLOAD, "grid": [n, n, n], "generator": "workloads.riemann3_case(n, seed=1 + rank)",
+            "instances_per_step": "one per rank", "precision": "f64", "l2": "inputs larger than L2 (340 MB metric)"}
+
+
 def reference_cpu_sample(side, seed=1):
-    """The reference's FileHFM_Riemann3 (built from its sources) on a bounded sample of the workload:
-    updates/s = nAccepted / (FMCPUTime + StencilCPUTime), one core."""
+    """The reference's FileHFM_Riemann3 (built from its sources) on one full solve of the benchmarked
+    instance: updates/s = nAccepted / (FMCPUTime + StencilCPUTime), one core."""
     from oracle.refrun import have_reference, run_reference
     from hamiltonfastmarching_b200 import workloads as W
     if not have_reference("Riemann3"):
@@ -161,9 +165,9 @@ def reference_cpu_sample(side, seed=1):
         return None
     cpu_s = out["FMCPUTime"] + out["StencilCPUTime"]
     return {"value": out["nAccepted"] / cpu_s, "unit": "grid-updates/s", "cores": 1, "kind": "reference",
-            "sample": f"FileHFM_Riemann3 on the same generator at {side}^3 ({int(out['nAccepted'])} reached cells); "
-                      f"FMCPUTime {out['FMCPUTime']:.2f} s + StencilCPUTime {out['StencilCPUTime']:.2f} s "
-                      f"(wall {wall:.1f} s incl. file IO)"}
+            "sample": f"FileHFM_Riemann3, one full solve of the benchmarked {side}^3 instance "
+                      f"({int(out['nAccepted'])} reached cells): FMCPUTime {out['FMCPUTime']:.2f} s + "
+                      f"StencilCPUTime {out['StencilCPUTime']:.2f} s (wall {wall:.1f} s incl. file IO)"}
 
 
 # ------------------------------------------------------------------------------- batched leg
@@ -421,13 +425,38 @@ def differentiation_leg(args):
             fd = (loss_of(torch.from_numpy(vpp.reshape(vp0.shape))) -
                   loss_of(torch.from_numpy(vpm.reshape(vp0.shape)))).item() / (2 * d)
         errs.append(abs(g[cell] - fd) / max(abs(fd), 1e-12))
-    return {"workload": f"TTI3 {n}^3, h = 10 m, Thomsen vp in [1.5,4.5] km/s, eps/delta in [0,0.2], dip <= 30 deg; "
-                        f"64 top-face receivers, T_obs from vp with a +5% Gaussian blob",
-            "forward_solve_s": fwd_s, "gpu_solve_s": out["GPUSolveTime"], "n_accepted": out["nAccepted"],
-            "grid_updates_per_s": out["nAccepted"] / fwd_s,
-            "loss": float(loss.item()), "autograd_forward_s": t1 - t0, "autograd_backward_s": t2 - t1,
-            "fd_voxels": len(errs), "fd_max_rel_err": max(errs) if errs else None,
-            "fd_step": "1e-4 vp, central", "dtype": "f64"}
+    res = {"workload": f"TTI3 {n}^3, h = 10 m, Thomsen vp in [1.5,4.5] km/s, eps/delta in [0,0.2], dip <= 30 deg; "
+                       f"64 top-face receivers, T_obs from vp with a +5% Gaussian blob",
+           "forward_solve_s": fwd_s, "gpu_solve_s": out["GPUSolveTime"], "n_accepted": out["nAccepted"],
+           "grid_updates_per_s": out["nAccepted"] / fwd_s,
+           "loss": float(loss.item()), "autograd_forward_s": t1 - t0, "autograd_backward_s": t2 - t1,
+           "fd_voxels": len(errs), "fd_max_rel_err": max(errs) if errs else None,
+           "fd_step": "1e-4 vp, central", "dtype": "f64"}
+    # the reference's backward differentiation (FileHFM_TTI3, inspectSensitivity at the receivers
+    # with the loss gradient 2 (T - T_obs) as weights) against the GPU's costSensitivity_0
+    from oracle.refrun import have_reference, run_reference
+    if not args.no_cpu_baseline and have_reference("TTI3"):
+        T = out["values"].reshape(-1)[receivers]
+        h_ = p["gridScale"]
+        pts = np.column_stack([(rx + 0.5) * h_, np.full(64, 0.5 * h_)])
+        wts = 2.0 * (T - t_obs.numpy())
+        q = dict(p, inspectSensitivity=pts, inspectSensitivityWeights=wts, inspectSensitivityLengths=np.array([64.0]),
+                 verbosity=0.0)
+        t0 = time.perf_counter()
+        gout = H.run(q)
+        gpu_sens_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref = run_reference(q)
+        ref_s = time.perf_counter() - t0
+        if ref.get("retcode") == 0:
+            a, b = ref["costSensitivity_0"], gout["costSensitivity_0"]
+            res["reference_backward"] = {
+                "costSensitivity_max_rel_diff": float(np.max(np.abs(a - b)) / np.max(np.abs(a))),
+                "values_max_rel_diff": float(np.max(np.abs(ref["values"] - gout["values"])) / np.max(np.abs(ref["values"]))),
+                "reference_wall_s": ref_s, "reference_fm_s": float(ref["FMCPUTime"]),
+                "reference_stencil_s": float(ref["StencilCPUTime"]), "gpu_run_with_sensitivity_s": gpu_sens_s,
+                "cores": 1, "kind": "reference"}
+    return res
 
 
 def geodesic_leg(args):
@@ -489,6 +518,37 @@ def geodesic_leg(args):
 
 
 # ------------------------------------------------------------------------------------- our arm
+
+def summarize(line):
+    """Headline figures of every leg in a few hundred bytes."""
+    def r(x, d=3):
+        return None if x is None else float(f"{x:.{d}g}")
+    out = {"fp64_updates_per_s": r(line["value"]), "fp32_updates_per_s": r(line["fp32"]["value"]),
+           "fp32_err": r(line["fp32"]["max_rel_err_vs_fp64"], 2), "roofline_frac": r(line["roofline"]["frac"], 3),
+           "e2e_updates_per_s": r((line.get("e2e") or {}).get("value"))}
+    b = line.get("batch")
+    if b:
+        out["batch"] = {"solves_per_s": r(b["batched"]["solves_per_s"]),
+                        "plain_solves_per_s": r(b["plain_one_at_a_time"]["solves_per_s"]),
+                        "speedup": r(b["speedup_solves_per_s"]), "speedup_tuned": r(b["speedup_autotuned_solves_per_s"]),
+                        "fp32_err": r(b["fp32_max_rel_err_vs_fp64"], 2)}
+    sv = line.get("serving")
+    if sv:
+        out["serving"] = {"fp32_err": r(sv["fp32_max_rel_err_vs_fp64"], 2), "rates": [
+            {"rate": x["rate_req_per_s"], "solves_per_s": r(x["served"]["solves_per_s"]),
+             "plain": r(x["plain_one_at_a_time"]["solves_per_s"]), "p50_ms": r(x["served"]["p50_ms"]),
+             "p99_ms": r(x["served"]["p99_ms"]), "plain_p50_ms": r(x["plain_one_at_a_time"]["p50_ms"]),
+             "plain_p99_ms": r(x["plain_one_at_a_time"]["p99_ms"])} for x in sv["rates"]]}
+    d = line.get("differentiation")
+    if d:
+        out["differentiation"] = {"forward_s": r(d["forward_solve_s"]), "backward_s": r(d["autograd_backward_s"]),
+                                  "fd_voxels": d["fd_voxels"], "fd_err": r(d["fd_max_rel_err"], 2),
+                                  "vs_reference_sens": r((d.get("reference_backward") or {}).get("costSensitivity_max_rel_diff"), 2)}
+    g = line.get("geodesics")
+    if g:
+        out["geodesics"] = {"tips_per_s": r(g["tips_per_s"]), "speedup_1core": r(g.get("speedup_tips_per_s_vs_1_core"))}
+    return out
+
 
 def run_ours(args):
     import torch
@@ -624,7 +684,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = reference_cpu_sample(args.cpu_sample_side)
+        cpu = reference_cpu_sample(n)
     batch = None
     if not args.no_batch:
         batch = batched_leg(args, rank, world)
@@ -643,11 +703,10 @@ def run_ours(args):
             "metric": "grid-updates/s", "value": r64["value"], "unit": "grid-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [n, n, n], "instances_per_gpu": 1,
-                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (340 MB metric)",
-                       "n_accepted": r64["n_accepted"]},
+            "config": bench_config(n),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": r64["clocks"],
             "gpu_launches": r64["launches"],
+            "n_accepted": r64["n_accepted"],
             "phases_ms": {"stencil_and_graph": r64["stencil_ms"], "solve": r64["solve_ms"]},
             "solver": {"rounds": r64["rounds"], "tile_activations": r64["tile_activations"],
                        "local_solves": r64["local_solves"]},
@@ -659,6 +718,8 @@ def run_ours(args):
             "differentiation": diff,
             "geodesics": geo,
         }
+        # compact digest last, so that a reader keeping only the end of the line still has it
+        line["summary"] = summarize(line)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -668,46 +729,65 @@ def run_ours(args):
 # ------------------------------------------------------------------------------ reference arm
 
 def run_reference_arm(args):
+    """The reference's own CPU implementation on the benchmarked workload: one step is one full
+    FileHFM_Riemann3 solve (the reference's executable, compiled from its sources, single-threaded)
+    of the 192^3 instance, from its input file to its output file. Steps run concurrently, one
+    process per host core (a pool over the steps); value = steps x nAccepted / wall time of the
+    timed steps. Warm-up steps run the same way before the timed region."""
+    import concurrent.futures as cf
     rank, world, _ = rank_env()
     if rank != 0:
         return
-    from oracle.refrun import have_reference, ref_executable, write_input, read_output
+    from oracle.refrun import have_reference, ref_executable, read_output, write_input
     from hamiltonfastmarching_b200 import workloads as W
-    side = args.cpu_sample_side
+    n = args.side
     if not have_reference("Riemann3"):
         print(json.dumps({"impl": "reference", "unavailable": "reference FileHFM_Riemann3 not built (make -C oracle ref)"}))
         return
     cores = os.cpu_count() or 1
-    p = W.riemann3_case(side, seed=1)
+    p = W.riemann3_case(n, seed=1)
     p["exportValues"] = 0.0
     tmp = tempfile.mkdtemp(prefix="hfmrefbench_")
     write_input(p, os.path.join(tmp, "input"))
+    del p
     exe = ref_executable("Riemann3")
+    counter = iter(range(1 << 30))
 
-    def step():
-        procs = [subprocess.Popen([exe, os.path.join(tmp, "input"), os.path.join(tmp, f"out{i}")],
-                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for i in range(cores)]
-        for pr in procs:
-            pr.wait()
-        return read_output(os.path.join(tmp, "out0"))
+    def one_solve(_):
+        out = os.path.join(tmp, f"out{next(counter)}")
+        subprocess.run([exe, os.path.join(tmp, "input"), out], stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL, check=True)
+        r = read_output(out)
+        for ext in ("_Format.txt", "_Data.dat"):
+            os.unlink(out + ext)
+        return r
 
-    for _ in range(args.warmup):
-        step()
+    def run_steps(k):
+        with cf.ThreadPoolExecutor(max_workers=max(1, min(cores, k))) as ex:
+            return list(ex.map(one_solve, range(k)))
+
+    if args.warmup > 0:
+        run_steps(args.warmup)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        out = step()
+    outs = run_steps(args.steps)
     el = time.perf_counter() - t0
-    nacc = out["nAccepted"]
-    value = cores * nacc * args.steps / el
+    nacc = outs[-1]["nAccepted"]
+    value = nacc * args.steps / el
+    waves = -(-args.steps // cores)
+    cpu_s = statistics.mean(o["FMCPUTime"] + o["StencilCPUTime"] for o in outs)
     line = {"impl": "reference", "metric": "grid-updates/s", "value": value, "unit": "grid-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [args.side] * 3, "sample_grid": [side] * 3},
-            "cpu_baseline": {"value": value, "unit": "grid-updates/s", "cores": cores, "kind": "reference",
-                             "sample": f"{cores} concurrent FileHFM_Riemann3 processes (reference code, one "
-                                       f"thread each) per step on the same generator at {side}^3"},
+            "config": bench_config(n),
+            "cpu_baseline": {"value": value, "unit": "grid-updates/s", "cores": min(cores, args.steps), "kind": "reference",
+                             "sample": f"{args.steps} full solves of the {n}^3 instance by FileHFM_Riemann3 (reference "
+                                       f"code, one thread each), {min(cores, args.steps)} at a time on {cores} host "
+                                       f"cores ({waves} wave(s)); {int(nacc)} reached cells per solve; mean "
+                                       f"FMCPUTime + StencilCPUTime {cpu_s:.1f} s per solve"},
             "e2e": {"value": value, "unit": "grid-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    import shutil
+    shutil.rmtree(tmp, ignore_errors=True)
 
 
 def main(argv=None):

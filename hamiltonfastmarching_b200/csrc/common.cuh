@@ -21,11 +21,6 @@
 
 namespace hfm {
 
-// Phase tracing for diagnosis: with HFM_DEBUG set in the environment, each traced step
-// synchronises the device and prints its name and the CUDA status to stderr.
-void trace_step(const char *what);
-#define HFM_TRACE(what) ::hfm::trace_step(what)
-
 // Device-side error bits, written to a status word the host reads after each phase.
 enum : unsigned {
     kErrBarrierTimeout = 1u,   // a grid barrier wait exceeded its iteration limit

@@ -22,7 +22,6 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
-#include <execinfo.h>
 
 #include <cstdio>
 #include <cstdlib>
@@ -34,27 +33,6 @@
 #include "solver.hpp"
 
 namespace hfm {
-
-static void trace_at_exit() {
-    void *frames[64];
-    const int n = backtrace(frames, 64);
-    std::fprintf(stderr, "[hfm] process exit requested; native backtrace:\n");
-    backtrace_symbols_fd(frames, n, 2);
-}
-
-void trace_step(const char *what) {
-    static const bool on = std::getenv("HFM_DEBUG") != nullptr;
-    if (!on) return;
-    static const bool registered = (std::atexit(trace_at_exit), true);
-    (void)registered;
-    const cudaError_t e = cudaDeviceSynchronize();
-    static auto last = std::chrono::steady_clock::now();
-    const auto now = std::chrono::steady_clock::now();
-    const double ms = std::chrono::duration<double, std::milli>(now - last).count();
-    last = now;
-    std::fprintf(stderr, "[hfm] %s: %s (+%.3f ms)\n", what, cudaGetErrorString(e), ms);
-    std::fflush(stderr);
-}
 
 GridGeom make_geom(int ndim, const int *dims, const int *periodic, const int *shift) {
     GridGeom g{};
@@ -1998,7 +1976,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     DeviceBuffer<int> tile_inst;
     tile_inst.upload(htile_inst, s);
     P.tile_inst = tile_inst.get();
-    HFM_TRACE("batch layout");
     DeviceBuffer<unsigned> status(1);
     status.zero(s);
     P.status = status.get();
@@ -2045,7 +2022,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             }
             metric_ptr = metric.get();
         }
-        HFM_TRACE("metric upload");
         if (want_stencils && KIND != kKindTTI) {
             plain_off.alloc(N * ND * 3);
             plain_w.alloc(N * ND);
@@ -2071,7 +2047,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                    plain_w.get());
         }
         HFM_CUDA(cudaGetLastError());
-        HFM_TRACE("stencil kernel");
         launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, P, maxw.get());
         maxw.download(hmaxw.data(), ninst, s);
         if (ninst > 1 && p0.ordered && !p0.diagonal) {
@@ -2124,7 +2099,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                 }
             hmaxw[i] = (unsigned)mw;
         }
-        HFM_TRACE("class tables and multipliers (host)");
         cls_w.upload(hw, s);
         cls_off.upload(ho, s);
         cls_en.upload(he, s);
@@ -2197,11 +2171,9 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         launch(wall_cap_kernel<Real>, nblocks(N, 256), 256, 0, s, P, wdist.get(), maxw.get(), wd8.get());
         HFM_CUDA(cudaGetLastError());
     }
-    HFM_TRACE("walls");
     launch(visibility_kernel<Real, NFWD, NSYM, KIND>, nblocks(ntc, 128), 128, 0, s, P, wd8.get(), cls_en.get());
     HFM_CUDA(cudaGetLastError());
     wdist.release();
-    HFM_TRACE("visibility");
 
     // ---- seeds (global cell indices) and their tiles
     std::vector<long long> hsi;
@@ -2237,7 +2209,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         sval.upload(hsv, s);
         launch(seeds_kernel<Real, KIND>, nblocks(ns, 128), 128, 0, s, P, sidx.get(), sval.get(), ns);
     }
-    HFM_TRACE("seeds");
 
     // ---- tile dependency graph (reverse CSR over the global tile space)
     DeviceBuffer<unsigned> dcnt(nt);
@@ -2297,7 +2268,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                    edmsk.get(), rptr.get(), cursor.get(), rtile.get(), rmask.get(), rdmask.get());
         HFM_CUDA(cudaGetLastError());
     }
-    HFM_TRACE("deps");
     P.dep_ptr = rptr.get();
     P.dep_tile = rtile.get();
     P.dep_mask = rmask.get();
@@ -2357,7 +2327,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         launch(init_lists_kernel<Real>, nblocks((long long)st.size() * 32, 128), 128, 0, s, P, stile.get(),
                smask.get(), (int)st.size());
         HFM_CUDA(cudaGetLastError());
-        HFM_TRACE("init lists");
         int dev = 0, nsm = 0, per_sm = 0;
         HFM_CUDA(cudaGetDevice(&dev));
         HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -2374,7 +2343,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, KIND>, dim3(grid),
                                              dim3(kWarpsPerCta * 32), args, 0, s));
     }
-    HFM_TRACE("fim kernel");
     const float t_solve = tm.stop(s);
     check_status(status, "solver");
     unsigned long long hs[4] = {0, 0, 0, 0};
@@ -2448,9 +2416,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         res.t_solve_ms = t_solve;
     }
     HFM_CUDA(cudaStreamSynchronize(s));
-    HFM_TRACE("outputs");
     run_geodesics<Real, NFWD, NSYM, KIND>(P, hinst, probs, results, any_walls ? wd8.get() : nullptr, s);
-    HFM_TRACE("geodesics");
     if (ninst == 1 && (!p0.adjoint_index.empty() || p0.fwd_nvar > 0)) {
         tm.start(s);
         FlowGraph G;

@@ -86,8 +86,7 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
 void reject_unsupported(Store &io) {
     static const char *keys[] = {"factoringValues", "speed_times", "cost_times",
                                  "metric_times", "dualMetric_times",
-                                 "euclideanScale", "seedFlags", "getStencils",
-                                 "factoringPointChoice"};
+                                 "euclideanScale", "seedFlags", "factoringPointChoice"};
     for (const char *k : keys)
         if (io.has_field(k))
             throw Error(HFM_ERR_UNSUPPORTED, std::string("option '") + k + "' is not supported by the GPU solve path");
@@ -983,9 +982,127 @@ struct Prepared {
     EulerProblem p;
     bool geo_keys[2] = {false, false};  // tips, tips_Unoriented present
     bool export_values = false, export_active = false, skip = false;
+    bool get_stencils = false;          // getStencils given: the cells whose stencils are printed
+    bool export_stencils = false;       // exportStencils: all Selling stencils as arrays
+    std::vector<int64_t> stencil_cells;
     std::vector<int64_t> dims;
     double *values_dst = nullptr;
 };
+
+size_t n_cells(const std::vector<int64_t> &dims);
+
+// getStencils (HFMInterface.hxx:360-375): the points are placed like seeds; a point out of range
+// is skipped with the reference's warning. Riemann stencils are exported from the GPU's Selling
+// arrays; the other models' stencils are their host tables.
+void read_get_stencils(Store &io, Prepared &q) {
+    if (!io.has_field("getStencils")) return;
+    const Param &pm = q.pm;
+    if (q.p.kind == StencilKind::TTI)
+        throw Error(HFM_ERR_UNSUPPORTED, "getStencils on TTI3 is not supported by the GPU solve path");
+    int64_t n = 0;
+    const std::vector<double> pts = io.get_vector("getStencils", pm.ndim, &n);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t lin;
+        if (!pm.index_of(&pts[i * pm.ndim], &lin)) {
+            std::ostringstream o;
+            o << "GetStencil error : point {";
+            for (int a = 0; a < pm.ndim; ++a) o << (a ? "," : "") << pts[i * pm.ndim + a];
+            o << "}is out of range.\n";
+            io.warn(o.str());
+            continue;
+        }
+        q.stencil_cells.push_back(lin);
+    }
+    q.get_stencils = true;
+    if (q.p.kind == StencilKind::RiemannPerCell && !q.p.diagonal) q.p.want_stencils = true;
+}
+
+// exportStencils (an extension, Riemann models): every cell's Selling stencil as arrays,
+// stencilOffsets (dims + (K, ndim)) and stencilWeights (dims + (K,)), K = 3 (2D) or 6 (3D), in the
+// order and with the full FP64 weights the solver uses.
+bool read_export_stencils(Store &io, Prepared &q) {
+    if (io.get_scalar("exportStencils", 0.0, 3) == 0) return false;
+    if (q.p.kind != StencilKind::RiemannPerCell || q.p.diagonal)
+        throw Error(HFM_ERR_UNSUPPORTED, "exportStencils applies to the Riemann models");
+    q.p.want_stencils = true;
+    return true;
+}
+
+// The `stencils` string in the reference's print format: "{" then, per point, "{" index ","
+// stencil "}," then "}"; a stencil prints as {"forward" -> {{diffs}},"symmetric" -> {{diffs}},}
+// (EulerianStencil.hxx:76-87 with ExportArrayRecursiveArrow, ExportArrow.h:101-102) and a
+// difference as {baseWeight,{offset}} with the stream's default 6 significant digits. The base
+// weight excludes the speed multiplier (Isotropic, Diagonal and curvature models print 1/h^2 or
+// their table weights whatever the speed or cost).
+void export_stencils(Store &io, const Prepared &q, const EulerResult &r) {
+    if (!q.get_stencils) return;
+    const EulerProblem &p = q.p;
+    const Param &pm = q.pm;
+    const int D = pm.ndim;
+    std::ostringstream o;
+    auto diff = [&](double w, const int8_t *off) {
+        o << "{" << w << ",{";
+        for (int a = 0; a < D; ++a) o << (a ? "," : "") << (int)off[a];
+        o << "}}";
+    };
+    o << "{";
+    for (int64_t x : q.stencil_cells) {
+        int64_t idx[3], rr = x;
+        for (int a = D - 1; a >= 0; --a) { idx[a] = rr % pm.dims[a]; rr /= pm.dims[a]; }
+        o << "{{";
+        for (int a = 0; a < D; ++a) o << (a ? "," : "") << idx[a];
+        o << "},{\"forward\" -> {{";
+        if (p.kind == StencilKind::SharedByTheta) {
+            const int ND = p.nfwd + p.nsym;
+            const int64_t cls = p.nclass > 1 ? idx[2] : 0;
+            for (int k = 0; k < p.nfwd; ++k) {
+                if (k) o << ",";
+                diff(p.cls_w[cls * ND + k], &p.cls_off[(cls * ND + k) * 3]);
+            }
+            o << "}},\"symmetric\" -> {{";
+            for (int k = p.nfwd; k < ND; ++k) {
+                if (k > p.nfwd) o << ",";
+                diff(p.cls_w[cls * ND + k], &p.cls_off[(cls * ND + k) * 3]);
+            }
+        } else if (p.diagonal) {  // one difference per axis, base weight 1 / h_i^2
+            o << "}},\"symmetric\" -> {{";
+            for (int k = 0; k < D; ++k) {
+                int8_t e[3] = {0, 0, 0};
+                e[k] = 1;
+                if (k) o << ",";
+                diff(1. / (p.h[k] * p.h[k]), e);
+            }
+        } else {
+            const int NK = D == 2 ? 3 : 6;
+            if (r.stencil_off.size() < (size_t)(x + 1) * NK * 3)
+                throw Error(HFM_ERR_VALUE, "stencils of the requested points were not exported");
+            o << "}},\"symmetric\" -> {{";
+            for (int k = 0; k < NK; ++k) {
+                int8_t e[3];
+                for (int a = 0; a < D; ++a) e[a] = r.stencil_off[((size_t)x * NK + k) * 3 + a];
+                if (k) o << ",";
+                diff(r.stencil_w[(size_t)x * NK + k], e);
+            }
+        }
+        o << "}},}},";
+    }
+    o << "}";
+    io.set_string("stencils", o.str());
+}
+
+void export_stencil_arrays(Store &io, const Prepared &q, const EulerResult &r) {
+    if (!q.export_stencils) return;
+    const int D = q.pm.ndim, NK = D == 2 ? 3 : 6;
+    const size_t n = n_cells(q.dims);
+    std::vector<double> off(n * NK * D);
+    for (size_t x = 0; x < n; ++x)
+        for (int k = 0; k < NK; ++k)
+            for (int a = 0; a < D; ++a) off[(x * NK + k) * D + a] = (double)r.stencil_off[(x * NK + k) * 3 + a];
+    std::vector<int64_t> od(q.dims);
+    od.push_back(NK);
+    io.set_field("stencilOffsets", od, D, off.data());
+    io.set_field("stencilWeights", od, 1, r.stencil_w.data());
+}
 
 void prepare_model(Store &io, const std::string &model, Prepared &q) {
     Param &pm = q.pm;
@@ -1053,6 +1170,8 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
         q.skip = true;
         return;
     }
+    read_get_stencils(io, q);
+    q.export_stencils = read_export_stencils(io, q);
     if (inspect) read_inspect(io, pm, p);
     read_forward_variation(io, pm, p);
     // the arrival times are downloaded straight into the output field when no reordering is needed
@@ -1142,6 +1261,8 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
     const std::vector<int64_t> &dims = q.dims;
     // Outputs (Run_SetupSolver/Run_RunSolver/Run_ExportData, CommonStoppingCriteria::Finally)
     io.set_scalar("MaxStencilWidth", r.max_stencil_width);
+    export_stencils(io, q, r);
+    export_stencil_arrays(io, q, r);
     io.set_scalar("StencilCPUTime", r.t_stencil_ms * 1e-3);
     io.set_scalar("FMCPUTime", r.t_solve_ms * 1e-3);
     io.set_scalar("GeodesicCPUTime", r.t_geodesic_ms * 1e-3);
@@ -1406,7 +1527,6 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
             qs[i] = std::move(q);
         });
     }
-    HFM_TRACE("batch: stores read");
     // Solving: instances of one stencil family and precision share one launch sequence; first
     // variation requests (inspectSensitivity, costVariation, seedValueVariation) run on their own.
     std::vector<char> done(n, 0);
@@ -1432,7 +1552,6 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
         for (int j : grp) probs.push_back(&qs[j]->p);
         std::vector<hfm::EulerResult> res;
         hfm_io *lead = ios[grp[0]];
-        HFM_TRACE("batch: group formed");
         int code = guarded(lead, [&] { hfm::solve_eulerian_batch(probs, res); });
         if (code != HFM_OK && code != HFM_ERR_CUDA && grp.size() > 1) {
             // an invalid instance (e.g. a non-SPD metric) fails its whole group: solve the members
@@ -1460,7 +1579,6 @@ int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *co
             rc[j] = guarded(ios[j], [&] { hfm::finish_model(ios[j]->store, *qs[j], res[k]); });
         }
     }
-    HFM_TRACE("batch: solved and exported");
     int first = HFM_OK;
     for (int i = 0; i < n; ++i) {
         if (rc[i] == HFM_OK) rc[i] = guarded(ios[i], [&] { ios[i]->store.usage_report(); });

@@ -13,14 +13,19 @@
 // rejected with HFM_ERR_VALUE); scratch size 9,453,824 bytes per device.
 //
 // The first call on a device looks up the device address of the buffer (cudaGetSymbolAddress)
-// with that device current; make that first call before any stream capture. All calls share the
+// with that device current. Every call reads the convergence words back to the host and waits for
+// its stream, so the entry point cannot be called inside a stream capture. All calls share the
 // one buffer and it keeps the last call's contents: the arrays a call reads are fully rewritten by
-// that call and the convergence word is cleared before use, but calls that overlap on the GPU
+// that call and the control words are cleared before use, but calls that overlap on the GPU
 // (other threads, other streams) race on the buffer and must be serialised by the caller.
 //
 // Method: the same Selling stencils (selling.cuh) and the same Hopf-Lax update as the main path,
 // iterated as chaotic Gauss-Seidel sweeps over all cells until no value changes; it reaches the
-// same fixed point as the tiled solver. It calls no cudaMalloc, cudaFree or allocating routine.
+// same fixed point as the tiled solver (within 1e-10 relative). Repeated seeds keep their first
+// value, as the main path does. Rounding can make a recomputed value land an ulp above the current
+// one and such increases can cycle: once the sweeps have taken 2 increases per cell (plus 128),
+// only decreases are taken, which terminates (the tiled solver's guard, per call instead of per
+// tile). It calls no cudaMalloc, cudaFree or allocating routine.
 #include <cstring>
 #include <mutex>
 
@@ -49,6 +54,7 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 struct View {
     unsigned *changed;     // control word 0
     unsigned *status;      // control word 1
+    unsigned *increases;   // control word 2: value increases taken since the start of the call
     const long long *seed_idx;
     const double *seed_val;
     unsigned *code;        // [3][N]
@@ -59,6 +65,7 @@ __host__ __device__ inline View view_of(unsigned char *base) {
     View v;
     v.changed = reinterpret_cast<unsigned *>(base);
     v.status = reinterpret_cast<unsigned *>(base) + 1;
+    v.increases = reinterpret_cast<unsigned *>(base) + 2;
     v.seed_idx = reinterpret_cast<const long long *>(base + kSeedIdxOff);
     v.seed_val = reinterpret_cast<const double *>(base + kSeedValOff);
     v.code = reinterpret_cast<unsigned *>(base + kCodeOff);
@@ -133,10 +140,11 @@ __device__ __forceinline__ double local_solve(const double (&v)[3], const double
     return r;
 }
 
-__global__ void sweep_kernel(int nx, int ny, int parity, unsigned char *base, double *values) {
+__global__ void sweep_kernel(int nx, int ny, int parity, int strict, unsigned char *base, double *values) {
     const long long N = (long long)nx * ny;
     const View V = view_of(base);
     bool changed = false;
+    unsigned ups = 0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
         const long long x = (parity & 1) ? N - 1 - t : t;  // alternate the sweep direction
         const unsigned c0 = V.code[x];
@@ -157,12 +165,17 @@ __global__ void sweep_kernel(int nx, int ny, int parity, unsigned char *base, do
             w[k] = V.weight[k * N + x];
         }
         const double nv = local_solve(v, w);
-        if (nv != __ldcg(values + x)) {
+        const double cur = __ldcg(values + x);
+        if (strict ? nv < cur : nv != cur) {
+            ups += nv > cur ? 1u : 0u;
             __stcg(values + x, nv);
             changed = true;
         }
     }
     if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(V.changed, 1u);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) ups += __shfl_xor_sync(0xffffffffu, ups, o);
+    if (ups && (threadIdx.x & 31) == 0) atomicAdd(V.increases, ups);
 }
 
 // Device address of the scratch buffer, looked up once per device with that device current.
@@ -199,37 +212,56 @@ extern "C" int hfm_solve_riemann2_static_scratch(int64_t nx, int64_t ny, double 
     };
     if (!metric || !values || !seed_index || !seed_value) return fail(HFM_ERR_ARG, "null argument");
     if (nx <= 0 || ny <= 0 || !(grid_scale > 0)) return fail(HFM_ERR_VALUE, "invalid grid");
-    if (nx * ny > kMaxCells)
-        return fail(HFM_ERR_VALUE, "grid of " + std::to_string(nx * ny) + " cells exceeds the " +
+    // each side first, so that the product below cannot overflow
+    if (nx > kMaxCells || ny > kMaxCells || nx * ny > kMaxCells)
+        return fail(HFM_ERR_VALUE, "grid of " + std::to_string(nx) + " x " + std::to_string(ny) + " cells exceeds the " +
                                        std::to_string(kMaxCells) + "-cell limit of the static-scratch entry point");
     if (nseeds < 1 || nseeds > kMaxSeeds)
         return fail(HFM_ERR_VALUE, "between 1 and " + std::to_string(kMaxSeeds) + " seeds are required");
     const long long N = nx * ny;
     for (int64_t s = 0; s < nseeds; ++s)
         if (seed_index[s] < 0 || seed_index[s] >= N) return fail(HFM_ERR_VALUE, "seed index out of range");
+    // Repeated seed indices keep their first value (the main path's std::map semantics): a stable
+    // insertion sort by index into fixed arrays, then the first entry of each run.
+    long long sidx[kMaxSeeds];
+    double sval[kMaxSeeds];
+    int ns = 0;
+    for (int64_t s = 0; s < nseeds; ++s) {
+        const long long x = seed_index[s];
+        int pos = ns;
+        while (pos > 0 && sidx[pos - 1] > x) --pos;
+        if (pos > 0 && sidx[pos - 1] == x) continue;  // an earlier seed holds this cell
+        for (int k = ns; k > pos; --k) { sidx[k] = sidx[k - 1]; sval[k] = sval[k - 1]; }
+        sidx[pos] = x;
+        sval[pos] = seed_value[s];
+        ++ns;
+    }
     try {
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         unsigned char *base = scratch_address();
         HFM_CUDA(cudaMemsetAsync(base, 0, kCtrlBytes, st));
-        HFM_CUDA(cudaMemcpyAsync(base + kSeedIdxOff, seed_index, nseeds * sizeof(long long), cudaMemcpyHostToDevice, st));
-        HFM_CUDA(cudaMemcpyAsync(base + kSeedValOff, seed_value, nseeds * sizeof(double), cudaMemcpyHostToDevice, st));
+        // pageable sources: each copy returns once the bytes are staged, so the arrays may go
+        HFM_CUDA(cudaMemcpyAsync(base + kSeedIdxOff, sidx, ns * sizeof(long long), cudaMemcpyHostToDevice, st));
+        HFM_CUDA(cudaMemcpyAsync(base + kSeedValOff, sval, ns * sizeof(double), cudaMemcpyHostToDevice, st));
         const unsigned blocks = (unsigned)((N + 255) / 256);
         hfm::launch(stencil_kernel, blocks, 256, 0, st, (int)nx, (int)ny, grid_scale, metric, dual, base, values);
-        hfm::launch(seed_kernel, (unsigned)((nseeds + 127) / 128), 128, 0, st, (int)nseeds, N, base, values);
+        hfm::launch(seed_kernel, (unsigned)((ns + 127) / 128), 128, 0, st, ns, N, base, values);
         HFM_CUDA(cudaGetLastError());
-        unsigned ctrl[2] = {0, 0};
+        unsigned ctrl[3] = {0, 0, 0};
         const long long max_sweeps = 64 * (nx + ny) + 4096;
-        bool converged = false;
+        const unsigned long long up_budget = 2ull * (unsigned long long)N + 128ull;
+        bool converged = false, strict = false;
         for (long long sweep = 0; sweep < max_sweeps && !converged; sweep += kSweepsPerCheck) {
             HFM_CUDA(cudaMemsetAsync(base, 0, sizeof(unsigned), st));
             for (int k = 0; k < kSweepsPerCheck; ++k)
                 hfm::launch(sweep_kernel, blocks < 1184u ? blocks : 1184u, 256, 0, st, (int)nx, (int)ny,
-                            (int)(sweep + k), base, values);
+                            (int)(sweep + k), strict ? 1 : 0, base, values);
             HFM_CUDA(cudaMemcpyAsync(ctrl, base, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
             HFM_CUDA(cudaStreamSynchronize(st));
             if (ctrl[1] & kErrSellingBit)
                 return fail(HFM_ERR_VALUE, "ObtuseSuperbase error : input must be positive definite");
             converged = ctrl[0] == 0;
+            strict = strict || ctrl[2] >= up_budget;
         }
         if (!converged) return fail(HFM_ERR_NOT_CONVERGED, "sweep cap reached before convergence");
         return HFM_OK;

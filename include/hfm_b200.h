@@ -183,9 +183,11 @@ int hfm_solve_riemann_device(const hfm_riemann_device_args *args, hfm_solve_stat
  * the caller passes the metric (`nx*ny*3` doubles, RowMajor, packed xx,xy,yy) and receives the
  * arrival times (`nx*ny` doubles) in its own device memory. Limits: nx*ny <= 262144 cells and
  * 1..1024 seeds (RowMajor linear indices, host arrays); larger inputs fail with HFM_ERR_VALUE.
- * The first call on a device looks up the buffer's device address (make it before any stream
- * capture). Calls share the buffer: concurrent or overlapping calls on the GPU race and must be
- * serialised by the caller. Results equal hfm_solve_riemann_device with precision 64. */
+ * Repeated seed indices keep their first value. The first call on a device looks up the buffer's
+ * device address; every call reads convergence words back and waits for its stream, so the entry
+ * point cannot be called inside a stream capture. Calls share the buffer: concurrent or
+ * overlapping calls on the GPU race and must be serialised by the caller. Results are within
+ * 1e-10 (relative max-norm) of hfm_solve_riemann_device with precision 64. */
 int hfm_solve_riemann2_static_scratch(int64_t nx, int64_t ny, double grid_scale, const double *metric,
                                       int dual, int64_t nseeds, const int64_t *seed_index,
                                       const double *seed_value, double *values, void *stream, char *err,

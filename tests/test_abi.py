@@ -145,3 +145,25 @@ def test_array_view_is_read_in_place():
     assert np.array_equal(io.get_array("metric"), np.zeros((2, 2)))
     io.set_array_view("empty", np.zeros((0, 3)))
     assert io.get_array("empty").shape == (0, 3)
+
+
+def test_static_scratch_entry_rejects_bad_arguments_before_any_device_work():
+    """The allocation-free entry validates its arguments on the host: no CUDA call is reached."""
+    import ctypes
+    L = _lib.load()
+    err = ctypes.create_string_buffer(256)
+    idx = np.zeros(2, np.int64)
+    val = np.zeros(2)
+
+    def call(nx, ny, h=0.1, metric=1, nseeds=1, sidx=idx, values=1):
+        return L.hfm_solve_riemann2_static_scratch(nx, ny, h, metric, 0, nseeds, sidx.ctypes.data,
+                                                   val.ctypes.data, values, None, err, 256)
+
+    assert call(8, 8, metric=0) == 7                      # null metric
+    assert call(8, 8, values=0) == 7                      # null output
+    assert call(0, 8) == 2 and call(8, 8, h=0.0) == 2     # empty grid, bad scale
+    assert call(1 << 40, 1 << 40) == 2 and b"limit" in err.value   # no overflow of nx * ny
+    assert call(600, 600) == 2 and b"262144-cell limit" in err.value
+    assert call(8, 8, nseeds=0) == 2 and call(8, 8, nseeds=1025) == 2
+    bad = np.array([64, 0], np.int64)
+    assert call(8, 8, nseeds=2, sidx=bad) == 2 and b"out of range" in err.value

@@ -2,7 +2,9 @@
 
 Tolerances: FP64 arrival times within 1e-10 relative max-norm of the reference (the solver
 reproduces fast marching's accumulation order, so most cells are bit-identical); stencil-derived
-integers (nAccepted, MaxStencilWidth) exact; FP32 path within 1e-4 relative of FP64.
+integers (nAccepted, MaxStencilWidth) exact; activeNeighs equal except where a symmetric
+difference's two neighbours hold exactly the same value (fast marching then takes the side it
+accepted first, this solver the +e side); FP32 path within 1e-5 relative of FP64.
 """
 import os
 import subprocess
@@ -48,7 +50,59 @@ def test_golden_values(name):
     assert same > 0.99, f"only {same:.4f} of the cells are bit-identical"
     act_ref = ref["activeNeighs"].astype(np.uint64)
     act = out["activeNeighs"].astype(np.uint64)
-    assert np.mean(act_ref != act) <= 1e-2
+    untied = untied_active_differences(params, ref["values"], act_ref, act)
+    assert not untied, f"activeNeighs differ away from exact ties at cells {untied[:10]}"
+
+
+def stencil_offsets_per_cell(params):
+    """(nfwd, offsets [N][nfwd+nsym][ndim]) of the stencil each cell of `params` uses."""
+    model = params["model"]
+    dims = [int(d) for d in params["dims"]]
+    if model.startswith("Riemann"):
+        out = gpu_solve(params, exportStencils=1.0, exportValues=0.0)
+        nk = 3 if len(dims) == 2 else 6
+        return 0, out["stencilOffsets"].reshape(-1, nk, len(dims)).astype(np.int64)
+    off, _ = O.curvature2_table(model, dims[2], float(params["gridScale"]), float(params.get("xi", 1.0)),
+                                float(params.get("eps", 0.1)), bool(params.get("projective", 0.0)))
+    nfwd = {"ReedsShepp2": 0, "ReedsSheppForward2": 3, "Elastica2": 27}[model]
+    theta = np.arange(int(np.prod(dims))) % dims[2]
+    return nfwd, off[theta].astype(np.int64)
+
+
+def untied_active_differences(params, values, act_ref, act):
+    """Cells whose activeNeighs differ other than by the side of an exactly tied symmetric pair."""
+    bad = np.flatnonzero(act_ref.ravel() != act.ravel())
+    if len(bad) == 0:
+        return []
+    nfwd, offs = stencil_offsets_per_cell(params)
+    dims = values.shape
+    periodic = [False] * (len(dims) - 1) + [params["model"] in ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")]
+    v = values.ravel()
+
+    def value_at(x, e):
+        idx = list(np.unravel_index(x, dims))
+        for a in range(len(dims)):
+            idx[a] += int(e[a])
+            if periodic[a]:
+                idx[a] %= dims[a]
+            elif not 0 <= idx[a] < dims[a]:
+                return np.inf
+        return v[np.ravel_multi_index(idx, dims)]
+
+    untied = []
+    for x in bad:
+        r, o = int(act_ref.ravel()[x]), int(act.ravel()[x])
+        fmask = (1 << nfwd) - 1
+        ok = (r & fmask) == (o & fmask)
+        for j in range(offs.shape[1] - nfwd):
+            rb, ob = (r >> (nfwd + 2 * j)) & 3, (o >> (nfwd + 2 * j)) & 3
+            if rb == ob:
+                continue
+            e = offs[x, nfwd + j]
+            ok = ok and rb in (1, 2) and ob in (1, 2) and value_at(x, e) == value_at(x, -e)
+        if not ok:
+            untied.append(int(x))
+    return untied
 
 
 @pytest.mark.parametrize("name", GOLDEN_SOLVES)
@@ -89,7 +143,7 @@ def test_fp32_path_close_to_fp64(case):
          "rs2_48x30": lambda: W.curvature2_case(48, 30, "ReedsShepp2")}[case]()
     o64 = gpu_solve(p)
     o32 = gpu_solve(p, solverPrecision="float32")
-    assert rel_err(o64["values"], o32["values"]) <= 1e-4
+    assert rel_err(o64["values"], o32["values"]) <= 1e-5
 
 
 def test_yxz_ordering_default_of_python_binding():
