@@ -48,10 +48,11 @@ def parse_args(argv=None):
     ap.add_argument("--batch-riemann", type=int, default=384, help="Riemann2 instances of the batched mix")
     ap.add_argument("--batch-lifted", type=int, default=128, help="ReedsShepp2/Elastica2 instances of the mix")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-model leg")
-    ap.add_argument("--serve-rates", default="50,200,1000", help="Poisson arrival rates (req/s) of the serving leg")
-    ap.add_argument("--serve-requests", type=int, default=200, help="requests per arrival rate")
+    ap.add_argument("--serve-rates", default="50,100,200,500,1000,2000",
+                    help="Poisson arrival rates (req/s) of the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=300, help="requests per arrival rate")
     ap.add_argument("--serve-pool", type=int, default=48, help="distinct request payloads the arrivals draw from")
-    ap.add_argument("--serve-lanes", type=int, default=2)
+    ap.add_argument("--serve-resident", type=int, default=64, help="instances resident at once in the served arm")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--tti-side", type=int, default=128, help="grid side of the TTI3 differentiation leg")
     ap.add_argument("--tti-fd-voxels", type=int, default=32, help="voxels checked by central differences")
@@ -286,10 +287,11 @@ def serving_leg(args, rank, world):
 
     Requests: 60% Riemann2 (64-1024 sides), 25% Riemann3 (64-192, walls), 15% ReedsShepp2
     (N x N x 60, N 64-256), 1-4 seeds, FP32, drawn from a pool of distinct seeded payloads;
-    Poisson arrivals at each rate. The served arm is hfm_server with `lanes` lanes (batches of the
-    waiting requests, admission by device memory); the plain arm is the same server with one lane
-    and batches of one request (one solve at a time on the whole GPU). Latency = completion - submit
-    (host clock of the server); throughput = requests / (last completion - first submit).
+    Poisson arrivals at each rate. The served arm is hfm_server with resident solvers (up to
+    --serve-resident instances at once, each released when its own tiles converge); the plain arm
+    is the same server with max_batch = 1 (every request through hfm_run, one at a time on the
+    whole GPU). Latency = completion - submit (host clock of the server); throughput = requests /
+    (last completion - first submit). Both arms run the same requests in the same order.
     """
     import threading
     import hamiltonfastmarching_b200 as H
@@ -307,13 +309,13 @@ def serving_leg(args, rank, world):
     cells = [int(np.prod(p["dims"])) for p in pool]
     rates = [float(r) for r in args.serve_rates.split(",") if r]
 
-    def run_arm(lanes, max_batch, rate, seed):
+    def run_arm(max_batch, rate, seed):
         rng = np.random.default_rng(seed)
         picks = rng.integers(0, len(pool), args.serve_requests)
         gaps = rng.exponential(1.0 / rate, args.serve_requests)
         tickets = [None] * args.serve_requests
         lat, done_t, sub_t = [], [], []
-        with Server(lanes=lanes, max_batch=max_batch) as srv:
+        with Server(max_batch=max_batch) as srv:
             def waiter():
                 for i in range(args.serve_requests):
                     while tickets[i] is None:
@@ -345,20 +347,23 @@ def serving_leg(args, rank, world):
                 "cells_per_s": ncell / span, "batches": st["batches"], "max_batch": st["max_batch"],
                 "peak_bytes": st["peak_bytes"]}
 
-    # warm-up of both paths
-    with Server(lanes=args.serve_lanes) as srv:
+    # warm-up of both paths (every family's resident solver and the plain path)
+    with Server(max_batch=args.serve_resident) as srv:
+        for t in [srv.submit(pool[k]) for k in range(min(8, len(pool)))]:
+            t.wait()
+    with Server(max_batch=1) as srv:
         for t in [srv.submit(pool[k]) for k in range(min(4, len(pool)))]:
             t.wait()
     out = []
     for r in rates:
-        served = run_arm(args.serve_lanes, 64, r, seed=11 + int(r))
-        plain = run_arm(1, 1, r, seed=11 + int(r))
+        served = run_arm(args.serve_resident, r, seed=11 + int(r))
+        plain = run_arm(1, r, seed=11 + int(r))
         out.append({"rate_req_per_s": r, "served": served, "plain_one_at_a_time": plain,
                     "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"],
                     "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]})
     # FP32 served results against the FP64 path on a 1% sample (at least 2) of the pool
     errs = []
-    with Server(lanes=args.serve_lanes) as srv:
+    with Server(max_batch=args.serve_resident) as srv:
         sample = list(range(0, len(pool), max(1, len(pool) // max(2, len(pool) // 100))))[:max(2, len(pool) // 100)]
         t32 = [srv.submit(pool[k]) for k in sample]
         t64 = [srv.submit(dict(pool[k], solverPrecision="float64")) for k in sample]
@@ -368,7 +373,9 @@ def serving_leg(args, rank, world):
             errs.append(float(np.max(np.abs(v64[fin] - v32[fin])) / np.max(np.abs(v64[fin]))))
     return {"workload": "60% Riemann2 (64-1024), 25% Riemann3 (64-192, walls), 15% ReedsShepp2 (N x N x 60, "
                         "N 64-256), 1-4 seeds, FP32, Poisson arrivals",
-            "requests_per_rate": args.serve_requests, "pool_payloads": len(pool), "lanes": args.serve_lanes,
+            "requests_per_rate": args.serve_requests, "pool_payloads": len(pool), "resident_max": args.serve_resident,
+            "size_note": f"{args.serve_requests} requests per rate (the config's 10,000 per rate would take hours "
+                         f"for both arms at 6 rates)",
             "rates": out, "fp32_max_rel_err_vs_fp64": max(errs), "fp64_sample": len(errs),
             "input_generation_s": gen_s,
             "path": "serving.Server (hfm_server C ABI) from host arrays, H2D/D2H inside the latency"}

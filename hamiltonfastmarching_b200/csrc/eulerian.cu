@@ -20,6 +20,8 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <map>
+#include <iterator>
 #include <chrono>
 #include <cmath>
 
@@ -109,6 +111,8 @@ struct Dev {
     long long ncells;         // total cells
     long long ntile;          // total tiles
     long long ntc;            // tile-major cell count = ntile * 64
+    long long sstride;        // distance between the stencil slots of a cell in code / weight (ntc,
+                              // or the arena's size when this is a view of one arena instance)
     Real *values;             // RowMajor
     unsigned *code;           // [ND][ntc] per-cell offsets + visibility/flags (per-cell stencils)
     Real *weight;             // [ND][ntc]
@@ -116,8 +120,10 @@ struct Dev {
     unsigned *vis;            // [ntc] slot visibility + flags (shared stencils)
     const int8_t *cls_off;    // [nclass][ND][3]
     const Real *cls_w;        // [nclass][ND]
-    // reverse tile dependencies: tile T -> tiles whose stencils read T, with the cells they read
+    // reverse tile dependencies: tile T -> tiles whose stencils read T, with the cells they read;
+    // entries [dep_ptr[T], dep_end[T]) (dep_end null: dep_ptr[T + 1], a CSR over the tile space)
     const long long *dep_ptr;
+    const long long *dep_end;
     const int *dep_tile;
     const unsigned long long *dep_mask;    // cells of T read by the dependent tile
     const unsigned long long *dep_dmask;   // cells of the dependent tile that read T
@@ -127,7 +133,10 @@ struct Dev {
     // largest value among a tile's solvable cells (+inf while any is unreached); values only
     // decrease, so a stale entry is an upper bound
     unsigned long long *maxval;            // [ntile]
-    unsigned long long *rstat;             // [8][4] per round slot: min key, max key, tiles solved, -
+    unsigned long long *rstat;             // [8][nslots][4] per round slot (and instance slot of a
+                                           // resident solver): min key, max key, tiles solved, -
+    int nslots;                            // 0 or 1: one statistics row per round (batch solver)
+    unsigned *live;                        // [3][nslots] tiles of each instance slot in each list, or null
     // per instance: key = value * kscale, so that the keys of a batch measure the progress of each
     // instance's front on a common scale (nullptr: keys are the values)
     const double *kscale;
@@ -261,9 +270,9 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
                 vm = (visw >> (s + 1)) & 1u;
             }
         } else {
-            const unsigned cd = P.code[k * P.ntc + c];
+            const unsigned cd = P.code[k * P.sstride + c];
             o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
-            w[k] = P.weight[k * P.ntc + c];
+            w[k] = P.weight[k * P.sstride + c];
             vp = cd & kVisPlus;
             vm = (k >= NFWD) && (cd & kVisMinus);
         }
@@ -328,17 +337,30 @@ __device__ __forceinline__ void cell_flags(const Dev<Real> &P, long long c, bool
     }
 }
 
-// Appends tile D to list `li` unless it is already there (flag dedupe). Called by all lanes with
-// their own `want`; one atomicAdd per warp reserves the slots.
+// Appends tile D (of instance slot `inst`) to list `li` unless it is already there (flag dedupe).
+// Called by all lanes with their own `want`; one atomicAdd per warp reserves the slots. A resident
+// solver also counts the tiles of each instance per list (all lanes of a call push tiles of one
+// instance).
 template <typename Real>
-__device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bool want, int lane) {
+__device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bool want, int lane, int inst) {
     if (want) want = atomicExch(&P.flag[li][D], 1u) == 0u;
     const unsigned ballot = __ballot_sync(0xffffffffu, want);
     if (!ballot) return;
     unsigned base = 0;
-    if (lane == __ffs(ballot) - 1) base = atomicAdd(P.count[li], (unsigned)__popc(ballot));
+    if (lane == __ffs(ballot) - 1) {
+        base = atomicAdd(P.count[li], (unsigned)__popc(ballot));
+        if (P.live) atomicAdd(P.live + li * P.nslots + inst, (unsigned)__popc(ballot));
+    }
     base = __shfl_sync(0xffffffffu, base, __ffs(ballot) - 1);
     if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
+}
+
+// Statistics row of round slot `slot` for instance slot `inst` (one row per round slot when the
+// solver keeps no per-instance statistics).
+template <typename Real>
+__device__ __forceinline__ unsigned long long *stat_row(const Dev<Real> &P, int slot, int inst) {
+    const int ns = P.nslots > 1 ? P.nslots : 1;
+    return P.rstat + ((long long)slot * ns + (ns > 1 ? inst : 0)) * 4;
 }
 
 // Pushes the dependents of tile T that read a cell of `mask`, marking as dirty the cells of each
@@ -350,8 +372,9 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
                                                 unsigned long long self_pending, unsigned long long mu,
                                                 unsigned long long kb, int lane) {
     bool any = false;
+    const int inst = P.tile_inst[T];
     if (mask) {
-        const long long b = P.dep_ptr[T], e = P.dep_ptr[T + 1];
+        const long long b = P.dep_ptr[T], e = P.dep_end ? P.dep_end[T] : P.dep_ptr[T + 1];
         for (long long base = b; base < e; base += 32) {
             const long long i = base + lane;
             bool want = false;
@@ -371,17 +394,18 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
                 }
             }
             any |= __any_sync(0xffffffffu, want);
-            push_tiles(P, li, D, want, lane);
+            push_tiles(P, li, D, want, lane, inst);
         }
     }
     if (self_pending && lane == 0) {
         atomicOr(P.dirty + T, self_pending);
         atomicMin(P.key + T, kb);
     }
-    push_tiles(P, li, T, self_pending != 0ull && lane == 0, lane);
+    push_tiles(P, li, T, self_pending != 0ull && lane == 0, lane, inst);
     if ((any || self_pending) && lane == 0) {
-        atomicMin(P.rstat + slot * 4 + 0, kb);
-        atomicMax(P.rstat + slot * 4 + 1, kb);
+        unsigned long long *row = stat_row(P, slot, inst);
+        atomicMin(row + 0, kb);
+        atomicMax(row + 1, kb);
     }
 }
 
@@ -403,7 +427,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
             o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
             bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
         } else {
-            const unsigned cd = P.code[k * P.ntc + c];
+            const unsigned cd = P.code[k * P.sstride + c];
             o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
             bits = ((cd & kVisPlus) ? 1u : 0u) | ((cd & kVisMinus) ? 2u : 0u);
         }
@@ -597,7 +621,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
             kt = __shfl_sync(0xffffffffu, kt, 0);
             if (__longlong_as_double(kt) > theta) {
                 // not yet in the band: carry to the next round with its key
-                push_tiles(P, nxt, T, lane == 0, lane);
+                push_tiles(P, nxt, T, lane == 0, lane, 0);
                 if (lane == 0) atomicMin(P.rstat + nslot * 4 + 0, kt);
                 continue;
             }
@@ -701,8 +725,8 @@ __global__ void riemann_stencil_kernel(Dev<Real> P, const double *metric, int8_t
     }
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-        P.code[k * P.ntc + R.c] = pack_off(off[k][0], off[k][1], off[k][2]);
-        P.weight[k * P.ntc + R.c] = (Real)w[k];
+        P.code[k * P.sstride + R.c] = pack_off(off[k][0], off[k][1], off[k][2]);
+        P.weight[k * P.sstride + R.c] = (Real)w[k];
         if (plain_off) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) plain_off[(x * NK + k) * 3 + a] = (int8_t)off[k][a];
@@ -728,8 +752,8 @@ __global__ void diagonal_stencil_kernel(Dev<Real> P, int D, const double *speed,
         const double w = base * (sp * sp);
         int o[3] = {0, 0, 0};
         o[k] = 1;
-        P.code[k * P.ntc + R.c] = pack_off(o[0], o[1], o[2]);
-        P.weight[k * P.ntc + R.c] = (Real)w;
+        P.code[k * P.sstride + R.c] = pack_off(o[0], o[1], o[2]);
+        P.weight[k * P.sstride + R.c] = (Real)w;
         if (plain_off) {
             for (int a = 0; a < 3; ++a) plain_off[(x * D + k) * 3 + a] = (int8_t)o[a];
             plain_w[x * D + k] = w;
@@ -761,8 +785,8 @@ __global__ void tti_setup_kernel(Dev<Real> P, const double *metric) {
 #pragma unroll
     for (int k = 0; k < NSYM; ++k) {
         const bool on = k < n && abs(off[k][0]) < 128 && abs(off[k][1]) < 128 && abs(off[k][2]) < 128;
-        P.code[k * P.ntc + R.c] = on ? pack_off(off[k][0], off[k][1], off[k][2]) : 0u;
-        P.weight[k * P.ntc + R.c] = on ? Real(1) : Real(0);
+        P.code[k * P.sstride + R.c] = on ? pack_off(off[k][0], off[k][1], off[k][2]) : 0u;
+        P.weight[k * P.sstride + R.c] = on ? Real(1) : Real(0);
     }
 }
 
@@ -805,8 +829,8 @@ __global__ void width_kernel(Dev<Real> P, unsigned *maxw) {
         const GridGeom &g = P.inst[R.i].g;
 #pragma unroll
         for (int k = 0; k < NSYM; ++k) {
-            if (P.weight[k * P.ntc + R.c] == Real(0)) continue;
-            const unsigned cd = P.code[k * P.ntc + R.c];
+            if (P.weight[k * P.sstride + R.c] == Real(0)) continue;
+            const unsigned cd = P.code[k * P.sstride + R.c];
             const int o0 = off_c(cd, 0), o1 = off_c(cd, 1), o2 = off_c(cd, 2);
             const unsigned l1 = abs(o0) + abs(o1) + abs(o2);
             for (int s = 1; s >= -1; s -= 2) {
@@ -972,9 +996,9 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
             o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
             nonzero = P.cls_w[(cls + x2) * ND + k] != Real(0);
         } else {
-            const unsigned cd = P.code[k * P.ntc + c];
+            const unsigned cd = P.code[k * P.sstride + c];
             o[0] = off_c(cd, 0); o[1] = off_c(cd, 1); o[2] = off_c(cd, 2);
-            nonzero = P.weight[k * P.ntc + c] != Real(0);
+            nonzero = P.weight[k * P.sstride + c] != Real(0);
         }
         unsigned bits = 0;
         for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
@@ -988,7 +1012,7 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
             if (SHARE) visw |= 1u << slot;
             else bits |= si == 0 ? kVisPlus : kVisMinus;
         }
-        if (!SHARE) P.code[k * P.ntc + c] |= bits;
+        if (!SHARE) P.code[k * P.sstride + c] |= bits;
     }
     if (SHARE) P.vis[c] = visw;
 }
@@ -1048,7 +1072,7 @@ __global__ void __launch_bounds__(kDepWarps * 32)
                 o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
                 bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
             } else {
-                const unsigned cd = P.code[k * P.ntc + c];
+                const unsigned cd = P.code[k * P.sstride + c];
                 o[0] = off_c(cd, 0); o[1] = off_c(cd, 1); o[2] = off_c(cd, 2);
                 bits = ((cd & kVisPlus) ? 1u : 0u) | ((cd & kVisMinus) ? 2u : 0u);
             }
@@ -1377,9 +1401,9 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
             o0 = o[0]; o1 = o[1]; o2 = o[2];
             wb = A::mul((double)P.cls_w[(I.cls0 + x2) * ND + k], A::mul(m, m));
         } else {
-            const unsigned cd = P.code[k * P.ntc + c];
+            const unsigned cd = P.code[k * P.sstride + c];
             o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
-            wb = (double)P.weight[k * P.ntc + c];
+            wb = (double)P.weight[k * P.sstride + c];
         }
         // active bits of this difference (see active_kernel)
         unsigned act = 0;  // bit0: +e, bit1: -e
@@ -1967,6 +1991,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     P.ncells = N;
     P.ntile = nt;
     P.ntc = ntc;
+    P.sstride = ntc;
     DeviceBuffer<Inst> dinst;
     dinst.upload(hinst, s);
     P.inst = dinst.get();
@@ -2450,9 +2475,35 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     for (EulerResult &r : results) r.t_total_ms = total;
 }
 
+#include "resident.cuh"
+
 }  // namespace detail
 
 using detail::run_batch_impl;
+
+std::string resident_family_key(const EulerProblem &p) {
+    const bool plain = p.adjoint_index.empty() && p.fwd_nvar == 0 && !p.has_stopping() && !p.bypass && !p.want_active &&
+                       !p.want_stencils && !p.retain && p.geo_tips.empty() && p.geo_tips_unoriented.empty() &&
+                       !p.want_geodesic_flow && !p.d_metric && !p.d_walls && !p.d_values_out;
+    if (!plain) return "";
+    const char *prec = p.fp64 ? "f64" : "f32";
+    if (p.kind == StencilKind::RiemannPerCell && !p.diagonal && (p.ndim == 2 || p.ndim == 3))
+        return std::string("riemann") + std::to_string(p.ndim) + "/" + prec;
+    if (p.kind == StencilKind::SharedByTheta && p.angular && p.nfwd == 0 && p.nsym == 4)
+        return std::string("reedsshepp2/") + prec;
+    return "";
+}
+
+std::unique_ptr<ResidentFamily> make_resident_family(const EulerProblem &p) {
+    using namespace detail;
+    if (p.kind == StencilKind::RiemannPerCell && p.ndim == 2)
+        return p.fp64 ? make_resident_impl<double, 0, 3, kKindRiemann>(p) : make_resident_impl<float, 0, 3, kKindRiemann>(p);
+    if (p.kind == StencilKind::RiemannPerCell && p.ndim == 3)
+        return p.fp64 ? make_resident_impl<double, 0, 6, kKindRiemann>(p) : make_resident_impl<float, 0, 6, kKindRiemann>(p);
+    if (p.kind == StencilKind::SharedByTheta && p.nfwd == 0 && p.nsym == 4)
+        return p.fp64 ? make_resident_impl<double, 0, 4, kKindShare>(p) : make_resident_impl<float, 0, 4, kKindShare>(p);
+    throw Error(HFM_ERR_UNSUPPORTED, "no resident solver for this model family");
+}
 
 void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
     if (probs.empty()) {

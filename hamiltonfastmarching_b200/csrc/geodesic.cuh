@@ -174,9 +174,9 @@ __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1,
                 o0 = o[0]; o1 = o[1]; o2 = o[2];
                 wb = A::mul((double)P.cls_w[(I.cls0 + x2) * ND + k], A::mul(m, m));
             } else {
-                const unsigned cd = P.code[k * P.ntc + c];
+                const unsigned cd = P.code[k * P.sstride + c];
                 o0 = off_c(cd, 0); o1 = off_c(cd, 1); o2 = off_c(cd, 2);
-                wb = (double)P.weight[k * P.ntc + c];
+                wb = (double)P.weight[k * P.sstride + c];
             }
             // active sides of this difference, as the activeNeighs bits (active_kernel)
             unsigned act = 0;  // bit0: +e, bit1: -e

@@ -1342,6 +1342,37 @@ void run_sensitivity(Store &io, const std::shared_ptr<void> &retained) {
 }
 
 }  // namespace
+
+namespace {
+struct PreparedRunImpl final : PreparedRun {
+    hfm_io *io;
+    Prepared q;
+    explicit PreparedRunImpl(hfm_io *h) : io(h) {}
+    ~PreparedRunImpl() override { io->store.current_setter = Setter::User; }
+    EulerProblem &problem() override { return q.p; }
+    bool skip() const override { return q.skip; }
+    void finish(const EulerResult &r) override {
+        finish_model(io->store, q, r);
+        io->store.usage_report();
+    }
+    void fail() override {
+        if (q.values_dst) io->store.erase_field("values");
+        q.values_dst = nullptr;
+    }
+};
+}  // namespace
+
+// Parses a store as hfm_run does; the store stays in the compute setter until the handle goes.
+std::unique_ptr<PreparedRun> prepare_run(hfm_io *io) {
+    auto r = std::make_unique<PreparedRunImpl>(io);
+    Store &st = io->store;
+    st.current_setter = Setter::Compute;
+    const std::string model = st.get_string("model");
+    prepare_model(st, model == "Elastica2_5" ? "Elastica2" : model, r->q);
+    r->q.p.retain = false;
+    return r;
+}
+
 }  // namespace hfm
 
 // =============================================================================== C ABI

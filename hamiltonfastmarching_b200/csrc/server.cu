@@ -1,15 +1,24 @@
-// Request loop for serving solves: continuous batching over lanes, admission by device memory.
+// Request loop for serving solves: continuous batching into resident persistent solvers, admission
+// by device memory.
 //
-// The reference answers one Run(IO&) at a time (Headers/DispatchAndRun.h:224-244). Here a client
-// submits filled stores; `lanes` worker threads each own a CUDA stream; a batch started while
-// others run gives its persistent solver 1/lanes of the SMs, a batch started alone the whole GPU.
-// A lane that is free takes, in arrival order, the waiting requests
-// whose estimated device footprint fits in what the running batches leave of the memory budget
-// (up to max_batch of them) and solves them as one batch (hfm_run_batch: instances of a family
-// share a launch sequence). Requests that arrive while other batches are on the device are
-// admitted by the next lane to free up, and their work overlaps with the running batches on the
-// device. Results land in each request's own store; per-request submit / start / done times are
-// kept for latency statistics.
+// The reference answers one Run(IO&) at a time (Headers/DispatchAndRun.h:224-244). Here clients
+// submit filled stores and one scheduler thread owns the GPU work:
+//   * a submitted request is parsed as hfm_run parses it (same keys, defaults and messages);
+//   * a plain solve (arrival times only) of a Riemann2, Riemann3 or ReedsShepp2 family is admitted,
+//     in arrival order, while its estimated device footprint fits in the memory budget and a slot
+//     is free, into the resident solver of its family (resident.cuh): its stencils, visibility and
+//     tile dependencies are built in the family's arena and its seed tiles join the running
+//     solver's lists at the next slice;
+//   * the resident solver runs in slices; a slice ends as soon as an instance converges, so each
+//     request is released when its own tiles drain, or soon after a new request arrives (the
+//     attention word, read by the solver between rounds), so that it is admitted while the others
+//     keep running; families with work take turns (4 ms slices when more than one has work);
+//   * other requests (geodesics, sensitivities, variations, stopping criteria, cached values,
+//     exports of stencils or activeNeighs, TTI3 and the other models) run through hfm_run between
+//     slices, one at a time.
+// With max_batch = 1 every request runs through hfm_run, one at a time: the plain loop.
+// Results land in each request's own store; per-request submit / start / done times are kept for
+// latency statistics.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +26,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -26,6 +36,7 @@
 
 #include "device_buffer.hpp"
 #include "io.hpp"
+#include "solver.hpp"
 #include "store_handle.hpp"
 
 namespace {
@@ -38,7 +49,9 @@ struct Request {
     size_t bytes = 0;
     double t_submit = 0, t_start = 0, t_done = 0;
     int status = HFM_OK;
-    bool done = false;
+    bool done = false, counted = false;
+    std::unique_ptr<hfm::PreparedRun> prep;
+    std::string family;
 };
 
 // Device bytes of a request: per-cell solver state of its model and precision (stencil codes and
@@ -69,88 +82,217 @@ size_t estimate_bytes(const hfm::Store &st) {
     return cells * per_cell + (size_t(4) << 20);
 }
 
+int error_code_of(const std::exception &e) {
+    if (const auto *h = dynamic_cast<const hfm::Error *>(&e)) return h->code;
+    if (dynamic_cast<const std::bad_alloc *>(&e)) return HFM_ERR_NOMEM;
+    return HFM_ERR_VALUE;
+}
+
 }  // namespace
 
 struct hfm_server {
     hfm_server_config cfg{};
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Request *> queue;
+    std::deque<Request *> queue;  // submitted, not yet taken by the scheduler
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
-    std::vector<std::thread> lanes;
+    std::thread scheduler;
     size_t budget = 0, in_use = 0, peak = 0;
     uint64_t next_ticket = 1;
-    unsigned long long submitted = 0, completed = 0, batches = 0, max_batch_seen = 0;
-    int running = 0;
+    unsigned long long submitted = 0, completed = 0, slices = 0, max_resident = 0, resident = 0;
     bool stop = false;
+    bool started = false, start_ok = false;
+    std::condition_variable cv_started;
+    // attention word: raised by submit, read by the running solver (host memory mapped to the GPU)
+    volatile unsigned *attn_host = nullptr;
+    unsigned *attn_dev = nullptr;
     Clock::time_point t0 = Clock::now();
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
-    void lane_main() {
+    void complete(Request *r, int status) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            r->status = status;
+            r->t_done = now();
+            r->done = true;
+            if (r->counted) in_use -= r->bytes;
+            r->counted = false;
+            ++completed;
+        }
+        cv_done.notify_all();
+    }
+
+    // A request through hfm_run (the ordinary single-solve path).
+    void run_plain(Request *r) {
+        r->prep.reset();  // hfm_run parses the store again
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            r->t_start = now();
+            in_use += r->bytes;
+            r->counted = true;
+            peak = std::max(peak, in_use);
+        }
+        const int rc = hfm_run(r->io, nullptr);
+        complete(r, rc);
+    }
+
+    void scheduler_main() {
         cudaStream_t stream = nullptr;
-        const bool ok = cudaSetDevice(cfg.device) == cudaSuccess &&
-                        cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess;
+        bool ok = cudaSetDevice(cfg.device) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess;
+        unsigned *host_word = nullptr;
+        if (ok) ok = cudaHostAlloc((void **)&host_word, sizeof(unsigned), cudaHostAllocMapped) == cudaSuccess;
+        if (ok) {
+            *host_word = 0u;
+            ok = cudaHostGetDevicePointer((void **)&attn_dev, host_word, 0) == cudaSuccess;
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            attn_host = host_word;
+            started = true;
+            start_ok = ok;
+        }
+        cv_started.notify_all();
+        if (!ok) {
+            if (host_word) cudaFreeHost(host_word);
+            if (stream) cudaStreamDestroy(stream);
+            return;
+        }
         hfm::current_stream() = stream;
-        std::vector<Request *> batch;
-        std::vector<hfm_io *> ios;
-        std::vector<int> codes;
+        std::deque<Request *> waiting;  // parsed resident requests, not yet admitted
+        std::map<std::string, std::unique_ptr<hfm::ResidentFamily>> fams;
+        std::unordered_map<int64_t, Request *> running;
+        size_t turn = 0;
         for (;;) {
-            size_t bytes = 0;
+            std::vector<Request *> incoming;
+            bool busy = !waiting.empty();
+            for (const auto &f : fams) busy = busy || f.second->has_work();
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] {
-                    return (stop && queue.empty()) || (!queue.empty() && in_use + queue.front()->bytes <= budget);
-                });
-                if (queue.empty()) break;  // stopping
-                batch.clear();
-                // leave a fair share of the waiting requests to the other free lanes
-                const int free_lanes = std::max(1, cfg.lanes - running);
-                const int limit = std::min<int>(cfg.max_batch, ((int)queue.size() + free_lanes - 1) / free_lanes);
-                while (!queue.empty() && (int)batch.size() < limit &&
-                       in_use + bytes + queue.front()->bytes <= budget) {
-                    bytes += queue.front()->bytes;
-                    batch.push_back(queue.front());
-                    queue.pop_front();
-                }
-                in_use += bytes;
-                peak = std::max(peak, in_use);
-                ++running;
-                // SM share of this batch's persistent solver: the whole GPU when it runs alone (low
-                // load: the latency of a plain solve), 1/lanes when other batches are on the device
-                // (their solvers then run side by side)
-                hfm::solver_share() = running > 1 ? cfg.lanes : 1;
-                const double t = now();
-                for (Request *r : batch) r->t_start = t;
-                if (!queue.empty()) cv_work.notify_one();  // leave the rest to another free lane
+                if (!busy) cv_work.wait(lk, [&] { return stop || !queue.empty(); });
+                if (stop && queue.empty() && !busy) break;
+                incoming.assign(queue.begin(), queue.end());
+                queue.clear();
+                *attn_host = 0u;
             }
-            ios.clear();
-            for (Request *r : batch) ios.push_back(r->io);
-            codes.assign(batch.size(), HFM_ERR_CUDA);
-            if (ok) {
-                hfm_run_batch(ios.data(), (int)ios.size(), nullptr, codes.data());
-                cudaStreamSynchronize(stream);
-            } else {
-                for (hfm_io *io : ios) io->last_error = "serving lane could not set up its CUDA stream";
+            // ---- parse: resident families wait for admission, the rest run now through hfm_run
+            for (Request *r : incoming) {
+                if (cfg.max_batch <= 1) {
+                    run_plain(r);
+                    continue;
+                }
+                r->io->last_error.clear();
+                try {
+                    r->prep = hfm::prepare_run(r->io);
+                    r->family = r->prep->skip() ? std::string() : hfm::resident_family_key(r->prep->problem());
+                } catch (const std::exception &e) {
+                    r->io->last_error = e.what();
+                    r->prep.reset();
+                    complete(r, error_code_of(e));
+                    continue;
+                }
+                if (r->family.empty()) run_plain(r);
+                else waiting.push_back(r);
+            }
+            // ---- admission in arrival order, by memory budget and free slots
+            while (!waiting.empty()) {
+                Request *r = waiting.front();
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    if ((in_use > 0 && in_use + r->bytes > budget) || resident >= (unsigned long long)cfg.max_batch) break;
+                    in_use += r->bytes;
+                    r->counted = true;
+                    peak = std::max(peak, in_use);
+                }
+                bool admitted = false;
+                try {
+                    auto &fam = fams[r->family];
+                    if (!fam) fam = hfm::make_resident_family(r->prep->problem());
+                    int mw = 0;
+                    admitted = fam->admit(r->prep->problem(), (int64_t)r->ticket, &mw);
+                } catch (const std::exception &e) {
+                    waiting.pop_front();
+                    r->io->last_error = e.what();
+                    r->prep->fail();
+                    r->prep.reset();
+                    complete(r, error_code_of(e));
+                    continue;
+                }
+                if (!admitted) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    in_use -= r->bytes;
+                    r->counted = false;
+                    break;
+                }
+                waiting.pop_front();
+                running[(int64_t)r->ticket] = r;
+                std::lock_guard<std::mutex> lk(mu);
+                r->t_start = now();
+                ++resident;
+                max_resident = std::max(max_resident, resident);
+            }
+            // ---- one slice of the next family with work
+            std::vector<std::string> keys;
+            for (const auto &f : fams)
+                if (f.second->has_work()) keys.push_back(f.first);
+            if (keys.empty()) continue;
+            const std::string key = keys[turn++ % keys.size()];
+            hfm::ResidentFamily &fam = *fams[key];
+            std::vector<std::pair<int64_t, hfm::EulerResult>> done;
+            int fail_code = HFM_OK;
+            std::string fail_msg;
+            try {
+                fam.slice(attn_dev, 1.0, keys.size() > 1 ? 4.0 : 0.0);
+                fam.collect(done);
+            } catch (const std::exception &e) {
+                fail_code = error_code_of(e);
+                fail_msg = e.what();
             }
             {
                 std::lock_guard<std::mutex> lk(mu);
-                const double t = now();
-                for (size_t k = 0; k < batch.size(); ++k) {
-                    batch[k]->status = codes[k];
-                    batch[k]->t_done = t;
-                    batch[k]->done = true;
-                }
-                in_use -= bytes;
-                --running;
-                completed += batch.size();
-                ++batches;
-                max_batch_seen = std::max<unsigned long long>(max_batch_seen, batch.size());
+                ++slices;
             }
-            cv_done.notify_all();
-            cv_work.notify_all();
+            for (auto &d : done) {
+                Request *r = running[d.first];
+                running.erase(d.first);
+                int rc = HFM_OK;
+                try {
+                    r->prep->finish(d.second);
+                } catch (const std::exception &e) {
+                    r->io->last_error = e.what();
+                    r->prep->fail();
+                    rc = error_code_of(e);
+                }
+                r->prep.reset();
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    --resident;
+                }
+                complete(r, rc);
+            }
+            if (fail_code != HFM_OK) {  // the family's solver failed: its requests fail with it
+                std::vector<int64_t> lost;
+                fam.abandon(lost);
+                for (int64_t t : lost) {
+                    Request *r = running[t];
+                    running.erase(t);
+                    r->io->last_error = fail_msg;
+                    r->prep->fail();
+                    r->prep.reset();
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        --resident;
+                    }
+                    complete(r, fail_code);
+                }
+                fams.erase(key);
+            }
         }
-        if (stream) cudaStreamDestroy(stream);
+        fams.clear();
+        cudaStreamSynchronize(stream);
+        cudaFreeHost(host_word);
+        cudaStreamDestroy(stream);
     }
 };
 
@@ -160,14 +302,23 @@ hfm_server *hfm_server_create(const hfm_server_config *cfg) {
     try {
         auto s = std::make_unique<hfm_server>();
         if (cfg) s->cfg = *cfg;
-        if (s->cfg.lanes <= 0) s->cfg.lanes = 2;
         if (s->cfg.max_batch <= 0) s->cfg.max_batch = 64;
+        if (s->cfg.max_batch > 256) s->cfg.max_batch = 256;
         if (cudaSetDevice(s->cfg.device) != cudaSuccess) return nullptr;
         hfm::keep_pool_cached();
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
         s->budget = s->cfg.hbm_budget_bytes > 0 ? (size_t)s->cfg.hbm_budget_bytes : (size_t)(0.8 * (double)free_b);
-        for (int i = 0; i < s->cfg.lanes; ++i) s->lanes.emplace_back([p = s.get()] { p->lane_main(); });
+        s->scheduler = std::thread([p = s.get()] { p->scheduler_main(); });
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_started.wait(lk, [&] { return s->started; });
+            if (!s->start_ok) {
+                lk.unlock();
+                s->scheduler.join();
+                return nullptr;
+            }
+        }
         return s.release();
     } catch (...) {
         return nullptr;
@@ -192,6 +343,7 @@ int hfm_server_submit(hfm_server *s, hfm_io *io, uint64_t *ticket) {
         s->queue.push_back(r.get());
         s->reqs.emplace(r->ticket, std::move(r));
         ++s->submitted;
+        if (s->attn_host) *s->attn_host = 1u;  // a running slice ends soon so that it is admitted
     } catch (...) {
         return HFM_ERR_NOMEM;
     }
@@ -231,10 +383,10 @@ int hfm_server_get_stats(hfm_server *s, hfm_server_stats *st) {
     std::lock_guard<std::mutex> lk(s->mu);
     st->submitted = s->submitted;
     st->completed = s->completed;
-    st->batches = s->batches;
-    st->max_batch = s->max_batch_seen;
+    st->batches = s->slices;
+    st->max_batch = s->max_resident;
     st->queued = s->queue.size();
-    st->running_batches = (unsigned long long)s->running;
+    st->running_batches = s->resident;
     st->budget_bytes = (double)s->budget;
     st->bytes_in_use = (double)s->in_use;
     st->peak_bytes = (double)s->peak;
@@ -248,7 +400,7 @@ void hfm_server_destroy(hfm_server *s) {
         s->stop = true;
     }
     s->cv_work.notify_all();
-    for (std::thread &t : s->lanes) t.join();
+    if (s->scheduler.joinable()) s->scheduler.join();
     delete s;
 }
 

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <string>
 #include <memory>
+#include <utility>
 #include <vector>
 
 namespace hfm {
@@ -159,6 +160,48 @@ void default_schedule(EulerProblem &p);
 // One launch sequence for many instances of one model family and precision (a global tile space
 // over all instances, one persistent solver launch). Results are in the order of `probs`.
 void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results);
+
+// Resident solver of one model family for the serving loop (resident.cuh): admitted instances live
+// in a device arena and one persistent solver runs them in slices; each instance is released as
+// soon as its own tiles drain. All calls come from one thread, on its current stream.
+class ResidentFamily {
+public:
+    virtual ~ResidentFamily() = default;
+    // Sets up `p` in the arena and queues its seed tiles for the next slice. False: no free slot.
+    // Throws Error for an invalid instance (nothing of it stays resident).
+    virtual bool admit(const EulerProblem &p, int64_t ticket, int *max_width) = 0;
+    // Runs the solver until an instance converges, every tile is done, the attention word (device
+    // view of host memory, may be null) is raised after min_ms, or max_ms (0: no limit) has passed.
+    virtual void slice(const volatile unsigned *attn_dev, double min_ms, double max_ms) = 0;
+    // Converged instances: their tickets and results (values, nAccepted, MaxStencilWidth, times).
+    virtual void collect(std::vector<std::pair<int64_t, EulerResult>> &done) = 0;
+    // Drops every instance after a failure of the solver; their tickets are appended.
+    virtual void abandon(std::vector<int64_t> &tickets) = 0;
+    virtual bool has_work() const = 0;
+    virtual int resident() const = 0;
+    virtual size_t arena_bytes() const = 0;
+};
+// A store's request parsed for the serving loop (the part of Run before the solver loop), and the
+// exports that finish it (run.cu): the same keys, defaults, messages and usage report as hfm_run.
+struct PreparedRun {
+    virtual ~PreparedRun() = default;
+    virtual EulerProblem &problem() = 0;
+    virtual bool skip() const = 0;    // no seeds and nothing cached: nothing to solve
+    // Exports a solve's results into the store and closes the request (usage report).
+    virtual void finish(const EulerResult &r) = 0;
+    // Closes a failed request: drops a partly created output field.
+    virtual void fail() = 0;
+};
+
+}  // namespace hfm
+struct hfm_io;
+namespace hfm {
+std::unique_ptr<PreparedRun> prepare_run(hfm_io *io);
+
+// Family of a problem for the resident solver ("" when it is solved through the batch path:
+// other models, or outputs beyond the arrival times), and a new resident solver for it.
+std::string resident_family_key(const EulerProblem &p);
+std::unique_ptr<ResidentFamily> make_resident_family(const EulerProblem &p);
 
 // Curvature model stencil tables built on the host with the C library's cos/sin
 // (Headers/Specializations/Curvature2.h:48-66, 86-100, 178-234, CommonTraits.h:118-161).

@@ -1,12 +1,17 @@
 """Serving loop: continuous batching of solve requests on one GPU (``hfm_server_*`` of the C ABI).
 
-``Server(lanes=2)`` starts the native request loop: ``lanes`` worker threads, each with its own
-CUDA stream and 1/lanes of the SMs for the persistent solver. ``submit(params)`` queues an
-``hfmIn`` dictionary and returns a :class:`Ticket`; a free lane admits, in arrival order, the
-waiting requests whose device footprint fits in the memory budget left by the running batches,
-and solves them as one batch. ``Ticket.result()`` returns the ``hfmOut`` dictionary that
-``hamiltonfastmarching_b200.run`` returns for the same request alone; ``Ticket.times`` gives the
-submit, start and completion times (seconds) used for latency statistics.
+``Server(max_batch=64)`` starts the native request loop: one scheduler thread and, per model
+family (Riemann2, Riemann3, ReedsShepp2, per precision), a resident persistent solver.
+``submit(params)`` queues an ``hfmIn`` dictionary and returns a :class:`Ticket`. A plain solve
+is admitted, in arrival order, while its device footprint fits in the memory budget and fewer
+than ``max_batch`` instances are resident; it joins the running solver at its next slice and is
+released as soon as its own tiles have converged, so requests that arrive while others run share
+the GPU with them and none waits for a larger one. Requests with other outputs (geodesics,
+sensitivities, activeNeighs ...) or other models run through ``hamiltonfastmarching_b200.run``
+between slices. ``max_batch=1`` serves every request that way, one at a time (the plain loop).
+``Ticket.result()`` returns the ``hfmOut`` dictionary that ``hamiltonfastmarching_b200.run``
+returns for the same request alone; ``Ticket.times`` gives the submit, start and completion times
+(seconds) used for latency statistics.
 """
 from __future__ import annotations
 
@@ -52,7 +57,8 @@ class Ticket:
 
 
 class Server:
-    def __init__(self, lanes: int = 2, max_batch: int = 64, hbm_budget_bytes: float = 0.0, device: int = 0):
+    def __init__(self, lanes: int = 1, max_batch: int = 64, hbm_budget_bytes: float = 0.0, device: int = 0):
+        """``lanes`` is accepted for compatibility and not used."""
         self._L = _lib.load()
         cfg = _lib.ServerConfig(device, lanes, max_batch, float(hbm_budget_bytes))
         self._h = self._L.hfm_server_create(ctypes.byref(cfg))

@@ -103,21 +103,24 @@ int hfm_run_sensitivity(hfm_io *io);
 int hfm_run_batch(hfm_io *const *ios, int n, const char *expected_model, int *codes);
 
 /* ---------------------------------------------------------------------------------------------
- * Serving (an extension: the reference answers one Run(IO&) at a time). A server owns `lanes`
- * worker threads, each with its own CUDA stream; a batch's persistent solver takes the whole GPU
- * when it starts alone and 1/lanes of the SMs when other batches are running.
- * A free lane takes the waiting requests in arrival order while their estimated device footprint
- * fits in the memory budget left by the running batches (at most max_batch of them) and solves
- * them as one hfm_run_batch; requests arriving meanwhile are admitted by the next lane to free up,
- * so batches overlap on the device (continuous batching). Each request's outputs are written into
- * its own store, exactly as hfm_run would; the store must stay alive and untouched until the
- * request is released.
+ * Serving (an extension: the reference answers one Run(IO&) at a time). A server owns one
+ * scheduler thread and a resident persistent solver per model family (Riemann2, Riemann3,
+ * ReedsShepp2, per precision). A plain solve (arrival times only) is admitted, in arrival order,
+ * while its estimated device footprint fits in the memory budget and fewer than max_batch
+ * instances are resident: its stencils are built in the family's device arena and its tiles join
+ * the running solver at its next slice; the solver releases each instance as soon as its own
+ * tiles have converged (continuous batching: no request waits for a larger one, and requests that
+ * arrive while others are on the GPU join them). Other requests (other models, geodesics,
+ * sensitivities, variations, stopping criteria, activeNeighs or stencil exports) run through
+ * hfm_run between slices. max_batch = 1 runs every request through hfm_run, one at a time.
+ * `lanes` is not used. Each request's outputs are written into its own store, exactly as hfm_run
+ * would; the store must stay alive and untouched until the request is released.
  */
 typedef struct hfm_server hfm_server;
 typedef struct {
     int device;              /* CUDA device ordinal                                           */
-    int lanes;               /* concurrent batches (default 2)                                 */
-    int max_batch;           /* requests per batch at most (default 64)                        */
+    int lanes;               /* unused (kept for the layout of this structure)                 */
+    int max_batch;           /* resident instances at most (default 64, at most 256; 1: plain)  */
     double hbm_budget_bytes; /* admission budget; <= 0: 80% of the free device memory          */
 } hfm_server_config;
 typedef struct {
@@ -136,7 +139,8 @@ int hfm_server_wait(hfm_server *s, uint64_t ticket, double timeout_s, int *statu
  * seconds since the server was created. */
 int hfm_server_release(hfm_server *s, uint64_t ticket, double *times);
 int hfm_server_get_stats(hfm_server *s, hfm_server_stats *stats);
-/* Finishes the queued and running requests, then stops the lanes. */
+/* Finishes the queued and running requests, then stops the scheduler. batches counts solver
+ * slices, max_batch the most instances resident at once, running_batches those resident now. */
 void hfm_server_destroy(hfm_server *s);
 
 /* Message of the last failure on `io` ("" if none). Valid until the next call on `io`. */
