@@ -103,6 +103,30 @@ __device__ __forceinline__ int inst_of_cell(const Inst *inst, int n, long long x
     return lo;
 }
 
+// Pending work of a tile: the cells whose inputs changed since their last solve and the smallest
+// new value among the changes behind them, updated and taken together by 16-byte atomics (a push
+// and the claim that consumes its cells always agree on the wake-up value).
+struct alignas(16) DirtyWake {
+    unsigned long long mask;   // cells of the tile
+    unsigned long long wake;   // bit pattern of a non-negative double (+inf: none)
+};
+constexpr unsigned long long kInfWake = 0x7ff0000000000000ull;
+
+__device__ __forceinline__ void dirty_add(DirtyWake *dw, unsigned long long bits, unsigned long long wake) {
+    DirtyWake old;  // a torn read only costs a failed compare
+    old.mask = ((volatile unsigned long long *)dw)[0];
+    old.wake = ((volatile unsigned long long *)dw)[1];
+    while (true) {
+        DirtyWake nw;
+        nw.mask = old.mask | bits;
+        nw.wake = wake < old.wake ? wake : old.wake;  // non-negative doubles order as their bits
+        if (nw.mask == old.mask && nw.wake == old.wake) return;
+        const DirtyWake seen = atomicCAS(dw, old, nw);
+        if (seen.mask == old.mask && seen.wake == old.wake) return;
+        old = seen;
+    }
+}
+
 template <typename Real>
 struct Dev {
     const Inst *inst;         // [ninst]
@@ -127,9 +151,12 @@ struct Dev {
     const int *dep_tile;
     const unsigned long long *dep_mask;    // cells of T read by the dependent tile
     const unsigned long long *dep_dmask;   // cells of the dependent tile that read T
-    unsigned long long *dirty;             // [ntile] cells whose inputs changed since their last solve
+    DirtyWake *dirty;                      // [ntile] cells whose inputs changed since their last solve
     // value-ordered scheduling: key = smallest changed value among the tiles that woke the tile
     unsigned long long *key;               // [ntile] bit patterns of non-negative doubles
+    // with the dirty bits, the smallest changed value (unscaled) behind them: a dirty cell whose
+    // value is at or below it cannot change (see process_tile); false: every dirty cell is solved
+    bool skip_settled;
     // largest value among a tile's solvable cells (+inf while any is unreached); values only
     // decrease, so a stale entry is an upper bound
     unsigned long long *maxval;            // [ntile]
@@ -366,7 +393,8 @@ __device__ __forceinline__ unsigned long long *stat_row(const Dev<Real> &P, int 
 // Pushes the dependents of tile T that read a cell of `mask`, marking as dirty the cells of each
 // dependent that read T; if `self_pending` is non-zero T itself is pushed with those cells dirty.
 // Dirty bits are set before the dedupe flag so that a dependent already queued, or one that has
-// just claimed itself, sees them on its next activation.
+// just claimed itself, sees them on its next activation. The wake-up value `mu` (smallest changed
+// value of T) goes with the dirty bits in one atomic update.
 template <typename Real>
 __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int slot, int T, unsigned long long mask,
                                                 unsigned long long self_pending, unsigned long long mu,
@@ -389,7 +417,7 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
                     want = __longlong_as_double(mu) < mx * (1.0 + 16.0 * DBL_EPSILON);
                 }
                 if (want) {
-                    atomicOr(P.dirty + D, P.dep_dmask[i]);
+                    dirty_add(P.dirty + D, P.dep_dmask[i], mu);
                     atomicMin(P.key + D, kb);
                 }
             }
@@ -398,7 +426,7 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
         }
     }
     if (self_pending && lane == 0) {
-        atomicOr(P.dirty + T, self_pending);
+        dirty_add(P.dirty + T, self_pending, mu);
         atomicMin(P.key + T, kb);
     }
     push_tiles(P, li, T, self_pending != 0ull && lane == 0, lane, inst);
@@ -451,6 +479,14 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 // One activation of tile T: solve the dirty cells, then, sweep after sweep, the cells reading an
 // in-tile cell that changed in the previous sweep, until nothing changes (warp vote) or the sweep
 // budget is spent (T re-queues itself with the cells still pending).
+//
+// A cell is solved only if its value is above the smallest new value among the neighbours that
+// changed since its last solve (the tile's wake-up value for the dirty cells, the smallest value
+// changed in the previous sweep for the others). The Hopf-Lax update uses only the candidates
+// below the cell's current value, which such changes leave in place, so the skipped solve would
+// return the same value bit for bit (fast marching's own rule: a neighbour accepted at or above a
+// cell's tentative value does not update it, HamiltonFastMarching.hxx:151). Not applied to TTI3,
+// whose update is an extremum over a family of such solves.
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves) {
@@ -460,9 +496,15 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
     int t0, t1, t2;
     g.tile_coords(T - I.tile0, t0, t1, t2);
     const int tx0 = t0 << g.tshift[0], tx1 = t1 << g.tshift[1], tx2 = t2 << g.tshift[2];
-    unsigned long long dirty = 0;
-    if (lane == 0) dirty = atomicExch(P.dirty + T, 0ull);
+    unsigned long long dirty = 0, wk = 0ull;
+    if (lane == 0) {
+        const DirtyWake taken = atomicExch(P.dirty + T, DirtyWake{0ull, kInfWake});
+        dirty = taken.mask;
+        wk = taken.wake;
+    }
     dirty = __shfl_sync(0xffffffffu, dirty, 0);
+    double lim = -1.0;  // solve a cell only if its value is above lim
+    if (KIND != kKindTTI && P.skip_settled) lim = __longlong_as_double(__shfl_sync(0xffffffffu, wk, 0));
     __threadfence();
     Real cur[2];
     bool upd[2], todo[2], chg[2] = {false, false};
@@ -484,7 +526,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         cur[j] = (valid && !dead) ? __ldcg(P.values + gi[j]) : INF;
         upd[j] = valid && !dead && !fixed;
         if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, KIND>(P, I, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
-        todo[j] = upd[j] && ((dirty >> l) & 1ull);
+        todo[j] = upd[j] && ((dirty >> l) & 1ull) && (double)cur[j] > lim;
         sv[l] = cur[j];
     }
     __syncwarp();
@@ -532,8 +574,17 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         const unsigned long long C = (unsigned long long)__ballot_sync(0xffffffffu, now[0]) |
                                      ((unsigned long long)__ballot_sync(0xffffffffu, now[1]) << 32);
         if (!C) { converged = true; break; }
+        if (KIND != kKindTTI && P.skip_settled) {  // smallest value changed in this sweep
+            double m = Arith<double>::inf();
 #pragma unroll
-        for (int j = 0; j < 2; ++j) todo[j] = upd[j] && (reads[j] & C) != 0ull;
+            for (int j = 0; j < 2; ++j)
+                if (now[j] && (double)cur[j] < m) m = (double)cur[j];
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+            lim = m;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) todo[j] = upd[j] && (reads[j] & C) != 0ull && (double)cur[j] > lim;
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) ups += __shfl_xor_sync(0xffffffffu, ups, o);
@@ -2297,14 +2348,17 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     P.dep_tile = rtile.get();
     P.dep_mask = rmask.get();
     P.dep_dmask = rdmask.get();
-    DeviceBuffer<unsigned long long> dirty(nt), key(nt), rstat(32), maxval(nt);
+    DeviceBuffer<unsigned long long> key(nt), rstat(32), maxval(nt);
+    DeviceBuffer<DirtyWake> dirty(nt);
     DeviceBuffer<unsigned> tile_up(nt);
     tile_up.zero(s);
     P.tile_up = tile_up.get();
-    dirty.zero(s);
+    launch(fill_kernel<DirtyWake>, nblocks(nt, 256), 256, 0, s, dirty.get(), nt, DirtyWake{0ull, kInfWake});
     P.dirty = dirty.get();
+    P.skip_settled = true;
     launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, key.get(), nt, 0x7ff0000000000000ull);
     launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, maxval.get(), nt, 0x7ff0000000000000ull);
+
     {
         unsigned long long h[32];
         for (int i = 0; i < 8; ++i) { h[4 * i] = 0x7ff0000000000000ull; h[4 * i + 1] = 0; h[4 * i + 2] = 0; h[4 * i + 3] = 0; }

@@ -260,7 +260,8 @@ class Resident final : public ResidentFamily {
     DeviceBuffer<Real> weight_, mult_, values_, cls_w_;
     DeviceBuffer<int8_t> cls_off_;
     DeviceBuffer<int> tile_inst_, lists_, dep_tile_, active_d_;
-    DeviceBuffer<unsigned long long> dirty_, key_, maxval_, dep_mask_, dep_dmask_, rstat_, stats_;
+    DeviceBuffer<unsigned long long> key_, maxval_, dep_mask_, dep_dmask_, rstat_, stats_;
+    DeviceBuffer<DirtyWake> dirty_;
     DeviceBuffer<long long> dep_beg_, dep_end_, round_out_;
     DeviceBuffer<double> delta_;
     DeviceBuffer<Inst> inst_;
@@ -303,6 +304,7 @@ class Resident final : public ResidentFamily {
         P.dep_dmask = dep_dmask_.get();
         P.dirty = dirty_.get();
         P.key = key_.get();
+        P.skip_settled = true;
         P.maxval = maxval_.get();
         P.rstat = rstat_.get();
         P.nslots = kMaxResident;
@@ -486,7 +488,8 @@ public:
             // fresh scheduling words for the range
             launch(fill_kernel<Real>, std::min<unsigned>(nblocks(nt * 64, 256), 4096), 256, 0, s, V.values, nt * 64,
                    Arith<Real>::inf());
-            HFM_CUDA(cudaMemsetAsync(dirty_.get() + tile0, 0, nt * sizeof(unsigned long long), s));
+            launch(fill_kernel<DirtyWake>, nblocks(nt, 256), 256, 0, s, dirty_.get() + tile0, nt,
+                   DirtyWake{0ull, kInfWake});
             HFM_CUDA(cudaMemsetAsync(tile_up_.get() + tile0, 0, nt * sizeof(unsigned), s));
             for (int l = 0; l < 3; ++l)
                 HFM_CUDA(cudaMemsetAsync(flags_.get() + l * cap_t_ + tile0, 0, nt * sizeof(unsigned), s));
@@ -494,6 +497,7 @@ public:
                    0x7ff0000000000000ull);
             launch(fill_kernel<unsigned long long>, nblocks(nt, 256), 256, 0, s, maxval_.get() + tile0, nt,
                    0x7ff0000000000000ull);
+
             // ---- stencils
             unsigned hmaxw = 0;
             DeviceBuffer<uint8_t> cls_en;
