@@ -6,6 +6,7 @@
 //   Voronoi1Vec (relaxed rank-one tensor, tolerances, reorientation)  CommonTraits.h:118-161
 //   StencilReedsShepp2::SetStencil                                      Curvature2.h:48-66
 //   StencilReedsSheppForward2::SetStencil                               Curvature2.h:86-100
+//   StencilDubins2::SetStencil                                          Curvature2.h:113-140
 //   StencilElastica2<5>::SetStencil and its Fejer weights               Curvature2.h:178-234
 #include <cmath>
 
@@ -81,6 +82,29 @@ void reedssheppforward2_table(int ntheta, double h, double xi, double eps, std::
         off[t * 12 + 10] = 0;
         off[t * 12 + 11] = -1;
         w[t * 4 + 3] = 1.0 / (xd * xd);
+    }
+}
+
+// Dubins car: per angle two stencils of 6 forward differences, the first the 3D Voronoi1Vec of
+// (cos/h, sin/h, 1/(xi dtheta)), the second the same differences with the angular component of
+// each offset negated (turning the other way). Layout per angle: 12 forward differences, stencil 0
+// then stencil 1.
+void dubins2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off, std::vector<double> &w) {
+    off.assign((size_t)ntheta * 12 * 3, 0);
+    w.assign((size_t)ntheta * 12, 0.0);
+    const double ds = (2.0 * kPi) / (double)ntheta;
+    for (int t = 0; t < ntheta; ++t) {
+        int8_t *O = &off[(size_t)t * 36];
+        double *W = &w[(size_t)t * 12];
+        const double theta = (double)t * ds;
+        const double v[3] = {std::cos(theta) / h, std::sin(theta) / h, 1. / (xi * ds)};
+        voronoi1vec<3>(v, eps, O, W);
+        for (int i = 0; i < 6; ++i) {
+            W[6 + i] = W[i];
+            O[(6 + i) * 3 + 0] = O[i * 3 + 0];
+            O[(6 + i) * 3 + 1] = O[i * 3 + 1];
+            O[(6 + i) * 3 + 2] = (int8_t)(-O[i * 3 + 2]);
+        }
     }
 }
 

@@ -64,7 +64,9 @@ constexpr unsigned kShFixed = 1u << 30, kShDead = 1u << 31;
 constexpr int kWarpsPerCta = 4;
 // Stencil families of the solver kernels (the KIND template parameter): per-cell Riemann
 // stencils, shared per-angle stencils (curvature models), per-cell TTI Selling paths.
-constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2;
+// kKindShare2: shared stencils of two groups of forward differences whose value is the smaller of
+// the two groups' solutions (Dubins2, nmax = 2).
+constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2, kKindShare2 = 3;
 // Value increases a tile may take before it accepts decreases only (termination guard).
 constexpr unsigned kUpBudget = 128;
 // Tile dependency tables: a small hash table per warp first (fast, high occupancy), the large one
@@ -244,6 +246,58 @@ __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real 
     return taken ? quad_root<Real>(minVal, a, b, c) : INF;
 }
 
+// Hopf-Lax update of two groups of forward differences (EulerianStencil<.,0,6,2>, Dubins2):
+// neighbours are taken in increasing order of value, each one only while below the current value,
+// and added to every difference whose offset reaches it (EulerianStencil.hxx:104-153); the
+// differences k < ND/2 accumulate in group 0, the others in group 1, from one shared minVal; the
+// value is minVal plus the smaller group root, group 0 on ties (QuadraticMax<.,2>::Solve,
+// EulerianStencil.hxx:30-50). `used` receives the added differences and, in bit ND, the group.
+template <typename Real, int ND>
+__device__ __forceinline__ Real hopf_lax_two_groups(const Real (&v)[ND], const Real (&w)[ND], const unsigned (&oc)[ND],
+                                                    unsigned *used) {
+    using A = Arith<Real>;
+    const Real INF = A::inf();
+    Real minVal = 0, a0 = 0, b0 = 0, c0 = -1, a1 = 0, b1 = 0, c1 = -1;
+    Real value = INF;
+    int imin = 0;
+    unsigned taken = 0;
+    for (int it = 0; it < ND; ++it) {
+        Real bv = INF;
+        int bk = -1;
+#pragma unroll
+        for (int k = 0; k < ND; ++k)
+            if (!((taken >> k) & 1u) && v[k] < bv) { bv = v[k]; bk = k; }
+        if (bk < 0) break;
+        if (it == 0) minVal = bv;
+        else if (!(bv < value)) break;  // ConditionalUpdate: values[x] <= acceptedValue
+        const unsigned ob = oc[bk];
+        const Real dv = A::sub(bv, minVal);
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+            if (((taken >> k) & 1u) || oc[k] != ob || !(v[k] < INF)) continue;
+            taken |= 1u << k;
+            const Real wv = A::mul(w[k], dv);
+            const Real wv2 = A::mul(wv, dv);
+            if (k < ND / 2) { a0 = A::add(a0, w[k]); b0 = A::add(b0, wv); c0 = A::add(c0, wv2); }
+            else { a1 = A::add(a1, w[k]); b1 = A::add(b1, wv); c1 = A::add(c1, wv2); }
+        }
+        Real res = INF;
+        imin = 0;
+        if (a0 != Real(0)) {
+            const Real d2 = A::sub(A::mul(b0, b0), A::mul(a0, c0));
+            res = A::div(A::add(b0, A::sqrt(Real(0) < d2 ? d2 : Real(0))), a0);
+        }
+        if (a1 != Real(0)) {
+            const Real d2 = A::sub(A::mul(b1, b1), A::mul(a1, c1));
+            const Real r1 = A::div(A::add(b1, A::sqrt(Real(0) < d2 ? d2 : Real(0))), a1);
+            if (r1 < res) { res = r1; imin = 1; }
+        }
+        value = A::add(minVal, res);
+    }
+    if (used) *used = taken | ((unsigned)imin << ND);
+    return taken ? value : INF;
+}
+
 // Local solve at one cell. `sv` holds the current values of the warp's tile (nullptr: read all
 // neighbours from global memory). `side` receives, per symmetric difference, 1 if the -e
 // neighbour provided the candidate.
@@ -251,7 +305,7 @@ template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1,
                                                    int x2, int tx0, int tx1, int tx2, const Real *sv, unsigned *used,
                                                    unsigned *side) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     using A = Arith<Real>;
     const Real INF = A::inf();
@@ -259,6 +313,7 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
     const Real *values = P.values + I.cell0;
     const long long cls = I.cls0 + x2;
     Real v[ND], w[ND];
+    [[maybe_unused]] unsigned oc[ND];  // packed offsets (two-group stencils: shared neighbours)
     Real m2 = 1;
     unsigned visw = 0;
     if (SHARE) {
@@ -288,6 +343,7 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
         if (SHARE) {
             const int8_t *o = P.cls_off + (cls * ND + k) * 3;
             o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
+            if constexpr (KIND == kKindShare2) oc[k] = pack_off(o0, o1, o2);
             w[k] = A::mul(__ldg(P.cls_w + cls * ND + k), m2);
             if (k < NFWD) {
                 vp = (visw >> k) & 1u;
@@ -312,7 +368,8 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
         v[k] = val;
     }
     if (side) *side = sides;
-    return hopf_lax_sorted<Real, ND>(v, w, used);
+    if constexpr (KIND == kKindShare2) return hopf_lax_two_groups<Real, ND>(v, w, oc, used);
+    else return hopf_lax_sorted<Real, ND>(v, w, used);
 }
 
 // TTI local solve at one cell (FP64): neighbour values from the tile in shared memory or global
@@ -352,7 +409,7 @@ __device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, lo
 
 template <typename Real, int KIND>
 __device__ __forceinline__ void cell_flags(const Dev<Real> &P, long long c, bool &fixed, bool &dead) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     if (SHARE) {
         const unsigned f = P.vis[c];
         fixed = f & kShFixed;
@@ -441,7 +498,7 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, const Inst &I, long long c, int x0,
                                                            int x1, int x2, int tx0, int tx1, int tx2) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     const GridGeom &g = I.g;
     unsigned long long m = 0;
@@ -490,7 +547,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
     int t0, t1, t2;
@@ -630,13 +687,13 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 // Elastica stencil whose local solve needs the registers).
 template <typename Real, int NFWD, int NSYM, int KIND>
 constexpr int fim_min_blocks() {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     return KIND == kKindTTI ? 1 : SHARE ? (NFWD + NSYM > 8 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 8;
 }
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD, NSYM, KIND>())) fim_kernel(Dev<Real> P) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long kInfBits = 0x7ff0000000000000ull;
@@ -1019,7 +1076,7 @@ __device__ bool wall_visible(const GridGeom &g, const int8_t *wd, int b0, int b1
 // (ConditionalUpdate, HamiltonFastMarching.hxx:136-154). Also marks padding cells dead.
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8_t *cls_enabled) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= P.ntc) return;
@@ -1070,7 +1127,7 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
 
 template <typename Real, int KIND>
 __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *val, int n) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     // idx: global cell indices
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1089,7 +1146,7 @@ template <typename Real, int NFWD, int NSYM, int KIND, int kDepCap, int kDepWarp
 __global__ void __launch_bounds__(kDepWarps * 32)
     deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
                 unsigned long long *msk, unsigned long long *dmsk) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     __shared__ int keys[kDepWarps][kDepCap];
     __shared__ unsigned long long masks[kDepWarps][kDepCap];
@@ -1233,7 +1290,7 @@ __global__ void count_finite_kernel(Dev<Real> P, unsigned long long *out) {
 // update adds every difference matching the accepted offset (EulerianStencil.hxx:114-123).
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= P.ncells) return;
@@ -1281,6 +1338,8 @@ __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
                 bits |= 1ull << (NFWD + 2 * (k - NFWD) + ((side >> (k - NFWD)) & 1u));
             }
         }
+        // the group of a two-group stencil, in the bit after the differences (SetIMax)
+        if constexpr (KIND == kKindShare2) bits |= (unsigned long long)((used >> ND) & 1u) << ND;
     }
     active[x] = bits;
 }
@@ -1335,7 +1394,7 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     // the adjoint runs on a batch of one instance
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
@@ -1470,6 +1529,9 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
         } else if ((used >> k) & 1u) {
             act = ((side >> (k - NFWD)) & 1u) ? 2u : 1u;
         }
+        // a two-group stencil recomputes with the named group only (HopfLaxRecompute,
+        // EulerianStencil.hxx:157-200)
+        if (KIND == kKindShare2 && (k < ND / 2 ? 0u : 1u) != ((used >> ND) & 1u)) act = 0;
         for (int si = 0; si < 2; ++si) {
             if (!((act >> si) & 1u)) continue;
             const int s = si ? -1 : 1;
@@ -1991,7 +2053,7 @@ struct Retained final : RetainedSolve {
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     constexpr int NB = NFWD + 2 * NSYM;
     const auto wall_t0 = std::chrono::steady_clock::now();
@@ -2567,7 +2629,7 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
     const EulerProblem &p = *probs[0];
     for (const EulerProblem *q : probs) {
         if (q->kind != p.kind || q->ndim != p.ndim || q->nfwd != p.nfwd || q->nsym != p.nsym || q->fp64 != p.fp64 ||
-            q->diagonal != p.diagonal)
+            q->diagonal != p.diagonal || q->nmax != p.nmax)
             throw Error(HFM_ERR_VALUE, "a batch must hold instances of one model family and one precision");
     }
     if (p.kind == StencilKind::TTI) {
@@ -2610,6 +2672,9 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
         } else if (p.nfwd == 27 && p.nsym == 0) {
             if (p.fp64) run_batch_impl<double, 27, 0, detail::kKindShare>(probs, results);
             else run_batch_impl<float, 27, 0, detail::kKindShare>(probs, results);
+        } else if (p.nfwd == 12 && p.nsym == 0 && p.nmax == 2) {
+            if (p.fp64) run_batch_impl<double, 12, 0, detail::kKindShare2>(probs, results);
+            else run_batch_impl<float, 12, 0, detail::kKindShare2>(probs, results);
         } else {
             throw Error(HFM_ERR_UNSUPPORTED, "unsupported shared stencil shape");
         }

@@ -86,7 +86,7 @@ __device__ __forceinline__ bool geo_packable(const int *ind) {
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1, int x2, unsigned *foff, double *fw,
                               double *value, double *width) {
-    [[maybe_unused]] constexpr bool SHARE = KIND == kKindShare;
+    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
     const GridGeom &g = I.g;
@@ -192,6 +192,8 @@ __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1,
             } else if ((used >> k) & 1u) {
                 act = ((side >> (k - NFWD)) & 1u) ? 2u : 1u;
             }
+            // a two-group stencil recomputes with the named group only
+            if (KIND == kKindShare2 && (k < ND / 2 ? 0u : 1u) != ((used >> ND) & 1u)) act = 0;
             for (int si = 0; si < 2; ++si) {
                 if (!((act >> si) & 1u) || n >= kGeoMaxFlow) continue;
                 const int s = si ? -1 : 1;
@@ -861,7 +863,7 @@ template <int NFWD, int NSYM, int KIND>
 constexpr bool geo_dim_ok(int d) {
     if (KIND == kKindRiemann && NFWD == 0 && NSYM == 2) return d == 2;
     if (KIND == kKindRiemann && NFWD == 0 && NSYM == 3) return true;
-    if (KIND == kKindShare && NFWD == 0 && NSYM == 2) return d == 2;
+    if ((KIND == kKindShare || KIND == kKindShare2) && NFWD == 0 && NSYM == 2) return d == 2;
     return d == 3;
 }
 

@@ -791,6 +791,11 @@ void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProble
         p.nfwd = 3;
         p.nsym = 1;
         reedssheppforward2_table(dims[2], h, xi, eps, p.cls_off, p.cls_w);
+    } else if (model == "Dubins2") {
+        p.nfwd = 12;
+        p.nsym = 0;
+        p.nmax = 2;
+        dubins2_table(dims[2], h, xi, eps, p.cls_off, p.cls_w);
     } else {
         p.nfwd = 27;
         p.nsym = 0;
@@ -1116,7 +1121,8 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     io.set_ordering(o);
     reject_unsupported(io);
 
-    const bool lifted = model == "ReedsShepp2" || model == "ReedsSheppForward2" || model == "Elastica2";
+    const bool lifted = model == "ReedsShepp2" || model == "ReedsSheppForward2" || model == "Elastica2" ||
+                        model == "Dubins2";
     if (model == "Riemann2") setup_riemann(io, 2, pm, p);
     else if (model == "Riemann3") setup_riemann(io, 3, pm, p);
     else if (model == "Isotropic2") setup_isotropic(io, 2, pm, p);

@@ -46,6 +46,7 @@ struct EulerProblem {
     // repeat one axis-aligned stencil on every index of the last axis).
     bool angular = true;
     int nfwd = 0, nsym = 0, nclass = 0;
+    int nmax = 1;                      // 2: two groups of nfwd/2 forward differences (Dubins2)
     std::vector<int8_t> cls_off;       // [nclass][nfwd+nsym][3]
     std::vector<double> cls_w;         // [nclass][nfwd+nsym]
     std::vector<uint8_t> cls_enabled;  // [nclass][nfwd+2*nsym] slot reachable from the class centre
@@ -211,5 +212,6 @@ void elastica2_table(int ntheta, double h, double xi, double eps, std::vector<in
                      std::vector<double> &w);
 void reedssheppforward2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,
                               std::vector<double> &w);
+void dubins2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off, std::vector<double> &w);
 
 }  // namespace hfm

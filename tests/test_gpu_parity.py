@@ -64,7 +64,7 @@ def stencil_offsets_per_cell(params):
         return 0, out["stencilOffsets"].reshape(-1, nk, len(dims)).astype(np.int64)
     off, _ = O.curvature2_table(model, dims[2], float(params["gridScale"]), float(params.get("xi", 1.0)),
                                 float(params.get("eps", 0.1)), bool(params.get("projective", 0.0)))
-    nfwd = {"ReedsShepp2": 0, "ReedsSheppForward2": 3, "Elastica2": 27}[model]
+    nfwd = {"ReedsShepp2": 0, "ReedsSheppForward2": 3, "Elastica2": 27, "Dubins2": 12}[model]
     theta = np.arange(int(np.prod(dims))) % dims[2]
     return nfwd, off[theta].astype(np.int64)
 
@@ -76,7 +76,8 @@ def untied_active_differences(params, values, act_ref, act):
         return []
     nfwd, offs = stencil_offsets_per_cell(params)
     dims = values.shape
-    periodic = [False] * (len(dims) - 1) + [params["model"] in ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")]
+    periodic = [False] * (len(dims) - 1) + [params["model"] in ("ReedsShepp2", "ReedsSheppForward2", "Elastica2",
+                                                                 "Dubins2")]
     v = values.ravel()
 
     def value_at(x, e):
@@ -93,8 +94,9 @@ def untied_active_differences(params, values, act_ref, act):
     for x in bad:
         r, o = int(act_ref.ravel()[x]), int(act.ravel()[x])
         fmask = (1 << nfwd) - 1
-        ok = (r & fmask) == (o & fmask)
-        for j in range(offs.shape[1] - nfwd):
+        nsym = offs.shape[1] - nfwd
+        ok = (r & fmask) == (o & fmask) and (r >> (nfwd + 2 * nsym)) == (o >> (nfwd + 2 * nsym))
+        for j in range(nsym):
             rb, ob = (r >> (nfwd + 2 * j)) & 3, (o >> (nfwd + 2 * j)) & 3
             if rb == ob:
                 continue
