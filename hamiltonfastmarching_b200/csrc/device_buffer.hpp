@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -22,6 +23,10 @@ cudaStream_t &current_stream();
 // serving lane leaves the rest of the SMs to the lanes that run beside it).
 int &solver_share();
 void keep_pool_cached();
+// Held from the launch of a cooperative (grid-synchronising) kernel until it completes: two such
+// kernels in flight from different threads could each hold part of the SMs while waiting at a grid
+// barrier for blocks that the other keeps from becoming resident.
+std::mutex &cooperative_mutex();
 // Kernel launches issued by this library (all threads), for launch accounting.
 void count_launch(unsigned n = 1);
 

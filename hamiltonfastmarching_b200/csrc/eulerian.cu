@@ -1832,10 +1832,13 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
         launch(adjoint_roots_kernel, nblocks(N, 256), 256, 0, s, A);
         void *args[] = {&A};
         count_launch();
+        {
+            std::lock_guard<std::mutex> coop(cooperative_mutex());
             HFM_CUDA(cudaLaunchCooperativeKernel((void *)adjoint_kernel,
                                                  dim3(std::max(1, nsm * per_sm / std::max(1, solver_share()))),
                                                  dim3(256), args, 0, s));
-        check_status(status, "adjoint");
+            check_status(status, "adjoint");
+        }
         AdjointResult ar;
         ar.sensitivity.resize((size_t)N * vdim);
         sens.download(ar.sensitivity.data(), (size_t)N * vdim, s);
@@ -2011,10 +2014,13 @@ void run_forward(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     launch(forward_roots_kernel, nblocks(N, 256), 256, 0, s, F);
     void *args[] = {&F};
     count_launch();
-    HFM_CUDA(cudaLaunchCooperativeKernel((void *)forward_kernel,
-                                         dim3(std::max(1, nsm * per_sm / std::max(1, solver_share()))), dim3(256),
-                                         args, 0, s));
-    check_status(status, "forward variation");
+    {
+        std::lock_guard<std::mutex> coop(cooperative_mutex());
+        HFM_CUDA(cudaLaunchCooperativeKernel((void *)forward_kernel,
+                                             dim3(std::max(1, nsm * per_sm / std::max(1, solver_share()))), dim3(256),
+                                             args, 0, s));
+        check_status(status, "forward variation");
+    }
     res.value_variation.resize((size_t)N * nvar);
     out.download(res.value_variation.data(), (size_t)N * nvar, s);
     HFM_CUDA(cudaStreamSynchronize(s));
@@ -2462,6 +2468,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_CUDA(cudaStreamSynchronize(s));
     }
     tm.start(s);
+    std::unique_lock<std::mutex> coop(cooperative_mutex(), std::defer_lock);
     if (!st.empty() && !bypass) {
         stile.upload(st, s);
         smask.upload(sm, s);
@@ -2481,10 +2488,12 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         P.order_hi = ordered ? (unsigned)std::max(2.0, p0.band_hi * nwarps) : 0u;
         void *args[] = {&P};
         count_launch();
+        coop.lock();
         HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_kernel<Real, NFWD, NSYM, KIND>, dim3(grid),
                                              dim3(kWarpsPerCta * 32), args, 0, s));
     }
     const float t_solve = tm.stop(s);
+    if (coop.owns_lock()) coop.unlock();
     check_status(status, "solver");
     unsigned long long hs[4] = {0, 0, 0, 0};
     stats.download(hs, 4, s);

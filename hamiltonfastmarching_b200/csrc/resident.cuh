@@ -752,13 +752,16 @@ public:
         C.max_rounds = sched_.max_rounds;
         void *args[] = {&P, &C};
         count_launch();
-        HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_resident_kernel<Real, NFWD, NSYM, KIND>, dim3(grid),
-                                             dim3(kWarpsPerCta * 32), args, 0, s));
         long long rout = round_;
         unsigned st = 0;
-        HFM_CUDA(cudaMemcpyAsync(&rout, round_out_.get(), sizeof(long long), cudaMemcpyDeviceToHost, s));
-        HFM_CUDA(cudaMemcpyAsync(&st, ctl_.get() + 8, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        HFM_CUDA(cudaStreamSynchronize(s));
+        {
+            std::lock_guard<std::mutex> coop(cooperative_mutex());
+            HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_resident_kernel<Real, NFWD, NSYM, KIND>, dim3(grid),
+                                                 dim3(kWarpsPerCta * 32), args, 0, s));
+            HFM_CUDA(cudaMemcpyAsync(&rout, round_out_.get(), sizeof(long long), cudaMemcpyDeviceToHost, s));
+            HFM_CUDA(cudaMemcpyAsync(&st, ctl_.get() + 8, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            HFM_CUDA(cudaStreamSynchronize(s));
+        }
         if (st & (kErrBarrierTimeout | kErrRoundCap)) {
             broken_ = true;
             throw Error(HFM_ERR_NOT_CONVERGED, st & kErrBarrierTimeout ? "resident solver: a grid barrier wait exceeded its limit"

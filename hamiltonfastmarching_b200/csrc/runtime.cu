@@ -23,6 +23,11 @@ int &solver_share() {
     return share;
 }
 
+std::mutex &cooperative_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+
 void keep_pool_cached() {
     // Once per device: keep freed blocks of the default pool cached instead of returning them at
     // every synchronisation, so repeated solves do not pay for new device mappings.
