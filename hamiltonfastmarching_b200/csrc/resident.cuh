@@ -119,9 +119,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
         ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
         if (!ok) break;
         if (*(volatile unsigned *)P.count[nxt] == 0u) { ++r; break; }  // every instance converged
+        // per-instance band update, identical in every block; each slot is one thread's
         bool finished = false;
-        if (threadIdx.x == 0) {
-            for (int a = 0; a < C.nactive; ++a) {
+        {
+            for (int a = threadIdx.x; a < C.nactive; a += blockDim.x) {
                 const int i = C.active[a];
                 if (*(volatile unsigned *)(P.live + nxt * P.nslots + i) == 0u) { finished = true; continue; }
                 const unsigned long long *row = P.rstat + ((long long)slot * P.nslots + i) * 4;
