@@ -170,6 +170,13 @@ struct Dev {
     // instance's front on a common scale (nullptr: keys are the values)
     const double *kscale;
     const TTICell *tti;                    // [ntc] TTI norms (TTI kind)
+    // static factoring of a single TTI instance (null: none): factor values, adimensional
+    // gradients and mask over the box [fac_lo, fac_lo + fac_dims) of cells
+    const double *fac_val;
+    const double *fac_grad;
+    const uint8_t *fac_mask;
+    int fac_lo[3], fac_dims[3];
+    int fac_sub;                           // the box is a subdomain (corrections vanish outside it)
     unsigned *tile_up;                     // [ntile] value increases taken by each tile
     // Diagonal models (a single instance): the speed (or cost) vector per cell, for the first
     // variations, which have one component per axis (var_dim = ndim; 1 elsewhere)
@@ -372,6 +379,69 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
     else return hopf_lax_sorted<Real, ND>(v, w, used);
 }
 
+// TTI local solve of a cell of the factoring box (StaticFactoring.hxx:33-64 with TTI.hpp:160-276).
+// A neighbour y = x + e enters with u(y) + <grad(x), e> + value(x) - value(y) (order-1 Correction;
+// the last two terms 0 when y leaves a subdomain box). Fast marching re-solves x from its accepted
+// neighbours each time one of them is accepted below x's current value, and keeps the smallest
+// result; with the corrections the neighbours above that value can change a solve, so that order
+// is reproduced: the neighbours the update can read, in increasing value, each one triggering a
+// solve over the neighbours at or below its value while it is below the smallest result so far.
+template <typename Real, typename Get>
+__device__ double solve_cell_tti_factored(const Dev<Real> &P, long long c, const int (&b)[3], long long bi, Get raw,
+                                          double *t_act, bool *interior) {
+    using A = Arith<double>;
+    const double INF = A::inf();
+    const double fx = P.fac_val[bi];
+    const double *gx = P.fac_grad + 3 * bi;
+    auto corr = [&](int o0, int o1, int o2) -> double {
+        const int e0 = b[0] + o0, e1 = b[1] + o1, e2 = b[2] + o2;
+        if ((unsigned)e0 >= (unsigned)P.fac_dims[0] || (unsigned)e1 >= (unsigned)P.fac_dims[1] ||
+            (unsigned)e2 >= (unsigned)P.fac_dims[2])
+            return 0.0;  // out of a subdomain box; a whole-domain box holds every neighbour read
+        const long long ei = ((long long)e0 * P.fac_dims[1] + e1) * P.fac_dims[2] + e2;
+        double deriv = 0.0;
+        deriv = A::add(deriv, A::mul(gx[0], (double)o0));
+        deriv = A::add(deriv, A::mul(gx[1], (double)o1));
+        deriv = A::add(deriv, A::mul(gx[2], (double)o2));
+        return A::add(deriv, A::sub(fx, P.fac_val[ei]));
+    };
+    // the values of the neighbours the update can read (the cell's Selling-path offsets, both signs)
+    constexpr int kMax = 2 * kTTISlots;
+    double th[kMax];
+    int nth = 0;
+    for (int k = 0; k < kTTISlots; ++k) {
+        if (P.weight[k * P.sstride + c] == Real(0)) continue;
+        const unsigned cd = P.code[k * P.sstride + c];
+        const int o0 = off_c(cd, 0), o1 = off_c(cd, 1), o2 = off_c(cd, 2);
+        for (int sg = 1; sg >= -1; sg -= 2) {
+            const double v = raw(sg * o0, sg * o1, sg * o2);
+            if (!(v < INF)) continue;
+            int q = nth++;
+            while (q > 0 && th[q - 1] > v) { th[q] = th[q - 1]; --q; }
+            th[q] = v;
+        }
+    }
+    double best = INF, tb = INF;
+    bool ib = false;
+    for (int q = 0; q < nth; ++q) {
+        const double theta = th[q];
+        if (q > 0 && theta == th[q - 1]) continue;
+        if (!(theta < best)) break;  // ConditionalUpdate: values[x] <= acceptedValue
+        auto get = [&](int o0, int o1, int o2) -> double {
+            const double v = raw(o0, o1, o2);
+            if (!(v <= theta)) return INF;
+            return A::add(v, corr(o0, o1, o2));
+        };
+        double ta = INF;
+        bool in = false;
+        const double sv = tti_solve(P.tti[c], get, &ta, &in);
+        if (sv < best) { best = sv; tb = ta; ib = in; }
+    }
+    if (t_act) *t_act = tb;
+    if (interior) *interior = ib;
+    return best;
+}
+
 // TTI local solve at one cell (FP64): neighbour values from the tile in shared memory or global
 // memory, +inf outside the domain.
 template <typename Real>
@@ -392,6 +462,14 @@ __device__ __forceinline__ Real solve_cell_tti(const Dev<Real> &P, const Inst &I
         }
         return (double)__ldcg(values + g.lin(n0, n1, n2));
     };
+    if (P.fac_val) {
+        const int b[3] = {x0 - P.fac_lo[0], x1 - P.fac_lo[1], x2 - P.fac_lo[2]};
+        if ((unsigned)b[0] < (unsigned)P.fac_dims[0] && (unsigned)b[1] < (unsigned)P.fac_dims[1] &&
+            (unsigned)b[2] < (unsigned)P.fac_dims[2]) {
+            const long long bi = ((long long)b[0] * P.fac_dims[1] + b[1]) * P.fac_dims[2] + b[2];
+            if (P.fac_mask[bi]) return (Real)solve_cell_tti_factored<Real>(P, c, b, bi, get, t_act, interior);
+        }
+    }
     return (Real)tti_solve(P.tti[c], get, t_act, interior);
 }
 
@@ -582,10 +660,12 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         gi[j] = valid ? I.cell0 + g.lin(xs[j][0], xs[j][1], xs[j][2]) : 0;
         cur[j] = (valid && !dead) ? __ldcg(P.values + gi[j]) : INF;
         upd[j] = valid && !dead && !fixed;
-        if (upd[j]) reads[j] = intile_reads<Real, NFWD, NSYM, KIND>(P, I, c, xs[j][0], xs[j][1], xs[j][2], tx0, tx1, tx2);
         todo[j] = upd[j] && ((dirty >> l) & 1ull) && (double)cur[j] > lim;
         sv[l] = cur[j];
     }
+    // nothing to solve (every dirty cell settled): the values and the tile's largest value stand
+    if (!__any_sync(0xffffffffu, todo[0] || todo[1])) return;
+    bool have_reads = false;  // in-tile read masks, built once a sweep has changed a cell
     __syncwarp();
     bool converged = false;
     unsigned ups = 0;  // increases taken by this lane in this activation
@@ -631,6 +711,14 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         const unsigned long long C = (unsigned long long)__ballot_sync(0xffffffffu, now[0]) |
                                      ((unsigned long long)__ballot_sync(0xffffffffu, now[1]) << 32);
         if (!C) { converged = true; break; }
+        if (!have_reads) {
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if (upd[j])
+                    reads[j] = intile_reads<Real, NFWD, NSYM, KIND>(P, I, (long long)T * 64 + lane + 32 * j, xs[j][0],
+                                                                    xs[j][1], xs[j][2], tx0, tx1, tx2);
+            have_reads = true;
+        }
         if (KIND != kKindTTI && P.skip_settled) {  // smallest value changed in this sweep
             double m = Arith<double>::inf();
 #pragma unroll
@@ -2137,6 +2225,8 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     DeviceBuffer<uint8_t> cls_en;
     DeviceBuffer<double> metric, plain_w, mult_rm, kscale;
     DeviceBuffer<TTICell> ttibuf;
+    DeviceBuffer<double> fac_val, fac_grad;
+    DeviceBuffer<uint8_t> fac_mask;
     std::vector<double> hscale;
     maxw.zero(s);
     std::vector<unsigned> hmaxw(ninst, 0);
@@ -2174,6 +2264,20 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
             ttibuf.alloc(ntc);
             ttibuf.zero(s);
             P.tti = ttibuf.get();
+            if (p0.has_factoring()) {  // the static factor of a single instance
+                if (ninst > 1) throw Error(HFM_ERR_UNSUPPORTED, "static factoring runs on single solves");
+                fac_val.upload(p0.fac_values, s);
+                fac_grad.upload(p0.fac_grads, s);
+                fac_mask.upload(p0.fac_mask, s);
+                P.fac_val = fac_val.get();
+                P.fac_grad = fac_grad.get();
+                P.fac_mask = fac_mask.get();
+                for (int a = 0; a < 3; ++a) {
+                    P.fac_lo[a] = p0.fac_lo[a];
+                    P.fac_dims[a] = p0.fac_dims[a];
+                }
+                P.fac_sub = p0.fac_subdomain ? 1 : 0;
+            }
             launch(tti_setup_kernel<NSYM, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr);
         } else if (p0.diagonal) {
             launch(diagonal_stencil_kernel<Real>, nblocks(N, 128), 128, 0, s, P, p0.ndim, metric_ptr, plain_off.get(),

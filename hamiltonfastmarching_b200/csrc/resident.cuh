@@ -14,8 +14,8 @@
 // Scheduling: the batch solver's value-ordered bands, kept per instance. Round r solves, for each
 // instance i, the active tiles whose key is at most (smallest key of i) + delta_i; delta_i starts
 // from the spread of i's first wake-up keys and doubles (halves) when i solved fewer (more) tiles
-// than its share [lo, hi] of the resident warps in the round before, so a small instance runs as
-// it would alone (all its tiles each round) while a large one keeps its own band. Per instance,
+// than [lo, hi] x the resident warps in the round before, as it would alone: a small instance takes
+// all its tiles each round while a large one keeps its own band. Per instance,
 // the statistics rows (smallest and largest wake-up key, tiles solved) and the count of its tiles
 // in each list are kept by the list pushes; an instance whose count in the next list is zero has
 // converged. A slice ends when an instance converges (so it is released at once), when no tile is
@@ -36,7 +36,7 @@ struct ServeCtl {
     const volatile unsigned *attn; // host-mapped attention word (requests waiting), or null
     unsigned long long min_ns;     // attention is honoured once the slice has run this long
     unsigned long long max_ns;     // hard slice length (0: none)
-    unsigned lo, hi;               // per-instance share of solved tiles per round
+    unsigned lo, hi;               // solved tiles per round and instance kept in [lo, hi]
     long long max_rounds;          // round cap of the slice
 };
 
@@ -736,7 +736,9 @@ public:
                                                                kWarpsPerCta * 32, 0));
         if (per_sm < 1) throw Error(HFM_ERR_CUDA, "resident solver kernel cannot be resident");
         const int grid = nsm * per_sm;
-        const double nwarps = (double)grid * kWarpsPerCta / (double)act.size();
+        // each instance keeps the band it would have alone: the tiles of a round are the union of
+        // the instances' bands, so a large instance is not slowed by the small ones beside it
+        const double nwarps = (double)grid * kWarpsPerCta;
         ServeCtl C{};
         C.round0 = round_;
         C.active = active_d_.get();

@@ -84,14 +84,11 @@ std::vector<double> read_point(Store &io, const std::string &key, int n, const s
 }
 
 void reject_unsupported(Store &io) {
-    static const char *keys[] = {"factoringValues", "speed_times", "cost_times",
-                                 "metric_times", "dualMetric_times",
-                                 "euclideanScale", "seedFlags", "factoringPointChoice"};
+    static const char *keys[] = {"speed_times", "cost_times", "metric_times", "dualMetric_times",
+                                 "euclideanScale", "seedFlags"};
     for (const char *k : keys)
         if (io.has_field(k))
             throw Error(HFM_ERR_UNSUPPORTED, std::string("option '") + k + "' is not supported by the GPU solve path");
-    if (io.has_field("factoringRadius") && io.get_scalar("factoringRadius") != 0)
-        throw Error(HFM_ERR_UNSUPPORTED, "option 'factoringRadius' (static factoring) is not supported by the GPU solve path");
     if (io.has_field("order") && io.get_scalar("order") != 1)
         throw Error(HFM_ERR_UNSUPPORTED, "only order=1 is supported by the GPU solve path");
     if (io.get_scalar("exportActiveOffsets", 0.0, 3) != 0)
@@ -195,6 +192,14 @@ struct SeedGuess {
     // divisions of vectors and matrices multiply by the reciprocal, as in the reference's algebra.
     static double tti_norm(const double *m, const double *v) {
         if (v[0] == 0. && v[1] == 0. && v[2] == 0.) return 0.;
+        double g[3];
+        tti_gradient(m, v, g);
+        double norm = 0.;
+        for (int i = 0; i < 3; ++i) norm += g[i] * v[i];
+        return norm;
+    }
+    // TTINorm::Gradient (TTINorm.hxx:268-329) at a non-zero vector v.
+    static void tti_gradient(const double *m, const double *v, double *grad) {
         const double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4];
         auto A = [&](int i, int j) { return m[5 + 3 * i + j]; };  // the guess reads the transform row by row
         double q1[3];
@@ -233,13 +238,11 @@ struct SeedGuess {
         }
         const double n01 = q[0];
         const double w[3] = {n01 == 0. ? 0. : pp[0] * q1[0] / n01, n01 == 0. ? 0. : pp[0] * q1[1] / n01, pp[1]};
-        double norm = 0.;
         for (int i = 0; i < 3; ++i) {
             double gi = 0.;
             for (int j = 0; j < 3; ++j) gi += A(j, i) * w[j];
-            norm += gi * v[i];
+            grad[i] = gi;
         }
-        return norm;
     }
     bool cell_of(const int64_t *idx, int64_t *lin) const {
         int64_t r = 0;
@@ -361,7 +364,7 @@ std::vector<std::array<int, 3>> reversed_offsets(const EulerProblem &p, const Pa
 // Seeds: points -> unique indices (first value kept), sorted; with seedRadius > 0 each seed is
 // spread to the cells whose centre lies within that many cells of it (StaticFactoring.hxx:242-346).
 
-void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_allowed) {
+void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_allowed, double default_radius) {
     std::map<int64_t, double> seeds;
     std::vector<double> pts;
     int64_t n = 0;
@@ -374,7 +377,7 @@ void read_seeds(Store &io, const Param &pm, EulerProblem &p, bool unoriented_all
             if (nv != n) throw Error(HFM_ERR_VALUE, "Error : Inconsistent size of seedValues.");
         }
         // seedRadius < 0: spread to |seedRadius|, then one step of the reversed stencils
-        const double radius_in = io.get_scalar("seedRadius", 0.0);
+        const double radius_in = io.get_scalar("seedRadius", default_radius);
         const bool stencil_step = radius_in < 0;
         const double radius = std::abs(radius_in);
         const bool shared_axes = p.diagonal || (p.kind == StencilKind::SharedByTheta && !p.angular);
@@ -981,6 +984,125 @@ void read_stopping(Store &io, const Param &pm, bool lifted, EulerProblem &p) {
     }
 }
 
+// Static factoring keys (StaticFactoring.hxx:66-84): imported (factoringValues) or computed
+// (factoringRadius != 0); either one makes seedRadius default to 2 (:270), the radius key alone too.
+struct FactorKeys {
+    bool import = false, compute = false, radius_key = false;
+};
+
+FactorKeys read_factor_keys(Store &io, const std::string &model) {
+    FactorKeys k;
+    k.import = io.has_field("factoringValues");
+    k.radius_key = io.has_field("factoringRadius");
+    k.compute = k.radius_key && io.get_scalar("factoringRadius") != 0;
+    if (k.import && k.compute)
+        throw Error(HFM_ERR_VALUE, "StaticFactoring error : factoringValues (import) and factoringRadius (compute) both specified.");
+    if ((k.import || k.compute) && model != "TTI3")
+        throw Error(HFM_ERR_UNSUPPORTED, "static factoring is supported for TTI3 only by the GPU solve path (the Eulerian "
+                                         "models apply it through an acceptance-time recompute)");
+    return k;
+}
+
+// ImportFactor (StaticFactoring.hxx:86-117): values, gradients (a co-vector: adimensionized by
+// multiplying by the grid scales), an optional mask and an optional index shift (a subdomain box).
+void import_factor(Store &io, const Param &pm, EulerProblem &p) {
+    const Field fv = io.get_field("factoringValues", pm.ndim, 1);
+    if (!io.has_field("factoringGradients"))
+        throw Error(HFM_ERR_VALUE, "StaticFactoring error : factoringGradients are not provided");
+    const Field fg = io.get_field("factoringGradients", pm.ndim, pm.ndim);
+    Field fm;
+    const bool has_mask = io.has_field("factoringMask");
+    if (has_mask) fm = io.get_field("factoringMask", pm.ndim, 1);
+    p.fac_subdomain = io.has_field("factoringIndexShift");
+    if (p.fac_subdomain) {
+        const std::vector<double> sh = read_point(io, "factoringIndexShift", pm.ndim, std::vector<double>(pm.ndim, 0.0));
+        for (int a = 0; a < pm.ndim; ++a) p.fac_lo[a] = (int)sh[a];
+    }
+    size_t n = 1;
+    for (int a = 0; a < pm.ndim; ++a) {
+        const int64_t want = p.fac_subdomain ? fv.dims[a] : pm.dims[a];
+        if (fv.dims[a] != want || fg.dims[a] != want || (has_mask && fm.dims[a] != want))
+            throw Error(HFM_ERR_VALUE, "Static factoring error : inconsistent data dimension.");
+        p.fac_dims[a] = (int)want;
+        n *= (size_t)want;
+    }
+    p.fac_values.assign(fv.ptr(), fv.ptr() + n);
+    p.fac_grads.assign(fg.ptr(), fg.ptr() + n * pm.ndim);
+    for (size_t i = 0; i < n; ++i)
+        for (int a = 0; a < pm.ndim; ++a) p.fac_grads[i * pm.ndim + a] *= pm.scale[a];  // ReDim
+    p.fac_mask.assign(n, 1);
+    if (has_mask)
+        for (size_t i = 0; i < n; ++i) p.fac_mask[i] = fm.ptr()[i] != 0.0;
+}
+
+// ComputeFactor with factoringPointChoice "Seed" (StaticFactoring.hxx:119-175): the distance from
+// the single seed x0 in the norm at the seed (interpolated), value(x) = <g, x - x0> with
+// g = -Gradient(x0 - x) (0 at the seed), on the cells of the box [floor(x0 - r), ceil(x0 + r)) clipped
+// to the domain (the whole domain for r < 0), r truncated to an integer.
+void compute_factor(Store &io, const Param &pm, EulerProblem &p) {
+    int64_t ns = 0;
+    const std::vector<double> pts = io.get_vector("seeds", pm.ndim, &ns);
+    if (ns != 1)
+        throw Error(HFM_ERR_VALUE, "Exactly one seed point must be specified for computing the factor, found " +
+                                       std::to_string(ns) + ".");
+    const std::string choice = io.get_string("factoringPointChoice", "Seed");
+    if (choice == "Both")
+        throw Error(HFM_ERR_UNSUPPORTED, "factoringPointChoice = 'Both' is not supported by the GPU solve path");
+    if (choice != "Seed" && choice != "Key")
+        throw Error(HFM_ERR_VALUE, "StaticFactoring error : Unsupported factoringPointChoice " + choice + ".");
+    const int radius = (int)io.get_scalar("factoringRadius");
+    const int D = pm.ndim;
+    double seed[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) seed[a] = (pts[a] - pm.origin[a]) / pm.scale[a];
+    p.fac_subdomain = radius >= 0;
+    size_t n = 1;
+    for (int a = 0; a < D; ++a) {
+        if (p.fac_subdomain) {
+            p.fac_lo[a] = std::max(0, (int)std::floor(seed[a] - radius));
+            const int top = std::min(pm.dims[a] - 1, (int)std::ceil(seed[a] + radius));
+            p.fac_dims[a] = std::max(0, top - p.fac_lo[a]);
+        } else {
+            p.fac_lo[a] = 0;
+            p.fac_dims[a] = pm.dims[a];
+        }
+        n *= (size_t)p.fac_dims[a];
+    }
+    SeedGuess G{p, pm};
+    double norm[14];
+    G.at_point(seed, norm);
+    p.fac_values.assign(n, 0.0);
+    p.fac_grads.assign(n * D, 0.0);
+    p.fac_mask.assign(n, 1);
+    for (size_t i = 0; i < n; ++i) {
+        int64_t idx[3], r = (int64_t)i;
+        for (int a = D - 1; a >= 0; --a) { idx[a] = r % p.fac_dims[a]; r /= p.fac_dims[a]; }
+        double v[3] = {0, 0, 0}, mv[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+        bool null = true;
+        for (int a = 0; a < D; ++a) {
+            v[a] = ((double)(idx[a] + p.fac_lo[a]) + 0.5) - seed[a];
+            mv[a] = -v[a];
+            null = null && v[a] == 0.0;
+        }
+        if (!null) {
+            SeedGuess::tti_gradient(norm, mv, g);
+            for (int a = 0; a < D; ++a) g[a] = -g[a];
+        }
+        double f = 0.0;
+        for (int a = 0; a < D; ++a) f += g[a] * v[a];
+        p.fac_values[i] = f;
+        for (int a = 0; a < D; ++a) p.fac_grads[i * D + a] = g[a];
+    }
+    if (io.get_scalar("exportFactoring", 0.0) != 0) {
+        const std::vector<int64_t> bd(p.fac_dims, p.fac_dims + D);
+        io.set_field("factoringValues", bd, 1, p.fac_values.data());
+        io.set_field("factoringGradients", bd, D, p.fac_grads.data());
+        if (p.fac_subdomain) {
+            const double sh[3] = {(double)p.fac_lo[0], (double)p.fac_lo[1], (double)p.fac_lo[2]};
+            io.set_vector("factoringIndexShift", D, 1, sh);
+        }
+    }
+}
+
 // A model read from its store, ready to solve (the part of Run before the solver loop).
 struct Prepared {
     Param pm;
@@ -1134,7 +1256,11 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);
     set_common_solver_options(io, p);
     read_walls(io, pm, lifted, p);
-    read_seeds(io, pm, p, lifted);
+    // StaticFactoring::Setup (StaticFactoring.hxx:66-84): import, seeds, compute
+    const FactorKeys fk = read_factor_keys(io, model);
+    if (fk.import) import_factor(io, pm, p);
+    read_seeds(io, pm, p, lifted, (fk.import || fk.radius_key) ? 2.0 : 0.0);
+    if (fk.compute) compute_factor(io, pm, p);
 
     read_stopping(io, pm, lifted, p);
     read_geodesics(io, pm, lifted, p, q.geo_keys);
@@ -1180,6 +1306,10 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     q.export_stencils = read_export_stencils(io, q);
     if (inspect) read_inspect(io, pm, p);
     read_forward_variation(io, pm, p);
+    if (p.has_factoring() && (inspect || p.fwd_nvar > 0 || p.has_stopping() || !p.geo_tips.empty() ||
+                              p.want_geodesic_flow || p.bypass || p.retain))
+        throw Error(HFM_ERR_UNSUPPORTED, "static factoring with first variations, geodesics, stopping criteria, cached "
+                                         "values or retained state is not supported by the GPU solve path");
     // the arrival times are downloaded straight into the output field when no reordering is needed
     q.values_dst = q.export_values ? io.create_field("values", q.dims, 1) : nullptr;
     p.h_values_out = q.values_dst;

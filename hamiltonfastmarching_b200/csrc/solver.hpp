@@ -70,6 +70,17 @@ struct EulerProblem {
     std::vector<int64_t> seed_index;   // sorted, unique
     std::vector<double> seed_value;
 
+    // Static factoring (TTI3): over the box of cells [fac_lo, fac_lo + fac_dims), the factor values
+    // and their adimensional gradients; a neighbour value u(x + e) read by the update of a cell x of
+    // the box (and of the mask) becomes u(x + e) + <grad(x), e> + value(x) - value(x + e), the last
+    // two terms from the box (0 when x + e leaves a subdomain box), StaticFactoring.hxx:33-64.
+    std::vector<double> fac_values;    // [box cells] RowMajor
+    std::vector<double> fac_grads;     // [box cells][3]
+    std::vector<uint8_t> fac_mask;     // [box cells]
+    int fac_lo[3] = {0, 0, 0}, fac_dims[3] = {0, 0, 0};
+    bool fac_subdomain = false;
+    bool has_factoring() const { return !fac_values.empty(); }
+
     bool want_active = false;          // export the activeNeighs bitsets
     // Reverse first variation: groups of (linear index, weight) points (inspectSensitivity).
     std::vector<std::vector<int64_t>> adjoint_index;
