@@ -1240,7 +1240,26 @@ typedef struct {
     const int64_t *dims;
     const double *values;
     const uint8_t *accepted;
+    const fmo_problem *fac;   /* static factoring (fac_values), or NULL */
 } tti_fm_ctx;
+
+/* StaticFactoring::Correction with order 1 (StaticFactoring.hxx:33-57) at cell x for the offset
+ * e: 0 unless x lies in the box and its mask; then <grad(x), e> + (value(x) - value(x + e)), the
+ * parenthesis dropped (Correction 0) when x + e leaves a subdomain box. */
+static double tti_fac_correction(const fmo_problem *f, int64_t x0, int64_t x1, int64_t x2, const int *off) {
+    const int64_t b[3] = {x0 - f->fac_lo[0], x1 - f->fac_lo[1], x2 - f->fac_lo[2]};
+    for (int a = 0; a < 3; ++a)
+        if (b[a] < 0 || b[a] >= f->fac_dims[a]) return 0.0;
+    const int64_t bi = (b[0] * f->fac_dims[1] + b[1]) * f->fac_dims[2] + b[2];
+    if (!f->fac_mask[bi]) return 0.0;
+    const int64_t e[3] = {b[0] + off[0], b[1] + off[1], b[2] + off[2]};
+    for (int a = 0; a < 3; ++a)
+        if (e[a] < 0 || e[a] >= f->fac_dims[a]) return 0.0;  /* subdomain; a whole-domain box holds x + e */
+    const int64_t ei = (e[0] * f->fac_dims[1] + e[1]) * f->fac_dims[2] + e[2];
+    double deriv = 0.0;
+    for (int a = 0; a < 3; ++a) deriv += f->fac_grads[3 * bi + a] * (double)off[a];
+    return deriv + (f->fac_values[bi] - f->fac_values[ei]);
+}
 
 static double tti_fm_get(void *vctx, int64_t cell, const int *off) {
     const tti_fm_ctx *c = (const tti_fm_ctx *)vctx;
@@ -1249,7 +1268,10 @@ static double tti_fm_get(void *vctx, int64_t cell, const int *off) {
     const int64_t y0 = x0 + off[0], y1 = x1 + off[1], y2 = x2 + off[2];
     if (y0 < 0 || y0 >= c->dims[0] || y1 < 0 || y1 >= n1 || y2 < 0 || y2 >= n2) return FMO_INF;
     const int64_t y = (y0 * n1 + y1) * n2 + y2;
-    return c->accepted[y] ? c->values[y] : FMO_INF;
+    if (!c->accepted[y]) return FMO_INF;
+    double r = c->values[y];  /* GetNeighborValue (HamiltonFastMarching.hxx:357-359) */
+    if (c->fac && c->fac->fac_values) r += tti_fac_correction(c->fac, x0, x1, x2, off);
+    return r;
 }
 
 int fmo_tti_norm(const double *metric, const double *h, double *out) {
@@ -1318,7 +1340,7 @@ int64_t fmo_tti_fast_marching_stop(const int64_t *dims, const double *h, const d
         qelem q = {seed_index[s], seed_value[s]};
         if (heap_push(&h_, q)) goto done;
     }
-    tti_fm_ctx ctx = {dims, values, accepted};
+    tti_fm_ctx ctx = {dims, values, accepted, stop};
     int64_t nacc = 0;
     if (stop && stop->nstop_all > 0) {
         all_left = (uint8_t *)calloc(N, 1);

@@ -72,6 +72,15 @@ typedef struct {
      * 104-153); activeNeighs bit nfwd records which one, and a Recompute (geodesics, first
      * variations) uses that stencil only. 0 or 1: one stencil. */
     int nmax;
+    /* Static factoring of TTI3 (StaticFactoring.hxx:33-64): over the box of cells
+     * [fac_lo, fac_lo + fac_dims), factor values, adimensional gradients [3] and mask; a neighbour
+     * value u(x + e) read by the update of a masked cell x of the box becomes
+     * u(x + e) + <grad(x), e> + (value(x) - value(x + e)), the parenthesis 0 when x + e leaves a
+     * subdomain box. fac_values NULL: none. Read by fmo_tti_fast_marching_stop. */
+    const double *fac_values, *fac_grads;
+    const uint8_t *fac_mask;
+    int fac_lo[3], fac_dims[3];
+    int fac_subdomain;
 } fmo_problem;
 
 /* Fast marching. values[N] out; active[N] out (bitset, forward bits then symmetric +/- pairs,

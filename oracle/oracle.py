@@ -55,6 +55,12 @@ class _Problem(ctypes.Structure):
         ("var_dim", ctypes.c_int),
         ("mult_vec", _P),
         ("nmax", ctypes.c_int),
+        ("fac_values", _P),
+        ("fac_grads", _P),
+        ("fac_mask", _P),
+        ("fac_lo", ctypes.c_int * 3),
+        ("fac_dims", ctypes.c_int * 3),
+        ("fac_subdomain", ctypes.c_int),
     ]
 
 
@@ -481,6 +487,21 @@ def tti_solve(params: Dict) -> Dict:
             setattr(stop, "n" + fld, len(arr))
             setattr(stop, fld, _ptr(arr))
             has_stop = True
+    # static factoring given as arrays (the reference's exported factoringValues / factoringGradients /
+    # factoringIndexShift: adimensional gradients, a subdomain box when the shift is given)
+    if "_factor" in params:
+        fv, fg, shift = params["_factor"]
+        fv = np.ascontiguousarray(fv, float)
+        fg = np.ascontiguousarray(np.asarray(fg, float).reshape(fv.shape + (3,)))
+        fm = np.ascontiguousarray((np.asarray(params["_factor_mask"]) != 0).astype(np.uint8) if "_factor_mask" in params
+                                  else np.ones(fv.shape, np.uint8))
+        keep += [fv, fg, fm]
+        stop.fac_values, stop.fac_grads, stop.fac_mask = _ptr(fv), _ptr(fg), _ptr(fm)
+        for a in range(3):
+            stop.fac_lo[a] = int(shift[a]) if shift is not None else 0
+            stop.fac_dims[a] = fv.shape[a]
+        stop.fac_subdomain = 1 if shift is not None else 0
+        has_stop = True
     nacc = lib().fmo_tti_fast_marching_stop(_ptr(d), _ptr(hs), _ptr(metric), len(sidx), _ptr(sidx), _ptr(sval),
                                             _ptr(values), _ptr(tact), ctypes.byref(stop) if has_stop else None)
     if nacc < 0:

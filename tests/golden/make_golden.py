@@ -105,7 +105,8 @@ def save(name, params, out, **extra):
         blob["in_" + k] = np.asarray(v) if not isinstance(v, str) else np.array(v)
     for k in ("values", "activeNeighs", "nAccepted", "MaxStencilWidth", "costSensitivity_0",
               "seedSensitivity_0", "spreadedSeeds", "spreadedSeedValues", "geodesicPoints", "geodesicLengths",
-              "geodesicPoints_Unoriented", "geodesicLengths_Unoriented", "geodesicFlow", "valueVariation"):
+              "geodesicPoints_Unoriented", "geodesicLengths_Unoriented", "geodesicFlow", "valueVariation",
+              "factoringValues", "factoringGradients", "factoringIndexShift"):
         if k in out:
             blob["out_" + k] = np.asarray(out[k])
     blob.update(extra)
@@ -304,6 +305,29 @@ def tti_spreading_fixtures():
                                              seeds=np.array([[0.0512, 0.0433, 0.0017]]), seedRadius=1.5))
 
 
+def tti_factoring_fixtures():
+    """Static factoring of TTI3 (StaticFactoring.hxx): computed over a subdomain box (radius 4, one
+    grid scale; radius 5, three grid scales), over the whole domain (radius < 0), and imported from
+    arrays (values, gradients in physical units, mask, index shift). The computed factors are
+    exported (exportFactoring), as are the spread seeds (seedRadius defaults to 2 with factoring)."""
+    p = W.tti3_case(16, h=0.01, seed=4)
+    p.pop("_vp")
+    solve_fixture("fac_tti3_16_r4", dict(p, factoringRadius=4.0, exportFactoring=1.0))
+    q = {k: v for k, v in W.tti3_case(14, h=0.01, seed=8).items() if k not in ("_vp", "gridScale")}
+    q = dict(q, gridScales=np.array([0.01, 0.012, 0.009]), seeds=np.array([[0.071, 0.052, 0.0313]]))
+    solve_fixture("fac_tti3_14_scales_r5", dict(q, factoringRadius=5.0, exportFactoring=1.0))
+    r = W.tti3_case(10, h=0.01, seed=9)
+    r.pop("_vp")
+    solve_fixture("fac_tti3_10_whole", dict(r, factoringRadius=-1.0, exportFactoring=1.0))
+    # imported: the radius-4 factor of the first case, gradients in physical units, half the box masked
+    z = np.load(os.path.join(HERE, "fac_tti3_16_r4.npz"))
+    fv, fg, sh = z["out_factoringValues"], z["out_factoringGradients"], z["out_factoringIndexShift"]
+    mask = np.ones(fv.shape)
+    mask[: fv.shape[0] // 2] = 0.0
+    solve_fixture("fac_tti3_16_import", dict(p, factoringValues=fv, factoringGradients=fg / 0.01,
+                                             factoringMask=mask, factoringIndexShift=sh))
+
+
 def diagonal_variation_fixtures():
     """First variations of the Diagonal models, per axis: costSensitivity dims + (D,), costVariation
     dims + (nVar, D)."""
@@ -415,6 +439,8 @@ if __name__ == "__main__":
         dubins_fixtures()
     elif sys.argv[1:] == ["spreadstep"]:
         stencil_step_spreading_fixtures()
+    elif sys.argv[1:] == ["factoring"]:
+        tti_factoring_fixtures()
     else:
         main()
         tti_fixtures()
