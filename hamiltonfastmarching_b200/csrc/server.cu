@@ -125,7 +125,10 @@ struct hfm_server {
 
     // A request through hfm_run (the ordinary single-solve path).
     void run_plain(Request *r) {
-        r->prep.reset();  // hfm_run parses the store again
+        if (r->prep) {  // hfm_run parses the store again: drop the output field the first parse made
+            r->prep->fail();
+            r->prep.reset();
+        }
         {
             std::lock_guard<std::mutex> lk(mu);
             r->t_start = now();

@@ -42,6 +42,7 @@ class Ticket:
         times = (ctypes.c_double * 3)()
         self._server._L.hfm_server_release(self._server._h, self.id, times)
         self.status, self.times = st.value, tuple(times)
+        self._server._pending.pop(self.id, None)
         return True
 
     def result(self, timeout: float = -1.0) -> Dict:
@@ -62,6 +63,9 @@ class Server:
         self._L = _lib.load()
         cfg = _lib.ServerConfig(device, lanes, max_batch, float(hbm_budget_bytes))
         self._h = self._L.hfm_server_create(ctypes.byref(cfg))
+        # stores of the requests not yet completed: the scheduler reads them until completion, so
+        # they live here even when the caller drops its tickets
+        self._pending: Dict[int, HFMIO] = {}
         if not self._h:
             raise RuntimeError("hfm_server_create failed (no CUDA device or no memory)")
 
@@ -77,6 +81,7 @@ class Server:
         rc = self._L.hfm_server_submit(self._h, io._h, ctypes.byref(t))
         if rc != 0:
             raise PyExp(rc, self._L.hfm_io_last_error(io._h).decode())
+        self._pending[t.value] = io
         return Ticket(self, io, t.value)
 
     def stats(self) -> Dict:
@@ -87,7 +92,8 @@ class Server:
     def close(self):
         h, self._h = getattr(self, "_h", None), None
         if h:
-            self._L.hfm_server_destroy(h)
+            self._L.hfm_server_destroy(h)  # returns once every submitted request has completed
+        self._pending = {}
 
     def __enter__(self):
         return self
