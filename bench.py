@@ -314,7 +314,7 @@ def serving_leg(args, rank, world):
         picks = rng.integers(0, len(pool), args.serve_requests)
         gaps = rng.exponential(1.0 / rate, args.serve_requests)
         tickets = [None] * args.serve_requests
-        lat, done_t, sub_t = [], [], []
+        lat, done_t, sub_t, slow = [], [], [], []
         with Server(max_batch=max_batch) as srv:
             def waiter():
                 for i in range(args.serve_requests):
@@ -327,6 +327,7 @@ def serving_leg(args, rank, world):
                     sub_t.append(t.times[0])
                     done_t.append(t.times[2])
                     lat.append(t.latency)
+                    slow.append((t.latency, i, t.times[1] - t.times[0]))
                     tickets[i] = False  # drop the store (and its outputs)
             th = threading.Thread(target=waiter)
             th.start()
@@ -342,7 +343,10 @@ def serving_leg(args, rank, world):
             st = srv.stats()
         span = max(done_t) - min(sub_t)
         ncell = float(sum(cells[k] for k in picks))
+        worst = [{"model": str(pool[picks[i]]["model"]), "cells": cells[picks[i]], "latency_ms": round(1e3 * l, 1),
+                  "queued_ms": round(1e3 * q, 1)} for l, i, q in sorted(slow, reverse=True)[:5]]
         return {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "slowest": worst,
                 "mean_ms": 1e3 * float(np.mean(lat)), "solves_per_s": args.serve_requests / span,
                 "cells_per_s": ncell / span, "batches": st["batches"], "max_batch": st["max_batch"],
                 "peak_bytes": st["peak_bytes"]}

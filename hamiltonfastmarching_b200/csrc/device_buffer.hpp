@@ -30,6 +30,16 @@ std::mutex &cooperative_mutex();
 // Kernel launches issued by this library (all threads), for launch accounting.
 void count_launch(unsigned n = 1);
 
+// Sets the calling thread's current stream for a scope (device allocations of the scope are
+// stream-ordered on it).
+struct StreamScope {
+    cudaStream_t saved;
+    explicit StreamScope(cudaStream_t s) : saved(current_stream()) { current_stream() = s; }
+    ~StreamScope() { current_stream() = saved; }
+    StreamScope(const StreamScope &) = delete;
+    StreamScope &operator=(const StreamScope &) = delete;
+};
+
 // Large host<->device copies of pageable memory: through two page-locked staging buffers of the
 // calling thread, the host-side copies split over a pool of worker threads and overlapped with the
 // DMA of the previous chunk. Copies below kStagedMin bytes go straight through cudaMemcpyAsync.
@@ -37,6 +47,8 @@ void count_launch(unsigned n = 1);
 // staged_download returns once the destination is written.
 constexpr size_t kStagedMin = size_t(8) << 20;
 void staged_upload(void *dst_dev, const void *src_host, size_t bytes, cudaStream_t s);
+// Sets up the calling thread's staging buffers and the copy workers ahead of the first transfer.
+void staging_warm_up();
 void staged_download(void *dst_host, const void *src_dev, size_t bytes, cudaStream_t s);
 
 // Counted kernel launch: launch(kernel, grid, block, shared_bytes, stream, args...).

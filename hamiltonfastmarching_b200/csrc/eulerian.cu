@@ -189,6 +189,11 @@ struct Dev {
     unsigned *count[3];
     unsigned *claim[3];
     unsigned *flag[3];
+    // tiles of the round's band (null: the list is solved in place); its count and claim words by
+    // round parity
+    int *work;
+    unsigned *wcount;
+    unsigned *wclaim;
     unsigned *bar_count;
     unsigned *bar_gen;
     unsigned *status;
@@ -517,12 +522,61 @@ __device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bo
     if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
 }
 
+// push_tiles for lanes whose tiles may belong to different instances (a resident solver's list
+// split): the per-instance list counts are added once per instance present.
+template <typename Real>
+__device__ __forceinline__ void push_tiles_mixed(const Dev<Real> &P, int li, int D, bool want, int lane, int inst) {
+    if (want) want = atomicExch(&P.flag[li][D], 1u) == 0u;
+    const unsigned ballot = __ballot_sync(0xffffffffu, want);
+    if (!ballot) return;
+    unsigned base = 0;
+    if (lane == __ffs(ballot) - 1) base = atomicAdd(P.count[li], (unsigned)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, __ffs(ballot) - 1);
+    if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
+    if (P.live) {
+        const unsigned grp = __match_any_sync(0xffffffffu, want ? inst : -1);
+        if (want && lane == __ffs(grp) - 1) atomicAdd(P.live + li * P.nslots + inst, (unsigned)__popc(grp));
+    }
+}
+
 // Statistics row of round slot `slot` for instance slot `inst` (one row per round slot when the
 // solver keeps no per-instance statistics).
 template <typename Real>
 __device__ __forceinline__ unsigned long long *stat_row(const Dev<Real> &P, int slot, int inst) {
     const int ns = P.nslots > 1 ? P.nslots : 1;
     return P.rstat + ((long long)slot * ns + (ns > 1 ? inst : 0)) * 4;
+}
+
+// Warp-local smallest and largest wake-up keys pushed for one instance in one round, merged into
+// its statistics row with two atomics when the instance or round changes and before the round's
+// barrier (instead of two atomics on the same row per pushed tile). Warp-uniform.
+struct StatAcc {
+    int inst = -1, slot = 0;
+    unsigned long long mn = ~0ull, mx = 0ull;
+};
+
+template <typename Real>
+__device__ __forceinline__ void stat_flush(const Dev<Real> &P, StatAcc &a, int lane) {
+    if (a.inst >= 0 && lane == 0) {
+        unsigned long long *row = stat_row(P, a.slot, a.inst);
+        if (a.mn != ~0ull) atomicMin(row + 0, a.mn);
+        if (a.mx) atomicMax(row + 1, a.mx);
+    }
+    a.inst = -1;
+    a.mn = ~0ull;
+    a.mx = 0ull;
+}
+
+template <typename Real>
+__device__ __forceinline__ void stat_add(const Dev<Real> &P, StatAcc &a, int slot, int inst, unsigned long long kmin,
+                                         unsigned long long kmax, int lane) {
+    if (a.inst != inst || a.slot != slot) {
+        stat_flush(P, a, lane);
+        a.inst = inst;
+        a.slot = slot;
+    }
+    a.mn = kmin < a.mn ? kmin : a.mn;
+    a.mx = kmax > a.mx ? kmax : a.mx;
 }
 
 // Pushes the dependents of tile T that read a cell of `mask`, marking as dirty the cells of each
@@ -533,7 +587,7 @@ __device__ __forceinline__ unsigned long long *stat_row(const Dev<Real> &P, int 
 template <typename Real>
 __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int slot, int T, unsigned long long mask,
                                                 unsigned long long self_pending, unsigned long long mu,
-                                                unsigned long long kb, int lane) {
+                                                unsigned long long kb, int lane, StatAcc &acc) {
     bool any = false;
     const int inst = P.tile_inst[T];
     if (mask) {
@@ -565,11 +619,22 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
         atomicMin(P.key + T, kb);
     }
     push_tiles(P, li, T, self_pending != 0ull && lane == 0, lane, inst);
-    if ((any || self_pending) && lane == 0) {
-        unsigned long long *row = stat_row(P, slot, inst);
-        atomicMin(row + 0, kb);
-        atomicMax(row + 1, kb);
+    if (any || self_pending) stat_add(P, acc, slot, inst, kb, kb, lane);
+}
+
+// Class of a list entry at the start of a round. Stale: no key and no pending cell (its cells were
+// solved after it was queued; a later push queues the tile again, so it is dropped). In the band:
+// key at most theta, or pending cells without a key (a push that raced with the tile's own
+// activation). Carried: a key above theta.
+constexpr int kEntryStale = 0, kEntryBand = 1, kEntryCarried = 2;
+
+template <typename Real>
+__device__ __forceinline__ int entry_class(const Dev<Real> &P, int T, unsigned long long kt, double theta) {
+    if (kt == 0x7ff0000000000000ull) {
+        const unsigned long long m = ((volatile const unsigned long long *)(P.dirty + T))[0];
+        return m ? kEntryBand : kEntryStale;
     }
+    return __longlong_as_double(kt) <= theta ? kEntryBand : kEntryCarried;
 }
 
 // Cells of the warp's tile that the cell at (x0,x1,x2) reads through its visible stencil entries.
@@ -624,7 +689,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 // whose update is an extremum over a family of such solves.
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
-                                             unsigned long long &n_solves) {
+                                             unsigned long long &n_solves, StatAcc &acc) {
     [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
@@ -762,7 +827,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
     __threadfence();
     const double kv = P.kscale ? mu * P.kscale[P.tile_inst[T]] : mu;
     push_dependents(P, li_next, slot, T, mask, pending, (unsigned long long)__double_as_longlong(mu),
-                    (unsigned long long)__double_as_longlong(kv), lane);
+                    (unsigned long long)__double_as_longlong(kv), lane, acc);
 }
 
 // Persistent cooperative solver: rounds over the triple-buffered active-tile lists. Round r solves
@@ -785,7 +850,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long kInfBits = 0x7ff0000000000000ull;
-    unsigned long long n_act = 0, n_solves = 0;
+    unsigned long long n_act = 0, n_solves = 0, n_carry = 0;
+    StatAcc acc;
     double delta = Arith<double>::inf();
     int r = 0;
     bool ok = true;
@@ -803,29 +869,95 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
         const double mk = __longlong_as_double(*(volatile unsigned long long *)(P.rstat + slot * 4 + 0));
         const double theta = (P.order_lo == 0u) ? Arith<double>::inf() : mk + delta;
         unsigned long long solved = 0;
-        while (true) {
-            unsigned i = 0;
-            if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
-            i = __shfl_sync(0xffffffffu, i, 0);
-            if (i >= n) break;
-            const int T = P.list[cur][i];
-            unsigned long long kt = 0;
-            if (lane == 0) {
-                P.flag[cur][T] = 0u;
-                kt = *(volatile unsigned long long *)(P.key + T);
+        if (P.work) {
+            // split the list 32 entries per claim: tiles in the band into the work list, the others
+            // carried to the next list with their keys (one claim, one push and one key minimum per
+            // 32 entries), stale entries dropped; then the work list is solved tile by tile
+            const int par = r & 1;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                P.wcount[par ^ 1] = 0u;
+                P.wclaim[par ^ 1] = 0u;
             }
-            kt = __shfl_sync(0xffffffffu, kt, 0);
-            if (__longlong_as_double(kt) > theta) {
-                // not yet in the band: carry to the next round with its key
-                push_tiles(P, nxt, T, lane == 0, lane, 0);
-                if (lane == 0) atomicMin(P.rstat + nslot * 4 + 0, kt);
-                continue;
+            while (true) {
+                unsigned base = 0;
+                if (lane == 0) base = atomicAdd(P.claim[cur], 32u);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= n) break;
+                int T = 0;
+                int cls = kEntryStale;
+                unsigned long long kt = kInfBits;
+                if (base + lane < n) {
+                    T = __ldcg(P.list[cur] + base + lane);
+                    P.flag[cur][T] = 0u;
+                    kt = *(volatile unsigned long long *)(P.key + T);
+                    cls = entry_class(P, T, kt, theta);
+                }
+                const bool carry = cls == kEntryCarried;
+                push_tiles(P, nxt, T, carry, lane, 0);
+                unsigned long long km = carry ? kt : ~0ull;
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    const unsigned long long ok2 = __shfl_xor_sync(0xffffffffu, km, o);
+                    km = ok2 < km ? ok2 : km;
+                }
+                if (km != ~0ull) stat_add(P, acc, nslot, 0, km, 0ull, lane);
+                n_carry += (unsigned)__popc(__ballot_sync(0xffffffffu, carry));
+                const unsigned b = __ballot_sync(0xffffffffu, cls == kEntryBand);
+                if (b) {
+                    unsigned wb = 0;
+                    if (lane == 0) wb = atomicAdd(P.wcount + par, (unsigned)__popc(b));
+                    wb = __shfl_sync(0xffffffffu, wb, 0);
+                    if (cls == kEntryBand) P.work[wb + __popc(b & ((1u << lane) - 1u))] = T;
+                }
             }
-            if (lane == 0) atomicExch(P.key + T, kInfBits);
-            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves);
-            ++n_act;
-            ++solved;
+            stat_flush(P, acc, lane);
+            ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
+            if (!ok) break;
+            const unsigned nw = *(volatile unsigned *)(P.wcount + par);
+            while (true) {
+                unsigned i = 0;
+                if (lane == 0) i = atomicAdd(P.wclaim + par, 1u);
+                i = __shfl_sync(0xffffffffu, i, 0);
+                if (i >= nw) break;
+                const int T = __ldcg(P.work + i);
+                if (lane == 0) atomicExch(P.key + T, kInfBits);
+                __threadfence();  // the key is cleared before the tile's pending cells are taken
+                process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
+                ++n_act;
+                ++solved;
+            }
+        } else {
+            while (true) {
+                unsigned i = 0;
+                if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
+                i = __shfl_sync(0xffffffffu, i, 0);
+                if (i >= n) break;
+                const int T = P.list[cur][i];
+                unsigned long long kt = 0;
+                int cls = 0;
+                if (lane == 0) {
+                    P.flag[cur][T] = 0u;
+                    kt = *(volatile unsigned long long *)(P.key + T);
+                    cls = entry_class(P, T, kt, theta);
+                }
+                kt = __shfl_sync(0xffffffffu, kt, 0);
+                cls = __shfl_sync(0xffffffffu, cls, 0);
+                if (cls == kEntryStale) continue;
+                if (cls == kEntryCarried) {
+                    // not yet in the band: carry to the next round with its key
+                    push_tiles(P, nxt, T, lane == 0, lane, 0);
+                    stat_add(P, acc, nslot, 0, kt, 0ull, lane);
+                    ++n_carry;
+                    continue;
+                }
+                if (lane == 0) atomicExch(P.key + T, kInfBits);
+                __threadfence();  // the key is cleared before the tile's pending cells are taken
+                process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
+                ++n_act;
+                ++solved;
+            }
         }
+        stat_flush(P, acc, lane);
         if (lane == 0 && solved) atomicAdd(P.rstat + slot * 4 + 2, solved);
         ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
         if (!ok) break;
@@ -846,6 +978,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
     if (ok && r >= P.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(P.status, (unsigned)kErrRoundCap);
     if (lane == 0) {
         atomicAdd(P.stats + 1, n_act);
+        atomicAdd(P.stats + 3, n_carry);
     }
     n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 16);
     n_solves += __shfl_xor_sync(0xffffffffu, n_solves, 8);
@@ -861,7 +994,9 @@ template <typename Real>
 __global__ void init_lists_kernel(Dev<Real> P, const int *seed_tiles, const unsigned long long *seed_masks, int n) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (wid >= n) return;
-    push_dependents(P, 0, 0, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, 0ull, lane);
+    StatAcc acc;
+    push_dependents(P, 0, 0, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, 0ull, lane, acc);
+    stat_flush(P, acc, lane);
 }
 
 // --------------------------------------------------------------------------------------------
@@ -2557,6 +2692,10 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     P.bar_count = counters.get() + 6;
     P.bar_gen = counters.get() + 7;
+    DeviceBuffer<int> work(nt);
+    P.work = work.get();
+    P.wcount = counters.get() + 8;
+    P.wclaim = counters.get() + 10;
     P.stats = stats.get();
     P.max_rounds = p0.max_rounds;
     P.sweeps = p0.sweeps_per_tile;
@@ -2590,6 +2729,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         const bool ordered = p0.ordered;
         P.order_lo = ordered ? (unsigned)std::max(1.0, p0.band_lo * nwarps) : 0u;
         P.order_hi = ordered ? (unsigned)std::max(2.0, p0.band_hi * nwarps) : 0u;
+        if (!ordered) P.work = nullptr;  // every tile is in the band: the list is solved in place
         void *args[] = {&P};
         count_launch();
         coop.lock();
@@ -2666,6 +2806,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         res.rounds = (long long)hs[0];
         res.tile_activations = (long long)hs[1];
         res.local_solves = (long long)hs[2];
+        res.tile_carries = (long long)hs[3];
         res.t_stencil_ms = t_stencil;
         res.t_solve_ms = t_solve;
     }
@@ -2733,6 +2874,8 @@ std::unique_ptr<ResidentFamily> make_resident_family(const EulerProblem &p) {
         return p.fp64 ? make_resident_impl<double, 0, 4, kKindShare>(p) : make_resident_impl<float, 0, 4, kKindShare>(p);
     throw Error(HFM_ERR_UNSUPPORTED, "no resident solver for this model family");
 }
+
+std::unique_ptr<StagedInputs> stage_resident_inputs(const EulerProblem &p) { return detail::stage_inputs_impl(p); }
 
 void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
     if (probs.empty()) {

@@ -23,6 +23,57 @@
 // slice has run its minimum time, or at its time limit when other families wait.
 
 constexpr int kMaxResident = 256;  // instance slots of a family (per-instance statistics rows)
+constexpr int kAdmissionSms = 8;   // SMs' worth of capacity a slice leaves to admission kernels
+
+// A request's large inputs on the device: the FP64 metric (Riemann models) or speed multiplier
+// (shared-stencil models) in the input's row-major order, and the walls as bytes.
+struct StagedImpl final : StagedInputs {
+    DeviceBuffer<double> field;
+    DeviceBuffer<uint8_t> walls;
+    cudaEvent_t ready = nullptr;  // recorded after the uploads, on the staging stream
+    size_t nbytes = 0;
+    size_t bytes() const override { return nbytes; }
+    ~StagedImpl() override {
+        // the buffers are freed on the destroying thread's stream, after the uploads
+        if (ready) {
+            cudaStreamWaitEvent(current_stream(), ready, 0);
+            cudaEventDestroy(ready);
+        }
+    }
+};
+
+inline std::unique_ptr<StagedInputs> stage_inputs_impl(const EulerProblem &p) {
+    cudaStream_t s = current_stream();
+    auto st = std::make_unique<StagedImpl>();
+    const long long N = (long long)p.dims[0] * p.dims[1] * p.dims[2];
+    if (p.kind == StencilKind::RiemannPerCell) {
+        const int NS = p.ndim * (p.ndim + 1) / 2;
+        const size_t rows = p.metric_constant ? 1 : (size_t)N;
+        st->field.alloc(rows * NS);
+        staged_upload(st->field.get(), p.metric_ptr ? p.metric_ptr : p.metric.data(), rows * NS * sizeof(double), s);
+        st->nbytes += rows * NS * sizeof(double);
+    } else {
+        const long long nm[4] = {1, p.dims[2], (long long)p.dims[0] * p.dims[1], N};
+        const long long len = nm[std::min(3, std::max(0, p.mult_depth))];
+        st->field.alloc(len);
+        staged_upload(st->field.get(), p.mult_ptr ? p.mult_ptr : p.mult.data(), len * sizeof(double), s);
+        st->nbytes += len * sizeof(double);
+    }
+    if (!p.walls.empty() || p.walls_f64) {
+        st->walls.alloc(N);
+        if (!p.walls.empty()) {
+            staged_upload(st->walls.get(), p.walls.data(), N, s);
+        } else {
+            DeviceBuffer<double> wf(N);
+            staged_upload(wf.get(), p.walls_f64, N * sizeof(double), s);
+            launch(walls_from_f64_kernel, nblocks(N, 256), 256, 0, s, N, (const double *)wf.get(), st->walls.get());
+        }
+        st->nbytes += N;
+    }
+    HFM_CUDA(cudaEventCreateWithFlags(&st->ready, cudaEventDisableTiming));
+    HFM_CUDA(cudaEventRecord(st->ready, s));
+    return st;
+}
 
 struct ServeCtl {
     long long round0;              // round at which the slice starts (lists and rows continue)
@@ -62,6 +113,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
     __syncthreads();
     const unsigned long long t0 = global_ns();
     unsigned long long n_act = 0, n_solves = 0;
+    StatAcc acc;
+    int cnt_inst = -1;               // tiles solved by this warp in this round for instance cnt_inst
+    unsigned long long cnt = 0;
     long long r = C.round0;
     bool ok = true;
     for (long long it = 0; it < C.max_rounds; ++it, ++r) {
@@ -82,33 +136,80 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
             }
         }
         const unsigned n = *(volatile unsigned *)P.count[cur];
+        // split the list 32 entries per claim: tiles in their instance's band into the work list,
+        // the others carried to the next list (one push per 32 entries; the key minimum and the list
+        // count once per instance present), stale entries dropped; then the work list is solved
+        const int par = (int)(r & 1);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            P.wcount[par ^ 1] = 0u;
+            P.wclaim[par ^ 1] = 0u;
+        }
         while (true) {
-            unsigned i = 0;
-            if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
-            i = __shfl_sync(0xffffffffu, i, 0);
-            if (i >= n) break;
-            const int T = P.list[cur][i];
-            const int inst = P.tile_inst[T];
-            unsigned long long kt = 0, mk = 0;
-            if (lane == 0) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(P.claim[cur], 32u);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) break;
+            int T = 0, inst = -1, cls = kEntryStale;
+            unsigned long long kt = kInfBits;
+            if (base + lane < n) {
+                T = __ldcg(P.list[cur] + base + lane);
+                inst = P.tile_inst[T];
                 P.flag[cur][T] = 0u;
                 kt = *(volatile unsigned long long *)(P.key + T);
-                mk = *(volatile unsigned long long *)(P.rstat + ((long long)slot * P.nslots + inst) * 4);
+                const unsigned long long mk =
+                    *(volatile unsigned long long *)(P.rstat + ((long long)slot * P.nslots + inst) * 4);
+                cls = entry_class(P, T, kt, __longlong_as_double(mk) + s_delta[inst]);
             }
-            kt = __shfl_sync(0xffffffffu, kt, 0);
-            mk = __shfl_sync(0xffffffffu, mk, 0);
-            const double theta = __longlong_as_double(mk) + s_delta[inst];
-            if (__longlong_as_double(kt) > theta) {
-                // not yet in its instance's band: carry to the next round with its key
-                push_tiles(P, nxt, T, lane == 0, lane, inst);
-                if (lane == 0) atomicMin(P.rstat + ((long long)nslot * P.nslots + inst) * 4, kt);
-                continue;
+            const bool carry = cls == kEntryCarried;
+            push_tiles_mixed(P, nxt, T, carry, lane, inst);
+            // smallest carried key of each instance present, into its statistics row
+            unsigned rem = __ballot_sync(0xffffffffu, carry);
+            while (rem) {
+                const int li = __shfl_sync(0xffffffffu, inst, __ffs(rem) - 1);
+                const bool mine = carry && inst == li;
+                unsigned long long km = mine ? kt : ~0ull;
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    const unsigned long long ok2 = __shfl_xor_sync(0xffffffffu, km, o);
+                    km = ok2 < km ? ok2 : km;
+                }
+                stat_add(P, acc, nslot, li, km, 0ull, lane);
+                rem &= ~__ballot_sync(0xffffffffu, mine);
             }
+            const unsigned b = __ballot_sync(0xffffffffu, cls == kEntryBand);
+            if (b) {
+                unsigned wb = 0;
+                if (lane == 0) wb = atomicAdd(P.wcount + par, (unsigned)__popc(b));
+                wb = __shfl_sync(0xffffffffu, wb, 0);
+                if (cls == kEntryBand) P.work[wb + __popc(b & ((1u << lane) - 1u))] = T;
+            }
+        }
+        stat_flush(P, acc, lane);
+        ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
+        if (!ok) break;
+        const unsigned nw = *(volatile unsigned *)(P.wcount + par);
+        while (true) {
+            unsigned i = 0;
+            if (lane == 0) i = atomicAdd(P.wclaim + par, 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nw) break;
+            const int T = __ldcg(P.work + i);
+            const int inst = P.tile_inst[T];
             if (lane == 0) atomicExch(P.key + T, kInfBits);
-            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves);
-            if (lane == 0) atomicAdd(P.rstat + ((long long)slot * P.nslots + inst) * 4 + 2, 1ull);
+            __threadfence();  // the key is cleared before the tile's pending cells are taken
+            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
+            if (inst != cnt_inst) {
+                if (cnt && lane == 0) atomicAdd(P.rstat + ((long long)slot * P.nslots + cnt_inst) * 4 + 2, cnt);
+                cnt_inst = inst;
+                cnt = 0;
+            }
+            ++cnt;
             ++n_act;
         }
+        stat_flush(P, acc, lane);
+        if (cnt && lane == 0) atomicAdd(P.rstat + ((long long)slot * P.nslots + cnt_inst) * 4 + 2, cnt);
+        cnt_inst = -1;
+        cnt = 0;
         // the stop decision is block 0's, published before the barrier so that every block reads
         // the same word after it
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -166,7 +267,9 @@ __global__ void inject_kernel(Dev<Real> P, int li, int slot, const int *seed_til
                               int n) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (wid >= n) return;
-    push_dependents(P, li, slot, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, 0ull, lane);
+    StatAcc acc;
+    push_dependents(P, li, slot, seed_tiles[wid], seed_masks[wid], ~0ull, 0ull, 0ull, lane, acc);
+    stat_flush(P, acc, lane);
 }
 
 // An instance's reverse dependency CSR (local tile ids) into the arena: per-tile entry ranges and
@@ -248,11 +351,13 @@ class Resident final : public ResidentFamily {
         int slot = -1;
         GridGeom g{};
         long long tile0 = 0, nt = 0, e0 = 0, ne = 0, cls0 = 0, ncls = 0;
-        long long round_in = 0;
+        long long round_in = 0, rounds = 0;
         int max_width = 0;
         double *h_out = nullptr;
         float setup_ms = 0;
-        std::chrono::steady_clock::time_point t_admit;
+        std::vector<int> seed_tiles;               // arena tiles holding seeds, with their cells
+        std::vector<unsigned long long> seed_masks;
+        std::chrono::steady_clock::time_point t_admit, t_solved;
     };
 
     // arena arrays
@@ -260,7 +365,7 @@ class Resident final : public ResidentFamily {
     DeviceBuffer<unsigned> code_, vis_, tile_up_, flags_, live_, ctl_, age_;
     DeviceBuffer<Real> weight_, mult_, values_, cls_w_;
     DeviceBuffer<int8_t> cls_off_;
-    DeviceBuffer<int> tile_inst_, lists_, dep_tile_, active_d_;
+    DeviceBuffer<int> tile_inst_, lists_, work_, dep_tile_, active_d_;
     DeviceBuffer<unsigned long long> key_, maxval_, dep_mask_, dep_dmask_, rstat_, stats_;
     DeviceBuffer<DirtyWake> dirty_;
     DeviceBuffer<long long> dep_beg_, dep_end_, round_out_;
@@ -268,8 +373,13 @@ class Resident final : public ResidentFamily {
     DeviceBuffer<Inst> inst_;
     RangeAlloc tiles_, entries_, classes_;
     std::vector<int> free_slots_;
-    std::map<int, Entry> active_;
+    std::map<int, Entry> pending_, active_;  // by slot: prepared, in the lists
+    std::map<int64_t, Entry> collected_;      // by ticket: converged, result not yet copied out
     long long round_ = 0;
+    bool in_slice_ = false;
+    cudaEvent_t done_ev_ = nullptr;           // end of the running slice
+    long long *h_ctl_ = nullptr;              // page-locked: round reached, status word
+    std::unique_lock<std::mutex> coop_;       // the cooperative-launch lock, held during a slice
     struct Schedule {
         int sweeps = 2;
         double band_lo = 2.0, band_hi = 8.0;
@@ -320,6 +430,9 @@ class Resident final : public ResidentFamily {
         P.bar_count = ctl_.get() + 6;
         P.bar_gen = ctl_.get() + 7;
         P.status = ctl_.get() + 8;
+        P.work = work_.get();
+        P.wcount = ctl_.get() + 11;
+        P.wclaim = ctl_.get() + 13;
         P.stats = stats_.get();
         P.max_rounds = (int)sched_.max_rounds;
         P.sweeps = sched_.sweeps;
@@ -355,6 +468,7 @@ class Resident final : public ResidentFamily {
             regrow(maxval_, ot, ct, 1, s);
             regrow(tile_up_, ot, ct, 1, s);
             regrow(lists_, ot, ct, 3, s);
+            work_.alloc(ct);  // per-round contents only
             regrow(flags_, ot, ct, 3, s);
             regrow(dep_beg_, ot, ct, 1, s);
             regrow(dep_end_, ot, ct, 1, s);
@@ -406,7 +520,9 @@ public:
         active_d_.alloc(kMaxResident);
         round_out_.alloc(1);
         for (int i = kMaxResident - 1; i >= 0; --i) free_slots_.push_back(i);
-        resize(1 << 12, 1 << 17, SHARE ? 1 << 10 : 0, s);
+        resize(1 << 15, 1 << 20, SHARE ? 1 << 10 : 0, s);
+        HFM_CUDA(cudaHostAlloc((void **)&h_ctl_, 2 * sizeof(long long), cudaHostAllocDefault));
+        h_ctl_[0] = h_ctl_[1] = 0;
     }
 
     size_t arena_bytes() const override {
@@ -414,12 +530,16 @@ public:
     }
 
     bool has_work() const override { return !active_.empty(); }
-    int resident() const override { return (int)active_.size(); }
+    bool has_pending() const override { return !pending_.empty(); }
+    int resident() const override { return (int)(active_.size() + pending_.size() + collected_.size()); }
 
-    bool admit(const EulerProblem &p, int64_t ticket, int *max_width) override {
+    Admit prepare(const EulerProblem &p, int64_t ticket, const StagedInputs *staged_in, bool may_grow, cudaStream_t s,
+                  int *max_width) override {
         if (broken_) throw Error(HFM_ERR_CUDA, "the resident solver of this family failed earlier");
-        if (free_slots_.empty()) return false;
-        cudaStream_t s = current_stream();
+        if (free_slots_.empty()) return kNoSlot;
+        StreamScope scope(s);  // temporaries of the build are stream-ordered on `s`
+        const StagedImpl *staged = dynamic_cast<const StagedImpl *>(staged_in);
+        if (staged) HFM_CUDA(cudaStreamWaitEvent(s, staged->ready, 0));
         const GridGeom g = make_geom(p.ndim, p.dims, p.periodic, p.tile_shift[0] >= 0 ? p.tile_shift : nullptr);
         const long long nt = g.ntile, N = g.ncells;
         const long long ncls = SHARE ? p.nclass : 0;
@@ -429,6 +549,7 @@ public:
         if (tile0 < 0 || cls0 < 0) {
             if (tile0 >= 0) tiles_.release(tile0, nt);
             if (cls0 >= 0 && SHARE) classes_.release(cls0, ncls);
+            if (!may_grow) return kNeedsGrow;
             resize(tile0 < 0 ? pow2_at_least(cap_t_ + nt) : cap_t_, cap_e_,
                    SHARE && cls0 < 0 ? pow2_at_least(cap_c_ + ncls) : cap_c_, s);
             tile0 = tiles_.alloc(nt);
@@ -444,6 +565,7 @@ public:
         E.ncls = ncls;
         E.h_out = p.h_values_out;
         E.t_admit = std::chrono::steady_clock::now();
+        bool grow_refused = false;
         auto undo = [&] {
             tiles_.release(tile0, nt);
             if (SHARE) classes_.release(cls0, ncls);
@@ -509,15 +631,20 @@ public:
                 }
                 const int NS = p.ndim * (p.ndim + 1) / 2;
                 DeviceBuffer<double> metric;
-                const size_t rows = p.metric_constant ? 1 : (size_t)N;
-                metric.alloc(rows * NS);
-                staged_upload(metric.get(), p.metric_ptr ? p.metric_ptr : p.metric.data(), rows * NS * sizeof(double), s);
+                const double *dmetric = staged ? staged->field.get() : nullptr;
+                if (!dmetric) {
+                    const size_t rows = p.metric_constant ? 1 : (size_t)N;
+                    metric.alloc(rows * NS);
+                    staged_upload(metric.get(), p.metric_ptr ? p.metric_ptr : p.metric.data(), rows * NS * sizeof(double),
+                                  s);
+                    dmetric = metric.get();
+                }
                 if (p.ndim == 2)
-                    launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, V, (const double *)metric.get(),
-                           (int8_t *)nullptr, (double *)nullptr);
+                    launch(riemann_stencil_kernel<2, Real>, nblocks(N, 128), 128, 0, s, V, dmetric, (int8_t *)nullptr,
+                           (double *)nullptr);
                 else
-                    launch(riemann_stencil_kernel<3, Real>, nblocks(N, 128), 128, 0, s, V, (const double *)metric.get(),
-                           (int8_t *)nullptr, (double *)nullptr);
+                    launch(riemann_stencil_kernel<3, Real>, nblocks(N, 128), 128, 0, s, V, dmetric, (int8_t *)nullptr,
+                           (double *)nullptr);
                 launch(width_kernel<Real, NSYM>, nblocks(N, 256), 256, 0, s, V, maxw.get());
                 maxw.download(&hmaxw, 1, s);
             } else {
@@ -527,11 +654,16 @@ public:
                 cls_en.upload(p.cls_enabled, s);
                 const long long nm[4] = {1, g.dims[2], (long long)g.dims[0] * g.dims[1], g.ncells};
                 const long long len = nm[std::min(3, std::max(0, p.mult_depth))];
-                DeviceBuffer<double> mult_rm(len);
-                staged_upload(mult_rm.get(), p.mult_ptr ? p.mult_ptr : p.mult.data(), len * sizeof(double), s);
+                DeviceBuffer<double> mult_rm;
+                const double *dmult = staged ? staged->field.get() : nullptr;
+                if (!dmult) {
+                    mult_rm.alloc(len);
+                    staged_upload(mult_rm.get(), p.mult_ptr ? p.mult_ptr : p.mult.data(), len * sizeof(double), s);
+                    dmult = mult_rm.get();
+                }
                 HFM_CUDA(cudaMemsetAsync(V.mult, 0, nt * 64 * sizeof(Real), s));
                 HFM_CUDA(cudaMemsetAsync(V.vis, 0, nt * 64 * sizeof(unsigned), s));
-                launch(mult_layout_kernel<Real>, nblocks(N, 256), 256, 0, s, V, (const double *)mult_rm.get());
+                launch(mult_layout_kernel<Real>, nblocks(N, 256), 256, 0, s, V, dmult);
                 int mw = 0;
                 for (int cl = 0; cl < p.nclass; ++cl)
                     for (int k = 0; k < ND; ++k) {
@@ -554,17 +686,21 @@ public:
             DeviceBuffer<int> wdist;
             DeviceBuffer<int8_t> wd8;
             if (I.has_walls) {
-                walls.alloc(N);
-                if (!p.walls.empty()) {
-                    staged_upload(walls.get(), p.walls.data(), N, s);
-                } else {
-                    DeviceBuffer<double> wf(N);
-                    staged_upload(wf.get(), p.walls_f64, N * sizeof(double), s);
-                    launch(walls_from_f64_kernel, nblocks(N, 256), 256, 0, s, N, (const double *)wf.get(), walls.get());
+                const uint8_t *dwalls = staged && staged->walls.get() ? staged->walls.get() : nullptr;
+                if (!dwalls) {
+                    walls.alloc(N);
+                    if (!p.walls.empty()) {
+                        staged_upload(walls.get(), p.walls.data(), N, s);
+                    } else {
+                        DeviceBuffer<double> wf(N);
+                        staged_upload(wf.get(), p.walls_f64, N * sizeof(double), s);
+                        launch(walls_from_f64_kernel, nblocks(N, 256), 256, 0, s, N, (const double *)wf.get(), walls.get());
+                    }
+                    dwalls = walls.get();
                 }
                 wdist.alloc(N);
                 wd8.alloc(N);
-                launch(wall_init_kernel, nblocks(N, 256), 256, 0, s, N, (const uint8_t *)walls.get(), wdist.get());
+                launch(wall_init_kernel, nblocks(N, 256), 256, 0, s, N, dwalls, wdist.get());
                 for (int a = 0; a < 3; ++a) {
                     if (g.dims[a] == 1) continue;
                     const long long nl = g.ncells / g.dims[a];
@@ -577,17 +713,19 @@ public:
                    (const int8_t *)wd8.get(), (const uint8_t *)cls_en.get());
             // ---- seeds (local indices) and their tiles
             std::vector<long long> hsi(p.seed_index.begin(), p.seed_index.end());
-            std::vector<int> st;
-            std::vector<unsigned long long> sm;
             for (long long x : hsi) {
                 const int x2 = (int)(x % g.dims[2]);
                 const long long rr = x / g.dims[2];
                 const int x1 = (int)(rr % g.dims[1]), x0 = (int)(rr / g.dims[1]);
                 const int T = (int)(tile0 + g.tile_of(x0, x1, x2));
                 const int b = g.local_of(x0, x1, x2);
-                auto it = std::find(st.begin(), st.end(), T);
-                if (it == st.end()) { st.push_back(T); sm.push_back(1ull << b); }
-                else sm[it - st.begin()] |= 1ull << b;
+                auto it = std::find(E.seed_tiles.begin(), E.seed_tiles.end(), T);
+                if (it == E.seed_tiles.end()) {
+                    E.seed_tiles.push_back(T);
+                    E.seed_masks.push_back(1ull << b);
+                } else {
+                    E.seed_masks[it - E.seed_tiles.begin()] |= 1ull << b;
+                }
             }
             DeviceBuffer<long long> sidx;
             DeviceBuffer<double> sval;
@@ -628,6 +766,10 @@ public:
             ho[nt] = ne;
             long long e0 = entries_.alloc(std::max(1ll, ne));
             if (e0 < 0) {
+                if (!may_grow) {
+                    grow_refused = true;
+                    throw Error(HFM_ERR_NOMEM, "dependency entries do not fit while the solver runs");
+                }
                 resize(cap_t_, pow2_at_least(cap_e_ + ne), cap_c_, s);
                 V.sstride = cap_t_ * 64;  // unchanged: only the entry space grew
                 e0 = entries_.alloc(std::max(1ll, ne));
@@ -691,43 +833,53 @@ public:
             const unsigned zero = 0;
             HFM_CUDA(cudaMemcpyAsync(delta_.get() + slot, &inf, sizeof(double), cudaMemcpyHostToDevice, s));
             HFM_CUDA(cudaMemcpyAsync(age_.get() + slot, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, s));
-            // ---- seed tiles into the list the next slice starts with
-            if (!st.empty()) {
-                DeviceBuffer<int> stile;
-                DeviceBuffer<unsigned long long> smask;
-                stile.upload(st, s);
-                smask.upload(sm, s);
-                launch(inject_kernel<Real>, nblocks((long long)st.size() * 32, 128), 128, 0, s, global_view(),
-                       (int)(round_ % 3), (int)(round_ & 7), (const int *)stile.get(),
-                       (const unsigned long long *)smask.get(), (int)st.size());
-            }
             HFM_CUDA(cudaGetLastError());
             HFM_CUDA(cudaStreamSynchronize(s));
-            E.round_in = round_;
             E.setup_ms = tm.stop(s);
             if (max_width) *max_width = E.max_width;
-            if (st.empty()) {  // nothing to solve: released at the next collection
-                E.round_in = -1;
-            }
-            active_.emplace(slot, E);
+            pending_.emplace(slot, std::move(E));
         } catch (...) {
             if (E.e0 || E.ne) entries_.release(E.e0, E.ne);
             undo();
             if (E.slot >= 0) free_slots_.push_back(E.slot);
+            if (grow_refused) return kNeedsGrow;
             throw;
         }
-        return true;
+        return kPrepared;
     }
 
-    void slice(const volatile unsigned *attn_dev, double min_ms, double max_ms) override {
-        if (active_.empty()) return;
+    void activate() override {
+        cudaStream_t s = current_stream();
+        for (auto &kv : pending_) {
+            Entry &E = kv.second;
+            if (!E.seed_tiles.empty()) {
+                DeviceBuffer<int> stile;
+                DeviceBuffer<unsigned long long> smask;
+                stile.upload(E.seed_tiles, s);
+                smask.upload(E.seed_masks, s);
+                launch(inject_kernel<Real>, nblocks((long long)E.seed_tiles.size() * 32, 128), 128, 0, s, global_view(),
+                       (int)(round_ % 3), (int)(round_ & 7), (const int *)stile.get(),
+                       (const unsigned long long *)smask.get(), (int)E.seed_tiles.size());
+                E.round_in = round_;
+            } else {
+                E.round_in = -1;  // nothing to solve: released at the next collection
+            }
+            E.t_admit = std::chrono::steady_clock::now();
+            active_.emplace(kv.first, std::move(E));
+        }
+        pending_.clear();
+        HFM_CUDA(cudaGetLastError());
+    }
+
+    void slice_begin(const volatile unsigned *attn_dev, double min_ms, double max_ms) override {
+        if (in_slice_) throw Error(HFM_ERR_CUDA, "resident solver: a slice is already running");
         cudaStream_t s = current_stream();
         std::vector<int> act;
         for (const auto &kv : active_)
             if (kv.second.round_in >= 0) act.push_back(kv.first);
         if (act.empty()) return;
         HFM_CUDA(cudaMemcpyAsync(active_d_.get(), act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-        HFM_CUDA(cudaMemsetAsync(ctl_.get() + 9, 0, 2 * sizeof(unsigned), s));  // stop words
+        HFM_CUDA(cudaMemsetAsync(ctl_.get() + 9, 0, 6 * sizeof(unsigned), s));  // stop words, work list words
         Dev<Real> P = global_view();
         int dev = 0, nsm = 0, per_sm = 0;
         HFM_CUDA(cudaGetDevice(&dev));
@@ -735,7 +887,8 @@ public:
         HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_resident_kernel<Real, NFWD, NSYM, KIND>,
                                                                kWarpsPerCta * 32, 0));
         if (per_sm < 1) throw Error(HFM_ERR_CUDA, "resident solver kernel cannot be resident");
-        const int grid = nsm * per_sm;
+        // the capacity of a few SMs stays free for the admission kernels issued while the slice runs
+        const int grid = std::max(1, nsm * per_sm - std::min(kAdmissionSms * per_sm, nsm * per_sm / 2));
         // each instance keeps the band it would have alone: the tiles of a round are the union of
         // the instances' bands, so a large instance is not slowed by the small ones beside it
         const double nwarps = (double)grid * kWarpsPerCta;
@@ -754,17 +907,49 @@ public:
         C.hi = (unsigned)std::max(2.0, sched_.band_hi * nwarps);
         C.max_rounds = sched_.max_rounds;
         void *args[] = {&P, &C};
+        if (!done_ev_) HFM_CUDA(cudaEventCreateWithFlags(&done_ev_, cudaEventDisableTiming));
         count_launch();
-        long long rout = round_;
-        unsigned st = 0;
-        {
-            std::lock_guard<std::mutex> coop(cooperative_mutex());
+        coop_ = std::unique_lock<std::mutex>(cooperative_mutex());
+        try {
             HFM_CUDA(cudaLaunchCooperativeKernel((void *)fim_resident_kernel<Real, NFWD, NSYM, KIND>, dim3(grid),
                                                  dim3(kWarpsPerCta * 32), args, 0, s));
-            HFM_CUDA(cudaMemcpyAsync(&rout, round_out_.get(), sizeof(long long), cudaMemcpyDeviceToHost, s));
-            HFM_CUDA(cudaMemcpyAsync(&st, ctl_.get() + 8, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-            HFM_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            coop_.unlock();
+            throw;
         }
+        try {
+            HFM_CUDA(cudaMemcpyAsync(h_ctl_, round_out_.get(), sizeof(long long), cudaMemcpyDeviceToHost, s));
+            HFM_CUDA(cudaMemcpyAsync(h_ctl_ + 1, ctl_.get() + 8, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            HFM_CUDA(cudaEventRecord(done_ev_, s));
+        } catch (...) {
+            cudaStreamSynchronize(s);  // the launched slice ends before its arrays can go
+            broken_ = true;
+            coop_.unlock();
+            throw;
+        }
+        in_slice_ = true;
+    }
+
+    bool slice_done() override {
+        if (!in_slice_) return true;
+        const cudaError_t e = cudaEventQuery(done_ev_);
+        if (e == cudaErrorNotReady) return false;
+        return true;  // an error is reported by slice_end
+    }
+
+    void slice_end() override {
+        if (!in_slice_) return;
+        in_slice_ = false;
+        const cudaError_t e = cudaEventSynchronize(done_ev_);
+        coop_.unlock();
+        if (e != cudaSuccess) {
+            broken_ = true;
+            throw Error(HFM_ERR_CUDA, std::string("resident solver: ") + cudaGetErrorString(e));
+        }
+        long long rout = 0;
+        unsigned st = 0;
+        std::memcpy(&rout, h_ctl_, sizeof(long long));
+        std::memcpy(&st, h_ctl_ + 1, sizeof(unsigned));
         if (st & (kErrBarrierTimeout | kErrRoundCap)) {
             broken_ = true;
             throw Error(HFM_ERR_NOT_CONVERGED, st & kErrBarrierTimeout ? "resident solver: a grid barrier wait exceeded its limit"
@@ -773,7 +958,7 @@ public:
         round_ = rout;
     }
 
-    void collect(std::vector<std::pair<int64_t, EulerResult>> &done) override {
+    void collect(std::vector<int64_t> &done) override {
         if (active_.empty()) return;
         cudaStream_t s = current_stream();
         std::vector<unsigned> live(kMaxResident);
@@ -781,9 +966,28 @@ public:
                                  cudaMemcpyDeviceToHost, s));
         HFM_CUDA(cudaStreamSynchronize(s));
         for (auto it = active_.begin(); it != active_.end();) {
-            const Entry &E = it->second;
+            Entry &E = it->second;
             if (E.round_in >= 0 && live[E.slot] != 0u) { ++it; continue; }
-            EulerResult res;
+            E.rounds = E.round_in >= 0 ? round_ - E.round_in : 0;
+            E.t_solved = std::chrono::steady_clock::now();
+            done.push_back(E.ticket);
+            collected_.emplace(E.ticket, std::move(E));
+            it = active_.erase(it);
+        }
+    }
+
+    void finish(int64_t ticket, EulerResult &res, cudaStream_t s) override {
+        auto it = collected_.find(ticket);
+        if (it == collected_.end()) throw Error(HFM_ERR_ARG, "resident solver: unknown instance");
+        const Entry E = std::move(it->second);
+        collected_.erase(it);
+        auto release = [&] {
+            tiles_.release(E.tile0, E.nt);
+            if (SHARE) classes_.release(E.cls0, E.ncls);
+            entries_.release(E.e0, E.ne);
+            free_slots_.push_back(E.slot);
+        };
+        try {
             const long long n = E.g.ncells;
             const Real *src = values_.get() + E.tile0 * 64;
             double *dst = E.h_out;
@@ -807,28 +1011,41 @@ public:
             res.n_accepted = reached;
             res.max_stencil_width = E.max_width;
             res.t_stencil_ms = E.setup_ms;
-            res.t_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - E.t_admit).count();
-            res.rounds = E.round_in >= 0 ? round_ - E.round_in : 0;
+            res.t_solve_ms = std::chrono::duration<double, std::milli>(E.t_solved - E.t_admit).count();
+            res.rounds = E.rounds;
             res.t_total_ms = res.t_solve_ms;
-            tiles_.release(E.tile0, E.nt);
-            if (SHARE) classes_.release(E.cls0, E.ncls);
-            entries_.release(E.e0, E.ne);
-            free_slots_.push_back(E.slot);
-            done.emplace_back(E.ticket, std::move(res));
-            it = active_.erase(it);
+        } catch (...) {
+            release();
+            throw;
         }
+        release();
     }
 
     // Drops every instance (after a failure of the solver): their tickets are returned.
     void abandon(std::vector<int64_t> &tickets) override {
-        for (const auto &kv : active_) {
-            tickets.push_back(kv.second.ticket);
-            tiles_.release(kv.second.tile0, kv.second.nt);
-            if (SHARE) classes_.release(kv.second.cls0, kv.second.ncls);
-            entries_.release(kv.second.e0, kv.second.ne);
-            free_slots_.push_back(kv.first);
-        }
+        auto drop = [&](const Entry &E) {
+            tickets.push_back(E.ticket);
+            tiles_.release(E.tile0, E.nt);
+            if (SHARE) classes_.release(E.cls0, E.ncls);
+            entries_.release(E.e0, E.ne);
+            free_slots_.push_back(E.slot);
+        };
+        for (const auto &kv : pending_) drop(kv.second);
+        for (const auto &kv : active_) drop(kv.second);
+        for (const auto &kv : collected_) drop(kv.second);
+        pending_.clear();
         active_.clear();
+        collected_.clear();
+    }
+
+    ~Resident() override {
+        if (in_slice_) {
+            cudaEventSynchronize(done_ev_);
+            in_slice_ = false;
+            coop_.unlock();
+        }
+        if (done_ev_) cudaEventDestroy(done_ev_);
+        if (h_ctl_) cudaFreeHost(h_ctl_);
     }
 };
 

@@ -1407,6 +1407,7 @@ void finish_model(Store &io, const Prepared &q, const EulerResult &r) {
     io.set_scalar("solverRounds", (double)r.rounds);
     io.set_scalar("tileActivations", (double)r.tile_activations);
     io.set_scalar("executedUpdates", (double)r.local_solves);
+    io.set_scalar("tileCarries", (double)r.tile_carries);
     if (io.verbosity >= 1) {
         std::ostringstream m;
         m << "Fast marching solver completed in " << r.t_solve_ms * 1e-3 << " s.\n";

@@ -143,6 +143,11 @@ Staging &staging() {
 
 }  // namespace
 
+void staging_warm_up() {
+    staging();
+    copy_pool();
+}
+
 void staged_upload(void *dst_dev, const void *src_host, size_t bytes, cudaStream_t s) {
     Staging &st = staging();
     if (bytes < kStagedMin || !st.ok) {
@@ -196,15 +201,7 @@ void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxe
 
 }  // namespace hfm
 
-namespace {
-
-struct StreamScope {
-    cudaStream_t saved;
-    explicit StreamScope(cudaStream_t s) : saved(hfm::current_stream()) { hfm::current_stream() = s; }
-    ~StreamScope() { hfm::current_stream() = saved; }
-};
-
-}  // namespace
+using hfm::StreamScope;
 
 extern "C" {
 

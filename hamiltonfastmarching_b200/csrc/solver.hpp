@@ -161,6 +161,7 @@ struct EulerResult {
     std::vector<double> value_variation;  // [N][fwd_nvar] forward first variation
     double t_stencil_ms = 0, t_solve_ms = 0, t_adjoint_ms = 0, t_geodesic_ms = 0, t_total_ms = 0;
     long long rounds = 0, tile_activations = 0, local_solves = 0;
+    long long tile_carries = 0;  // list entries passed on to the next round (key above the band)
     std::shared_ptr<RetainedSolve> retained;  // set when EulerProblem::retain (single instance)
 };
 
@@ -173,23 +174,50 @@ void default_schedule(EulerProblem &p);
 // over all instances, one persistent solver launch). Results are in the order of `probs`.
 void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results);
 
+// Device copies of a request's large inputs (metric or speed multiplier, walls), uploaded ahead of
+// its admission by another thread while the solver runs (stage_resident_inputs).
+struct StagedInputs {
+    virtual ~StagedInputs() = default;
+    virtual size_t bytes() const = 0;
+};
+// Issues the uploads on the calling thread's current stream and returns once the host sources have
+// been read; admission waits for the copies on its own stream.
+std::unique_ptr<StagedInputs> stage_resident_inputs(const EulerProblem &p);
+
 // Resident solver of one model family for the serving loop (resident.cuh): admitted instances live
 // in a device arena and one persistent solver runs them in slices; each instance is released as
-// soon as its own tiles drain. All calls come from one thread, on its current stream.
+// soon as its own tiles drain. All calls come from one thread. The slice runs on the thread's
+// current stream; prepare() and finish() take their own stream and may run while a slice of this
+// family is in flight: they only touch arena ranges that the running solver does not read.
 class ResidentFamily {
 public:
+    enum Admit { kPrepared, kNoSlot, kNeedsGrow };
     virtual ~ResidentFamily() = default;
-    // Sets up `p` in the arena and queues its seed tiles for the next slice. False: no free slot.
+    // Builds `p` in the arena on stream `s` (stencils, walls, visibility, seeds, tile
+    // dependencies, slot) from the staged inputs when given; it joins the solver's lists at the
+    // next activate(). kNeedsGrow: the arena is full and `may_grow` is false (a slice is running).
     // Throws Error for an invalid instance (nothing of it stays resident).
-    virtual bool admit(const EulerProblem &p, int64_t ticket, int *max_width) = 0;
-    // Runs the solver until an instance converges, every tile is done, the attention word (device
-    // view of host memory, may be null) is raised after min_ms, or max_ms (0: no limit) has passed.
-    virtual void slice(const volatile unsigned *attn_dev, double min_ms, double max_ms) = 0;
-    // Converged instances: their tickets and results (values, nAccepted, MaxStencilWidth, times).
-    virtual void collect(std::vector<std::pair<int64_t, EulerResult>> &done) = 0;
-    // Drops every instance after a failure of the solver; their tickets are appended.
+    virtual Admit prepare(const EulerProblem &p, int64_t ticket, const StagedInputs *staged, bool may_grow,
+                          cudaStream_t s, int *max_width) = 0;
+    // Seed tiles of the prepared instances into the lists (no slice running).
+    virtual void activate() = 0;
+    // Launches a slice: the solver runs until an instance converges, every tile is done, the
+    // attention word (device view of host memory, may be null) is raised after min_ms, or max_ms
+    // (0: no limit) has passed. slice_done() polls it; slice_end() waits for it and throws Error
+    // when the solver failed.
+    virtual void slice_begin(const volatile unsigned *attn_dev, double min_ms, double max_ms) = 0;
+    virtual bool slice_done() = 0;
+    virtual void slice_end() = 0;
+    // Converged instances (no slice running): they leave the lists; their tickets are appended.
+    virtual void collect(std::vector<int64_t> &done) = 0;
+    // Result of a collected instance (values, nAccepted, MaxStencilWidth, times), copied out on
+    // stream `s` into its output field; then its arena range and slot are free.
+    virtual void finish(int64_t ticket, EulerResult &res, cudaStream_t s) = 0;
+    // Drops every instance (prepared, running or collected) after a failure of the solver; their
+    // tickets are appended.
     virtual void abandon(std::vector<int64_t> &tickets) = 0;
-    virtual bool has_work() const = 0;
+    virtual bool has_work() const = 0;     // instances in the lists
+    virtual bool has_pending() const = 0;  // prepared instances waiting for activate()
     virtual int resident() const = 0;
     virtual size_t arena_bytes() const = 0;
 };
