@@ -49,6 +49,10 @@ constexpr size_t kStagedMin = size_t(8) << 20;
 void staged_upload(void *dst_dev, const void *src_host, size_t bytes, cudaStream_t s);
 // Sets up the calling thread's staging buffers and the copy workers ahead of the first transfer.
 void staging_warm_up();
+// Small page-locked host words for asynchronous device-to-host reads (bump-allocated from a pool
+// set up once per process and kept: page-locking memory synchronises the device, which must not
+// happen while a persistent solver runs). 16-byte aligned; throws when the pool is spent.
+void *pinned_words(size_t bytes);
 void staged_download(void *dst_host, const void *src_dev, size_t bytes, cudaStream_t s);
 
 // Counted kernel launch: launch(kernel, grid, block, shared_bytes, stream, args...).

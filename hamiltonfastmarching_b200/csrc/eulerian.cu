@@ -178,6 +178,8 @@ struct Dev {
     int fac_lo[3], fac_dims[3];
     int fac_sub;                           // the box is a subdomain (corrections vanish outside it)
     unsigned *tile_up;                     // [ntile] value increases taken by each tile
+    unsigned up_budget;                    // increases a tile may take before it takes only
+                                           // decreases (0: kUpBudget)
     // Diagonal models (a single instance): the speed (or cost) vector per cell, for the first
     // variations, which have one component per axis (var_dim = ndim; 1 elsewhere)
     const double *diag_src;
@@ -189,11 +191,6 @@ struct Dev {
     unsigned *count[3];
     unsigned *claim[3];
     unsigned *flag[3];
-    // tiles of the round's band (null: the list is solved in place); its count and claim words by
-    // round parity
-    int *work;
-    unsigned *wcount;
-    unsigned *wclaim;
     unsigned *bar_count;
     unsigned *bar_gen;
     unsigned *status;
@@ -522,23 +519,6 @@ __device__ __forceinline__ void push_tiles(const Dev<Real> &P, int li, int D, bo
     if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
 }
 
-// push_tiles for lanes whose tiles may belong to different instances (a resident solver's list
-// split): the per-instance list counts are added once per instance present.
-template <typename Real>
-__device__ __forceinline__ void push_tiles_mixed(const Dev<Real> &P, int li, int D, bool want, int lane, int inst) {
-    if (want) want = atomicExch(&P.flag[li][D], 1u) == 0u;
-    const unsigned ballot = __ballot_sync(0xffffffffu, want);
-    if (!ballot) return;
-    unsigned base = 0;
-    if (lane == __ffs(ballot) - 1) base = atomicAdd(P.count[li], (unsigned)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, __ffs(ballot) - 1);
-    if (want) P.list[li][base + __popc(ballot & ((1u << lane) - 1u))] = D;
-    if (P.live) {
-        const unsigned grp = __match_any_sync(0xffffffffu, want ? inst : -1);
-        if (want && lane == __ffs(grp) - 1) atomicAdd(P.live + li * P.nslots + inst, (unsigned)__popc(grp));
-    }
-}
-
 // Statistics row of round slot `slot` for instance slot `inst` (one row per round slot when the
 // solver keeps no per-instance statistics).
 template <typename Real>
@@ -736,7 +716,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
     unsigned ups = 0;  // increases taken by this lane in this activation
     unsigned tile_ups = 0;
     if (lane == 0) tile_ups = __ldcg(P.tile_up + T);
-    const bool strict = __shfl_sync(0xffffffffu, tile_ups, 0) >= kUpBudget;
+    const bool strict = __shfl_sync(0xffffffffu, tile_ups, 0) >= (P.up_budget ? P.up_budget : kUpBudget);
     for (int sweep = 0; sweep < P.sweeps; ++sweep) {
         Real nv[2] = {cur[0], cur[1]};
         // one copy of the (large) local solve for both cells; the per-cell operands are selected,
@@ -869,93 +849,34 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
         const double mk = __longlong_as_double(*(volatile unsigned long long *)(P.rstat + slot * 4 + 0));
         const double theta = (P.order_lo == 0u) ? Arith<double>::inf() : mk + delta;
         unsigned long long solved = 0;
-        if (P.work) {
-            // split the list 32 entries per claim: tiles in the band into the work list, the others
-            // carried to the next list with their keys (one claim, one push and one key minimum per
-            // 32 entries), stale entries dropped; then the work list is solved tile by tile
-            const int par = r & 1;
-            if (blockIdx.x == 0 && threadIdx.x == 0) {
-                P.wcount[par ^ 1] = 0u;
-                P.wclaim[par ^ 1] = 0u;
+        while (true) {
+            unsigned i = 0;
+            if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= n) break;
+            const int T = P.list[cur][i];
+            unsigned long long kt = 0;
+            int cls = 0;
+            if (lane == 0) {
+                P.flag[cur][T] = 0u;
+                kt = *(volatile unsigned long long *)(P.key + T);
+                cls = entry_class(P, T, kt, theta);
             }
-            while (true) {
-                unsigned base = 0;
-                if (lane == 0) base = atomicAdd(P.claim[cur], 32u);
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (base >= n) break;
-                int T = 0;
-                int cls = kEntryStale;
-                unsigned long long kt = kInfBits;
-                if (base + lane < n) {
-                    T = __ldcg(P.list[cur] + base + lane);
-                    P.flag[cur][T] = 0u;
-                    kt = *(volatile unsigned long long *)(P.key + T);
-                    cls = entry_class(P, T, kt, theta);
-                }
-                const bool carry = cls == kEntryCarried;
-                push_tiles(P, nxt, T, carry, lane, 0);
-                unsigned long long km = carry ? kt : ~0ull;
-#pragma unroll
-                for (int o = 16; o; o >>= 1) {
-                    const unsigned long long ok2 = __shfl_xor_sync(0xffffffffu, km, o);
-                    km = ok2 < km ? ok2 : km;
-                }
-                if (km != ~0ull) stat_add(P, acc, nslot, 0, km, 0ull, lane);
-                n_carry += (unsigned)__popc(__ballot_sync(0xffffffffu, carry));
-                const unsigned b = __ballot_sync(0xffffffffu, cls == kEntryBand);
-                if (b) {
-                    unsigned wb = 0;
-                    if (lane == 0) wb = atomicAdd(P.wcount + par, (unsigned)__popc(b));
-                    wb = __shfl_sync(0xffffffffu, wb, 0);
-                    if (cls == kEntryBand) P.work[wb + __popc(b & ((1u << lane) - 1u))] = T;
-                }
+            kt = __shfl_sync(0xffffffffu, kt, 0);
+            cls = __shfl_sync(0xffffffffu, cls, 0);
+            if (cls == kEntryStale) continue;
+            if (cls == kEntryCarried) {
+                // not yet in the band: carry to the next round with its key
+                push_tiles(P, nxt, T, lane == 0, lane, 0);
+                stat_add(P, acc, nslot, 0, kt, 0ull, lane);
+                ++n_carry;
+                continue;
             }
-            stat_flush(P, acc, lane);
-            ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
-            if (!ok) break;
-            const unsigned nw = *(volatile unsigned *)(P.wcount + par);
-            while (true) {
-                unsigned i = 0;
-                if (lane == 0) i = atomicAdd(P.wclaim + par, 1u);
-                i = __shfl_sync(0xffffffffu, i, 0);
-                if (i >= nw) break;
-                const int T = __ldcg(P.work + i);
-                if (lane == 0) atomicExch(P.key + T, kInfBits);
-                __threadfence();  // the key is cleared before the tile's pending cells are taken
-                process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
-                ++n_act;
-                ++solved;
-            }
-        } else {
-            while (true) {
-                unsigned i = 0;
-                if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
-                i = __shfl_sync(0xffffffffu, i, 0);
-                if (i >= n) break;
-                const int T = P.list[cur][i];
-                unsigned long long kt = 0;
-                int cls = 0;
-                if (lane == 0) {
-                    P.flag[cur][T] = 0u;
-                    kt = *(volatile unsigned long long *)(P.key + T);
-                    cls = entry_class(P, T, kt, theta);
-                }
-                kt = __shfl_sync(0xffffffffu, kt, 0);
-                cls = __shfl_sync(0xffffffffu, cls, 0);
-                if (cls == kEntryStale) continue;
-                if (cls == kEntryCarried) {
-                    // not yet in the band: carry to the next round with its key
-                    push_tiles(P, nxt, T, lane == 0, lane, 0);
-                    stat_add(P, acc, nslot, 0, kt, 0ull, lane);
-                    ++n_carry;
-                    continue;
-                }
-                if (lane == 0) atomicExch(P.key + T, kInfBits);
-                __threadfence();  // the key is cleared before the tile's pending cells are taken
-                process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
-                ++n_act;
-                ++solved;
-            }
+            if (lane == 0) atomicExch(P.key + T, kInfBits);
+            __threadfence();  // the key is cleared before the tile's pending cells are taken
+            process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
+            ++n_act;
+            ++solved;
         }
         stat_flush(P, acc, lane);
         if (lane == 0 && solved) atomicAdd(P.rstat + slot * 4 + 2, solved);
@@ -2412,6 +2333,9 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                     P.fac_dims[a] = p0.fac_dims[a];
                 }
                 P.fac_sub = p0.fac_subdomain ? 1 : 0;
+                // the corrected update is not monotone: cells rise and fall a few times on the way
+                // to the fixed point, so a tile gets a larger budget of increases
+                P.up_budget = 64 * kUpBudget;
             }
             launch(tti_setup_kernel<NSYM, Real>, nblocks(N, 128), 128, 0, s, P, metric_ptr);
         } else if (p0.diagonal) {
@@ -2692,10 +2616,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     }
     P.bar_count = counters.get() + 6;
     P.bar_gen = counters.get() + 7;
-    DeviceBuffer<int> work(nt);
-    P.work = work.get();
-    P.wcount = counters.get() + 8;
-    P.wclaim = counters.get() + 10;
     P.stats = stats.get();
     P.max_rounds = p0.max_rounds;
     P.sweeps = p0.sweeps_per_tile;
@@ -2729,7 +2649,6 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         const bool ordered = p0.ordered;
         P.order_lo = ordered ? (unsigned)std::max(1.0, p0.band_lo * nwarps) : 0u;
         P.order_hi = ordered ? (unsigned)std::max(2.0, p0.band_hi * nwarps) : 0u;
-        if (!ordered) P.work = nullptr;  // every tile is in the band: the list is solved in place
         void *args[] = {&P};
         count_launch();
         coop.lock();

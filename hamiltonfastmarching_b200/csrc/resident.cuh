@@ -136,65 +136,31 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD,
             }
         }
         const unsigned n = *(volatile unsigned *)P.count[cur];
-        // split the list 32 entries per claim: tiles in their instance's band into the work list,
-        // the others carried to the next list (one push per 32 entries; the key minimum and the list
-        // count once per instance present), stale entries dropped; then the work list is solved
-        const int par = (int)(r & 1);
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            P.wcount[par ^ 1] = 0u;
-            P.wclaim[par ^ 1] = 0u;
-        }
         while (true) {
-            unsigned base = 0;
-            if (lane == 0) base = atomicAdd(P.claim[cur], 32u);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (base >= n) break;
-            int T = 0, inst = -1, cls = kEntryStale;
-            unsigned long long kt = kInfBits;
-            if (base + lane < n) {
-                T = __ldcg(P.list[cur] + base + lane);
-                inst = P.tile_inst[T];
+            unsigned i = 0;
+            if (lane == 0) i = atomicAdd(P.claim[cur], 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= n) break;
+            const int T = P.list[cur][i];
+            const int inst = P.tile_inst[T];
+            unsigned long long kt = 0;
+            int cls = 0;
+            if (lane == 0) {
                 P.flag[cur][T] = 0u;
                 kt = *(volatile unsigned long long *)(P.key + T);
                 const unsigned long long mk =
                     *(volatile unsigned long long *)(P.rstat + ((long long)slot * P.nslots + inst) * 4);
                 cls = entry_class(P, T, kt, __longlong_as_double(mk) + s_delta[inst]);
             }
-            const bool carry = cls == kEntryCarried;
-            push_tiles_mixed(P, nxt, T, carry, lane, inst);
-            // smallest carried key of each instance present, into its statistics row
-            unsigned rem = __ballot_sync(0xffffffffu, carry);
-            while (rem) {
-                const int li = __shfl_sync(0xffffffffu, inst, __ffs(rem) - 1);
-                const bool mine = carry && inst == li;
-                unsigned long long km = mine ? kt : ~0ull;
-#pragma unroll
-                for (int o = 16; o; o >>= 1) {
-                    const unsigned long long ok2 = __shfl_xor_sync(0xffffffffu, km, o);
-                    km = ok2 < km ? ok2 : km;
-                }
-                stat_add(P, acc, nslot, li, km, 0ull, lane);
-                rem &= ~__ballot_sync(0xffffffffu, mine);
+            kt = __shfl_sync(0xffffffffu, kt, 0);
+            cls = __shfl_sync(0xffffffffu, cls, 0);
+            if (cls == kEntryStale) continue;
+            if (cls == kEntryCarried) {
+                // not yet in its instance's band: carry to the next round with its key
+                push_tiles(P, nxt, T, lane == 0, lane, inst);
+                stat_add(P, acc, nslot, inst, kt, 0ull, lane);
+                continue;
             }
-            const unsigned b = __ballot_sync(0xffffffffu, cls == kEntryBand);
-            if (b) {
-                unsigned wb = 0;
-                if (lane == 0) wb = atomicAdd(P.wcount + par, (unsigned)__popc(b));
-                wb = __shfl_sync(0xffffffffu, wb, 0);
-                if (cls == kEntryBand) P.work[wb + __popc(b & ((1u << lane) - 1u))] = T;
-            }
-        }
-        stat_flush(P, acc, lane);
-        ok = grid_barrier(P.bar_count, P.bar_gen, gridDim.x, P.status, kBarrierPolls);
-        if (!ok) break;
-        const unsigned nw = *(volatile unsigned *)(P.wcount + par);
-        while (true) {
-            unsigned i = 0;
-            if (lane == 0) i = atomicAdd(P.wclaim + par, 1u);
-            i = __shfl_sync(0xffffffffu, i, 0);
-            if (i >= nw) break;
-            const int T = __ldcg(P.work + i);
-            const int inst = P.tile_inst[T];
             if (lane == 0) atomicExch(P.key + T, kInfBits);
             __threadfence();  // the key is cleared before the tile's pending cells are taken
             process_tile<Real, NFWD, NSYM, KIND>(P, T, s_vals[warp], lane, nxt, nslot, n_solves, acc);
@@ -365,7 +331,7 @@ class Resident final : public ResidentFamily {
     DeviceBuffer<unsigned> code_, vis_, tile_up_, flags_, live_, ctl_, age_;
     DeviceBuffer<Real> weight_, mult_, values_, cls_w_;
     DeviceBuffer<int8_t> cls_off_;
-    DeviceBuffer<int> tile_inst_, lists_, work_, dep_tile_, active_d_;
+    DeviceBuffer<int> tile_inst_, lists_, dep_tile_, active_d_;
     DeviceBuffer<unsigned long long> key_, maxval_, dep_mask_, dep_dmask_, rstat_, stats_;
     DeviceBuffer<DirtyWake> dirty_;
     DeviceBuffer<long long> dep_beg_, dep_end_, round_out_;
@@ -378,7 +344,7 @@ class Resident final : public ResidentFamily {
     long long round_ = 0;
     bool in_slice_ = false;
     cudaEvent_t done_ev_ = nullptr;           // end of the running slice
-    long long *h_ctl_ = nullptr;              // page-locked: round reached, status word
+    long long *h_ctl_ = nullptr;              // page-locked (pinned_words): round reached, status word
     std::unique_lock<std::mutex> coop_;       // the cooperative-launch lock, held during a slice
     struct Schedule {
         int sweeps = 2;
@@ -430,9 +396,6 @@ class Resident final : public ResidentFamily {
         P.bar_count = ctl_.get() + 6;
         P.bar_gen = ctl_.get() + 7;
         P.status = ctl_.get() + 8;
-        P.work = work_.get();
-        P.wcount = ctl_.get() + 11;
-        P.wclaim = ctl_.get() + 13;
         P.stats = stats_.get();
         P.max_rounds = (int)sched_.max_rounds;
         P.sweeps = sched_.sweeps;
@@ -468,7 +431,6 @@ class Resident final : public ResidentFamily {
             regrow(maxval_, ot, ct, 1, s);
             regrow(tile_up_, ot, ct, 1, s);
             regrow(lists_, ot, ct, 3, s);
-            work_.alloc(ct);  // per-round contents only
             regrow(flags_, ot, ct, 3, s);
             regrow(dep_beg_, ot, ct, 1, s);
             regrow(dep_end_, ot, ct, 1, s);
@@ -521,7 +483,7 @@ public:
         round_out_.alloc(1);
         for (int i = kMaxResident - 1; i >= 0; --i) free_slots_.push_back(i);
         resize(1 << 15, 1 << 20, SHARE ? 1 << 10 : 0, s);
-        HFM_CUDA(cudaHostAlloc((void **)&h_ctl_, 2 * sizeof(long long), cudaHostAllocDefault));
+        h_ctl_ = static_cast<long long *>(pinned_words(2 * sizeof(long long)));
         h_ctl_[0] = h_ctl_[1] = 0;
     }
 
@@ -879,7 +841,7 @@ public:
             if (kv.second.round_in >= 0) act.push_back(kv.first);
         if (act.empty()) return;
         HFM_CUDA(cudaMemcpyAsync(active_d_.get(), act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-        HFM_CUDA(cudaMemsetAsync(ctl_.get() + 9, 0, 6 * sizeof(unsigned), s));  // stop words, work list words
+        HFM_CUDA(cudaMemsetAsync(ctl_.get() + 9, 0, 2 * sizeof(unsigned), s));  // stop words
         Dev<Real> P = global_view();
         int dev = 0, nsm = 0, per_sm = 0;
         HFM_CUDA(cudaGetDevice(&dev));
@@ -1044,8 +1006,7 @@ public:
             in_slice_ = false;
             coop_.unlock();
         }
-        if (done_ev_) cudaEventDestroy(done_ev_);
-        if (h_ctl_) cudaFreeHost(h_ctl_);
+        if (done_ev_) cudaEventDestroy(done_ev_);  // h_ctl_ stays in the process's pool
     }
 };
 

@@ -143,6 +143,20 @@ Staging &staging() {
 
 }  // namespace
 
+void *pinned_words(size_t bytes) {
+    static std::mutex mu;
+    static char *pool = nullptr;
+    static size_t used = 0;
+    constexpr size_t kPool = size_t(64) << 10;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pool) HFM_CUDA(cudaHostAlloc((void **)&pool, kPool, cudaHostAllocDefault));
+    const size_t n = (bytes + 15) & ~size_t(15);
+    if (used + n > kPool) throw Error(HFM_ERR_NOMEM, "page-locked word pool spent");
+    void *p = pool + used;
+    used += n;
+    return p;
+}
+
 void staging_warm_up() {
     staging();
     copy_pool();

@@ -237,6 +237,11 @@ struct hfm_server {
         }
         hfm::current_stream() = stream;
         hfm::staging_warm_up();
+        // page-locked words of the families' solvers: set up now, before any slice runs
+        try {
+            hfm::pinned_words(0);
+        } catch (...) {
+        }
         std::deque<Request *> waiting;  // staged resident requests, not yet admitted (arrival order)
         std::deque<Request *> plain;    // requests for hfm_run
         std::map<std::string, std::unique_ptr<hfm::ResidentFamily>> fams;

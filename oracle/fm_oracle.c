@@ -1381,6 +1381,89 @@ done:
     return ret;
 }
 
+/* Order-independent restatement of the factored TTI update, for the fixed-point check of the
+ * parallel solvers: at each cell of `values` (a finished fast marching), the smallest of the local
+ * solves triggered, in fast marching, by the acceptance of each stencil neighbour y = x + e, taken in
+ * increasing value while below the result so far; each solve reads the neighbours of value at most
+ * that of y (the ones accepted by then), with the corrections. Seeds keep their values. */
+typedef struct {
+    tti_fm_ctx base;
+    double theta;
+} tti_prefix_ctx;
+
+static double tti_prefix_get(void *vctx, int64_t cell, const int *off) {
+    const tti_prefix_ctx *c = (const tti_prefix_ctx *)vctx;
+    const int64_t n1 = c->base.dims[1], n2 = c->base.dims[2];
+    const int64_t x0 = cell / (n1 * n2), x1 = (cell / n2) % n1, x2 = cell % n2;
+    const int64_t y0 = x0 + off[0], y1 = x1 + off[1], y2 = x2 + off[2];
+    if (y0 < 0 || y0 >= c->base.dims[0] || y1 < 0 || y1 >= n1 || y2 < 0 || y2 >= n2) return FMO_INF;
+    const double v = c->base.values[(y0 * n1 + y1) * n2 + y2];
+    if (!(v <= c->theta)) return FMO_INF;
+    double r = v;
+    if (c->base.fac && c->base.fac->fac_values) r += tti_fac_correction(c->base.fac, x0, x1, x2, off);
+    return r;
+}
+
+int fmo_tti_prefix_solve(const int64_t *dims, const double *h, const double *metric, const double *values,
+                         const uint8_t *is_seed, const fmo_problem *fac, double *out) {
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    enum { CAP = 64 };
+    int nb[CAP][3];
+    for (int64_t x = 0; x < N; ++x) {
+        if (is_seed[x]) { out[x] = values[x]; continue; }
+        tti_norm n;
+        if (tti_setup(metric + 14 * x, h, &n)) return -1;
+        const int k = tti_neighbors(&n, nb, CAP);
+        if (k < 0) return -1;
+        const int64_t x0 = x / (dims[1] * dims[2]), x1 = (x / dims[2]) % dims[1], x2 = x % dims[2];
+        double th[CAP];
+        int nth = 0;
+        for (int q = 0; q < k; ++q) {
+            const int64_t y0 = x0 + nb[q][0], y1 = x1 + nb[q][1], y2 = x2 + nb[q][2];
+            if (y0 < 0 || y0 >= dims[0] || y1 < 0 || y1 >= dims[1] || y2 < 0 || y2 >= dims[2]) continue;
+            const double v = values[(y0 * dims[1] + y1) * dims[2] + y2];
+            if (!(v < FMO_INF)) continue;
+            int i = nth++;
+            while (i > 0 && th[i - 1] > v) { th[i] = th[i - 1]; --i; }
+            th[i] = v;
+        }
+        double best = FMO_INF;
+        tti_prefix_ctx ctx = {{dims, values, NULL, fac}, 0.0};
+        for (int q = 0; q < nth; ++q) {
+            if (q > 0 && th[q] == th[q - 1]) continue;
+            if (!(th[q] < best)) break;
+            ctx.theta = th[q];
+            double ta = FMO_INF;
+            int in = 0;
+            const double v = tti_local_solve(&n, x, tti_prefix_get, &ctx, &ta, &in);
+            if (v < best) best = v;
+        }
+        out[x] = best;
+    }
+    return 0;
+}
+
+/* The fixed point of that form reached by Jacobi iteration from the seeds (the parallel solvers'
+ * result): values holds the seed values (and +inf elsewhere) on entry and the fixed point on exit.
+ * Returns the number of sweeps, or -1 (no fixed point within max_sweeps, or an invalid norm). */
+int fmo_tti_prefix_fixed_point(const int64_t *dims, const double *h, const double *metric, double *values,
+                               const uint8_t *is_seed, const fmo_problem *fac, int max_sweeps) {
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    double *nv = (double *)malloc(N * sizeof(double));
+    if (!nv) return -1;
+    int it = 0;
+    for (; it < max_sweeps; ++it) {
+        if (fmo_tti_prefix_solve(dims, h, metric, values, is_seed, fac, nv)) { it = -1; break; }
+        int same = 1;
+        for (int64_t x = 0; x < N; ++x)
+            if (nv[x] != values[x]) { same = 0; break; }
+        memcpy(values, nv, N * sizeof(double));
+        if (same) break;
+    }
+    free(nv);
+    return it < max_sweeps ? it : -1;
+}
+
 /* _HopfLaxRecompute at the stored extremum t (TTI.hpp:278-389, order 1): Riemannian update of the
  * Selling decomposition at t, its value and the discrete flow (offset * sign, (sol - v) w). */
 static double tti_recompute(const tti_norm *n, const int64_t *dims, const double *values, int64_t x, double t,

@@ -121,6 +121,11 @@ int64_t fmo_tti_backward_variation(const int64_t *dims, const double *h, const d
                                    int64_t max_seeds, int64_t *seed_out_index, double *seed_out_weight);
 /* Properties of one TTI norm: out = {tmin, tmax, optimDirection, Multiplier(tmin), Multiplier(tmax)}. */
 int fmo_tti_norm(const double *metric, const double *h, double *out);
+/* Fixed-point form of the (factored) TTI update over finished values; see fm_oracle.c. */
+int fmo_tti_prefix_solve(const int64_t *dims, const double *h, const double *metric, const double *values,
+                         const uint8_t *is_seed, const fmo_problem *fac, double *out);
+int fmo_tti_prefix_fixed_point(const int64_t *dims, const double *h, const double *metric, double *values,
+                               const uint8_t *is_seed, const fmo_problem *fac, int max_sweeps);
 
 /* Discrete geodesic backtracking from ntips tips (dimensionless coordinates: cell i spans [i, i+1)),
  * from the values and activeNeighs of fmo_fast_marching. points[max_points][ndim] receive the

@@ -98,6 +98,8 @@ def lib():
         L.fmo_tti_fast_marching_stop.argtypes = [_P, _P, _P, ctypes.c_int, _P, _P, _P, _P, ctypes.POINTER(_Problem)]
         L.fmo_tti_fast_marching_stop.restype = ctypes.c_int64
         L.fmo_tti_norm.argtypes = [_P, _P, _P]
+        L.fmo_tti_prefix_solve.argtypes = [_P, _P, _P, _P, _P, ctypes.POINTER(_Problem), _P]
+        L.fmo_tti_prefix_fixed_point.argtypes = [_P, _P, _P, _P, _P, ctypes.POINTER(_Problem), ctypes.c_int]
         L.fmo_tti_backward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int64,
                                                  _P, _P]
         L.fmo_tti_backward_variation.restype = ctypes.c_int64
@@ -507,7 +509,44 @@ def tti_solve(params: Dict) -> Dict:
     if nacc < 0:
         raise RuntimeError("oracle TTI fast marching failed")
     return {"values": values.reshape(dims), "activeNeighs": tact.reshape(dims), "nAccepted": int(nacc),
-            "_tti": (d, hs, metric, origin)}
+            "_tti": (d, hs, metric, origin), "_seeds": sidx, "_stop": (stop, keep) if has_stop else None}
+
+
+def tti_prefix_solve(res: Dict) -> np.ndarray:
+    """The TTI update of every cell recomputed from the finished values of a :func:`tti_solve`
+    result, in the order-independent form that the parallel solver iterates to (each neighbour's
+    acceptance triggering a solve over the neighbours at or below it, while below the result so
+    far), with the same static factor. Equal to the values when fast marching's result is a fixed
+    point of that form."""
+    d, hs, metric, origin = res["_tti"]
+    values = np.ascontiguousarray(res["values"].ravel(), float)
+    seed = np.zeros(values.size, np.uint8)
+    seed[res["_seeds"]] = 1
+    out = np.empty_like(values)
+    st = res["_stop"]
+    rc = lib().fmo_tti_prefix_solve(_ptr(d), _ptr(hs), _ptr(metric), _ptr(values), _ptr(seed),
+                                    ctypes.byref(st[0]) if st else None, _ptr(out))
+    if rc != 0:
+        raise RuntimeError("oracle TTI prefix solve failed")
+    return out.reshape(res["values"].shape)
+
+
+def tti_prefix_fixed_point(res: Dict, max_sweeps: int = 100000) -> np.ndarray:
+    """The fixed point of the order-independent TTI update (:func:`tti_prefix_solve`) reached by
+    Jacobi sweeps from the seeds of a :func:`tti_solve` result: what a parallel solver converges to.
+    With static factoring it can differ from fast marching, whose corrected updates are taken in
+    acceptance order; without it the two agree."""
+    d, hs, metric, origin = res["_tti"]
+    v = np.full(res["values"].size, np.inf)
+    seed = np.zeros(v.size, np.uint8)
+    seed[res["_seeds"]] = 1
+    v[res["_seeds"]] = res["values"].ravel()[res["_seeds"]]
+    st = res["_stop"]
+    it = lib().fmo_tti_prefix_fixed_point(_ptr(d), _ptr(hs), _ptr(metric), _ptr(v), _ptr(seed),
+                                          ctypes.byref(st[0]) if st else None, int(max_sweeps))
+    if it < 0:
+        raise RuntimeError("oracle TTI fixed point: no convergence")
+    return v.reshape(res["values"].shape)
 
 
 def tti_backward_variation(res: Dict, points, weights=None):

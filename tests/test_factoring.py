@@ -82,3 +82,25 @@ def test_factoring_argument_errors():
     with pytest.raises(H.PyExp) as e:  # Eulerian models: refused before any device work
         H.run(p)
     assert e.value.code == 3
+
+
+@pytest.mark.parametrize("name", COMPUTED + ["fac_tti3_16_import"])
+def test_factored_fast_marching_is_order_dependent(name):
+    """The corrected update is not causal: fast marching's factored result is not a fixed point of
+    the order-independent update at a few cells (the unfactored result is one everywhere), and the
+    Jacobi fixed point of that update stays within 3e-2 of the reference (relative max-norm)."""
+    q, ref = oracle_inputs(name)
+    res = O.tti_solve(q)
+    v = res["values"]
+    fin = np.isfinite(v)
+    again = O.tti_prefix_solve(res)
+    moved = int(np.sum(again[fin] != v[fin]))
+    assert 0 < moved <= 16
+    plain = dict(q)
+    plain.pop("_factor", None)
+    plain.pop("_factor_mask", None)
+    r0 = O.tti_solve(plain)
+    assert np.array_equal(O.tti_prefix_solve(r0), r0["values"])
+    fp = O.tti_prefix_fixed_point(res)
+    a = ref["values"]
+    assert np.max(np.abs(fp[fin] - a[fin])) / np.max(np.abs(a[fin])) <= 3e-2
