@@ -687,6 +687,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
     if (KIND != kKindTTI && P.skip_settled) lim = __longlong_as_double(__shfl_sync(0xffffffffu, wk, 0));
     __threadfence();
     Real cur[2];
+    [[maybe_unused]] Real first[2];  // TTI3: the values before the activation (see the wake-up key)
     bool upd[2], todo[2], chg[2] = {false, false};
     unsigned long long reads[2] = {0ull, 0ull};
     int xs[2][3];
@@ -707,6 +708,7 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
         upd[j] = valid && !dead && !fixed;
         todo[j] = upd[j] && ((dirty >> l) & 1ull) && (double)cur[j] > lim;
         sv[l] = cur[j];
+        if constexpr (KIND == kKindTTI) first[j] = cur[j];
     }
     // nothing to solve (every dirty cell settled): the values and the tile's largest value stand
     if (!__any_sync(0xffffffffu, todo[0] || todo[1])) return;
@@ -797,11 +799,17 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 #pragma unroll
     for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) __stcg(P.maxval + T, (unsigned long long)__double_as_longlong(mx));
-    // smallest changed value: the wake-up key of the dependents
+    // smallest changed value: the wake-up key of the dependents. A TTI3 update can rise (static
+    // factoring makes it non-monotone), and a neighbour that rose may have been below a dependent's
+    // value before: the smaller of the old and new values wakes the dependents then.
     double mu = Arith<double>::inf();
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
-        if (chg[j] && (double)cur[j] < mu) mu = (double)cur[j];
+    for (int j = 0; j < 2; ++j) {
+        if (!chg[j]) continue;
+        double m = (double)cur[j];
+        if constexpr (KIND == kKindTTI) m = (double)first[j] < m ? (double)first[j] : m;
+        mu = m < mu ? m : mu;
+    }
 #pragma unroll
     for (int o = 16; o; o >>= 1) mu = fmin(mu, __shfl_xor_sync(0xffffffffu, mu, o));
     __threadfence();
@@ -1733,8 +1741,8 @@ struct AdjDev {
     double *acc;             // inspection weights
     double *sens;
     int var_dim;             // components of var / sens per cell
-    int *list[3];
-    unsigned *count[3];
+    int *list[3];            // list[0]: the ready queue (the three point at it)
+    unsigned *count[3];      // [0] cells queued, [1] slots claimed
     long long *seed_idx;
     double *seed_w;
     unsigned *seed_count;
@@ -1742,8 +1750,7 @@ struct AdjDev {
     unsigned *bar_count;
     unsigned *bar_gen;
     unsigned *status;
-    unsigned long long *rounds;
-    long long max_rounds;
+    unsigned long long *processed;  // cells processed (diagnostics)
 };
 
 __global__ void adjoint_roots_kernel(AdjDev A) {
@@ -1758,60 +1765,81 @@ __global__ void adjoint_roots_kernel(AdjDev A) {
     if (want) A.list[0][base + __popc(bal & ((1u << lane) - 1u))] = (int)x;
 }
 
+// The sweeps run over a ready queue instead of rounds: list[0] holds every cell once, in the order
+// the cells become ready (count[0] of them so far, the slots beyond still -1); warps claim 32 slots
+// at a time (count[1]) and each lane processes its cell as soon as its slot is filled, so a cell is
+// processed one queue hop after its last dependency and no grid barrier separates fronts. Every
+// cell is pushed exactly once and the graph is acyclic, so a claimed slot is always filled by a
+// cell whose own dependencies other warps are processing (all blocks are resident: cooperative
+// launch). A warp that sees no progress for kQueuePolls polls sets kErrBarrierTimeout and leaves.
+constexpr unsigned long long kQueuePolls = 1ull << 24;
+
+__device__ __forceinline__ void queue_push(int *q, unsigned *tail, bool want, int v, int lane) {
+    const unsigned bal = __ballot_sync(0xffffffffu, want);
+    if (!bal) return;
+    unsigned base = 0;
+    if (lane == __ffs(bal) - 1) base = atomicAdd(tail, (unsigned)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+    if (want) ((volatile int *)q)[base + __popc(bal & ((1u << lane) - 1u))] = v;
+}
+
 __global__ void adjoint_kernel(AdjDev A) {
-    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long nth = (long long)gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
-    long long r = 0;
-    bool ok = true;
-    for (; r < A.max_rounds; ++r) {
-        const int cur = (int)(r % 3), nxt = (int)((r + 1) % 3), old = (int)((r + 2) % 3);
-        if (blockIdx.x == 0 && threadIdx.x == 0) *A.count[old] = 0;
-        const long long n = *(volatile unsigned *)A.count[cur];
-        const long long nround = (n + 31) / 32 * 32;
-        for (long long i = tid; i < nround; i += nth) {
+    int *q = A.list[0];
+    unsigned long long processed = 0;
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(A.count[1], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((long long)base >= A.N) break;
+        const long long i = (long long)base + lane;
+        bool pending = i < A.N;
+        unsigned long long idle = 0;
+        while (__any_sync(0xffffffffu, pending)) {
             int x = -1;
-            if (i < n) x = A.list[cur][i];
+            if (pending) x = ((volatile int *)q)[i];
+            const bool ready = pending && x >= 0;
+            if (!__any_sync(0xffffffffu, ready)) {
+                if (++idle > kQueuePolls) {
+                    if (lane == 0) atomicOr(A.status, (unsigned)kErrBarrierTimeout);
+                    return;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            idle = 0;
+            __threadfence();  // the downstream values written before this cell was queued
             int nf = 0;
-            double lam = 0.0;
-            if (x >= 0) {
-                lam = __ldcg(A.acc + x);
+            if (ready) {
+                double lam = __ldcg(A.acc + x);
                 for (long long k = A.rptr[x], e = A.rptr[x + 1]; k < e; ++k)
                     lam = __dadd_rn(lam, __dmul_rn(A.rw[k], __ldcg(A.lam + A.rx[k])));
                 __stcg(A.lam + x, lam);
                 nf = A.nflow[x];
-                __threadfence();
                 if (lam != 0.0) {
-                    for (int i = 0; i < A.var_dim; ++i) A.sens[(long long)x * A.var_dim + i] = lam * A.var[(long long)x * A.var_dim + i];
+                    for (int v = 0; v < A.var_dim; ++v)
+                        A.sens[(long long)x * A.var_dim + v] = lam * A.var[(long long)x * A.var_dim + v];
                     if (nf == 0) {
                         const unsigned si = atomicAdd(A.seed_count, 1u);
                         if (si < A.seed_cap) { A.seed_idx[si] = x; A.seed_w[si] = lam; }
                     }
                 }
+                __threadfence();
+                ++processed;
             }
-            for (int j = 0; j < 32; ++j) {
+            for (int j = 0; __any_sync(0xffffffffu, j < nf); ++j) {
                 bool want = false;
                 int y = 0;
                 if (j < nf) {
                     y = A.fidx[j * A.N + x];
                     want = atomicSub(A.indeg + y, 1) == 1;
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, want);
-                if (bal) {
-                    unsigned base = 0;
-                    if (lane == __ffs(bal) - 1) base = atomicAdd(A.count[nxt], (unsigned)__popc(bal));
-                    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
-                    if (want) A.list[nxt][base + __popc(bal & ((1u << lane) - 1u))] = y;
-                }
-                if (!__any_sync(0xffffffffu, j + 1 < nf)) break;
+                queue_push(q, A.count[0], want, y, lane);
             }
+            if (ready) pending = false;
         }
-        ok = grid_barrier(A.bar_count, A.bar_gen, gridDim.x, A.status, kBarrierPolls);
-        if (!ok) break;
-        if (*(volatile unsigned *)A.count[nxt] == 0u) { ++r; break; }
     }
-    if (ok && r >= A.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(A.status, (unsigned)kErrRoundCap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *A.rounds = (unsigned long long)r;
+    if (processed) atomicAdd(A.processed, processed);
 }
 
 // Reverse adjacency of the upwind graph: for every cell y, the (downwind cell, weight) pairs of
@@ -1920,7 +1948,7 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     DeviceBuffer<double> &fw = G.fw, &var = G.var, &rw = G.rw;
     DeviceBuffer<uint8_t> &nflow = G.nflow;
     DeviceBuffer<long long> &rptr = G.rptr;
-    DeviceBuffer<int> lists(3 * N);
+    DeviceBuffer<int> queue(N);
     DeviceBuffer<unsigned> counters(8);
     const unsigned seed_cap = 1u << 20;
     DeviceBuffer<long long> seed_idx(seed_cap);
@@ -1940,7 +1968,7 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     A.acc = acc.get();
     A.sens = sens.get();
     A.var_dim = vdim;
-    for (int i = 0; i < 3; ++i) { A.list[i] = lists.get() + i * N; A.count[i] = counters.get() + i; }
+    for (int i = 0; i < 3; ++i) { A.list[i] = queue.get(); A.count[i] = counters.get() + i; }
     A.seed_count = counters.get() + 3;
     A.bar_count = counters.get() + 4;
     A.bar_gen = counters.get() + 5;
@@ -1948,8 +1976,7 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     A.seed_w = seed_w.get();
     A.seed_cap = seed_cap;
     A.status = status.get();
-    A.rounds = rounds.get();
-    A.max_rounds = N + 2;
+    A.processed = rounds.get();
     int dev = 0, nsm = 0, per_sm = 0;
     HFM_CUDA(cudaGetDevice(&dev));
     HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1961,6 +1988,8 @@ void run_adjoint(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
         acc.zero(s);
         sens.zero(s);
         counters.zero(s);
+        rounds.zero(s);
+        HFM_CUDA(cudaMemsetAsync(queue.get(), 0xff, N * sizeof(int), s));  // empty slots read -1
         // std::map::insert keeps the first weight of a repeated point
         std::vector<double> hacc_w;
         std::vector<long long> hacc_i;
@@ -2029,8 +2058,7 @@ struct FwdDev {
     unsigned *bar_count;
     unsigned *bar_gen;
     unsigned *status;
-    unsigned long long *rounds;
-    long long max_rounds;
+    unsigned long long *processed;  // cells processed (diagnostics)
 };
 
 __global__ void forward_roots_kernel(FwdDev F) {
@@ -2046,30 +2074,42 @@ __global__ void forward_roots_kernel(FwdDev F) {
 }
 
 __global__ void forward_kernel(FwdDev F) {
-    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long nth = (long long)gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
-    long long r = 0;
-    bool ok = true;
-    for (; r < F.max_rounds; ++r) {
-        const int cur = (int)(r % 3), nxt = (int)((r + 1) % 3), old = (int)((r + 2) % 3);
-        if (blockIdx.x == 0 && threadIdx.x == 0) *F.count[old] = 0;
-        const long long n = *(volatile unsigned *)F.count[cur];
-        const long long nround = (n + 31) / 32 * 32;
-        for (long long i = tid; i < nround; i += nth) {
+    int *q = F.list[0];
+    unsigned long long processed = 0;
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(F.count[1], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((long long)base >= F.N) break;
+        const long long i = (long long)base + lane;
+        bool pending = i < F.N;
+        unsigned long long idle = 0;
+        while (__any_sync(0xffffffffu, pending)) {
             int x = -1;
-            if (i < n) x = F.list[cur][i];
+            if (pending) x = ((volatile int *)q)[i];
+            const bool ready = pending && x >= 0;
+            if (!__any_sync(0xffffffffu, ready)) {
+                if (++idle > kQueuePolls) {
+                    if (lane == 0) atomicOr(F.status, (unsigned)kErrBarrierTimeout);
+                    return;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            idle = 0;
+            __threadfence();  // the upwind results written before this cell was queued
             long long e = 0, ee = 0;
-            if (x >= 0) {
+            if (ready) {
                 const int nf = F.nflow[x];
                 const int vd = F.var_dim;
                 for (int k = 0; k < F.nvar; ++k) {
                     double acc = __ldcg(F.res + (long long)x * F.nvar + k);
                     // the local derivative paired with the cost variation (DiffHelper::Scal)
                     double sc = 0.0;
-                    for (int i = 0; i < vd; ++i)
-                        sc = __dadd_rn(sc, __dmul_rn(F.var[(long long)x * vd + i],
-                                                     F.cost ? F.cost[((long long)x * F.nvar + k) * vd + i] : 0.0));
+                    for (int v = 0; v < vd; ++v)
+                        sc = __dadd_rn(sc, __dmul_rn(F.var[(long long)x * vd + v],
+                                                     F.cost ? F.cost[((long long)x * F.nvar + k) * vd + v] : 0.0));
                     acc = __dadd_rn(acc, sc);
                     for (int j = 0; j < nf; ++j) {
                         const long long y = F.fidx[j * F.N + x];
@@ -2080,8 +2120,9 @@ __global__ void forward_kernel(FwdDev F) {
                 __threadfence();
                 e = F.rptr[x];
                 ee = F.rptr[x + 1];
+                ++processed;
             }
-            // downwind cells whose last pending input this was join the next round
+            // downwind cells whose last pending input this was join the queue
             while (__any_sync(0xffffffffu, e < ee)) {
                 bool want = false;
                 int z = 0;
@@ -2090,21 +2131,12 @@ __global__ void forward_kernel(FwdDev F) {
                     want = atomicSub(F.cnt + z, 1) == 1;
                     ++e;
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, want);
-                if (bal) {
-                    unsigned base = 0;
-                    if (lane == __ffs(bal) - 1) base = atomicAdd(F.count[nxt], (unsigned)__popc(bal));
-                    base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
-                    if (want) F.list[nxt][base + __popc(bal & ((1u << lane) - 1u))] = z;
-                }
+                queue_push(q, F.count[0], want, z, lane);
             }
+            if (ready) pending = false;
         }
-        ok = grid_barrier(F.bar_count, F.bar_gen, gridDim.x, F.status, kBarrierPolls);
-        if (!ok) break;
-        if (*(volatile unsigned *)F.count[nxt] == 0u) { ++r; break; }
     }
-    if (ok && r >= F.max_rounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(F.status, (unsigned)kErrRoundCap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *F.rounds = (unsigned long long)r;
+    if (processed) atomicAdd(F.processed, processed);
 }
 
 __global__ void nflow_to_count_kernel(long long N, const uint8_t *nflow, int *cnt) {
@@ -2126,10 +2158,12 @@ void run_forward(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
         cost.alloc((size_t)N * nvar * vdim);
         cost.upload(p.fwd_cost.data(), (size_t)N * nvar * vdim, s);
     }
-    DeviceBuffer<int> cnt(N), lists(3 * N);
+    DeviceBuffer<int> cnt(N), queue(N);
     DeviceBuffer<unsigned> counters(8);
     DeviceBuffer<unsigned long long> rounds(1);
     counters.zero(s);
+    rounds.zero(s);
+    HFM_CUDA(cudaMemsetAsync(queue.get(), 0xff, N * sizeof(int), s));  // empty slots read -1
     launch(nflow_to_count_kernel, nblocks(N, 256), 256, 0, s, N, G.nflow.get(), cnt.get());
     FwdDev F{};
     F.N = N;
@@ -2144,12 +2178,11 @@ void run_forward(const Dev<Real> &P, long long N, const EulerProblem &p, EulerRe
     F.var_dim = vdim;
     F.res = out.get();
     F.cnt = cnt.get();
-    for (int i = 0; i < 3; ++i) { F.list[i] = lists.get() + i * N; F.count[i] = counters.get() + i; }
+    for (int i = 0; i < 3; ++i) { F.list[i] = queue.get(); F.count[i] = counters.get() + i; }
     F.bar_count = counters.get() + 4;
     F.bar_gen = counters.get() + 5;
     F.status = status.get();
-    F.rounds = rounds.get();
-    F.max_rounds = N + 2;
+    F.processed = rounds.get();
     int dev = 0, nsm = 0, per_sm = 0;
     HFM_CUDA(cudaGetDevice(&dev));
     HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
