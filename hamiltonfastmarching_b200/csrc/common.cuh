@@ -27,6 +27,7 @@ enum : unsigned {
     kErrRoundCap = 2u,         // the solver exceeded its round cap
     kErrTableOverflow = 4u,    // a tile's dependency table overflowed
     kErrSelling = 8u,          // Selling did not terminate / non positive definite metric
+    kErrIndexRange = 16u,      // a flow or queue index left its array (the access was skipped)
 };
 
 // ------------------------------------------------------------------------------------------

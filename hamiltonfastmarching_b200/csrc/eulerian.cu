@@ -580,8 +580,10 @@ __device__ __forceinline__ void push_dependents(const Dev<Real> &P, int li, int 
                 D = P.dep_tile[i];
                 want = (P.dep_mask[i] & mask) != 0ull;
                 // a neighbour value v improves x only if v < u(x) (ConditionalUpdate,
-                // HamiltonFastMarching.hxx:151): no cell of D can gain from values >= max u(D)
-                if (want) {
+                // HamiltonFastMarching.hxx:151): no cell of D can gain from values >= max u(D).
+                // Not with static factoring: D's values can rise during an activation that has not
+                // yet published its larger maximum, so a stale maximum would drop a needed wake-up
+                if (want && !P.fac_val) {
                     const double mx = __longlong_as_double(__ldcg(P.maxval + D));
                     want = __longlong_as_double(mu) < mx * (1.0 + 16.0 * DBL_EPSILON);
                 }
@@ -1528,6 +1530,7 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
     if (st & kErrBarrierTimeout)
         throw Error(HFM_ERR_NOT_CONVERGED, std::string(phase) + ": a grid barrier wait exceeded its limit");
     if (st & kErrRoundCap) throw Error(HFM_ERR_NOT_CONVERGED, std::string(phase) + ": round cap reached before convergence");
+    if (st & kErrIndexRange) throw Error(HFM_ERR_CUDA, std::string(phase) + ": a flow index left its array");
 }
 
 // --------------------------------------------------------------------------------------------
@@ -1688,7 +1691,10 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
             if (!((act >> si) & 1u)) continue;
             const int s = si ? -1 : 1;
             int y0 = x0 + s * o0, y1 = x1 + s * o1, y2 = x2 + s * o2;
-            g.wrap(y0, y1, y2);
+            if (!g.wrap(y0, y1, y2)) {  // an active neighbour is inside the grid
+                atomicOr(P.status, (unsigned)kErrIndexRange);
+                continue;
+            }
             const long long y = g.lin(y0, y1, y2);
             const double d = A::sub(u, (double)P.values[y]);
             const double vd = 0.0 < d ? d : 0.0;
@@ -1798,8 +1804,14 @@ __global__ void adjoint_kernel(AdjDev A) {
         while (__any_sync(0xffffffffu, pending)) {
             int x = -1;
             if (pending) x = ((volatile int *)q)[i];
+            if (x >= A.N) {  // a queued cell is a cell of the grid
+                atomicOr(A.status, (unsigned)kErrIndexRange);
+                x = -1;
+                pending = false;
+            }
             const bool ready = pending && x >= 0;
             if (!__any_sync(0xffffffffu, ready)) {
+                if (!__any_sync(0xffffffffu, pending)) break;
                 if (++idle > kQueuePolls) {
                     if (lane == 0) atomicOr(A.status, (unsigned)kErrBarrierTimeout);
                     return;
@@ -1832,7 +1844,8 @@ __global__ void adjoint_kernel(AdjDev A) {
                 int y = 0;
                 if (j < nf) {
                     y = A.fidx[j * A.N + x];
-                    want = atomicSub(A.indeg + y, 1) == 1;
+                    if ((unsigned)y < (unsigned)A.N) want = atomicSub(A.indeg + y, 1) == 1;
+                    else atomicOr(A.status, (unsigned)kErrIndexRange);
                 }
                 queue_push(q, A.count[0], want, y, lane);
             }
@@ -2088,8 +2101,14 @@ __global__ void forward_kernel(FwdDev F) {
         while (__any_sync(0xffffffffu, pending)) {
             int x = -1;
             if (pending) x = ((volatile int *)q)[i];
+            if (x >= F.N) {  // a queued cell is a cell of the grid
+                atomicOr(F.status, (unsigned)kErrIndexRange);
+                x = -1;
+                pending = false;
+            }
             const bool ready = pending && x >= 0;
             if (!__any_sync(0xffffffffu, ready)) {
+                if (!__any_sync(0xffffffffu, pending)) break;
                 if (++idle > kQueuePolls) {
                     if (lane == 0) atomicOr(F.status, (unsigned)kErrBarrierTimeout);
                     return;
@@ -2128,7 +2147,8 @@ __global__ void forward_kernel(FwdDev F) {
                 int z = 0;
                 if (e < ee) {
                     z = F.rx[e];
-                    want = atomicSub(F.cnt + z, 1) == 1;
+                    if ((unsigned)z < (unsigned)F.N) want = atomicSub(F.cnt + z, 1) == 1;
+                    else atomicOr(F.status, (unsigned)kErrIndexRange);
                     ++e;
                 }
                 queue_push(q, F.count[0], want, z, lane);

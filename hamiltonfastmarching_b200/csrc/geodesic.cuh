@@ -394,10 +394,11 @@ __device__ int geodesic_pass(const Dev<Real> &P, const Inst &I, const GeoRec &R,
         geo_unpack(bk, ind);
         sums(-ew, ind);
         int q0 = ind[0], q1 = ind[1], q2 = ind[2];
-        g.wrap(q0, q1, q2);
         // the extracted cell's flow, from the records computed for every cell before the launch
+        // (entries are cells of the grid: a failed wrap is reported, not read)
+        if (!g.wrap(q0, q1, q2)) { status |= kGeoRange; return 0; }
         const long long gx = I.cell0 + g.lin(q0, q1, q2);
-        const int nf = R.nf[gx];
+        const int nf = R.nf[gx] < kGeoMaxFlow ? R.nf[gx] : kGeoMaxFlow;
         if (lane < nf) {
             S.foff[lane] = R.foff[lane * R.N + gx];
             S.fw[lane] = R.fw[lane * R.N + gx];
