@@ -4,7 +4,7 @@ FileHFM-compatible command-line front-end, for sm_100a only.
     python -m hamiltonfastmarching_b200.build [--force] [--jobs N]
 
 Each CUDA translation unit is compiled separately (parallel) with
-``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked with the static CUDA runtime,
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -fmad=false`` and linked with the static CUDA runtime,
 so the library carries no dependency on torch. Outputs live next to this file.
 """
 from __future__ import annotations
@@ -36,7 +36,9 @@ def nvcc() -> str:
 
 
 def _flags(extra=()):
-    return ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
+    # -fmad=false: device arithmetic rounds every product and sum, as the reference's x86-64 build
+    # does (no fused multiply-add); the Selling decompositions of the TTI3 path depend on it
+    return ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
             "-I", os.path.join(ROOT, "include"), *ARCH, *extra]
 
 

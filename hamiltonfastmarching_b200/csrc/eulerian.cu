@@ -218,11 +218,76 @@ __device__ __forceinline__ Real quad_root(Real minVal, Real a, Real b, Real c) {
     return A::add(minVal, A::div(A::add(b, d), a));
 }
 
+// Compare-exchange of (value, index) pairs by value, then index: a total order, so a sorting
+// network gives the selection order of the loop below (smallest value, ties by index).
+template <typename Real>
+__device__ __forceinline__ void cex(Real &va, Real &wa, int &ka, Real &vb, Real &wb, int &kb) {
+    const bool sw = vb < va || (vb == va && kb < ka);
+    const Real tv = sw ? vb : va, tw = sw ? wb : wa;
+    const int tk = sw ? kb : ka;
+    vb = sw ? va : vb;
+    wb = sw ? wa : wb;
+    kb = sw ? ka : kb;
+    va = tv;
+    wa = tw;
+    ka = tk;
+}
+
+// Optimal sorting networks for the small stencils (2, 3, 4 and 6 differences).
 template <typename Real, int ND>
-__device__ __forceinline__ Real hopf_lax_sorted(const Real (&v)[ND], const Real (&w)[ND], unsigned *used) {
+__device__ __forceinline__ void sort_candidates(Real (&v)[ND], Real (&w)[ND], int (&k)[ND]) {
+#define HFM_CX(a, b) cex<Real>(v[a], w[a], k[a], v[b], w[b], k[b])
+    if constexpr (ND == 2) {
+        HFM_CX(0, 1);
+    } else if constexpr (ND == 3) {
+        HFM_CX(1, 2); HFM_CX(0, 2); HFM_CX(0, 1);
+    } else if constexpr (ND == 4) {
+        HFM_CX(0, 1); HFM_CX(2, 3); HFM_CX(0, 2); HFM_CX(1, 3); HFM_CX(1, 2);
+    } else if constexpr (ND == 6) {
+        HFM_CX(1, 2); HFM_CX(0, 2); HFM_CX(0, 1); HFM_CX(4, 5); HFM_CX(3, 5); HFM_CX(3, 4);
+        HFM_CX(0, 3); HFM_CX(1, 4); HFM_CX(2, 5); HFM_CX(2, 4); HFM_CX(1, 3); HFM_CX(2, 3);
+    }
+#undef HFM_CX
+}
+
+template <typename Real, int ND>
+__device__ __forceinline__ Real hopf_lax_sorted(const Real (&v_in)[ND], const Real (&w_in)[ND], unsigned *used) {
     using A = Arith<Real>;
     const Real INF = A::inf();
     const Real band = sizeof(Real) == 8 ? Real(1e-12) : Real(1e-5);
+    if constexpr (ND == 2 || ND == 3 || ND == 4 || ND == 6) {
+        // the same additions in the same order as the selection loop below, on sorted candidates
+        Real v[ND], w[ND];
+        int k[ND];
+#pragma unroll
+        for (int i = 0; i < ND; ++i) { v[i] = v_in[i]; w[i] = w_in[i]; k[i] = i; }
+        sort_candidates<Real, ND>(v, w, k);
+        unsigned taken = 0;
+        Real minVal = v[0], a = 0, b = 0, c = -1;
+#pragma unroll
+        for (int it = 0; it < ND; ++it) {
+            const Real bv = v[it], bw = w[it];
+            if (!(bv < INF)) break;
+            if (it > 0) {
+                const Real t = A::sub(bv, minVal);
+                const Real at2 = A::mul(A::mul(a, t), t), bt2 = A::mul(Real(2), A::mul(b, t));
+                const Real q = A::add(A::sub(at2, bt2), c);
+                const Real mag = A::add(A::add(fabs(at2), fabs(bt2)), fabs(c));
+                if (q > band * mag) break;
+                if (!(q < -band * mag) && !(bv < quad_root<Real>(minVal, a, b, c))) break;
+            }
+            const Real dv = A::sub(bv, minVal);
+            const Real wv = A::mul(bw, dv);
+            a = A::add(a, bw);
+            b = A::add(b, wv);
+            c = A::add(c, A::mul(wv, dv));
+            taken |= 1u << k[it];
+        }
+        if (used) *used = taken;
+        return taken ? quad_root<Real>(minVal, a, b, c) : INF;
+    }
+    const Real (&v)[ND] = v_in;
+    const Real (&w)[ND] = w_in;
     unsigned taken = 0;
     Real minVal = 0, a = 0, b = 0, c = -1;
     for (int it = 0; it < ND; ++it) {

@@ -55,14 +55,8 @@ struct Request {
     std::unique_ptr<hfm::PreparedRun> prep;
     std::unique_ptr<hfm::StagedInputs> staged;  // device copies of its large inputs, until admission
     std::string family;
-    long long cells = 0;
 };
 
-// Instances up to this many cells are built beside a running slice (on the few SMs it leaves
-// free); larger ones wait for the slice to end, when the build has the whole GPU.
-constexpr long long kBesideSliceCells = 1ll << 20;
-// Time spent building instances between two slices before the next slice starts (at least one).
-constexpr double kBetweenSlicesMs = 3.0;
 
 // Device bytes of a request: per-cell solver state of its model and precision (stencil codes and
 // weights or visibility words, values, the FP64 metric or speed field on upload, output staging),
@@ -188,8 +182,6 @@ struct hfm_server {
                 try {
                     r->prep = hfm::prepare_run(r->io);
                     r->family = r->prep->skip() ? std::string() : hfm::resident_family_key(r->prep->problem());
-                    const hfm::EulerProblem &pb = r->prep->problem();
-                    r->cells = (long long)pb.dims[0] * pb.dims[1] * pb.dims[2];
                     if (!r->family.empty()) {
                         {
                             std::unique_lock<std::mutex> lk(mu);
@@ -281,17 +273,11 @@ struct hfm_server {
             fams.erase(key);
         };
         // Admits waiting requests in arrival order, by memory budget and free slots, at most `limit`
-        // of them and, past the first, for at most `budget_ms`; each is built on the side stream.
-        // The family `running_key` has a slice in flight and cannot grow its arena meanwhile.
-        // Returns true when the head of the queue waits for the running slice to end.
-        auto admit_waiting = [&](const std::string &running_key, size_t limit, double budget_ms) -> bool {
-            const Clock::time_point ta = Clock::now();
+        // of them; each is built on the side stream. The family `running_key` has a slice in flight
+        // and cannot grow its arena meanwhile: true when a request of it waits for that.
+        auto admit_waiting = [&](const std::string &running_key, size_t limit) -> bool {
             for (size_t n = 0; n < limit && !waiting.empty(); ++n) {
-                if (n > 0 && budget_ms > 0 &&
-                    std::chrono::duration<double, std::milli>(Clock::now() - ta).count() >= budget_ms)
-                    break;
                 Request *r = waiting.front();
-                if (!running_key.empty() && r->cells > kBesideSliceCells) return true;
                 {
                     std::lock_guard<std::mutex> lk(mu);
                     if ((in_use > 0 && in_use + r->bytes > budget) || resident >= (unsigned long long)cfg.max_batch)
@@ -363,7 +349,7 @@ struct hfm_server {
             // its minimum time), or, after 4 ms, when other work waits
             std::vector<std::pair<std::string, int64_t>> finished;
             if (!cur.empty()) {
-                const bool want_stop = admit_waiting(cur, 1, 0.0);
+                const bool want_stop = admit_waiting(cur, 1);
                 hfm::ResidentFamily &F = *fams[cur];
                 const double el = std::chrono::duration<double, std::milli>(Clock::now() - slice_t0).count();
                 bool others = !plain.empty() || want_stop;
@@ -393,7 +379,7 @@ struct hfm_server {
             }
             // ---- no slice in flight: admission (arenas may grow), single solves, the next slice
             if (cur.empty()) {
-                admit_waiting(std::string(), waiting.size(), kBetweenSlicesMs);
+                admit_waiting(std::string(), waiting.size());
                 while (!plain.empty()) {
                     Request *r = plain.front();
                     plain.pop_front();
