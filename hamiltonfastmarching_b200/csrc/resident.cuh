@@ -24,6 +24,7 @@
 
 constexpr int kMaxResident = 256;  // instance slots of a family (per-instance statistics rows)
 constexpr int kAdmissionSms = 8;   // SMs' worth of capacity a slice leaves to admission kernels
+constexpr int kSliceCarveoutPct = 50;  // shared-memory carveout of a slice's SMs, percent of the maximum
 
 // A request's large inputs on the device: the FP64 metric (Riemann models) or speed multiplier
 // (shared-stencil models) in the input's row-major order, and the walls as bytes.
@@ -846,6 +847,14 @@ public:
         int dev = 0, nsm = 0, per_sm = 0;
         HFM_CUDA(cudaGetDevice(&dev));
         HFM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        // the SMs that run a slice keep shared memory for the admission kernels beside it (their
+        // dependency tables): without this the carveout can be sized for the slice's blocks alone,
+        // and an admission waits for the slice to end
+        static std::once_flag carveout;
+        std::call_once(carveout, [] {
+            HFM_CUDA(cudaFuncSetAttribute(fim_resident_kernel<Real, NFWD, NSYM, KIND>,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout, kSliceCarveoutPct));
+        });
         HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fim_resident_kernel<Real, NFWD, NSYM, KIND>,
                                                                kWarpsPerCta * 32, 0));
         if (per_sm < 1) throw Error(HFM_ERR_CUDA, "resident solver kernel cannot be resident");

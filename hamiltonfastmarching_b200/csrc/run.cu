@@ -1306,6 +1306,11 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     q.export_stencils = read_export_stencils(io, q);
     if (inspect) read_inspect(io, pm, p);
     read_forward_variation(io, pm, p);
+    // Dubins2 first variations and geodesics: an illegal memory access was met twice on the GPU on
+    // a fixture with both (its cause is not found); they stay off the device until it is
+    if (p.nmax == 2 && (inspect || p.fwd_nvar > 0 || !p.geo_tips.empty() || !p.geo_tips_unoriented.empty() ||
+                        p.want_geodesic_flow))
+        throw Error(HFM_ERR_UNSUPPORTED, "Dubins2 first variations and geodesics are not supported by the GPU solve path");
     if (p.has_factoring() && (inspect || p.fwd_nvar > 0 || p.has_stopping() || !p.geo_tips.empty() ||
                               p.want_geodesic_flow || p.bypass || p.retain))
         throw Error(HFM_ERR_UNSUPPORTED, "static factoring with first variations, geodesics, stopping criteria, cached "
