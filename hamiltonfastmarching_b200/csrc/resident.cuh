@@ -24,7 +24,7 @@
 
 constexpr int kMaxResident = 256;  // instance slots of a family (per-instance statistics rows)
 constexpr int kAdmissionSms = 8;   // SMs' worth of capacity a slice leaves to admission kernels
-constexpr int kSliceCarveoutPct = 50;  // shared-memory carveout of a slice's SMs, percent of the maximum
+constexpr int kSliceCarveoutPct = 100;  // shared-memory carveout of a slice's SMs, percent of the maximum
 
 // A request's large inputs on the device: the FP64 metric (Riemann models) or speed multiplier
 // (shared-stencil models) in the input's row-major order, and the walls as bytes.
@@ -698,6 +698,15 @@ public:
                    (const long long *)sidx.get(), (const double *)sval.get(), (int)hsi.size());
             // ---- reverse tile dependencies (local CSR), then into the arena's entry space
             DeviceBuffer<unsigned> dcnt(nt);
+            // the dependency kernels hold shared-memory tables: they ask for the slice's carveout, so
+            // that an SM running slice blocks is already split the way they want
+            static std::once_flag deps_carveout;
+            std::call_once(deps_carveout, [] {
+                HFM_CUDA(cudaFuncSetAttribute(deps_kernel<Real, NFWD, NSYM, KIND, kDepCapSmall, kDepWarpsSmall>,
+                                              cudaFuncAttributePreferredSharedMemoryCarveout, kSliceCarveoutPct));
+                HFM_CUDA(cudaFuncSetAttribute(deps_kernel<Real, NFWD, NSYM, KIND, kDepCapLarge, kDepWarpsLarge>,
+                                              cudaFuncAttributePreferredSharedMemoryCarveout, kSliceCarveoutPct));
+            });
             auto deps_pass = [&](bool large, int pass, const long long *offs, int *src, int *dst, unsigned long long *msk,
                                  unsigned long long *dmsk) {
                 if (large)

@@ -231,6 +231,41 @@ def curvature2_case(n: int = 128, ntheta: int = 60, model: str = "ReedsShepp2", 
     }
 
 
+def reedsshepp3_case(n: int = 32, ntheta: int = 8, seed: int = 6, xi: float = 0.3, eps: float = 0.1,
+                     dual: bool = False, projective: bool = False, cost: str = "spatial", n_seeds: int = 1) -> Dict:
+    """ReedsShepp3 on the grid (x, y, z, theta, phi) of n^3 x ntheta x nphi points, nphi = 2 ntheta
+    (4 ntheta projective). The cost is 1 + |smooth field| over (x, y, z) ("spatial"), over
+    (theta, phi) ("angular"), over the whole grid ("full"), or 1.5 ("constant"); seeds are full
+    5-D points."""
+    rng = np.random.default_rng(seed)
+    nphi = (4 if projective else 2) * ntheta
+    dims = (n, n, n, ntheta, nphi)
+    if cost == "spatial":
+        c = 1.0 + np.abs(smooth_field(rng, (n, n, n), 1.0 / n))
+    elif cost == "angular":
+        c = 1.0 + np.abs(smooth_field(rng, (ntheta, nphi), 1.0 / nphi))
+    elif cost == "full":
+        c = 1.0 + np.abs(smooth_field(rng, dims, 1.0 / n))
+    else:
+        c = 1.5
+    pts = rng.uniform(0.3, 0.7, size=(n_seeds, 3))
+    theta = rng.uniform(0.1, (0.5 if projective else 1.0) * math.pi - 0.1, size=(n_seeds, 1))
+    phi = rng.uniform(0.0, 2.0 * math.pi, size=(n_seeds, 1))
+    return {
+        "model": "ReedsShepp3",
+        "arrayOrdering": "RowMajor",
+        "dims": np.array(dims, dtype=float),
+        "gridScale": 1.0 / n,
+        "xi": float(xi),
+        "eps": float(eps),
+        "dual": float(bool(dual)),
+        "projective": float(bool(projective)),
+        "cost": c,
+        "seeds": np.concatenate([pts, theta, phi], axis=1),
+        "exportValues": 1.0,
+    }
+
+
 def thomsen_tti(vp, eps, delta, dip, azimuth) -> np.ndarray:
     """TTI metric elements (..., 14) from Thomsen parameters and tilt angles.
 

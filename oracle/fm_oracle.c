@@ -2273,3 +2273,198 @@ int64_t fmo_tti_geodesic_ode(const int64_t *dims, const double *h, const double 
     return ode_all(&g, tti_flow, &T, seed_index, nseeds, ntips, tips, step, causality, max_points, points, lengths,
                    failed);
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* ReedsShepp3 on R^3 x S^2 (Headers/Specializations/Curvature3.h:11-70): axes x, y, z closed,
+ * theta Sphere2_0 and phi Sphere2_1 (PeriodicGrid.hxx:120-186); one stencil per (theta, phi)
+ * index, shared by the spatial points (HFM_StencilShare.hxx); eight symmetric differences. */
+
+#define RS3_NSYM 8
+
+int fmo_rs3_stencil(int ntheta, int nphi, double h, double xi, double eps, int dual, int8_t *offsets,
+                    double *weights) {
+    /* param.Setup(that, 2 pi / dims.back()) (Curvature3.h:61, HFM_ParamDefault.hxx:19-34) */
+    const double ds = (2.0 * 3.141592653589793238462643383279502884) / (double)nphi;
+    const double e2 = eps * eps;
+    for (int it = 0; it < ntheta; ++it)
+        for (int ip = 0; ip < nphi; ++ip) {
+            const int cls = it * nphi + ip;
+            int8_t *O = offsets + (int64_t)cls * RS3_NSYM * 5;
+            double *W = weights + (int64_t)cls * RS3_NSYM;
+            const double theta = (it + 0.5) * ds, phi = ip * ds;
+            const double v[3] = {cos(theta), sin(theta) * cos(phi), sin(theta) * sin(phi)};
+            /* m = (1 - eps^2) v v^T + eps^2 Id, or (eps^2 - 1) v v^T + Id for the dual model,
+             * then / gridScale^2 (Curvature3.h:50-55), a division that multiplies every component
+             * by the reciprocal (Vector::operator/=, LinearAlgebra/VectorType.h:37-42) */
+            double d[6];
+            const double a = dual ? (e2 - 1.0) : (1.0 - e2), b = dual ? 1.0 : e2, rh2 = 1.0 / (h * h);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j <= i; ++j) {
+                    const double r = v[i] * v[j];
+                    d[sym_index(i, j)] = (a * r + (i == j ? b : 0.0)) * rh2;
+                }
+            int8_t o3[18];
+            double w3[6];
+            memset(O, 0, RS3_NSYM * 5);
+            if (fmo_selling_mat(3, d, o3, w3)) return -1;
+            for (int k = 0; k < 6; ++k) {
+                for (int c = 0; c < 3; ++c) O[5 * k + c] = o3[3 * k + c];
+                W[k] = w3[k];
+            }
+            O[5 * 6 + 3] = 1;
+            W[6] = 1.0 / ((xi * ds) * (xi * ds));
+            O[5 * 7 + 4] = 1;
+            const double sx = sin(theta) * xi * ds;
+            W[7] = 1.0 / (sx * sx);
+        }
+    return 0;
+}
+
+/* PeriodizeNoBase on indices (PeriodicGrid.hxx:120-160): closed axes reject, theta reflects at
+ * the poles into [0, ntheta) while phi turns by nphi / 2, phi wraps. Returns 0 outside. */
+static int rs3_periodize(const int64_t *dims, int64_t *x, int *flip) {
+    *flip = 0;
+    for (int a = 0; a < 3; ++a)
+        if (x[a] < 0 || x[a] >= dims[a]) return 0;
+    const int64_t nt = dims[3], np = dims[4];
+    int64_t t = x[3] % (2 * nt);
+    if (t < 0) t += 2 * nt;
+    if (t >= nt) {
+        t = 2 * nt - t - 1;
+        *flip = 1;
+        x[4] += np / 2;
+    }
+    x[3] = t;
+    int64_t ph = x[4] % np;
+    if (ph < 0) ph += np;
+    x[4] = ph;
+    return 1;
+}
+
+static inline int64_t rs3_linear(const int64_t *dims, const int64_t *x) {
+    int64_t r = 0;
+    for (int a = 0; a < 5; ++a) r = r * dims[a] + x[a];
+    return r;
+}
+
+typedef struct { int64_t key; int8_t o[5]; } rs3_pair;
+
+static int rs3_pair_cmp(const void *a, const void *b) {
+    const rs3_pair *x = (const rs3_pair *)a, *y = (const rs3_pair *)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    for (int c = 0; c < 5; ++c)
+        if (x->o[c] != y->o[c]) return x->o[c] < y->o[c] ? -1 : 1;
+    return 0;
+}
+
+int64_t fmo_rs3_fast_marching(const int64_t *dims, const int8_t *offsets, const double *weights,
+                              const double *mult, int nseeds, const int64_t *seed_index,
+                              const double *seed_value, double *values, uint64_t *active,
+                              int *max_stencil_width) {
+    const int64_t nt = dims[3], np = dims[4], ncls = nt * np;
+    int64_t N = 1;
+    for (int a = 0; a < 5; ++a) N *= dims[a];
+    /* Reversed offsets (HFM_StencilShare.hxx:132-181): from the centre point of each class, the
+     * offsets of non-zero weight whose target lies in the domain, pulled back through the
+     * reflection (Transform::PullVector, PeriodicGrid.hxx:19-25), keyed by the target's class,
+     * sorted and deduplicated */
+    rs3_pair *pairs = (rs3_pair *)malloc((size_t)ncls * 2 * RS3_NSYM * sizeof(rs3_pair));
+    if (!pairs) return -1;
+    int64_t npairs = 0;
+    for (int64_t cl = 0; cl < ncls; ++cl) {
+        const int8_t *O = offsets + cl * RS3_NSYM * 5;
+        const double *W = weights + cl * RS3_NSYM;
+        for (int k = 0; k < RS3_NSYM; ++k) {
+            if (W[k] == 0.0) continue;
+            for (int sg = 1; sg >= -1; sg -= 2) {
+                int64_t y[5] = {dims[0] / 2, dims[1] / 2, dims[2] / 2, cl / np, cl % np};
+                int8_t e[5];
+                for (int c = 0; c < 5; ++c) { e[c] = (int8_t)(sg * O[5 * k + c]); y[c] += e[c]; }
+                int flip;
+                if (!rs3_periodize(dims, y, &flip)) continue;
+                if (flip) e[3] = (int8_t)(-e[3]);
+                rs3_pair rp;
+                rp.key = y[3] * np + y[4];
+                memcpy(rp.o, e, 5);
+                pairs[npairs++] = rp;
+            }
+        }
+    }
+    qsort(pairs, npairs, sizeof(rs3_pair), rs3_pair_cmp);
+    int64_t nu = 0;
+    for (int64_t i = 0; i < npairs; ++i)
+        if (nu == 0 || rs3_pair_cmp(&pairs[nu - 1], &pairs[i]) != 0) pairs[nu++] = pairs[i];
+    int64_t *split = (int64_t *)calloc(ncls + 1, sizeof(int64_t));
+    if (!split) { free(pairs); return -1; }
+    int mw = 0;
+    for (int64_t i = 0; i < nu; ++i) {
+        split[pairs[i].key + 1]++;
+        int l1 = 0;
+        for (int c = 0; c < 5; ++c) l1 += abs(pairs[i].o[c]);
+        if (l1 > mw) mw = l1;
+    }
+    for (int64_t k = 0; k < ncls; ++k) split[k + 1] += split[k];
+    if (max_stencil_width) *max_stencil_width = mw;
+
+    uint8_t *accepted = (uint8_t *)calloc(N, 1);
+    uint64_t *act = active ? active : (uint64_t *)calloc(N, sizeof(uint64_t));
+    quad_t *quads = (quad_t *)calloc(N, sizeof(quad_t));
+    heap_t heap = {0};
+    if (!accepted || !act || !quads) return -1;
+    if (active) memset(active, 0, N * sizeof(uint64_t));
+    for (int64_t x = 0; x < N; ++x) values[x] = FMO_INF;
+    for (int s = 0; s < nseeds; ++s) {
+        values[seed_index[s]] = seed_value[s];
+        heap_push(&heap, (qelem){seed_index[s], seed_value[s]});
+    }
+    int64_t nAccepted = 0;
+    while (heap.n > 0) {
+        /* RunOnce (HamiltonFastMarching.hxx:86-112) */
+        const qelem top = heap_pop(&heap);
+        if (accepted[top.idx]) continue;
+        ++nAccepted;
+        accepted[top.idx] = 1;
+        int64_t aidx[5], r = top.idx;
+        for (int a = 4; a >= 0; --a) { aidx[a] = r % dims[a]; r /= dims[a]; }
+        const int64_t key = aidx[3] * np + aidx[4];
+        for (int64_t ri = split[key]; ri < split[key + 1]; ++ri) {
+            /* ConditionalUpdate (HamiltonFastMarching.hxx:136-154): updated = accepted - e, and the
+             * offset pulled back through that periodization is the updated cell's own */
+            int8_t e[5];
+            memcpy(e, pairs[ri].o, 5);
+            int64_t uidx[5];
+            for (int a = 0; a < 5; ++a) uidx[a] = aidx[a] - e[a];
+            int flip;
+            if (!rs3_periodize(dims, uidx, &flip)) continue;
+            if (flip) e[3] = (int8_t)(-e[3]);
+            const int64_t u = rs3_linear(dims, uidx);
+            if (accepted[u]) continue;
+            if (act[u] == 0 && values[u] != FMO_INF) continue;
+            if (values[u] <= top.val) continue;
+            /* Update + HopfLaxUpdate (HFM_StencilShare.hxx:74-84, EulerianStencil.hxx:104-153) */
+            quad_t *q = &quads[u];
+            if (!q->used) { q->used = 1; q->minVal = top.val; q->a = 0; q->b = 0; q->c = -1; }
+            const int64_t cl = uidx[3] * np + uidx[4];
+            const int8_t *O = offsets + cl * RS3_NSYM * 5;
+            const double *W = weights + cl * RS3_NSYM;
+            const double m = mult ? mult[u] : 1.0;
+            for (int k = 0, bit = 0; k < RS3_NSYM; ++k, bit += 2) {
+                const int8_t *o = O + 5 * k;
+                int pos = 1, neg = 1;
+                for (int c = 0; c < 5; ++c) { pos &= o[c] == e[c]; neg &= o[c] == -e[c]; }
+                const double w = mult ? W[k] * (m * m) : W[k];
+                if (pos && !(act[u] & (1ULL << (bit + 1)))) { act[u] |= 1ULL << bit; quad_add(q, top.val, w); }
+                if (neg && !(act[u] & (1ULL << bit))) { act[u] |= 1ULL << (bit + 1); quad_add(q, top.val, w); }
+            }
+            values[u] = quad_solve(q);
+            heap_push(&heap, (qelem){u, values[u]});
+        }
+    }
+    free(heap.a);
+    free(quads);
+    free(accepted);
+    if (!active) free(act);
+    free(split);
+    free(pairs);
+    return nAccepted;
+}

@@ -119,6 +119,10 @@ def lib():
         L.fmo_tti_geodesic_ode.restype = ctypes.c_int64
         L.fmo_tti_forward_variation.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, _P, _P]
         L.fmo_tti_geodesic_flow.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
+        L.fmo_rs3_stencil.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, _P, _P]
+        L.fmo_rs3_fast_marching.argtypes = [_P, _P, _P, _P, ctypes.c_int, _P, _P, _P, _P, _P]
+        L.fmo_rs3_fast_marching.restype = ctypes.c_int64
         _lib = L
     return _lib
 
@@ -728,3 +732,85 @@ def forward_variation(res: Dict, params: Dict) -> np.ndarray:
     if rc != 0:
         raise RuntimeError("oracle forward variation failed")
     return result.reshape(dims + (nvar,))
+
+
+# ------------------------------------------------------------------------------- ReedsShepp3
+
+def rs3_stencil(ntheta: int, nphi: int, h: float, xi: float, eps: float, dual: bool = False):
+    """Shared ReedsShepp3 stencils per class (theta, phi) = it * nphi + ip: offsets [ncls, 8, 5]
+    (x, y, z, theta, phi) and weights [ncls, 8] (``Curvature3.h:37-58``)."""
+    ncls = ntheta * nphi
+    off = np.zeros((ncls, 8, 5), np.int8)
+    w = np.zeros((ncls, 8))
+    if lib().fmo_rs3_stencil(ntheta, nphi, h, xi, eps, int(bool(dual)), _ptr(off), _ptr(w)) != 0:
+        raise RuntimeError("ObtuseSuperbase error in the ReedsShepp3 stencil")
+    return off, w
+
+
+def _rs3_seed_index(q, dims):
+    """Index of an adimensionalized point: floor per axis, then the index periodization
+    (``StaticFactoring.hxx:384-390``, ``PeriodicGrid.hxx:120-160``); None outside."""
+    idx = [int(math.floor(c)) for c in q]
+    if not all(0 <= idx[a] < dims[a] for a in range(3)):
+        return None
+    nt, nph = dims[3], dims[4]
+    t = idx[3] % (2 * nt)
+    if t >= nt:
+        t = 2 * nt - t - 1
+        idx[4] += nph // 2
+    idx[3] = t
+    idx[4] %= nph
+    return int(np.ravel_multi_index(tuple(idx), dims))
+
+
+def rs3_solve(params: Dict) -> Dict:
+    """ReedsShepp3 fast marching on the CPU (``Curvature3.h:29-70``): values (dims), activeNeighs
+    (uint64), nAccepted, MaxStencilWidth. Keys: dims (5), gridScale, origin (3), xi, eps, dual,
+    projective (nphi = 4 ntheta instead of 2 ntheta), speed or cost (scalar; (x, y, z);
+    (theta, phi); or the full grid), seeds (n, 5), seedValues."""
+    dims = tuple(int(round(d)) for d in np.asarray(params["dims"]).ravel())
+    if len(dims) != 5:
+        raise ValueError("ReedsShepp3 takes five dims")
+    nt, nph = dims[3], dims[4]
+    projective = bool(_get(params, "projective", 0.0))
+    if nph != (4 if projective else 2) * nt:
+        raise ValueError("ReedsShepp3 setup error : inconsistent bundle dimensions")
+    h = float(params["gridScale"])
+    xi, eps = float(_get(params, "xi", 1.0)), float(_get(params, "eps", 0.1))
+    dual = bool(_get(params, "dual", 0.0))
+    off, w = rs3_stencil(nt, nph, h, xi, eps, dual)
+    if "speed" in params:
+        sp = np.asarray(params["speed"], float)
+    else:
+        sp = 1.0 / np.asarray(params["cost"], float)
+    if sp.ndim == 2:       # a field over (theta, phi)
+        sp = sp.reshape((1, 1, 1, nt, nph))
+    elif sp.ndim == 3:     # a field over (x, y, z)
+        sp = sp.reshape(dims[:3] + (1, 1))
+    mult = np.ascontiguousarray(np.broadcast_to(sp, dims), dtype=np.float64)
+    ds = 2.0 * math.pi / nph
+    origin = np.asarray(_get(params, "origin", np.zeros(3)), float).ravel()
+    seen = {}
+    if "seeds" in params:
+        pts = np.atleast_2d(np.asarray(params["seeds"], float))
+        vals = np.asarray(_get(params, "seedValues", np.zeros(len(pts))), float).ravel()
+        for p, v in zip(pts, vals):
+            q = [(p[0] - origin[0]) / h, (p[1] - origin[1]) / h, (p[2] - origin[2]) / h, p[3] / ds,
+                 (p[4] + ds / 2.0) / ds]
+            lin = _rs3_seed_index(q, dims)
+            if lin is not None:
+                seen.setdefault(lin, float(v))
+    keys = sorted(seen)
+    sidx = np.array(keys, np.int64)
+    sval = np.array([seen[k] for k in keys], float)
+    n = int(np.prod(dims))
+    values = np.empty(n)
+    active = np.zeros(n, np.uint64)
+    mw = ctypes.c_int(0)
+    d = np.array(dims, np.int64)
+    nacc = lib().fmo_rs3_fast_marching(_ptr(d), _ptr(off), _ptr(w), _ptr(mult), len(sidx), _ptr(sidx), _ptr(sval),
+                                       _ptr(values), _ptr(active), ctypes.byref(mw))
+    if nacc < 0:
+        raise RuntimeError("oracle ReedsShepp3 fast marching failed")
+    return {"values": values.reshape(dims), "activeNeighs": active, "nAccepted": int(nacc),
+            "MaxStencilWidth": int(mw.value)}

@@ -411,9 +411,17 @@ def forward_curvature_fixtures():
     solve_fixture("rsf2_24x16_walls", p)
 
 
+
+def reedsshepp3_fixtures():
+    """ReedsShepp3 (Curvature3.h:29-70): primal and dual, projective, each kind of cost field."""
+    solve_fixture("rs3_10x6", W.reedsshepp3_case(10, 6, seed=31))
+    solve_fixture("rs3_8x4_dual", W.reedsshepp3_case(8, 4, seed=32, dual=True, cost="full"))
+    solve_fixture("rs3_8x4_projective", W.reedsshepp3_case(8, 4, seed=33, projective=True, cost="angular"))
+    solve_fixture("rs3_12x6_xi1", W.reedsshepp3_case(12, 6, seed=34, xi=1.0, eps=0.2, cost="constant", n_seeds=2))
+
 if __name__ == "__main__":
     # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread|dubins|
-    # spreadstep`
+    # spreadstep|factoring|rs3`
     # regenerates only those fixtures
     if sys.argv[1:] == ["tti"]:
         tti_fixtures()
@@ -441,6 +449,8 @@ if __name__ == "__main__":
         stencil_step_spreading_fixtures()
     elif sys.argv[1:] == ["factoring"]:
         tti_factoring_fixtures()
+    elif sys.argv[1:] == ["rs3"]:
+        reedsshepp3_fixtures()
     else:
         main()
         tti_fixtures()
