@@ -8,6 +8,8 @@
 //   StencilReedsSheppForward2::SetStencil                               Curvature2.h:86-100
 //   StencilDubins2::SetStencil                                          Curvature2.h:113-140
 //   StencilElastica2<5>::SetStencil and its Fejer weights               Curvature2.h:178-234
+//   StencilReedsShepp3::SetStencil (R^3 x S^2, Voronoi1Mat)             Curvature3.h:37-58
+//   StencilReedsSheppForward3::SetStencil (R^3 x S^2, Voronoi1Vec)      Curvature3.h:79-95
 #include <cmath>
 
 #include "selling.cuh"
@@ -135,6 +137,73 @@ void elastica2_table(int ntheta, double h, double xi, double eps, std::vector<in
         voronoi1vec<2>(v2, eps, O + 6 * (nF - 1) * 3, W + 6 * (nF - 1));
         for (int i = 0; i < 3; ++i) W[6 * (nF - 1) + i] *= fejer[nF / 2];
     }
+}
+
+// ReedsShepp3: one stencil per (theta, phi), theta = (it + 1/2) ds, phi = ip ds, ds = 2 pi / nphi
+// (param.Setup(that, 2 pi / dims.back())). The 3x3 matrix (1 - eps^2) v v^T + eps^2 Id (dual:
+// (eps^2 - 1) v v^T + Id) of the direction v = (cos theta, sin theta cos phi, sin theta sin phi),
+// scaled by the reciprocal of gridScale^2 (the reference's matrix / scalar multiplies by 1 / s),
+// is decomposed by Selling with the 1000 eps Tr cut-off of Voronoi1Mat (CommonTraits.h:82-105);
+// then the theta and phi steps of weights 1 / (xi ds)^2 and 1 / (sin(theta) xi ds)^2.
+void reedsshepp3_table(int nth, int nph, double h, double xi, double eps, bool dual, std::vector<int8_t> &off,
+                       std::vector<int8_t> &ang, std::vector<double> &w) {
+    const int ncls = nth * nph;
+    off.assign((size_t)ncls * 8 * 3, 0);
+    ang.assign((size_t)ncls * 8 * 2, 0);
+    w.assign((size_t)ncls * 8, 0.0);
+    const double ds = (2.0 * kPi) / (double)nph;
+    const double e2 = eps * eps;
+    const double a = dual ? (e2 - 1.0) : (1.0 - e2), b = dual ? 1.0 : e2, rh2 = 1.0 / (h * h);
+    for (int it = 0; it < nth; ++it)
+        for (int ip = 0; ip < nph; ++ip) {
+            const int c = it * nph + ip;
+            const double theta = ((double)it + 0.5) * ds, phi = (double)ip * ds;
+            const double v[3] = {std::cos(theta), std::sin(theta) * std::cos(phi), std::sin(theta) * std::sin(phi)};
+            double d[6];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j <= i; ++j) d[sym_idx(i, j)] = (a * (v[i] * v[j]) + (i == j ? b : 0.0)) * rh2;
+            int o[6][3];
+            double ww[6];
+            if (!tensor_decomposition<3>(d, o, ww))
+                throw Error(HFM_ERR_VALUE, "ObtuseSuperbase error : input must be positive definite");
+            const double atol = (1000.0 * 2.220446049250313080847e-16) * sym_trace<3>(d);
+            for (int k = 0; k < 6; ++k) {
+                w[c * 8 + k] = ww[k] < atol ? 0.0 : ww[k];
+                for (int q = 0; q < 3; ++q) off[(c * 8 + k) * 3 + q] = (int8_t)o[k][q];
+            }
+            ang[(c * 8 + 6) * 2 + 0] = 1;
+            w[c * 8 + 6] = 1.0 / ((xi * ds) * (xi * ds));
+            ang[(c * 8 + 7) * 2 + 1] = 1;
+            const double sx = std::sin(theta) * xi * ds;
+            w[c * 8 + 7] = 1.0 / (sx * sx);
+        }
+}
+
+// ReedsSheppForward3 (Curvature3.h:72-107): per (theta, phi), theta = pi (it + 1/2) / ntheta and
+// phi = 2 pi ip / nphi, the 6 forward differences of Voronoi1Vec of
+// v = (cos theta, sin theta cos phi, sin theta sin phi) / gridScale, then the theta and phi steps
+// of weights 1 / (xi ds)^2 and 1 / (sin(theta) xi ds)^2, ds = 2 pi / nphi.
+void reedssheppforward3_table(int nth, int nph, double h, double xi, double eps, std::vector<int8_t> &off,
+                              std::vector<int8_t> &ang, std::vector<double> &w) {
+    const int ncls = nth * nph;
+    off.assign((size_t)ncls * 8 * 3, 0);
+    ang.assign((size_t)ncls * 8 * 2, 0);
+    w.assign((size_t)ncls * 8, 0.0);
+    const double ds = (2.0 * kPi) / (double)nph;
+    const double ih = 1.0 / h;
+    for (int it = 0; it < nth; ++it)
+        for (int ip = 0; ip < nph; ++ip) {
+            const int c = it * nph + ip;
+            const double theta = kPi * ((double)it + 0.5) / (double)nth, phi = (2.0 * kPi * (double)ip) / (double)nph;
+            const double v[3] = {std::cos(theta) * ih, std::sin(theta) * std::cos(phi) * ih,
+                                 std::sin(theta) * std::sin(phi) * ih};
+            voronoi1vec<3>(v, eps, &off[c * 8 * 3], &w[c * 8]);
+            ang[(c * 8 + 6) * 2 + 0] = 1;
+            w[c * 8 + 6] = 1.0 / ((xi * ds) * (xi * ds));
+            ang[(c * 8 + 7) * 2 + 1] = 1;
+            const double sx = std::sin(theta) * xi * ds;
+            w[c * 8 + 7] = 1.0 / (sx * sx);
+        }
 }
 
 }  // namespace hfm

@@ -65,8 +65,10 @@ constexpr int kWarpsPerCta = 4;
 // Stencil families of the solver kernels (the KIND template parameter): per-cell Riemann
 // stencils, shared per-angle stencils (curvature models), per-cell TTI Selling paths.
 // kKindShare2: shared stencils of two groups of forward differences whose value is the smaller of
-// the two groups' solutions (Dubins2, nmax = 2).
-constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2, kKindShare2 = 3;
+// the two groups' solutions (Dubins2, nmax = 2). kKindShareS2: shared stencils over R^3 x S^2
+// (ReedsShepp3), one class per (theta, phi) pair (see s2_step).
+constexpr int kKindRiemann = 0, kKindShare = 1, kKindTTI = 2, kKindShare2 = 3, kKindShareS2 = 4;
+constexpr bool is_share(int kind) { return kind == kKindShare || kind == kKindShare2 || kind == kKindShareS2; }
 // Value increases a tile may take before it accepts decreases only (termination guard).
 constexpr unsigned kUpBudget = 128;
 // Tile dependency tables: a small hash table per warp first (fast, high occupancy), the large one
@@ -92,6 +94,7 @@ struct Inst {
     double h[3];
     int dual, metric_const, has_walls;
     int mult_depth, mult_inverse, pad;
+    int nth, nph;        // ReedsShepp3: theta and phi extents (0 elsewhere)
 };
 
 // Instance holding global cell x (binary search over the increasing cell0 offsets).
@@ -146,6 +149,7 @@ struct Dev {
     unsigned *vis;            // [ntc] slot visibility + flags (shared stencils)
     const int8_t *cls_off;    // [nclass][ND][3]
     const Real *cls_w;        // [nclass][ND]
+    const int8_t *cls_ang;    // [nclass][ND][2] theta and phi steps of the differences (kKindShareS2)
     // reverse tile dependencies: tile T -> tiles whose stencils read T, with the cells they read;
     // entries [dep_ptr[T], dep_end[T]) (dep_end null: dep_ptr[T + 1], a CSR over the tile space)
     const long long *dep_ptr;
@@ -199,6 +203,52 @@ struct Dev {
     int sweeps;
 };
 
+// Shared stencils over R^3 x S^2 (ReedsShepp3, Curvature3.h:11-70). The grid (x, y, z, theta, phi)
+// is held RowMajor as the 3-D grid (x, y, w), w = (z * ntheta + theta) * nphi + phi: values, tiles
+// and scheduling are those of a 3-D grid, and the class of a cell is its (theta, phi) pair. A step
+// (dz, dtheta, dphi) from w is periodized as PeriodicGrid.hxx:120-160 does: z is closed, theta
+// reflects at the poles (index 2 ntheta - 1 - t) while phi turns by nphi / 2, phi wraps. False
+// where the step leaves the domain.
+__host__ __device__ __forceinline__ bool s2_step(const Inst &I, int x2, int dz, int dth, int dph, int &y2) {
+    const int nth = I.nth, nph = I.nph, nang = nth * nph;
+    int z = x2 / nang;
+    const int r = x2 - z * nang;
+    int th = r / nph, ph = r - th * nph;
+    z += dz;
+    if (z < 0 || z >= I.g.dims[2] / nang) return false;
+    th += dth;
+    ph += dph;
+    th %= 2 * nth;
+    if (th < 0) th += 2 * nth;
+    if (th >= nth) {
+        th = 2 * nth - th - 1;
+        ph += nph / 2;
+    }
+    ph %= nph;
+    if (ph < 0) ph += nph;
+    y2 = (z * nth + th) * nph + ph;
+    return true;
+}
+
+// Global class of the cell at third coordinate x2 of a shared-stencil instance.
+template <int KIND>
+__host__ __device__ __forceinline__ long long share_class(const Inst &I, int x2) {
+    if constexpr (KIND == kKindShareS2) return I.cls0 + x2 % (I.nth * I.nph);
+    else return I.cls0 + x2;
+}
+
+// Neighbour y = x + s e of difference k of class cls (kKindShareS2): false outside the domain.
+template <typename Real, int ND>
+__device__ __forceinline__ bool s2_neighbor(const Dev<Real> &P, const Inst &I, long long cls, int k, int s, int x0,
+                                            int x1, int x2, int &y0, int &y1, int &y2) {
+    const int8_t *o = P.cls_off + (cls * ND + k) * 3;
+    const int8_t *a = P.cls_ang + (cls * ND + k) * 2;
+    y0 = x0 + s * __ldg(o);
+    y1 = x1 + s * __ldg(o + 1);
+    if (y0 < 0 || y0 >= I.g.dims[0] || y1 < 0 || y1 >= I.g.dims[1]) return false;
+    return s2_step(I, x2, s * __ldg(o + 2), s * __ldg(a), s * __ldg(a + 1), y2);
+}
+
 // --------------------------------------------------------------------------------------------
 // Hopf-Lax update over neighbour candidates v[k] (+inf if unusable) with weights w[k], taken in
 // increasing order (ties by k); see the file header. `used` receives the bitmask of taken k.
@@ -233,7 +283,7 @@ __device__ __forceinline__ void cex(Real &va, Real &wa, int &ka, Real &vb, Real 
     ka = tk;
 }
 
-// Optimal sorting networks for the small stencils (2, 3, 4 and 6 differences).
+// Sorting networks for the small stencils (2, 3, 4, 6 and 8 differences; optimal sizes).
 template <typename Real, int ND>
 __device__ __forceinline__ void sort_candidates(Real (&v)[ND], Real (&w)[ND], int (&k)[ND]) {
 #define HFM_CX(a, b) cex<Real>(v[a], w[a], k[a], v[b], w[b], k[b])
@@ -246,6 +296,10 @@ __device__ __forceinline__ void sort_candidates(Real (&v)[ND], Real (&w)[ND], in
     } else if constexpr (ND == 6) {
         HFM_CX(1, 2); HFM_CX(0, 2); HFM_CX(0, 1); HFM_CX(4, 5); HFM_CX(3, 5); HFM_CX(3, 4);
         HFM_CX(0, 3); HFM_CX(1, 4); HFM_CX(2, 5); HFM_CX(2, 4); HFM_CX(1, 3); HFM_CX(2, 3);
+    } else if constexpr (ND == 8) {
+        HFM_CX(0, 2); HFM_CX(1, 3); HFM_CX(4, 6); HFM_CX(5, 7); HFM_CX(0, 4); HFM_CX(1, 5); HFM_CX(2, 6);
+        HFM_CX(3, 7); HFM_CX(0, 1); HFM_CX(2, 3); HFM_CX(4, 5); HFM_CX(6, 7); HFM_CX(2, 4); HFM_CX(3, 5);
+        HFM_CX(1, 4); HFM_CX(3, 6); HFM_CX(1, 2); HFM_CX(3, 4); HFM_CX(5, 6);
     }
 #undef HFM_CX
 }
@@ -255,7 +309,7 @@ __device__ __forceinline__ Real hopf_lax_sorted(const Real (&v_in)[ND], const Re
     using A = Arith<Real>;
     const Real INF = A::inf();
     const Real band = sizeof(Real) == 8 ? Real(1e-12) : Real(1e-5);
-    if constexpr (ND == 2 || ND == 3 || ND == 4 || ND == 6) {
+    if constexpr (ND == 2 || ND == 3 || ND == 4 || ND == 6 || ND == 8) {
         // the same additions in the same order as the selection loop below, on sorted candidates
         Real v[ND], w[ND];
         int k[ND];
@@ -379,13 +433,13 @@ template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Inst &I, long long c, int x0, int x1,
                                                    int x2, int tx0, int tx1, int tx2, const Real *sv, unsigned *used,
                                                    unsigned *side) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     using A = Arith<Real>;
     const Real INF = A::inf();
     const GridGeom &g = I.g;
     const Real *values = P.values + I.cell0;
-    const long long cls = I.cls0 + x2;
+    const long long cls = share_class<KIND>(I, x2);
     Real v[ND], w[ND];
     [[maybe_unused]] unsigned oc[ND];  // packed offsets (two-group stencils: shared neighbours)
     Real m2 = 1;
@@ -396,19 +450,21 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
         visw = P.vis[c];
     }
     unsigned sides = 0;
-    auto fetch = [&](int o0, int o1, int o2) -> Real {
-        const int n0 = x0 + o0, n1 = x1 + o1;
-        int n2 = x2 + o2;
-        if (SHARE && g.periodic[2]) {
-            n2 %= g.dims[2];
-            if (n2 < 0) n2 += g.dims[2];
-        }
+    auto fetch_at = [&](int n0, int n1, int n2) -> Real {
         if (sv) {
             const unsigned l0 = n0 - tx0, l1 = n1 - tx1, l2 = n2 - tx2;
             if (l0 < (1u << g.tshift[0]) && l1 < (1u << g.tshift[1]) && l2 < (1u << g.tshift[2]))
                 return sv[((l0 << g.tshift[1] | l1) << g.tshift[2]) | l2];
         }
         return __ldcg(values + g.lin(n0, n1, n2));
+    };
+    auto fetch = [&](int o0, int o1, int o2) -> Real {
+        int n2 = x2 + o2;
+        if (SHARE && g.periodic[2]) {
+            n2 %= g.dims[2];
+            if (n2 < 0) n2 += g.dims[2];
+        }
+        return fetch_at(x0 + o0, x1 + o1, n2);
     };
 #pragma unroll
     for (int k = 0; k < ND; ++k) {
@@ -434,10 +490,20 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
             vm = (k >= NFWD) && (cd & kVisMinus);
         }
         Real val = INF;
-        if (vp) val = fetch(o0, o1, o2);
-        if (vm) {
-            const Real vv = fetch(-o0, -o1, -o2);
-            if (vv < val) { val = vv; if (k >= NFWD) sides |= 1u << (k - NFWD); }
+        if constexpr (KIND == kKindShareS2) {
+            // the visibility bits hold only steps that stay in the domain
+            int y0, y1, y2;
+            if (vp && s2_neighbor<Real, ND>(P, I, cls, k, 1, x0, x1, x2, y0, y1, y2)) val = fetch_at(y0, y1, y2);
+            if (vm && s2_neighbor<Real, ND>(P, I, cls, k, -1, x0, x1, x2, y0, y1, y2)) {
+                const Real vv = fetch_at(y0, y1, y2);
+                if (vv < val) { val = vv; if (k >= NFWD) sides |= 1u << (k - NFWD); }
+            }
+        } else {
+            if (vp) val = fetch(o0, o1, o2);
+            if (vm) {
+                const Real vv = fetch(-o0, -o1, -o2);
+                if (vv < val) { val = vv; if (k >= NFWD) sides |= 1u << (k - NFWD); }
+            }
         }
         v[k] = val;
     }
@@ -554,7 +620,7 @@ __device__ __forceinline__ Real solve_cell(const Dev<Real> &P, const Inst &I, lo
 
 template <typename Real, int KIND>
 __device__ __forceinline__ void cell_flags(const Dev<Real> &P, long long c, bool &fixed, bool &dead) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     if (SHARE) {
         const unsigned f = P.vis[c];
         fixed = f & kShFixed;
@@ -688,17 +754,18 @@ __device__ __forceinline__ int entry_class(const Dev<Real> &P, int T, unsigned l
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, const Inst &I, long long c, int x0,
                                                            int x1, int x2, int tx0, int tx1, int tx2) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     const GridGeom &g = I.g;
     unsigned long long m = 0;
     const unsigned visw = SHARE ? P.vis[c] : 0u;
+    [[maybe_unused]] const long long cls = share_class<KIND>(I, x2);
 #pragma unroll
     for (int k = 0; k < ND; ++k) {
         int o0, o1, o2;
         unsigned bits;
         if (SHARE) {
-            const int8_t *o = P.cls_off + ((I.cls0 + x2) * ND + k) * 3;
+            const int8_t *o = P.cls_off + (cls * ND + k) * 3;
             o0 = __ldg(o); o1 = __ldg(o + 1); o2 = __ldg(o + 2);
             bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
         } else {
@@ -710,12 +777,14 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
         for (int si = 0; si < 2; ++si) {
             if (!((bits >> si) & 1u)) continue;
             const int s = si ? -1 : 1;
-            int n2 = x2 + s * o2;
-            if (SHARE && g.periodic[2]) {
+            int n0 = x0 + s * o0, n1 = x1 + s * o1, n2 = x2 + s * o2;
+            if constexpr (KIND == kKindShareS2) {
+                if (!s2_neighbor<Real, ND>(P, I, cls, k, s, x0, x1, x2, n0, n1, n2)) continue;
+            } else if (SHARE && g.periodic[2]) {
                 n2 %= g.dims[2];
                 if (n2 < 0) n2 += g.dims[2];
             }
-            const unsigned l0 = x0 + s * o0 - tx0, l1 = x1 + s * o1 - tx1, l2 = n2 - tx2;
+            const unsigned l0 = n0 - tx0, l1 = n1 - tx1, l2 = n2 - tx2;
             if (l0 < (1u << g.tshift[0]) && l1 < (1u << g.tshift[1]) && l2 < (1u << g.tshift[2]))
                 m |= 1ull << (((l0 << g.tshift[1] | l1) << g.tshift[2]) | l2);
         }
@@ -737,7 +806,7 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv, int lane, int li_next, int slot,
                                              unsigned long long &n_solves, StatAcc &acc) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
     int t0, t1, t2;
@@ -895,13 +964,15 @@ __device__ __forceinline__ void process_tile(const Dev<Real> &P, int T, Real *sv
 // Elastica stencil whose local solve needs the registers).
 template <typename Real, int NFWD, int NSYM, int KIND>
 constexpr int fim_min_blocks() {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
-    return KIND == kKindTTI ? 1 : SHARE ? (NFWD + NSYM > 8 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 8;
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
+    // ReedsShepp3: 4 blocks per SM (up to 128 registers), which keeps its 8-difference update and
+    // the sphere periodization out of local memory
+    return KIND == kKindTTI ? 1 : KIND == kKindShareS2 ? 4 : SHARE ? (NFWD + NSYM > 8 ? (sizeof(Real) == 8 ? 1 : 4) : 8) : 8;
 }
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, (fim_min_blocks<Real, NFWD, NSYM, KIND>())) fim_kernel(Dev<Real> P) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     __shared__ Real s_vals[kWarpsPerCta][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long kInfBits = 0x7ff0000000000000ull;
@@ -1186,9 +1257,17 @@ __global__ void mult_layout_kernel(Dev<Real> P, const double *src) {
     const CellRef R = cell_ref(P.inst, P.ninst, x);
     const Inst &I = P.inst[R.i];
     long long k = 0;
-    if (I.mult_depth == 3) k = R.xl;
-    else if (I.mult_depth == 2) k = (long long)R.x0 * I.g.dims[1] + R.x1;
-    else if (I.mult_depth == 1) k = R.x2;
+    if (I.mult_depth == 3) {
+        k = R.xl;
+    } else if (I.nth > 0) {  // ReedsShepp3: (x, y, z) or (theta, phi)
+        const int nang = I.nth * I.nph;
+        if (I.mult_depth == 2) k = ((long long)R.x0 * I.g.dims[1] + R.x1) * (I.g.dims[2] / nang) + R.x2 / nang;
+        else if (I.mult_depth == 1) k = R.x2 % nang;
+    } else if (I.mult_depth == 2) {
+        k = (long long)R.x0 * I.g.dims[1] + R.x1;
+    } else if (I.mult_depth == 1) {
+        k = R.x2;
+    }
     double m = src[I.mult0 + k];
     if (I.mult_inverse) m = 1.0 / m;
     P.mult[R.c] = (Real)m;
@@ -1295,7 +1374,7 @@ __device__ bool wall_visible(const GridGeom &g, const int8_t *wd, int b0, int b1
 // (ConditionalUpdate, HamiltonFastMarching.hxx:136-154). Also marks padding cells dead.
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8_t *cls_enabled) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= P.ntc) return;
@@ -1303,7 +1382,6 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
     const Inst &I = P.inst[P.tile_inst[T]];
     const GridGeom &g = I.g;
     const int8_t *wd = (wd_all && I.has_walls) ? wd_all + I.cell0 : nullptr;
-    const long long cls = I.cls0;
     int t0, t1, t2, l0, l1, l2;
     g.tile_coords(T - I.tile0, t0, t1, t2);
     g.local_coords(l, l0, l1, l2);
@@ -1314,14 +1392,15 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
         return;
     }
     unsigned visw = 0;
+    const long long cls = share_class<KIND>(I, x2);
 #pragma unroll 1
     for (int k = 0; k < ND; ++k) {
         int o[3];
         bool nonzero;
         if (SHARE) {
-            const int8_t *oo = P.cls_off + ((cls + x2) * ND + k) * 3;
+            const int8_t *oo = P.cls_off + (cls * ND + k) * 3;
             o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
-            nonzero = P.cls_w[(cls + x2) * ND + k] != Real(0);
+            nonzero = P.cls_w[cls * ND + k] != Real(0);
         } else {
             const unsigned cd = P.code[k * P.sstride + c];
             o[0] = off_c(cd, 0); o[1] = off_c(cd, 1); o[2] = off_c(cd, 2);
@@ -1332,9 +1411,13 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
             const int s = si == 0 ? 1 : -1;
             const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
             if (!nonzero) continue;
-            if (SHARE && !cls_enabled[(cls + x2) * (NFWD + 2 * NSYM) + slot]) continue;
+            if (SHARE && !cls_enabled[cls * (NFWD + 2 * NSYM) + slot]) continue;
             int y0 = x0 + s * o[0], y1 = x1 + s * o[1], y2 = x2 + s * o[2];
-            if (!g.wrap(y0, y1, y2)) continue;
+            if constexpr (KIND == kKindShareS2) {
+                if (!s2_neighbor<Real, ND>(P, I, cls, k, s, x0, x1, x2, y0, y1, y2)) continue;
+            } else if (!g.wrap(y0, y1, y2)) {
+                continue;
+            }
             if (wd && !wall_visible(g, wd, y0, y1, y2, -s * o[0], -s * o[1], -s * o[2], x0, x1, x2)) continue;
             if (SHARE) visw |= 1u << slot;
             else bits |= si == 0 ? kVisPlus : kVisMinus;
@@ -1346,7 +1429,7 @@ __global__ void visibility_kernel(Dev<Real> P, const int8_t *wd_all, const uint8
 
 template <typename Real, int KIND>
 __global__ void seeds_kernel(Dev<Real> P, const long long *idx, const double *val, int n) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     // idx: global cell indices
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1365,7 +1448,7 @@ template <typename Real, int NFWD, int NSYM, int KIND, int kDepCap, int kDepWarp
 __global__ void __launch_bounds__(kDepWarps * 32)
     deps_kernel(Dev<Real> P, int pass, unsigned *cnt, const long long *offs, int *src, int *dst,
                 unsigned long long *msk, unsigned long long *dmsk) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     __shared__ int keys[kDepWarps][kDepCap];
     __shared__ unsigned long long masks[kDepWarps][kDepCap];
@@ -1391,11 +1474,12 @@ __global__ void __launch_bounds__(kDepWarps * 32)
         const long long c = D * 64 + l;
         if (x0 >= g.dims[0] || x1 >= g.dims[1] || x2 >= g.dims[2]) continue;
         unsigned visw = SHARE ? P.vis[c] : 0u;
+        [[maybe_unused]] const long long cls = share_class<KIND>(I, x2);
         for (int k = 0; k < ND; ++k) {
             int o[3];
             unsigned bits;
             if (SHARE) {
-                const int8_t *oo = P.cls_off + ((I.cls0 + x2) * ND + k) * 3;
+                const int8_t *oo = P.cls_off + (cls * ND + k) * 3;
                 o[0] = oo[0]; o[1] = oo[1]; o[2] = oo[2];
                 bits = k < NFWD ? ((visw >> k) & 1u) : ((visw >> (NFWD + 2 * (k - NFWD))) & 3u);
             } else {
@@ -1407,7 +1491,11 @@ __global__ void __launch_bounds__(kDepWarps * 32)
                 if (!((bits >> si) & 1u)) continue;
                 const int s = si == 0 ? 1 : -1;
                 int y0 = x0 + s * o[0], y1 = x1 + s * o[1], y2 = x2 + s * o[2];
-                g.wrap(y0, y1, y2);
+                if constexpr (KIND == kKindShareS2) {
+                    if (!s2_neighbor<Real, ND>(P, I, cls, k, s, x0, x1, x2, y0, y1, y2)) continue;
+                } else {
+                    g.wrap(y0, y1, y2);
+                }
                 const int T = (int)(I.tile0 + g.tile_of(y0, y1, y2));
                 if (T == D) continue;
                 const int b = g.local_of(y0, y1, y2);
@@ -1509,7 +1597,7 @@ __global__ void count_finite_kernel(Dev<Real> P, unsigned long long *out) {
 // update adds every difference matching the accepted offset (EulerianStencil.hxx:114-123).
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= P.ncells) return;
@@ -1535,7 +1623,7 @@ __global__ void active_kernel(Dev<Real> P, unsigned long long *active) {
     const Inst &I = P.inst[R.i];
     const int x0 = R.x0, x1 = R.x1, x2 = R.x2;
     const long long c = R.c;
-    const long long cls = I.cls0 + x2;
+    const long long cls = share_class<KIND>(I, x2);
     bool fixed, dead;
     cell_flags<Real, KIND>(P, c, fixed, dead);
     unsigned long long bits = 0;
@@ -1614,7 +1702,7 @@ void check_status(const DeviceBuffer<unsigned> &status, const char *phase) {
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uint8_t *nflow, int *indeg) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     // the adjoint runs on a batch of one instance
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
@@ -1623,6 +1711,11 @@ __global__ void flow_kernel(Dev<Real> P, int *fidx, double *fw, double *var, uin
     const GridGeom &g = I.g;
     const long long N = g.ncells;
     if (x >= N) return;
+    if constexpr (KIND == kKindShareS2) {
+        // ReedsShepp3 first variations are refused by the host before any launch
+        if (x == 0) atomicOr(P.status, (unsigned)kErrIndexRange);
+        return;
+    }
     const int x2 = (int)(x % g.dims[2]);
     const long long r = x / g.dims[2];
     const int x1 = (int)(r % g.dims[1]);
@@ -2297,7 +2390,7 @@ struct Retained final : RetainedSolve {
     DeviceBuffer<int> tile_inst;
     DeviceBuffer<unsigned> status, code, vis;
     DeviceBuffer<Real> values, weight, mult, cls_w;
-    DeviceBuffer<int8_t> cls_off;
+    DeviceBuffer<int8_t> cls_off, cls_ang;
     DeviceBuffer<TTICell> tti;
     DeviceBuffer<double> diag;  // per-axis speeds of a Diagonal model (P.diag_src points here)
     void adjoint(const EulerProblem &p, EulerResult &res) override {
@@ -2321,7 +2414,7 @@ struct Retained final : RetainedSolve {
 
 template <typename Real, int NFWD, int NSYM, int KIND>
 void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<EulerResult> &results) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     constexpr int NB = NFWD + 2 * NSYM;
     const auto wall_t0 = std::chrono::steady_clock::now();
@@ -2354,8 +2447,17 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         I.mult0 = nmult;
         I.mult_depth = p.mult_depth;
         I.mult_inverse = p.mult_inverse ? 1 : 0;
+        I.nth = p.sphere_nth;
+        I.nph = p.sphere_nph;
+        if ((KIND == kKindShareS2) != (p.sphere_nth > 0))
+            throw Error(HFM_ERR_VALUE, "R^3 x S^2 grids take the sphere-bundle stencil family");
         if (SHARE) {
-            const long long nm[4] = {1, I.g.dims[2], (long long)I.g.dims[0] * I.g.dims[1], I.g.ncells};
+            // multiplier over the whole grid, the angular part (theta for the curvature models,
+            // (theta, phi) for ReedsShepp3), the spatial part, or a constant
+            const long long nang = I.nth > 0 ? (long long)I.nth * I.nph : 0;
+            const long long nm[4] = {1, nang ? nang : I.g.dims[2],
+                                     (long long)I.g.dims[0] * I.g.dims[1] * (nang ? I.g.dims[2] / nang : 1),
+                                     I.g.ncells};
             nmult += nm[std::min(3, std::max(0, p.mult_depth))];
         }
         any_walls |= I.has_walls != 0;
@@ -2395,7 +2497,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     tm.start(s);
     DeviceBuffer<unsigned> code, vis, maxw(ninst);
     DeviceBuffer<Real> weight, mult, cls_w;
-    DeviceBuffer<int8_t> cls_off, plain_off;
+    DeviceBuffer<int8_t> cls_off, cls_ang, plain_off;
     DeviceBuffer<uint8_t> cls_en;
     DeviceBuffer<double> metric, plain_w, mult_rm, kscale;
     DeviceBuffer<TTICell> ttibuf;
@@ -2489,13 +2591,18 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         HFM_CUDA(cudaStreamSynchronize(s));
     } else {
         std::vector<Real> hw;
-        std::vector<int8_t> ho;
+        std::vector<int8_t> ho, ha;
         std::vector<uint8_t> he;
         mult_rm.alloc(std::max(1ll, nmult));
         for (int i = 0; i < ninst; ++i) {
             const EulerProblem &p = *probs[i];
             for (double w : p.cls_w) hw.push_back((Real)w);
             ho.insert(ho.end(), p.cls_off.begin(), p.cls_off.end());
+            if (KIND == kKindShareS2) {
+                if (p.cls_ang.size() != (size_t)p.nclass * ND * 2)
+                    throw Error(HFM_ERR_VALUE, "sphere-bundle stencils need their angular steps");
+                ha.insert(ha.end(), p.cls_ang.begin(), p.cls_ang.end());
+            }
             he.insert(he.end(), p.cls_enabled.begin(), p.cls_enabled.end());
             const long long len = (i + 1 < ninst ? hinst[i + 1].mult0 : nmult) - hinst[i].mult0;
             const double *msrc = p.mult_ptr ? p.mult_ptr : p.mult.data();
@@ -2519,7 +2626,10 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                     for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
                         const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD) + si;
                         if (!p.cls_enabled[cl * NB + slot]) continue;
-                        mw = std::max(mw, std::abs(o[0]) + std::abs(o[1]) + std::abs(o[2]));
+                        int l1 = std::abs(o[0]) + std::abs(o[1]) + std::abs(o[2]);
+                        if (KIND == kKindShareS2)
+                            l1 += std::abs(p.cls_ang[(cl * ND + k) * 2]) + std::abs(p.cls_ang[(cl * ND + k) * 2 + 1]);
+                        mw = std::max(mw, l1);
                     }
                 }
             hmaxw[i] = (unsigned)mw;
@@ -2530,6 +2640,10 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         maxw.upload(hmaxw, s);
         P.cls_w = cls_w.get();
         P.cls_off = cls_off.get();
+        if (KIND == kKindShareS2) {
+            cls_ang.upload(ha, s);
+            P.cls_ang = cls_ang.get();
+        }
         mult.alloc(ntc);
         mult.zero(s);
         P.mult = mult.get();
@@ -2874,6 +2988,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         r->mult = std::move(mult);
         r->cls_w = std::move(cls_w);
         r->cls_off = std::move(cls_off);
+        r->cls_ang = std::move(cls_ang);
         r->tti = std::move(ttibuf);
         if (p0.diagonal) r->diag = std::move(metric);
         results[0].retained = r;
@@ -2922,7 +3037,7 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
     const EulerProblem &p = *probs[0];
     for (const EulerProblem *q : probs) {
         if (q->kind != p.kind || q->ndim != p.ndim || q->nfwd != p.nfwd || q->nsym != p.nsym || q->fp64 != p.fp64 ||
-            q->diagonal != p.diagonal || q->nmax != p.nmax)
+            q->diagonal != p.diagonal || q->nmax != p.nmax || (q->sphere_nth > 0) != (p.sphere_nth > 0))
             throw Error(HFM_ERR_VALUE, "a batch must hold instances of one model family and one precision");
     }
     if (p.kind == StencilKind::TTI) {
@@ -2968,6 +3083,12 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
         } else if (p.nfwd == 12 && p.nsym == 0 && p.nmax == 2) {
             if (p.fp64) run_batch_impl<double, 12, 0, detail::kKindShare2>(probs, results);
             else run_batch_impl<float, 12, 0, detail::kKindShare2>(probs, results);
+        } else if (p.nfwd == 0 && p.nsym == 8 && p.sphere_nth > 0) {
+            if (p.fp64) run_batch_impl<double, 0, 8, detail::kKindShareS2>(probs, results);
+            else run_batch_impl<float, 0, 8, detail::kKindShareS2>(probs, results);
+        } else if (p.nfwd == 6 && p.nsym == 2 && p.sphere_nth > 0) {
+            if (p.fp64) run_batch_impl<double, 6, 2, detail::kKindShareS2>(probs, results);
+            else run_batch_impl<float, 6, 2, detail::kKindShareS2>(probs, results);
         } else {
             throw Error(HFM_ERR_UNSUPPORTED, "unsupported shared stencil shape");
         }

@@ -86,7 +86,7 @@ __device__ __forceinline__ bool geo_packable(const int *ind) {
 template <typename Real, int NFWD, int NSYM, int KIND>
 __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1, int x2, unsigned *foff, double *fw,
                               double *value, double *width) {
-    [[maybe_unused]] constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    [[maybe_unused]] constexpr bool SHARE = is_share(KIND);
     constexpr int ND = NFWD + NSYM;
     using A = Arith<double>;
     const GridGeom &g = I.g;
@@ -98,6 +98,7 @@ __device__ int recompute_flow(const Dev<Real> &P, const Inst &I, int x0, int x1,
     bool fixed, dead;
     cell_flags<Real, KIND>(P, c, fixed, dead);
     if (fixed || dead || !(u < A::inf())) return 0;
+    if constexpr (KIND == kKindShareS2) return 0;  // ReedsShepp3 geodesics are refused by the host
     if constexpr (KIND == kKindTTI) {
         double ta = 0.0;
         bool inner = false;
@@ -864,7 +865,7 @@ template <int NFWD, int NSYM, int KIND>
 constexpr bool geo_dim_ok(int d) {
     if (KIND == kKindRiemann && NFWD == 0 && NSYM == 2) return d == 2;
     if (KIND == kKindRiemann && NFWD == 0 && NSYM == 3) return true;
-    if ((KIND == kKindShare || KIND == kKindShare2) && NFWD == 0 && NSYM == 2) return d == 2;
+    if (is_share(KIND) && NFWD == 0 && NSYM == 2) return d == 2;
     return d == 3;
 }
 

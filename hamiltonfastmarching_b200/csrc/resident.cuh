@@ -310,7 +310,7 @@ private:
 template <typename Real, int NFWD, int NSYM, int KIND>
 class Resident final : public ResidentFamily {
     static constexpr int ND = NFWD + NSYM, NB = NFWD + 2 * NSYM;
-    static constexpr bool SHARE = (KIND == kKindShare || KIND == kKindShare2);
+    static constexpr bool SHARE = is_share(KIND);
     static_assert(KIND != kKindTTI, "TTI3 is served through the single-solve path");
 
     struct Entry {

@@ -32,16 +32,29 @@ const double kPi = 3.141592653589793238462643383279502884;
 
 struct Param {
     int ndim = 2;
-    int dims[3] = {1, 1, 1};
-    int periodic[3] = {0, 0, 0};
-    double origin[3] = {0, 0, 0};
-    double scale[3] = {1, 1, 1};  // grid scale per axis (dependScale on the angular axis)
-    // point -> index (HFM_ParamDefault.hxx ADim + BaseGrid::IndexFromPoint + PeriodizeNoBase)
+    int dims[5] = {1, 1, 1, 1, 1};
+    int periodic[5] = {0, 0, 0, 0, 0};
+    double origin[5] = {0, 0, 0, 0, 0};
+    double scale[5] = {1, 1, 1, 1, 1};  // grid scale per axis (dependScale on the angular axes)
+    int sphere = -1;  // axis of a Sphere2_0 / Sphere2_1 pair (theta, phi: ReedsShepp3), or -1
+    // point -> index (HFM_ParamDefault.hxx ADim + BaseGrid::IndexFromPoint + PeriodizeNoBase,
+    // PeriodicGrid.hxx:120-160: closed axes reject, theta reflects at the poles while phi turns by
+    // half a circle, periodic axes wrap)
     bool index_of(const double *p, int64_t *lin) const {
+        long long idx[5];
+        for (int a = 0; a < ndim; ++a) idx[a] = (long long)std::floor((p[a] - origin[a]) / scale[a]);
         int64_t r = 0;
         for (int a = 0; a < ndim; ++a) {
-            long long i = (long long)std::floor((p[a] - origin[a]) / scale[a]);
-            if (periodic[a]) {
+            long long i = idx[a];
+            if (a == sphere) {
+                const long long n2 = 2LL * dims[a];
+                i %= n2;
+                if (i < 0) i += n2;
+                if (i >= dims[a]) {
+                    i = n2 - i - 1;
+                    idx[a + 1] += dims[a + 1] / 2;
+                }
+            } else if (periodic[a] || (sphere >= 0 && a == sphere + 1)) {
                 i %= dims[a];
                 if (i < 0) i += dims[a];
             } else if (i < 0 || i >= dims[a]) {
@@ -830,6 +843,104 @@ void setup_curvature(Store &io, const std::string &model, Param &pm, EulerProble
     }
 }
 
+// ReedsShepp3 and ReedsSheppForward3 on R^3 x S^2 (Headers/Specializations/Curvature3.h:29-107):
+// the grid (x, y, z, theta, phi), theta in (0, pi) at (i + 1/2) ds and phi at j ds, ds = 2 pi / nphi
+// (nphi = 2 ntheta, or 4 ntheta for the projective ReedsShepp3), Sphere2 boundary conditions on
+// (theta, phi). The solver holds it as the 3-D grid (x, y, (z * ntheta + theta) * nphi + phi) with
+// one shared stencil per (theta, phi); the speed (or cost) is a constant or a field over the whole
+// grid, (x, y, z) or (theta, phi) (SpecializationsDefault::GetField, HFMInterface.hxx:23-32).
+void setup_reedsshepp3(Store &io, Param &pm, EulerProblem &p, bool forward) {
+    const std::vector<int> dims = read_dims(io, 5);
+    const double eps = io.get_scalar("eps", 0.1);
+    const double xi = io.get_scalar("xi", 1.0);
+    const bool dual = forward ? false : io.get_scalar("dual", 0.0) != 0;
+    const bool projective = forward ? false : io.get_scalar("projective", 0.0) != 0;
+    const double h = io.get_scalar("gridScale");
+    if (!(h > 0)) throw Error(HFM_ERR_VALUE, "Parametrization error : gridscale should be positive");
+    const std::string name = forward ? "ReedsSheppForward3" : "ReedsShepp3";
+    if (projective && dims[4] != 4 * dims[3])
+        throw Error(HFM_ERR_VALUE, name + " setup error : inconsistent bundle dimensions (projective : nPhi=4*nTheta).");
+    if (!projective && dims[4] != 2 * dims[3])
+        throw Error(HFM_ERR_VALUE, name + " setup error : inconsistent bundle dimensions (expected : nPhi=2*nTheta).");
+    const long long nw = (long long)dims[2] * dims[3] * dims[4];
+    if (nw >= (1ll << 30) || (long long)dims[0] * dims[1] * nw >= (1ll << 40))
+        throw Error(HFM_ERR_UNSUPPORTED, "ReedsShepp3 grid too large for the GPU solve path");
+    const double ds = (2.0 * kPi) / (double)dims[4];
+    pm.ndim = 5;
+    for (int a = 0; a < 5; ++a) pm.dims[a] = dims[a];
+    const std::vector<double> origin = read_point(io, "origin", 3, {0.0, 0.0, 0.0});
+    for (int a = 0; a < 3; ++a) {
+        pm.origin[a] = origin[a];
+        pm.scale[a] = h;
+    }
+    pm.origin[3] = 0.0;
+    pm.origin[4] = -ds / 2.0;  // HFM_ParamDefault.hxx:25
+    pm.scale[3] = pm.scale[4] = ds;
+    pm.sphere = 3;
+    p.ndim = 3;
+    p.dims[0] = dims[0];
+    p.dims[1] = dims[1];
+    p.dims[2] = (int)nw;
+    p.h[0] = p.h[1] = p.h[2] = h;  // the class tables carry the scales; h only sizes the domain
+    p.kind = StencilKind::SharedByTheta;
+    p.angular = true;
+    p.nfwd = forward ? 6 : 0;
+    p.nsym = forward ? 2 : 8;
+    p.nclass = dims[3] * dims[4];
+    p.sphere_nth = dims[3];
+    p.sphere_nph = dims[4];
+    if (forward) reedssheppforward3_table(dims[3], dims[4], h, xi, eps, p.cls_off, p.cls_ang, p.cls_w);
+    else reedsshepp3_table(dims[3], dims[4], h, xi, eps, dual, p.cls_off, p.cls_ang, p.cls_w);
+    // slots reachable from each class centre (dims / 2 on x, y, z; the sphere steps always land
+    // in the domain) (HFM_StencilShare.hxx:132-175)
+    const int NB = p.nfwd + 2 * p.nsym;
+    p.cls_enabled.assign((size_t)p.nclass * NB, 0);
+    for (int c = 0; c < p.nclass; ++c)
+        for (int k = 0; k < 8; ++k)
+            for (int si = 0; si < (k < p.nfwd ? 1 : 2); ++si) {
+                const int s = si ? -1 : 1;
+                const int slot = k < p.nfwd ? k : p.nfwd + 2 * (k - p.nfwd) + si;
+                bool in = true;
+                for (int a = 0; a < 3; ++a) {
+                    const int y = dims[a] / 2 + s * p.cls_off[(c * 8 + k) * 3 + a];
+                    in = in && y >= 0 && y < dims[a];
+                }
+                p.cls_enabled[c * NB + slot] = in ? 1 : 0;
+            }
+    const bool has_speed = io.has_field("speed");
+    const std::string key = has_speed ? "speed" : "cost";
+    const std::vector<int64_t> dd = io.field_domain_dims(key, 1);
+    const int depth = (int)dd.size();
+    if (depth != 0 && depth != 2 && depth != 3 && depth != 5)
+        throw Error(HFM_ERR_VALUE, "Field " + key + " has incorrect depth.\n");
+    Field f = io.get_field(key, depth, 1);
+    const int first = depth == 2 ? 3 : 0;
+    for (int a = 0; a < depth; ++a)
+        if (f.dims[a] != dims[first + a])
+            throw Error(HFM_ERR_VALUE, "Error : Field " + key + " has inconsistent dimensions.");
+    p.mult_depth = depth == 5 ? 3 : depth == 3 ? 2 : depth == 2 ? 1 : 0;
+    p.mult_inverse = !has_speed;
+    if (f.view) {
+        p.mult_ptr = f.view;
+    } else {
+        p.mult = std::move(f.data);
+        p.mult_ptr = nullptr;
+    }
+    // the GPU solve path covers the arrival times (values, activeNeighs, nAccepted and the stencil
+    // width) of this model
+    static const char *kRefused[] = {"walls",        "seeds_Unoriented",     "stopWhenAnyAccepted_Unoriented",
+                                     "stopWhenAllAccepted_Unoriented", "tips", "tips_Unoriented",
+                                     "inspectSensitivity", "costVariation", "seedValueVariation",
+                                     "values",       "activeNeighs",         "getStencils"};
+    for (const char *k : kRefused)
+        if (io.has_field(k))
+            throw Error(HFM_ERR_UNSUPPORTED, name + " with " + k + " is not supported by the GPU solve path");
+    if (io.has_field("seedRadius") && io.get_scalar("seedRadius") != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, name + " with seedRadius is not supported by the GPU solve path");
+    if (io.get_scalar("exportGeodesicFlow", 0.0, 3) != 0 || io.get_scalar("retainState", 0.0, 3) != 0)
+        throw Error(HFM_ERR_UNSUPPORTED, name + " geodesic flow and retained state are not supported by the GPU solve path");
+}
+
 // inspectSensitivity groups (FirstVariation::Finally, FirstVariation.h:60-102): weighted points.
 void read_inspect(Store &io, const Param &pm, EulerProblem &p) {
     p.adjoint_index.clear();
@@ -1252,6 +1363,8 @@ void prepare_model(Store &io, const std::string &model, Prepared &q) {
     else if (model == "Diagonal2") setup_diagonal(io, 2, pm, p);
     else if (model == "Diagonal3") setup_diagonal(io, 3, pm, p);
     else if (lifted) setup_curvature(io, model, pm, p);
+    else if (model == "ReedsShepp3" || model == "ReedsSheppForward3")
+        setup_reedsshepp3(io, pm, p, model == "ReedsSheppForward3");
     else if (model == "TTI3") setup_tti(io, pm, p);
     else throw Error(HFM_ERR_UNSUPPORTED, "Unrecognized model : " + model);
     set_common_solver_options(io, p);

@@ -50,6 +50,12 @@ struct EulerProblem {
     std::vector<int8_t> cls_off;       // [nclass][nfwd+nsym][3]
     std::vector<double> cls_w;         // [nclass][nfwd+nsym]
     std::vector<uint8_t> cls_enabled;  // [nclass][nfwd+2*nsym] slot reachable from the class centre
+    // ReedsShepp3 (R^3 x S^2): the grid (x, y, z, theta, phi) is held as the 3-D grid
+    // (x, y, (z * sphere_nth + theta) * sphere_nph + phi); the classes are the (theta, phi) pairs
+    // and cls_ang [nclass][nsym][2] holds the theta and phi steps of each difference (cls_off the
+    // x, y, z steps). 0: no sphere bundle.
+    int sphere_nth = 0, sphere_nph = 0;
+    std::vector<int8_t> cls_ang;
     // Speed multiplier of the shared stencils, given compactly as in the reference's lifted scalar
     // fields (HFMInterface.hxx:23-32): depth 0 (one value), 1 (per angle), 2 (per physical point
     // x,y) or 3 (per cell), RowMajor at mult_ptr (host, not owned, or `mult` when null); the cost
@@ -247,6 +253,13 @@ std::unique_ptr<ResidentFamily> make_resident_family(const EulerProblem &p);
 // (Headers/Specializations/Curvature2.h:48-66, 86-100, 178-234, CommonTraits.h:118-161).
 void reedsshepp2_table(int ntheta, double h, double xi, double eps, bool projective,
                        std::vector<int8_t> &off, std::vector<double> &w);
+// ReedsShepp3 classes (theta, phi) = it * nphi + ip: x, y, z steps [ncls][8][3], theta and phi
+// steps [ncls][8][2], weights [ncls][8].
+void reedsshepp3_table(int nth, int nph, double h, double xi, double eps, bool dual, std::vector<int8_t> &off,
+                       std::vector<int8_t> &ang, std::vector<double> &w);
+// ReedsSheppForward3: the same layout, 6 forward differences then the 2 angular ones.
+void reedssheppforward3_table(int nth, int nph, double h, double xi, double eps, std::vector<int8_t> &off,
+                              std::vector<int8_t> &ang, std::vector<double> &w);
 void elastica2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,
                      std::vector<double> &w);
 void reedssheppforward2_table(int ntheta, double h, double xi, double eps, std::vector<int8_t> &off,

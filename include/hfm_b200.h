@@ -78,7 +78,8 @@ int hfm_io_computed_keys(hfm_io *io, char *buf, size_t cap, size_t *len);
 
 /* Replaces `void Run(IO&)` (DispatchAndRun.h:224-244) followed by IO::UsageReport
  * (main.cpp:14, BaseIO.hxx:64-104): dispatches at run time on the "model" key
- * (Riemann2, Riemann3, ReedsShepp2, ReedsSheppForward2, Elastica2, TTI3, Isotropic2/3, Diagonal2/3),
+ * (Riemann2, Riemann3, ReedsShepp2, ReedsSheppForward2, Dubins2, Elastica2, ReedsShepp3, TTI3,
+ * Isotropic2/3, Diagonal2/3),
  * solves on the current CUDA device and writes the outputs (values, nAccepted, MaxStencilWidth,
  * costSensitivity_i, ...) into `io`.
  * If `expected_model` is non-NULL the call fails when "model" names another model, as the

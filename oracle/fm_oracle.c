@@ -2357,10 +2357,43 @@ static int rs3_pair_cmp(const void *a, const void *b) {
     return 0;
 }
 
-int64_t fmo_rs3_fast_marching(const int64_t *dims, const int8_t *offsets, const double *weights,
-                              const double *mult, int nseeds, const int64_t *seed_index,
-                              const double *seed_value, double *values, uint64_t *active,
-                              int *max_stencil_width) {
+/* ReedsSheppForward3 (Curvature3.h:72-107): per class, 6 forward differences of Voronoi1Vec of
+ * v = (cos theta, sin theta cos phi, sin theta sin phi) / gridScale (theta = pi (it + 1/2) / ntheta,
+ * phi = 2 pi ip / nphi; the division multiplies by the reciprocal), then the theta and phi steps
+ * (symmetric) of weights 1 / (xi ds)^2 and 1 / (sin(theta) xi ds)^2, ds = 2 pi / nphi. */
+int fmo_rsf3_stencil(int ntheta, int nphi, double h, double xi, double eps, int8_t *offsets, double *weights) {
+    const double pi = 3.141592653589793238462643383279502884;
+    const double ds = (2.0 * pi) / (double)nphi;
+    const double ih = 1.0 / h;
+    for (int it = 0; it < ntheta; ++it)
+        for (int ip = 0; ip < nphi; ++ip) {
+            const int cls = it * nphi + ip;
+            int8_t *O = offsets + (int64_t)cls * 8 * 5;
+            double *W = weights + (int64_t)cls * 8;
+            const double theta = pi * (it + 0.5) / (double)ntheta, phi = (2.0 * pi * ip) / (double)nphi;
+            const double v[3] = {cos(theta) * ih, sin(theta) * cos(phi) * ih, sin(theta) * sin(phi) * ih};
+            int8_t o3[18];
+            double w3[6];
+            memset(O, 0, 8 * 5);
+            if (fmo_voronoi1vec(3, v, eps, o3, w3)) return -1;
+            for (int k = 0; k < 6; ++k) {
+                for (int c = 0; c < 3; ++c) O[5 * k + c] = o3[3 * k + c];
+                W[k] = w3[k];
+            }
+            O[5 * 6 + 3] = 1;
+            W[6] = 1.0 / ((xi * ds) * (xi * ds));
+            O[5 * 7 + 4] = 1;
+            const double sx = sin(theta) * xi * ds;
+            W[7] = 1.0 / (sx * sx);
+        }
+    return 0;
+}
+
+int64_t fmo_s2_fast_marching(const int64_t *dims, int nfwd, int nsym, const int8_t *offsets,
+                             const double *weights, const double *mult, int nseeds, const int64_t *seed_index,
+                             const double *seed_value, double *values, uint64_t *active,
+                             int *max_stencil_width) {
+    const int nd = nfwd + nsym;
     const int64_t nt = dims[3], np = dims[4], ncls = nt * np;
     int64_t N = 1;
     for (int a = 0; a < 5; ++a) N *= dims[a];
@@ -2368,15 +2401,16 @@ int64_t fmo_rs3_fast_marching(const int64_t *dims, const int8_t *offsets, const 
      * offsets of non-zero weight whose target lies in the domain, pulled back through the
      * reflection (Transform::PullVector, PeriodicGrid.hxx:19-25), keyed by the target's class,
      * sorted and deduplicated */
-    rs3_pair *pairs = (rs3_pair *)malloc((size_t)ncls * 2 * RS3_NSYM * sizeof(rs3_pair));
+    rs3_pair *pairs = (rs3_pair *)malloc((size_t)ncls * 2 * nd * sizeof(rs3_pair));
     if (!pairs) return -1;
     int64_t npairs = 0;
     for (int64_t cl = 0; cl < ncls; ++cl) {
-        const int8_t *O = offsets + cl * RS3_NSYM * 5;
-        const double *W = weights + cl * RS3_NSYM;
-        for (int k = 0; k < RS3_NSYM; ++k) {
+        const int8_t *O = offsets + cl * nd * 5;
+        const double *W = weights + cl * nd;
+        for (int k = 0; k < nd; ++k) {
             if (W[k] == 0.0) continue;
             for (int sg = 1; sg >= -1; sg -= 2) {
+                if (sg == -1 && k < nfwd) break;
                 int64_t y[5] = {dims[0] / 2, dims[1] / 2, dims[2] / 2, cl / np, cl % np};
                 int8_t e[5];
                 for (int c = 0; c < 5; ++c) { e[c] = (int8_t)(sg * O[5 * k + c]); y[c] += e[c]; }
@@ -2445,10 +2479,17 @@ int64_t fmo_rs3_fast_marching(const int64_t *dims, const int8_t *offsets, const 
             quad_t *q = &quads[u];
             if (!q->used) { q->used = 1; q->minVal = top.val; q->a = 0; q->b = 0; q->c = -1; }
             const int64_t cl = uidx[3] * np + uidx[4];
-            const int8_t *O = offsets + cl * RS3_NSYM * 5;
-            const double *W = weights + cl * RS3_NSYM;
+            const int8_t *O = offsets + cl * nd * 5;
+            const double *W = weights + cl * nd;
             const double m = mult ? mult[u] : 1.0;
-            for (int k = 0, bit = 0; k < RS3_NSYM; ++k, bit += 2) {
+            int bit = 0;
+            for (int k = 0; k < nfwd; ++k, ++bit) {
+                const int8_t *o = O + 5 * k;
+                int pos = 1;
+                for (int c = 0; c < 5; ++c) pos &= o[c] == e[c];
+                if (pos) { act[u] |= 1ULL << bit; quad_add(q, top.val, mult ? W[k] * (m * m) : W[k]); }
+            }
+            for (int k = nfwd; k < nd; ++k, bit += 2) {
                 const int8_t *o = O + 5 * k;
                 int pos = 1, neg = 1;
                 for (int c = 0; c < 5; ++c) { pos &= o[c] == e[c]; neg &= o[c] == -e[c]; }

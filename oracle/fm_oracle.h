@@ -164,16 +164,19 @@ int64_t fmo_tti_geodesic_ode(const int64_t *dims, const double *h, const double 
 int fmo_tti_geodesic_flow(const int64_t *dims, const double *h, const double *metric, const double *values,
                           const double *t_active, double *flow, double *value, double *width);
 
-/* ReedsShepp3 (Headers/Specializations/Curvature3.h:11-70) on dims (x, y, z, theta, phi), RowMajor.
- * fmo_rs3_stencil: per class (theta, phi) = it * nphi + ip, 8 symmetric differences, offsets
- * [ncls][8][5] and weights [ncls][8]. fmo_rs3_fast_marching: mult [N] (speed; weights scale by its
- * square) or NULL; seeds as increasing unique row-major indices. Returns nAccepted, or -1. */
+/* ReedsShepp3 / ReedsSheppForward3 (Headers/Specializations/Curvature3.h:11-107) on dims
+ * (x, y, z, theta, phi), RowMajor. The stencil builders fill, per class (theta, phi) =
+ * it * nphi + ip, 8 differences: offsets [ncls][8][5] and weights [ncls][8] (ReedsShepp3: 8
+ * symmetric; ReedsSheppForward3: 6 forward, then 2 symmetric). fmo_s2_fast_marching: mult [N]
+ * (speed; weights scale by its square) or NULL; seeds as increasing unique row-major indices.
+ * Returns nAccepted, or -1. */
 int fmo_rs3_stencil(int ntheta, int nphi, double h, double xi, double eps, int dual, int8_t *offsets,
                     double *weights);
-int64_t fmo_rs3_fast_marching(const int64_t *dims, const int8_t *offsets, const double *weights,
-                              const double *mult, int nseeds, const int64_t *seed_index,
-                              const double *seed_value, double *values, uint64_t *active,
-                              int *max_stencil_width);
+int fmo_rsf3_stencil(int ntheta, int nphi, double h, double xi, double eps, int8_t *offsets, double *weights);
+int64_t fmo_s2_fast_marching(const int64_t *dims, int nfwd, int nsym, const int8_t *offsets,
+                             const double *weights, const double *mult, int nseeds, const int64_t *seed_index,
+                             const double *seed_value, double *values, uint64_t *active,
+                             int *max_stencil_width);
 
 #ifdef __cplusplus
 }

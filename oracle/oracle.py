@@ -121,8 +121,11 @@ def lib():
         L.fmo_tti_geodesic_flow.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
         L.fmo_rs3_stencil.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_int, _P, _P]
-        L.fmo_rs3_fast_marching.argtypes = [_P, _P, _P, _P, ctypes.c_int, _P, _P, _P, _P, _P]
-        L.fmo_rs3_fast_marching.restype = ctypes.c_int64
+        L.fmo_rsf3_stencil.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, _P, _P]
+        L.fmo_s2_fast_marching.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_int, _P, _P, _P,
+                                           _P, _P]
+        L.fmo_s2_fast_marching.restype = ctypes.c_int64
         _lib = L
     return _lib
 
@@ -736,13 +739,19 @@ def forward_variation(res: Dict, params: Dict) -> np.ndarray:
 
 # ------------------------------------------------------------------------------- ReedsShepp3
 
-def rs3_stencil(ntheta: int, nphi: int, h: float, xi: float, eps: float, dual: bool = False):
+def rs3_stencil(ntheta: int, nphi: int, h: float, xi: float, eps: float, dual: bool = False,
+                forward: bool = False):
     """Shared ReedsShepp3 stencils per class (theta, phi) = it * nphi + ip: offsets [ncls, 8, 5]
-    (x, y, z, theta, phi) and weights [ncls, 8] (``Curvature3.h:37-58``)."""
+    (x, y, z, theta, phi) and weights [ncls, 8] (``Curvature3.h:37-58``); ``forward``: the
+    ReedsSheppForward3 stencils, 6 forward differences then the 2 angular ones (``:79-95``)."""
     ncls = ntheta * nphi
     off = np.zeros((ncls, 8, 5), np.int8)
     w = np.zeros((ncls, 8))
-    if lib().fmo_rs3_stencil(ntheta, nphi, h, xi, eps, int(bool(dual)), _ptr(off), _ptr(w)) != 0:
+    if forward:
+        rc = lib().fmo_rsf3_stencil(ntheta, nphi, h, xi, eps, _ptr(off), _ptr(w))
+    else:
+        rc = lib().fmo_rs3_stencil(ntheta, nphi, h, xi, eps, int(bool(dual)), _ptr(off), _ptr(w))
+    if rc != 0:
         raise RuntimeError("ObtuseSuperbase error in the ReedsShepp3 stencil")
     return off, w
 
@@ -764,21 +773,24 @@ def _rs3_seed_index(q, dims):
 
 
 def rs3_solve(params: Dict) -> Dict:
-    """ReedsShepp3 fast marching on the CPU (``Curvature3.h:29-70``): values (dims), activeNeighs
-    (uint64), nAccepted, MaxStencilWidth. Keys: dims (5), gridScale, origin (3), xi, eps, dual,
-    projective (nphi = 4 ntheta instead of 2 ntheta), speed or cost (scalar; (x, y, z);
-    (theta, phi); or the full grid), seeds (n, 5), seedValues."""
+    """ReedsShepp3 / ReedsSheppForward3 fast marching on the CPU (``Curvature3.h:29-107``): values
+    (dims), activeNeighs (uint64), nAccepted, MaxStencilWidth. Keys: model, dims (5), gridScale,
+    origin (3), xi, eps, dual and projective (ReedsShepp3; projective: nphi = 4 ntheta instead of
+    2 ntheta), speed or cost (scalar; (x, y, z); (theta, phi); or the full grid), seeds (n, 5),
+    seedValues."""
     dims = tuple(int(round(d)) for d in np.asarray(params["dims"]).ravel())
     if len(dims) != 5:
         raise ValueError("ReedsShepp3 takes five dims")
+    forward = params.get("model") == "ReedsSheppForward3"
     nt, nph = dims[3], dims[4]
-    projective = bool(_get(params, "projective", 0.0))
+    projective = bool(_get(params, "projective", 0.0)) and not forward
     if nph != (4 if projective else 2) * nt:
         raise ValueError("ReedsShepp3 setup error : inconsistent bundle dimensions")
     h = float(params["gridScale"])
     xi, eps = float(_get(params, "xi", 1.0)), float(_get(params, "eps", 0.1))
-    dual = bool(_get(params, "dual", 0.0))
-    off, w = rs3_stencil(nt, nph, h, xi, eps, dual)
+    dual = bool(_get(params, "dual", 0.0)) and not forward
+    off, w = rs3_stencil(nt, nph, h, xi, eps, dual, forward)
+    nfwd, nsym = (6, 2) if forward else (0, 8)
     if "speed" in params:
         sp = np.asarray(params["speed"], float)
     else:
@@ -808,8 +820,8 @@ def rs3_solve(params: Dict) -> Dict:
     active = np.zeros(n, np.uint64)
     mw = ctypes.c_int(0)
     d = np.array(dims, np.int64)
-    nacc = lib().fmo_rs3_fast_marching(_ptr(d), _ptr(off), _ptr(w), _ptr(mult), len(sidx), _ptr(sidx), _ptr(sval),
-                                       _ptr(values), _ptr(active), ctypes.byref(mw))
+    nacc = lib().fmo_s2_fast_marching(_ptr(d), nfwd, nsym, _ptr(off), _ptr(w), _ptr(mult), len(sidx), _ptr(sidx),
+                                      _ptr(sval), _ptr(values), _ptr(active), ctypes.byref(mw))
     if nacc < 0:
         raise RuntimeError("oracle ReedsShepp3 fast marching failed")
     return {"values": values.reshape(dims), "activeNeighs": active, "nAccepted": int(nacc),

@@ -413,11 +413,19 @@ def forward_curvature_fixtures():
 
 
 def reedsshepp3_fixtures():
-    """ReedsShepp3 (Curvature3.h:29-70): primal and dual, projective, each kind of cost field."""
+    """ReedsShepp3 (Curvature3.h:29-70): primal and dual, projective, each kind of cost field; and
+    ReedsSheppForward3 (Curvature3.h:72-107)."""
     solve_fixture("rs3_10x6", W.reedsshepp3_case(10, 6, seed=31))
     solve_fixture("rs3_8x4_dual", W.reedsshepp3_case(8, 4, seed=32, dual=True, cost="full"))
     solve_fixture("rs3_8x4_projective", W.reedsshepp3_case(8, 4, seed=33, projective=True, cost="angular"))
     solve_fixture("rs3_12x6_xi1", W.reedsshepp3_case(12, 6, seed=34, xi=1.0, eps=0.2, cost="constant", n_seeds=2))
+    for name, kw in (("rsf3_10x6", dict(seed=35, cost="full")),
+                     ("rsf3_8x4_angular", dict(seed=36, cost="angular", xi=1.0, eps=0.3, n_seeds=2))):
+        n, nt = (10, 6) if name == "rsf3_10x6" else (8, 4)
+        p = W.reedsshepp3_case(n, nt, **kw)
+        p["model"] = "ReedsSheppForward3"
+        del p["dual"], p["projective"]
+        solve_fixture(name, p)
 
 if __name__ == "__main__":
     # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread|dubins|

@@ -1,0 +1,133 @@
+"""ReedsShepp3 and ReedsSheppForward3 (R^3 x S^2, Headers/Specializations/Curvature3.h:29-107) on
+the GPU, through the C ABI.
+
+Tolerances as for the other Eulerian models: FP64 arrival times within 1e-10 relative max-norm
+of the reference's FileHFM_ReedsShepp3 / FileHFM_ReedsSheppForward3 and of the oracle (fast
+marching's accumulation order is reproduced, so most cells are bit-identical); nAccepted and
+MaxStencilWidth exact; activeNeighs
+equal except where a symmetric difference's two neighbours hold exactly the same value; FP32
+within 1e-5 of FP64.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+import hamiltonfastmarching_b200 as H
+from hamiltonfastmarching_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RS3_FIXTURES = ["rs3_10x6", "rs3_8x4_dual", "rs3_8x4_projective", "rs3_12x6_xi1", "rsf3_10x6", "rsf3_8x4_angular"]
+FP64_RTOL = 1e-10
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    assert np.array_equal(np.isinf(a), np.isinf(b)), "reached sets differ"
+    fin = np.isfinite(a)
+    return float(np.max(np.abs(a[fin] - b[fin])) / np.max(np.abs(a[fin])))
+
+
+def _neighbor(dims, x, e):
+    """x + e on the 5-D grid, periodized as PeriodicGrid.hxx:120-160 (None outside)."""
+    y = [x[a] + e[a] for a in range(5)]
+    if not all(0 <= y[a] < dims[a] for a in range(3)):
+        return None
+    nt, nph = dims[3], dims[4]
+    t = y[3] % (2 * nt)
+    if t >= nt:
+        t = 2 * nt - t - 1
+        y[4] += nph // 2
+    y[3] = t
+    y[4] %= nph
+    return tuple(y)
+
+
+def untied_active_differences(params, values, act_ref, act):
+    """Cells whose activeNeighs differ other than by the side of an exactly tied symmetric pair."""
+    dims = values.shape
+    forward = params["model"] == "ReedsSheppForward3"
+    off, _ = O.rs3_stencil(dims[3], dims[4], float(params["gridScale"]), float(params.get("xi", 1.0)),
+                           float(params.get("eps", 0.1)), bool(params.get("dual", 0.0)), forward)
+    nfwd = 6 if forward else 0
+    bad = []
+    for lin in np.flatnonzero(act_ref.ravel() != act.ravel()):
+        x = np.unravel_index(lin, dims)
+        cls = x[3] * dims[4] + x[4]
+        diff = int(act_ref.ravel()[lin]) ^ int(act.ravel()[lin])
+        if diff & ((1 << nfwd) - 1):  # forward differences have no tie rule
+            bad.append(int(lin))
+            continue
+        for k in range(nfwd, 8):
+            if not (diff >> (nfwd + 2 * (k - nfwd))) & 3:
+                continue
+            yp = _neighbor(dims, x, off[cls, k])
+            ym = _neighbor(dims, x, -off[cls, k].astype(int))
+            if yp is None or ym is None or values[yp] != values[ym]:
+                bad.append(int(lin))
+                break
+    return bad
+
+
+@pytest.mark.parametrize("name", RS3_FIXTURES)
+def test_rs3_golden(name):
+    params, ref, _ = load_golden(name)
+    out = H.run(dict(params, verbosity=0.0, exportActiveNeighs=1.0))
+    assert out["values"].shape == ref["values"].shape
+    assert rel_err(ref["values"], out["values"]) <= FP64_RTOL
+    assert int(out["nAccepted"]) == int(ref["nAccepted"])
+    assert int(out["MaxStencilWidth"]) == int(ref["MaxStencilWidth"])
+    same = np.mean(ref["values"] == out["values"])
+    assert same > 0.99, f"only {same:.4f} of the cells are bit-identical"
+    untied = untied_active_differences(params, ref["values"], ref["activeNeighs"].astype(np.uint64),
+                                       out["activeNeighs"].astype(np.uint64))
+    assert not untied, f"activeNeighs differ away from exact ties at cells {untied[:10]}"
+
+
+@pytest.mark.parametrize("kw", [dict(cost="spatial"), dict(cost="full", dual=True, seed=41),
+                                dict(cost="angular", projective=True, seed=42, n_seeds=3),
+                                dict(cost="spatial", seed=46, forward=True)])
+def test_rs3_against_oracle_at_24(kw):
+    forward = kw.pop("forward", False)
+    p = W.reedsshepp3_case(24, 8, **kw)
+    if forward:
+        p["model"] = "ReedsSheppForward3"
+        del p["dual"], p["projective"]
+    out = H.run(dict(p, verbosity=0.0))
+    res = O.rs3_solve(p)
+    assert rel_err(res["values"], out["values"]) <= FP64_RTOL
+    assert int(out["nAccepted"]) == res["nAccepted"]
+    assert int(out["MaxStencilWidth"]) == res["MaxStencilWidth"]
+
+
+def test_rs3_fp32_close_to_fp64():
+    p = W.reedsshepp3_case(20, 8, seed=43)
+    o64 = H.run(dict(p, verbosity=0.0))
+    o32 = H.run(dict(p, verbosity=0.0, solverPrecision="float32"))
+    assert rel_err(o64["values"], o32["values"]) <= 1e-5
+
+
+def test_rs3_seed_across_the_pole_and_origin():
+    """A seed given beyond theta = pi lands on the reflected index with phi turned by pi
+    (PeriodicGrid.hxx:128-146); an origin shifts the spatial axes only."""
+    p = W.reedsshepp3_case(12, 6, seed=44, cost="constant")
+    ds = 2 * math.pi / 12
+    p["origin"] = np.array([0.25, -0.5, 0.125])
+    p["seeds"] = np.array([[0.8, -0.1, 0.6, math.pi + 0.5 * ds, 0.3]])
+    out = H.run(dict(p, verbosity=0.0))
+    res = O.rs3_solve(p)
+    assert rel_err(res["values"], out["values"]) <= FP64_RTOL
+    assert int(out["nAccepted"]) == res["nAccepted"]
+
+
+def test_rs3_unsupported_keys_are_refused():
+    p = W.reedsshepp3_case(8, 4, seed=45)
+    with pytest.raises(Exception, match="not supported"):
+        H.run(dict(p, verbosity=0.0, walls=np.zeros((8, 8, 8, 4, 8))))
+    with pytest.raises(Exception, match="not supported"):
+        H.run(dict(p, verbosity=0.0, inspectSensitivity=p["seeds"]))
+    with pytest.raises(Exception, match="inconsistent bundle dimensions"):
+        H.run(dict(p, verbosity=0.0, dims=np.array([8, 8, 8, 4, 12], float)))
