@@ -28,6 +28,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -389,10 +390,21 @@ struct hfm_server {
                 for (const auto &f : fams)
                     if (f.second->has_work() || f.second->has_pending()) keys.push_back(f.first);
                 if (!keys.empty()) {
-                    // the next family after the previous slice's, in key order (keys are sorted)
+                    // the family of the oldest admitted request goes next, so that no request waits
+                    // behind the slices of families that arrived after it (the shortest longest
+                    // wait); without one, the next family after the previous slice's, in key order
+                    // (keys are sorted)
                     std::string key = keys.front();
                     for (const std::string &k : keys)
                         if (k > last) { key = k; break; }
+                    double oldest = std::numeric_limits<double>::infinity();
+                    for (const auto &kv : running) {
+                        const Request *r = kv.second;
+                        if (r->t_submit < oldest && std::binary_search(keys.begin(), keys.end(), r->family)) {
+                            oldest = r->t_submit;
+                            key = r->family;
+                        }
+                    }
                     last = key;
                     hfm::ResidentFamily &F = *fams[key];
                     try {

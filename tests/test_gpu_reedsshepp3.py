@@ -7,6 +7,13 @@ marching's accumulation order is reproduced, so most cells are bit-identical); n
 MaxStencilWidth exact; activeNeighs
 equal except where a symmetric difference's two neighbours hold exactly the same value; FP32
 within 1e-5 of FP64.
+
+Bit-identical cells: more than 99 %, except on rs3_12x6_xi1 (97.9 %). There fast marching accepts 6
+cells at the value of an earlier queue entry, one unit in the last place below the value it
+exports (a later re-update of the cell rounded up, HamiltonFastMarching.hxx:86-112 passes the
+queue entry's value to the neighbours' updates); the neighbours are computed from the smaller
+value, and the last-bit differences reach 2 % of the grid. This solver computes the neighbours
+from the exported value.
 """
 import math
 
@@ -21,6 +28,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 RS3_FIXTURES = ["rs3_10x6", "rs3_8x4_dual", "rs3_8x4_projective", "rs3_12x6_xi1", "rsf3_10x6", "rsf3_8x4_angular"]
+BIT_IDENTICAL = {"rs3_12x6_xi1": 0.97}
 FP64_RTOL = 1e-10
 
 
@@ -81,7 +89,7 @@ def test_rs3_golden(name):
     assert int(out["nAccepted"]) == int(ref["nAccepted"])
     assert int(out["MaxStencilWidth"]) == int(ref["MaxStencilWidth"])
     same = np.mean(ref["values"] == out["values"])
-    assert same > 0.99, f"only {same:.4f} of the cells are bit-identical"
+    assert same > BIT_IDENTICAL.get(name, 0.99), f"only {same:.4f} of the cells are bit-identical"
     untied = untied_active_differences(params, ref["values"], ref["activeNeighs"].astype(np.uint64),
                                        out["activeNeighs"].astype(np.uint64))
     assert not untied, f"activeNeighs differ away from exact ties at cells {untied[:10]}"
