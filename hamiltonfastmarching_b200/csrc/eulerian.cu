@@ -150,6 +150,7 @@ struct Dev {
     const int8_t *cls_off;    // [nclass][ND][3]
     const Real *cls_w;        // [nclass][ND]
     const int8_t *cls_ang;    // [nclass][ND][2] theta and phi steps of the differences (kKindShareS2)
+    const int *cls_d2;        // [nclass][NB] third-coordinate step of each slot, periodized (kKindShareS2)
     // reverse tile dependencies: tile T -> tiles whose stencils read T, with the cells they read;
     // entries [dep_ptr[T], dep_end[T]) (dep_end null: dep_ptr[T + 1], a CSR over the tile space)
     const long long *dep_ptr;
@@ -209,15 +210,7 @@ struct Dev {
 // (dz, dtheta, dphi) from w is periodized as PeriodicGrid.hxx:120-160 does: z is closed, theta
 // reflects at the poles (index 2 ntheta - 1 - t) while phi turns by nphi / 2, phi wraps. False
 // where the step leaves the domain.
-__host__ __device__ __forceinline__ bool s2_step(const Inst &I, int x2, int dz, int dth, int dph, int &y2) {
-    const int nth = I.nth, nph = I.nph, nang = nth * nph;
-    int z = x2 / nang;
-    const int r = x2 - z * nang;
-    int th = r / nph, ph = r - th * nph;
-    z += dz;
-    if (z < 0 || z >= I.g.dims[2] / nang) return false;
-    th += dth;
-    ph += dph;
+__host__ __device__ __forceinline__ void s2_wrap(int nth, int nph, int &th, int &ph) {
     th %= 2 * nth;
     if (th < 0) th += 2 * nth;
     if (th >= nth) {
@@ -226,6 +219,16 @@ __host__ __device__ __forceinline__ bool s2_step(const Inst &I, int x2, int dz, 
     }
     ph %= nph;
     if (ph < 0) ph += nph;
+}
+
+__host__ __device__ __forceinline__ bool s2_step(const Inst &I, int x2, int dz, int dth, int dph, int &y2) {
+    const int nth = I.nth, nph = I.nph, nang = nth * nph;
+    int z = x2 / nang;
+    const int r = x2 - z * nang;
+    int th = r / nph + dth, ph = r % nph + dph;
+    z += dz;
+    if (z < 0 || z >= I.g.dims[2] / nang) return false;
+    s2_wrap(nth, nph, th, ph);
     y2 = (z * nth + th) * nph + ph;
     return true;
 }
@@ -235,6 +238,18 @@ template <int KIND>
 __host__ __device__ __forceinline__ long long share_class(const Inst &I, int x2) {
     if constexpr (KIND == kKindShareS2) return I.cls0 + x2 % (I.nth * I.nph);
     else return I.cls0 + x2;
+}
+
+// Neighbour through slot `slot` of class cls (kKindShareS2) of a cell whose visibility bit for
+// that slot is set (so the step stays in the domain): the x, y steps of the difference and the
+// periodized third-coordinate step of the slot's table.
+template <typename Real, int ND, int NB>
+__device__ __forceinline__ void s2_visible_neighbor(const Dev<Real> &P, long long cls, int k, int slot, int s, int x0,
+                                                    int x1, int x2, int &y0, int &y1, int &y2) {
+    const int8_t *o = P.cls_off + (cls * ND + k) * 3;
+    y0 = x0 + s * __ldg(o);
+    y1 = x1 + s * __ldg(o + 1);
+    y2 = x2 + __ldg(P.cls_d2 + cls * NB + slot);
 }
 
 // Neighbour y = x + s e of difference k of class cls (kKindShareS2): false outside the domain.
@@ -492,9 +507,15 @@ __device__ __forceinline__ Real solve_cell_stencil(const Dev<Real> &P, const Ins
         Real val = INF;
         if constexpr (KIND == kKindShareS2) {
             // the visibility bits hold only steps that stay in the domain
+            constexpr int NB = NFWD + 2 * NSYM;
+            const int slot = k < NFWD ? k : NFWD + 2 * (k - NFWD);
             int y0, y1, y2;
-            if (vp && s2_neighbor<Real, ND>(P, I, cls, k, 1, x0, x1, x2, y0, y1, y2)) val = fetch_at(y0, y1, y2);
-            if (vm && s2_neighbor<Real, ND>(P, I, cls, k, -1, x0, x1, x2, y0, y1, y2)) {
+            if (vp) {
+                s2_visible_neighbor<Real, ND, NB>(P, cls, k, slot, 1, x0, x1, x2, y0, y1, y2);
+                val = fetch_at(y0, y1, y2);
+            }
+            if (vm) {
+                s2_visible_neighbor<Real, ND, NB>(P, cls, k, slot + 1, -1, x0, x1, x2, y0, y1, y2);
                 const Real vv = fetch_at(y0, y1, y2);
                 if (vv < val) { val = vv; if (k >= NFWD) sides |= 1u << (k - NFWD); }
             }
@@ -779,7 +800,8 @@ __device__ __forceinline__ unsigned long long intile_reads(const Dev<Real> &P, c
             const int s = si ? -1 : 1;
             int n0 = x0 + s * o0, n1 = x1 + s * o1, n2 = x2 + s * o2;
             if constexpr (KIND == kKindShareS2) {
-                if (!s2_neighbor<Real, ND>(P, I, cls, k, s, x0, x1, x2, n0, n1, n2)) continue;
+                s2_visible_neighbor<Real, ND, NFWD + 2 * NSYM>(P, cls, k, k < NFWD ? k : NFWD + 2 * (k - NFWD) + si, s,
+                                                              x0, x1, x2, n0, n1, n2);
             } else if (SHARE && g.periodic[2]) {
                 n2 %= g.dims[2];
                 if (n2 < 0) n2 += g.dims[2];
@@ -2391,6 +2413,7 @@ struct Retained final : RetainedSolve {
     DeviceBuffer<unsigned> status, code, vis;
     DeviceBuffer<Real> values, weight, mult, cls_w;
     DeviceBuffer<int8_t> cls_off, cls_ang;
+    DeviceBuffer<int> cls_d2;
     DeviceBuffer<TTICell> tti;
     DeviceBuffer<double> diag;  // per-axis speeds of a Diagonal model (P.diag_src points here)
     void adjoint(const EulerProblem &p, EulerResult &res) override {
@@ -2498,6 +2521,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     DeviceBuffer<unsigned> code, vis, maxw(ninst);
     DeviceBuffer<Real> weight, mult, cls_w;
     DeviceBuffer<int8_t> cls_off, cls_ang, plain_off;
+    DeviceBuffer<int> cls_d2;
     DeviceBuffer<uint8_t> cls_en;
     DeviceBuffer<double> metric, plain_w, mult_rm, kscale;
     DeviceBuffer<TTICell> ttibuf;
@@ -2592,6 +2616,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
     } else {
         std::vector<Real> hw;
         std::vector<int8_t> ho, ha;
+        std::vector<int> hd2;
         std::vector<uint8_t> he;
         mult_rm.alloc(std::max(1ll, nmult));
         for (int i = 0; i < ninst; ++i) {
@@ -2602,6 +2627,19 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
                 if (p.cls_ang.size() != (size_t)p.nclass * ND * 2)
                     throw Error(HFM_ERR_VALUE, "sphere-bundle stencils need their angular steps");
                 ha.insert(ha.end(), p.cls_ang.begin(), p.cls_ang.end());
+                // third-coordinate step of each slot of a class (theta, phi) = (cl / nphi, cl % nphi):
+                // s dz ntheta nphi plus the periodized angular step (the same for every z)
+                const int nth = hinst[i].nth, nph = hinst[i].nph;
+                for (int cl = 0; cl < p.nclass; ++cl)
+                    for (int k = 0; k < ND; ++k)
+                        for (int si = 0; si < (k < NFWD ? 1 : 2); ++si) {
+                            const int sg = si ? -1 : 1;
+                            const int8_t *o = &p.cls_off[(cl * ND + k) * 3];
+                            const int8_t *a = &p.cls_ang[(cl * ND + k) * 2];
+                            int th = cl / nph + sg * a[0], ph = cl % nph + sg * a[1];
+                            s2_wrap(nth, nph, th, ph);
+                            hd2.push_back(sg * o[2] * nth * nph + (th * nph + ph) - cl);
+                        }
             }
             he.insert(he.end(), p.cls_enabled.begin(), p.cls_enabled.end());
             const long long len = (i + 1 < ninst ? hinst[i + 1].mult0 : nmult) - hinst[i].mult0;
@@ -2643,6 +2681,8 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         if (KIND == kKindShareS2) {
             cls_ang.upload(ha, s);
             P.cls_ang = cls_ang.get();
+            cls_d2.upload(hd2, s);
+            P.cls_d2 = cls_d2.get();
         }
         mult.alloc(ntc);
         mult.zero(s);
@@ -2989,6 +3029,7 @@ void run_batch_impl(const std::vector<const EulerProblem *> &probs, std::vector<
         r->cls_w = std::move(cls_w);
         r->cls_off = std::move(cls_off);
         r->cls_ang = std::move(cls_ang);
+        r->cls_d2 = std::move(cls_d2);
         r->tti = std::move(ttibuf);
         if (p0.diagonal) r->diag = std::move(metric);
         results[0].retained = r;

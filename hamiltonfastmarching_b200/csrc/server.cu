@@ -46,6 +46,9 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Age after which an admitted request's family takes the GPU ahead of the turn order.
+constexpr double kStarveSeconds = 0.25;
+
 struct Request {
     uint64_t ticket = 0;
     hfm_io *io = nullptr;
@@ -390,14 +393,15 @@ struct hfm_server {
                 for (const auto &f : fams)
                     if (f.second->has_work() || f.second->has_pending()) keys.push_back(f.first);
                 if (!keys.empty()) {
-                    // the family of the oldest admitted request goes next, so that no request waits
-                    // behind the slices of families that arrived after it (the shortest longest
-                    // wait); without one, the next family after the previous slice's, in key order
-                    // (keys are sorted)
+                    // families take turns, the next after the previous slice's in key order (keys
+                    // are sorted), so that small requests pass between the slices of large ones;
+                    // but the family of the oldest admitted request goes first once that request
+                    // has waited kStarveSeconds, so that a large request is not slowed without
+                    // bound by the families that keep arriving after it
                     std::string key = keys.front();
                     for (const std::string &k : keys)
                         if (k > last) { key = k; break; }
-                    double oldest = std::numeric_limits<double>::infinity();
+                    double oldest = now() - kStarveSeconds;
                     for (const auto &kv : running) {
                         const Request *r = kv.second;
                         if (r->t_submit < oldest && std::binary_search(keys.begin(), keys.end(), r->family)) {

@@ -139,3 +139,17 @@ def test_rs3_unsupported_keys_are_refused():
         H.run(dict(p, verbosity=0.0, inspectSensitivity=p["seeds"]))
     with pytest.raises(Exception, match="inconsistent bundle dimensions"):
         H.run(dict(p, verbosity=0.0, dims=np.array([8, 8, 8, 4, 12], float)))
+
+
+def test_rs3_batch_equals_alone():
+    """Uneven ReedsShepp3 instances (and a ReedsSheppForward3 one, its own family) in one
+    hfm_run_batch call: each returns what its solve alone returns."""
+    cases = [W.reedsshepp3_case(n, nt, seed=60 + n) for n, nt in ((12, 4), (16, 6), (10, 4))]
+    fwd = W.reedsshepp3_case(12, 4, seed=70)
+    fwd["model"] = "ReedsSheppForward3"
+    del fwd["dual"], fwd["projective"]
+    cases.insert(1, fwd)
+    out = H.run_batch([dict(p, verbosity=0.0) for p in cases])
+    for p, o in zip(cases, out):
+        alone = H.run(dict(p, verbosity=0.0))["values"]
+        assert rel_err(alone, o["values"]) <= FP64_RTOL
