@@ -30,6 +30,8 @@ SPACE = {
         "2d": [(8, 8), (16, 4), (4, 16)],
         "3d": [(4, 4, 4), (8, 4, 2), (2, 4, 8), (4, 8, 2)],
         "lifted": [(4, 4, 4), (8, 8, 1), (2, 2, 16), (8, 4, 2)],
+        # ReedsShepp3: (x, y, (z, theta, phi)) as the solver holds the sphere bundle
+        "sphere": [(4, 4, 4), (8, 8, 1), (2, 4, 8), (8, 4, 2)],
     },
 }
 # The library's default schedule per model (default_schedule in the solver), the search's start.
@@ -44,6 +46,8 @@ DEFAULT = {
     "ReedsSheppForward2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
     "Elastica2": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
     "TTI3": {"tileSweeps": 1, "queue": ("band", 1.0, 4.0)},
+    "ReedsShepp3": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
+    "ReedsSheppForward3": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
 }
 _LIFTED = ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")
 
@@ -51,6 +55,8 @@ _LIFTED = ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")
 def _domain_kind(params: Dict) -> str:
     if params["model"] in _LIFTED:
         return "lifted"
+    if params["model"] in ("ReedsShepp3", "ReedsSheppForward3"):
+        return "sphere"
     return "2d" if len(np.asarray(params["dims"]).ravel()) == 2 else "3d"
 
 
