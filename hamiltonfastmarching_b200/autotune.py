@@ -25,7 +25,7 @@ __all__ = ["Autotuner", "family_key", "SPACE"]
 # Candidates per parameter; tile shapes per domain kind (extents per axis, 64 cells).
 SPACE = {
     "tileSweeps": [1, 2, 3, 4, 6],
-    "queue": [("band", 1.0, 4.0), ("band", 2.0, 8.0), ("band", 4.0, 16.0), ("fifo", None, None)],
+    "queue": [("band", 0.5, 4.0), ("band", 1.0, 4.0), ("band", 2.0, 8.0), ("band", 4.0, 16.0), ("fifo", None, None)],
     "tileShape": {
         "2d": [(8, 8), (16, 4), (4, 16)],
         "3d": [(4, 4, 4), (8, 4, 2), (2, 4, 8), (4, 8, 2)],
@@ -36,12 +36,12 @@ SPACE = {
 }
 # The library's default schedule per model (default_schedule in the solver), the search's start.
 DEFAULT = {
-    "Riemann3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
+    "Riemann3": {"tileSweeps": 2, "queue": ("band", 0.5, 4.0)},
     "Riemann2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
     "Isotropic2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
-    "Isotropic3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
+    "Isotropic3": {"tileSweeps": 2, "queue": ("band", 0.5, 4.0)},
     "Diagonal2": {"tileSweeps": 3, "queue": ("band", 2.0, 8.0)},
-    "Diagonal3": {"tileSweeps": 2, "queue": ("band", 1.0, 4.0)},
+    "Diagonal3": {"tileSweeps": 2, "queue": ("band", 0.5, 4.0)},
     "ReedsShepp2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
     "ReedsSheppForward2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
     "Elastica2": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},

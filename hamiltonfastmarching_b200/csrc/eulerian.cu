@@ -3140,7 +3140,7 @@ void default_schedule(EulerProblem &p) {
     if (p.kind == StencilKind::TTI) { p.sweeps_per_tile = 1; p.band_lo = 1; p.band_hi = 4; }
     else if (p.kind == StencilKind::SharedByTheta && p.angular && p.nfwd + p.nsym > 4) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
     else if (p.kind == StencilKind::SharedByTheta && p.angular) { p.sweeps_per_tile = 4; p.band_lo = 2; p.band_hi = 8; }
-    else if (p.ndim == 3) { p.sweeps_per_tile = 2; p.band_lo = 1; p.band_hi = 4; }
+    else if (p.ndim == 3) { p.sweeps_per_tile = 2; p.band_lo = 0.5; p.band_hi = 4; }
     else { p.sweeps_per_tile = 3; p.band_lo = 2; p.band_hi = 8; }
 }
 
