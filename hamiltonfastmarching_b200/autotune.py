@@ -31,7 +31,7 @@ SPACE = {
         "3d": [(4, 4, 4), (8, 4, 2), (2, 4, 8), (4, 8, 2)],
         "lifted": [(4, 4, 4), (8, 8, 1), (2, 2, 16), (8, 4, 2)],
         # ReedsShepp3: (x, y, (z, theta, phi)) as the solver holds the sphere bundle
-        "sphere": [(4, 4, 4), (8, 8, 1), (2, 4, 8), (8, 4, 2)],
+        "sphere": [(8, 8, 1), (4, 4, 4), (16, 4, 1), (8, 4, 2)],
     },
 }
 # The library's default schedule per model (default_schedule in the solver), the search's start.
@@ -46,8 +46,8 @@ DEFAULT = {
     "ReedsSheppForward2": {"tileSweeps": 4, "queue": ("band", 2.0, 8.0)},
     "Elastica2": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
     "TTI3": {"tileSweeps": 1, "queue": ("band", 1.0, 4.0)},
-    "ReedsShepp3": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
-    "ReedsSheppForward3": {"tileSweeps": 2, "queue": ("band", 4.0, 16.0)},
+    "ReedsShepp3": {"tileSweeps": 1, "queue": ("band", 4.0, 16.0)},
+    "ReedsSheppForward3": {"tileSweeps": 1, "queue": ("band", 4.0, 16.0)},
 }
 _LIFTED = ("ReedsShepp2", "ReedsSheppForward2", "Elastica2")
 

@@ -3138,6 +3138,12 @@ void solve_eulerian_batch(const std::vector<const EulerProblem *> &probs, std::v
 
 void default_schedule(EulerProblem &p) {
     if (p.kind == StencilKind::TTI) { p.sweeps_per_tile = 1; p.band_lo = 1; p.band_hi = 4; }
+    else if (p.sphere_nth > 0) {
+        // ReedsShepp3: 8 x 8 x 1 tiles (one (z, theta, phi) column of 64 (x, y) cells) and one sweep
+        // per activation measured 11-19 % faster than 4 x 4 x 4 with two sweeps
+        p.sweeps_per_tile = 1; p.band_lo = 4; p.band_hi = 16;
+        if (p.tile_shift[0] < 0) { p.tile_shift[0] = 3; p.tile_shift[1] = 3; p.tile_shift[2] = 0; }
+    }
     else if (p.kind == StencilKind::SharedByTheta && p.angular && p.nfwd + p.nsym > 4) { p.sweeps_per_tile = 2; p.band_lo = 4; p.band_hi = 16; }
     else if (p.kind == StencilKind::SharedByTheta && p.angular) { p.sweeps_per_tile = 4; p.band_lo = 2; p.band_hi = 8; }
     else if (p.ndim == 3) { p.sweeps_per_tile = 2; p.band_lo = 0.5; p.band_hi = 4; }
