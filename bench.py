@@ -729,9 +729,16 @@ def run_ours(args):
             "differentiation": diff,
             "geodesics": geo,
         }
-        # compact digest last, so that a reader keeping only the end of the line still has it
-        line["summary"] = summarize(line)
-        print(json.dumps(line), flush=True)
+        # the compact digest (batch and serving speed-ups, p50/p99, FP32 errors) goes right after the
+        # headline keys, before the long per-leg data, so that a record keeping only the beginning
+        # of the line still has it
+        digest = summarize(line)
+        ordered = {}
+        for k, v in line.items():
+            ordered[k] = v
+            if k == "gpu_launches":
+                ordered["summary"] = digest
+        print(json.dumps(ordered), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
