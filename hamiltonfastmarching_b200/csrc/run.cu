@@ -12,11 +12,13 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
 #include <limits>
 #include <set>
 #include <sstream>
+#include <thread>
 
 #include "common.cuh"
 #include "io.hpp"
@@ -317,19 +319,39 @@ void riemann_cell_stencil(const EulerProblem &p, const Param &pm, int64_t lin, i
     if (!ok) throw Error(HFM_ERR_VALUE, "Error : metric is not positive definite");
 }
 
+// Largest offset component over every cell's stencil (the search box of the reversed offsets).
+// The width is needed before any device work; the cells are split among host threads, since one
+// Selling decomposition per cell of a large grid takes seconds on one core.
 int riemann_max_width(const EulerProblem &p, const Param &pm) {
     int64_t ncell = 1;
     for (int a = 0; a < pm.ndim; ++a) ncell *= pm.dims[a];
-    int width = 0;
-    for (int64_t lin = 0; lin < ncell; ++lin) {
-        int off[6][3];
-        double w[6];
-        riemann_cell_stencil(p, pm, lin, off, w);
-        for (int k = 0; k < (pm.ndim == 2 ? 3 : 6); ++k)
-            for (int a = 0; a < pm.ndim; ++a) width = std::max(width, std::abs(off[k][a]));
-        if (p.metric_constant) break;
-    }
-    return width;
+    if (p.metric_constant) ncell = 1;
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(hw, ncell / 65536));
+    std::vector<int> widths(nt, 0);
+    std::vector<std::exception_ptr> errors(nt);
+    auto work = [&](int t) {
+        try {
+            int width = 0;
+            for (int64_t lin = ncell * t / nt; lin < ncell * (t + 1) / nt; ++lin) {
+                int off[6][3];
+                double w[6];
+                riemann_cell_stencil(p, pm, lin, off, w);
+                for (int k = 0; k < (pm.ndim == 2 ? 3 : 6); ++k)
+                    for (int a = 0; a < pm.ndim; ++a) width = std::max(width, std::abs(off[k][a]));
+            }
+            widths[t] = width;
+        } catch (...) {
+            errors[t] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (std::thread &th : pool) th.join();
+    for (const std::exception_ptr &e : errors)
+        if (e) std::rethrow_exception(e);
+    return *std::max_element(widths.begin(), widths.end());
 }
 
 std::vector<std::array<int, 3>> reversed_offsets(const EulerProblem &p, const Param &pm, const int64_t *x, int width) {
