@@ -953,7 +953,7 @@ void setup_reedsshepp3(Store &io, Param &pm, EulerProblem &p, bool forward) {
     static const char *kRefused[] = {"walls",        "seeds_Unoriented",     "stopWhenAnyAccepted_Unoriented",
                                      "stopWhenAllAccepted_Unoriented", "tips", "tips_Unoriented",
                                      "inspectSensitivity", "costVariation", "seedValueVariation",
-                                     "values",       "activeNeighs",         "getStencils"};
+                                     "values",       "activeNeighs"};
     for (const char *k : kRefused)
         if (io.has_field(k))
             throw Error(HFM_ERR_UNSUPPORTED, name + " with " + k + " is not supported by the GPU solve path");
@@ -1300,29 +1300,33 @@ void export_stencils(Store &io, const Prepared &q, const EulerResult &r) {
     const Param &pm = q.pm;
     const int D = pm.ndim;
     std::ostringstream o;
-    auto diff = [&](double w, const int8_t *off) {
+    // a difference's offset: its D components (the sphere bundle's are the x, y, z steps followed by
+    // the theta and phi steps)
+    auto diff = [&](double w, const int8_t *off, const int8_t *ang = nullptr) {
         o << "{" << w << ",{";
-        for (int a = 0; a < D; ++a) o << (a ? "," : "") << (int)off[a];
+        for (int a = 0; a < D; ++a) o << (a ? "," : "") << (int)(a < 3 || !ang ? off[a] : ang[a - 3]);
         o << "}}";
     };
     o << "{";
     for (int64_t x : q.stencil_cells) {
-        int64_t idx[3], rr = x;
+        int64_t idx[5], rr = x;
         for (int a = D - 1; a >= 0; --a) { idx[a] = rr % pm.dims[a]; rr /= pm.dims[a]; }
         o << "{{";
         for (int a = 0; a < D; ++a) o << (a ? "," : "") << idx[a];
         o << "},{\"forward\" -> {{";
         if (p.kind == StencilKind::SharedByTheta) {
             const int ND = p.nfwd + p.nsym;
-            const int64_t cls = p.nclass > 1 ? idx[2] : 0;
+            const bool s2 = p.sphere_nth > 0;
+            const int64_t cls = s2 ? idx[3] * p.sphere_nph + idx[4] : p.nclass > 1 ? idx[2] : 0;
+            auto ang = [&](int k) { return s2 ? &p.cls_ang[(cls * ND + k) * 2] : nullptr; };
             for (int k = 0; k < p.nfwd; ++k) {
                 if (k) o << ",";
-                diff(p.cls_w[cls * ND + k], &p.cls_off[(cls * ND + k) * 3]);
+                diff(p.cls_w[cls * ND + k], &p.cls_off[(cls * ND + k) * 3], ang(k));
             }
             o << "}},\"symmetric\" -> {{";
             for (int k = p.nfwd; k < ND; ++k) {
                 if (k > p.nfwd) o << ",";
-                diff(p.cls_w[cls * ND + k], &p.cls_off[(cls * ND + k) * 3]);
+                diff(p.cls_w[cls * ND + k], &p.cls_off[(cls * ND + k) * 3], ang(k));
             }
         } else if (p.diagonal) {  // one difference per axis, base weight 1 / h_i^2
             o << "}},\"symmetric\" -> {{";

@@ -426,6 +426,19 @@ def reedsshepp3_fixtures():
         p["model"] = "ReedsSheppForward3"
         del p["dual"], p["projective"]
         solve_fixture(name, p)
+    # getStencils on the sphere bundle: the reference's `stencils` string at a few cells, the poles'
+    # classes included
+    for name, model in (("rs3_stencils_6x4", "ReedsShepp3"), ("rsf3_stencils_6x4", "ReedsSheppForward3")):
+        p = W.reedsshepp3_case(6, 4, seed=37, cost="constant")
+        if model != "ReedsShepp3":
+            p["model"] = model
+            del p["dual"], p["projective"]
+        ds = 2 * np.pi / 8
+        p["getStencils"] = np.array([[0.5, 0.5, 0.5, 0.5 * ds, 0.0], [0.1, 0.9, 0.3, 3.5 * ds, 5 * ds],
+                                     [0.7, 0.2, 0.6, 1.5 * ds, 2 * ds], [0.3, 0.3, 0.3, 2.5 * ds, 7 * ds]])
+        out = run_reference(p)
+        assert out["retcode"] == 0, out["log"]
+        save(name, p, out, ref_stencils=np.array(out["stencils"]))
 
 if __name__ == "__main__":
     # `make_golden.py tti|geodesic|variation|isotropic|ode|stopping|spreading|diagvar|rsf2|ttispread|dubins|

@@ -153,3 +153,12 @@ def test_rs3_batch_equals_alone():
     for p, o in zip(cases, out):
         alone = H.run(dict(p, verbosity=0.0))["values"]
         assert rel_err(alone, o["values"]) <= FP64_RTOL
+
+
+@pytest.mark.parametrize("name", ["rs3_stencils_6x4", "rsf3_stencils_6x4"])
+def test_rs3_get_stencils_string_equals_reference(name):
+    """getStencils (HFMInterface.hxx:360-375): the reference's `stencils` string at cells of several
+    (theta, phi) classes, the poles' included, character for character."""
+    params, _, extra = load_golden(name)
+    out = H.run(dict(params, verbosity=0.0))
+    assert out["stencils"] == str(extra["ref_stencils"])
