@@ -426,6 +426,13 @@ def reedsshepp3_fixtures():
         p["model"] = "ReedsSheppForward3"
         del p["dual"], p["projective"]
         solve_fixture(name, p)
+    # seeds given beyond the pole (theta > pi, reflected with phi turned by pi) and an origin
+    p = W.reedsshepp3_case(8, 4, seed=38, cost="spatial")
+    ds = 2 * np.pi / 8
+    p["origin"] = np.array([0.25, -0.5, 0.125])
+    p["seeds"] = np.array([[0.8, -0.1, 0.6, np.pi + 0.5 * ds, 0.3], [0.5, 0.2, 0.4, -0.5 * ds, 1.0]])
+    p["seedValues"] = np.array([0.0, 0.05])
+    solve_fixture("rs3_8x4_pole_seeds", p)
     # getStencils on the sphere bundle: the reference's `stencils` string at a few cells, the poles'
     # classes included
     for name, model in (("rs3_stencils_6x4", "ReedsShepp3"), ("rsf3_stencils_6x4", "ReedsSheppForward3")):
