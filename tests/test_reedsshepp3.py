@@ -5,8 +5,8 @@ the oracle against the reference's own FileHFM_ReedsShepp3 / FileHFM_ReedsSheppF
 The fixtures (tests/golden/make_golden.py rs3) cover the primal and dual models, the projective
 bundle (nphi = 4 ntheta), and a cost field over (x, y, z), over (theta, phi), over the whole grid
 and constant; ReedsSheppForward3 with a full and an angular cost; seeds given beyond the poles
-with an origin. The oracle reproduces values,
-activeNeighs, nAccepted and MaxStencilWidth bit for bit: the shared stencils (one per (theta, phi)), the Sphere2 periodization of theta and phi
+with an origin. The oracle reproduces values, activeNeighs, nAccepted and MaxStencilWidth bit for
+bit: the shared stencils (one per (theta, phi)), the Sphere2 periodization of theta and phi
 (PeriodicGrid.hxx:120-160) and the reversed offsets taken from each class's centre point
 (HFM_StencilShare.hxx:132-181).
 """
