@@ -204,12 +204,12 @@ struct Dev {
     int sweeps;
 };
 
-// Shared stencils over R^3 x S^2 (ReedsShepp3, Curvature3.h:11-70). The grid (x, y, z, theta, phi)
-// is held RowMajor as the 3-D grid (x, y, w), w = (z * ntheta + theta) * nphi + phi: values, tiles
-// and scheduling are those of a 3-D grid, and the class of a cell is its (theta, phi) pair. A step
-// (dz, dtheta, dphi) from w is periodized as PeriodicGrid.hxx:120-160 does: z is closed, theta
-// reflects at the poles (index 2 ntheta - 1 - t) while phi turns by nphi / 2, phi wraps. False
-// where the step leaves the domain.
+// Shared stencils over R^3 x S^2 (ReedsShepp3 and ReedsSheppForward3, Curvature3.h:11-107). The
+// grid (x, y, z, theta, phi) is held RowMajor as the 3-D grid (x, y, w),
+// w = (z * ntheta + theta) * nphi + phi: values, tiles and scheduling are those of a 3-D grid, and
+// the class of a cell is its (theta, phi) pair. Angular indices are periodized as
+// PeriodicGrid.hxx:120-160 does: theta reflects at the poles (index 2 ntheta - 1 - t) while phi
+// turns by nphi / 2, phi wraps.
 __host__ __device__ __forceinline__ void s2_wrap(int nth, int nph, int &th, int &ph) {
     th %= 2 * nth;
     if (th < 0) th += 2 * nth;
@@ -221,6 +221,7 @@ __host__ __device__ __forceinline__ void s2_wrap(int nth, int nph, int &th, int 
     if (ph < 0) ph += nph;
 }
 
+// Step (dz, dtheta, dphi) from third coordinate x2 (z closed): false where it leaves the domain.
 __host__ __device__ __forceinline__ bool s2_step(const Inst &I, int x2, int dz, int dth, int dph, int &y2) {
     const int nth = I.nth, nph = I.nph, nang = nth * nph;
     int z = x2 / nang;
