@@ -59,3 +59,23 @@ def test_rs3_bundle_dimensions_checked():
     bad = dict(params, dims=np.array([8, 8, 8, 4, 12], float))
     with pytest.raises(ValueError):
         O.rs3_solve(bad)
+
+
+def test_rs3_host_refusals_before_device_work():
+    """The setup checks and the refused keys of the GPU solve path answer before any device work:
+    HFM_ERR_VALUE (2) for inconsistent bundle dimensions (Curvature3.h:63-67, 97-98), and
+    HFM_ERR_UNSUPPORTED (3) for the outputs this path does not build on the sphere bundle."""
+    import hamiltonfastmarching_b200 as H
+    from hamiltonfastmarching_b200 import workloads as W
+    p = W.reedsshepp3_case(8, 4, seed=45)
+    cases = [(dict(dims=np.array([8, 8, 8, 4, 12.0])), 2, "inconsistent bundle dimensions"),
+             (dict(model="ReedsSheppForward3", projective=1.0, dims=np.array([8, 8, 8, 4, 16.0])), 2,
+              "ReedsSheppForward3 setup error"),
+             (dict(walls=np.zeros((8, 8, 8, 4, 8))), 3, "walls"),
+             (dict(inspectSensitivity=p["seeds"]), 3, "inspectSensitivity"),
+             (dict(seedRadius=1.0), 3, "seedRadius"),
+             (dict(tips=p["seeds"]), 3, "tips")]
+    for extra, code, text in cases:
+        with pytest.raises(H.PyExp) as e:
+            H.run(dict(p, verbosity=0.0, **extra))
+        assert e.value.code == code and text in str(e.value), (extra, e.value.code, str(e.value))
